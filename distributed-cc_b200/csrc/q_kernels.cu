@@ -1,0 +1,231 @@
+// (Q) denominator-and-energy loop: the reference's separate division and
+// factor kernels, and one fused per-task epilogue that evaluates
+//   t~4 = factor(abcd) * P4_444_ijkl((t4 + z4) / D)
+// and both energy dot products without writing any block back.
+#include "s4_orbit.cuh"
+
+namespace dcc {
+
+int p4_coef(const char *pattern, double alpha, double beta, P4Coef &k);
+
+struct QRange {
+    int a0, a1, b0, b1, c0, c1, d0, d1;
+};
+
+// r4[abcd][ijkl] /= D (src/rccsdt_q.c:474-588): D = ((e_i+e_j)+(e_k+e_l)) + neg,
+// neg = -(((e_a+e_b)+e_c)+e_d); exact zero where |D| <= 1e-15.
+__global__ void k_q_division(double *r4, const double *eo, const double *ev, QRange R, int bb, int bc, int bd, int no) {
+    const int64_t n4 = (int64_t)no * no * no * no;
+    const int ba_ = R.a1 - R.a0, bb_ = R.b1 - R.b0, bc_ = R.c1 - R.c0, bd_ = R.d1 - R.d0;
+    const int64_t nsub = (int64_t)ba_ * bb_ * bc_ * bd_;
+    for (int64_t s = blockIdx.y; s < nsub; s += gridDim.y) {
+        int id = (int)(s % bd_), ic = (int)((s / bd_) % bc_), ib = (int)((s / ((int64_t)bd_ * bc_)) % bb_),
+            ia = (int)(s / ((int64_t)bd_ * bc_ * bb_));
+        int a = R.a0 + ia, b = R.b0 + ib, c = R.c0 + ic, d = R.d0 + id;
+        double neg = -dadd(dadd(dadd(ev[a], ev[b]), ev[c]), ev[d]);
+        double *blk = r4 + ((((int64_t)ia * bb + ib) * bc + ic) * bd + id) * n4;
+        for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n4; e += (int64_t)gridDim.x * blockDim.x) {
+            int l = (int)(e % no), k = (int)((e / no) % no), j = (int)((e / ((int64_t)no * no)) % no),
+                i = (int)(e / ((int64_t)no * no * no));
+            double den = dadd(dadd(dadd(eo[i], eo[j]), dadd(eo[k], eo[l])), neg);
+            blk[e] = (fabs(den) > 1e-15) ? __ddiv_rn(blk[e], den) : 0.0;
+        }
+    }
+}
+
+__global__ void k_q_factor(double *t4, const double *factor, int64_t nsub, int64_t n4) {
+    for (int64_t s = blockIdx.y; s < nsub; s += gridDim.y) {
+        double f = factor[s];
+        double *blk = t4 + s * n4;
+        for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n4; e += (int64_t)gridDim.x * blockDim.x)
+            blk[e] = (f == 0.0) ? 0.0 : dmul(blk[e], f);
+    }
+}
+
+// factor of a virtual quadruple (distr_cc/rccsdt_q.py:410-428)
+__device__ __forceinline__ double q_factor(int a, int b, int c, int d) {
+    if (a < b && b < c && c < d) return 24.0;
+    if ((a == b && b < c && c < d) || (a < b && b == c && c < d) || (a < b && b < c && c == d)) return 12.0;
+    if (a == b && b < c && c == d) return 6.0;
+    return 0.0;
+}
+
+constexpr int QE_THREADS = 256;
+constexpr int QE_WARPS = QE_THREADS / 32;
+
+// One warp per (valid abcd sub-block, ijkl orbit).  Per-CTA partial sums of
+// <t~4, z4sq> and <t~4, z4> go to ws[2*cta].
+__global__ void __launch_bounds__(QE_THREADS) k_q_epilogue(const double *t4, const double *z4, const double *vvoo,
+                                                           const double *t2, const double *eo, const double *ev,
+                                                           QRange R, int blk, int no, int nv, int64_t norb,
+                                                           P4Coef k, double *ws) {
+    const int lane = threadIdx.x & 31;
+    int partner[6];
+    s4_partners(lane, partner);
+    const int64_t n4 = (int64_t)no * no * no * no;
+    const int ba = R.a1 - R.a0, bb = R.b1 - R.b0, bc = R.c1 - R.c0, bd = R.d1 - R.d0;
+    const int64_t nsub = (int64_t)ba * bb * bc * bd;
+    const int64_t total = nsub * norb;
+    const int64_t no2 = (int64_t)no * no;
+    double s_br = 0.0, s_pa = 0.0;
+    for (int64_t w = (int64_t)blockIdx.x * QE_WARPS + (threadIdx.x >> 5); w < total; w += (int64_t)gridDim.x * QE_WARPS) {
+        int64_t s = w / norb, r = w % norb;
+        int id = (int)(s % bd), ic = (int)((s / bd) % bc), ib = (int)((s / ((int64_t)bd * bc)) % bb),
+            ia = (int)(s / ((int64_t)bd * bc * bb));
+        int a = R.a0 + ia, b = R.b0 + ib, c = R.c0 + ic, d = R.d0 + id;
+        double f = q_factor(a, b, c, d);
+        if (f == 0.0) continue;  // warp-uniform: the whole sub-block contributes exactly zero
+        int asc[4], base[4], pos[4];
+        decode_tri4(r, no, asc);
+        base[0] = asc[3]; base[1] = asc[2]; base[2] = asc[1]; base[3] = asc[0];
+        int64_t off = s4_lane_offset(lane, base, no, pos);
+        int64_t q = (((int64_t)ia * blk + ib) * blk + ic) * blk + id;
+        int i = pos[0], j = pos[1], kk = pos[2], l = pos[3];
+        double zt = z4[q * n4 + off];
+        double x = dadd(t4[q * n4 + off], zt);
+        double neg = -dadd(dadd(dadd(ev[a], ev[b]), ev[c]), ev[d]);
+        double den = dadd(dadd(dadd(eo[i], eo[j]), dadd(eo[kk], eo[l])), neg);
+        x = (fabs(den) > 1e-15) ? __ddiv_rn(x, den) : 0.0;
+        double y = dmul(p4_apply(x, partner, k), f);
+        if (s4_first_holder(lane, off)) {
+            // disconnected vvoo x t2 product (distr_cc/rccsdt_q.py:1143-1150)
+#define VO(p, q_, m, n) (((int64_t)(p) * nv + (q_)) * no2 + (int64_t)(m) * no + (n))
+            double zsq = vvoo[VO(a, b, i, j)] * t2[VO(c, d, kk, l)] + vvoo[VO(a, c, i, kk)] * t2[VO(b, d, j, l)] +
+                         vvoo[VO(a, d, i, l)] * t2[VO(b, c, j, kk)] + vvoo[VO(b, c, j, kk)] * t2[VO(a, d, i, l)] +
+                         vvoo[VO(b, d, j, l)] * t2[VO(a, c, i, kk)] + vvoo[VO(c, d, kk, l)] * t2[VO(a, b, i, j)];
+#undef VO
+            s_br += y * zsq;
+            s_pa += y * zt;
+        }
+    }
+    __shared__ double red[2][QE_WARPS];
+    for (int o = 16; o > 0; o >>= 1) {
+        s_br += __shfl_down_sync(0xffffffffu, s_br, o);
+        s_pa += __shfl_down_sync(0xffffffffu, s_pa, o);
+    }
+    if (lane == 0) {
+        red[0][threadIdx.x >> 5] = s_br;
+        red[1][threadIdx.x >> 5] = s_pa;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double x = 0.0, y = 0.0;
+        for (int t = 0; t < QE_WARPS; t++) {
+            x += red[0][t];
+            y += red[1][t];
+        }
+        ws[2 * blockIdx.x] = x;
+        ws[2 * blockIdx.x + 1] = y;
+    }
+}
+
+// out[0] += B/12, out[1] += P/12 + B/12, summing the partials in a fixed order.
+__global__ void k_q_finish(const double *ws, int64_t n, double *out) {
+    __shared__ double red[2][32];
+    double x = 0.0, y = 0.0;
+    for (int64_t t = threadIdx.x; t < n; t += blockDim.x) {
+        x += ws[2 * t];
+        y += ws[2 * t + 1];
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        x += __shfl_down_sync(0xffffffffu, x, o);
+        y += __shfl_down_sync(0xffffffffu, y, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        red[0][threadIdx.x >> 5] = x;
+        red[1][threadIdx.x >> 5] = y;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double B = 0.0, P = 0.0;
+        for (int t = 0; t < (int)(blockDim.x >> 5); t++) {
+            B += red[0][t];
+            P += red[1][t];
+        }
+        double tb = B / 12.0;
+        double tp = P / 12.0 + tb;
+        out[0] += tb;
+        out[1] += tp;
+    }
+}
+
+static unsigned q_epilogue_grid(int64_t nwarps) {
+    int64_t g = (nwarps + QE_WARPS - 1) / QE_WARPS;
+    return (unsigned)(g < 148 * 16 ? (g ? g : 1) : 148 * 16);
+}
+
+}  // namespace dcc
+
+using namespace dcc;
+
+extern "C" int dcc_e_abcdijkl_division(double *r4, const double *e_occ, const double *e_vir, int64_t a0, int64_t a1,
+                                       int64_t b0, int64_t b1, int64_t c0, int64_t c1, int64_t d0, int64_t d1,
+                                       int64_t blk_a, int64_t blk_b, int64_t blk_c, int64_t blk_d, int64_t nocc,
+                                       void *stream) {
+    clear_error();
+    DCC_REQUIRE(a1 - a0 <= blk_a && b1 - b0 <= blk_b && c1 - c0 <= blk_c && d1 - d0 <= blk_d, DCC_ERR_SHAPE,
+                "virtual ranges exceed the block extents");
+    DCC_REQUIRE(a0 <= a1 && b0 <= b1 && c0 <= c1 && d0 <= d1 && nocc >= 0, DCC_ERR_SHAPE, "bad ranges");
+    int64_t nsub = (a1 - a0) * (b1 - b0) * (c1 - c0) * (d1 - d0);
+    if (nsub == 0 || nocc == 0) return DCC_OK;
+    DCC_REQUIRE(r4 && e_occ && e_vir, DCC_ERR_NULL, "NULL buffer");
+    int64_t n4 = nocc * nocc * nocc * nocc;
+    unsigned gx = ceil_div(n4, 256);
+    gx = gx > 32 ? 32 : gx;
+    dim3 grid(gx, (unsigned)(nsub < 65535 ? nsub : 65535));
+    QRange R{(int)a0, (int)a1, (int)b0, (int)b1, (int)c0, (int)c1, (int)d0, (int)d1};
+    k_q_division<<<grid, 256, 0, as_stream(stream)>>>(r4, e_occ, e_vir, R, (int)blk_b, (int)blk_c, (int)blk_d,
+                                                      (int)nocc);
+    return launch_status("e_abcdijkl_division");
+}
+
+extern "C" int dcc_t4_multiply_factor(double *t4_blk, const double *factor_blk, int64_t blk_a, int64_t blk_b,
+                                      int64_t blk_c, int64_t blk_d, int64_t nocc, void *stream) {
+    clear_error();
+    DCC_REQUIRE(blk_a >= 0 && blk_b >= 0 && blk_c >= 0 && blk_d >= 0 && nocc >= 0, DCC_ERR_SHAPE, "negative size");
+    int64_t nsub = blk_a * blk_b * blk_c * blk_d, n4 = nocc * nocc * nocc * nocc;
+    if (nsub == 0 || n4 == 0) return DCC_OK;
+    DCC_REQUIRE(t4_blk && factor_blk, DCC_ERR_NULL, "NULL buffer");
+    unsigned gx = ceil_div(n4, 256);
+    gx = gx > 32 ? 32 : gx;
+    dim3 grid(gx, (unsigned)(nsub < 65535 ? nsub : 65535));
+    k_q_factor<<<grid, 256, 0, as_stream(stream)>>>(t4_blk, factor_blk, nsub, n4);
+    return launch_status("t4_multiply_factor");
+}
+
+extern "C" size_t dcc_q_epilogue_workspace_bytes(int64_t blksize, int64_t nocc) {
+    int64_t nwarps = blksize * blksize * blksize * blksize * binom(nocc + 3, 4);
+    return (size_t)q_epilogue_grid(nwarps) * 2 * sizeof(double);
+}
+
+extern "C" int dcc_q_task_epilogue(const double *t4, const double *z4, const double *eris_vvoo,
+                                   const double *t2_vvoo, const double *e_occ, const double *e_vir, int64_t a0,
+                                   int64_t a1, int64_t b0, int64_t b1, int64_t c0, int64_t c1, int64_t d0,
+                                   int64_t d1, int64_t blksize, int64_t nocc, int64_t nvir, double *out,
+                                   void *workspace, size_t workspace_bytes, void *stream) {
+    clear_error();
+    DCC_REQUIRE(0 <= a0 && a0 <= a1 && a1 <= nvir && 0 <= b0 && b0 <= b1 && b1 <= nvir && 0 <= c0 && c0 <= c1 &&
+                    c1 <= nvir && 0 <= d0 && d0 <= d1 && d1 <= nvir,
+                DCC_ERR_SHAPE, "virtual range out of bounds");
+    DCC_REQUIRE(a1 - a0 <= blksize && b1 - b0 <= blksize && c1 - c0 <= blksize && d1 - d0 <= blksize,
+                DCC_ERR_SHAPE, "range longer than blksize");
+    DCC_REQUIRE(t4 && z4 && eris_vvoo && t2_vvoo && e_occ && e_vir && out && workspace, DCC_ERR_NULL,
+                "NULL buffer");
+    size_t need = dcc_q_epilogue_workspace_bytes(blksize, nocc);
+    DCC_REQUIRE(workspace_bytes >= need, DCC_ERR_WORKSPACE, "workspace needs %zu bytes, got %zu", need,
+                workspace_bytes);
+    P4Coef k;
+    int rc = p4_coef("P4_444", 1.0, 0.0, k);
+    if (rc) return rc;
+    int64_t norb = binom(nocc + 3, 4);
+    int64_t nwarps_grid = blksize * blksize * blksize * blksize * norb;
+    unsigned grid = q_epilogue_grid(nwarps_grid);
+    QRange R{(int)a0, (int)a1, (int)b0, (int)b1, (int)c0, (int)c1, (int)d0, (int)d1};
+    cudaStream_t st = as_stream(stream);
+    k_q_epilogue<<<grid, QE_THREADS, 0, st>>>(t4, z4, eris_vvoo, t2_vvoo, e_occ, e_vir, R, (int)blksize, (int)nocc,
+                                              (int)nvir, norb, k, (double *)workspace);
+    rc = launch_status("q_task_epilogue");
+    if (rc) return rc;
+    k_q_finish<<<1, 256, 0, st>>>((const double *)workspace, grid, out);
+    return launch_status("q_task_epilogue finish");
+}

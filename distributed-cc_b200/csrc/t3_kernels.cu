@@ -1,0 +1,627 @@
+// T3 kernels: P3 spin summation, triple-sym, transpose-add, block unpack /
+// gather, denominator division + update + norms, IJK->ABC transform and the
+// ABC block fill of the (Q) loop.
+//
+// The symmetrizers use "orbit tiles": the nvir^3 block is cut into 8^3 tiles,
+// and one CTA owns the set of tiles {sigma(I,J,K)} for a canonical I<=J<=K
+// and every axis permutation sigma.  Every position that the permutations of
+// a position in that set reach lies in the same set, so a CTA reads its tiles
+// once from HBM into shared memory, evaluates each output from six shared
+// loads, and writes each element once: the kernel moves exactly the
+// algorithmic 2 x 8 bytes per element (in place) and needs no global scratch.
+#include <stdarg.h>
+#include <string.h>
+
+#include "dcc_common.cuh"
+
+namespace dcc {
+
+constexpr int TE = 8;            // tile edge
+constexpr int TE3 = TE * TE * TE;
+constexpr int SLOT = TE * 68;    // padded tile footprint in doubles
+constexpr int OT_THREADS = 256;
+
+// Conflict-free for all six axis permutations of an 8^3 tile read by 32
+// consecutive (x,y,z) in row-major order (two lanes per 8-byte bank pair).
+__device__ __forceinline__ int sidx(int x, int y, int z) { return x * 68 + y * 8 + ((z + y) & 7); }
+
+// (t0 <= t1 <= t2) from its lexicographic rank among n tile indices.
+__device__ __forceinline__ void decode_tri3(int64_t r, int n, int &t0, int &t1, int &t2) {
+    int a = 0;
+    for (;; a++) {
+        int64_t m = (int64_t)(n - a) * (n - a + 1) / 2;
+        if (r < m) break;
+        r -= m;
+    }
+    int b = a;
+    for (;; b++) {
+        int64_t m = n - b;
+        if (r < m) break;
+        r -= m;
+    }
+    t0 = a;
+    t1 = b;
+    t2 = b + (int)r;
+}
+
+struct OrbitSet {
+    int nslot;
+    int tile[6][3];
+    int nbr[6][6];  // nbr[s][pi]: slot holding axis permutation pi of slot s's tile
+};
+
+// Thread 0 builds the distinct permuted tiles of (t0,t1,t2) and the
+// neighbour table; everybody waits.
+__device__ void build_orbit_set(OrbitSet &os, int t0, int t1, int t2) {
+    if (threadIdx.x == 0) {
+        int T[3] = {t0, t1, t2};
+        int n = 0;
+        for (int s = 0; s < 6; s++) {
+            int c[3] = {T[perm3(s, 0)], T[perm3(s, 1)], T[perm3(s, 2)]};
+            bool dup = false;
+            for (int q = 0; q < n; q++)
+                if (os.tile[q][0] == c[0] && os.tile[q][1] == c[1] && os.tile[q][2] == c[2]) dup = true;
+            if (!dup) {
+                os.tile[n][0] = c[0];
+                os.tile[n][1] = c[1];
+                os.tile[n][2] = c[2];
+                n++;
+            }
+        }
+        os.nslot = n;
+        for (int s = 0; s < n; s++)
+            for (int p = 0; p < 6; p++) {
+                int c[3] = {os.tile[s][perm3(p, 0)], os.tile[s][perm3(p, 1)], os.tile[s][perm3(p, 2)]};
+                int q = 0;
+                while (!(os.tile[q][0] == c[0] && os.tile[q][1] == c[1] && os.tile[q][2] == c[2])) q++;
+                os.nbr[s][p] = q;
+            }
+    }
+    __syncthreads();
+}
+
+// Value at axis permutation p of local position (x,y,z) in slot s.
+__device__ __forceinline__ double pv(const double *sm, const OrbitSet &os, int s, int p, int x, int y, int z) {
+    int l[3] = {x, y, z};
+    return sm[os.nbr[s][p] * SLOT + sidx(l[perm3(p, 0)], l[perm3(p, 1)], l[perm3(p, 2)])];
+}
+
+__device__ __forceinline__ void load_orbit_tiles(double *sm, const OrbitSet &os, const double *blk, int nv) {
+    for (int s = 0; s < os.nslot; s++) {
+        const int X0 = os.tile[s][0] * TE, Y0 = os.tile[s][1] * TE, Z0 = os.tile[s][2] * TE;
+        for (int e = threadIdx.x; e < TE3; e += blockDim.x) {
+            int x = e >> 6, y = (e >> 3) & 7, z = e & 7;
+            int gx = X0 + x, gy = Y0 + y, gz = Z0 + z;
+            if (gx < nv && gy < nv && gz < nv) sm[s * SLOT + sidx(x, y, z)] = blk[((int64_t)gx * nv + gy) * nv + gz];
+        }
+    }
+}
+
+struct P3Coef {
+    double p0, p1, p2, p3, p4, alpha, beta, p012, ap34;
+};
+
+// Orbit-tile kernel.  MODE 0: P3 spin summation in place (out0 == in).
+// MODE 1: triple-sym (out0..out2).  MODE 2: transpose-add (out0).
+template <int MODE>
+__global__ void __launch_bounds__(OT_THREADS) k_orbit3(const double *in, double *out0, double *out1, double *out2,
+                                                       int64_t nblocks, int nv, int ntile, P3Coef k) {
+    __shared__ double sm[6 * SLOT];
+    __shared__ OrbitSet os;
+    int t0, t1, t2;
+    decode_tri3(blockIdx.x, ntile, t0, t1, t2);
+    build_orbit_set(os, t0, t1, t2);
+    const int64_t n3 = (int64_t)nv * nv * nv;
+    for (int64_t b = blockIdx.y; b < nblocks; b += gridDim.y) {
+        const double *src = in + b * n3;
+        load_orbit_tiles(sm, os, src, nv);
+        __syncthreads();
+        for (int s = 0; s < os.nslot; s++) {
+            const int X0 = os.tile[s][0] * TE, Y0 = os.tile[s][1] * TE, Z0 = os.tile[s][2] * TE;
+            for (int e = threadIdx.x; e < TE3; e += blockDim.x) {
+                int x = e >> 6, y = (e >> 3) & 7, z = e & 7;
+                int gx = X0 + x, gy = Y0 + y, gz = Z0 + z;
+                if (gx >= nv || gy >= nv || gz >= nv) continue;
+                int64_t g = b * n3 + ((int64_t)gx * nv + gy) * nv + gz;
+                double a0 = pv(sm, os, s, 0, x, y, z);
+                if (MODE == 0) {
+                    double r;
+                    if (gx == gy && gy == gz) {
+                        r = dadd(dmul(k.beta, a0), dmul(k.ap34, dmul(k.p012, a0)));
+                    } else {
+                        // T(u) = p0 A(u) + p1 A(u2,u1,u0) + p2 A(u1,u0,u2); T at (u0,u2,u1)
+                        double tu = dadd(dadd(dmul(k.p0, a0), dmul(k.p1, pv(sm, os, s, 5, x, y, z))),
+                                         dmul(k.p2, pv(sm, os, s, 2, x, y, z)));
+                        double tw = dadd(dadd(dmul(k.p0, pv(sm, os, s, 1, x, y, z)), dmul(k.p1, pv(sm, os, s, 3, x, y, z))),
+                                         dmul(k.p2, pv(sm, os, s, 4, x, y, z)));
+                        r = dadd(dmul(k.beta, a0), dmul(k.alpha, dadd(dmul(k.p3, tu), dmul(k.p4, tw))));
+                    }
+                    out0[g] = r;
+                } else if (MODE == 1) {
+                    double bac = pv(sm, os, s, 2, x, y, z), acb = pv(sm, os, s, 1, x, y, z),
+                           cba = pv(sm, os, s, 5, x, y, z);
+                    double two = dmul(2.0, a0);
+                    double d0 = dsub(dsub(two, acb), cba);
+                    out0[g] = d0;
+                    out1[g] = dsub(dsub(two, bac), acb);
+                    out2[g] = dsub(dadd(d0, acb), bac);
+                } else {
+                    out0[g] = dadd(a0, pv(sm, os, s, 4, x, y, z));
+                }
+            }
+        }
+        __syncthreads();
+    }
+}
+
+int p3_pattern(const char *name, double p[5]) {
+    static const struct {
+        const char *n;
+        double c[5];
+    } tab[] = {{"P3_full", {1.0, 1.0, 1.0, 1.0, 1.0}},
+               {"P3_422", {2.0, -1.0, -1.0, 2.0, -1.0}},
+               {"P3_201", {2.0, -1.0, -1.0, 1.0, 0.0}}};
+    if (!name) return -1;
+    for (auto &t : tab)
+        if (strcmp(name, t.n) == 0) {
+            memcpy(p, t.c, sizeof(t.c));
+            return 0;
+        }
+    return -1;
+}
+
+static int orbit3_launch(int mode, const double *in, double *o0, double *o1, double *o2, int64_t nblocks,
+                         int64_t nvir, const P3Coef &k, void *stream) {
+    if (nblocks == 0 || nvir == 0) return DCC_OK;
+    int ntile = (int)ceil_div(nvir, TE);
+    int64_t ntri = (int64_t)ntile * (ntile + 1) * (ntile + 2) / 6;
+    dim3 grid((unsigned)ntri, (unsigned)(nblocks < 65535 ? nblocks : 65535));
+    cudaStream_t st = as_stream(stream);
+    if (mode == 0)
+        k_orbit3<0><<<grid, OT_THREADS, 0, st>>>(in, o0, o1, o2, nblocks, (int)nvir, ntile, k);
+    else if (mode == 1)
+        k_orbit3<1><<<grid, OT_THREADS, 0, st>>>(in, o0, o1, o2, nblocks, (int)nvir, ntile, k);
+    else
+        k_orbit3<2><<<grid, OT_THREADS, 0, st>>>(in, o0, o1, o2, nblocks, (int)nvir, ntile, k);
+    return launch_status("orbit-tile T3 kernel");
+}
+
+// ---------------------------------------------------------------- unpack
+
+// out[n] = T3[ijk[n]] for any ordering; one CTA per (8^3 output tile, n).
+__global__ void __launch_bounds__(OT_THREADS) k_take_t3(const double *t3, double *out, const int32_t *ijk,
+                                                        const int64_t *loc, int64_t count, int nocc, int nv,
+                                                        int ntile) {
+    __shared__ double sm[SLOT];
+    const int64_t n3 = (int64_t)nv * nv * nv;
+    int T[3] = {(int)(blockIdx.x / (ntile * ntile)), (int)((blockIdx.x / ntile) % ntile), (int)(blockIdx.x % ntile)};
+    for (int64_t n = blockIdx.y; n < count; n += gridDim.y) {
+        int64_t s[3];
+        int i = ijk[3 * n], j = ijk[3 * n + 1], k = ijk[3 * n + 2];
+        bool ok = i >= 0 && j >= 0 && k >= 0 && i < nocc && j < nocc && k < nocc;
+        int cs = order_case3(ok ? i : 0, ok ? j : 0, ok ? k : 0, s);
+        int64_t l = ok ? loc[ijk_linear(s[0], s[1], s[2], nocc)] : -1;
+        double *dst = out + n * n3;
+        // output tile T <- source tile V with V[perm3(cs,m)] = T[m]
+        int V[3];
+        for (int m = 0; m < 3; m++) V[perm3(cs, m)] = T[m];
+        if (l >= 0) {
+            const double *src = t3 + l * n3;
+            for (int e = threadIdx.x; e < TE3; e += blockDim.x) {
+                int x = e >> 6, y = (e >> 3) & 7, z = e & 7;
+                int gx = V[0] * TE + x, gy = V[1] * TE + y, gz = V[2] * TE + z;
+                if (gx < nv && gy < nv && gz < nv) sm[sidx(x, y, z)] = src[((int64_t)gx * nv + gy) * nv + gz];
+            }
+        }
+        __syncthreads();
+        for (int e = threadIdx.x; e < TE3; e += blockDim.x) {
+            int u[3] = {e >> 6, (e >> 3) & 7, e & 7};
+            int gx = T[0] * TE + u[0], gy = T[1] * TE + u[1], gz = T[2] * TE + u[2];
+            if (gx >= nv || gy >= nv || gz >= nv) continue;
+            int v[3];
+            for (int m = 0; m < 3; m++) v[perm3(cs, m)] = u[m];
+            dst[((int64_t)gx * nv + gy) * nv + gz] = (l >= 0) ? sm[sidx(v[0], v[1], v[2])] : 0.0;
+        }
+        __syncthreads();
+    }
+}
+
+// Whole-block copies: out[r] = in[map[req[r]]] (map/req optional).
+__global__ void k_copy_blocks(const double *in, double *out, const int32_t *req, const int64_t *map, int64_t nreq,
+                              int64_t blk) {
+    for (int64_t r = blockIdx.y; r < nreq; r += gridDim.y) {
+        int64_t l = map ? map[req ? req[r] : r] : (req ? req[r] : r);
+        if (l < 0) continue;
+        const double *s = in + l * blk;
+        double *d = out + r * blk;
+        for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < blk; e += (int64_t)gridDim.x * blockDim.x)
+            d[e] = s[e];
+    }
+}
+
+// ---------------------------------------------------------------- divide / update
+
+__global__ void k_r3_divide(double *r3, const double *eia, const int32_t *ijk, int64_t nblocks, int nv) {
+    const int64_t n3 = (int64_t)nv * nv * nv;
+    for (int64_t q = blockIdx.y; q < nblocks; q += gridDim.y) {
+        const double *ei = eia + (int64_t)ijk[3 * q] * nv, *ej = eia + (int64_t)ijk[3 * q + 1] * nv,
+                     *ek = eia + (int64_t)ijk[3 * q + 2] * nv;
+        double *blk = r3 + q * n3;
+        for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n3; e += (int64_t)gridDim.x * blockDim.x) {
+            int c = (int)(e % nv), b = (int)((e / nv) % nv), a = (int)(e / ((int64_t)nv * nv));
+            blk[e] = __ddiv_rn(blk[e], dadd(dadd(ei[a], ej[b]), ek[c]));
+        }
+    }
+}
+
+constexpr int UPD_THREADS = 256;
+constexpr int UPD_GRID_X = 64;
+
+__device__ __forceinline__ double warp_sum(double v) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Fused divide + t3 update + squared norms; per-CTA partials go to ws[2*cta].
+__global__ void __launch_bounds__(UPD_THREADS) k_t3_divide_update(double *t3, double *r3, const double *eia,
+                                                                  const int32_t *ijk, int64_t nblocks, int nv,
+                                                                  int nact, int write_r3, double *ws) {
+    const int64_t n3 = (int64_t)nv * nv * nv;
+    double s_all = 0.0, s_act = 0.0;
+    for (int64_t q = blockIdx.y; q < nblocks; q += gridDim.y) {
+        const double *ei = eia + (int64_t)ijk[3 * q] * nv, *ej = eia + (int64_t)ijk[3 * q + 1] * nv,
+                     *ek = eia + (int64_t)ijk[3 * q + 2] * nv;
+        double *rb = r3 + q * n3, *tb = t3 + q * n3;
+        for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n3; e += (int64_t)gridDim.x * blockDim.x) {
+            int c = (int)(e % nv), b = (int)((e / nv) % nv), a = (int)(e / ((int64_t)nv * nv));
+            double r = __ddiv_rn(rb[e], dadd(dadd(ei[a], ej[b]), ek[c]));
+            if (write_r3) rb[e] = r;
+            tb[e] = dadd(tb[e], r);
+            double r2 = r * r;
+            s_all += r2;
+            if (a < nact && b < nact && c < nact) s_act += r2;
+        }
+    }
+    __shared__ double red[2][UPD_THREADS / 32];
+    s_all = warp_sum(s_all);
+    s_act = warp_sum(s_act);
+    int w = threadIdx.x >> 5;
+    if ((threadIdx.x & 31) == 0) {
+        red[0][w] = s_all;
+        red[1][w] = s_act;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double a = 0.0, b = 0.0;
+        for (int i = 0; i < UPD_THREADS / 32; i++) {
+            a += red[0][i];
+            b += red[1][i];
+        }
+        int64_t cta = (int64_t)blockIdx.y * gridDim.x + blockIdx.x;
+        ws[2 * cta] = a;
+        ws[2 * cta + 1] = b;
+    }
+}
+
+// Deterministic final sum of n partial pairs into out[0..1].
+__global__ void k_sum_pairs(const double *ws, int64_t n, double *out) {
+    __shared__ double red[2][32];
+    double a = 0.0, b = 0.0;
+    for (int64_t i = threadIdx.x; i < n; i += blockDim.x) {
+        a += ws[2 * i];
+        b += ws[2 * i + 1];
+    }
+    a = warp_sum(a);
+    b = warp_sum(b);
+    if ((threadIdx.x & 31) == 0) {
+        red[0][threadIdx.x >> 5] = a;
+        red[1][threadIdx.x >> 5] = b;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double x = 0.0, y = 0.0;
+        for (int i = 0; i < (int)(blockDim.x >> 5); i++) {
+            x += red[0][i];
+            y += red[1][i];
+        }
+        out[0] = x;
+        out[1] = y;
+    }
+}
+
+static unsigned update_grid_y(int64_t nblocks) { return (unsigned)(nblocks < 4096 ? nblocks : 4096); }
+
+// ---------------------------------------------------------------- IJK -> ABC
+
+// t3_abc[g][x][y][z]: the canonical block of sorted(x,y,z) read at
+// sigma_p^{-1}(A,B,C) for the largest axis map p with sigma_p^{-1}(x,y,z)
+// sorted (the last record the reference's pack order writes there).
+__global__ void k_ijk_to_abc(const double *t3_ijk, double *t3_abc, int no, int nv, int64_t nabc) {
+    const int64_t o3 = (int64_t)no * no * no;
+    for (int64_t g = blockIdx.y; g < nabc; g += gridDim.y) {
+        // decode g -> A<=B<=C
+        int64_t r = g;
+        int A = 0;
+        for (;; A++) {
+            int64_t m = (int64_t)(nv - A) * (nv - A + 1) / 2;
+            if (r < m) break;
+            r -= m;
+        }
+        int B = A;
+        for (;; B++) {
+            if (r < nv - B) break;
+            r -= nv - B;
+        }
+        int C = B + (int)r;
+        int tgt[3] = {A, B, C};
+        for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < o3; e += (int64_t)gridDim.x * blockDim.x) {
+            int xyz[3] = {(int)(e / (no * no)), (int)((e / no) % no), (int)(e % no)};
+            int best = 0, w0 = 0, w1 = 0, w2 = 0;
+            for (int p = 0; p < 6; p++) {
+                int w[3];
+                for (int m = 0; m < 3; m++) w[perm3(p, m)] = xyz[m];
+                if (w[0] <= w[1] && w[1] <= w[2]) {
+                    best = p;
+                    w0 = w[0];
+                    w1 = w[1];
+                    w2 = w[2];
+                }
+            }
+            int abc[3];
+            for (int m = 0; m < 3; m++) abc[perm3(best, m)] = tgt[m];
+            const double *blk = t3_ijk + ijk_linear(w0, w1, w2, no) * (int64_t)nv * nv * nv;
+            t3_abc[g * o3 + e] = blk[((int64_t)abc[0] * nv + abc[1]) * nv + abc[2]];
+        }
+    }
+}
+
+// Ordering case of (a,b,c) chosen by the reference's three c-regions
+// (src/rccsdt_q.c:690-743).
+__device__ __forceinline__ int abc_case(int a, int b, int c, int s[3]) {
+    int lo = a < b ? a : b, hi = a < b ? b : a, cs;
+    if (c > hi) cs = (a <= b) ? 0 : 2;
+    else if (c > lo) cs = (a <= b) ? ((b <= c) ? 0 : 1) : ((a <= c) ? 2 : 4);
+    else cs = (a <= b) ? ((a <= c) ? 1 : 3) : ((b <= c) ? 4 : 5);
+    int v[3] = {a, b, c};
+    // sorted triple = (v[perm3(cs,0)], ...) read through the case's axis map
+    int srt[6][3] = {{0, 1, 2}, {0, 2, 1}, {1, 0, 2}, {2, 0, 1}, {1, 2, 0}, {2, 1, 0}};
+    s[0] = v[srt[cs][0]];
+    s[1] = v[srt[cs][1]];
+    s[2] = v[srt[cs][2]];
+    return cs;
+}
+
+// One CTA per (ia, ib, c) block of nocc^3: load the ABC block, write it with
+// the occupied axes permuted.
+__global__ void k_fill_t3_abc(double *target, int a0, int a1, int b0, int b1, int nv, int no,
+                              const double *t3_abc, int64_t ld_b) {
+    extern __shared__ double blk[];
+    const int o3 = no * no * no;
+    const int ba = a1 - a0, bb = b1 - b0;
+    const int64_t nwork = (int64_t)ba * bb * nv;
+    for (int64_t w = blockIdx.x; w < nwork; w += gridDim.x) {
+        int c = (int)(w % nv), ib = (int)((w / nv) % bb), ia = (int)(w / ((int64_t)nv * bb));
+        int s[3];
+        int cs = abc_case(a0 + ia, b0 + ib, c, s);
+        const double *src = t3_abc + abc_linear(s[0], s[1], s[2], nv) * o3;
+        for (int e = threadIdx.x; e < o3; e += blockDim.x) blk[e] = src[e];
+        __syncthreads();
+        double *dst = target + (((int64_t)ia * ld_b + ib) * nv + c) * o3;
+        for (int e = threadIdx.x; e < o3; e += blockDim.x) {
+            int u[3] = {e / (no * no), (e / no) % no, e % no};
+            // dst[v[P0],v[P1],v[P2]] = src[v]  =>  src index v with v[P[m]] = u[m]
+            int v[3];
+            for (int m = 0; m < 3; m++) v[perm3(cs, m)] = u[m];
+            dst[e] = blk[(v[0] * no + v[1]) * no + v[2]];
+        }
+        __syncthreads();
+    }
+}
+
+// Single-block unpack with the case and source block resolved on the host.
+__global__ void __launch_bounds__(OT_THREADS) k_take_t3_one(const double *t3, double *out, int i, int j, int k,
+                                                            int64_t l, int nv, int ntile) {
+    __shared__ double sm[SLOT];
+    const int64_t n3 = (int64_t)nv * nv * nv;
+    int T[3] = {(int)(blockIdx.x / (ntile * ntile)), (int)((blockIdx.x / ntile) % ntile), (int)(blockIdx.x % ntile)};
+    int64_t s[3];
+    int cs = order_case3(i, j, k, s);
+    int V[3];
+    for (int m = 0; m < 3; m++) V[perm3(cs, m)] = T[m];
+    const double *src = t3 + l * n3;
+    for (int e = threadIdx.x; e < TE3; e += blockDim.x) {
+        int x = e >> 6, y = (e >> 3) & 7, z = e & 7;
+        int gx = V[0] * TE + x, gy = V[1] * TE + y, gz = V[2] * TE + z;
+        if (gx < nv && gy < nv && gz < nv) sm[sidx(x, y, z)] = src[((int64_t)gx * nv + gy) * nv + gz];
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < TE3; e += blockDim.x) {
+        int u[3] = {e >> 6, (e >> 3) & 7, e & 7};
+        int gx = T[0] * TE + u[0], gy = T[1] * TE + u[1], gz = T[2] * TE + u[2];
+        if (gx >= nv || gy >= nv || gz >= nv) continue;
+        int v[3];
+        for (int m = 0; m < 3; m++) v[perm3(cs, m)] = u[m];
+        out[((int64_t)gx * nv + gy) * nv + gz] = sm[sidx(v[0], v[1], v[2])];
+    }
+}
+
+}  // namespace dcc
+
+using namespace dcc;
+
+// ---------------------------------------------------------------- C ABI
+
+static int p3_coef(const char *pattern, double alpha, double beta, P3Coef &k) {
+    double p[5];
+    if (p3_pattern(pattern, p)) {
+        set_error("unrecognized pattern \"%s\"", pattern ? pattern : "(null)");
+        return DCC_ERR_PATTERN;
+    }
+    k = P3Coef{p[0], p[1], p[2], p[3], p[4], alpha, beta, (p[0] + p[1]) + p[2], alpha * (p[3] + p[4])};
+    return DCC_OK;
+}
+
+extern "C" int dcc_t3_spin_summation_inplace(double *A, int64_t nblocks, int64_t nvir, const char *pattern,
+                                             double alpha, double beta, void *stream) {
+    clear_error();
+    P3Coef k;
+    int rc = p3_coef(pattern, alpha, beta, k);
+    if (rc) return rc;
+    DCC_REQUIRE(nblocks >= 0 && nvir >= 0, DCC_ERR_SHAPE, "negative size");
+    DCC_REQUIRE(A || nblocks * nvir == 0, DCC_ERR_NULL, "A is NULL");
+    return orbit3_launch(0, A, A, nullptr, nullptr, nblocks, nvir, k, stream);
+}
+
+extern "C" int dcc_t3_single_spin_summation_inplace(double *A, int64_t nvir, const char *pattern, double alpha,
+                                                    double beta, void *stream) {
+    return dcc_t3_spin_summation_inplace(A, 1, nvir, pattern, alpha, beta, stream);
+}
+
+extern "C" int dcc_t3_spin_summation_triple_sym(const double *A, double *B0, double *B1, double *B2,
+                                                int64_t nblocks, int64_t nvir, void *stream) {
+    clear_error();
+    DCC_REQUIRE(nblocks >= 0 && nvir >= 0, DCC_ERR_SHAPE, "negative size");
+    DCC_REQUIRE((A && B0 && B1 && B2) || nblocks * nvir == 0, DCC_ERR_NULL, "NULL buffer");
+    DCC_REQUIRE(A != B0 && A != B1 && A != B2, DCC_ERR_SHAPE, "triple_sym is out of place");
+    P3Coef k{};
+    return orbit3_launch(1, A, B0, B1, B2, nblocks, nvir, k, stream);
+}
+
+extern "C" int dcc_t3_transpose_add(const double *A, double *B, int64_t nblocks, int64_t nvir, void *stream) {
+    clear_error();
+    DCC_REQUIRE(nblocks >= 0 && nvir >= 0, DCC_ERR_SHAPE, "negative size");
+    DCC_REQUIRE((A && B) || nblocks * nvir == 0, DCC_ERR_NULL, "NULL buffer");
+    DCC_REQUIRE(A != B, DCC_ERR_SHAPE, "transpose_add is out of place");
+    P3Coef k{};
+    return orbit3_launch(2, A, B, nullptr, nullptr, nblocks, nvir, k, stream);
+}
+
+extern "C" int dcc_take_t3_batched(const double *t3_local, double *out, const int32_t *ijk,
+                                   const int64_t *ijk_to_local_idx, int64_t count, int64_t nocc, int64_t nvir,
+                                   void *stream) {
+    clear_error();
+    DCC_REQUIRE(count >= 0 && nocc >= 0 && nvir >= 0, DCC_ERR_SHAPE, "negative size");
+    if (count == 0 || nvir == 0) return DCC_OK;
+    DCC_REQUIRE(t3_local && out && ijk && ijk_to_local_idx, DCC_ERR_NULL, "NULL buffer");
+    int ntile = (int)ceil_div(nvir, TE);
+    dim3 grid((unsigned)(ntile * ntile * ntile), (unsigned)(count < 65535 ? count : 65535));
+    k_take_t3<<<grid, OT_THREADS, 0, as_stream(stream)>>>(t3_local, out, ijk, ijk_to_local_idx, count, (int)nocc,
+                                                          (int)nvir, ntile);
+    return launch_status("take_t3");
+}
+
+extern "C" int dcc_take_t3_ijk_single(const double *t3_local, double *t3_blk, const int64_t *ijk_to_local_idx,
+                                      int64_t i, int64_t j, int64_t k, int64_t nocc, int64_t nvir, void *stream) {
+    clear_error();
+    DCC_REQUIRE(i >= 0 && j >= 0 && k >= 0 && i < nocc && j < nocc && k < nocc, DCC_ERR_SHAPE,
+                "occupied index out of range");
+    DCC_REQUIRE(ijk_to_local_idx && t3_local && t3_blk, DCC_ERR_NULL, "NULL buffer");
+    int64_t s[3];
+    int cs = order_case3(i, j, k, s);
+    int64_t loc = ijk_to_local_idx[ijk_linear(s[0], s[1], s[2], nocc)];
+    if (loc < 0) {
+        set_error("block (%lld,%lld,%lld) is not stored", (long long)s[0], (long long)s[1], (long long)s[2]);
+        return DCC_ERR_NOT_LOCAL;
+    }
+    (void)cs;
+    int ntile = (int)ceil_div(nvir, TE);
+    k_take_t3_one<<<dim3((unsigned)(ntile * ntile * ntile)), OT_THREADS, 0, as_stream(stream)>>>(
+        t3_local, t3_blk, (int)i, (int)j, (int)k, loc, (int)nvir, ntile);
+    return launch_status("take_t3_ijk_single");
+}
+
+extern "C" int dcc_fill_local_data_ijk(const double *t3_local, double *send_data, const int32_t *requests,
+                                       const int64_t *ijk_to_local_idx, int64_t n_requests, int64_t nvir,
+                                       void *stream) {
+    clear_error();
+    DCC_REQUIRE(n_requests >= 0 && nvir >= 0, DCC_ERR_SHAPE, "negative size");
+    if (n_requests == 0 || nvir == 0) return DCC_OK;
+    DCC_REQUIRE(t3_local && send_data && requests && ijk_to_local_idx, DCC_ERR_NULL, "NULL buffer");
+    int64_t blk = nvir * nvir * nvir;
+    dim3 grid(ceil_div(blk, 256 * 4) < 64 ? ceil_div(blk, 256 * 4) : 64,
+              (unsigned)(n_requests < 65535 ? n_requests : 65535));
+    k_copy_blocks<<<grid, 256, 0, as_stream(stream)>>>(t3_local, send_data, requests, ijk_to_local_idx, n_requests,
+                                                       blk);
+    return launch_status("fill_local_data_ijk");
+}
+
+extern "C" int dcc_r3_tri_divide_e(double *r3, const double *eia, const int32_t *ijk, int64_t nblocks, int64_t nvir,
+                                   void *stream) {
+    clear_error();
+    DCC_REQUIRE(nblocks >= 0 && nvir >= 0, DCC_ERR_SHAPE, "negative size");
+    if (nblocks == 0 || nvir == 0) return DCC_OK;
+    DCC_REQUIRE(r3 && eia && ijk, DCC_ERR_NULL, "NULL buffer");
+    int64_t n3 = nvir * nvir * nvir;
+    dim3 grid(ceil_div(n3, 256 * 8) < 64 ? ceil_div(n3, 256 * 8) : 64, update_grid_y(nblocks));
+    k_r3_divide<<<grid, 256, 0, as_stream(stream)>>>(r3, eia, ijk, nblocks, (int)nvir);
+    return launch_status("r3_tri_divide_e");
+}
+
+static unsigned update_grid_x(int64_t nvir) {
+    int64_t n3 = nvir * nvir * nvir;
+    unsigned gx = ceil_div(n3, UPD_THREADS * 8);
+    return gx < (unsigned)UPD_GRID_X ? (gx ? gx : 1) : (unsigned)UPD_GRID_X;
+}
+
+extern "C" size_t dcc_t3_update_workspace_bytes(int64_t nblocks, int64_t nvir) {
+    if (nblocks <= 0 || nvir <= 0) return 16;
+    return (size_t)update_grid_x(nvir) * update_grid_y(nblocks) * 2 * sizeof(double);
+}
+
+extern "C" int dcc_t3_divide_update(double *t3, double *r3, const double *eia, const int32_t *ijk, int64_t nblocks,
+                                    int64_t nvir, int64_t nvir_active, int write_r3, double *norms, void *workspace,
+                                    size_t workspace_bytes, void *stream) {
+    clear_error();
+    DCC_REQUIRE(nblocks >= 0 && nvir >= 0, DCC_ERR_SHAPE, "negative size");
+    DCC_REQUIRE(norms, DCC_ERR_NULL, "norms is NULL");
+    cudaStream_t st = as_stream(stream);
+    if (nblocks == 0 || nvir == 0) {
+        if (cudaMemsetAsync(norms, 0, 2 * sizeof(double), st) != cudaSuccess) return launch_status("memset");
+        return DCC_OK;
+    }
+    DCC_REQUIRE(t3 && r3 && eia && ijk && workspace, DCC_ERR_NULL, "NULL buffer");
+    size_t need = dcc_t3_update_workspace_bytes(nblocks, nvir);
+    DCC_REQUIRE(workspace_bytes >= need, DCC_ERR_WORKSPACE, "workspace needs %zu bytes, got %zu", need,
+                workspace_bytes);
+    if (nvir_active < 0 || nvir_active > nvir) nvir_active = nvir;
+    dim3 grid(update_grid_x(nvir), update_grid_y(nblocks));
+    k_t3_divide_update<<<grid, UPD_THREADS, 0, st>>>(t3, r3, eia, ijk, nblocks, (int)nvir, (int)nvir_active,
+                                                      write_r3, (double *)workspace);
+    int rc = launch_status("t3_divide_update");
+    if (rc) return rc;
+    k_sum_pairs<<<1, 256, 0, st>>>((const double *)workspace, (int64_t)grid.x * grid.y, norms);
+    return launch_status("t3_divide_update reduce");
+}
+
+extern "C" int dcc_redistribute_ijk_to_abc(const double *t3_ijk, double *t3_abc, int64_t nocc, int64_t nvir,
+                                           void *stream) {
+    clear_error();
+    DCC_REQUIRE(nocc >= 0 && nvir >= 0, DCC_ERR_SHAPE, "negative size");
+    if (nocc == 0 || nvir == 0) return DCC_OK;
+    DCC_REQUIRE(t3_ijk && t3_abc, DCC_ERR_NULL, "NULL buffer");
+    int64_t nabc = nvir * (nvir + 1) * (nvir + 2) / 6;
+    int64_t o3 = nocc * nocc * nocc;
+    dim3 grid(ceil_div(o3, 256) < 16 ? ceil_div(o3, 256) : 16, (unsigned)(nabc < 65535 ? nabc : 65535));
+    k_ijk_to_abc<<<grid, 256, 0, as_stream(stream)>>>(t3_ijk, t3_abc, (int)nocc, (int)nvir, nabc);
+    return launch_status("redistribute_ijk_to_abc");
+}
+
+extern "C" int dcc_fill_t3_from_abc(double *target, int64_t a0, int64_t a1, int64_t b0, int64_t b1, int64_t nvir,
+                                    int64_t nocc, const double *t3_abc, int64_t ld_b, void *stream) {
+    clear_error();
+    DCC_REQUIRE(0 <= a0 && a0 <= a1 && a1 <= nvir && 0 <= b0 && b0 <= b1 && b1 <= nvir, DCC_ERR_SHAPE,
+                "virtual range out of bounds");
+    DCC_REQUIRE(ld_b >= b1 - b0, DCC_ERR_SHAPE, "ld_b smaller than the b range");
+    if (a1 == a0 || b1 == b0 || nocc == 0) return DCC_OK;
+    DCC_REQUIRE(target && t3_abc, DCC_ERR_NULL, "NULL buffer");
+    int64_t o3 = nocc * nocc * nocc;
+    DCC_REQUIRE(o3 * 8 <= 200 * 1024, DCC_ERR_UNSUPPORTED, "nocc^3 block exceeds shared memory");
+    int64_t nwork = (a1 - a0) * (b1 - b0) * nvir;
+    unsigned grid = (unsigned)(nwork < 148 * 16 ? nwork : 148 * 16);
+    size_t smem = (size_t)o3 * sizeof(double);
+    if (smem > 48 * 1024)
+        cudaFuncSetAttribute(k_fill_t3_abc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_fill_t3_abc<<<grid, 256, smem, as_stream(stream)>>>(target, (int)a0, (int)a1, (int)b0, (int)b1, (int)nvir,
+                                                          (int)nocc, t3_abc, ld_b);
+    return launch_status("fill_t3_from_abc");
+}

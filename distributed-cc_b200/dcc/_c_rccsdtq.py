@@ -1,0 +1,106 @@
+"""T4 helpers on the GPU, mirroring distr_cc/_c_rccsdtq.py and the t4_add_ of
+distr_cc/_rccsdtq_core.py (same names and argument meaning, torch CUDA tensors)."""
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from . import _lib as L
+
+f64, i32, i64 = torch.float64, torch.int32, torch.int64
+
+
+def t4_project_1_minus_p4_p31_inplace_(A, nocc4, nvir, alpha=1.0, beta=0.0):
+    """A <- beta*A + alpha*(1 - P[4] - P[3,1])A (src/rccsdtq.c:262-308)."""
+    A = L.as_tensor(A, f64, "A")
+    if A.numel() != nocc4 * nvir ** 4:
+        raise ValueError("A must hold nocc4 blocks of nvir^4")
+    L.call("dcc_t4_project_1_minus_p4_p31_inplace", L.ptr(A), nocc4, nvir, float(alpha), float(beta),
+           L.stream_ptr())
+    return A
+
+
+def t4_single_spin_summation_inplace_(A, nvir, pattern, alpha=1.0, beta=0.0):
+    """P4_full | P4_442 | P4_201 on one nvir^4 block (src/rccsdtq.c:316-916)."""
+    A = L.as_tensor(A, f64, "A")
+    if A.numel() != nvir ** 4:
+        raise ValueError("A must hold one nvir^4 block")
+    if pattern not in ("P4_full", "P4_442", "P4_201"):
+        raise ValueError('unrecognized pattern "%s"' % pattern)
+    L.call("dcc_t4_spin_summation_inplace", L.ptr(A), 1, nvir, L.pattern(pattern), float(alpha), float(beta),
+           L.stream_ptr())
+    return A
+
+
+def t4_transpose_add_(src, dst, nvir):
+    """dst = src + src[c,a,b,d] + src[d,a,c,b] (src/rccsdtq.c:990-1005)."""
+    src = L.as_tensor(src, f64, "src")
+    dst = L.as_tensor(dst, f64, "dst")
+    if tuple(src.shape) != (nvir,) * 4 or tuple(dst.shape) != (nvir,) * 4:
+        raise ValueError("src and dst must have shape (nvir, nvir, nvir, nvir)")
+    L.call("dcc_t4_transpose_add", L.ptr(src), L.ptr(dst), nvir, L.stream_ptr())
+    return dst
+
+
+def t4_spin_summation_quadruple_sym_(src, B0, B1, B2, B3, nvir):
+    """The four P4_201 variants (src/rccsdtq.c:1018-1047)."""
+    bufs = [L.as_tensor(b, f64, n) for b, n in ((src, "src"), (B0, "B0"), (B1, "B1"), (B2, "B2"), (B3, "B3"))]
+    if any(tuple(b.shape) != (nvir,) * 4 for b in bufs):
+        raise ValueError("all T4 buffers must have shape (nvir, nvir, nvir, nvir)")
+    L.call("dcc_t4_spin_summation_quadruple_sym", *[L.ptr(b) for b in bufs], nvir, L.stream_ptr())
+    return B0, B1, B2, B3
+
+
+def r4_local_tri_divide(r4_local, eia, local_ijkl):
+    """r4[q] /= eia[i,a]+eia[j,b]+eia[k,c]+eia[l,d] (src/rccsdtq.c:1055-1088)."""
+    r4_local = L.as_tensor(r4_local, f64, "r4_local")
+    eia = L.as_tensor(eia, f64, "eia")
+    local_ijkl = L.as_tensor(local_ijkl, i32, "local_ijkl")
+    nvir = eia.shape[1]
+    if r4_local.shape != (local_ijkl.shape[0],) + (nvir,) * 4:
+        raise ValueError("r4_local has inconsistent local T4 shape")
+    L.call("dcc_r4_local_tri_divide_e", L.ptr(r4_local), L.ptr(eia), L.ptr(local_ijkl), local_ijkl.shape[0], nvir,
+           L.stream_ptr())
+    return r4_local
+
+
+def r4_local_tri_divide_e_(mycc, dt4, r4_local, mo_energy):
+    """Reference-shaped wrapper (distr_cc/_c_rccsdtq.py:63-74)."""
+    nocc = mycc.nocc
+    mo = torch.as_tensor(np.asarray(mo_energy), dtype=f64, device=r4_local.device)
+    eia = (mo[:nocc, None] - mo[None, nocc:] - mycc.level_shift).contiguous()
+    ijkl = torch.as_tensor(np.asarray(dt4.local_quadruples, dtype=np.int32).reshape(-1, 4), device=r4_local.device)
+    return r4_local_tri_divide(r4_local, eia, ijkl)
+
+
+def fill_local_data_ijkl_(t4_local, send_data, requests, ijkl_to_local_idx, n_requests, nvir):
+    """Gather requested T4 blocks (src/rccsdtq.c:1090-1102)."""
+    t4_local = L.as_tensor(t4_local, f64, "t4_local")
+    send_data = L.as_tensor(send_data, f64, "send_data")
+    requests = L.as_tensor(requests, i32, "requests")
+    ijkl_to_local_idx = L.as_tensor(ijkl_to_local_idx, i64, "ijkl_to_local_idx")
+    L.call("dcc_fill_local_data_ijkl", L.ptr(t4_local), L.ptr(send_data), L.ptr(requests),
+           L.ptr(ijkl_to_local_idx), n_requests, nvir, L.stream_ptr())
+    return send_data
+
+
+def unpack_t4_ijkl_single_(t4_local, t4_blk, ijkl_to_local_idx, i, j, k, l, nocc, nvir):
+    """T4[i,j,k,l] for any ordering; zero-rule blocks come back zero
+    (src/rccsdtq.c:1104-1125).  ijkl_to_local_idx is a host int64 array."""
+    t4_local = L.as_tensor(t4_local, f64, "t4_local")
+    t4_blk = L.as_tensor(t4_blk, f64, "t4_blk")
+    m = np.ascontiguousarray(np.asarray(ijkl_to_local_idx, dtype=np.int64))
+    L.call("dcc_unpack_t4_ijkl_single", L.ptr(t4_local), L.ptr(t4_blk), m.ctypes.data_as(L.c_vp), i, j, k, l, nocc,
+           nvir, L.stream_ptr())
+    return t4_blk
+
+
+def t4_add_(t4, r4, nocc4, nvir):
+    """t4 += r4 over nocc4 blocks of nvir^4 (PySCF libccsdt t4_add_, distr_cc/_rccsdtq_core.py:43-48)."""
+    t4 = L.as_tensor(t4, f64, "t4")
+    r4 = L.as_tensor(r4, f64, "r4")
+    n = nocc4 * nvir ** 4
+    if t4.numel() < n or r4.numel() < n:
+        raise ValueError("t4/r4 smaller than nocc4 * nvir^4")
+    L.call("dcc_t4_add", L.ptr(t4), L.ptr(r4), n, L.stream_ptr())
+    return t4

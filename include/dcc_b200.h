@@ -1,0 +1,208 @@
+/*
+ * dcc_b200.h -- C ABI of the B200 (sm_100a) library for Distributed-CC's
+ * triples/quadruples hot path.
+ *
+ * Conventions
+ *  - Tensor arguments are DEVICE pointers to C-contiguous float64 (or the
+ *    stated integer type) buffers owned by the caller; the library writes in
+ *    place exactly like the reference helpers and allocates nothing unless an
+ *    entry point says so.  Arguments documented as "host" are host pointers.
+ *  - `stream` is a cudaStream_t passed as void*; NULL is the legacy stream.
+ *    Calls are asynchronous on that stream unless documented otherwise.
+ *  - Every entry point returns DCC_OK (0) or an error code; dcc_last_error()
+ *    then holds a message for the calling thread.  Nothing aborts.
+ *  - Pattern names are the reference's strings ("P3_full", "P4_444", ...).
+ *
+ * Each declaration names the reference interface it replaces, by file:line in
+ * the Distributed-CC project (the reference binds those through ctypes in
+ * distr_cc/_c_rccsdt.py, distr_cc/_c_rccsdt_q.py, distr_cc/_c_rccsdtq.py).
+ */
+#ifndef DCC_B200_H
+#define DCC_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define DCC_API __attribute__((visibility("default")))
+#else
+#define DCC_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    DCC_OK = 0,
+    DCC_ERR_PATTERN = 1,     /* unknown pattern string */
+    DCC_ERR_SHAPE = 2,       /* inconsistent sizes / indices out of range */
+    DCC_ERR_NULL = 3,        /* required pointer is NULL */
+    DCC_ERR_CUDA = 4,        /* CUDA runtime / launch failure */
+    DCC_ERR_TIMEOUT = 5,     /* a bounded device-side wait gave up */
+    DCC_ERR_UNSUPPORTED = 6, /* valid request this build does not implement */
+    DCC_ERR_NOT_LOCAL = 7,   /* requested block is not stored (reference: silent no-op) */
+    DCC_ERR_WORKSPACE = 8    /* workspace argument too small */
+};
+
+/* Message for the last failing call on this thread ("" after success). */
+DCC_API const char *dcc_last_error(void);
+/* Library ABI version (major*100 + minor). */
+DCC_API int dcc_version(void);
+
+/* ----------------------------------------------------------------------
+ * T3 helpers (replace src/rccsdt.c)
+ * ---------------------------------------------------------------------- */
+
+/* A <- beta*A + alpha*P(A) on one nvir^3 block; P = P3_full | P3_422 | P3_201.
+ * Replaces t3_single_spin_summation_inplace_ (src/rccsdt.c:131-233). */
+DCC_API int dcc_t3_single_spin_summation_inplace(double *A, int64_t nvir, const char *pattern, double alpha,
+                                         double beta, void *stream);
+
+/* Same on nblocks consecutive nvir^3 blocks in one launch.  Replaces the
+ * multi-block t3_spin_summation_inplace_(r3, n3, nvir, "P3_full", -1/6, 1)
+ * called at distr_cc/rccsdt.py:947 (PySCF pyscf/cc/rccsdt.py). */
+DCC_API int dcc_t3_spin_summation_inplace(double *A, int64_t nblocks, int64_t nvir, const char *pattern, double alpha,
+                                  double beta, void *stream);
+
+/* B0 = 2T - T_acb - T_cba, B1 = 2T - T_bac - T_acb, B2 = B0 + T_acb - T_bac on
+ * nblocks blocks.  Replaces t3_spin_summation_triple_sym_ (src/rccsdt.c:245-310). */
+DCC_API int dcc_t3_spin_summation_triple_sym(const double *A, double *B0, double *B1, double *B2, int64_t nblocks,
+                                     int64_t nvir, void *stream);
+
+/* B[a,b,c] = A[a,b,c] + A[c,a,b] on nblocks blocks.
+ * Replaces t3_transpose_add_ (src/rccsdt.c:320-375). */
+DCC_API int dcc_t3_transpose_add(const double *A, double *B, int64_t nblocks, int64_t nvir, void *stream);
+
+/* t3_blk = T3[i,j,k] for any ordering, unpacked from canonical storage.
+ * ijk_to_local_idx is a HOST array of nocc3 int64 (-1: not stored).  Returns
+ * DCC_ERR_NOT_LOCAL when the block is not stored (the reference silently
+ * returns).  Replaces take_t3_ijk_single_ (src/rccsdt.c:119-129). */
+DCC_API int dcc_take_t3_ijk_single(const double *t3_local, double *t3_blk, const int64_t *ijk_to_local_idx, int64_t i,
+                           int64_t j, int64_t k, int64_t nocc, int64_t nvir, void *stream);
+
+/* Batched unpack: out[n] = T3[ijk[n][0], ijk[n][1], ijk[n][2]] for n < count;
+ * ijk (int32 [count][3]) and ijk_to_local_idx (int64 [nocc3]) are DEVICE
+ * arrays.  Blocks that are not stored are zero-filled.  Batched form of
+ * take_t3_ijk_single_ (src/rccsdt.c:119-129) as used by
+ * distr_cc/rccsdt.py:266-267,300. */
+DCC_API int dcc_take_t3_batched(const double *t3_local, double *out, const int32_t *ijk, const int64_t *ijk_to_local_idx,
+                        int64_t count, int64_t nocc, int64_t nvir, void *stream);
+
+/* send_data[r] = t3_local[ijk_to_local_idx[requests[r]]] for stored blocks
+ * (DEVICE index arrays).  Replaces fill_local_data_ijk_ (src/rccsdt.c:105-117). */
+DCC_API int dcc_fill_local_data_ijk(const double *t3_local, double *send_data, const int32_t *requests,
+                            const int64_t *ijk_to_local_idx, int64_t n_requests, int64_t nvir, void *stream);
+
+/* r3[q,a,b,c] /= eia[i,a] + eia[j,b] + eia[k,c] for the canonical triple
+ * (i,j,k) = ijk[q] (DEVICE int32 [nblocks][3]; eia DEVICE [nocc][nvir],
+ * already including -level_shift).  Replaces r3_tri_divide_e_
+ * (distr_cc/rccsdt.py:734-744). */
+DCC_API int dcc_r3_tri_divide_e(double *r3, const double *eia, const int32_t *ijk, int64_t nblocks, int64_t nvir,
+                        void *stream);
+
+/* Fused T3 update: r3 /= D (as dcc_r3_tri_divide_e), t3 += r3, and
+ * norms[0] = sum r3^2, norms[1] = sum over a,b,c < nvir_active of r3^2
+ * (DEVICE double[2]).  write_r3 != 0 also stores the divided r3.  The
+ * workspace (DEVICE, >= dcc_t3_update_workspace_bytes()) holds per-CTA
+ * partial sums.  Replaces distr_cc/rccsdt.py:949-971. */
+DCC_API size_t dcc_t3_update_workspace_bytes(int64_t nblocks, int64_t nvir);
+DCC_API int dcc_t3_divide_update(double *t3, double *r3, const double *eia, const int32_t *ijk, int64_t nblocks,
+                         int64_t nvir, int64_t nvir_active, int write_r3, double *norms, void *workspace,
+                         size_t workspace_bytes, void *stream);
+
+/* IJK -> ABC layout transform at one rank: t3_abc[g][x][y][z] (g the rank of
+ * a<=b<=c) from t3_ijk[q][a][b][c] (q the rank of i<=j<=k).  Reproduces the
+ * record pack + Alltoallv + unpack of distr_cc/distribute_t3.py:1544-1642 with
+ * src/rccsdt.c:411-561 (last record wins where records collide). */
+DCC_API int dcc_redistribute_ijk_to_abc(const double *t3_ijk, double *t3_abc, int64_t nocc, int64_t nvir, void *stream);
+
+/* target[ia][ib][c][i][j][k] (row pitch ld_b over ib) for a in [a0,a1),
+ * b in [b0,b1), all c, from ABC storage t3_abc[g][x][y][z] with the occupied
+ * axes permuted by the virtual ordering case.  Replaces fill_t3_from_ptr_array
+ * (src/rccsdt_q.c:655-828); at one rank every ABC block is local, so the
+ * pointer table becomes one contiguous array. */
+DCC_API int dcc_fill_t3_from_abc(double *target, int64_t a0, int64_t a1, int64_t b0, int64_t b1, int64_t nvir,
+                         int64_t nocc, const double *t3_abc, int64_t ld_b, void *stream);
+
+/* ----------------------------------------------------------------------
+ * T4 helpers (replace src/rccsdtq.c and PySCF libccsdt.t4_add_)
+ * ---------------------------------------------------------------------- */
+
+/* A <- beta*A + alpha*Q(A), Q = 1 - P[4] - P[3,1] on nocc4 blocks of nvir^4.
+ * Replaces t4_project_1_minus_p4_p31_inplace_ (src/rccsdtq.c:262-308). */
+DCC_API int dcc_t4_project_1_minus_p4_p31_inplace(double *A, int64_t nocc4, int64_t nvir, double alpha, double beta,
+                                          void *stream);
+
+/* A <- alpha*P(A) + beta*A on nouter blocks of ninner^4, P = P4_full | P4_444 |
+ * P4_442 | P4_201.  Replaces t4_spin_summation_inplace_ (src/rccsdt_q.c:33-472,
+ * used with outer = abcd, inner = nocc at distr_cc/rccsdt_q.py:1133) and, with
+ * nouter = 1, t4_single_spin_summation_inplace_ (src/rccsdtq.c:316-916). */
+DCC_API int dcc_t4_spin_summation_inplace(double *A, int64_t nouter, int64_t ninner, const char *pattern, double alpha,
+                                  double beta, void *stream);
+
+/* dst = src + src[c,a,b,d] + src[d,a,c,b].  Replaces t4_transpose_add_
+ * (src/rccsdtq.c:990-1005). */
+DCC_API int dcc_t4_transpose_add(const double *src, double *dst, int64_t nvir, void *stream);
+
+/* Four P4_201 variants B0..B3.  Replaces t4_spin_summation_quadruple_sym_
+ * (src/rccsdtq.c:1018-1047). */
+DCC_API int dcc_t4_spin_summation_quadruple_sym(const double *src, double *B0, double *B1, double *B2, double *B3,
+                                        int64_t nvir, void *stream);
+
+/* r4[q] /= eia[i,a]+eia[j,b]+eia[k,c]+eia[l,d] for ijkl = local_ijkl[q]
+ * (DEVICE int32 [nlocal][4]).  Replaces r4_local_tri_divide_e_
+ * (src/rccsdtq.c:1055-1088). */
+DCC_API int dcc_r4_local_tri_divide_e(double *r4_local, const double *eia, const int32_t *local_ijkl, int64_t nlocal,
+                              int64_t nvir, void *stream);
+
+/* t4_blk = T4[i,j,k,l] for any ordering; zero-rule blocks are zero-filled.
+ * ijkl_to_local_idx is a HOST array over the full triangular index.
+ * Replaces unpack_t4_ijkl_single_ (src/rccsdtq.c:1104-1125). */
+DCC_API int dcc_unpack_t4_ijkl_single(const double *t4_local, double *t4_blk, const int64_t *ijkl_to_local_idx, int64_t i,
+                              int64_t j, int64_t k, int64_t l, int64_t nocc, int64_t nvir, void *stream);
+
+/* send_data[r] = t4_local[ijkl_to_local_idx[requests[r]]] (DEVICE index
+ * arrays).  Replaces fill_local_data_ijkl_ (src/rccsdtq.c:1090-1102). */
+DCC_API int dcc_fill_local_data_ijkl(const double *t4_local, double *send_data, const int32_t *requests,
+                             const int64_t *ijkl_to_local_idx, int64_t n_requests, int64_t nvir, void *stream);
+
+/* t4 += r4 over n doubles.  Replaces PySCF libccsdt t4_add_ as bound at
+ * distr_cc/_rccsdtq_core.py:43-48 (elementwise add over nocc4*nvir^4). */
+DCC_API int dcc_t4_add(double *t4, const double *r4, int64_t n, void *stream);
+
+/* ----------------------------------------------------------------------
+ * (Q) denominator-and-energy loop (replace src/rccsdt_q.c, distr_cc/rccsdt_q.py)
+ * ---------------------------------------------------------------------- */
+
+/* r4[abcd][ijkl] /= D, zero where |D| <= 1e-15.  e_occ/e_vir DEVICE.
+ * Replaces e_abcdijkl_division_ (src/rccsdt_q.c:474-588). */
+DCC_API int dcc_e_abcdijkl_division(double *r4, const double *e_occ, const double *e_vir, int64_t a0, int64_t a1,
+                            int64_t b0, int64_t b1, int64_t c0, int64_t c1, int64_t d0, int64_t d1, int64_t blk_a,
+                            int64_t blk_b, int64_t blk_c, int64_t blk_d, int64_t nocc, void *stream);
+
+/* t4[abcd][:] *= factor[abcd] (exact zero where factor == 0); factor DEVICE.
+ * Replaces t4_multiply_factor_ (src/rccsdt_q.c:590-650). */
+DCC_API int dcc_t4_multiply_factor(double *t4_blk, const double *factor_blk, int64_t blk_a, int64_t blk_b, int64_t blk_c,
+                           int64_t blk_d, int64_t nocc, void *stream);
+
+/* Fused per-task epilogue of the (Q) loop (distr_cc/rccsdt_q.py:1131-1154):
+ *   t~4 = factor(abcd) * P4_444_ijkl((t4 + z4) / D)
+ *   out[0] += <t~4, z4sq>/12            ([Q] bracket)
+ *   out[1] += <t~4, z4>/12 + that term  ((Q) paren)
+ * where z4sq is the disconnected vvoo x t2 product of distr_cc/rccsdt_q.py:1143-1150
+ * formed on the fly from eris_vvoo [nvir][nvir][nocc][nocc] and t2_vvoo
+ * [nvir][nvir][nocc][nocc] (DEVICE).  t4 and z4 ([blk]^4 x nocc^4, DEVICE) are
+ * only read.  out is DEVICE double[2] and is accumulated into.  The workspace
+ * (>= dcc_q_epilogue_workspace_bytes()) holds per-CTA partial sums. */
+DCC_API size_t dcc_q_epilogue_workspace_bytes(int64_t blksize, int64_t nocc);
+DCC_API int dcc_q_task_epilogue(const double *t4, const double *z4, const double *eris_vvoo, const double *t2_vvoo,
+                        const double *e_occ, const double *e_vir, int64_t a0, int64_t a1, int64_t b0, int64_t b1,
+                        int64_t c0, int64_t c1, int64_t d0, int64_t d1, int64_t blksize, int64_t nocc,
+                        int64_t nvir, double *out, void *workspace, size_t workspace_bytes, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DCC_B200_H */
