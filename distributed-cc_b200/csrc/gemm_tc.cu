@@ -1,0 +1,464 @@
+// Split-precision tensor-core GEMM for the dense T3 residual contractions
+// (tcgen05 + TMEM + TMA, sm_100a).
+//
+//   C[row_off(m) + col_off(n)] = alpha * sum_k A[m][k] B[n][k] + beta * C[...]
+//
+// A and B are FP64 operands that have been split into two bf16 (or tf32)
+// pieces, x = x_hi + x_lo, stored K-major with K padded to the k-block.  The
+// product is accumulated in FP32 in tensor memory as
+//   A_hi B_hi + A_hi B_lo + A_lo B_hi
+// (the dropped A_lo B_lo term is below the pieces' own rounding), and the
+// epilogue adds alpha * acc into an FP64 C with beta scaling.  The output
+// address is two-level strided,
+//   row_off(m) = (m / rdiv) * rs1 + (m % rdiv) * rs2,
+//   col_off(n) = (n / cdiv) * cs1 + (n % cdiv) * cs2,
+// so permuted contraction outputs (e.g. r3[a,b,c] += X[(q,c),(a,b)]) are
+// accumulated in place without a transposed temporary.
+//
+// CTA = 6 warps: warp 0 issues TMA loads, warp 1 owns TMEM and issues the
+// MMAs from one thread, warps 2..5 drain the accumulator (one TMEM lane
+// quarter each).  Every mbarrier wait is bounded; on timeout the kernel sets
+// *status = DCC_ERR_TIMEOUT, waits (bounded) for its own copies and MMAs,
+// frees TMEM and returns.
+#include <cuda.h>
+#include <cuda_bf16.h>
+#include <stdint.h>
+#include <string.h>
+
+#include "dcc_common.cuh"
+
+namespace dcc {
+
+constexpr int GM = 128;       // tile rows (UMMA M)
+constexpr int GN = 256;       // tile cols (UMMA N)
+constexpr int GK_BYTES = 128; // one k-block row: 128 bytes (SWIZZLE_128B)
+constexpr int GSTAGES = 2;
+constexpr int G_THREADS = 192;
+constexpr uint64_t WAIT_NS = 2000000000ull;  // 2 s bound on any single wait
+
+struct GemmEpi {
+    int64_t rdiv, rs1, rs2, cdiv, cs1, cs2;
+};
+
+// ----------------------------------------------------------------- PTX helpers
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ uint64_t globaltimer() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count));
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Bounded wait: false (and *status set) when the phase did not complete in time.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, int *status) {
+    if (mbar_try(bar, parity)) return true;
+    uint64_t t0 = globaltimer();
+    for (uint32_t it = 1;; it++) {
+        if (mbar_try(bar, parity)) return true;
+        if ((it & 255) == 0) {
+            if (*(volatile int *)status != 0) return false;  // another role already gave up
+            if (globaltimer() - t0 > WAIT_NS) {
+                atomicExch(status, DCC_ERR_TIMEOUT);
+                return false;
+            }
+        }
+    }
+}
+
+// Bounded wait that reports nothing (used while draining after an abort).
+__device__ __forceinline__ void mbar_wait_quiet(uint32_t bar, uint32_t parity) {
+    uint64_t t0 = globaltimer();
+    while (!mbar_try(bar, parity))
+        if (globaltimer() - t0 > WAIT_NS) return;
+}
+
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap *map, uint32_t bar, int c0, int c1) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];"
+        ::"r"(dst), "l"(map), "r"(bar), "r"(c0), "r"(c1)
+        : "memory");
+}
+
+__device__ __forceinline__ void tma_prefetch_desc(const CUtensorMap *map) {
+    asm volatile("prefetch.tensormap [%0];" ::"l"(map) : "memory");
+}
+
+// K-major, 128-byte-swizzled operand tile: rows of 128 bytes, 8-row groups
+// 1024 bytes apart (stride byte offset), Blackwell descriptor version 1.
+__device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
+    uint64_t d = (uint64_t)((saddr >> 4) & 0x3FFF);
+    d |= (uint64_t)1 << 16;            // leading byte offset (unused for swizzled K-major): 16 B
+    d |= (uint64_t)(1024 >> 4) << 32;  // stride byte offset: 1024 B
+    d |= (uint64_t)1 << 46;            // descriptor version
+    d |= (uint64_t)2 << 61;            // SWIZZLE_128B
+    return d;
+}
+
+template <int KIND>  // 0: kind::f16 (bf16 x bf16), 1: kind::tf32
+__device__ __forceinline__ void umma(uint32_t tmem_d, uint64_t ad, uint64_t bd, uint32_t idesc, uint32_t acc) {
+    if (KIND == 0)
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+            "l"(ad), "l"(bd), "r"(idesc), "r"(acc));
+    else
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+            "l"(ad), "l"(bd), "r"(idesc), "r"(acc));
+}
+
+__device__ __forceinline__ void umma_commit(uint32_t bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+                 : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
+    uint32_t r[32];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 32; i++) v[i] = __uint_as_float(r[i]);
+}
+
+// ----------------------------------------------------------------- kernel
+
+struct GemmSmem {
+    uint64_t full[GSTAGES];
+    uint64_t empty[GSTAGES];
+    uint64_t acc_full;
+    uint32_t tmem_base;
+    int64_t col_off[GN];
+};
+
+// KIND 0: bf16 pieces (64 elements per k-block); KIND 1: tf32 pieces (32).
+template <int KIND>
+__global__ void __launch_bounds__(G_THREADS, 1)
+    k_gemm_split3(const __grid_constant__ CUtensorMap tmAh, const __grid_constant__ CUtensorMap tmAl,
+                  const __grid_constant__ CUtensorMap tmBh, const __grid_constant__ CUtensorMap tmBl, int M, int N,
+                  int nkb, double *C, GemmEpi epi, double alpha, double beta, int *status) {
+    extern __shared__ __align__(1024) uint8_t g_smem[];
+    // operand stages first (1024-byte aligned), then the control block
+    uint8_t *base = (uint8_t *)(((uintptr_t)g_smem + 1023) & ~(uintptr_t)1023);
+    constexpr uint32_t A_BYTES = GM * GK_BYTES, B_BYTES = GN * GK_BYTES;
+    constexpr uint32_t STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;
+    GemmSmem *cs = (GemmSmem *)(base + GSTAGES * STAGE_BYTES);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int n0 = blockIdx.x * GN, m0 = blockIdx.y * GM;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < GSTAGES; s++) {
+            mbar_init(smem_u32(&cs->full[s]), 1);
+            mbar_init(smem_u32(&cs->empty[s]), 1);
+        }
+        mbar_init(smem_u32(&cs->acc_full), 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        tma_prefetch_desc(&tmAh);
+        tma_prefetch_desc(&tmAl);
+        tma_prefetch_desc(&tmBh);
+        tma_prefetch_desc(&tmBl);
+    }
+    for (int j = threadIdx.x; j < GN; j += G_THREADS) {
+        int64_t n = n0 + j;
+        cs->col_off[j] = (n / epi.cdiv) * epi.cs1 + (n % epi.cdiv) * epi.cs2;
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         smem_u32(&cs->tmem_base)),
+                     "r"(GN)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = cs->tmem_base;
+
+    if (warp == 0 && lane == 0) {
+        // ---------------- TMA producer
+        int issued = 0;
+        for (int kb = 0; kb < nkb; kb++) {
+            const int s = kb % GSTAGES;
+            const uint32_t ph = (uint32_t)(kb / GSTAGES) & 1u;
+            if (!mbar_wait(smem_u32(&cs->empty[s]), ph ^ 1u, status)) break;
+            uint8_t *st = base + s * STAGE_BYTES;
+            const uint32_t fb = smem_u32(&cs->full[s]);
+            mbar_expect_tx(fb, STAGE_BYTES);
+            const int kc = kb * (KIND == 0 ? 64 : 32);
+            tma_load_2d(smem_u32(st), &tmAh, fb, kc, m0);
+            tma_load_2d(smem_u32(st + A_BYTES), &tmAl, fb, kc, m0);
+            tma_load_2d(smem_u32(st + 2 * A_BYTES), &tmBh, fb, kc, n0);
+            tma_load_2d(smem_u32(st + 2 * A_BYTES + B_BYTES), &tmBl, fb, kc, n0);
+            issued = kb + 1;
+        }
+        // on an early exit, wait (bounded) for the copies still landing in shared memory
+        if (*(volatile int *)status != 0) {
+            int first = issued - GSTAGES < 0 ? 0 : issued - GSTAGES;
+            for (int kb = first; kb < issued; kb++)
+                mbar_wait_quiet(smem_u32(&cs->full[kb % GSTAGES]), (uint32_t)(kb / GSTAGES) & 1u);
+        }
+    } else if (warp == 1 && lane == 0) {
+        // ---------------- MMA issuer
+        constexpr uint32_t idesc = (1u << 4)                          // D: f32
+                                   | ((KIND == 0 ? 1u : 2u) << 7)     // A: bf16 | tf32
+                                   | ((KIND == 0 ? 1u : 2u) << 10)    // B: bf16 | tf32
+                                   | ((uint32_t)(GN >> 3) << 17)      // N
+                                   | ((uint32_t)(GM >> 4) << 24);     // M
+        constexpr int KSTEPS = (KIND == 0) ? 4 : 4;  // 32-byte k-steps per 128-byte row
+        for (int kb = 0; kb < nkb; kb++) {
+            const int s = kb % GSTAGES;
+            const uint32_t ph = (uint32_t)(kb / GSTAGES) & 1u;
+            if (!mbar_wait(smem_u32(&cs->full[s]), ph, status)) break;
+            tc_fence_after();
+            const uint32_t st = smem_u32(base + s * STAGE_BYTES);
+            const uint64_t ah = sw128_desc(st), al = sw128_desc(st + A_BYTES), bh = sw128_desc(st + 2 * A_BYTES),
+                           bl = sw128_desc(st + 2 * A_BYTES + B_BYTES);
+#pragma unroll
+            for (int k = 0; k < KSTEPS; k++) {
+                const uint64_t dk = (uint64_t)(k * 32) >> 4;  // advance 32 bytes along K
+                const uint32_t first = (kb | k) != 0;
+                umma<KIND>(tmem, ah + dk, bh + dk, idesc, first);
+                umma<KIND>(tmem, ah + dk, bl + dk, idesc, 1u);
+                umma<KIND>(tmem, al + dk, bh + dk, idesc, 1u);
+            }
+            umma_commit(smem_u32(&cs->empty[s]));  // stage free once these MMAs retire
+        }
+        umma_commit(smem_u32(&cs->acc_full));  // accumulator complete (or drained after an abort)
+    } else if (warp >= 2) {
+        // ---------------- epilogue: TMEM -> FP64 C
+        const int q = warp & 3;  // TMEM lane quarter of this warp
+        bool ok = mbar_wait(smem_u32(&cs->acc_full), 0u, status);
+        ok = __all_sync(0xffffffffu, ok && *(volatile int *)status == 0);  // tcgen05.ld is warp-collective
+        tc_fence_after();
+        const int m = m0 + q * 32 + lane;
+        if (ok) {
+            const int64_t roff = ((int64_t)m / epi.rdiv) * epi.rs1 + ((int64_t)m % epi.rdiv) * epi.rs2;
+            for (int c = 0; c < GN; c += 32) {
+                float v[32];
+                tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)c, v);
+                if (m < M) {
+#pragma unroll
+                    for (int j = 0; j < 32; j++) {
+                        if (n0 + c + j < N) {
+                            double *p = C + roff + cs->col_off[c + j];
+                            double x = alpha * (double)v[j];
+                            *p = (beta == 0.0) ? x : fma(beta, *p, x);
+                        }
+                    }
+                }
+            }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 1) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(GN) : "memory");
+    }
+}
+
+// ----------------------------------------------------------------- split kernels
+
+// x = hi + lo with hi = bf16(x), lo = bf16(x - hi).
+__device__ __forceinline__ void split_bf16(double x, __nv_bfloat16 &hi, __nv_bfloat16 &lo) {
+    hi = __float2bfloat16_rn((float)x);
+    lo = __float2bfloat16_rn((float)(x - (double)__bfloat162float(hi)));
+}
+
+// x = hi + lo with hi, lo rounded to tf32 (10 explicit mantissa bits).
+__device__ __forceinline__ float round_tf32(float f) {
+    uint32_t u = __float_as_uint(f);
+    if ((u & 0x7f800000u) == 0x7f800000u) return f;
+    u += 0x1000u;  // round half away from zero on the 13 dropped bits
+    u &= 0xffffe000u;
+    return __uint_as_float(u);
+}
+__device__ __forceinline__ void split_tf32(double x, float &hi, float &lo) {
+    hi = round_tf32((float)x);
+    lo = round_tf32((float)(x - (double)hi));
+}
+
+// Generic split of a strided FP64 operand into K-major pieces:
+//   dst[m][k] for m < M, k < Kp (k >= K zero-filled) from
+//   src[(m / mdiv)*ms1 + (m % mdiv)*ms2 + (k / kdiv)*ks1 + (k % kdiv)*ks2].
+// 32x32 tiles through shared memory so both sides are coalesced whichever
+// index is contiguous in the source.
+struct SplitMap {
+    int64_t mdiv, ms1, ms2, kdiv, ks1, ks2;
+};
+
+template <int KIND>
+__global__ void k_split(const double *src, void *hi, void *lo, int64_t M, int64_t K, int64_t Kp, SplitMap mp) {
+    __shared__ double tile[32][33];
+    const int64_t mt = (int64_t)blockIdx.y * 32, kt = (int64_t)blockIdx.x * 32;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8 threads
+    // read: pick the tile orientation that keeps the source reads contiguous
+    const bool k_fast = mp.ks2 == 1 && mp.kdiv >= 32;
+    const int mdiv = (int)mp.mdiv, kdiv = (int)mp.kdiv;
+    for (int r = ty; r < 32; r += 8) {
+        int m = (int)mt + (k_fast ? r : tx), k = (int)kt + (k_fast ? tx : r);
+        double v = 0.0;
+        if (m < M && k < K)
+            v = src[(int64_t)(m / mdiv) * mp.ms1 + (int64_t)(m % mdiv) * mp.ms2 + (int64_t)(k / kdiv) * mp.ks1 +
+                    (int64_t)(k % kdiv) * mp.ks2];
+        if (k_fast)
+            tile[r][tx] = v;
+        else
+            tile[tx][r] = v;
+    }
+    __syncthreads();
+    for (int r = ty; r < 32; r += 8) {
+        int64_t m = mt + r, k = kt + tx;
+        if (m >= M || k >= Kp) continue;
+        double v = tile[r][tx];
+        if (KIND == 0) {
+            __nv_bfloat16 h, l;
+            split_bf16(v, h, l);
+            ((__nv_bfloat16 *)hi)[m * Kp + k] = h;
+            ((__nv_bfloat16 *)lo)[m * Kp + k] = l;
+        } else {
+            float h, l;
+            split_tf32(v, h, l);
+            ((float *)hi)[m * Kp + k] = h;
+            ((float *)lo)[m * Kp + k] = l;
+        }
+    }
+}
+
+// ----------------------------------------------------------------- host side
+
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static EncodeTiledFn encode_fn() {
+    static EncodeTiledFn fn = nullptr;
+    if (!fn) {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (EncodeTiledFn)p;
+    }
+    return fn;
+}
+
+// 2-D K-major piece [rows][Kp] with a (k-block x box_rows) box, 128-byte swizzle.
+static int make_map(CUtensorMap *map, const void *ptr, int kind, int64_t rows, int64_t Kp, int box_rows) {
+    EncodeTiledFn fn = encode_fn();
+    if (!fn) {
+        set_error("cuTensorMapEncodeTiled is unavailable");
+        return DCC_ERR_CUDA;
+    }
+    const int esz = kind == 0 ? 2 : 4;
+    cuuint64_t dims[2] = {(cuuint64_t)Kp, (cuuint64_t)rows};
+    cuuint64_t strides[1] = {(cuuint64_t)(Kp * esz)};
+    cuuint32_t box[2] = {(cuuint32_t)(GK_BYTES / esz), (cuuint32_t)box_rows};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult r = fn(map, kind == 0 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2,
+                    const_cast<void *>(ptr), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                    CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) {
+        set_error("cuTensorMapEncodeTiled failed (%d)", (int)r);
+        return DCC_ERR_CUDA;
+    }
+    return DCC_OK;
+}
+
+static size_t gemm_smem_bytes() {
+    return 1024 + GSTAGES * (size_t)(2 * GM * GK_BYTES + 2 * GN * GK_BYTES) + sizeof(GemmSmem);
+}
+
+}  // namespace dcc
+
+using namespace dcc;
+
+extern "C" int dcc_split_operand(const double *src, void *hi, void *lo, int64_t M, int64_t K, int64_t Kp,
+                                 const int64_t *map6, int kind, void *stream) {
+    clear_error();
+    DCC_REQUIRE(M >= 0 && K >= 0 && Kp >= K, DCC_ERR_SHAPE, "bad split sizes (M=%lld K=%lld Kp=%lld)",
+                (long long)M, (long long)K, (long long)Kp);
+    DCC_REQUIRE(kind == 0 || kind == 1, DCC_ERR_UNSUPPORTED, "split kind must be 0 (bf16) or 1 (tf32)");
+    if (M == 0 || Kp == 0) return DCC_OK;
+    DCC_REQUIRE(src && hi && lo && map6, DCC_ERR_NULL, "NULL buffer");
+    SplitMap mp{map6[0], map6[1], map6[2], map6[3], map6[4], map6[5]};
+    DCC_REQUIRE(mp.mdiv > 0 && mp.kdiv > 0, DCC_ERR_SHAPE, "split map divisors must be positive");
+    DCC_REQUIRE(M < (1ll << 31) && Kp < (1ll << 31) && mp.mdiv < (1ll << 31) && mp.kdiv < (1ll << 31), DCC_ERR_SHAPE,
+                "split sizes must fit in 31 bits");
+    dim3 grid(ceil_div(Kp, 32), ceil_div(M, 32));
+    DCC_REQUIRE(grid.y <= 65535, DCC_ERR_UNSUPPORTED, "M too large for one split launch");
+    if (kind == 0)
+        k_split<0><<<grid, 256, 0, as_stream(stream)>>>(src, hi, lo, M, K, Kp, mp);
+    else
+        k_split<1><<<grid, 256, 0, as_stream(stream)>>>(src, hi, lo, M, K, Kp, mp);
+    return launch_status("split_operand");
+}
+
+extern "C" int dcc_gemm_split3(const void *A_hi, const void *A_lo, const void *B_hi, const void *B_lo, int64_t M,
+                               int64_t N, int64_t Kp, double *C, const int64_t *epi6, double alpha, double beta,
+                               int kind, int *status, void *stream) {
+    clear_error();
+    DCC_REQUIRE(kind == 0 || kind == 1, DCC_ERR_UNSUPPORTED, "kind must be 0 (bf16x3) or 1 (tf32x3)");
+    const int kblk = kind == 0 ? 64 : 32;
+    DCC_REQUIRE(M >= 0 && N >= 0 && Kp >= 0 && Kp % kblk == 0, DCC_ERR_SHAPE,
+                "Kp (%lld) must be a multiple of %d", (long long)Kp, kblk);
+    DCC_REQUIRE(M < (1ll << 31) && N < (1ll << 31), DCC_ERR_SHAPE, "M, N must fit in 31 bits");
+    if (M == 0 || N == 0) return DCC_OK;
+    DCC_REQUIRE(A_hi && A_lo && B_hi && B_lo && C && epi6 && status, DCC_ERR_NULL, "NULL buffer");
+    DCC_REQUIRE(Kp > 0, DCC_ERR_SHAPE, "empty contraction");
+    GemmEpi epi{epi6[0], epi6[1], epi6[2], epi6[3], epi6[4], epi6[5]};
+    DCC_REQUIRE(epi.rdiv > 0 && epi.cdiv > 0, DCC_ERR_SHAPE, "epilogue divisors must be positive");
+    CUtensorMap mAh, mAl, mBh, mBl;
+    int rc;
+    if ((rc = make_map(&mAh, A_hi, kind, M, Kp, GM)) || (rc = make_map(&mAl, A_lo, kind, M, Kp, GM)) ||
+        (rc = make_map(&mBh, B_hi, kind, N, Kp, GN)) || (rc = make_map(&mBl, B_lo, kind, N, Kp, GN)))
+        return rc;
+    size_t smem = gemm_smem_bytes();
+    dim3 grid(ceil_div(N, GN), ceil_div(M, GM));
+    DCC_REQUIRE(grid.y <= 65535, DCC_ERR_UNSUPPORTED, "M too large for one launch");
+    cudaStream_t st = as_stream(stream);
+    int nkb = (int)(Kp / kblk);
+    if (kind == 0) {
+        cudaFuncSetAttribute(k_gemm_split3<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        k_gemm_split3<0><<<grid, G_THREADS, smem, st>>>(mAh, mAl, mBh, mBl, (int)M, (int)N, nkb, C, epi, alpha, beta,
+                                                        status);
+    } else {
+        cudaFuncSetAttribute(k_gemm_split3<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        k_gemm_split3<1><<<grid, G_THREADS, smem, st>>>(mAh, mAl, mBh, mBl, (int)M, (int)N, nkb, C, epi, alpha, beta,
+                                                        status);
+    }
+    return launch_status("gemm_split3");
+}

@@ -80,19 +80,38 @@ __device__ void build_orbit_set(OrbitSet &os, int t0, int t1, int t2) {
     __syncthreads();
 }
 
-// Value at axis permutation p of local position (x,y,z) in slot s.
-__device__ __forceinline__ double pv(const double *sm, const OrbitSet &os, int s, int p, int x, int y, int z) {
-    int l[3] = {x, y, z};
-    return sm[os.nbr[s][p] * SLOT + sidx(l[perm3(p, 0)], l[perm3(p, 1)], l[perm3(p, 2)])];
+// Value at axis permutation p of local position (x,y,z) in slot s; the six
+// maps are 0:(x,y,z) 1:(x,z,y) 2:(y,x,z) 3:(y,z,x) 4:(z,x,y) 5:(z,y,x).
+template <int P>
+__device__ __forceinline__ double pv(const double *sm, const int *nbr, int x, int y, int z) {
+    int o = nbr[P] * SLOT;
+    if (P == 0) return sm[o + sidx(x, y, z)];
+    if (P == 1) return sm[o + sidx(x, z, y)];
+    if (P == 2) return sm[o + sidx(y, x, z)];
+    if (P == 3) return sm[o + sidx(y, z, x)];
+    if (P == 4) return sm[o + sidx(z, x, y)];
+    return sm[o + sidx(z, y, x)];
 }
 
-__device__ __forceinline__ void load_orbit_tiles(double *sm, const OrbitSet &os, const double *blk, int nv) {
+__device__ __forceinline__ void cp_async8(double *smem, const double *gmem) {
+    unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
+}
+
+// Issue asynchronous copies of every slot of the orbit set of block `blk`
+// into `sm` (no wait): each thread has all of its loads in flight at once.
+__device__ __forceinline__ void load_orbit_tiles_async(double *sm, const OrbitSet &os, const double *blk, int nv) {
     for (int s = 0; s < os.nslot; s++) {
         const int X0 = os.tile[s][0] * TE, Y0 = os.tile[s][1] * TE, Z0 = os.tile[s][2] * TE;
         for (int e = threadIdx.x; e < TE3; e += blockDim.x) {
             int x = e >> 6, y = (e >> 3) & 7, z = e & 7;
             int gx = X0 + x, gy = Y0 + y, gz = Z0 + z;
-            if (gx < nv && gy < nv && gz < nv) sm[s * SLOT + sidx(x, y, z)] = blk[((int64_t)gx * nv + gy) * nv + gz];
+            if (gx < nv && gy < nv && gz < nv) cp_async8(sm + s * SLOT + sidx(x, y, z), blk + ((int64_t)gx * nv + gy) * nv + gz);
         }
     }
 }
@@ -103,54 +122,69 @@ struct P3Coef {
 
 // Orbit-tile kernel.  MODE 0: P3 spin summation in place (out0 == in).
 // MODE 1: triple-sym (out0..out2).  MODE 2: transpose-add (out0).
+// Each CTA owns one canonical tile triple and walks the blocks
+// b = blockIdx.y, blockIdx.y + gridDim.y, ...; the copies of block b+gridDim.y
+// are in flight (double buffer) while block b is evaluated and stored.
 template <int MODE>
 __global__ void __launch_bounds__(OT_THREADS) k_orbit3(const double *in, double *out0, double *out1, double *out2,
                                                        int64_t nblocks, int nv, int ntile, P3Coef k) {
-    __shared__ double sm[6 * SLOT];
+    extern __shared__ double sm[];  // 2 x 6 x SLOT doubles
     __shared__ OrbitSet os;
     int t0, t1, t2;
     decode_tri3(blockIdx.x, ntile, t0, t1, t2);
     build_orbit_set(os, t0, t1, t2);
     const int64_t n3 = (int64_t)nv * nv * nv;
-    for (int64_t b = blockIdx.y; b < nblocks; b += gridDim.y) {
-        const double *src = in + b * n3;
-        load_orbit_tiles(sm, os, src, nv);
+    int64_t b = blockIdx.y;
+    if (b >= nblocks) return;
+    load_orbit_tiles_async(sm, os, in + b * n3, nv);
+    cp_async_commit();
+    for (int stage = 0; b < nblocks; b += gridDim.y, stage ^= 1) {
+        const int64_t nb = b + gridDim.y;
+        if (nb < nblocks) {
+            load_orbit_tiles_async(sm + (stage ^ 1) * 6 * SLOT, os, in + nb * n3, nv);
+            cp_async_commit();
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
+        }
         __syncthreads();
+        const double *buf = sm + stage * 6 * SLOT;
         for (int s = 0; s < os.nslot; s++) {
             const int X0 = os.tile[s][0] * TE, Y0 = os.tile[s][1] * TE, Z0 = os.tile[s][2] * TE;
+            const int *nbr = os.nbr[s];
             for (int e = threadIdx.x; e < TE3; e += blockDim.x) {
                 int x = e >> 6, y = (e >> 3) & 7, z = e & 7;
                 int gx = X0 + x, gy = Y0 + y, gz = Z0 + z;
                 if (gx >= nv || gy >= nv || gz >= nv) continue;
                 int64_t g = b * n3 + ((int64_t)gx * nv + gy) * nv + gz;
-                double a0 = pv(sm, os, s, 0, x, y, z);
+                double a0 = pv<0>(buf, nbr, x, y, z);
                 if (MODE == 0) {
                     double r;
                     if (gx == gy && gy == gz) {
                         r = dadd(dmul(k.beta, a0), dmul(k.ap34, dmul(k.p012, a0)));
                     } else {
                         // T(u) = p0 A(u) + p1 A(u2,u1,u0) + p2 A(u1,u0,u2); T at (u0,u2,u1)
-                        double tu = dadd(dadd(dmul(k.p0, a0), dmul(k.p1, pv(sm, os, s, 5, x, y, z))),
-                                         dmul(k.p2, pv(sm, os, s, 2, x, y, z)));
-                        double tw = dadd(dadd(dmul(k.p0, pv(sm, os, s, 1, x, y, z)), dmul(k.p1, pv(sm, os, s, 3, x, y, z))),
-                                         dmul(k.p2, pv(sm, os, s, 4, x, y, z)));
+                        double tu = dadd(dadd(dmul(k.p0, a0), dmul(k.p1, pv<5>(buf, nbr, x, y, z))),
+                                         dmul(k.p2, pv<2>(buf, nbr, x, y, z)));
+                        double tw = dadd(dadd(dmul(k.p0, pv<1>(buf, nbr, x, y, z)), dmul(k.p1, pv<3>(buf, nbr, x, y, z))),
+                                         dmul(k.p2, pv<4>(buf, nbr, x, y, z)));
                         r = dadd(dmul(k.beta, a0), dmul(k.alpha, dadd(dmul(k.p3, tu), dmul(k.p4, tw))));
                     }
                     out0[g] = r;
                 } else if (MODE == 1) {
-                    double bac = pv(sm, os, s, 2, x, y, z), acb = pv(sm, os, s, 1, x, y, z),
-                           cba = pv(sm, os, s, 5, x, y, z);
+                    double bac = pv<2>(buf, nbr, x, y, z), acb = pv<1>(buf, nbr, x, y, z),
+                           cba = pv<5>(buf, nbr, x, y, z);
                     double two = dmul(2.0, a0);
                     double d0 = dsub(dsub(two, acb), cba);
                     out0[g] = d0;
                     out1[g] = dsub(dsub(two, bac), acb);
                     out2[g] = dsub(dadd(d0, acb), bac);
                 } else {
-                    out0[g] = dadd(a0, pv(sm, os, s, 4, x, y, z));
+                    out0[g] = dadd(a0, pv<4>(buf, nbr, x, y, z));
                 }
             }
         }
-        __syncthreads();
+        __syncthreads();  // buf is refilled two iterations later
     }
 }
 
@@ -175,54 +209,96 @@ static int orbit3_launch(int mode, const double *in, double *o0, double *o1, dou
     if (nblocks == 0 || nvir == 0) return DCC_OK;
     int ntile = (int)ceil_div(nvir, TE);
     int64_t ntri = (int64_t)ntile * (ntile + 1) * (ntile + 2) / 6;
-    dim3 grid((unsigned)ntri, (unsigned)(nblocks < 65535 ? nblocks : 65535));
+    // about 8 CTA waves of 148 SMs x 4 resident CTAs, each CTA walking several blocks
+    int64_t gy = (148 * 4 * 8 + ntri - 1) / ntri;
+    gy = gy < 1 ? 1 : (gy > nblocks ? nblocks : gy);
+    gy = gy > 65535 ? 65535 : gy;
+    dim3 grid((unsigned)ntri, (unsigned)gy);
+    size_t smem = 2 * 6 * SLOT * sizeof(double);
     cudaStream_t st = as_stream(stream);
+    if (mode == 0) cudaFuncSetAttribute(k_orbit3<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (mode == 1) cudaFuncSetAttribute(k_orbit3<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (mode == 2) cudaFuncSetAttribute(k_orbit3<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (mode == 0)
-        k_orbit3<0><<<grid, OT_THREADS, 0, st>>>(in, o0, o1, o2, nblocks, (int)nvir, ntile, k);
+        k_orbit3<0><<<grid, OT_THREADS, smem, st>>>(in, o0, o1, o2, nblocks, (int)nvir, ntile, k);
     else if (mode == 1)
-        k_orbit3<1><<<grid, OT_THREADS, 0, st>>>(in, o0, o1, o2, nblocks, (int)nvir, ntile, k);
+        k_orbit3<1><<<grid, OT_THREADS, smem, st>>>(in, o0, o1, o2, nblocks, (int)nvir, ntile, k);
     else
-        k_orbit3<2><<<grid, OT_THREADS, 0, st>>>(in, o0, o1, o2, nblocks, (int)nvir, ntile, k);
+        k_orbit3<2><<<grid, OT_THREADS, smem, st>>>(in, o0, o1, o2, nblocks, (int)nvir, ntile, k);
     return launch_status("orbit-tile T3 kernel");
 }
 
 // ---------------------------------------------------------------- unpack
 
-// out[n] = T3[ijk[n]] for any ordering; one CTA per (8^3 output tile, n).
+// out[n] = T3[ijk[n]] for any ordering.  A CTA owns one 8^3 output tile
+// position and walks n = blockIdx.y, blockIdx.y + gridDim.y, ...; the source
+// tile of the next n is copied asynchronously while the current one is
+// written out through the shared-memory transpose.
+struct TakeSrc {
+    int cs;
+    int64_t l;
+    int V[3];
+};
+
+__device__ __forceinline__ TakeSrc take_src(const int32_t *ijk, const int64_t *loc, int64_t n, int nocc,
+                                            const int T[3]) {
+    TakeSrc r;
+    int64_t s[3];
+    int i = ijk[3 * n], j = ijk[3 * n + 1], k = ijk[3 * n + 2];
+    bool ok = i >= 0 && j >= 0 && k >= 0 && i < nocc && j < nocc && k < nocc;
+    r.cs = order_case3(ok ? i : 0, ok ? j : 0, ok ? k : 0, s);
+    r.l = ok ? loc[ijk_linear(s[0], s[1], s[2], nocc)] : -1;
+    // output tile T comes from source tile V with V[perm3(cs,m)] = T[m]
+    for (int m = 0; m < 3; m++) r.V[perm3(r.cs, m)] = T[m];
+    return r;
+}
+
+__device__ __forceinline__ void take_load_async(double *sm, const double *t3, const TakeSrc &src, int nv) {
+    if (src.l < 0) return;
+    const double *blk = t3 + src.l * (int64_t)nv * nv * nv;
+    for (int e = threadIdx.x; e < TE3; e += blockDim.x) {
+        int x = e >> 6, y = (e >> 3) & 7, z = e & 7;
+        int gx = src.V[0] * TE + x, gy = src.V[1] * TE + y, gz = src.V[2] * TE + z;
+        if (gx < nv && gy < nv && gz < nv) cp_async8(sm + sidx(x, y, z), blk + ((int64_t)gx * nv + gy) * nv + gz);
+    }
+}
+
 __global__ void __launch_bounds__(OT_THREADS) k_take_t3(const double *t3, double *out, const int32_t *ijk,
                                                         const int64_t *loc, int64_t count, int nocc, int nv,
                                                         int ntile) {
-    __shared__ double sm[SLOT];
+    __shared__ double sm[2 * SLOT];
     const int64_t n3 = (int64_t)nv * nv * nv;
-    int T[3] = {(int)(blockIdx.x / (ntile * ntile)), (int)((blockIdx.x / ntile) % ntile), (int)(blockIdx.x % ntile)};
-    for (int64_t n = blockIdx.y; n < count; n += gridDim.y) {
-        int64_t s[3];
-        int i = ijk[3 * n], j = ijk[3 * n + 1], k = ijk[3 * n + 2];
-        bool ok = i >= 0 && j >= 0 && k >= 0 && i < nocc && j < nocc && k < nocc;
-        int cs = order_case3(ok ? i : 0, ok ? j : 0, ok ? k : 0, s);
-        int64_t l = ok ? loc[ijk_linear(s[0], s[1], s[2], nocc)] : -1;
-        double *dst = out + n * n3;
-        // output tile T <- source tile V with V[perm3(cs,m)] = T[m]
-        int V[3];
-        for (int m = 0; m < 3; m++) V[perm3(cs, m)] = T[m];
-        if (l >= 0) {
-            const double *src = t3 + l * n3;
-            for (int e = threadIdx.x; e < TE3; e += blockDim.x) {
-                int x = e >> 6, y = (e >> 3) & 7, z = e & 7;
-                int gx = V[0] * TE + x, gy = V[1] * TE + y, gz = V[2] * TE + z;
-                if (gx < nv && gy < nv && gz < nv) sm[sidx(x, y, z)] = src[((int64_t)gx * nv + gy) * nv + gz];
-            }
+    const int T[3] = {(int)(blockIdx.x / (ntile * ntile)), (int)((blockIdx.x / ntile) % ntile),
+                      (int)(blockIdx.x % ntile)};
+    int64_t n = blockIdx.y;
+    if (n >= count) return;
+    TakeSrc cur = take_src(ijk, loc, n, nocc, T);
+    take_load_async(sm, t3, cur, nv);
+    cp_async_commit();
+    for (int stage = 0; n < count; n += gridDim.y, stage ^= 1) {
+        const int64_t nn = n + gridDim.y;
+        TakeSrc nxt;
+        if (nn < count) {
+            nxt = take_src(ijk, loc, nn, nocc, T);
+            take_load_async(sm + (stage ^ 1) * SLOT, t3, nxt, nv);
+            cp_async_commit();
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
         }
         __syncthreads();
+        const double *buf = sm + stage * SLOT;
+        double *dst = out + n * n3;
         for (int e = threadIdx.x; e < TE3; e += blockDim.x) {
             int u[3] = {e >> 6, (e >> 3) & 7, e & 7};
             int gx = T[0] * TE + u[0], gy = T[1] * TE + u[1], gz = T[2] * TE + u[2];
             if (gx >= nv || gy >= nv || gz >= nv) continue;
             int v[3];
-            for (int m = 0; m < 3; m++) v[perm3(cs, m)] = u[m];
-            dst[((int64_t)gx * nv + gy) * nv + gz] = (l >= 0) ? sm[sidx(v[0], v[1], v[2])] : 0.0;
+            for (int m = 0; m < 3; m++) v[perm3(cur.cs, m)] = u[m];
+            dst[((int64_t)gx * nv + gy) * nv + gz] = (cur.l >= 0) ? buf[sidx(v[0], v[1], v[2])] : 0.0;
         }
         __syncthreads();
+        if (nn < count) cur = nxt;
     }
 }
 
@@ -241,65 +317,71 @@ __global__ void k_copy_blocks(const double *in, double *out, const int32_t *req,
 
 // ---------------------------------------------------------------- divide / update
 
+// One warp per row (q, a, b) of nvir contiguous elements; D_ab is formed once
+// per row, lanes stride over c.  D = (eia[i,a] + eia[j,b]) + eia[k,c].
 __global__ void k_r3_divide(double *r3, const double *eia, const int32_t *ijk, int64_t nblocks, int nv) {
-    const int64_t n3 = (int64_t)nv * nv * nv;
-    for (int64_t q = blockIdx.y; q < nblocks; q += gridDim.y) {
-        const double *ei = eia + (int64_t)ijk[3 * q] * nv, *ej = eia + (int64_t)ijk[3 * q + 1] * nv,
-                     *ek = eia + (int64_t)ijk[3 * q + 2] * nv;
-        double *blk = r3 + q * n3;
-        for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n3; e += (int64_t)gridDim.x * blockDim.x) {
-            int c = (int)(e % nv), b = (int)((e / nv) % nv), a = (int)(e / ((int64_t)nv * nv));
-            blk[e] = __ddiv_rn(blk[e], dadd(dadd(ei[a], ej[b]), ek[c]));
-        }
+    const int lane = threadIdx.x & 31;
+    const int64_t nrow = nblocks * nv * nv;
+    for (int64_t row = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; row < nrow;
+         row += ((int64_t)gridDim.x * blockDim.x) >> 5) {
+        int64_t q = row / (nv * nv);
+        int ab = (int)(row - q * nv * nv), a = ab / nv, b = ab - a * nv;
+        double dab = dadd(eia[(int64_t)ijk[3 * q] * nv + a], eia[(int64_t)ijk[3 * q + 1] * nv + b]);
+        const double *ek = eia + (int64_t)ijk[3 * q + 2] * nv;
+        double *r = r3 + row * nv;
+        for (int c = lane; c < nv; c += 32) r[c] = __ddiv_rn(r[c], dadd(dab, ek[c]));
     }
 }
 
 constexpr int UPD_THREADS = 256;
-constexpr int UPD_GRID_X = 64;
 
 __device__ __forceinline__ double warp_sum(double v) {
     for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
     return v;
 }
 
-// Fused divide + t3 update + squared norms; per-CTA partials go to ws[2*cta].
+// Fused divide + t3 update + squared norms, one warp per row (q, a, b);
+// per-CTA partials go to ws[2*cta].
 __global__ void __launch_bounds__(UPD_THREADS) k_t3_divide_update(double *t3, double *r3, const double *eia,
                                                                   const int32_t *ijk, int64_t nblocks, int nv,
                                                                   int nact, int write_r3, double *ws) {
-    const int64_t n3 = (int64_t)nv * nv * nv;
+    const int lane = threadIdx.x & 31;
+    const int64_t nrow = nblocks * nv * nv;
     double s_all = 0.0, s_act = 0.0;
-    for (int64_t q = blockIdx.y; q < nblocks; q += gridDim.y) {
-        const double *ei = eia + (int64_t)ijk[3 * q] * nv, *ej = eia + (int64_t)ijk[3 * q + 1] * nv,
-                     *ek = eia + (int64_t)ijk[3 * q + 2] * nv;
-        double *rb = r3 + q * n3, *tb = t3 + q * n3;
-        for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n3; e += (int64_t)gridDim.x * blockDim.x) {
-            int c = (int)(e % nv), b = (int)((e / nv) % nv), a = (int)(e / ((int64_t)nv * nv));
-            double r = __ddiv_rn(rb[e], dadd(dadd(ei[a], ej[b]), ek[c]));
-            if (write_r3) rb[e] = r;
-            tb[e] = dadd(tb[e], r);
+    for (int64_t row = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; row < nrow;
+         row += ((int64_t)gridDim.x * blockDim.x) >> 5) {
+        int64_t q = row / (nv * nv);
+        int ab = (int)(row - q * nv * nv), a = ab / nv, b = ab - a * nv;
+        double dab = dadd(eia[(int64_t)ijk[3 * q] * nv + a], eia[(int64_t)ijk[3 * q + 1] * nv + b]);
+        const double *ek = eia + (int64_t)ijk[3 * q + 2] * nv;
+        double *rr = r3 + row * nv, *tt = t3 + row * nv;
+        const bool act_ab = a < nact && b < nact;
+        for (int c = lane; c < nv; c += 32) {
+            double r = __ddiv_rn(rr[c], dadd(dab, ek[c]));
+            if (write_r3) rr[c] = r;
+            tt[c] = dadd(tt[c], r);
             double r2 = r * r;
             s_all += r2;
-            if (a < nact && b < nact && c < nact) s_act += r2;
+            if (act_ab && c < nact) s_act += r2;
         }
     }
     __shared__ double red[2][UPD_THREADS / 32];
     s_all = warp_sum(s_all);
     s_act = warp_sum(s_act);
     int w = threadIdx.x >> 5;
-    if ((threadIdx.x & 31) == 0) {
+    if (lane == 0) {
         red[0][w] = s_all;
         red[1][w] = s_act;
     }
     __syncthreads();
     if (threadIdx.x == 0) {
-        double a = 0.0, b = 0.0;
+        double x = 0.0, y = 0.0;
         for (int i = 0; i < UPD_THREADS / 32; i++) {
-            a += red[0][i];
-            b += red[1][i];
+            x += red[0][i];
+            y += red[1][i];
         }
-        int64_t cta = (int64_t)blockIdx.y * gridDim.x + blockIdx.x;
-        ws[2 * cta] = a;
-        ws[2 * cta + 1] = b;
+        ws[2 * blockIdx.x] = x;
+        ws[2 * blockIdx.x + 1] = y;
     }
 }
 
@@ -329,7 +411,11 @@ __global__ void k_sum_pairs(const double *ws, int64_t n, double *out) {
     }
 }
 
-static unsigned update_grid_y(int64_t nblocks) { return (unsigned)(nblocks < 4096 ? nblocks : 4096); }
+// 1-D grid of row-walking CTAs: 148 SMs x 8 resident CTAs x 4 waves at most.
+static unsigned row_grid(int64_t nrow, int threads) {
+    int64_t g = (nrow * 32 + threads - 1) / threads;
+    return (unsigned)(g < 148 * 32 ? (g ? g : 1) : 148 * 32);
+}
 
 // ---------------------------------------------------------------- IJK -> ABC
 
@@ -504,7 +590,11 @@ extern "C" int dcc_take_t3_batched(const double *t3_local, double *out, const in
     if (count == 0 || nvir == 0) return DCC_OK;
     DCC_REQUIRE(t3_local && out && ijk && ijk_to_local_idx, DCC_ERR_NULL, "NULL buffer");
     int ntile = (int)ceil_div(nvir, TE);
-    dim3 grid((unsigned)(ntile * ntile * ntile), (unsigned)(count < 65535 ? count : 65535));
+    int64_t nt3 = (int64_t)ntile * ntile * ntile;
+    int64_t gy = (148 * 8 * 8 + nt3 - 1) / nt3;
+    gy = gy < 1 ? 1 : (gy > count ? count : gy);
+    gy = gy > 65535 ? 65535 : gy;
+    dim3 grid((unsigned)nt3, (unsigned)gy);
     k_take_t3<<<grid, OT_THREADS, 0, as_stream(stream)>>>(t3_local, out, ijk, ijk_to_local_idx, count, (int)nocc,
                                                           (int)nvir, ntile);
     return launch_status("take_t3");
@@ -551,21 +641,13 @@ extern "C" int dcc_r3_tri_divide_e(double *r3, const double *eia, const int32_t 
     DCC_REQUIRE(nblocks >= 0 && nvir >= 0, DCC_ERR_SHAPE, "negative size");
     if (nblocks == 0 || nvir == 0) return DCC_OK;
     DCC_REQUIRE(r3 && eia && ijk, DCC_ERR_NULL, "NULL buffer");
-    int64_t n3 = nvir * nvir * nvir;
-    dim3 grid(ceil_div(n3, 256 * 8) < 64 ? ceil_div(n3, 256 * 8) : 64, update_grid_y(nblocks));
-    k_r3_divide<<<grid, 256, 0, as_stream(stream)>>>(r3, eia, ijk, nblocks, (int)nvir);
+    k_r3_divide<<<row_grid(nblocks * nvir * nvir, 256), 256, 0, as_stream(stream)>>>(r3, eia, ijk, nblocks, (int)nvir);
     return launch_status("r3_tri_divide_e");
-}
-
-static unsigned update_grid_x(int64_t nvir) {
-    int64_t n3 = nvir * nvir * nvir;
-    unsigned gx = ceil_div(n3, UPD_THREADS * 8);
-    return gx < (unsigned)UPD_GRID_X ? (gx ? gx : 1) : (unsigned)UPD_GRID_X;
 }
 
 extern "C" size_t dcc_t3_update_workspace_bytes(int64_t nblocks, int64_t nvir) {
     if (nblocks <= 0 || nvir <= 0) return 16;
-    return (size_t)update_grid_x(nvir) * update_grid_y(nblocks) * 2 * sizeof(double);
+    return (size_t)row_grid(nblocks * nvir * nvir, UPD_THREADS) * 2 * sizeof(double);
 }
 
 extern "C" int dcc_t3_divide_update(double *t3, double *r3, const double *eia, const int32_t *ijk, int64_t nblocks,
@@ -584,12 +666,12 @@ extern "C" int dcc_t3_divide_update(double *t3, double *r3, const double *eia, c
     DCC_REQUIRE(workspace_bytes >= need, DCC_ERR_WORKSPACE, "workspace needs %zu bytes, got %zu", need,
                 workspace_bytes);
     if (nvir_active < 0 || nvir_active > nvir) nvir_active = nvir;
-    dim3 grid(update_grid_x(nvir), update_grid_y(nblocks));
+    unsigned grid = row_grid(nblocks * nvir * nvir, UPD_THREADS);
     k_t3_divide_update<<<grid, UPD_THREADS, 0, st>>>(t3, r3, eia, ijk, nblocks, (int)nvir, (int)nvir_active,
                                                       write_r3, (double *)workspace);
     int rc = launch_status("t3_divide_update");
     if (rc) return rc;
-    k_sum_pairs<<<1, 256, 0, st>>>((const double *)workspace, (int64_t)grid.x * grid.y, norms);
+    k_sum_pairs<<<1, 256, 0, st>>>((const double *)workspace, (int64_t)grid, norms);
     return launch_status("t3_divide_update reduce");
 }
 

@@ -1,0 +1,155 @@
+"""Dense T3 residual contractions on the tensor cores (split-BF16x3 / TF32x3
+with FP32 accumulation, FP64 results) and their plain FP64 counterparts.
+
+The reference evaluates these as per-block `_einsum` calls with
+out=..., alpha, beta (distr_cc/rccsdt.py:385-427).  Here the whole batch of
+canonical blocks is one GEMM per einsum string: the FP64 operands are split
+once into two pieces (x = hi + lo), the GEMM accumulates
+A_hi B_hi + A_hi B_lo + A_lo B_hi in tensor memory, and the epilogue adds the
+result straight into the FP64 r3 with the einsum's output permutation.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+import torch
+
+from . import _lib as L
+
+f64 = torch.float64
+
+KIND = {"bf16x3": 0, "tf32x3": 1}
+_KBLK = {0: 64, 1: 32}
+
+_split = L.bind("dcc_split_operand", [L.c_vp, L.c_vp, L.c_vp, L.c_i64, L.c_i64, L.c_i64, L.c_vp, L.c_int, L.c_vp])
+_gemm = L.bind("dcc_gemm_split3", [L.c_vp] * 4 + [L.c_i64] * 3 + [L.c_vp, L.c_vp, L.c_dbl, L.c_dbl, L.c_int,
+                                                                   L.c_vp, L.c_vp])
+
+BIG = 1 << 40  # divisor that makes a level of the two-level map a plain stride
+
+
+def _i64x6(v):
+    a = (ctypes.c_int64 * 6)(*[int(x) for x in v])
+    return a
+
+
+def padded_k(K, kind):
+    b = _KBLK[kind]
+    return (K + b - 1) // b * b
+
+
+class Split:
+    """Two-piece K-major copy of an FP64 operand: rows M, contraction K padded to Kp."""
+
+    def __init__(self, M, K, kind, device="cuda", buffers=None):
+        self.M, self.K, self.kind = int(M), int(K), int(kind)
+        self.Kp = padded_k(self.K, self.kind)
+        dt = torch.bfloat16 if self.kind == 0 else torch.float32
+        if buffers is None:
+            self.hi = torch.empty((self.M, self.Kp), dtype=dt, device=device)
+            self.lo = torch.empty((self.M, self.Kp), dtype=dt, device=device)
+        else:
+            self.hi, self.lo = buffers
+
+    def fill(self, src, map6):
+        """dst[m][k] = src[(m/d0)*s1 + (m%d0)*s2 + (k/d1)*s3 + (k%d1)*s4]."""
+        L.as_tensor(src, f64, "src")
+        L.check(_split(L.ptr(src), L.ptr(self.hi), L.ptr(self.lo), self.M, self.K, self.Kp, _i64x6(map6), self.kind,
+                       L.stream_ptr()))
+        return self
+
+
+def gemm_(A, B, C, epi6, alpha=1.0, beta=1.0, status=None):
+    """C[row_off(m) + col_off(n)] = alpha * A B^T + beta * C (A: Split [M,K], B: Split [N,K])."""
+    if A.kind != B.kind or A.Kp != B.Kp:
+        raise ValueError("A and B must be split with the same kind and padded K")
+    L.as_tensor(C, f64, "C")
+    if status is None:
+        status = torch.zeros(1, dtype=torch.int32, device=C.device)
+    L.check(_gemm(L.ptr(A.hi), L.ptr(A.lo), L.ptr(B.hi), L.ptr(B.lo), A.M, B.M, A.Kp, L.ptr(C), _i64x6(epi6),
+                  float(alpha), float(beta), A.kind, L.ptr(status), L.stream_ptr()))
+    return status
+
+
+def matmul_split3(A, B, kind="bf16x3"):
+    """A @ B^T in split precision (test helper): A [M,K], B [N,K] FP64 CUDA tensors."""
+    k = KIND[kind]
+    M, K = A.shape
+    N = B.shape[0]
+    a = Split(M, K, k).fill(A.contiguous(), (BIG, 0, K, BIG, 0, 1))
+    b = Split(N, K, k).fill(B.contiguous(), (BIG, 0, K, BIG, 0, 1))
+    C = torch.zeros((M, N), dtype=f64, device=A.device)
+    st = gemm_(a, b, C, (BIG, 0, N, BIG, 0, 1), 1.0, 0.0)
+    return C, st
+
+
+# ----------------------------------------------------------------------------
+# W_vvvv . t3 (distr_cc/rccsdt.py:421-427), all canonical blocks at once
+#   r3[q,a,b,c] += sum_de W[a,b,d,e] t3[q,d,e,c]     'abde,dec->abc'
+#   r3[q,a,b,c] += sum_de W[a,c,d,e] t3[q,d,b,e]     'acde,dbe->abc'
+#   r3[q,a,b,c] += sum_de W[b,c,d,e] t3[q,a,d,e]     'bcde,ade->abc'
+# ----------------------------------------------------------------------------
+
+def wvvvv_maps(nv):
+    """(A split map, epilogue map) of the three einsum strings for blocks of nv^3."""
+    n2, n3 = nv * nv, nv ** 3
+    return [
+        # 'abde,dec->abc': rows (q,c), K (d,e): t3[q][d][e][c]; out r3[q][a][b][c] = (q,c) x (a,b)
+        ((nv, n3, 1, BIG, 0, nv), (nv, n3, 1, BIG, 0, nv)),
+        # 'acde,dbe->abc': rows (q,b), K (d,e): t3[q][d][b][e]; out (q,b) x (a,c)
+        ((nv, n3, nv, nv, n2, 1), (nv, n3, nv, nv, n2, 1)),
+        # 'bcde,ade->abc': rows (q,a), K (d,e): t3[q][a][d][e]; out (q,a) x (b,c)
+        ((BIG, 0, n2, BIG, 0, 1), (nv, n3, n2, BIG, 0, 1)),
+    ]
+
+
+class WvvvvT3:
+    """Split-precision W_vvvv . t3 for a fixed (nblocks, nvir); buffers are reused across calls."""
+
+    def __init__(self, nblocks, nvir, kind="bf16x3", device="cuda"):
+        self.n, self.nv, self.kind = int(nblocks), int(nvir), KIND[kind]
+        K = nvir * nvir
+        self.W = Split(K, K, self.kind, device)
+        self.A = Split(self.n * nvir, K, self.kind, device)
+        self.status = torch.zeros(1, dtype=torch.int32, device=device)
+        self.maps = wvvvv_maps(nvir)
+
+    def __call__(self, r3, W, t3, alpha=1.0):
+        nv = self.nv
+        L.as_tensor(r3, f64, "r3")
+        L.as_tensor(t3, f64, "t3")
+        self.W.fill(W.reshape(nv * nv, nv * nv), (BIG, 0, nv * nv, BIG, 0, 1))
+        for amap, emap in self.maps:
+            self.A.fill(t3, amap)
+            gemm_(self.A, self.W, r3, emap, alpha, 1.0, self.status)
+        return r3
+
+
+def wvvvv_t3_fp64_(r3, W, t3, alpha=1.0):
+    """Plain FP64 GPU path of the same three einsums (cuBLAS DGEMM through torch)."""
+    n, nv = t3.shape[0], t3.shape[1]
+    W2 = W.reshape(nv * nv, nv * nv)
+    # 'abde,dec->abc': (ab) x (de) . (de) x c per block
+    r3.view(n, nv * nv, nv).add_(torch.matmul(W2, t3.view(n, nv * nv, nv)), alpha=alpha)
+    # 'acde,dbe->abc': X[q,b,(ac)] = t3[q][d][b][e] as [q][b][(de)] . W2^T
+    X = torch.matmul(t3.permute(0, 2, 1, 3).reshape(n, nv, nv * nv), W2.t())  # [q][b][(a c)]
+    r3.add_(X.view(n, nv, nv, nv).permute(0, 2, 1, 3), alpha=alpha)
+    # 'bcde,ade->abc': [q a][(de)] . W2^T -> [q a][(bc)]
+    r3.view(n * nv, nv * nv).add_(torch.matmul(t3.view(n * nv, nv * nv), W2.t()), alpha=alpha)
+    return r3
+
+
+def wvvvv_flops(nblocks, nvir):
+    """Algorithmic FLOPs of the three einsums (2 M N K each)."""
+    return 3 * 2 * nblocks * nvir ** 5
+
+
+def einsum_reference(W, t3):
+    """numpy FP64 restatement of the three einsums (test oracle helper)."""
+    r = np.zeros_like(t3)
+    for q in range(t3.shape[0]):
+        r[q] += np.einsum("abde,dec->abc", W, t3[q])
+        r[q] += np.einsum("acde,dbe->abc", W, t3[q])
+        r[q] += np.einsum("bcde,ade->abc", W, t3[q])
+    return r

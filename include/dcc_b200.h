@@ -201,6 +201,31 @@ DCC_API int dcc_q_task_epilogue(const double *t4, const double *z4, const double
                         int64_t c0, int64_t c1, int64_t d0, int64_t d1, int64_t blksize, int64_t nocc,
                         int64_t nvir, double *out, void *workspace, size_t workspace_bytes, void *stream);
 
+/* ----------------------------------------------------------------------
+ * Split-precision tensor-core contractions (the dense T3/T4 residual terms)
+ * ---------------------------------------------------------------------- */
+
+/* Split an FP64 operand into two K-major pieces, x = hi + lo:
+ *   dst[m][k] (m < M, k < Kp; k >= K zero-filled) from
+ *   src[(m/d0)*s1 + (m%d0)*s2 + (k/d1)*s3 + (k%d1)*s4], map6 = {d0,s1,s2,d1,s3,s4}
+ * (HOST array).  kind 0: bf16 pieces (Kp multiple of 64), kind 1: tf32
+ * pieces stored as float (Kp multiple of 32).  Replaces the FP64 operand of
+ * the _einsum calls of distr_cc/rccsdt.py:385-427 (PySCF _einsum backend). */
+DCC_API int dcc_split_operand(const double *src, void *hi, void *lo, int64_t M, int64_t K, int64_t Kp,
+                              const int64_t *map6, int kind, void *stream);
+
+/* C[row_off(m) + col_off(n)] = alpha * (A_hi B_hi + A_hi B_lo + A_lo B_hi)[m][n]
+ * + beta * C, FP32 accumulation in tensor memory (tcgen05), FP64 C.  A is
+ * [M][Kp], B is [N][Kp] (pieces from dcc_split_operand).  epi6 = {rdiv, rs1,
+ * rs2, cdiv, cs1, cs2} (HOST): row_off(m) = (m/rdiv)*rs1 + (m%rdiv)*rs2,
+ * col_off(n) = (n/cdiv)*cs1 + (n%cdiv)*cs2.  *status (DEVICE int, zero before
+ * the call) becomes DCC_ERR_TIMEOUT if a bounded wait gave up.  Replaces the
+ * out=..., alpha, beta semantics of the _einsum calls at distr_cc/rccsdt.py:421-427
+ * ("abde,dec->abc", "acde,dbe->abc", "bcde,ade->abc"). */
+DCC_API int dcc_gemm_split3(const void *A_hi, const void *A_lo, const void *B_hi, const void *B_lo, int64_t M,
+                            int64_t N, int64_t Kp, double *C, const int64_t *epi6, double alpha, double beta,
+                            int kind, int *status, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
