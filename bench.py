@@ -1,0 +1,373 @@
+"""Benchmark: one RCCSDT T3 iteration on the kernel-level synthetic workload
+(nocc=10, nvir=90, 220 canonical i<=j<=k blocks of 90^3, FP64 storage).
+
+A step is one pass of the triples hot path over the 220 blocks:
+  r3 = W_vvvo.t2 - W_vooo.t2 + F_vv.t3 + W_vvvv.t3      (compute_r3_tri terms)
+  r3 <- P3_full(r3, -1/6, 1); r3 /= D; t3 += r3; |r3|^2 (update)
+with the large contractions as split-BF16x3 tcgen05 GEMMs (FP32 accumulate,
+FP64 storage, denominators, update and norms).  The same step on the plain
+FP64 GPU path (cuBLAS DGEMM) is timed beside it.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+N > 1 (torchrun): every rank runs an independent replica of the workload
+(value = all ranks' iterations / max time).  Prints one JSON line on rank 0.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "distributed-cc_b200"))
+
+NOCC, NVIR = 10, 90
+METRIC = "RCCSDT T3 iteration time (mixed split-BF16x3 batched path), nocc=10 nvir=90 synthetic"
+UNIT = "s/iter"
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return d.get("hbm_gbs", 6650.0), d.get("bf16_tflops", 1590.0), d.get("bf16_tflops_sustained", 1400.0), "measured"
+    return 6650.0, 1590.0, 1400.0, "fallback"
+
+
+def profile_traffic(name):
+    """Per-launch DRAM bytes of a kernel from a committed ncu summary (profiles/<name>.md)."""
+    p = os.path.join(ROOT, "profiles", name + ".md")
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        if line.strip().startswith("traffic_bytes_per_launch:"):
+            try:
+                return float(line.split(":", 1)[1].strip())
+            except ValueError:
+                return None
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples every 200 ms while the timed region runs."""
+
+    def __init__(self, index=0):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is None:
+            return
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        self.lines = [l for l in out.splitlines() if l.strip()]
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in self.lines:
+            f = [x.strip() for x in l.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# --------------------------------------------------------------------------- CPU side
+
+def cpu_sample(nblk_sample=2, seed=0):
+    """The reference's CPU path of one step on a bounded sample of blocks: the
+    reference C helpers (oracle/_ref, OpenMP) for P3 symmetrize and division,
+    numpy (BLAS) for the einsums.  Returns seconds for the sample and the
+    scale factor to the full 220-block step."""
+    import numpy as np
+    import ctypes
+    os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count()))
+    from oracle.oracle import Reference, reference_available, Oracle
+    rng = np.random.default_rng(seed)
+    no, nv = NOCC, NVIR
+    trip = [(i, j, k) for i in range(no) for j in range(i, no) for k in range(j, no)]
+    sample = trip[::len(trip) // nblk_sample][:nblk_sample]
+    W_vvvv = rng.standard_normal((nv,) * 4) * 0.1
+    W_vvvo = rng.standard_normal((nv, nv, nv, no)) * 0.1
+    W_vooo = rng.standard_normal((nv, no, no, no)) * 0.1
+    F_vv = np.diag(rng.uniform(0.1, 3.0, nv))
+    t2 = rng.standard_normal((no, no, nv, nv)) * 1e-2
+    t3 = rng.standard_normal((len(sample), nv, nv, nv)) * 1e-3
+    eia = rng.uniform(-4.5, -0.4, (no, nv))
+    use_ref = reference_available()
+    lib = Reference() if use_ref else Oracle()
+    e = lambda s, a, b: np.einsum(s, a, b, optimize=True)  # noqa: E731
+    t0 = time.perf_counter()
+    r3 = np.empty_like(t3)
+    for q, (i, j, k) in enumerate(sample):
+        r = e('abd,dc->abc', W_vvvo[..., j], t2[i, k])
+        r += e('acd,db->abc', W_vvvo[..., k], t2[i, j])
+        r += e('bad,dc->abc', W_vvvo[..., i], t2[j, k])
+        r += e('bcd,da->abc', W_vvvo[..., k], t2[j, i])
+        r += e('cad,db->abc', W_vvvo[..., i], t2[k, j])
+        r += e('cbd,da->abc', W_vvvo[..., j], t2[k, i])
+        r -= e('al,lbc->abc', W_vooo[:, :, i, j], t2[:, k])
+        r -= e('al,lcb->abc', W_vooo[:, :, i, k], t2[:, j])
+        r -= e('bl,lac->abc', W_vooo[:, :, j, i], t2[:, k])
+        r -= e('bl,lca->abc', W_vooo[:, :, j, k], t2[:, i])
+        r -= e('cl,lab->abc', W_vooo[:, :, k, i], t2[:, j])
+        r -= e('cl,lba->abc', W_vooo[:, :, k, j], t2[:, i])
+        r += e('ad,dbc->abc', F_vv, t3[q])
+        r += e('bd,adc->abc', F_vv, t3[q])
+        r += e('cd,abd->abc', F_vv, t3[q])
+        r += e('abde,dec->abc', W_vvvv, t3[q])
+        r += e('acde,dbe->abc', W_vvvv, t3[q])
+        r += e('bcde,ade->abc', W_vvvv, t3[q])
+        r3[q] = r
+    for q in range(len(sample)):
+        blk = np.ascontiguousarray(r3[q])
+        if use_ref:
+            lib.t3_single_spin_summation_inplace_(blk.ctypes.data_as(ctypes.c_void_p), nv, b"P3_full",
+                                                  -1.0 / 6.0, 1.0)
+        else:
+            lib.t3_spin_sum(blk, nv, "P3_full", -1.0 / 6.0, 1.0)
+        i, j, k = sample[q]
+        blk /= eia[i][:, None, None] + eia[j][None, :, None] + eia[k][None, None, :]
+        t3[q] += blk
+    float(np.sum(r3 ** 2))
+    dt = time.perf_counter() - t0
+    kind = "reference" if use_ref else "port"
+    return dt, len(trip) / len(sample), kind, len(sample)
+
+
+def reference_arm(args, rank, world):
+    """`--impl reference`: the reference's CPU path on this host's cores."""
+    if rank != 0:
+        return 0
+    times = []
+    nblk = 2
+    for s in range(args.warmup + args.steps):
+        dt, scale, kind, n = cpu_sample(nblk, seed=s)
+        if s >= args.warmup:
+            times.append(dt * scale)
+    v = statistics.mean(times)
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": v * 1e3, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded numpy, BASELINE config 2 distributions)",
+            "config": {"workload": "rccsdt_t3_iteration", "nocc": NOCC, "nvir": NVIR, "n_blocks": 220},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": os.cpu_count(), "kind": kind,
+                             "sample": "%d of 220 blocks per step, scaled by 220/%d; reference C helpers (OpenMP) for "
+                                       "P3/divide, numpy+BLAS einsums" % (n, n)},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# --------------------------------------------------------------------------- GPU side
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="dcc", choices=["dcc", "reference"])
+    ap.add_argument("--precision", default="bf16x3", choices=["bf16x3", "tf32x3"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    import torch
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    if args.impl == "reference":
+        rc = reference_arm(args, rank, world)
+        if dist is not None:
+            dist.destroy_process_group()
+        return rc
+
+    torch.cuda.set_device(local)
+    from dcc import synthetic, t3_residual, contract
+
+    d = synthetic.make_inputs(NOCC, NVIR, seed=0)
+    n3 = d.t3.shape[0]
+    mixed = t3_residual.T3Residual(NOCC, NVIR, args.precision)
+    fp64 = t3_residual.T3Residual(NOCC, NVIR, "fp64")
+    r3 = torch.empty_like(d.t3)
+    t3w = d.t3.clone()
+    norms = torch.empty(2, dtype=torch.float64, device="cuda")
+    ws = torch.empty(1 << 16, dtype=torch.float64, device="cuda")
+
+    # accuracy of the split path against the FP64 path on identical inputs
+    r_ref = fp64.compute(d, d.t3)
+    r_mix = mixed.compute(d, d.t3)
+    torch.cuda.synchronize()
+    rel_err = float((r_mix - r_ref).abs().max() / r_ref.abs().max())
+    del r_ref, r_mix
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def step(res):
+        res.compute(d, t3w, r3)
+        t3_residual.update_t3_(t3w, r3, d, norms=norms, workspace=ws, write_r3=False)
+
+    # live timing of the dominant kernel (the W_vvvv.t3 split GEMM launches)
+    gemm_ev = []
+    orig_gemm = contract.gemm_
+
+    def timed_gemm(A, B, C, epi6, alpha=1.0, beta=1.0, status=None):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        st = orig_gemm(A, B, C, epi6, alpha, beta, status)
+        e1.record()
+        if A.M == mixed.wvvvv.A.M and B.M == mixed.wvvvv.W.M:
+            gemm_ev.append((e0, e1))
+        return st
+
+    def timed_run(res, steps, warmup, track=False):
+        for _ in range(warmup):
+            step(res)
+        barrier()
+        if track:
+            contract.gemm_ = timed_gemm
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(steps):
+            step(res)
+        e1.record()
+        barrier()
+        contract.gemm_ = orig_gemm
+        ms = e0.elapsed_time(e1)
+        if dist is not None:
+            t = torch.tensor([ms], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms
+
+    with ClockSampler(local) as clk:
+        ms_mixed = timed_run(mixed, args.steps, args.warmup, track=True)
+    ok = mixed.status_ok()
+    ms_fp64 = timed_run(fp64, max(2, args.steps // 3), 3)
+
+    gemm_ms = [a.elapsed_time(b) for a, b in gemm_ev]
+    gemm_avg = statistics.mean(gemm_ms) if gemm_ms else None
+    flops_launch = 2.0 * n3 * NVIR ** 5  # one of the three W_vvvv.t3 strings
+    hbm, bf16, bf16_sus, src = peaks()
+    peak_useful = bf16_sus / 3.0  # three bf16 products per FP64-equivalent flop
+    achieved = flops_launch / (gemm_avg * 1e-3) / 1e12 if gemm_avg else None
+
+    # e2e: host (pinned) buffers through the public API, copies inside the timed region
+    host = {k: getattr(d, k).cpu().pin_memory() for k in
+            ("t3", "t2", "W_vvvo", "W_vooo", "W_vvvv", "F_vv", "eia")}
+    h2d = sum(v.numel() * v.element_size() for v in host.values())
+    out_host = torch.empty_like(host["t3"]).pin_memory()
+    norms_host = torch.empty(2, dtype=torch.float64).pin_memory()
+    d2h = out_host.numel() * 8 + 16
+
+    class Dev:
+        pass
+
+    dd = Dev()
+    dd.ijk = d.ijk
+    for k, v in host.items():
+        setattr(dd, k, torch.empty(v.shape, dtype=v.dtype, device="cuda"))
+
+    def e2e_step():
+        for k, v in host.items():
+            getattr(dd, k).copy_(v, non_blocking=True)
+        mixed.compute(dd, dd.t3, r3)
+        t3_residual.update_t3_(dd.t3, r3, dd, norms=norms, workspace=ws, write_r3=False)
+        out_host.copy_(dd.t3, non_blocking=True)
+        norms_host.copy_(norms, non_blocking=True)
+
+    for _ in range(2):
+        e2e_step()
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e2e_steps = max(2, args.steps // 2)
+    e0.record()
+    for _ in range(e2e_steps):
+        e2e_step()
+    e1.record()
+    barrier()
+    e2e_ms = e0.elapsed_time(e1) / e2e_steps
+
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        dt, scale, kind, n = cpu_sample(2)
+        cpu = {"value": dt * scale, "unit": UNIT, "cores": os.cpu_count(), "kind": kind,
+               "sample": "%d of 220 blocks of one step, scaled by 220/%d; reference C helpers (OpenMP) for "
+                         "P3/divide + numpy/BLAS einsums" % (n, n)}
+
+    value = ms_mixed / args.steps / 1e3 / world  # whole-job s per iteration (replicas)
+    launches_per_step = 14 if args.precision else 0
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms_mixed / args.steps, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64 storage; " + args.precision + " products, f32 accumulate",
+        "data": "synthetic (seeded torch generator; BASELINE config 2 distributions)",
+        "config": {"workload": "rccsdt_t3_iteration", "nocc": NOCC, "nvir": NVIR, "n_blocks": n3,
+                   "terms": "W_vvvo.t2, W_vooo.t2, F_vv.t3, W_vvvv.t3, P3_full, divide, update, norms",
+                   "precision": args.precision, "l2": "inputs larger than L2 (t3 1.28 GB, W_vvvv 0.52 GB)",
+                   "parallelism": "replicas" if world > 1 else "single"},
+        "fp64_path_s_per_iter": ms_fp64 / max(2, args.steps // 3) / 1e3,
+        "speedup_vs_fp64": (ms_fp64 / max(2, args.steps // 3)) / (ms_mixed / args.steps),
+        "r3_max_rel_err_vs_fp64": rel_err, "device_status_ok": ok,
+        "roofline": {"kernel": "dcc::k_gemm_split3<0> (W_vvvv.t3 string)", "bound": "tensor",
+                     "achieved": achieved, "peak": peak_useful, "unit": "TFLOP/s",
+                     "frac": (achieved / peak_useful) if achieved else None,
+                     "peak_note": "bf16 dense %s sustained %.1f TF/s / 3 products (of %s)" % (src, bf16_sus, src),
+                     "flops_per_launch": flops_launch, "launch_ms": gemm_avg,
+                     "traffic": profile_traffic("gemm_split3_wvvvv_c2")},
+        "cpu_baseline": cpu,
+        "e2e": {"value": e2e_ms / 1e3, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "gpu_launches": launches_per_step * args.steps,
+        "clocks": clk.summary(),
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -707,3 +707,68 @@ extern "C" int dcc_fill_t3_from_abc(double *target, int64_t a0, int64_t a1, int6
                                                           (int)nocc, t3_abc, ld_b);
     return launch_status("fill_t3_from_abc");
 }
+
+// ---------------------------------------------------------------- S3 gather
+
+namespace dcc {
+
+struct S3Src {
+    const double *base;
+    double scale;
+    int64_t st[6];  // strides of (x, y, z, a, b, c)
+};
+
+// r3[q][a][b][c] = beta * r3 + sum_s scale_s * sum_sigma U_s(sigma(i,j,k), sigma(a,b,c))
+// for the canonical triple (i,j,k) = ijk[q]; sigma runs over the six
+// simultaneous permutations of the occupied and virtual index triples.
+// One warp per output row (q, a, b); lanes stride over c.
+__global__ void k_s3_gather(double *r3, const int32_t *ijk, int64_t nblocks, int nv, double beta, S3Src s0, S3Src s1,
+                            int nsrc) {
+    const int lane = threadIdx.x & 31;
+    const int64_t nrow = nblocks * nv * nv;
+    for (int64_t row = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; row < nrow;
+         row += ((int64_t)gridDim.x * blockDim.x) >> 5) {
+        int64_t q = row / (nv * nv);
+        int ab = (int)(row - q * nv * nv), a = ab / nv, b = ab - a * nv;
+        const int o[3] = {ijk[3 * q], ijk[3 * q + 1], ijk[3 * q + 2]};
+        double *out = r3 + row * nv;
+        for (int c = lane; c < nv; c += 32) {
+            const int v[3] = {a, b, c};
+            double acc = 0.0;
+            for (int s = 0; s < nsrc; s++) {
+                const S3Src &S = s ? s1 : s0;
+                double part = 0.0;
+#pragma unroll
+                for (int p = 0; p < 6; p++) {
+                    const int m0 = perm3(p, 0), m1 = perm3(p, 1), m2 = perm3(p, 2);
+                    part += S.base[o[m0] * S.st[0] + o[m1] * S.st[1] + o[m2] * S.st[2] + v[m0] * S.st[3] +
+                                   v[m1] * S.st[4] + v[m2] * S.st[5]];
+                }
+                acc = fma(S.scale, part, acc);
+            }
+            out[c] = (beta == 0.0) ? acc : fma(beta, out[c], acc);
+        }
+    }
+}
+
+}  // namespace dcc
+
+extern "C" int dcc_t3_s3_gather(double *r3, const int32_t *ijk, int64_t nblocks, int64_t nvir, double beta,
+                                const double *u0, double scale0, const int64_t *strides0, const double *u1,
+                                double scale1, const int64_t *strides1, void *stream) {
+    clear_error();
+    DCC_REQUIRE(nblocks >= 0 && nvir >= 0, DCC_ERR_SHAPE, "negative size");
+    if (nblocks == 0 || nvir == 0) return DCC_OK;
+    DCC_REQUIRE(r3 && ijk && u0 && strides0, DCC_ERR_NULL, "NULL buffer");
+    S3Src s0{u0, scale0, {strides0[0], strides0[1], strides0[2], strides0[3], strides0[4], strides0[5]}};
+    S3Src s1 = s0;
+    int nsrc = 1;
+    if (u1) {
+        DCC_REQUIRE(strides1, DCC_ERR_NULL, "strides1 is NULL");
+        s1 = S3Src{u1, scale1, {strides1[0], strides1[1], strides1[2], strides1[3], strides1[4], strides1[5]}};
+        nsrc = 2;
+    }
+    k_s3_gather<<<row_grid(nblocks * nvir * nvir, 256), 256, 0, as_stream(stream)>>>(r3, ijk, nblocks, (int)nvir,
+                                                                                     beta, s0, s1, nsrc);
+    return launch_status("t3_s3_gather");
+}

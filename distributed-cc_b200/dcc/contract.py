@@ -26,7 +26,7 @@ _split = L.bind("dcc_split_operand", [L.c_vp, L.c_vp, L.c_vp, L.c_i64, L.c_i64, 
 _gemm = L.bind("dcc_gemm_split3", [L.c_vp] * 4 + [L.c_i64] * 3 + [L.c_vp, L.c_vp, L.c_dbl, L.c_dbl, L.c_int,
                                                                    L.c_vp, L.c_vp])
 
-BIG = 1 << 40  # divisor that makes a level of the two-level map a plain stride
+BIG = 1 << 30  # divisor that makes a level of the two-level map a plain stride (< 2^31)
 
 
 def _i64x6(v):

@@ -1,0 +1,91 @@
+"""Small, self-contained launches of single kernels for profiler captures.
+
+    python -m dcc.profile_cases gemm   [--kind bf16x3] [--reps 3]
+    python -m dcc.profile_cases p3     [--reps 3]
+    python -m dcc.profile_cases update [--reps 3]
+    python -m dcc.profile_cases q      [--reps 3]
+
+Each case builds its inputs once and launches the kernel `reps` times, so a
+profiler can skip the warm-up launches and capture the last one.  Sizes are
+the nocc=10 / nvir=90 workload (inputs larger than L2, a few GB on the device).
+"""
+from __future__ import annotations
+
+import argparse
+import os
+import sys
+
+sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+
+import torch  # noqa: E402
+
+
+def case_gemm(kind, reps):
+    from dcc import contract
+    n3, nv = 220, 90
+    g = torch.Generator(device="cuda").manual_seed(0)
+    t3 = torch.randn(n3, nv, nv, nv, dtype=torch.float64, device="cuda", generator=g) * 1e-3
+    W = torch.randn(nv, nv, nv, nv, dtype=torch.float64, device="cuda", generator=g) * 0.1
+    r3 = torch.zeros_like(t3)
+    op = contract.WvvvvT3(n3, nv, kind)
+    op.W.fill(W.reshape(nv * nv, nv * nv), (contract.BIG, 0, nv * nv, contract.BIG, 0, 1))
+    amap, emap = op.maps[2]
+    op.A.fill(t3, amap)
+    for _ in range(reps):
+        contract.gemm_(op.A, op.W, r3, emap, 1.0, 1.0, op.status)
+    torch.cuda.synchronize()
+    assert int(op.status.item()) == 0
+
+
+def case_p3(reps):
+    from dcc import _c_rccsdt
+    t3 = torch.randn(220, 90, 90, 90, dtype=torch.float64, device="cuda")
+    for _ in range(reps):
+        _c_rccsdt.t3_spin_summation_inplace_(t3, 220, 90, "P3_full", -1.0 / 6.0, 1.0)
+    torch.cuda.synchronize()
+
+
+def case_update(reps):
+    from dcc import synthetic, t3_residual
+    d = synthetic.make_inputs(10, 90, seed=0)
+    r3 = torch.randn_like(d.t3) * 1e-4
+    for _ in range(reps):
+        t3_residual.update_t3_(d.t3, r3, d, write_r3=False)
+    torch.cuda.synchronize()
+
+
+def case_q(reps):
+    from dcc import _c_rccsdt_q
+    no, nv, blk = 10, 90, 4
+    g = torch.Generator(device="cuda").manual_seed(0)
+    t4 = torch.randn((blk,) * 4 + (no,) * 4, dtype=torch.float64, device="cuda", generator=g) * 1e-3
+    z4 = torch.randn_like(t4)
+    vvoo = torch.randn(nv, nv, no, no, dtype=torch.float64, device="cuda", generator=g) * 0.1
+    t2 = torch.randn(nv, nv, no, no, dtype=torch.float64, device="cuda", generator=g) * 0.01
+    eo = torch.linspace(-1.5, -0.3, no, dtype=torch.float64, device="cuda")
+    ev = torch.linspace(0.1, 3.0, nv, dtype=torch.float64, device="cuda")
+    out = torch.zeros(2, dtype=torch.float64, device="cuda")
+    for _ in range(reps):
+        _c_rccsdt_q.q_task_epilogue(t4, z4, vvoo, t2, eo, ev, (0, 4, 4, 8, 8, 12, 12, 16), blk, no, nv, out)
+    torch.cuda.synchronize()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("case", choices=["gemm", "p3", "update", "q"])
+    ap.add_argument("--kind", default="bf16x3")
+    ap.add_argument("--reps", type=int, default=3)
+    a = ap.parse_args()
+    if a.case == "gemm":
+        case_gemm(a.kind, a.reps)
+    elif a.case == "p3":
+        case_p3(a.reps)
+    elif a.case == "update":
+        case_update(a.reps)
+    else:
+        case_q(a.reps)
+    print("ok")
+
+
+if __name__ == "__main__":
+    main()

@@ -125,6 +125,17 @@ DCC_API int dcc_redistribute_ijk_to_abc(const double *t3_ijk, double *t3_abc, in
 DCC_API int dcc_fill_t3_from_abc(double *target, int64_t a0, int64_t a1, int64_t b0, int64_t b1, int64_t nvir,
                          int64_t nocc, const double *t3_abc, int64_t ld_b, void *stream);
 
+/* r3[q][a][b][c] = beta*r3 + sum_s scale_s * sum_sigma U_s(sigma(i,j,k), sigma(a,b,c))
+ * over the six simultaneous permutations sigma of (i,j,k) and (a,b,c), for the
+ * canonical triples ijk[q] (DEVICE int32 [nblocks][3]).  U_s is addressed by
+ * HOST strides {x,y,z,a,b,c} (in doubles); the second source is optional
+ * (u1 == NULL).  Replaces the twelve per-block einsums W_vvvo.t2 / W_vooo.t2
+ * of compute_r3_tri (distr_cc/rccsdt.py:385-396): each group of six is the
+ * S3 symmetrization of one contraction over all ordered (i,j,k). */
+DCC_API int dcc_t3_s3_gather(double *r3, const int32_t *ijk, int64_t nblocks, int64_t nvir, double beta,
+                             const double *u0, double scale0, const int64_t *strides0, const double *u1,
+                             double scale1, const int64_t *strides1, void *stream);
+
 /* ----------------------------------------------------------------------
  * T4 helpers (replace src/rccsdtq.c and PySCF libccsdt.t4_add_)
  * ---------------------------------------------------------------------- */

@@ -85,3 +85,37 @@ def test_python_mirrors_validate_like_reference():
         _c_rccsdt.t3_single_spin_summation_inplace_(torch.zeros(4, 2, dtype=torch.float64).t(), 2, "P3_full")
     with pytest.raises(ValueError):  # host tensor: this library computes on the GPU only
         _c_rccsdt.t3_single_spin_summation_inplace_(torch.zeros(8, dtype=torch.float64), 2, "P3_full")
+
+
+def test_split_gemm_host_validation_accepts_our_maps(L):
+    """The maps the drivers pass must clear the host-side checks: on a box
+    without a GPU a valid call gets as far as the launch (DCC_ERR_CUDA), an
+    invalid one stops at DCC_ERR_SHAPE."""
+    import torch
+    from dcc import contract
+    if torch.cuda.is_available():
+        pytest.skip("checks the no-device fall-through")
+    fake = ctypes.c_void_p(4096)
+    nv, n = 90, 220
+    for amap, emap in contract.wvvvv_maps(nv):
+        rc = contract._split(fake, fake, fake, n * nv, nv * nv, contract.padded_k(nv * nv, 0),
+                             contract._i64x6(amap), 0, None)
+        assert rc == 4, L.last_error()
+        rc = contract._gemm(fake, fake, fake, fake, n * nv, nv * nv, contract.padded_k(nv * nv, 0), fake,
+                            contract._i64x6(emap), 1.0, 1.0, 0, fake, None)
+        assert rc == 4, L.last_error()
+    rc = contract._gemm(fake, fake, fake, fake, 10, 10, 100, fake, contract._i64x6((1, 0, 1, 1, 0, 1)), 1.0, 0.0, 0,
+                        fake, None)
+    assert rc == 2  # Kp not a multiple of 64
+
+
+def test_residual_split_maps_clear_host_checks(L):
+    import torch
+    from dcc import contract
+    if torch.cuda.is_available():
+        pytest.skip("checks the no-device fall-through")
+    fake = ctypes.c_void_p(4096)
+    no, nv, B = 10, 90, contract.BIG
+    for M, K, m6 in [(no * nv * nv, nv, (nv * nv, 1, nv * no, B, 0, no)), (no * no * nv, nv, (nv, nv * nv, 1, B, 0, nv))]:
+        rc = contract._split(fake, fake, fake, M, K, contract.padded_k(K, 0), contract._i64x6(m6), 0, None)
+        assert rc == 4, L.last_error()

@@ -1,0 +1,56 @@
+"""Batched T3 residual (W.t2 via full-X GEMM + S3 gather, F_vv.t3, W_vvvv.t3)
+and the fused update, against the literal per-block numpy restatement of
+compute_r3_tri.  FP64 path: rtol 1e-11.  Split paths: relative to the largest
+|r3|, 1e-4 (bf16x3) and 1e-5 (tf32x3 -- its accumulation limits it to that)."""
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+TOL = {"bf16x3": 1e-4, "tf32x3": 1e-4}
+
+
+@pytest.fixture(scope="module")
+def mods():
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from dcc import synthetic, t3_residual
+    from oracle import einsum_ref
+    return synthetic, t3_residual, einsum_ref
+
+
+def _ref_r3(er, dn):
+    imds = er.Imds(dn.F_vv, dn.F_oo, dn.W_vvvo, dn.W_vooo, dn.W_vvvv, dn.W_ovov, dn.W_ovvo, dn.W_oooo)
+    r3 = er.vt2_ref(imds, dn.t2, dn.t3, dn.nocc)
+    return er.wvvvv_ref(imds, dn.t3, r3)
+
+
+@pytest.mark.parametrize("nocc,nvir", [(2, 5), (3, 7), (4, 10)])
+@pytest.mark.parametrize("precision", ["fp64", "bf16x3", "tf32x3"])
+def test_residual(mods, nocc, nvir, precision):
+    syn, tr, er = mods
+    d = syn.make_inputs(nocc, nvir, seed=nocc * 100 + nvir)
+    dn = syn.to_numpy(d)
+    want = _ref_r3(er, dn)
+    res = tr.T3Residual(nocc, nvir, precision)
+    got = res.compute(d, d.t3).cpu().numpy()
+    assert res.status_ok()
+    if precision == "fp64":
+        np.testing.assert_allclose(got, want, rtol=1e-11, atol=1e-13 * np.abs(want).max())
+    else:
+        assert np.abs(got - want).max() / np.abs(want).max() < TOL[precision]
+
+
+@pytest.mark.parametrize("nocc,nvir,nact", [(3, 7, 5), (4, 9, 9)])
+def test_update(mods, nocc, nvir, nact):
+    syn, tr, er = mods
+    d = syn.make_inputs(nocc, nvir, seed=7)
+    dn = syn.to_numpy(d)
+    r3 = torch.randn_like(d.t3) * 1e-4
+    want_t3, want_r3, want_n = er.r3_update_ref(dn.t3, r3.cpu().numpy(), dn.eia, nocc, nact)
+    t3 = d.t3.clone()
+    norms = tr.update_t3_(t3, r3, d, nvir_active=nact)
+    assert np.array_equal(r3.cpu().numpy(), want_r3)
+    assert np.array_equal(t3.cpu().numpy(), want_t3)
+    np.testing.assert_allclose(norms.cpu().numpy(), want_n, rtol=1e-12)
