@@ -772,3 +772,84 @@ extern "C" int dcc_t3_s3_gather(double *r3, const int32_t *ijk, int64_t nblocks,
                                                                                      beta, s0, s1, nsrc);
     return launch_status("t3_s3_gather");
 }
+
+// ---------------------------------------------------------------- no-allocation update
+
+#include <mutex>
+
+namespace dcc {
+
+// Rows (q, a, b) per CTA of the no-allocation update, and the most CTAs the
+// static scratch can serve: 8192 pairs of partial sums = 128 KiB, which
+// covers nblocks * nvir^2 <= 8 388 608 rows (e.g. 680 blocks of nvir = 93).
+constexpr int64_t NOALLOC_ROWS_PER_CTA = 1024;
+constexpr int64_t NOALLOC_MAX_CTAS = 8192;
+
+// Partial squared norms of dcc_t3_divide_update_noalloc, two doubles per CTA.
+// Every GPU that loads the library holds this array until the process exits;
+// all calls on a device share it.
+static __device__ __align__(256) double g_update_scratch[2 * NOALLOC_MAX_CTAS];
+
+// Device address of g_update_scratch for the current device, looked up once per
+// device.  In host code the symbol names a host-side stand-in, so kernels must
+// be given this address instead.
+static int update_scratch_address(double **out) {
+    static std::mutex mu;
+    static double *addr[128] = {nullptr};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) {
+        set_error("cudaGetDevice: %s", cudaGetErrorString(e));
+        return DCC_ERR_CUDA;
+    }
+    if (dev < 0 || dev >= 128) {
+        set_error("device ordinal %d out of range", dev);
+        return DCC_ERR_UNSUPPORTED;
+    }
+    std::lock_guard<std::mutex> lock(mu);
+    if (!addr[dev]) {
+        void *p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_update_scratch);
+        if (e != cudaSuccess || !p) {
+            set_error("cudaGetSymbolAddress(update scratch): %s", cudaGetErrorString(e));
+            return DCC_ERR_CUDA;
+        }
+        addr[dev] = (double *)p;
+    }
+    *out = addr[dev];
+    return DCC_OK;
+}
+
+}  // namespace dcc
+
+extern "C" int dcc_t3_divide_update_noalloc(double *t3, double *r3, const double *eia, const int32_t *ijk,
+                                            int64_t nblocks, int64_t nvir, int64_t nvir_active, int write_r3,
+                                            double *norms, void *stream) {
+    clear_error();
+    DCC_REQUIRE(nblocks >= 0 && nvir >= 0, DCC_ERR_SHAPE, "negative size");
+    DCC_REQUIRE(norms, DCC_ERR_NULL, "norms is NULL");
+    cudaStream_t st = as_stream(stream);
+    if (nblocks == 0 || nvir == 0) {
+        if (cudaMemsetAsync(norms, 0, 2 * sizeof(double), st) != cudaSuccess) return launch_status("memset");
+        return DCC_OK;
+    }
+    DCC_REQUIRE(t3 && r3 && eia && ijk, DCC_ERR_NULL, "NULL buffer");
+    const int64_t rows = nblocks * nvir * nvir;
+    const int64_t ctas = (rows + NOALLOC_ROWS_PER_CTA - 1) / NOALLOC_ROWS_PER_CTA;
+    DCC_REQUIRE(ctas <= NOALLOC_MAX_CTAS, DCC_ERR_SHAPE,
+                "nblocks*nvir^2 = %lld rows exceeds the no-allocation limit of %lld rows (static scratch of %lld "
+                "partial sums); use dcc_t3_divide_update with a workspace",
+                (long long)rows, (long long)(NOALLOC_MAX_CTAS * NOALLOC_ROWS_PER_CTA), (long long)NOALLOC_MAX_CTAS);
+    double *scratch = nullptr;
+    int rc = update_scratch_address(&scratch);
+    if (rc) return rc;
+    if (nvir_active < 0 || nvir_active > nvir) nvir_active = nvir;
+    // every CTA overwrites its own pair before k_sum_pairs reads exactly `ctas` pairs,
+    // so nothing left by an earlier call needs clearing
+    k_t3_divide_update<<<(unsigned)ctas, UPD_THREADS, 0, st>>>(t3, r3, eia, ijk, nblocks, (int)nvir, (int)nvir_active,
+                                                               write_r3, scratch);
+    rc = launch_status("t3_divide_update_noalloc");
+    if (rc) return rc;
+    k_sum_pairs<<<1, 256, 0, st>>>(scratch, ctas, norms);
+    return launch_status("t3_divide_update_noalloc reduce");
+}

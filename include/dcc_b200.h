@@ -111,6 +111,24 @@ DCC_API int dcc_t3_divide_update(double *t3, double *r3, const double *eia, cons
                          int64_t nvir, int64_t nvir_active, int write_r3, double *norms, void *workspace,
                          size_t workspace_bytes, void *stream);
 
+/* The same fused update for callers that cannot allocate device memory: a
+ * host runtime that owns every device allocation through its own pool and
+ * forbids libraries to call cudaMalloc, or a thin ctypes caller (like the
+ * reference's wrappers) that holds only the amplitude tensors and has no
+ * allocator to obtain a workspace from.  No counterpart in the reference
+ * (its C helpers run on the host and malloc their scratch).
+ * The per-CTA partial sums live in a static 128 KiB device array inside the
+ * library (every GPU that loads the library holds it until exit), so this
+ * call allocates nothing; it serves nblocks * nvir^2 <= 8 388 608 rows and
+ * returns DCC_ERR_SHAPE with a message beyond that.  The first call on a
+ * device looks up the array's device address (cudaGetSymbolAddress); make
+ * that first call before any stream capture.  All calls on a device share
+ * the array, so calls that overlap on the GPU (different streams, no
+ * ordering between them) race on it. */
+DCC_API int dcc_t3_divide_update_noalloc(double *t3, double *r3, const double *eia, const int32_t *ijk,
+                                         int64_t nblocks, int64_t nvir, int64_t nvir_active, int write_r3,
+                                         double *norms, void *stream);
+
 /* IJK -> ABC layout transform at one rank: t3_abc[g][x][y][z] (g the rank of
  * a<=b<=c) from t3_ijk[q][a][b][c] (q the rank of i<=j<=k).  Reproduces the
  * record pack + Alltoallv + unpack of distr_cc/distribute_t3.py:1544-1642 with
