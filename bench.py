@@ -2,7 +2,8 @@
 (nocc=10, nvir=90, 220 canonical i<=j<=k blocks of 90^3, FP64 storage).
 
 A step is one pass of the triples hot path over the 220 blocks:
-  r3 = W_vvvo.t2 - W_vooo.t2 + F_vv.t3 + W_vvvv.t3      (compute_r3_tri terms)
+  r3 = compute_r3_tri: W_vvvo.t2 - W_vooo.t2 + F_vv.t3 + OO batch terms
+       (W_ovov / W_ovvo / F_oo / W_oooo . t3) + W_vvvv.t3
   r3 <- P3_full(r3, -1/6, 1); r3 /= D; t3 += r3; |r3|^2 (update)
 with the large contractions as split-BF16x3 tcgen05 GEMMs (FP32 accumulate,
 FP64 storage, denominators, update and norms).  The same step on the plain
@@ -120,6 +121,10 @@ def cpu_sample(nblk_sample=2, seed=0):
     trip = [(i, j, k) for i in range(no) for j in range(i, no) for k in range(j, no)]
     sample = trip[::len(trip) // nblk_sample][:nblk_sample]
     W_vvvv = rng.standard_normal((nv,) * 4) * 0.1
+    W_ovov = rng.standard_normal((no, nv, no, nv)) * 0.1
+    W_ovvo = rng.standard_normal((no, nv, nv, no)) * 0.1
+    t3_src = rng.standard_normal((3, nv, nv, nv)) * 1e-3  # stand-ins for the batch blocks each l reads
+    t3_batch = rng.standard_normal((len(trip) // 10, nv * nv * nv)) * 1e-3
     W_vvvo = rng.standard_normal((nv, nv, nv, no)) * 0.1
     W_vooo = rng.standard_normal((nv, no, no, no)) * 0.1
     F_vv = np.diag(rng.uniform(0.1, 3.0, nv))
@@ -147,10 +152,32 @@ def cpu_sample(nblk_sample=2, seed=0):
         r += e('ad,dbc->abc', F_vv, t3[q])
         r += e('bd,adc->abc', F_vv, t3[q])
         r += e('cd,abd->abc', F_vv, t3[q])
+        # OO batch terms: per target block, for every l the four W_ovov/W_ovvo einsums of
+        # each of the three parts (distr_cc/rccsdt.py:538-596), plus the transpose-add /
+        # triple-sym of the batch blocks (reference C helpers) and the prefactor GEMMs
+        for l in range(no):
+            T, T2_, V0 = t3_src[0], t3_src[1], t3_src[2]
+            for occ in (i, j, k):
+                r -= e('bd,dca->abc', W_ovov[l, :, occ, :], T)
+                r -= 0.5 * e('ad,dcb->abc', W_ovov[l, :, occ, :], T2_)
+                r -= e('cd,bda->abc', W_ovov[l, :, occ, :], T)
+                r += 0.5 * e('ad,bcd->abc', W_ovvo[l, :, :, occ], V0)
+        pf = rng.standard_normal((6, t3_batch.shape[0]))
+        for m in range(6):  # 'pq,pabc->qabc' column of one target block, on a tenth of the batch
+            r += (10.0 * (pf[m] @ t3_batch)).reshape(nv, nv, nv)
         r += e('abde,dec->abc', W_vvvv, t3[q])
         r += e('acde,dbe->abc', W_vvvv, t3[q])
         r += e('bcde,ade->abc', W_vvvv, t3[q])
         r3[q] = r
+    # per-step helper work on the batch blocks, scaled to this sample's share of blocks
+    for q in range(len(sample)):
+        blk = np.ascontiguousarray(t3[q])
+        if use_ref:
+            b0, b1, b2, b3 = (np.empty_like(blk) for _ in range(4))
+            lib.t3_transpose_add_(blk.ctypes.data_as(ctypes.c_void_p), b0.ctypes.data_as(ctypes.c_void_p), nv)
+            lib.t3_spin_summation_triple_sym_(blk.ctypes.data_as(ctypes.c_void_p), b1.ctypes.data_as(ctypes.c_void_p),
+                                              b2.ctypes.data_as(ctypes.c_void_p), b3.ctypes.data_as(ctypes.c_void_p),
+                                              nv)
     for q in range(len(sample)):
         blk = np.ascontiguousarray(r3[q])
         if use_ref:
@@ -225,8 +252,8 @@ def main():
 
     d = synthetic.make_inputs(NOCC, NVIR, seed=0)
     n3 = d.t3.shape[0]
-    mixed = t3_residual.T3Residual(NOCC, NVIR, args.precision)
-    fp64 = t3_residual.T3Residual(NOCC, NVIR, "fp64")
+    mixed = t3_residual.T3Residual(NOCC, NVIR, args.precision, with_oo=True)
+    fp64 = t3_residual.T3Residual(NOCC, NVIR, "fp64", with_oo=True)
     r3 = torch.empty_like(d.t3)
     t3w = d.t3.clone()
     norms = torch.empty(2, dtype=torch.float64, device="cuda")
@@ -252,10 +279,10 @@ def main():
     gemm_ev = []
     orig_gemm = contract.gemm_
 
-    def timed_gemm(A, B, C, epi6, alpha=1.0, beta=1.0, status=None):
+    def timed_gemm(A, B, C, frow, fcol, alpha=1.0, beta=1.0, status=None):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
-        st = orig_gemm(A, B, C, epi6, alpha, beta, status)
+        st = orig_gemm(A, B, C, frow, fcol, alpha, beta, status)
         e1.record()
         if A.M == mixed.wvvvv.A.M and B.M == mixed.wvvvv.W.M:
             gemm_ev.append((e0, e1))
@@ -295,7 +322,7 @@ def main():
 
     # e2e: host (pinned) buffers through the public API, copies inside the timed region
     host = {k: getattr(d, k).cpu().pin_memory() for k in
-            ("t3", "t2", "W_vvvo", "W_vooo", "W_vvvv", "F_vv", "eia")}
+            ("t3", "t2", "W_vvvo", "W_vooo", "W_vvvv", "W_ovov", "W_ovvo", "W_oooo", "F_vv", "F_oo", "eia")}
     h2d = sum(v.numel() * v.element_size() for v in host.values())
     out_host = torch.empty_like(host["t3"]).pin_memory()
     norms_host = torch.empty(2, dtype=torch.float64).pin_memory()
@@ -334,17 +361,20 @@ def main():
         dt, scale, kind, n = cpu_sample(2)
         cpu = {"value": dt * scale, "unit": UNIT, "cores": os.cpu_count(), "kind": kind,
                "sample": "%d of 220 blocks of one step, scaled by 220/%d; reference C helpers (OpenMP) for "
-                         "P3/divide + numpy/BLAS einsums" % (n, n)}
+                         "P3/divide/transpose-add/triple-sym + numpy/BLAS einsums" % (n, n)}
 
     value = ms_mixed / args.steps / 1e3 / world  # whole-job s per iteration (replicas)
-    launches_per_step = 14 if args.precision else 0
+    # own kernels per mixed step: 6 (W.t2) + 13 (OO: unpack, 7 splits, 5 GEMMs) + 1 gather
+    # + 7 (W_vvvv: 4 splits, 3 GEMMs) + 3 (P3, update, reduce)
+    launches_per_step = 30
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms_mixed / args.steps, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64 storage; " + args.precision + " products, f32 accumulate",
         "data": "synthetic (seeded torch generator; BASELINE config 2 distributions)",
         "config": {"workload": "rccsdt_t3_iteration", "nocc": NOCC, "nvir": NVIR, "n_blocks": n3,
-                   "terms": "W_vvvo.t2, W_vooo.t2, F_vv.t3, W_vvvv.t3, P3_full, divide, update, norms",
+                   "terms": "compute_r3_tri (W_vvvo.t2, W_vooo.t2, F_vv.t3, OO W_ovov/W_ovvo/F_oo/W_oooo.t3, "
+                            "W_vvvv.t3), P3_full, divide, update, norms",
                    "precision": args.precision, "l2": "inputs larger than L2 (t3 1.28 GB, W_vvvv 0.52 GB)",
                    "parallelism": "replicas" if world > 1 else "single"},
         "fp64_path_s_per_iter": ms_fp64 / max(2, args.steps // 3) / 1e3,

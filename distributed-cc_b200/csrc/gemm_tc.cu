@@ -8,10 +8,9 @@
 // product is accumulated in FP32 in tensor memory as
 //   A_hi B_hi + A_hi B_lo + A_lo B_hi
 // (the dropped A_lo B_lo term is below the pieces' own rounding), and the
-// epilogue adds alpha * acc into an FP64 C with beta scaling.  The output
-// address is two-level strided,
-//   row_off(m) = (m / rdiv) * rs1 + (m % rdiv) * rs2,
-//   col_off(n) = (n / cdiv) * cs1 + (n % cdiv) * cs2,
+// epilogue adds alpha * acc into an FP64 C with beta scaling.  Row and column
+// offsets are three-digit mixed-radix maps,
+//   off(m) = (m / (R1*R2)) * S0 + ((m / R2) % R1) * S1 + (m % R2) * S2,
 // so permuted contraction outputs (e.g. r3[a,b,c] += X[(q,c),(a,b)]) are
 // accumulated in place without a transposed temporary.
 //
@@ -31,13 +30,28 @@ namespace dcc {
 
 constexpr int GM = 128;       // tile rows (UMMA M)
 constexpr int GN = 256;       // tile cols (UMMA N)
-constexpr int GK_BYTES = 128; // one k-block row: 128 bytes (SWIZZLE_128B)
-constexpr int GSTAGES = 2;
 constexpr int G_THREADS = 192;
+
+// Tunable pipeline shape: bytes of K per operand row and k-block (128, 64 or
+// 32 -> 128/64/32-byte swizzle), ring depth, and the number of M-tiles per
+// raster group (CTAs that run together share B tiles in L2).
+struct GemmConfig {
+    int kb_bytes, stages, group_m;
+};
+static GemmConfig g_cfg = {64, 4, 16};
 constexpr uint64_t WAIT_NS = 2000000000ull;  // 2 s bound on any single wait
 
+// off(m) = (m / (R1*R2)) * S0 + ((m / R2) % R1) * S1 + (m % R2) * S2
+struct Map3 {
+    int64_t R1, R2, S0, S1, S2;
+};
+
+__host__ __device__ __forceinline__ int64_t map3(const Map3 &f, int64_t m) {
+    return (m / (f.R1 * f.R2)) * f.S0 + ((m / f.R2) % f.R1) * f.S1 + (m % f.R2) * f.S2;
+}
+
 struct GemmEpi {
-    int64_t rdiv, rs1, rs2, cdiv, cs1, cs2;
+    Map3 row, col;
 };
 
 // ----------------------------------------------------------------- PTX helpers
@@ -104,14 +118,17 @@ __device__ __forceinline__ void tma_prefetch_desc(const CUtensorMap *map) {
     asm volatile("prefetch.tensormap [%0];" ::"l"(map) : "memory");
 }
 
-// K-major, 128-byte-swizzled operand tile: rows of 128 bytes, 8-row groups
-// 1024 bytes apart (stride byte offset), Blackwell descriptor version 1.
-__device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
+// K-major, swizzled operand tile with rows of KB bytes (KB = 128/64/32 ->
+// SWIZZLE_128B/64B/32B): 8-row groups 8*KB bytes apart (stride byte offset),
+// Blackwell descriptor version 1.
+template <int KB>
+__device__ __forceinline__ uint64_t swz_desc(uint32_t saddr) {
+    constexpr uint64_t layout = KB == 128 ? 2 : (KB == 64 ? 4 : 6);
     uint64_t d = (uint64_t)((saddr >> 4) & 0x3FFF);
-    d |= (uint64_t)1 << 16;            // leading byte offset (unused for swizzled K-major): 16 B
-    d |= (uint64_t)(1024 >> 4) << 32;  // stride byte offset: 1024 B
-    d |= (uint64_t)1 << 46;            // descriptor version
-    d |= (uint64_t)2 << 61;            // SWIZZLE_128B
+    d |= (uint64_t)1 << 16;                 // leading byte offset (unused for swizzled K-major): 16 B
+    d |= (uint64_t)((8 * KB) >> 4) << 32;   // stride byte offset: one 8-row group
+    d |= (uint64_t)1 << 46;                 // descriptor version
+    d |= layout << 61;
     return d;
 }
 
@@ -154,32 +171,44 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
 
 // ----------------------------------------------------------------- kernel
 
+template <int ST>
 struct GemmSmem {
-    uint64_t full[GSTAGES];
-    uint64_t empty[GSTAGES];
+    uint64_t full[ST];
+    uint64_t empty[ST];
     uint64_t acc_full;
     uint32_t tmem_base;
     int64_t col_off[GN];
 };
 
-// KIND 0: bf16 pieces (64 elements per k-block); KIND 1: tf32 pieces (32).
-template <int KIND>
+// KIND 0: bf16 pieces; KIND 1: tf32 pieces.  KB: bytes of K per row and
+// k-block; ST: ring depth.  blockIdx.x is a linear tile id, rasterized in
+// groups of group_m M-tiles.
+template <int KIND, int KB, int ST>
 __global__ void __launch_bounds__(G_THREADS, 1)
     k_gemm_split3(const __grid_constant__ CUtensorMap tmAh, const __grid_constant__ CUtensorMap tmAl,
                   const __grid_constant__ CUtensorMap tmBh, const __grid_constant__ CUtensorMap tmBl, int M, int N,
-                  int nkb, double *C, GemmEpi epi, double alpha, double beta, int *status) {
+                  int nkb, double *C, GemmEpi epi, double alpha, double beta, int *status, int group_m) {
     extern __shared__ __align__(1024) uint8_t g_smem[];
     // operand stages first (1024-byte aligned), then the control block
     uint8_t *base = (uint8_t *)(((uintptr_t)g_smem + 1023) & ~(uintptr_t)1023);
-    constexpr uint32_t A_BYTES = GM * GK_BYTES, B_BYTES = GN * GK_BYTES;
+    constexpr uint32_t A_BYTES = GM * KB, B_BYTES = GN * KB;
     constexpr uint32_t STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;
-    GemmSmem *cs = (GemmSmem *)(base + GSTAGES * STAGE_BYTES);
+    GemmSmem<ST> *cs = (GemmSmem<ST> *)(base + ST * STAGE_BYTES);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int n0 = blockIdx.x * GN, m0 = blockIdx.y * GM;
+    int tile_m, tile_n;
+    {
+        const int num_m = (M + GM - 1) / GM, num_n = (N + GN - 1) / GN;
+        const int pid = blockIdx.x, per_group = group_m * num_n;
+        const int first_m = (pid / per_group) * group_m;
+        const int gsz = (num_m - first_m) < group_m ? (num_m - first_m) : group_m;
+        tile_m = first_m + (pid % per_group) % gsz;
+        tile_n = (pid % per_group) / gsz;
+    }
+    const int n0 = tile_n * GN, m0 = tile_m * GM;
 
     if (threadIdx.x == 0) {
-        for (int s = 0; s < GSTAGES; s++) {
+        for (int s = 0; s < ST; s++) {
             mbar_init(smem_u32(&cs->full[s]), 1);
             mbar_init(smem_u32(&cs->empty[s]), 1);
         }
@@ -190,10 +219,7 @@ __global__ void __launch_bounds__(G_THREADS, 1)
         tma_prefetch_desc(&tmBh);
         tma_prefetch_desc(&tmBl);
     }
-    for (int j = threadIdx.x; j < GN; j += G_THREADS) {
-        int64_t n = n0 + j;
-        cs->col_off[j] = (n / epi.cdiv) * epi.cs1 + (n % epi.cdiv) * epi.cs2;
-    }
+    for (int j = threadIdx.x; j < GN; j += G_THREADS) cs->col_off[j] = map3(epi.col, (int64_t)n0 + j);
     if (warp == 1) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
                          smem_u32(&cs->tmem_base)),
@@ -210,13 +236,13 @@ __global__ void __launch_bounds__(G_THREADS, 1)
         // ---------------- TMA producer
         int issued = 0;
         for (int kb = 0; kb < nkb; kb++) {
-            const int s = kb % GSTAGES;
-            const uint32_t ph = (uint32_t)(kb / GSTAGES) & 1u;
+            const int s = kb % ST;
+            const uint32_t ph = (uint32_t)(kb / ST) & 1u;
             if (!mbar_wait(smem_u32(&cs->empty[s]), ph ^ 1u, status)) break;
             uint8_t *st = base + s * STAGE_BYTES;
             const uint32_t fb = smem_u32(&cs->full[s]);
             mbar_expect_tx(fb, STAGE_BYTES);
-            const int kc = kb * (KIND == 0 ? 64 : 32);
+            const int kc = kb * (KB / (KIND == 0 ? 2 : 4));
             tma_load_2d(smem_u32(st), &tmAh, fb, kc, m0);
             tma_load_2d(smem_u32(st + A_BYTES), &tmAl, fb, kc, m0);
             tma_load_2d(smem_u32(st + 2 * A_BYTES), &tmBh, fb, kc, n0);
@@ -225,9 +251,9 @@ __global__ void __launch_bounds__(G_THREADS, 1)
         }
         // on an early exit, wait (bounded) for the copies still landing in shared memory
         if (*(volatile int *)status != 0) {
-            int first = issued - GSTAGES < 0 ? 0 : issued - GSTAGES;
+            int first = issued - ST < 0 ? 0 : issued - ST;
             for (int kb = first; kb < issued; kb++)
-                mbar_wait_quiet(smem_u32(&cs->full[kb % GSTAGES]), (uint32_t)(kb / GSTAGES) & 1u);
+                mbar_wait_quiet(smem_u32(&cs->full[kb % ST]), (uint32_t)(kb / ST) & 1u);
         }
     } else if (warp == 1 && lane == 0) {
         // ---------------- MMA issuer
@@ -236,15 +262,15 @@ __global__ void __launch_bounds__(G_THREADS, 1)
                                    | ((KIND == 0 ? 1u : 2u) << 10)    // B: bf16 | tf32
                                    | ((uint32_t)(GN >> 3) << 17)      // N
                                    | ((uint32_t)(GM >> 4) << 24);     // M
-        constexpr int KSTEPS = (KIND == 0) ? 4 : 4;  // 32-byte k-steps per 128-byte row
+        constexpr int KSTEPS = KB / 32;  // one UMMA consumes 32 bytes of K
         for (int kb = 0; kb < nkb; kb++) {
-            const int s = kb % GSTAGES;
-            const uint32_t ph = (uint32_t)(kb / GSTAGES) & 1u;
+            const int s = kb % ST;
+            const uint32_t ph = (uint32_t)(kb / ST) & 1u;
             if (!mbar_wait(smem_u32(&cs->full[s]), ph, status)) break;
             tc_fence_after();
             const uint32_t st = smem_u32(base + s * STAGE_BYTES);
-            const uint64_t ah = sw128_desc(st), al = sw128_desc(st + A_BYTES), bh = sw128_desc(st + 2 * A_BYTES),
-                           bl = sw128_desc(st + 2 * A_BYTES + B_BYTES);
+            const uint64_t ah = swz_desc<KB>(st), al = swz_desc<KB>(st + A_BYTES),
+                           bh = swz_desc<KB>(st + 2 * A_BYTES), bl = swz_desc<KB>(st + 2 * A_BYTES + B_BYTES);
 #pragma unroll
             for (int k = 0; k < KSTEPS; k++) {
                 const uint64_t dk = (uint64_t)(k * 32) >> 4;  // advance 32 bytes along K
@@ -264,7 +290,7 @@ __global__ void __launch_bounds__(G_THREADS, 1)
         tc_fence_after();
         const int m = m0 + q * 32 + lane;
         if (ok) {
-            const int64_t roff = ((int64_t)m / epi.rdiv) * epi.rs1 + ((int64_t)m % epi.rdiv) * epi.rs2;
+            const int64_t roff = map3(epi.row, (int64_t)m);
             for (int c = 0; c < GN; c += 32) {
                 float v[32];
                 tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)c, v);
@@ -311,12 +337,11 @@ __device__ __forceinline__ void split_tf32(double x, float &hi, float &lo) {
 }
 
 // Generic split of a strided FP64 operand into K-major pieces:
-//   dst[m][k] for m < M, k < Kp (k >= K zero-filled) from
-//   src[(m / mdiv)*ms1 + (m % mdiv)*ms2 + (k / kdiv)*ks1 + (k % kdiv)*ks2].
-// 32x32 tiles through shared memory so both sides are coalesced whichever
-// index is contiguous in the source.
+//   dst[m][k] for m < M, k < Kp (k >= K zero-filled) from src[mmap(m) + kmap(k)]
+// with three-digit mixed-radix maps.  32x32 tiles through shared memory so
+// both sides are coalesced whichever index is contiguous in the source.
 struct SplitMap {
-    int64_t mdiv, ms1, ms2, kdiv, ks1, ks2;
+    Map3 m, k;
 };
 
 template <int KIND>
@@ -325,14 +350,18 @@ __global__ void k_split(const double *src, void *hi, void *lo, int64_t M, int64_
     const int64_t mt = (int64_t)blockIdx.y * 32, kt = (int64_t)blockIdx.x * 32;
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8 threads
     // read: pick the tile orientation that keeps the source reads contiguous
-    const bool k_fast = mp.ks2 == 1 && mp.kdiv >= 32;
-    const int mdiv = (int)mp.mdiv, kdiv = (int)mp.kdiv;
+    const bool k_fast = mp.k.S2 == 1 && mp.k.R2 >= 32;
+    const int mR1 = (int)mp.m.R1, mR2 = (int)mp.m.R2, kR1 = (int)mp.k.R1, kR2 = (int)mp.k.R2;
     for (int r = ty; r < 32; r += 8) {
         int m = (int)mt + (k_fast ? r : tx), k = (int)kt + (k_fast ? tx : r);
         double v = 0.0;
-        if (m < M && k < K)
-            v = src[(int64_t)(m / mdiv) * mp.ms1 + (int64_t)(m % mdiv) * mp.ms2 + (int64_t)(k / kdiv) * mp.ks1 +
-                    (int64_t)(k % kdiv) * mp.ks2];
+        if (m < M && k < K) {
+            const int64_t mo = (int64_t)(m / (mR1 * mR2)) * mp.m.S0 + (int64_t)((m / mR2) % mR1) * mp.m.S1 +
+                               (int64_t)(m % mR2) * mp.m.S2;
+            const int64_t ko = (int64_t)(k / (kR1 * kR2)) * mp.k.S0 + (int64_t)((k / kR2) % kR1) * mp.k.S1 +
+                               (int64_t)(k % kR2) * mp.k.S2;
+            v = src[mo + ko];
+        }
         if (k_fast)
             tile[r][tx] = v;
         else
@@ -357,6 +386,8 @@ __global__ void k_split(const double *src, void *hi, void *lo, int64_t M, int64_
     }
 }
 
+static bool map3_ok(const int64_t *f) { return f[0] >= 1 && f[1] >= 1 && f[0] * f[1] < (1ll << 31); }
+
 // ----------------------------------------------------------------- host side
 
 typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
@@ -375,8 +406,10 @@ static EncodeTiledFn encode_fn() {
     return fn;
 }
 
-// 2-D K-major piece [rows][Kp] with a (k-block x box_rows) box, 128-byte swizzle.
-static int make_map(CUtensorMap *map, const void *ptr, int kind, int64_t rows, int64_t Kp, int box_rows) {
+// 2-D K-major piece [rows][Kp] with a (k-block x box_rows) box and the
+// swizzle that matches kb_bytes.
+static int make_map(CUtensorMap *map, const void *ptr, int kind, int64_t rows, int64_t Kp, int box_rows,
+                    int kb_bytes) {
     EncodeTiledFn fn = encode_fn();
     if (!fn) {
         set_error("cuTensorMapEncodeTiled is unavailable");
@@ -385,12 +418,13 @@ static int make_map(CUtensorMap *map, const void *ptr, int kind, int64_t rows, i
     const int esz = kind == 0 ? 2 : 4;
     cuuint64_t dims[2] = {(cuuint64_t)Kp, (cuuint64_t)rows};
     cuuint64_t strides[1] = {(cuuint64_t)(Kp * esz)};
-    cuuint32_t box[2] = {(cuuint32_t)(GK_BYTES / esz), (cuuint32_t)box_rows};
+    cuuint32_t box[2] = {(cuuint32_t)(kb_bytes / esz), (cuuint32_t)box_rows};
     cuuint32_t estr[2] = {1, 1};
+    CUtensorMapSwizzle sw = kb_bytes == 128 ? CU_TENSOR_MAP_SWIZZLE_128B
+                                            : (kb_bytes == 64 ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_32B);
     CUresult r = fn(map, kind == 0 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2,
-                    const_cast<void *>(ptr), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                    CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+                    const_cast<void *>(ptr), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, sw,
+                    CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) {
         set_error("cuTensorMapEncodeTiled failed (%d)", (int)r);
         return DCC_ERR_CUDA;
@@ -398,8 +432,21 @@ static int make_map(CUtensorMap *map, const void *ptr, int kind, int64_t rows, i
     return DCC_OK;
 }
 
-static size_t gemm_smem_bytes() {
-    return 1024 + GSTAGES * (size_t)(2 * GM * GK_BYTES + 2 * GN * GK_BYTES) + sizeof(GemmSmem);
+template <int ST>
+static size_t gemm_smem_bytes(int kb_bytes) {
+    return 1024 + ST * (size_t)(2 * GM * kb_bytes + 2 * GN * kb_bytes) + sizeof(GemmSmem<ST>);
+}
+
+template <int KIND, int KB, int ST>
+static int gemm_launch(const CUtensorMap &a, const CUtensorMap &b, const CUtensorMap &c, const CUtensorMap &d, int M,
+                       int N, int nkb, double *C, const GemmEpi &epi, double alpha, double beta, int *status,
+                       int group_m, cudaStream_t st) {
+    size_t smem = gemm_smem_bytes<ST>(KB);
+    unsigned tiles = ceil_div(N, GN) * ceil_div(M, GM);
+    cudaFuncSetAttribute(k_gemm_split3<KIND, KB, ST>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_gemm_split3<KIND, KB, ST><<<tiles, G_THREADS, smem, st>>>(a, b, c, d, M, N, nkb, C, epi, alpha, beta, status,
+                                                                group_m);
+    return launch_status("gemm_split3");
 }
 
 }  // namespace dcc
@@ -407,17 +454,16 @@ static size_t gemm_smem_bytes() {
 using namespace dcc;
 
 extern "C" int dcc_split_operand(const double *src, void *hi, void *lo, int64_t M, int64_t K, int64_t Kp,
-                                 const int64_t *map6, int kind, void *stream) {
+                                 const int64_t *map10, int kind, void *stream) {
     clear_error();
     DCC_REQUIRE(M >= 0 && K >= 0 && Kp >= K, DCC_ERR_SHAPE, "bad split sizes (M=%lld K=%lld Kp=%lld)",
                 (long long)M, (long long)K, (long long)Kp);
     DCC_REQUIRE(kind == 0 || kind == 1, DCC_ERR_UNSUPPORTED, "split kind must be 0 (bf16) or 1 (tf32)");
     if (M == 0 || Kp == 0) return DCC_OK;
-    DCC_REQUIRE(src && hi && lo && map6, DCC_ERR_NULL, "NULL buffer");
-    SplitMap mp{map6[0], map6[1], map6[2], map6[3], map6[4], map6[5]};
-    DCC_REQUIRE(mp.mdiv > 0 && mp.kdiv > 0, DCC_ERR_SHAPE, "split map divisors must be positive");
-    DCC_REQUIRE(M < (1ll << 31) && Kp < (1ll << 31) && mp.mdiv < (1ll << 31) && mp.kdiv < (1ll << 31), DCC_ERR_SHAPE,
-                "split sizes must fit in 31 bits");
+    DCC_REQUIRE(src && hi && lo && map10, DCC_ERR_NULL, "NULL buffer");
+    DCC_REQUIRE(map3_ok(map10) && map3_ok(map10 + 5), DCC_ERR_SHAPE, "map radices must be >= 1 with R1*R2 < 2^31");
+    DCC_REQUIRE(M < (1ll << 31) && Kp < (1ll << 31), DCC_ERR_SHAPE, "split sizes must fit in 31 bits");
+    SplitMap mp{{map10[0], map10[1], map10[2], map10[3], map10[4]}, {map10[5], map10[6], map10[7], map10[8], map10[9]}};
     dim3 grid(ceil_div(Kp, 32), ceil_div(M, 32));
     DCC_REQUIRE(grid.y <= 65535, DCC_ERR_UNSUPPORTED, "M too large for one split launch");
     if (kind == 0)
@@ -428,7 +474,7 @@ extern "C" int dcc_split_operand(const double *src, void *hi, void *lo, int64_t 
 }
 
 extern "C" int dcc_gemm_split3(const void *A_hi, const void *A_lo, const void *B_hi, const void *B_lo, int64_t M,
-                               int64_t N, int64_t Kp, double *C, const int64_t *epi6, double alpha, double beta,
+                               int64_t N, int64_t Kp, double *C, const int64_t *epi10, double alpha, double beta,
                                int kind, int *status, void *stream) {
     clear_error();
     DCC_REQUIRE(kind == 0 || kind == 1, DCC_ERR_UNSUPPORTED, "kind must be 0 (bf16x3) or 1 (tf32x3)");
@@ -437,28 +483,54 @@ extern "C" int dcc_gemm_split3(const void *A_hi, const void *A_lo, const void *B
                 "Kp (%lld) must be a multiple of %d", (long long)Kp, kblk);
     DCC_REQUIRE(M < (1ll << 31) && N < (1ll << 31), DCC_ERR_SHAPE, "M, N must fit in 31 bits");
     if (M == 0 || N == 0) return DCC_OK;
-    DCC_REQUIRE(A_hi && A_lo && B_hi && B_lo && C && epi6 && status, DCC_ERR_NULL, "NULL buffer");
+    DCC_REQUIRE(A_hi && A_lo && B_hi && B_lo && C && epi10 && status, DCC_ERR_NULL, "NULL buffer");
     DCC_REQUIRE(Kp > 0, DCC_ERR_SHAPE, "empty contraction");
-    GemmEpi epi{epi6[0], epi6[1], epi6[2], epi6[3], epi6[4], epi6[5]};
-    DCC_REQUIRE(epi.rdiv > 0 && epi.cdiv > 0, DCC_ERR_SHAPE, "epilogue divisors must be positive");
+    DCC_REQUIRE(map3_ok(epi10) && map3_ok(epi10 + 5), DCC_ERR_SHAPE, "map radices must be >= 1 with R1*R2 < 2^31");
+    GemmEpi epi{{epi10[0], epi10[1], epi10[2], epi10[3], epi10[4]}, {epi10[5], epi10[6], epi10[7], epi10[8], epi10[9]}};
+    const GemmConfig cfg = g_cfg;
+    DCC_REQUIRE(Kp % (cfg.kb_bytes / (kind == 0 ? 2 : 4)) == 0, DCC_ERR_SHAPE,
+                "Kp (%lld) must be a multiple of the k-block", (long long)Kp);
     CUtensorMap mAh, mAl, mBh, mBl;
     int rc;
-    if ((rc = make_map(&mAh, A_hi, kind, M, Kp, GM)) || (rc = make_map(&mAl, A_lo, kind, M, Kp, GM)) ||
-        (rc = make_map(&mBh, B_hi, kind, N, Kp, GN)) || (rc = make_map(&mBl, B_lo, kind, N, Kp, GN)))
+    if ((rc = make_map(&mAh, A_hi, kind, M, Kp, GM, cfg.kb_bytes)) ||
+        (rc = make_map(&mAl, A_lo, kind, M, Kp, GM, cfg.kb_bytes)) ||
+        (rc = make_map(&mBh, B_hi, kind, N, Kp, GN, cfg.kb_bytes)) ||
+        (rc = make_map(&mBl, B_lo, kind, N, Kp, GN, cfg.kb_bytes)))
         return rc;
-    size_t smem = gemm_smem_bytes();
-    dim3 grid(ceil_div(N, GN), ceil_div(M, GM));
-    DCC_REQUIRE(grid.y <= 65535, DCC_ERR_UNSUPPORTED, "M too large for one launch");
     cudaStream_t st = as_stream(stream);
-    int nkb = (int)(Kp / kblk);
-    if (kind == 0) {
-        cudaFuncSetAttribute(k_gemm_split3<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        k_gemm_split3<0><<<grid, G_THREADS, smem, st>>>(mAh, mAl, mBh, mBl, (int)M, (int)N, nkb, C, epi, alpha, beta,
-                                                        status);
-    } else {
-        cudaFuncSetAttribute(k_gemm_split3<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        k_gemm_split3<1><<<grid, G_THREADS, smem, st>>>(mAh, mAl, mBh, mBl, (int)M, (int)N, nkb, C, epi, alpha, beta,
-                                                        status);
-    }
-    return launch_status("gemm_split3");
+    const int nkb = (int)(Kp / (cfg.kb_bytes / (kind == 0 ? 2 : 4)));
+    const int iM = (int)M, iN = (int)N, gm = cfg.group_m;
+#define DCC_GEMM_CASE(K_, KB_, ST_)                                                                           \
+    if (kind == K_ && cfg.kb_bytes == KB_ && cfg.stages == ST_)                                              \
+        return gemm_launch<K_, KB_, ST_>(mAh, mAl, mBh, mBl, iM, iN, nkb, C, epi, alpha, beta, status, gm, st);
+    DCC_GEMM_CASE(0, 128, 2)
+    DCC_GEMM_CASE(0, 64, 4)
+    DCC_GEMM_CASE(0, 64, 3)
+    DCC_GEMM_CASE(0, 32, 8)
+    DCC_GEMM_CASE(1, 128, 2)
+    DCC_GEMM_CASE(1, 64, 4)
+    DCC_GEMM_CASE(1, 64, 3)
+    DCC_GEMM_CASE(1, 32, 8)
+#undef DCC_GEMM_CASE
+    set_error("no kernel for k-block %d bytes x %d stages", cfg.kb_bytes, cfg.stages);
+    return DCC_ERR_UNSUPPORTED;
+}
+
+extern "C" int dcc_gemm_set_config(int kb_bytes, int stages, int group_m) {
+    clear_error();
+    const bool ok = (kb_bytes == 128 && stages == 2) || (kb_bytes == 64 && (stages == 3 || stages == 4)) ||
+                    (kb_bytes == 32 && stages == 8);
+    DCC_REQUIRE(ok, DCC_ERR_UNSUPPORTED, "unsupported pipeline (k-block %d bytes, %d stages)", kb_bytes, stages);
+    DCC_REQUIRE(group_m >= 1 && group_m <= 4096, DCC_ERR_SHAPE, "group_m must be in [1, 4096]");
+    dcc::g_cfg = dcc::GemmConfig{kb_bytes, stages, group_m};
+    return DCC_OK;
+}
+
+extern "C" int dcc_gemm_get_config(int *kb_bytes, int *stages, int *group_m) {
+    clear_error();
+    DCC_REQUIRE(kb_bytes && stages && group_m, DCC_ERR_NULL, "NULL argument");
+    *kb_bytes = dcc::g_cfg.kb_bytes;
+    *stages = dcc::g_cfg.stages;
+    *group_m = dcc::g_cfg.group_m;
+    return DCC_OK;
 }

@@ -120,6 +120,63 @@ struct P3Coef {
     double p0, p1, p2, p3, p4, alpha, beta, p012, ap34;
 };
 
+// kComp[X][s]: the axis map equal to "s, then X" (X(s(u)) = kComp[X][s](u)).
+__constant__ int kComp[6][6] = {{0, 1, 2, 3, 4, 5}, {1, 0, 3, 2, 5, 4}, {2, 4, 0, 5, 1, 3},
+                                {3, 5, 1, 4, 0, 2}, {4, 2, 5, 0, 3, 1}, {5, 3, 4, 1, 2, 0}};
+
+// P3 spin summation of a whole orbit set in shared memory, in place.  Each
+// thread takes canonical positions u (global u0 <= u1 <= u2, all inside slot
+// 0), reads the six values v[s] = A(s(u)) once and writes the six results
+//   R(w) = beta A(w) + alpha (p3 T(w) + p4 T(w0,w2,w1)),
+//   T(w) = p0 A(w) + p1 A(w2,w1,w0) + p2 A(w1,w0,w2),     w = s(u),
+// which read only values of the same orbit; positions that coincide (equal
+// indices) get identical values from the same thread.
+__device__ __forceinline__ void p3_orbits_inplace(double *buf, const OrbitSet &os, int t0, int t1, int t2, int nv,
+                                                  const P3Coef &k) {
+    const int *nbr = os.nbr[0];
+    for (int e = threadIdx.x; e < TE3; e += blockDim.x) {
+        const int x = e >> 6, y = (e >> 3) & 7, z = e & 7;
+        const int gx = t0 * TE + x, gy = t1 * TE + y, gz = t2 * TE + z;
+        if (gx >= nv || gy >= nv || gz >= nv) continue;
+        if ((t0 == t1 && x > y) || (t1 == t2 && y > z)) continue;  // not canonical
+        int a[6];
+        a[0] = nbr[0] * SLOT + sidx(x, y, z);
+        a[1] = nbr[1] * SLOT + sidx(x, z, y);
+        a[2] = nbr[2] * SLOT + sidx(y, x, z);
+        a[3] = nbr[3] * SLOT + sidx(y, z, x);
+        a[4] = nbr[4] * SLOT + sidx(z, x, y);
+        a[5] = nbr[5] * SLOT + sidx(z, y, x);
+        double v[6];
+#pragma unroll
+        for (int q = 0; q < 6; q++) v[q] = buf[a[q]];
+        if (gx == gy && gy == gz) {
+            buf[a[0]] = dadd(dmul(k.beta, v[0]), dmul(k.ap34, dmul(k.p012, v[0])));
+            continue;
+        }
+        double r[6];
+#pragma unroll
+        for (int q = 0; q < 6; q++) {
+            double tu = dadd(dadd(dmul(k.p0, v[q]), dmul(k.p1, v[kComp[5][q]])), dmul(k.p2, v[kComp[2][q]]));
+            double tw = dadd(dadd(dmul(k.p0, v[kComp[1][q]]), dmul(k.p1, v[kComp[3][q]])), dmul(k.p2, v[kComp[4][q]]));
+            r[q] = dadd(dmul(k.beta, v[q]), dmul(k.alpha, dadd(dmul(k.p3, tu), dmul(k.p4, tw))));
+        }
+#pragma unroll
+        for (int q = 0; q < 6; q++) buf[a[q]] = r[q];
+    }
+}
+
+// Coalesced store of every slot of an orbit set from shared memory.
+__device__ __forceinline__ void store_orbit_tiles(double *blk, const double *buf, const OrbitSet &os, int nv) {
+    for (int s = 0; s < os.nslot; s++) {
+        const int X0 = os.tile[s][0] * TE, Y0 = os.tile[s][1] * TE, Z0 = os.tile[s][2] * TE;
+        for (int e = threadIdx.x; e < TE3; e += blockDim.x) {
+            int x = e >> 6, y = (e >> 3) & 7, z = e & 7;
+            int gx = X0 + x, gy = Y0 + y, gz = Z0 + z;
+            if (gx < nv && gy < nv && gz < nv) blk[((int64_t)gx * nv + gy) * nv + gz] = buf[s * SLOT + sidx(x, y, z)];
+        }
+    }
+}
+
 // Orbit-tile kernel.  MODE 0: P3 spin summation in place (out0 == in).
 // MODE 1: triple-sym (out0..out2).  MODE 2: transpose-add (out0).
 // Each CTA owns one canonical tile triple and walks the blocks
@@ -148,6 +205,13 @@ __global__ void __launch_bounds__(OT_THREADS) k_orbit3(const double *in, double 
             cp_async_wait<0>();
         }
         __syncthreads();
+        if (MODE == 0) {
+            p3_orbits_inplace(sm + stage * 6 * SLOT, os, t0, t1, t2, nv, k);
+            __syncthreads();
+            store_orbit_tiles(out0 + b * n3, sm + stage * 6 * SLOT, os, nv);
+            __syncthreads();  // buf is refilled two iterations later
+            continue;
+        }
         const double *buf = sm + stage * 6 * SLOT;
         for (int s = 0; s < os.nslot; s++) {
             const int X0 = os.tile[s][0] * TE, Y0 = os.tile[s][1] * TE, Z0 = os.tile[s][2] * TE;
@@ -188,6 +252,119 @@ __global__ void __launch_bounds__(OT_THREADS) k_orbit3(const double *in, double 
     }
 }
 
+// In-place P3 spin summation.  The tile geometry of a CTA is the same for
+// every block, so each thread computes its shared/global offsets once: up to
+// 12 (slot, element) copies and up to 2 canonical orbits (6 shared addresses
+// each).  Per block the CTA then issues its cp.async copies, sums its orbits
+// in shared memory and stores, while the copies of the next block are in
+// flight; thread 0 also stages its share of the block after next into L2
+// (cp.async.bulk.prefetch.L2) so the 64-byte tile rows are read from L2.
+__global__ void __launch_bounds__(OT_THREADS, 3) k_p3_inplace(double *A, int64_t nblocks, int nv, int ntile, P3Coef k) {
+    extern __shared__ double sm[];  // 2 x 6 x SLOT doubles
+    __shared__ OrbitSet os;
+    int t0, t1, t2;
+    decode_tri3(blockIdx.x, ntile, t0, t1, t2);
+    build_orbit_set(os, t0, t1, t2);
+    const int64_t n3 = (int64_t)nv * nv * nv;
+    // copies: pair j -> slot j / 2, element threadIdx.x + 256 * (j % 2)
+    int goff[12];
+    unsigned short soff[12];
+    unsigned nload = 0;
+    for (int j = 0; j < 12; j++) {
+        const int sl = j >> 1, e = threadIdx.x + OT_THREADS * (j & 1);
+        goff[j] = -1;
+        soff[j] = 0;
+        if (sl >= os.nslot) continue;
+        const int x = e >> 6, y = (e >> 3) & 7, z = e & 7;
+        const int gx = os.tile[sl][0] * TE + x, gy = os.tile[sl][1] * TE + y, gz = os.tile[sl][2] * TE + z;
+        if (gx >= nv || gy >= nv || gz >= nv) continue;
+        goff[j] = (gx * nv + gy) * nv + gz;
+        soff[j] = (unsigned short)(sl * SLOT + sidx(x, y, z));
+        nload |= 1u << j;
+    }
+    // canonical orbit positions of this thread (inside slot 0)
+    unsigned short oa[2][6];
+    int ocls[2];  // 0: none, 1: generic, 2: all indices equal
+    for (int h = 0; h < 2; h++) {
+        const int e = threadIdx.x + OT_THREADS * h;
+        const int x = e >> 6, y = (e >> 3) & 7, z = e & 7;
+        const int gx = t0 * TE + x, gy = t1 * TE + y, gz = t2 * TE + z;
+        ocls[h] = 0;
+        if (gx >= nv || gy >= nv || gz >= nv || (t0 == t1 && x > y) || (t1 == t2 && y > z)) continue;
+        const int *nb = os.nbr[0];
+        oa[h][0] = (unsigned short)(nb[0] * SLOT + sidx(x, y, z));
+        oa[h][1] = (unsigned short)(nb[1] * SLOT + sidx(x, z, y));
+        oa[h][2] = (unsigned short)(nb[2] * SLOT + sidx(y, x, z));
+        oa[h][3] = (unsigned short)(nb[3] * SLOT + sidx(y, z, x));
+        oa[h][4] = (unsigned short)(nb[4] * SLOT + sidx(z, x, y));
+        oa[h][5] = (unsigned short)(nb[5] * SLOT + sidx(z, y, x));
+        ocls[h] = (gx == gy && gy == gz) ? 2 : 1;
+    }
+    // this CTA's share of a block for the L2 staging prefetch
+    const int64_t ntri = gridDim.x;
+    const int64_t share = ((n3 * 8 + ntri - 1) / ntri + 15) / 16 * 16;
+    const int64_t pf_off = share * blockIdx.x;
+    const int64_t pf_len = pf_off >= n3 * 8 ? 0 : (pf_off + share > n3 * 8 ? ((n3 * 8 - pf_off) / 16) * 16 : share);
+
+    int64_t b = blockIdx.y;
+    if (b >= nblocks) return;
+    auto issue = [&](double *buf, const double *blk) {
+#pragma unroll
+        for (int j = 0; j < 12; j++)
+            if (nload & (1u << j)) cp_async8(buf + soff[j], blk + goff[j]);
+    };
+    auto stage_l2 = [&](int64_t bb) {
+        const char *src = (const char *)(A + bb * n3) + pf_off;
+        // the bulk prefetch needs a 16-byte aligned source (blocks of odd nvir^3 are only 8-aligned)
+        if (threadIdx.x == 0 && bb < nblocks && pf_len > 0 && (((uintptr_t)src) & 15) == 0) {
+            asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"((unsigned)pf_len) : "memory");
+        }
+    };
+    stage_l2(b + gridDim.y);
+    issue(sm, A + b * n3);
+    cp_async_commit();
+    for (int stage = 0; b < nblocks; b += gridDim.y, stage ^= 1) {
+        const int64_t nb_ = b + gridDim.y;
+        stage_l2(nb_ + gridDim.y);
+        if (nb_ < nblocks) {
+            issue(sm + (stage ^ 1) * 6 * SLOT, A + nb_ * n3);
+            cp_async_commit();
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
+        }
+        __syncthreads();
+        double *buf = sm + stage * 6 * SLOT;
+#pragma unroll 1
+        for (int h = 0; h < 2; h++) {
+            if (ocls[h] == 0) continue;
+            double v[6];
+#pragma unroll
+            for (int q = 0; q < 6; q++) v[q] = buf[oa[h][q]];
+            if (ocls[h] == 2) {
+                buf[oa[h][0]] = dadd(dmul(k.beta, v[0]), dmul(k.ap34, dmul(k.p012, v[0])));
+                continue;
+            }
+            double r[6];
+#pragma unroll
+            for (int q = 0; q < 6; q++) {
+                double tu = dadd(dadd(dmul(k.p0, v[q]), dmul(k.p1, v[kComp[5][q]])), dmul(k.p2, v[kComp[2][q]]));
+                double tw =
+                    dadd(dadd(dmul(k.p0, v[kComp[1][q]]), dmul(k.p1, v[kComp[3][q]])), dmul(k.p2, v[kComp[4][q]]));
+                r[q] = dadd(dmul(k.beta, v[q]), dmul(k.alpha, dadd(dmul(k.p3, tu), dmul(k.p4, tw))));
+            }
+#pragma unroll
+            for (int q = 0; q < 6; q++) buf[oa[h][q]] = r[q];
+        }
+        __syncthreads();
+        double *blk = A + b * n3;
+#pragma unroll
+        for (int j = 0; j < 12; j++)
+            if (nload & (1u << j)) blk[goff[j]] = buf[soff[j]];
+        __syncthreads();  // buf is refilled two iterations later
+    }
+}
+
 int p3_pattern(const char *name, double p[5]) {
     static const struct {
         const char *n;
@@ -216,6 +393,11 @@ static int orbit3_launch(int mode, const double *in, double *o0, double *o1, dou
     dim3 grid((unsigned)ntri, (unsigned)gy);
     size_t smem = 2 * 6 * SLOT * sizeof(double);
     cudaStream_t st = as_stream(stream);
+    if (mode == 0 && nvir <= 1290) {  // 32-bit element offsets inside a block
+        cudaFuncSetAttribute(k_p3_inplace, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        k_p3_inplace<<<grid, OT_THREADS, smem, st>>>(o0, nblocks, (int)nvir, ntile, k);
+        return launch_status("P3 spin summation");
+    }
     if (mode == 0) cudaFuncSetAttribute(k_orbit3<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (mode == 1) cudaFuncSetAttribute(k_orbit3<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (mode == 2) cudaFuncSetAttribute(k_orbit3<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -356,13 +538,27 @@ __global__ void __launch_bounds__(UPD_THREADS) k_t3_divide_update(double *t3, do
         const double *ek = eia + (int64_t)ijk[3 * q + 2] * nv;
         double *rr = r3 + row * nv, *tt = t3 + row * nv;
         const bool act_ab = a < nact && b < nact;
-        for (int c = lane; c < nv; c += 32) {
-            double r = __ddiv_rn(rr[c], dadd(dab, ek[c]));
-            if (write_r3) rr[c] = r;
-            tt[c] = dadd(tt[c], r);
-            double r2 = r * r;
-            s_all += r2;
-            if (act_ab && c < nact) s_act += r2;
+        for (int c0 = 0; c0 < nv; c0 += 96) {
+            // issue every load of this chunk before the first use
+            double rv[3], tv[3], ev[3];
+#pragma unroll
+            for (int u = 0; u < 3; u++) {
+                const int c = c0 + lane + 32 * u;
+                rv[u] = c < nv ? rr[c] : 0.0;
+                tv[u] = c < nv ? tt[c] : 0.0;
+                ev[u] = c < nv ? ek[c] : 1.0;
+            }
+#pragma unroll
+            for (int u = 0; u < 3; u++) {
+                const int c = c0 + lane + 32 * u;
+                if (c >= nv) continue;
+                double r = __ddiv_rn(rv[u], dadd(dab, ev[u]));
+                if (write_r3) rr[c] = r;
+                tt[c] = dadd(tv[u], r);
+                double r2 = r * r;
+                s_all += r2;
+                if (act_ab && c < nact) s_act += r2;
+            }
         }
     }
     __shared__ double red[2][UPD_THREADS / 32];
@@ -708,69 +904,170 @@ extern "C" int dcc_fill_t3_from_abc(double *target, int64_t a0, int64_t a1, int6
     return launch_status("fill_t3_from_abc");
 }
 
-// ---------------------------------------------------------------- S3 gather
+// ---------------------------------------------------------------- permutation gather
 
 namespace dcc {
 
-struct S3Src {
+constexpr int PG_MAX_SRC = 4;
+constexpr int PG_MAX_SLOTS = 12;
+
+struct PermSrc {
     const double *base;
     double scale;
     int64_t st[6];  // strides of (x, y, z, a, b, c)
+    int mask;       // bit p set: include the simultaneous permutation p
 };
 
-// r3[q][a][b][c] = beta * r3 + sum_s scale_s * sum_sigma U_s(sigma(i,j,k), sigma(a,b,c))
-// for the canonical triple (i,j,k) = ijk[q]; sigma runs over the six
-// simultaneous permutations of the occupied and virtual index triples.
-// One warp per output row (q, a, b); lanes stride over c.
-__global__ void k_s3_gather(double *r3, const int32_t *ijk, int64_t nblocks, int nv, double beta, S3Src s0, S3Src s1,
-                            int nsrc) {
-    const int lane = threadIdx.x & 31;
-    const int64_t nrow = nblocks * nv * nv;
-    for (int64_t row = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; row < nrow;
-         row += ((int64_t)gridDim.x * blockDim.x) >> 5) {
-        int64_t q = row / (nv * nv);
-        int ab = (int)(row - q * nv * nv), a = ab / nv, b = ab - a * nv;
-        const int o[3] = {ijk[3 * q], ijk[3 * q + 1], ijk[3 * q + 2]};
-        double *out = r3 + row * nv;
-        for (int c = lane; c < nv; c += 32) {
-            const int v[3] = {a, b, c};
-            double acc = 0.0;
-            for (int s = 0; s < nsrc; s++) {
-                const S3Src &S = s ? s1 : s0;
-                double part = 0.0;
+struct PermGatherArgs {
+    PermSrc src[PG_MAX_SRC];
+    int nsrc, nslot;
+    int slot_src[PG_MAX_SLOTS], slot_perm[PG_MAX_SLOTS];
+    double slot_scale[PG_MAX_SLOTS];
+};
+
+// r3[q][a][b][c] = beta*r3 + sum_s scale_s sum_{p in mask_s} U_s(p(ijk), p(abc)).
+// A CTA owns one 8^3 output tile and walks the blocks q; the source tiles of
+// the next block are copied while the current block is summed.  The virtual
+// part of every source offset and every shared address depend only on the
+// tile, so each thread computes them once (2 elements x up to 12 slots).
+__global__ void __launch_bounds__(256) k_perm_gather(double *r3, const int32_t *ijk, int64_t nblocks, int nv,
+                                                     int ntile, double beta, PermGatherArgs g) {
+    extern __shared__ double pg_sm[];  // 2 x nslot x SLOT
+    const int T[3] = {(int)(blockIdx.x / (ntile * ntile)), (int)((blockIdx.x / ntile) % ntile),
+                      (int)(blockIdx.x % ntile)};
+    const int64_t n3 = (int64_t)nv * nv * nv;
+    int voff[PG_MAX_SLOTS][2];            // virtual offset of the copied source element, -1: none
+    unsigned short rd[PG_MAX_SLOTS][2];   // shared address read for output element h
+    unsigned short wr[2];                 // shared address the copy of element h lands at (per slot base added)
+    int ooff[2];                          // output element offset in the block, -1: outside
 #pragma unroll
-                for (int p = 0; p < 6; p++) {
-                    const int m0 = perm3(p, 0), m1 = perm3(p, 1), m2 = perm3(p, 2);
-                    part += S.base[o[m0] * S.st[0] + o[m1] * S.st[1] + o[m2] * S.st[2] + v[m0] * S.st[3] +
-                                   v[m1] * S.st[4] + v[m2] * S.st[5]];
-                }
-                acc = fma(S.scale, part, acc);
-            }
-            out[c] = (beta == 0.0) ? acc : fma(beta, out[c], acc);
+    for (int h = 0; h < 2; h++) {
+        const int e = threadIdx.x + 256 * h;
+        const int u[3] = {e >> 6, (e >> 3) & 7, e & 7};
+        wr[h] = (unsigned short)sidx(u[0], u[1], u[2]);
+        const int ga = T[0] * TE + u[0], gb = T[1] * TE + u[1], gc = T[2] * TE + u[2];
+        ooff[h] = (ga < nv && gb < nv && gc < nv) ? (ga * nv + gb) * nv + gc : -1;
+#pragma unroll
+        for (int sl = 0; sl < PG_MAX_SLOTS; sl++) {
+            voff[sl][h] = -1;
+            rd[sl][h] = 0;
+            if (sl >= g.nslot) continue;
+            const PermSrc &S = g.src[g.slot_src[sl]];
+            const int p = g.slot_perm[sl];
+            // copy: slot tile = p(T), element u in the source's own order
+            const int TT[3] = {T[perm3(p, 0)], T[perm3(p, 1)], T[perm3(p, 2)]};
+            const int sa = TT[0] * TE + u[0], sb = TT[1] * TE + u[1], sc = TT[2] * TE + u[2];
+            if (sa < nv && sb < nv && sc < nv) voff[sl][h] = (int)(sa * S.st[3] + sb * S.st[4] + sc * S.st[5]);
+            // read: output element u needs the source element p(u) of the slot
+            rd[sl][h] = (unsigned short)(sl * SLOT + sidx(u[perm3(p, 0)], u[perm3(p, 1)], u[perm3(p, 2)]));
         }
+    }
+    auto issue = [&](double *buf, int64_t q) {
+        const int o[3] = {ijk[3 * q], ijk[3 * q + 1], ijk[3 * q + 2]};
+#pragma unroll
+        for (int sl = 0; sl < PG_MAX_SLOTS; sl++) {
+            if (sl >= g.nslot) continue;
+            const PermSrc &S = g.src[g.slot_src[sl]];
+            const int p = g.slot_perm[sl];
+            const double *base = S.base + o[perm3(p, 0)] * S.st[0] + o[perm3(p, 1)] * S.st[1] + o[perm3(p, 2)] * S.st[2];
+#pragma unroll
+            for (int h = 0; h < 2; h++)
+                if (voff[sl][h] >= 0) cp_async8(buf + sl * SLOT + wr[h], base + voff[sl][h]);
+        }
+    };
+    int64_t q = blockIdx.y;
+    if (q >= nblocks) return;
+    issue(pg_sm, q);
+    cp_async_commit();
+    for (int stage = 0; q < nblocks; q += gridDim.y, stage ^= 1) {
+        const int64_t nq = q + gridDim.y;
+        if (nq < nblocks) {
+            issue(pg_sm + (stage ^ 1) * g.nslot * SLOT, nq);
+            cp_async_commit();
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
+        }
+        __syncthreads();
+        const double *buf = pg_sm + stage * g.nslot * SLOT;
+        double *dst = r3 + q * n3;
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            if (ooff[h] < 0) continue;
+            double acc = 0.0;
+#pragma unroll
+            for (int sl = 0; sl < PG_MAX_SLOTS; sl++)
+                if (sl < g.nslot) acc = fma(g.slot_scale[sl], buf[rd[sl][h]], acc);
+            double *out = dst + ooff[h];
+            *out = (beta == 0.0) ? acc : fma(beta, *out, acc);
+        }
+        __syncthreads();
     }
 }
 
 }  // namespace dcc
 
+extern "C" int dcc_t3_perm_gather(double *r3, const int32_t *ijk, int64_t nblocks, int64_t nvir, double beta,
+                                  int nsrc, const double *const *bases, const double *scales, const int64_t *strides,
+                                  const int *masks, void *stream) {
+    clear_error();
+    DCC_REQUIRE(nblocks >= 0 && nvir >= 0, DCC_ERR_SHAPE, "negative size");
+    DCC_REQUIRE(nsrc >= 1 && nsrc <= PG_MAX_SRC, DCC_ERR_SHAPE, "1..%d sources", PG_MAX_SRC);
+    if (nblocks == 0 || nvir == 0) return DCC_OK;
+    DCC_REQUIRE(r3 && ijk && bases && scales && strides && masks, DCC_ERR_NULL, "NULL argument");
+    PermGatherArgs g{};
+    g.nsrc = nsrc;
+    int nslot = 0;
+    for (int s = 0; s < nsrc; s++) {
+        DCC_REQUIRE(bases[s], DCC_ERR_NULL, "source %d is NULL", s);
+        DCC_REQUIRE(masks[s] > 0 && masks[s] < 64, DCC_ERR_SHAPE, "source %d: permutation mask must be in 1..63", s);
+        g.src[s].base = bases[s];
+        g.src[s].scale = scales[s];
+        for (int m = 0; m < 6; m++) g.src[s].st[m] = strides[6 * s + m];
+        g.src[s].mask = masks[s];
+        for (int p = 0; p < 6; p++)
+            if (masks[s] & (1 << p)) {
+                DCC_REQUIRE(nslot < PG_MAX_SLOTS, DCC_ERR_UNSUPPORTED, "more than %d source tiles", PG_MAX_SLOTS);
+                g.slot_src[nslot] = s;
+                g.slot_perm[nslot] = p;
+                g.slot_scale[nslot] = scales[s];
+                nslot++;
+            }
+    }
+    g.nslot = nslot;
+    for (int s = 0; s < nsrc; s++) {
+        const int64_t vmax = (nvir + 7) / 8 * 8 * (g.src[s].st[3] + g.src[s].st[4] + g.src[s].st[5]);
+        DCC_REQUIRE(g.src[s].st[3] >= 0 && g.src[s].st[4] >= 0 && g.src[s].st[5] >= 0 && vmax < (1ll << 31),
+                    DCC_ERR_UNSUPPORTED, "source %d: virtual strides must be non-negative and span < 2^31", s);
+    }
+    DCC_REQUIRE(nvir <= 1290, DCC_ERR_UNSUPPORTED, "nvir > 1290 exceeds 32-bit block offsets");
+    int ntile = (int)ceil_div(nvir, TE);
+    int64_t nt3 = (int64_t)ntile * ntile * ntile;
+    int64_t gy = (148 * 4 * 8 + nt3 - 1) / nt3;
+    gy = gy < 1 ? 1 : (gy > nblocks ? nblocks : gy);
+    gy = gy > 65535 ? 65535 : gy;
+    size_t smem = (size_t)2 * nslot * SLOT * sizeof(double);
+    cudaFuncSetAttribute(k_perm_gather, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_perm_gather<<<dim3((unsigned)nt3, (unsigned)gy), 256, smem, as_stream(stream)>>>(r3, ijk, nblocks, (int)nvir,
+                                                                                       ntile, beta, g);
+    return launch_status("t3_perm_gather");
+}
+
 extern "C" int dcc_t3_s3_gather(double *r3, const int32_t *ijk, int64_t nblocks, int64_t nvir, double beta,
                                 const double *u0, double scale0, const int64_t *strides0, const double *u1,
                                 double scale1, const int64_t *strides1, void *stream) {
     clear_error();
-    DCC_REQUIRE(nblocks >= 0 && nvir >= 0, DCC_ERR_SHAPE, "negative size");
-    if (nblocks == 0 || nvir == 0) return DCC_OK;
-    DCC_REQUIRE(r3 && ijk && u0 && strides0, DCC_ERR_NULL, "NULL buffer");
-    S3Src s0{u0, scale0, {strides0[0], strides0[1], strides0[2], strides0[3], strides0[4], strides0[5]}};
-    S3Src s1 = s0;
-    int nsrc = 1;
-    if (u1) {
-        DCC_REQUIRE(strides1, DCC_ERR_NULL, "strides1 is NULL");
-        s1 = S3Src{u1, scale1, {strides1[0], strides1[1], strides1[2], strides1[3], strides1[4], strides1[5]}};
-        nsrc = 2;
+    DCC_REQUIRE(u0 && strides0, DCC_ERR_NULL, "first source is NULL");
+    const double *bases[2] = {u0, u1};
+    double scales[2] = {scale0, scale1};
+    int64_t st[12];
+    for (int m = 0; m < 6; m++) {
+        st[m] = strides0[m];
+        st[6 + m] = u1 ? strides1[m] : 0;
     }
-    k_s3_gather<<<row_grid(nblocks * nvir * nvir, 256), 256, 0, as_stream(stream)>>>(r3, ijk, nblocks, (int)nvir,
-                                                                                     beta, s0, s1, nsrc);
-    return launch_status("t3_s3_gather");
+    int masks[2] = {63, 63};
+    if (u1) DCC_REQUIRE(strides1, DCC_ERR_NULL, "strides1 is NULL");
+    return dcc_t3_perm_gather(r3, ijk, nblocks, nvir, beta, u1 ? 2 : 1, bases, scales, st, masks, stream);
 }
 
 // ---------------------------------------------------------------- no-allocation update

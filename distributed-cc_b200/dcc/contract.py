@@ -26,12 +26,30 @@ _split = L.bind("dcc_split_operand", [L.c_vp, L.c_vp, L.c_vp, L.c_i64, L.c_i64, 
 _gemm = L.bind("dcc_gemm_split3", [L.c_vp] * 4 + [L.c_i64] * 3 + [L.c_vp, L.c_vp, L.c_dbl, L.c_dbl, L.c_int,
                                                                    L.c_vp, L.c_vp])
 
-BIG = 1 << 30  # divisor that makes a level of the two-level map a plain stride (< 2^31)
+BIG = 1 << 30  # radix that makes a digit of a map a plain stride (< 2^31)
 
 
-def _i64x6(v):
-    a = (ctypes.c_int64 * 6)(*[int(x) for x in v])
-    return a
+def lin(s):
+    """m -> m * s."""
+    return (1, BIG, 0, 0, s)
+
+
+def two(d, s1, s2):
+    """m -> (m / d) * s1 + (m % d) * s2."""
+    return (1, d, s1, 0, s2)
+
+
+def three(R1, R2, S0, S1, S2):
+    """m -> (m / (R1 R2)) * S0 + ((m / R2) % R1) * S1 + (m % R2) * S2."""
+    return (R1, R2, S0, S1, S2)
+
+
+def _i64x10(f, g):
+    """Two three-digit maps as the HOST int64[10] the C ABI takes."""
+    v = tuple(f) + tuple(g)
+    if len(v) != 10:
+        raise ValueError("a map pair needs 2 x 5 values")
+    return (ctypes.c_int64 * 10)(*[int(x) for x in v])
 
 
 def padded_k(K, kind):
@@ -52,22 +70,22 @@ class Split:
         else:
             self.hi, self.lo = buffers
 
-    def fill(self, src, map6):
-        """dst[m][k] = src[(m/d0)*s1 + (m%d0)*s2 + (k/d1)*s3 + (k%d1)*s4]."""
+    def fill(self, src, fm, fk):
+        """dst[m][k] = src[fm(m) + fk(k)] for three-digit maps fm, fk."""
         L.as_tensor(src, f64, "src")
-        L.check(_split(L.ptr(src), L.ptr(self.hi), L.ptr(self.lo), self.M, self.K, self.Kp, _i64x6(map6), self.kind,
-                       L.stream_ptr()))
+        L.check(_split(L.ptr(src), L.ptr(self.hi), L.ptr(self.lo), self.M, self.K, self.Kp, _i64x10(fm, fk),
+                       self.kind, L.stream_ptr()))
         return self
 
 
-def gemm_(A, B, C, epi6, alpha=1.0, beta=1.0, status=None):
-    """C[row_off(m) + col_off(n)] = alpha * A B^T + beta * C (A: Split [M,K], B: Split [N,K])."""
+def gemm_(A, B, C, frow, fcol, alpha=1.0, beta=1.0, status=None):
+    """C[frow(m) + fcol(n)] = alpha * A B^T + beta * C (A: Split [M,K], B: Split [N,K])."""
     if A.kind != B.kind or A.Kp != B.Kp:
         raise ValueError("A and B must be split with the same kind and padded K")
     L.as_tensor(C, f64, "C")
     if status is None:
         status = torch.zeros(1, dtype=torch.int32, device=C.device)
-    L.check(_gemm(L.ptr(A.hi), L.ptr(A.lo), L.ptr(B.hi), L.ptr(B.lo), A.M, B.M, A.Kp, L.ptr(C), _i64x6(epi6),
+    L.check(_gemm(L.ptr(A.hi), L.ptr(A.lo), L.ptr(B.hi), L.ptr(B.lo), A.M, B.M, A.Kp, L.ptr(C), _i64x10(frow, fcol),
                   float(alpha), float(beta), A.kind, L.ptr(status), L.stream_ptr()))
     return status
 
@@ -77,10 +95,10 @@ def matmul_split3(A, B, kind="bf16x3"):
     k = KIND[kind]
     M, K = A.shape
     N = B.shape[0]
-    a = Split(M, K, k).fill(A.contiguous(), (BIG, 0, K, BIG, 0, 1))
-    b = Split(N, K, k).fill(B.contiguous(), (BIG, 0, K, BIG, 0, 1))
+    a = Split(M, K, k).fill(A.contiguous(), lin(K), lin(1))
+    b = Split(N, K, k).fill(B.contiguous(), lin(K), lin(1))
     C = torch.zeros((M, N), dtype=f64, device=A.device)
-    st = gemm_(a, b, C, (BIG, 0, N, BIG, 0, 1), 1.0, 0.0)
+    st = gemm_(a, b, C, lin(N), lin(1), 1.0, 0.0)
     return C, st
 
 
@@ -92,15 +110,16 @@ def matmul_split3(A, B, kind="bf16x3"):
 # ----------------------------------------------------------------------------
 
 def wvvvv_maps(nv):
-    """(A split map, epilogue map) of the three einsum strings for blocks of nv^3."""
+    """(A row map, A k map, out row map, out col map) of the three einsum strings
+    for blocks of nv^3 (A rows and out rows run over (q, free index))."""
     n2, n3 = nv * nv, nv ** 3
     return [
         # 'abde,dec->abc': rows (q,c), K (d,e): t3[q][d][e][c]; out r3[q][a][b][c] = (q,c) x (a,b)
-        ((nv, n3, 1, BIG, 0, nv), (nv, n3, 1, BIG, 0, nv)),
+        (two(nv, n3, 1), lin(nv), two(nv, n3, 1), lin(nv)),
         # 'acde,dbe->abc': rows (q,b), K (d,e): t3[q][d][b][e]; out (q,b) x (a,c)
-        ((nv, n3, nv, nv, n2, 1), (nv, n3, nv, nv, n2, 1)),
+        (two(nv, n3, nv), two(nv, n2, 1), two(nv, n3, nv), two(nv, n2, 1)),
         # 'bcde,ade->abc': rows (q,a), K (d,e): t3[q][a][d][e]; out (q,a) x (b,c)
-        ((BIG, 0, n2, BIG, 0, 1), (nv, n3, n2, BIG, 0, 1)),
+        (lin(n2), lin(1), two(nv, n3, n2), lin(1)),
     ]
 
 
@@ -119,10 +138,10 @@ class WvvvvT3:
         nv = self.nv
         L.as_tensor(r3, f64, "r3")
         L.as_tensor(t3, f64, "t3")
-        self.W.fill(W.reshape(nv * nv, nv * nv), (BIG, 0, nv * nv, BIG, 0, 1))
-        for amap, emap in self.maps:
-            self.A.fill(t3, amap)
-            gemm_(self.A, self.W, r3, emap, alpha, 1.0, self.status)
+        self.W.fill(W.reshape(nv * nv, nv * nv), lin(nv * nv), lin(1))
+        for am, ak, er, ec in self.maps:
+            self.A.fill(t3, am, ak)
+            gemm_(self.A, self.W, r3, er, ec, alpha, 1.0, self.status)
         return r3
 
 

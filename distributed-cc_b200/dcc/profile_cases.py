@@ -4,6 +4,7 @@
     python -m dcc.profile_cases p3     [--reps 3]
     python -m dcc.profile_cases update [--reps 3]
     python -m dcc.profile_cases q      [--reps 3]
+    python -m dcc.profile_cases gather [--reps 3]
 
 Each case builds its inputs once and launches the kernel `reps` times, so a
 profiler can skip the warm-up launches and capture the last one.  Sizes are
@@ -28,11 +29,11 @@ def case_gemm(kind, reps):
     W = torch.randn(nv, nv, nv, nv, dtype=torch.float64, device="cuda", generator=g) * 0.1
     r3 = torch.zeros_like(t3)
     op = contract.WvvvvT3(n3, nv, kind)
-    op.W.fill(W.reshape(nv * nv, nv * nv), (contract.BIG, 0, nv * nv, contract.BIG, 0, 1))
-    amap, emap = op.maps[2]
-    op.A.fill(t3, amap)
+    op.W.fill(W.reshape(nv * nv, nv * nv), contract.lin(nv * nv), contract.lin(1))
+    am, ak, er, ec = op.maps[2]
+    op.A.fill(t3, am, ak)
     for _ in range(reps):
-        contract.gemm_(op.A, op.W, r3, emap, 1.0, 1.0, op.status)
+        contract.gemm_(op.A, op.W, r3, er, ec, 1.0, 1.0, op.status)
     torch.cuda.synchronize()
     assert int(op.status.item()) == 0
 
@@ -70,9 +71,20 @@ def case_q(reps):
     torch.cuda.synchronize()
 
 
+def case_gather(reps):
+    from dcc import synthetic, t3_residual
+    d = synthetic.make_inputs(10, 90, seed=0)
+    tr = t3_residual.T3Residual(10, 90, "fp64")
+    r3 = torch.empty_like(d.t3)
+    tr.vt2_(r3, d)
+    for _ in range(reps):
+        t3_residual.s3_gather_(r3, d.ijk, 90, 0.0, tr.X, 1.0, tr.x_strides, tr.Y, -1.0, tr.y_strides)
+    torch.cuda.synchronize()
+
+
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("case", choices=["gemm", "p3", "update", "q"])
+    ap.add_argument("case", choices=["gemm", "p3", "update", "q", "gather"])
     ap.add_argument("--kind", default="bf16x3")
     ap.add_argument("--reps", type=int, default=3)
     a = ap.parse_args()
@@ -82,6 +94,8 @@ def main():
         case_p3(a.reps)
     elif a.case == "update":
         case_update(a.reps)
+    elif a.case == "gather":
+        case_gather(a.reps)
     else:
         case_q(a.reps)
     print("ok")

@@ -154,6 +154,16 @@ DCC_API int dcc_t3_s3_gather(double *r3, const int32_t *ijk, int64_t nblocks, in
                              const double *u0, double scale0, const int64_t *strides0, const double *u1,
                              double scale1, const int64_t *strides1, void *stream);
 
+/* General form: r3[q][abc] = beta*r3 + sum_s scales[s] * sum_{p in masks[s]} U_s(p(ijk), p(abc))
+ * for nsrc <= 4 sources (HOST arrays: bases[s], scales[s], strides[6*s..6*s+5],
+ * masks[s] = 6-bit subset of the simultaneous permutations in the order
+ * (x,y,z), (x,z,y), (y,x,z), (y,z,x), (z,x,y), (z,y,x)); at most 12 (source,
+ * permutation) pairs.  Used for the W.t2 terms and the OO batch terms of
+ * compute_r3_tri (distr_cc/rccsdt.py:385-396, 435-732). */
+DCC_API int dcc_t3_perm_gather(double *r3, const int32_t *ijk, int64_t nblocks, int64_t nvir, double beta, int nsrc,
+                               const double *const *bases, const double *scales, const int64_t *strides,
+                               const int *masks, void *stream);
+
 /* ----------------------------------------------------------------------
  * T4 helpers (replace src/rccsdtq.c and PySCF libccsdt.t4_add_)
  * ---------------------------------------------------------------------- */
@@ -234,26 +244,35 @@ DCC_API int dcc_q_task_epilogue(const double *t4, const double *z4, const double
  * Split-precision tensor-core contractions (the dense T3/T4 residual terms)
  * ---------------------------------------------------------------------- */
 
-/* Split an FP64 operand into two K-major pieces, x = hi + lo:
- *   dst[m][k] (m < M, k < Kp; k >= K zero-filled) from
- *   src[(m/d0)*s1 + (m%d0)*s2 + (k/d1)*s3 + (k%d1)*s4], map6 = {d0,s1,s2,d1,s3,s4}
- * (HOST array).  kind 0: bf16 pieces (Kp multiple of 64), kind 1: tf32
- * pieces stored as float (Kp multiple of 32).  Replaces the FP64 operand of
- * the _einsum calls of distr_cc/rccsdt.py:385-427 (PySCF _einsum backend). */
-DCC_API int dcc_split_operand(const double *src, void *hi, void *lo, int64_t M, int64_t K, int64_t Kp,
-                              const int64_t *map6, int kind, void *stream);
+/* Index maps below are three-digit mixed radix, f = {R1, R2, S0, S1, S2}:
+ *   f(m) = (m / (R1*R2))*S0 + ((m / R2) % R1)*S1 + (m % R2)*S2   (R1, R2 >= 1).
+ * A plain stride s is {1, 2^30, 0, 0, s}. */
 
-/* C[row_off(m) + col_off(n)] = alpha * (A_hi B_hi + A_hi B_lo + A_lo B_hi)[m][n]
+/* Split an FP64 operand into two K-major pieces, x = hi + lo:
+ *   dst[m][k] (m < M, k < Kp; k >= K zero-filled) from src[fm(m) + fk(k)],
+ * map10 = {fm, fk} (HOST array).  kind 0: bf16 pieces (Kp multiple of 64),
+ * kind 1: tf32 pieces stored as float (Kp multiple of 32).  Replaces the FP64
+ * operand of the _einsum calls of distr_cc/rccsdt.py:385-427 (PySCF _einsum
+ * backend). */
+DCC_API int dcc_split_operand(const double *src, void *hi, void *lo, int64_t M, int64_t K, int64_t Kp,
+                              const int64_t *map10, int kind, void *stream);
+
+/* C[frow(m) + fcol(n)] = alpha * (A_hi B_hi + A_hi B_lo + A_lo B_hi)[m][n]
  * + beta * C, FP32 accumulation in tensor memory (tcgen05), FP64 C.  A is
- * [M][Kp], B is [N][Kp] (pieces from dcc_split_operand).  epi6 = {rdiv, rs1,
- * rs2, cdiv, cs1, cs2} (HOST): row_off(m) = (m/rdiv)*rs1 + (m%rdiv)*rs2,
- * col_off(n) = (n/cdiv)*cs1 + (n%cdiv)*cs2.  *status (DEVICE int, zero before
- * the call) becomes DCC_ERR_TIMEOUT if a bounded wait gave up.  Replaces the
- * out=..., alpha, beta semantics of the _einsum calls at distr_cc/rccsdt.py:421-427
- * ("abde,dec->abc", "acde,dbe->abc", "bcde,ade->abc"). */
+ * [M][Kp], B is [N][Kp] (pieces from dcc_split_operand), epi10 = {frow, fcol}
+ * (HOST).  *status (DEVICE int, zero before the call) becomes
+ * DCC_ERR_TIMEOUT if a bounded wait gave up.  Replaces the out=..., alpha,
+ * beta semantics of the _einsum calls at distr_cc/rccsdt.py:385-427. */
 DCC_API int dcc_gemm_split3(const void *A_hi, const void *A_lo, const void *B_hi, const void *B_lo, int64_t M,
-                            int64_t N, int64_t Kp, double *C, const int64_t *epi6, double alpha, double beta,
+                            int64_t N, int64_t Kp, double *C, const int64_t *epi10, double alpha, double beta,
                             int kind, int *status, void *stream);
+
+/* Pipeline shape of dcc_gemm_split3 (process-wide): bytes of K per k-block
+ * (128, 64 or 32 -> matching TMA/UMMA swizzle), ring depth (2 | 3,4 | 8) and
+ * the raster group height in M-tiles.  Set by the tile autotuner
+ * (dcc.autotune) for each problem shape; no reference counterpart. */
+DCC_API int dcc_gemm_set_config(int kb_bytes, int stages, int group_m);
+DCC_API int dcc_gemm_get_config(int *kb_bytes, int *stages, int *group_m);
 
 #ifdef __cplusplus
 }

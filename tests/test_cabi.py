@@ -92,30 +92,33 @@ def test_split_gemm_host_validation_accepts_our_maps(L):
     without a GPU a valid call gets as far as the launch (DCC_ERR_CUDA), an
     invalid one stops at DCC_ERR_SHAPE."""
     import torch
-    from dcc import contract
+    from dcc import contract as c
     if torch.cuda.is_available():
         pytest.skip("checks the no-device fall-through")
     fake = ctypes.c_void_p(4096)
-    nv, n = 90, 220
-    for amap, emap in contract.wvvvv_maps(nv):
-        rc = contract._split(fake, fake, fake, n * nv, nv * nv, contract.padded_k(nv * nv, 0),
-                             contract._i64x6(amap), 0, None)
+    nv, n, no = 90, 220, 10
+    N = no * no * nv
+    splits = [(n * nv, nv * nv, am, ak) for am, ak, _, _ in c.wvvvv_maps(nv)]
+    splits += [(no * nv * nv, nv, c.two(nv * nv, 1, nv * no), c.lin(no)), (no * no * nv, nv, c.two(nv, nv * nv, 1), c.lin(nv)),
+               (no * no * nv, no, c.three(no, nv, no, 1, no ** 3), c.lin(no * no)), (no * nv * nv, no, c.lin(1), c.lin(no * nv * nv))]
+    for M, K, fm, fk in splits:
+        rc = c._split(fake, fake, fake, M, K, c.padded_k(K, 0), c._i64x10(fm, fk), 0, None)
         assert rc == 4, L.last_error()
-        rc = contract._gemm(fake, fake, fake, fake, n * nv, nv * nv, contract.padded_k(nv * nv, 0), fake,
-                            contract._i64x6(emap), 1.0, 1.0, 0, fake, None)
+    epis = [(n * nv, nv * nv, er, ec) for _, _, er, ec in c.wvvvv_maps(nv)]
+    epis += [(no * nv * nv, N, c.lin(N), c.lin(1)),
+             (no * no * nv, no * nv * nv, c.three(no, nv, no * nv, nv * nv * N, nv * N), c.three(nv, nv, nv, N, 1))]
+    for M, Nn, fr, fc in epis:
+        rc = c._gemm(fake, fake, fake, fake, M, Nn, 128, fake, c._i64x10(fr, fc), 1.0, 1.0, 0, fake, None)
         assert rc == 4, L.last_error()
-    rc = contract._gemm(fake, fake, fake, fake, 10, 10, 100, fake, contract._i64x6((1, 0, 1, 1, 0, 1)), 1.0, 0.0, 0,
-                        fake, None)
+    rc = c._gemm(fake, fake, fake, fake, 10, 10, 100, fake, c._i64x10(c.lin(10), c.lin(1)), 1.0, 0.0, 0, fake, None)
     assert rc == 2  # Kp not a multiple of 64
+    rc = c._split(fake, fake, fake, 10, 10, 64, c._i64x10((0, 1, 0, 0, 1), c.lin(1)), 0, None)
+    assert rc == 2  # radix 0
 
 
-def test_residual_split_maps_clear_host_checks(L):
-    import torch
-    from dcc import contract
-    if torch.cuda.is_available():
-        pytest.skip("checks the no-device fall-through")
-    fake = ctypes.c_void_p(4096)
-    no, nv, B = 10, 90, contract.BIG
-    for M, K, m6 in [(no * nv * nv, nv, (nv * nv, 1, nv * no, B, 0, no)), (no * no * nv, nv, (nv, nv * nv, 1, B, 0, nv))]:
-        rc = contract._split(fake, fake, fake, M, K, contract.padded_k(K, 0), contract._i64x6(m6), 0, None)
-        assert rc == 4, L.last_error()
+def test_three_digit_map_helpers():
+    from dcc import contract as c
+    f = lambda m, R1, R2, S0, S1, S2: (m // (R1 * R2)) * S0 + ((m // R2) % R1) * S1 + (m % R2) * S2  # noqa: E731
+    for m in [0, 1, 7, 89, 90, 8099, 8100, 19799]:
+        assert f(m, *c.lin(3)) == 3 * m
+        assert f(m, *c.two(90, 1000, 7)) == (m // 90) * 1000 + (m % 90) * 7

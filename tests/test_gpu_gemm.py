@@ -55,3 +55,21 @@ def test_wvvvv_t3_matches_einsum(C, kind, nblk, nv):
     r64 = torch.from_numpy(r0.copy()).cuda()
     C.wvvvv_t3_fp64_(r64, dW, dt3)
     np.testing.assert_allclose(r64.cpu().numpy(), want, rtol=1e-12, atol=1e-15)
+
+
+@pytest.mark.parametrize("cfg", [(128, 2, 16), (64, 4, 16), (64, 3, 8), (32, 8, 32), (64, 4, 1)])
+@pytest.mark.parametrize("kind", ["bf16x3", "tf32x3"])
+def test_every_pipeline_shape(C, cfg, kind):
+    from dcc import autotune
+    old = autotune.get_config()
+    try:
+        autotune.set_config(*cfg)
+        g = torch.Generator(device="cuda").manual_seed(sum(cfg))
+        A = torch.randn(700, 300, dtype=torch.float64, device="cuda", generator=g)
+        B = torch.randn(600, 300, dtype=torch.float64, device="cuda", generator=g)
+        got, st = C.matmul_split3(A, B, kind)
+        torch.cuda.synchronize()
+        assert int(st.item()) == 0
+        assert _rel(got, A @ B.t()) < TOL[kind]
+    finally:
+        autotune.set_config(*old)

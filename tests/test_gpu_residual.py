@@ -20,20 +20,20 @@ def mods():
     return synthetic, t3_residual, einsum_ref
 
 
-def _ref_r3(er, dn):
+def _ref_r3(er, dn, with_oo=True):
     imds = er.Imds(dn.F_vv, dn.F_oo, dn.W_vvvo, dn.W_vooo, dn.W_vvvv, dn.W_ovov, dn.W_ovvo, dn.W_oooo)
-    r3 = er.vt2_ref(imds, dn.t2, dn.t3, dn.nocc)
-    return er.wvvvv_ref(imds, dn.t3, r3)
+    return er.compute_r3_tri_ref(imds, dn.t2, dn.t3, dn.nocc, with_oo=with_oo)
 
 
 @pytest.mark.parametrize("nocc,nvir", [(2, 5), (3, 7), (4, 10)])
 @pytest.mark.parametrize("precision", ["fp64", "bf16x3", "tf32x3"])
-def test_residual(mods, nocc, nvir, precision):
+@pytest.mark.parametrize("with_oo", [False, True])
+def test_residual(mods, nocc, nvir, precision, with_oo):
     syn, tr, er = mods
     d = syn.make_inputs(nocc, nvir, seed=nocc * 100 + nvir)
     dn = syn.to_numpy(d)
-    want = _ref_r3(er, dn)
-    res = tr.T3Residual(nocc, nvir, precision)
+    want = _ref_r3(er, dn, with_oo)
+    res = tr.T3Residual(nocc, nvir, precision, with_oo=with_oo)
     got = res.compute(d, d.t3).cpu().numpy()
     assert res.status_ok()
     if precision == "fp64":
