@@ -175,55 +175,66 @@ template <int ST>
 struct GemmSmem {
     uint64_t full[ST];
     uint64_t empty[ST];
-    uint64_t acc_full;
+    uint64_t acc_full[2];   // accumulator b holds a finished tile
+    uint64_t acc_empty[2];  // accumulator b has been read out by every epilogue warp
+    uint64_t drain;         // all MMAs of this CTA retired (end of kernel)
     uint32_t tmem_base;
-    int64_t col_off[GN];
 };
 
+constexpr int EPI_WARPS = 4;
+// per epilogue warp: a 32x33 float transpose buffer and 32 row (or column) offsets
+constexpr uint32_t EPI_WARP_BYTES = 32 * 33 * 4 + 32 * 8;
+
+__device__ __forceinline__ void tile_coords(int t, int num_m, int num_n, int group_m, int &tm, int &tn) {
+    const int per_group = group_m * num_n;
+    const int first_m = (t / per_group) * group_m;
+    const int gsz = (num_m - first_m) < group_m ? (num_m - first_m) : group_m;
+    tm = first_m + (t % per_group) % gsz;
+    tn = (t % per_group) / gsz;
+}
+
+// Persistent: CTA c takes tiles c, c + gridDim.x, ... (linear ids rasterized
+// in groups of group_m M-tiles).  Two TMEM accumulators of GN columns let the
+// MMAs of tile t+1 run while the epilogue warps drain tile t.
 // KIND 0: bf16 pieces; KIND 1: tf32 pieces.  KB: bytes of K per row and
-// k-block; ST: ring depth.  blockIdx.x is a linear tile id, rasterized in
-// groups of group_m M-tiles.
+// k-block; ST: ring depth.
 template <int KIND, int KB, int ST>
 __global__ void __launch_bounds__(G_THREADS, 1)
     k_gemm_split3(const __grid_constant__ CUtensorMap tmAh, const __grid_constant__ CUtensorMap tmAl,
                   const __grid_constant__ CUtensorMap tmBh, const __grid_constant__ CUtensorMap tmBl, int M, int N,
-                  int nkb, double *C, GemmEpi epi, double alpha, double beta, int *status, int group_m) {
+                  int nkb, double *C, GemmEpi epi, double alpha, double beta, int *status, int group_m,
+                  int epi_cols) {
     extern __shared__ __align__(1024) uint8_t g_smem[];
-    // operand stages first (1024-byte aligned), then the control block
+    // operand stages first (1024-byte aligned), then the epilogue buffers and the control block
     uint8_t *base = (uint8_t *)(((uintptr_t)g_smem + 1023) & ~(uintptr_t)1023);
     constexpr uint32_t A_BYTES = GM * KB, B_BYTES = GN * KB;
     constexpr uint32_t STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;
-    GemmSmem<ST> *cs = (GemmSmem<ST> *)(base + ST * STAGE_BYTES);
+    uint8_t *epi_base = base + ST * STAGE_BYTES;
+    GemmSmem<ST> *cs = (GemmSmem<ST> *)(epi_base + EPI_WARPS * EPI_WARP_BYTES);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    int tile_m, tile_n;
-    {
-        const int num_m = (M + GM - 1) / GM, num_n = (N + GN - 1) / GN;
-        const int pid = blockIdx.x, per_group = group_m * num_n;
-        const int first_m = (pid / per_group) * group_m;
-        const int gsz = (num_m - first_m) < group_m ? (num_m - first_m) : group_m;
-        tile_m = first_m + (pid % per_group) % gsz;
-        tile_n = (pid % per_group) / gsz;
-    }
-    const int n0 = tile_n * GN, m0 = tile_m * GM;
+    const int num_m = (M + GM - 1) / GM, num_n = (N + GN - 1) / GN, ntiles = num_m * num_n;
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < ST; s++) {
             mbar_init(smem_u32(&cs->full[s]), 1);
             mbar_init(smem_u32(&cs->empty[s]), 1);
         }
-        mbar_init(smem_u32(&cs->acc_full), 1);
+        for (int b = 0; b < 2; b++) {
+            mbar_init(smem_u32(&cs->acc_full[b]), 1);
+            mbar_init(smem_u32(&cs->acc_empty[b]), EPI_WARPS);
+        }
+        mbar_init(smem_u32(&cs->drain), 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         tma_prefetch_desc(&tmAh);
         tma_prefetch_desc(&tmAl);
         tma_prefetch_desc(&tmBh);
         tma_prefetch_desc(&tmBl);
     }
-    for (int j = threadIdx.x; j < GN; j += G_THREADS) cs->col_off[j] = map3(epi.col, (int64_t)n0 + j);
     if (warp == 1) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
                          smem_u32(&cs->tmem_base)),
-                     "r"(GN)
+                     "r"(2 * GN)
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
@@ -234,26 +245,32 @@ __global__ void __launch_bounds__(G_THREADS, 1)
 
     if (warp == 0 && lane == 0) {
         // ---------------- TMA producer
-        int issued = 0;
-        for (int kb = 0; kb < nkb; kb++) {
-            const int s = kb % ST;
-            const uint32_t ph = (uint32_t)(kb / ST) & 1u;
-            if (!mbar_wait(smem_u32(&cs->empty[s]), ph ^ 1u, status)) break;
-            uint8_t *st = base + s * STAGE_BYTES;
-            const uint32_t fb = smem_u32(&cs->full[s]);
-            mbar_expect_tx(fb, STAGE_BYTES);
-            const int kc = kb * (KB / (KIND == 0 ? 2 : 4));
-            tma_load_2d(smem_u32(st), &tmAh, fb, kc, m0);
-            tma_load_2d(smem_u32(st + A_BYTES), &tmAl, fb, kc, m0);
-            tma_load_2d(smem_u32(st + 2 * A_BYTES), &tmBh, fb, kc, n0);
-            tma_load_2d(smem_u32(st + 2 * A_BYTES + B_BYTES), &tmBl, fb, kc, n0);
-            issued = kb + 1;
+        uint32_t g = 0;  // k-blocks issued by this CTA
+        bool ok = true;
+        for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
+            int tm, tn;
+            tile_coords(t, num_m, num_n, group_m, tm, tn);
+            for (int kb = 0; kb < nkb; kb++) {
+                const uint32_t s = g % ST, ph = (g / ST) & 1u;
+                if (!mbar_wait(smem_u32(&cs->empty[s]), ph ^ 1u, status)) {
+                    ok = false;
+                    break;
+                }
+                uint8_t *st = base + s * STAGE_BYTES;
+                const uint32_t fb = smem_u32(&cs->full[s]);
+                mbar_expect_tx(fb, STAGE_BYTES);
+                const int kc = kb * (KB / (KIND == 0 ? 2 : 4));
+                tma_load_2d(smem_u32(st), &tmAh, fb, kc, tm * GM);
+                tma_load_2d(smem_u32(st + A_BYTES), &tmAl, fb, kc, tm * GM);
+                tma_load_2d(smem_u32(st + 2 * A_BYTES), &tmBh, fb, kc, tn * GN);
+                tma_load_2d(smem_u32(st + 2 * A_BYTES + B_BYTES), &tmBl, fb, kc, tn * GN);
+                g++;
+            }
         }
         // on an early exit, wait (bounded) for the copies still landing in shared memory
-        if (*(volatile int *)status != 0) {
-            int first = issued - ST < 0 ? 0 : issued - ST;
-            for (int kb = first; kb < issued; kb++)
-                mbar_wait_quiet(smem_u32(&cs->full[kb % ST]), (uint32_t)(kb / ST) & 1u);
+        if (!ok) {
+            const uint32_t first = g > (uint32_t)ST ? g - ST : 0u;
+            for (uint32_t k = first; k < g; k++) mbar_wait_quiet(smem_u32(&cs->full[k % ST]), (k / ST) & 1u);
         }
     } else if (warp == 1 && lane == 0) {
         // ---------------- MMA issuer
@@ -263,55 +280,122 @@ __global__ void __launch_bounds__(G_THREADS, 1)
                                    | ((uint32_t)(GN >> 3) << 17)      // N
                                    | ((uint32_t)(GM >> 4) << 24);     // M
         constexpr int KSTEPS = KB / 32;  // one UMMA consumes 32 bytes of K
-        for (int kb = 0; kb < nkb; kb++) {
-            const int s = kb % ST;
-            const uint32_t ph = (uint32_t)(kb / ST) & 1u;
-            if (!mbar_wait(smem_u32(&cs->full[s]), ph, status)) break;
+        uint32_t g = 0;
+        bool ok = true;
+        int it = 0;
+        for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x, it++) {
+            const int b = it & 1;
+            if (!mbar_wait(smem_u32(&cs->acc_empty[b]), (((uint32_t)it >> 1) & 1u) ^ 1u, status)) break;
             tc_fence_after();
-            const uint32_t st = smem_u32(base + s * STAGE_BYTES);
-            const uint64_t ah = swz_desc<KB>(st), al = swz_desc<KB>(st + A_BYTES),
-                           bh = swz_desc<KB>(st + 2 * A_BYTES), bl = swz_desc<KB>(st + 2 * A_BYTES + B_BYTES);
+            const uint32_t d = tmem + (uint32_t)(b * GN);
+            for (int kb = 0; kb < nkb; kb++) {
+                const uint32_t s = g % ST, ph = (g / ST) & 1u;
+                if (!mbar_wait(smem_u32(&cs->full[s]), ph, status)) {
+                    ok = false;
+                    break;
+                }
+                tc_fence_after();
+                const uint32_t st = smem_u32(base + s * STAGE_BYTES);
+                const uint64_t ah = swz_desc<KB>(st), al = swz_desc<KB>(st + A_BYTES),
+                               bh = swz_desc<KB>(st + 2 * A_BYTES), bl = swz_desc<KB>(st + 2 * A_BYTES + B_BYTES);
 #pragma unroll
-            for (int k = 0; k < KSTEPS; k++) {
-                const uint64_t dk = (uint64_t)(k * 32) >> 4;  // advance 32 bytes along K
-                const uint32_t first = (kb | k) != 0;
-                umma<KIND>(tmem, ah + dk, bh + dk, idesc, first);
-                umma<KIND>(tmem, ah + dk, bl + dk, idesc, 1u);
-                umma<KIND>(tmem, al + dk, bh + dk, idesc, 1u);
+                for (int k = 0; k < KSTEPS; k++) {
+                    const uint64_t dk = (uint64_t)(k * 32) >> 4;  // advance 32 bytes along K
+                    const uint32_t first = (kb | k) != 0;
+                    umma<KIND>(d, ah + dk, bh + dk, idesc, first);
+                    umma<KIND>(d, ah + dk, bl + dk, idesc, 1u);
+                    umma<KIND>(d, al + dk, bh + dk, idesc, 1u);
+                }
+                umma_commit(smem_u32(&cs->empty[s]));  // stage free once these MMAs retire
+                g++;
             }
-            umma_commit(smem_u32(&cs->empty[s]));  // stage free once these MMAs retire
+            if (ok) umma_commit(smem_u32(&cs->acc_full[b]));  // tile complete
         }
-        umma_commit(smem_u32(&cs->acc_full));  // accumulator complete (or drained after an abort)
+        // every MMA issued above retires before TMEM is released
+        umma_commit(smem_u32(&cs->drain));
+        mbar_wait_quiet(smem_u32(&cs->drain), 0u);
     } else if (warp >= 2) {
         // ---------------- epilogue: TMEM -> FP64 C
         const int q = warp & 3;  // TMEM lane quarter of this warp
-        bool ok = mbar_wait(smem_u32(&cs->acc_full), 0u, status);
-        ok = __all_sync(0xffffffffu, ok && *(volatile int *)status == 0);  // tcgen05.ld is warp-collective
-        tc_fence_after();
-        const int m = m0 + q * 32 + lane;
-        if (ok) {
+        float *stg = reinterpret_cast<float *>(epi_base + (warp - 2) * EPI_WARP_BYTES);
+        int64_t *offs = reinterpret_cast<int64_t *>(epi_base + (warp - 2) * EPI_WARP_BYTES + 32 * 33 * 4);
+        int it = 0;
+        for (int t = blockIdx.x; t < ntiles; t += gridDim.x, it++) {
+            const int b = it & 1;
+            bool ok = mbar_wait(smem_u32(&cs->acc_full[b]), ((uint32_t)it >> 1) & 1u, status);
+            ok = __all_sync(0xffffffffu, ok && *(volatile int *)status == 0);  // tcgen05.ld is warp-collective
+            if (!ok) break;
+            tc_fence_after();
+            int tm, tn;
+            tile_coords(t, num_m, num_n, group_m, tm, tn);
+            const int m0 = tm * GM + q * 32, n0 = tn * GN;  // first row of this warp, first column of the tile
+            const int m = m0 + lane;
             const int64_t roff = map3(epi.row, (int64_t)m);
+            if (epi_cols) offs[lane] = roff;
             for (int c = 0; c < GN; c += 32) {
                 float v[32];
-                tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)c, v);
-                if (m < M) {
+                tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * GN + c), v);
+                if (c == GN - 32) {
+                    // the accumulator is in registers: hand it back to the MMA warp
+                    tc_fence_before();
+                    __syncwarp();
+                    if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(
+                                                    smem_u32(&cs->acc_empty[b]))
+                                                : "memory");
+                }
+                const int col = n0 + c + lane;
+                const bool cval = col < N;
+                const int64_t coff = map3(epi.col, (int64_t)(cval ? col : 0));
+                if (epi_cols) {
+                    // lanes walk the 32 columns of one row at a time (columns contiguous in C)
 #pragma unroll
-                    for (int j = 0; j < 32; j++) {
-                        if (n0 + c + j < N) {
-                            double *p = C + roff + cs->col_off[c + j];
-                            double x = alpha * (double)v[j];
-                            *p = (beta == 0.0) ? x : fma(beta, *p, x);
+                    for (int j = 0; j < 32; j++) stg[lane * 33 + j] = v[j];
+                    __syncwarp();
+                    const int nrow = (M - m0) < 32 ? (M - m0) : 32;
+                    if (beta == 0.0) {
+#pragma unroll 8
+                        for (int r = 0; r < 32; r++)
+                            if (cval && r < nrow) C[offs[r] + coff] = alpha * (double)stg[r * 33 + lane];
+                    } else {
+                        double old[32];
+#pragma unroll
+                        for (int r = 0; r < 32; r++)
+                            old[r] = (cval && r < nrow) ? __ldcg(C + offs[r] + coff) : 0.0;
+#pragma unroll
+                        for (int r = 0; r < 32; r++)
+                            if (cval && r < nrow) C[offs[r] + coff] = fma(beta, old[r], alpha * (double)stg[r * 33 + lane]);
+                    }
+                    __syncwarp();
+                } else {
+                    // lanes are rows (rows contiguous in C): each thread writes its row's 32 columns
+                    offs[lane] = coff;
+                    __syncwarp();
+                    const int nvalid = (N - n0 - c) < 32 ? (N - n0 - c) : 32;
+                    if (m < M) {
+                        if (beta == 0.0) {
+#pragma unroll
+                            for (int j = 0; j < 32; j++)
+                                if (j < nvalid) C[roff + offs[j]] = alpha * (double)v[j];
+                        } else {
+                            double old[32];
+#pragma unroll
+                            for (int j = 0; j < 32; j++) old[j] = (j < nvalid) ? __ldcg(C + roff + offs[j]) : 0.0;
+#pragma unroll
+                            for (int j = 0; j < 32; j++)
+                                if (j < nvalid) C[roff + offs[j]] = fma(beta, old[j], alpha * (double)v[j]);
                         }
                     }
+                    __syncwarp();
                 }
             }
+            __syncwarp();
         }
     }
     tc_fence_before();
     __syncthreads();
     if (warp == 1) {
         tc_fence_after();
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(GN) : "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * GN) : "memory");
     }
 }
 
@@ -337,51 +421,99 @@ __device__ __forceinline__ void split_tf32(double x, float &hi, float &lo) {
 }
 
 // Generic split of a strided FP64 operand into K-major pieces:
-//   dst[m][k] for m < M, k < Kp (k >= K zero-filled) from src[mmap(m) + kmap(k)]
-// with three-digit mixed-radix maps.  32x32 tiles through shared memory so
-// both sides are coalesced whichever index is contiguous in the source.
+//   dst[m][k0 + k] for m < M, k < kw (k >= K zero-filled) from src[mmap(m) + kmap(k)]
+// with three-digit mixed-radix maps; dst rows are ld elements apart, so a
+// K-concatenated operand is filled piece by piece.  A CTA moves a 32-row x
+// 64-k tile through shared memory: reads run along whichever index is
+// contiguous in the source (mode 0: k; mode 1: m; mode 2: the middle digit of
+// m, the tile's rows then step that digit), writes are 16-byte packs along k.
 struct SplitMap {
     Map3 m, k;
 };
 
+constexpr int SP_TM = 32, SP_TK = 64;
+
 template <int KIND>
-__global__ void k_split(const double *src, void *hi, void *lo, int64_t M, int64_t K, int64_t Kp, SplitMap mp) {
-    __shared__ double tile[32][33];
-    const int64_t mt = (int64_t)blockIdx.y * 32, kt = (int64_t)blockIdx.x * 32;
-    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8 threads
-    // read: pick the tile orientation that keeps the source reads contiguous
-    const bool k_fast = mp.k.S2 == 1 && mp.k.R2 >= 32;
-    const int mR1 = (int)mp.m.R1, mR2 = (int)mp.m.R2, kR1 = (int)mp.k.R1, kR2 = (int)mp.k.R2;
-    for (int r = ty; r < 32; r += 8) {
-        int m = (int)mt + (k_fast ? r : tx), k = (int)kt + (k_fast ? tx : r);
-        double v = 0.0;
-        if (m < M && k < K) {
-            const int64_t mo = (int64_t)(m / (mR1 * mR2)) * mp.m.S0 + (int64_t)((m / mR2) % mR1) * mp.m.S1 +
-                               (int64_t)(m % mR2) * mp.m.S2;
-            const int64_t ko = (int64_t)(k / (kR1 * kR2)) * mp.k.S0 + (int64_t)((k / kR2) % kR1) * mp.k.S1 +
-                               (int64_t)(k % kR2) * mp.k.S2;
-            v = src[mo + ko];
-        }
-        if (k_fast)
-            tile[r][tx] = v;
-        else
-            tile[tx][r] = v;
+__global__ void __launch_bounds__(256) k_split(const double *src, void *hi, void *lo, int64_t M, int64_t K, int64_t kw,
+                                               int64_t ld, int64_t k0, SplitMap mp, int mode, int64_t nty) {
+    __shared__ double tile[SP_TM][SP_TK + 1];
+    __shared__ int64_t smo[SP_TM], srow[SP_TM], sko[SP_TK];
+    const int t = threadIdx.x;
+    const int64_t kt = (int64_t)blockIdx.x * SP_TK;
+    if (t < SP_TK) {
+        const int64_t k = kt + t;
+        sko[t] = k < K ? map3(mp.k, k) : -1;  // -1: zero column (padding) or outside the piece
     }
-    __syncthreads();
-    for (int r = ty; r < 32; r += 8) {
-        int64_t m = mt + r, k = kt + tx;
-        if (m >= M || k >= Kp) continue;
-        double v = tile[r][tx];
-        if (KIND == 0) {
-            __nv_bfloat16 h, l;
-            split_bf16(v, h, l);
-            ((__nv_bfloat16 *)hi)[m * Kp + k] = h;
-            ((__nv_bfloat16 *)lo)[m * Kp + k] = l;
+    for (int64_t ty = blockIdx.y; ty < nty; ty += gridDim.y) {
+        __syncthreads();  // previous tile fully consumed
+        if (t < SP_TM) {
+            int64_t m;
+            bool valid;
+            if (mode == 2) {
+                const int64_t R1 = mp.m.R1, R2 = mp.m.R2, nb1 = (R1 + SP_TM - 1) / SP_TM;
+                const int64_t a2 = ty % R2, a1 = ((ty / R2) % nb1) * SP_TM + t, a0 = ty / (R2 * nb1);
+                valid = a1 < R1;
+                m = (a0 * R1 + a1) * R2 + a2;
+            } else {
+                m = ty * SP_TM + t;
+                valid = m < M;
+            }
+            srow[t] = valid ? m : -1;
+            smo[t] = valid ? map3(mp.m, m) : 0;
+        }
+        __syncthreads();
+        if (mode == 0) {
+            const int kk = t & (SP_TK - 1);
+            const int64_t ko = sko[kk];
+#pragma unroll
+            for (int r = t >> 6; r < SP_TM; r += 4)
+                tile[r][kk] = (srow[r] >= 0 && ko >= 0) ? __ldg(src + smo[r] + ko) : 0.0;
         } else {
-            float h, l;
-            split_tf32(v, h, l);
-            ((float *)hi)[m * Kp + k] = h;
-            ((float *)lo)[m * Kp + k] = l;
+            const int r = t & 31;
+            const bool rv = srow[r] >= 0;
+            const int64_t mo = smo[r];
+#pragma unroll
+            for (int kk = t >> 5; kk < SP_TK; kk += 8) {
+                const int64_t ko = sko[kk];
+                tile[r][kk] = (rv && ko >= 0) ? __ldg(src + mo + ko) : 0.0;
+            }
+        }
+        __syncthreads();
+        const int r = t >> 3, kc = (t & 7) * 8;
+        const int64_t row = srow[r];
+        const int64_t kbeg = kt + kc;
+        if (row < 0 || kbeg >= kw) continue;
+        const int64_t dst = row * ld + k0 + kbeg;
+        if (KIND == 0) {
+            __nv_bfloat16 h[8], l[8];
+#pragma unroll
+            for (int j = 0; j < 8; j++) split_bf16(tile[r][kc + j], h[j], l[j]);
+            __nv_bfloat16 *H = (__nv_bfloat16 *)hi + dst, *Lo = (__nv_bfloat16 *)lo + dst;
+            if (kbeg + 8 <= kw && (dst & 7) == 0) {
+                *(uint4 *)H = *(uint4 *)h;
+                *(uint4 *)Lo = *(uint4 *)l;
+            } else {
+                for (int j = 0; j < 8 && kbeg + j < kw; j++) {
+                    H[j] = h[j];
+                    Lo[j] = l[j];
+                }
+            }
+        } else {
+            float h[8], l[8];
+#pragma unroll
+            for (int j = 0; j < 8; j++) split_tf32(tile[r][kc + j], h[j], l[j]);
+            float *H = (float *)hi + dst, *Lo = (float *)lo + dst;
+            if (kbeg + 8 <= kw && (dst & 3) == 0) {
+                ((float4 *)H)[0] = *(float4 *)h;
+                ((float4 *)H)[1] = *(float4 *)(h + 4);
+                ((float4 *)Lo)[0] = *(float4 *)l;
+                ((float4 *)Lo)[1] = *(float4 *)(l + 4);
+            } else {
+                for (int j = 0; j < 8 && kbeg + j < kw; j++) {
+                    H[j] = h[j];
+                    Lo[j] = l[j];
+                }
+            }
         }
     }
 }
@@ -408,8 +540,8 @@ static EncodeTiledFn encode_fn() {
 
 // 2-D K-major piece [rows][Kp] with a (k-block x box_rows) box and the
 // swizzle that matches kb_bytes.
-static int make_map(CUtensorMap *map, const void *ptr, int kind, int64_t rows, int64_t Kp, int box_rows,
-                    int kb_bytes) {
+static int make_map(CUtensorMap *map, const void *ptr, int kind, int64_t rows, int64_t Kp, int64_t ld,
+                    int box_rows, int kb_bytes) {
     EncodeTiledFn fn = encode_fn();
     if (!fn) {
         set_error("cuTensorMapEncodeTiled is unavailable");
@@ -417,7 +549,7 @@ static int make_map(CUtensorMap *map, const void *ptr, int kind, int64_t rows, i
     }
     const int esz = kind == 0 ? 2 : 4;
     cuuint64_t dims[2] = {(cuuint64_t)Kp, (cuuint64_t)rows};
-    cuuint64_t strides[1] = {(cuuint64_t)(Kp * esz)};
+    cuuint64_t strides[1] = {(cuuint64_t)(ld * esz)};
     cuuint32_t box[2] = {(cuuint32_t)(kb_bytes / esz), (cuuint32_t)box_rows};
     cuuint32_t estr[2] = {1, 1};
     CUtensorMapSwizzle sw = kb_bytes == 128 ? CU_TENSOR_MAP_SWIZZLE_128B
@@ -434,18 +566,26 @@ static int make_map(CUtensorMap *map, const void *ptr, int kind, int64_t rows, i
 
 template <int ST>
 static size_t gemm_smem_bytes(int kb_bytes) {
-    return 1024 + ST * (size_t)(2 * GM * kb_bytes + 2 * GN * kb_bytes) + sizeof(GemmSmem<ST>);
+    return 1024 + ST * (size_t)(2 * GM * kb_bytes + 2 * GN * kb_bytes) + EPI_WARPS * EPI_WARP_BYTES +
+           sizeof(GemmSmem<ST>);
 }
 
 template <int KIND, int KB, int ST>
 static int gemm_launch(const CUtensorMap &a, const CUtensorMap &b, const CUtensorMap &c, const CUtensorMap &d, int M,
                        int N, int nkb, double *C, const GemmEpi &epi, double alpha, double beta, int *status,
                        int group_m, cudaStream_t st) {
+    // write along columns when the column map's fastest digit is contiguous,
+    // along rows when only the row map's is
+    const int epi_cols = (epi.col.S2 == 1 || epi.row.S2 != 1) ? 1 : 0;
     size_t smem = gemm_smem_bytes<ST>(KB);
-    unsigned tiles = ceil_div(N, GN) * ceil_div(M, GM);
+    const int64_t tiles = (int64_t)ceil_div(N, GN) * (int64_t)ceil_div(M, GM);
+    DCC_REQUIRE(tiles < (1ll << 31), DCC_ERR_SHAPE, "too many output tiles");
+    int dev = 0, nsm = 148;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    const unsigned grid = (unsigned)(tiles < nsm ? tiles : nsm);  // persistent: one CTA per SM
     cudaFuncSetAttribute(k_gemm_split3<KIND, KB, ST>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k_gemm_split3<KIND, KB, ST><<<tiles, G_THREADS, smem, st>>>(a, b, c, d, M, N, nkb, C, epi, alpha, beta, status,
-                                                                group_m);
+    k_gemm_split3<KIND, KB, ST><<<grid, G_THREADS, smem, st>>>(a, b, c, d, M, N, nkb, C, epi, alpha, beta, status,
+                                                                group_m, epi_cols);
     return launch_status("gemm_split3");
 }
 
@@ -453,35 +593,58 @@ static int gemm_launch(const CUtensorMap &a, const CUtensorMap &b, const CUtenso
 
 using namespace dcc;
 
-extern "C" int dcc_split_operand(const double *src, void *hi, void *lo, int64_t M, int64_t K, int64_t Kp,
-                                 const int64_t *map10, int kind, void *stream) {
+extern "C" int dcc_split_operand_at(const double *src, void *hi, void *lo, int64_t M, int64_t K, int64_t kw,
+                                    int64_t ld, int64_t k0, const int64_t *map10, int kind, void *stream) {
     clear_error();
-    DCC_REQUIRE(M >= 0 && K >= 0 && Kp >= K, DCC_ERR_SHAPE, "bad split sizes (M=%lld K=%lld Kp=%lld)",
-                (long long)M, (long long)K, (long long)Kp);
+    DCC_REQUIRE(M >= 0 && K >= 0 && kw >= K && k0 >= 0 && k0 + kw <= ld, DCC_ERR_SHAPE,
+                "bad split sizes (M=%lld K=%lld kw=%lld k0=%lld ld=%lld)", (long long)M, (long long)K, (long long)kw,
+                (long long)k0, (long long)ld);
     DCC_REQUIRE(kind == 0 || kind == 1, DCC_ERR_UNSUPPORTED, "split kind must be 0 (bf16) or 1 (tf32)");
-    if (M == 0 || Kp == 0) return DCC_OK;
+    if (M == 0 || kw == 0) return DCC_OK;
     DCC_REQUIRE(src && hi && lo && map10, DCC_ERR_NULL, "NULL buffer");
     DCC_REQUIRE(map3_ok(map10) && map3_ok(map10 + 5), DCC_ERR_SHAPE, "map radices must be >= 1 with R1*R2 < 2^31");
-    DCC_REQUIRE(M < (1ll << 31) && Kp < (1ll << 31), DCC_ERR_SHAPE, "split sizes must fit in 31 bits");
+    DCC_REQUIRE(M < (1ll << 31) && ld < (1ll << 31), DCC_ERR_SHAPE, "split sizes must fit in 31 bits");
     SplitMap mp{{map10[0], map10[1], map10[2], map10[3], map10[4]}, {map10[5], map10[6], map10[7], map10[8], map10[9]}};
-    dim3 grid(ceil_div(Kp, 32), ceil_div(M, 32));
-    DCC_REQUIRE(grid.y <= 65535, DCC_ERR_UNSUPPORTED, "M too large for one split launch");
-    if (kind == 0)
-        k_split<0><<<grid, 256, 0, as_stream(stream)>>>(src, hi, lo, M, K, Kp, mp);
+    // read along the contiguous source index: k, else m, else m's middle digit
+    int mode;
+    if (mp.k.S2 == 1 && mp.k.R2 >= 16)
+        mode = 0;
+    else if (mp.m.S2 == 1 || mp.m.R2 == 1)
+        mode = 1;
+    else if (mp.m.S1 == 1 && mp.m.R1 > 1)
+        mode = 2;
     else
-        k_split<1><<<grid, 256, 0, as_stream(stream)>>>(src, hi, lo, M, K, Kp, mp);
+        mode = mp.k.S2 == 1 ? 0 : 1;
+    if (mode == 2) DCC_REQUIRE(mp.m.R1 * mp.m.R2 * ((M + mp.m.R1 * mp.m.R2 - 1) / (mp.m.R1 * mp.m.R2)) == M,
+                               DCC_ERR_SHAPE, "row map does not tile M");
+    const int64_t nty = mode == 2 ? (M / (mp.m.R1 * mp.m.R2)) * ((mp.m.R1 + SP_TM - 1) / SP_TM) * mp.m.R2
+                                  : (M + SP_TM - 1) / SP_TM;
+    dim3 grid(ceil_div(kw, SP_TK), (unsigned)(nty < 65535 ? nty : 65535));
+    if (kind == 0)
+        k_split<0><<<grid, 256, 0, as_stream(stream)>>>(src, hi, lo, M, K, kw, ld, k0, mp, mode, nty);
+    else
+        k_split<1><<<grid, 256, 0, as_stream(stream)>>>(src, hi, lo, M, K, kw, ld, k0, mp, mode, nty);
     return launch_status("split_operand");
 }
 
-extern "C" int dcc_gemm_split3(const void *A_hi, const void *A_lo, const void *B_hi, const void *B_lo, int64_t M,
-                               int64_t N, int64_t Kp, double *C, const int64_t *epi10, double alpha, double beta,
-                               int kind, int *status, void *stream) {
+extern "C" int dcc_split_operand(const double *src, void *hi, void *lo, int64_t M, int64_t K, int64_t Kp,
+                                 const int64_t *map10, int kind, void *stream) {
+    return dcc_split_operand_at(src, hi, lo, M, K, Kp, Kp, 0, map10, kind, stream);
+}
+
+extern "C" int dcc_gemm_split3_ld(const void *A_hi, const void *A_lo, int64_t lda, const void *B_hi,
+                                  const void *B_lo, int64_t ldb, int64_t M, int64_t N, int64_t Kp, double *C,
+                                  const int64_t *epi10, double alpha, double beta, int kind, int *status,
+                                  void *stream) {
     clear_error();
     DCC_REQUIRE(kind == 0 || kind == 1, DCC_ERR_UNSUPPORTED, "kind must be 0 (bf16x3) or 1 (tf32x3)");
     const int kblk = kind == 0 ? 64 : 32;
     DCC_REQUIRE(M >= 0 && N >= 0 && Kp >= 0 && Kp % kblk == 0, DCC_ERR_SHAPE,
                 "Kp (%lld) must be a multiple of %d", (long long)Kp, kblk);
     DCC_REQUIRE(M < (1ll << 31) && N < (1ll << 31), DCC_ERR_SHAPE, "M, N must fit in 31 bits");
+    DCC_REQUIRE(lda >= Kp && ldb >= Kp && lda % 8 == 0 && ldb % 8 == 0 && lda < (1ll << 31) && ldb < (1ll << 31),
+                DCC_ERR_SHAPE, "row pitches (lda=%lld ldb=%lld) must be >= Kp and multiples of 8", (long long)lda,
+                (long long)ldb);
     if (M == 0 || N == 0) return DCC_OK;
     DCC_REQUIRE(A_hi && A_lo && B_hi && B_lo && C && epi10 && status, DCC_ERR_NULL, "NULL buffer");
     DCC_REQUIRE(Kp > 0, DCC_ERR_SHAPE, "empty contraction");
@@ -492,10 +655,10 @@ extern "C" int dcc_gemm_split3(const void *A_hi, const void *A_lo, const void *B
                 "Kp (%lld) must be a multiple of the k-block", (long long)Kp);
     CUtensorMap mAh, mAl, mBh, mBl;
     int rc;
-    if ((rc = make_map(&mAh, A_hi, kind, M, Kp, GM, cfg.kb_bytes)) ||
-        (rc = make_map(&mAl, A_lo, kind, M, Kp, GM, cfg.kb_bytes)) ||
-        (rc = make_map(&mBh, B_hi, kind, N, Kp, GN, cfg.kb_bytes)) ||
-        (rc = make_map(&mBl, B_lo, kind, N, Kp, GN, cfg.kb_bytes)))
+    if ((rc = make_map(&mAh, A_hi, kind, M, Kp, lda, GM, cfg.kb_bytes)) ||
+        (rc = make_map(&mAl, A_lo, kind, M, Kp, lda, GM, cfg.kb_bytes)) ||
+        (rc = make_map(&mBh, B_hi, kind, N, Kp, ldb, GN, cfg.kb_bytes)) ||
+        (rc = make_map(&mBl, B_lo, kind, N, Kp, ldb, GN, cfg.kb_bytes)))
         return rc;
     cudaStream_t st = as_stream(stream);
     const int nkb = (int)(Kp / (cfg.kb_bytes / (kind == 0 ? 2 : 4)));
@@ -514,6 +677,12 @@ extern "C" int dcc_gemm_split3(const void *A_hi, const void *A_lo, const void *B
 #undef DCC_GEMM_CASE
     set_error("no kernel for k-block %d bytes x %d stages", cfg.kb_bytes, cfg.stages);
     return DCC_ERR_UNSUPPORTED;
+}
+
+extern "C" int dcc_gemm_split3(const void *A_hi, const void *A_lo, const void *B_hi, const void *B_lo, int64_t M,
+                               int64_t N, int64_t Kp, double *C, const int64_t *epi10, double alpha, double beta,
+                               int kind, int *status, void *stream) {
+    return dcc_gemm_split3_ld(A_hi, A_lo, Kp, B_hi, B_lo, Kp, M, N, Kp, C, epi10, alpha, beta, kind, status, stream);
 }
 
 extern "C" int dcc_gemm_set_config(int kb_bytes, int stages, int group_m) {

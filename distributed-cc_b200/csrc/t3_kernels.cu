@@ -904,6 +904,94 @@ extern "C" int dcc_fill_t3_from_abc(double *target, int64_t a0, int64_t a1, int6
     return launch_status("fill_t3_from_abc");
 }
 
+// ---------------------------------------------------------------- unpack every ordering
+
+namespace dcc {
+
+// U[(x*nocc + y)*nocc + z] = T3[x,y,z] for every ordered (x,y,z), from the
+// canonical blocks.  A CTA owns one canonical tile triple: it loads the
+// orbit set of block q once and writes it to each distinct ordering of q's
+// triple (up to 6 output blocks x up to 6 tiles), every output tile being a
+// permuted tile of the same set.
+__global__ void __launch_bounds__(OT_THREADS) k_unpack_all(const double *t3, double *U, int64_t nblocks, int nocc,
+                                                           int nv, int ntile) {
+    extern __shared__ double sm[];  // 2 x 6 x SLOT
+    __shared__ OrbitSet os;
+    __shared__ int qtrip[3];
+    int t0, t1, t2;
+    decode_tri3(blockIdx.x, ntile, t0, t1, t2);
+    build_orbit_set(os, t0, t1, t2);
+    const int64_t n3 = (int64_t)nv * nv * nv;
+    const int pinv[6] = {0, 1, 2, 4, 3, 5};  // inverse of each axis map
+    int64_t q = blockIdx.y;
+    if (q >= nblocks) return;
+    load_orbit_tiles_async(sm, os, t3 + q * n3, nv);
+    cp_async_commit();
+    for (int stage = 0; q < nblocks; q += gridDim.y, stage ^= 1) {
+        const int64_t nq = q + gridDim.y;
+        if (nq < nblocks) {
+            load_orbit_tiles_async(sm + (stage ^ 1) * 6 * SLOT, os, t3 + nq * n3, nv);
+            cp_async_commit();
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
+        }
+        if (threadIdx.x == 0) {
+            // canonical triple of block q (lexicographic rank -> i<=j<=k)
+            int a, b, c;
+            decode_tri3(q, nocc, a, b, c);
+            qtrip[0] = a;
+            qtrip[1] = b;
+            qtrip[2] = c;
+        }
+        __syncthreads();
+        const double *buf = sm + stage * 6 * SLOT;
+        const int o[3] = {qtrip[0], qtrip[1], qtrip[2]};
+        for (int sg = 0; sg < 6; sg++) {
+            const int xyz[3] = {o[perm3(sg, 0)], o[perm3(sg, 1)], o[perm3(sg, 2)]};
+            bool dup = false;  // the same ordered triple from an earlier map (repeated indices)
+            for (int sp = 0; sp < sg; sp++)
+                if (o[perm3(sp, 0)] == xyz[0] && o[perm3(sp, 1)] == xyz[1] && o[perm3(sp, 2)] == xyz[2]) dup = true;
+            if (dup) continue;
+            int64_t srt[3];
+            const int cs = order_case3(xyz[0], xyz[1], xyz[2], srt);
+            const int pi = pinv[cs];
+            double *dst = U + (((int64_t)xyz[0] * nocc + xyz[1]) * nocc + xyz[2]) * n3;
+            for (int s = 0; s < os.nslot; s++) {
+                const int src_slot = os.nbr[s][pi];
+                const int X0 = os.tile[s][0] * TE, Y0 = os.tile[s][1] * TE, Z0 = os.tile[s][2] * TE;
+                for (int e = threadIdx.x; e < TE3; e += blockDim.x) {
+                    const int u[3] = {e >> 6, (e >> 3) & 7, e & 7};
+                    const int gx = X0 + u[0], gy = Y0 + u[1], gz = Z0 + u[2];
+                    if (gx >= nv || gy >= nv || gz >= nv) continue;
+                    dst[((int64_t)gx * nv + gy) * nv + gz] =
+                        buf[src_slot * SLOT + sidx(u[perm3(pi, 0)], u[perm3(pi, 1)], u[perm3(pi, 2)])];
+                }
+            }
+        }
+        __syncthreads();
+    }
+}
+
+}  // namespace dcc
+
+extern "C" int dcc_t3_unpack_all(const double *t3, double *U, int64_t nocc, int64_t nvir, void *stream) {
+    clear_error();
+    DCC_REQUIRE(nocc >= 0 && nvir >= 0, DCC_ERR_SHAPE, "negative size");
+    if (nocc == 0 || nvir == 0) return DCC_OK;
+    DCC_REQUIRE(t3 && U && t3 != U, DCC_ERR_NULL, "NULL or aliased buffer");
+    const int64_t nblocks = nocc * (nocc + 1) * (nocc + 2) / 6;
+    int ntile = (int)ceil_div(nvir, TE);
+    int64_t ntri = (int64_t)ntile * (ntile + 1) * (ntile + 2) / 6;
+    int64_t gy = (148 * 4 * 8 + ntri - 1) / ntri;
+    gy = gy < 1 ? 1 : (gy > nblocks ? nblocks : gy);
+    size_t smem = 2 * 6 * SLOT * sizeof(double);
+    cudaFuncSetAttribute(k_unpack_all, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_unpack_all<<<dim3((unsigned)ntri, (unsigned)gy), OT_THREADS, smem, as_stream(stream)>>>(t3, U, nblocks, (int)nocc,
+                                                                                            (int)nvir, ntile);
+    return launch_status("t3_unpack_all");
+}
+
 // ---------------------------------------------------------------- permutation gather
 
 namespace dcc {

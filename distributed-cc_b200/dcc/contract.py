@@ -22,9 +22,9 @@ f64 = torch.float64
 KIND = {"bf16x3": 0, "tf32x3": 1}
 _KBLK = {0: 64, 1: 32}
 
-_split = L.bind("dcc_split_operand", [L.c_vp, L.c_vp, L.c_vp, L.c_i64, L.c_i64, L.c_i64, L.c_vp, L.c_int, L.c_vp])
-_gemm = L.bind("dcc_gemm_split3", [L.c_vp] * 4 + [L.c_i64] * 3 + [L.c_vp, L.c_vp, L.c_dbl, L.c_dbl, L.c_int,
-                                                                   L.c_vp, L.c_vp])
+_split = L.bind("dcc_split_operand_at", [L.c_vp, L.c_vp, L.c_vp] + [L.c_i64] * 5 + [L.c_vp, L.c_int, L.c_vp])
+_gemm = L.bind("dcc_gemm_split3_ld", [L.c_vp, L.c_vp, L.c_i64, L.c_vp, L.c_vp] + [L.c_i64] * 4 +
+               [L.c_vp, L.c_vp, L.c_dbl, L.c_dbl, L.c_int, L.c_vp, L.c_vp])
 
 BIG = 1 << 30  # radix that makes a digit of a map a plain stride (< 2^31)
 
@@ -58,11 +58,24 @@ def padded_k(K, kind):
 
 
 class Split:
-    """Two-piece K-major copy of an FP64 operand: rows M, contraction K padded to Kp."""
+    """Two-piece K-major copy of an FP64 operand: rows M, contraction K padded to Kp.
 
-    def __init__(self, M, K, kind, device="cuda", buffers=None):
-        self.M, self.K, self.kind = int(M), int(K), int(kind)
+    With pieces=[K0, K1, ...] the contraction is the concatenation of several
+    operands (each piece starts on a multiple of 8 columns; the gaps and the
+    tail are zero), filled one by one with fill_piece."""
+
+    def __init__(self, M, K=None, kind=0, device="cuda", buffers=None, pieces=None):
+        self.M, self.kind = int(M), int(kind)
+        if pieces is None:
+            pieces = [int(K)]
+        offs, o = [], 0
+        for k in pieces:
+            offs.append(o)
+            o += (int(k) + 7) // 8 * 8
+        self.K = o if len(pieces) > 1 else int(pieces[0])
         self.Kp = padded_k(self.K, self.kind)
+        ends = offs[1:] + [self.Kp]
+        self.pieces = [(off, int(k), end - off) for off, k, end in zip(offs, pieces, ends)]
         dt = torch.bfloat16 if self.kind == 0 else torch.float32
         if buffers is None:
             self.hi = torch.empty((self.M, self.Kp), dtype=dt, device=device)
@@ -70,23 +83,38 @@ class Split:
         else:
             self.hi, self.lo = buffers
 
-    def fill(self, src, fm, fk):
-        """dst[m][k] = src[fm(m) + fk(k)] for three-digit maps fm, fk."""
+    def fill_piece(self, i, src, fm, fk):
+        """Columns of piece i: dst[m][off + k] = src[fm(m) + fk(k)] (zero past the piece's K)."""
         L.as_tensor(src, f64, "src")
-        L.check(_split(L.ptr(src), L.ptr(self.hi), L.ptr(self.lo), self.M, self.K, self.Kp, _i64x10(fm, fk),
+        off, k, w = self.pieces[i]
+        L.check(_split(L.ptr(src), L.ptr(self.hi), L.ptr(self.lo), self.M, k, w, self.Kp, off, _i64x10(fm, fk),
                        self.kind, L.stream_ptr()))
         return self
 
+    def fill(self, src, fm, fk):
+        """dst[m][k] = src[fm(m) + fk(k)] for three-digit maps fm, fk."""
+        if len(self.pieces) != 1:
+            raise ValueError("a K-concatenated operand is filled with fill_piece")
+        return self.fill_piece(0, src, fm, fk)
 
-def gemm_(A, B, C, frow, fcol, alpha=1.0, beta=1.0, status=None):
-    """C[frow(m) + fcol(n)] = alpha * A B^T + beta * C (A: Split [M,K], B: Split [N,K])."""
-    if A.kind != B.kind or A.Kp != B.Kp:
-        raise ValueError("A and B must be split with the same kind and padded K")
+
+def gemm_(A, B, C, frow, fcol, alpha=1.0, beta=1.0, status=None, Kp=None):
+    """C[frow(m) + fcol(n)] = alpha * A B^T + beta * C (A: Split [M,K], B: Split [N,K]).
+
+    Kp (default: both operands' padded K) contracts only the leading Kp columns."""
+    if A.kind != B.kind:
+        raise ValueError("A and B must be split with the same kind")
+    if Kp is None:
+        if A.Kp != B.Kp:
+            raise ValueError("A and B must have the same padded K (or pass Kp)")
+        Kp = A.Kp
+    if Kp > A.Kp or Kp > B.Kp:
+        raise ValueError("Kp exceeds an operand's columns")
     L.as_tensor(C, f64, "C")
     if status is None:
         status = torch.zeros(1, dtype=torch.int32, device=C.device)
-    L.check(_gemm(L.ptr(A.hi), L.ptr(A.lo), L.ptr(B.hi), L.ptr(B.lo), A.M, B.M, A.Kp, L.ptr(C), _i64x10(frow, fcol),
-                  float(alpha), float(beta), A.kind, L.ptr(status), L.stream_ptr()))
+    L.check(_gemm(L.ptr(A.hi), L.ptr(A.lo), A.Kp, L.ptr(B.hi), L.ptr(B.lo), B.Kp, A.M, B.M, int(Kp), L.ptr(C),
+                  _i64x10(frow, fcol), float(alpha), float(beta), A.kind, L.ptr(status), L.stream_ptr()))
     return status
 
 

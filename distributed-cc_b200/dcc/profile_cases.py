@@ -5,6 +5,9 @@
     python -m dcc.profile_cases update [--reps 3]
     python -m dcc.profile_cases q      [--reps 3]
     python -m dcc.profile_cases gather [--reps 3]
+    python -m dcc.profile_cases xgemm  [--reps 3]
+    python -m dcc.profile_cases oogemm [--reps 3]
+    python -m dcc.profile_cases unpack [--reps 3]
 
 Each case builds its inputs once and launches the kernel `reps` times, so a
 profiler can skip the warm-up launches and capture the last one.  Sizes are
@@ -71,22 +74,56 @@ def case_q(reps):
     torch.cuda.synchronize()
 
 
-def case_gather(reps):
+def case_gather(reps, nocc=10):
     from dcc import synthetic, t3_residual
-    d = synthetic.make_inputs(10, 90, seed=0)
-    tr = t3_residual.T3Residual(10, 90, "fp64")
+    d = synthetic.make_inputs(nocc, 90, seed=0)
+    tr = t3_residual.T3Residual(nocc, 90, "bf16x3", with_oo=False)
     r3 = torch.empty_like(d.t3)
-    tr.vt2_(r3, d)
+    S, Y = tr.s_(d, d.t3), tr.y_(d)
+    src = [(S, 1.0, t3_residual.full_strides(nocc, 90), t3_residual.ALL_S3),
+           (Y, -1.0, tr.y_strides, t3_residual.ALL_S3)]
     for _ in range(reps):
-        t3_residual.s3_gather_(r3, d.ijk, 90, 0.0, tr.X, 1.0, tr.x_strides, tr.Y, -1.0, tr.y_strides)
+        t3_residual.perm_gather_(r3, d.ijk, 90, 0.0, src)
+    torch.cuda.synchronize()
+
+
+def case_xgemm(reps, nocc=10):
+    """The W_vvvo.t2 GEMM (K = nvir, written into the full-layout S): epilogue-bound."""
+    from dcc import synthetic, t3_residual
+    d = synthetic.make_inputs(nocc, 90, seed=0)
+    tr = t3_residual.T3Residual(nocc, 90, "bf16x3", with_oo=False)
+    for _ in range(reps):
+        tr.s_(d, d.t3)
+    torch.cuda.synchronize()
+    assert tr.status_ok()
+
+
+def case_oogemm(reps, nocc=6):
+    """The K-concatenated OO GEMM and the T1 GEMM at nocc=6 (a few GB on the device)."""
+    from dcc import synthetic, t3_residual
+    d = synthetic.make_inputs(nocc, 90, seed=0)
+    tr = t3_residual.T3Residual(nocc, 90, "bf16x3", with_oo=True)
+    for _ in range(reps):
+        tr.s_(d, d.t3)
+    torch.cuda.synchronize()
+    assert tr.status_ok()
+
+
+def case_unpack(reps, nocc=10):
+    from dcc import synthetic, t3_residual
+    d = synthetic.make_inputs(nocc, 90, seed=0)
+    U = torch.empty((nocc ** 3, 90, 90, 90), dtype=torch.float64, device="cuda")
+    for _ in range(reps):
+        t3_residual.unpack_all_(d.t3, U, nocc, 90)
     torch.cuda.synchronize()
 
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("case", choices=["gemm", "p3", "update", "q", "gather"])
+    ap.add_argument("case", choices=["gemm", "p3", "update", "q", "gather", "xgemm", "oogemm", "unpack"])
     ap.add_argument("--kind", default="bf16x3")
     ap.add_argument("--reps", type=int, default=3)
+    ap.add_argument("--nocc", type=int, default=None, help="occupied orbitals (xgemm, oogemm, gather, unpack)")
     a = ap.parse_args()
     if a.case == "gemm":
         case_gemm(a.kind, a.reps)
@@ -94,8 +131,9 @@ def main():
         case_p3(a.reps)
     elif a.case == "update":
         case_update(a.reps)
-    elif a.case == "gather":
-        case_gather(a.reps)
+    elif a.case in ("gather", "xgemm", "oogemm", "unpack"):
+        fn = {"gather": case_gather, "xgemm": case_xgemm, "oogemm": case_oogemm, "unpack": case_unpack}[a.case]
+        fn(a.reps, **({} if a.nocc is None else {"nocc": a.nocc}))
     else:
         case_q(a.reps)
     print("ok")

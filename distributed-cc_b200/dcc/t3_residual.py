@@ -1,30 +1,43 @@
-"""Batched T3 residual on the GPU (distr_cc/rccsdt.py:368-433, 947-971).
+"""Batched T3 residual on the GPU (distr_cc/rccsdt.py:368-732, 947-971).
 
 The reference walks the canonical blocks and issues one `_einsum` per block
-and einsum string.  Here each group of strings becomes one large contraction
-over all blocks:
+and einsum string.  Here the strings become a few large contractions over
+all blocks.  With U the unpacked t3 of every ordered (i,j,k) (U is invariant
+under simultaneous permutations of (i,j,k) and (a,b,c)), every W_vvvo.t2,
+W_vooo.t2 and OO batch string (distr_cc/rccsdt.py:385-396, 435-732) is part
+of one full symmetrization
 
-* The twelve W_vvvo.t2 / W_vooo.t2 strings (distr_cc/rccsdt.py:385-396) are
-  the simultaneous S3 symmetrization of two contractions taken over every
-  ordered (i,j,k):
-      X[ijk][abc] = sum_d W_vvvo[a,b,d,j] t2[i,k,d,c]
-      Y[ijk][abc] = sum_l W_vooo[a,l,i,j] t2[l,k,b,c]
-      r3[ijk][abc] = sum_sigma (X - Y)[sigma(ijk)][sigma(abc)]
-  so they are two GEMMs and one gather (dcc_t3_perm_gather).
-* The OO batch terms (distr_cc/rccsdt.py:435-732: masked W_ovov / W_ovvo
-  einsums per batch block and the F_oo / W_oooo prefactor matrices) are the
-  partial symmetrization over {identity, (jik;bac), (kij;cab)} of one tensor
-  Z over every ordered (i,j,k), built by five GEMMs over the unpacked t3
-  (K = nocc*nvir) and two small FP64 GEMMs; the same gather adds it.
-* F_vv.t3 (three strings) are three batched GEMMs.
-* W_vvvv.t3 (three strings, the dominant cost) are three GEMMs over all
-  blocks; in mixed precision they run on the tcgen05 split-BF16x3 kernel and
-  accumulate straight into r3.
+    r3[ijk][abc] = sum_{p in S3} (S - Y)[p(ijk)][p(abc)]
+
+of two tensors over every ordered (i,j,k):
+
+    Y  = sum_l W_vooo[a,l,i,j] t2[l,k,b,c]                       (FP64, K = nocc)
+    S  = X + T1 + T2 + T5/2 + (W_oooo.U - F_oo.U)/2
+    X  = sum_d W_vvvo[a,b,d,j] t2[i,k,d,c]
+    T1 = - sum_{l,d} W_ovov[l,b,i,d] U[jkl][d,c,a]
+    T2 =   sum_{l,d} G2[l,a,i,d] U[jkl][d,c,b],   G2 = -(W_ovov[l,a,i,d] + W_ovvo[l,a,d,i]) / 2
+    T5 =   sum_{l,d} W_ovvo[l,a,d,i] U[jkl][b,c,d]
+    W_oooo.U = sum_{l,m} W_oooo[l,m,i,j] U[lmk][abc],   F_oo.U = sum_l F_oo[l,i] U[ljk][abc]
+
+The reference's two remaining W_ovov strings are T1 and T2 composed with
+(i,k,j; a,c,b) and drop out of the S3 sum; T5, F_oo.U and (for a W_oooo with
+the pair symmetry W[l,m,i,j] = W[m,l,j,i]) W_oooo.U are invariant under that
+permutation, hence the halves.  A W_oooo without the pair symmetry keeps its
+antisymmetric part on the reference's own permutation set
+{identity, (i,k,j; a,c,b), (j,k,i; b,c,a)}.
+
+In mixed precision S is built by three split-precision tcgen05 GEMMs written
+straight into S's [i][j][k][a][b][c] layout (X; T2 and T5/2 as one GEMM over
+the concatenated contraction index; T1 reusing T2's U operand) plus an FP64
+GEMM for the K = nocc^2 W_oooo / F_oo part, and one gather kernel applies the
+symmetrization to S and Y.  F_vv.t3 (three strings) are FP64 batched GEMMs;
+W_vvvv.t3 (three strings, the dominant cost) are three split-precision GEMMs
+that accumulate straight into r3.
 
 precision = "fp64" runs every contraction in FP64 (cuBLAS DGEMM through
 torch): the plain FP64 GPU path.  "bf16x3" / "tf32x3" run the large
-contractions (X and W_vvvv.t3) as split products with FP32 accumulation;
-the denominators, update, norms and all sums stay FP64.
+contractions as split products with FP32 accumulation; the denominators,
+update, norms and all sums stay FP64.
 """
 from __future__ import annotations
 
@@ -60,6 +73,7 @@ _pgather = L.bind("dcc_t3_perm_gather", [L.c_vp, L.c_vp, L.c_i64, L.c_i64, L.c_d
 # p in the order (x,y,z), (x,z,y), (y,x,z), (y,z,x), (z,x,y), (z,y,x))
 ALL_S3 = 63
 OO_SET = (1 << 0) | (1 << 2) | (1 << 4)  # identity, (j,i,k;b,a,c), (k,i,j;c,a,b)
+OOOO_SET = (1 << 0) | (1 << 1) | (1 << 3)  # identity, (i,k,j;a,c,b), (j,k,i;b,c,a)
 
 
 def perm_gather_(r3, ijk, nvir, beta, sources):
@@ -74,10 +88,63 @@ def perm_gather_(r3, ijk, nvir, beta, sources):
     return r3
 
 
+_unpack_all = L.bind("dcc_t3_unpack_all", [L.c_vp, L.c_vp, L.c_i64, L.c_i64, L.c_vp])
+
+
+def unpack_all_(t3, U, nocc, nvir):
+    """U[(x*nocc+y)*nocc+z] = T3[x,y,z] for every ordered triple (take_t3 of all orderings)."""
+    L.check(_unpack_all(L.ptr(t3), L.ptr(U), nocc, nvir, L.stream_ptr()))
+    return U
+
+
 def full_strides(no, nv):
     """Strides (x,y,z,a,b,c) of a full ordered-triple tensor laid out [x][y][z][a][b][c]."""
     n3 = nv ** 3
     return (no * no * n3, no * n3, n3, nv * nv, nv, 1)
+
+
+def s_plan(no, nv):
+    """Operand and output maps of the split-precision GEMMs that build S.
+
+    Each entry: A pieces and B pieces as (name, row map, k map), the output
+    (row map, column map) into S = [i][j][k][a][b][c], alpha and beta.  The
+    T1 GEMM takes the first piece of the T2/T5 GEMM's B operand (the same
+    U layout) and contracts only its leading columns."""
+    c = contract
+    n3v = nv ** 3
+    return {
+        # X: rows (j,a,b) of W_vvvo[a,b,d,j], cols (i,k,c) of t2[i,k,d,c], K = d
+        "x": dict(a=[("W_vvvo", c.two(nv * nv, 1, nv * no), c.lin(no))],
+                  b=[("t2", c.two(nv, nv * nv, 1), c.lin(nv))],
+                  out=(c.three(nv, nv, no * n3v, nv * nv, nv), c.three(no, nv, no * no * n3v, n3v, 1)),
+                  alpha=1.0, beta=0.0),
+        # T2 + T5/2: rows (i,a), cols (jk,b,c), K = (l,d) of G2, then (l,d) of W_ovvo/2
+        "oo": dict(a=[("G2", c.lin(no * nv), c.lin(1)),
+                      ("Wvo_half", c.two(nv, 1, nv * no), c.two(nv, nv * nv * no, no))],
+                   b=[("U", c.three(nv, nv, no * n3v, 1, nv), c.two(nv, n3v, nv * nv)),     # U[jkl][d,c,b]
+                      ("U", c.three(nv, nv, no * n3v, nv * nv, nv), c.two(nv, n3v, 1))],   # U[jkl][b,c,d]
+                   out=(c.two(nv, no * no * n3v, nv * nv), c.three(nv, nv, n3v, nv, 1)),
+                   alpha=1.0, beta=1.0),
+        # T1: rows (i,b) of W_ovov[l,b,i,d], cols (jk,a,c) of U[jkl][d,c,a] (= piece 0 of oo.b)
+        "t1": dict(a=[("W_ovov", c.two(nv, nv, no * nv), c.two(nv, nv * no * nv, 1))],
+                   out=(c.two(nv, no * no * n3v, nv), c.three(nv, nv, n3v, nv * nv, 1)),
+                   alpha=-1.0, beta=1.0),
+    }
+
+
+def woooo_foo_matrix(W_oooo, F_oo, sym_tol=1e-14):
+    """(A, W_anti): A[(i,j)][(l,m)] = (Ws[l,m,i,j] - F_oo[l,i] delta_mj) / 2 with Ws the
+    pair-symmetric part of W_oooo; W_anti = the antisymmetric part, or None when it is
+    below sym_tol relative to max|W_oooo| (one device-to-host read of two scalars)."""
+    no = W_oooo.shape[0]
+    Wt = W_oooo.permute(1, 0, 3, 2)
+    Wa = 0.5 * (W_oooo - Wt)
+    big = torch.stack([Wa.abs().max(), W_oooo.abs().max()]).cpu()
+    anti = float(big[0]) > sym_tol * max(float(big[1]), 1e-300)
+    Ws = W_oooo - Wa if anti else W_oooo
+    eye = torch.eye(no, dtype=W_oooo.dtype, device=W_oooo.device)
+    A = 0.5 * Ws.permute(2, 3, 0, 1) - 0.5 * torch.einsum("li,mj->ijlm", F_oo, eye)
+    return A.reshape(no * no, no * no).contiguous(), (Wa.contiguous() if anti else None)
 
 
 class T3Residual:
@@ -89,117 +156,97 @@ class T3Residual:
         self.n3 = no * (no + 1) * (no + 2) // 6
         self.dev = device
         self.with_oo = with_oo
-        if with_oo:
-            self.U = torch.empty((no ** 3, nv, nv, nv), dtype=f64, device=device)  # every ordered (x,y,z)
-            self.Z = torch.empty_like(self.U)
-            trip = [(x, y, z) for x in range(no) for y in range(no) for z in range(no)]
-            self.all_xyz = torch.tensor(trip, dtype=torch.int32, device=device)
-            self.loc = torch.arange(self.n3, dtype=torch.int64, device=device)
-        self.X = torch.empty((no * nv * nv, no * no * nv), dtype=f64, device=device)  # [(j,a,b),(i,k,c)]
-        self.Y = (torch.empty((no * no * nv, no * nv * nv), dtype=f64, device=device)  # [(i,j,a),(k,b,c)]
-                  if precision == "fp64" else None)
-        N = no * no * nv
-        self.x_strides = (no * nv, nv * nv * N, nv, nv * N, N, 1)
+        full = (no ** 3, nv, nv, nv)
+        self.S = torch.empty(full, dtype=f64, device=device)  # [i][j][k][a][b][c]
+        self.U = torch.empty(full, dtype=f64, device=device) if with_oo else None
+        self.Y = torch.empty((no * no * nv, no * nv * nv), dtype=f64, device=device)  # [(i,j,a),(k,b,c)]
         Ny = no * nv * nv
         self.y_strides = (no * nv * Ny, nv * Ny, nv * nv, Ny, nv, 1)
+        self.Ganti = None
         if precision != "fp64":
             k = contract.KIND[precision]
             self.kind = k
+            self.plan = s_plan(no, nv)
             self.xa = contract.Split(no * nv * nv, nv, k, device)
             self.xb = contract.Split(no * no * nv, nv, k, device)
-            self.ya = contract.Split(no * no * nv, no, k, device)
-            self.yb = contract.Split(no * nv * nv, no, k, device)
             self.wvvvv = contract.WvvvvT3(self.n3, nv, precision, device)
             self.status = torch.zeros(1, dtype=torch.int32, device=device)
             if with_oo:
                 K = no * nv
-                self.oa = contract.Split(no * nv, K, k, device)           # W side, rows (i,x), K (l,d)
-                self.ob = contract.Split(no * no * nv * nv, K, k, device)  # U side, rows (jk,y,z), K (l,d)
+                self.ooa = contract.Split(no * nv, kind=k, device=device, pieces=[K, K])
+                self.oob = contract.Split(no * no * nv * nv, kind=k, device=device, pieces=[K, K])
+                self.t1a = contract.Split(no * nv, K, k, device)
+        else:
+            self.X = torch.empty((no * nv * nv, no * no * nv), dtype=f64, device=device)  # [(j,a,b),(i,k,c)]
 
     # ------------------------------------------------------------ pieces
-    def vt2_(self, d):
-        """X such that the twelve W_vvvo.t2 / W_vooo.t2 strings are sum_{p in S3} X[p(ijk)][p(abc)].
-
-        X[(j,a,b),(i,k,c)] = sum_d W_vvvo[a,b,d,j] t2[i,k,d,c] is formed first;
-        Y[ijk][abc] = sum_l W_vooo[a,l,i,j] t2[l,k,b,c] is then subtracted in X's layout."""
+    def y_(self, d):
+        """Y[(i,j,a),(k,b,c)] = sum_l W_vooo[a,l,i,j] t2[l,k,b,c] (FP64: K = nocc is bandwidth-bound)."""
         no, nv = self.no, self.nv
-        N = no * no * nv
-        if self.precision == "fp64":
-            Wt = d.W_vvvo.permute(3, 0, 1, 2).reshape(no * nv * nv, nv)
-            T2m = d.t2.permute(0, 1, 3, 2).reshape(no * no * nv, nv)
-            torch.matmul(Wt, T2m.t(), out=self.X)
-            A = d.W_vooo.permute(2, 3, 0, 1).reshape(no * no * nv, no)
-            Bm = d.t2.permute(1, 2, 3, 0).reshape(no * nv * nv, no)
-            torch.matmul(A, Bm.t(), out=self.Y)
-            # X[j,a,b,i,k,c] -= Y[i,j,a,k,b,c]
-            self.X.view(no, nv, nv, no, no, nv).sub_(self.Y.view(no, no, nv, no, nv, nv).permute(1, 2, 4, 0, 3, 5))
-        else:
-            c = contract
-            self.xa.fill(d.W_vvvo, c.two(nv * nv, 1, nv * no), c.lin(no))
-            self.xb.fill(d.t2, c.two(nv, nv * nv, 1), c.lin(nv))
-            c.gemm_(self.xa, self.xb, self.X, c.lin(N), c.lin(1), 1.0, 0.0, self.status)
-            # Y rows (i,j,a) from W_vooo[a,l,i,j], cols (k,b,c) from t2[l,k,b,c], K = l;
-            # accumulated with alpha = -1 straight into X[(j,a,b),(i,k,c)]
-            self.ya.fill(d.W_vooo, c.three(no, nv, no, 1, no ** 3), c.lin(no * no))
-            self.yb.fill(d.t2, c.lin(1), c.lin(no * nv * nv))
-            c.gemm_(self.ya, self.yb, self.X, c.three(no, nv, no * nv, nv * nv * N, nv * N),
-                    c.three(nv, nv, nv, N, 1), -1.0, 1.0, self.status)
-        return self.X
+        A = d.W_vooo.permute(2, 3, 0, 1).reshape(no * no * nv, no)
+        Bm = d.t2.permute(1, 2, 3, 0).reshape(no * nv * nv, no)
+        torch.matmul(A, Bm.t(), out=self.Y)
+        return self.Y
 
-    # ------------------------------------------------------------ OO batch terms
-    def oo_(self, d, t3):
-        """Z[ijk][abc] over every ordered (i,j,k) such that the OO batch terms of
-        compute_r3_tri (distr_cc/rccsdt.py:435-732) are sum_{p in OO_SET} Z[p(ijk)][p(abc)].
-
-        With U the unpacked t3 of every ordered triple,
-          Z = - sum Wov[l,b,i,d] U[jkl][d,c,a] + sum G2[l,a,i,d] (U[jkl][d,c,b] + U[jkl][b,d,c])
-              - sum Wov[l,c,i,d] U[jkl][b,d,a] + sum Wvo[l,a,d,i] U[jkl][b,c,d]
-              + sum W_oooo[l,m,j,k] U[lmi][b,c,a] - sum F_oo[l,i] U[ljk][a,b,c],
-          G2[l,a,i,d] = -(Wov[l,a,i,d] + Wvo[l,a,d,i]) / 2,
-        Wov = W_ovov, Wvo = W_ovvo (sums over l and d, or l and m)."""
+    def s_(self, d, t3):
+        """S (see the module docstring); U = unpacked t3 when the OO terms are on."""
         no, nv = self.no, self.nv
-        n3v = nv ** 3
-        _c_rccsdt.take_t3_batched(t3, self.U, self.all_xyz, self.loc, no, nv)
-        U, Z = self.U, self.Z
-        G2 = (-0.5 * (d.W_ovov + d.W_ovvo.permute(0, 1, 3, 2))).permute(2, 1, 0, 3).contiguous()  # [i][x][l][d]
+        S = self.S
+        if self.with_oo:
+            unpack_all_(t3, self.U, no, nv)
         if self.precision == "fp64":
-            Zv = Z.view(no, no, no, nv, nv, nv)
-            e = torch.einsum
-            Zv.copy_(-e('lbid,jkldca->ijkabc', d.W_ovov, U.view(no, no, no, nv, nv, nv)))
-            Zv.add_(e('iald,jkldcb->ijkabc', G2, U.view(no, no, no, nv, nv, nv)))
-            Zv.add_(e('iald,jklbdc->ijkabc', G2, U.view(no, no, no, nv, nv, nv)))
-            Zv.sub_(e('lcid,jklbda->ijkabc', d.W_ovov, U.view(no, no, no, nv, nv, nv)))
-            Zv.add_(e('ladi,jklbcd->ijkabc', d.W_ovvo, U.view(no, no, no, nv, nv, nv)))
+            self._s_fp64(d)
         else:
-            c = contract
-            Zrow = lambda xs: c.two(nv, no * no * n3v, xs)  # noqa: E731  (i, x): x placed at stride xs
-            Zcol = lambda ys, zs: c.three(nv, nv, n3v, ys, zs)  # noqa: E731  (jk, y, z)
-            wov_rows, wov_k = c.two(nv, nv, no * nv), c.two(nv, nv * no * nv, 1)   # Wov[l,x,i,d]
-            g2_rows, g2_k = c.lin(no * nv), c.lin(1)                              # G2[i][x][l][d]
-            wvo_rows, wvo_k = c.two(nv, 1, nv * no), c.two(nv, nv * nv * no, no)  # Wvo[l,x,d,i]
-            urow = lambda ys, zs: c.three(nv, nv, no * n3v, ys, zs)  # noqa: E731  U[j,k,.] rows (jk, y, z)
-            st = self.status
-            # U[jkl][d, y, z]
-            self.ob.fill(U, urow(nv, 1), c.two(nv, n3v, nv * nv))
-            self.oa.fill(d.W_ovov, wov_rows, wov_k)
-            c.gemm_(self.oa, self.ob, Z, Zrow(nv), Zcol(1, nv * nv), -1.0, 0.0, st)       # a=z, b=x, c=y
-            self.oa.fill(G2, g2_rows, g2_k)
-            c.gemm_(self.oa, self.ob, Z, Zrow(nv * nv), Zcol(1, nv), 1.0, 1.0, st)         # a=x, b=z, c=y
-            # U[jkl][y, d, z]
-            self.ob.fill(U, urow(nv * nv, 1), c.two(nv, n3v, nv))
-            c.gemm_(self.oa, self.ob, Z, Zrow(nv * nv), Zcol(nv, 1), 1.0, 1.0, st)         # a=x, b=y, c=z
-            self.oa.fill(d.W_ovov, wov_rows, wov_k)
-            c.gemm_(self.oa, self.ob, Z, Zrow(1), Zcol(nv, nv * nv), -1.0, 1.0, st)        # a=z, b=y, c=x
-            # U[jkl][y, z, d]
-            self.ob.fill(U, urow(nv * nv, nv), c.two(nv, n3v, 1))
-            self.oa.fill(d.W_ovvo, wvo_rows, wvo_k)
-            c.gemm_(self.oa, self.ob, Z, Zrow(nv * nv), Zcol(nv, 1), 1.0, 1.0, st)         # a=x, b=y, c=z
-        # W_oooo and F_oo pieces: bandwidth-bound, FP64 in both precisions
-        Zv = Z.view(no, no, no, nv, nv, nv)
-        G = torch.matmul(d.W_oooo.reshape(no * no, no * no).t(), U.view(no * no, no * n3v))  # [(j,k),(i,b,c,a)]
-        Zv.add_(G.view(no, no, no, nv, nv, nv).permute(2, 0, 1, 5, 3, 4))
-        Z.view(no, -1).sub_(torch.matmul(d.F_oo.t(), U.view(no, -1)))
-        return Z
+            self._s_split(d)
+        if self.with_oo:
+            A, Wa = woooo_foo_matrix(d.W_oooo, d.F_oo)
+            S.view(no * no, -1).addmm_(A, self.U.view(no * no, -1))
+            if Wa is not None:
+                if self.Ganti is None:
+                    self.Ganti = torch.empty_like(self.S)
+                torch.matmul(Wa.reshape(no * no, no * no).t(), self.U.view(no * no, -1),
+                             out=self.Ganti.view(no * no, -1))
+            else:
+                self.Ganti = None
+        return S
+
+    def _s_split(self, d):
+        c, pl, st = contract, self.plan, self.status
+        no, nv = self.no, self.nv
+        S = self.S
+        x = pl["x"]
+        self.xa.fill(d.W_vvvo, *x["a"][0][1:])
+        self.xb.fill(d.t2, *x["b"][0][1:])
+        c.gemm_(self.xa, self.xb, S, *x["out"], x["alpha"], x["beta"], st)
+        if not self.with_oo:
+            return
+        src = {"G2": (-0.5 * (d.W_ovov + d.W_ovvo.permute(0, 1, 3, 2))).permute(2, 1, 0, 3).contiguous(),
+               "Wvo_half": 0.5 * d.W_ovvo, "W_ovov": d.W_ovov, "U": self.U}
+        oo, t1 = pl["oo"], pl["t1"]
+        for i, (name, fm, fk) in enumerate(oo["a"]):
+            self.ooa.fill_piece(i, src[name], fm, fk)
+        for i, (name, fm, fk) in enumerate(oo["b"]):
+            self.oob.fill_piece(i, src[name], fm, fk)
+        name, fm, fk = t1["a"][0]
+        self.t1a.fill(src[name], fm, fk)
+        c.gemm_(self.ooa, self.oob, S, *oo["out"], oo["alpha"], oo["beta"], st)
+        c.gemm_(self.t1a, self.oob, S, *t1["out"], t1["alpha"], t1["beta"], st, Kp=self.t1a.Kp)
+
+    def _s_fp64(self, d):
+        no, nv = self.no, self.nv
+        Sv = self.S.view(no, no, no, nv, nv, nv)
+        Wt = d.W_vvvo.permute(3, 0, 1, 2).reshape(no * nv * nv, nv)
+        T2m = d.t2.permute(0, 1, 3, 2).reshape(no * no * nv, nv)
+        torch.matmul(Wt, T2m.t(), out=self.X)
+        Sv.copy_(self.X.view(no, nv, nv, no, no, nv).permute(3, 0, 4, 1, 2, 5))  # (j,a,b,i,k,c) -> (i,j,k,a,b,c)
+        if not self.with_oo:
+            return
+        Uv = self.U.view(no, no, no, nv, nv, nv)
+        e = torch.einsum
+        G2 = -0.5 * (d.W_ovov + d.W_ovvo.permute(0, 1, 3, 2))
+        Sv.sub_(e('lbid,jkldca->ijkabc', d.W_ovov, Uv))
+        Sv.add_(e('laid,jkldcb->ijkabc', G2, Uv))
+        Sv.add_(e('ladi,jklbcd->ijkabc', 0.5 * d.W_ovvo, Uv))
 
     def fvv_(self, r3, d, t3):
         """F_vv.t3 (distr_cc/rccsdt.py:400-402), FP64 in both precisions (bandwidth-bound)."""
@@ -219,13 +266,12 @@ class T3Residual:
         """r3 = compute_r3_tri for canonical t3 (the OO batch terms included when with_oo)."""
         if r3 is None:
             r3 = torch.empty_like(t3)
-        nv = self.nv
-        X = self.vt2_(d)
-        src = [(X, 1.0, self.x_strides, ALL_S3)]
-        if self.with_oo:
-            Z = self.oo_(d, t3)
-            src.append((Z, 1.0, full_strides(self.no, nv), OO_SET))
-        perm_gather_(r3, d.ijk, nv, 0.0, src)
+        no, nv = self.no, self.nv
+        S = self.s_(d, t3)
+        Y = self.y_(d)
+        perm_gather_(r3, d.ijk, nv, 0.0, [(S, 1.0, full_strides(no, nv), ALL_S3), (Y, -1.0, self.y_strides, ALL_S3)])
+        if self.Ganti is not None:
+            perm_gather_(r3, d.ijk, nv, 1.0, [(self.Ganti, 1.0, full_strides(no, nv), OOOO_SET)])
         self.fvv_(r3, d, t3)
         self.wvvvv_(r3, d, t3)
         return r3

@@ -89,6 +89,12 @@ DCC_API int dcc_take_t3_ijk_single(const double *t3_local, double *t3_blk, const
 DCC_API int dcc_take_t3_batched(const double *t3_local, double *out, const int32_t *ijk, const int64_t *ijk_to_local_idx,
                         int64_t count, int64_t nocc, int64_t nvir, void *stream);
 
+/* U[(x*nocc + y)*nocc + z] = T3[x,y,z] for every ordered occupied triple (U is
+ * DEVICE [nocc^3][nvir^3]) from the canonical blocks of one rank: the
+ * all-orderings form of take_t3_ijk_single_ (src/rccsdt.c:119-129), reading
+ * every canonical block once. */
+DCC_API int dcc_t3_unpack_all(const double *t3, double *U, int64_t nocc, int64_t nvir, void *stream);
+
 /* send_data[r] = t3_local[ijk_to_local_idx[requests[r]]] for stored blocks
  * (DEVICE index arrays).  Replaces fill_local_data_ijk_ (src/rccsdt.c:105-117). */
 DCC_API int dcc_fill_local_data_ijk(const double *t3_local, double *send_data, const int32_t *requests,
@@ -257,6 +263,14 @@ DCC_API int dcc_q_task_epilogue(const double *t4, const double *z4, const double
 DCC_API int dcc_split_operand(const double *src, void *hi, void *lo, int64_t M, int64_t K, int64_t Kp,
                               const int64_t *map10, int kind, void *stream);
 
+/* One piece of a K-concatenated operand: columns [k0, k0 + kw) of pieces
+ * whose rows are ld elements apart, dst[m][k0 + k] = src[map(m) + map(k)] for
+ * k < K and zero for K <= k < kw.  dcc_split_operand is the case k0 = 0,
+ * kw = ld = Kp.  Several einsum strings with the same output permutation
+ * (distr_cc/rccsdt.py:435-732) become one GEMM over the concatenated K. */
+DCC_API int dcc_split_operand_at(const double *src, void *hi, void *lo, int64_t M, int64_t K, int64_t kw,
+                                 int64_t ld, int64_t k0, const int64_t *map10, int kind, void *stream);
+
 /* C[frow(m) + fcol(n)] = alpha * (A_hi B_hi + A_hi B_lo + A_lo B_hi)[m][n]
  * + beta * C, FP32 accumulation in tensor memory (tcgen05), FP64 C.  A is
  * [M][Kp], B is [N][Kp] (pieces from dcc_split_operand), epi10 = {frow, fcol}
@@ -266,6 +280,13 @@ DCC_API int dcc_split_operand(const double *src, void *hi, void *lo, int64_t M, 
 DCC_API int dcc_gemm_split3(const void *A_hi, const void *A_lo, const void *B_hi, const void *B_lo, int64_t M,
                             int64_t N, int64_t Kp, double *C, const int64_t *epi10, double alpha, double beta,
                             int kind, int *status, void *stream);
+
+/* dcc_gemm_split3 over the first Kp columns of pieces whose rows are lda / ldb
+ * elements apart (multiples of 8, >= Kp): one operand of a K-concatenated
+ * pair serves a GEMM that needs only its leading piece. */
+DCC_API int dcc_gemm_split3_ld(const void *A_hi, const void *A_lo, int64_t lda, const void *B_hi, const void *B_lo,
+                               int64_t ldb, int64_t M, int64_t N, int64_t Kp, double *C, const int64_t *epi10,
+                               double alpha, double beta, int kind, int *status, void *stream);
 
 /* Pipeline shape of dcc_gemm_split3 (process-wide): bytes of K per k-block
  * (128, 64 or 32 -> matching TMA/UMMA swizzle), ring depth (2 | 3,4 | 8) and

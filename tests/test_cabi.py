@@ -95,25 +95,40 @@ def test_split_gemm_host_validation_accepts_our_maps(L):
     from dcc import contract as c
     if torch.cuda.is_available():
         pytest.skip("checks the no-device fall-through")
+    from dcc import t3_residual as tr
     fake = ctypes.c_void_p(4096)
     nv, n, no = 90, 220, 10
-    N = no * no * nv
-    splits = [(n * nv, nv * nv, am, ak) for am, ak, _, _ in c.wvvvv_maps(nv)]
-    splits += [(no * nv * nv, nv, c.two(nv * nv, 1, nv * no), c.lin(no)), (no * no * nv, nv, c.two(nv, nv * nv, 1), c.lin(nv)),
-               (no * no * nv, no, c.three(no, nv, no, 1, no ** 3), c.lin(no * no)), (no * nv * nv, no, c.lin(1), c.lin(no * nv * nv))]
-    for M, K, fm, fk in splits:
-        rc = c._split(fake, fake, fake, M, K, c.padded_k(K, 0), c._i64x10(fm, fk), 0, None)
+    K = no * nv
+    plan = tr.s_plan(no, nv)
+    # (M, K, kw, ld, k0, row map, k map) of every split the drivers issue
+    splits = [(n * nv, nv * nv, 8128, 8128, 0, am, ak) for am, ak, _, _ in c.wvvvv_maps(nv)]
+    splits += [(no * nv * nv, nv, 128, 128, 0) + plan["x"]["a"][0][1:],
+               (no * no * nv, nv, 128, 128, 0) + plan["x"]["b"][0][1:],
+               (no * nv, K, 960, 960, 0) + plan["t1"]["a"][0][1:]]
+    for rows, ent in ((no * nv, plan["oo"]["a"]), (no * no * nv * nv, plan["oo"]["b"])):
+        sp = c.Split(rows, kind=0, device="cpu", pieces=[K, K])
+        splits += [(rows, k, w, sp.Kp, off, fm, fk) for (off, k, w), (_, fm, fk) in zip(sp.pieces, ent)]
+    for M, Kk, kw, ld, k0, fm, fk in splits:
+        rc = c._split(fake, fake, fake, M, Kk, kw, ld, k0, c._i64x10(fm, fk), 0, None)
         assert rc == 4, L.last_error()
-    epis = [(n * nv, nv * nv, er, ec) for _, _, er, ec in c.wvvvv_maps(nv)]
-    epis += [(no * nv * nv, N, c.lin(N), c.lin(1)),
-             (no * no * nv, no * nv * nv, c.three(no, nv, no * nv, nv * nv * N, nv * N), c.three(nv, nv, nv, N, 1))]
-    for M, Nn, fr, fc in epis:
-        rc = c._gemm(fake, fake, fake, fake, M, Nn, 128, fake, c._i64x10(fr, fc), 1.0, 1.0, 0, fake, None)
+    # (M, N, Kp, lda, ldb, out maps) of every GEMM
+    epis = [(n * nv, nv * nv, 8128, 8128, 8128, er, ec) for _, _, er, ec in c.wvvvv_maps(nv)]
+    epis += [(no * nv * nv, no * no * nv, 128, 128, 128) + plan["x"]["out"],
+             (no * nv, no * no * nv * nv, 1856, 1856, 1856) + plan["oo"]["out"],
+             (no * nv, no * no * nv * nv, 960, 960, 1856) + plan["t1"]["out"]]
+    for M, Nn, Kp, lda, ldb, fr, fc in epis:
+        rc = c._gemm(fake, fake, lda, fake, fake, ldb, M, Nn, Kp, fake, c._i64x10(fr, fc), 1.0, 1.0, 0, fake, None)
         assert rc == 4, L.last_error()
-    rc = c._gemm(fake, fake, fake, fake, 10, 10, 100, fake, c._i64x10(c.lin(10), c.lin(1)), 1.0, 0.0, 0, fake, None)
+    rc = c._gemm(fake, fake, 100, fake, fake, 100, 10, 10, 100, fake, c._i64x10(c.lin(10), c.lin(1)), 1.0, 0.0, 0,
+                 fake, None)
     assert rc == 2  # Kp not a multiple of 64
-    rc = c._split(fake, fake, fake, 10, 10, 64, c._i64x10((0, 1, 0, 0, 1), c.lin(1)), 0, None)
+    rc = c._gemm(fake, fake, 64, fake, fake, 60, 10, 10, 64, fake, c._i64x10(c.lin(10), c.lin(1)), 1.0, 0.0, 0,
+                 fake, None)
+    assert rc == 2  # ldb < Kp
+    rc = c._split(fake, fake, fake, 10, 10, 64, 64, 0, c._i64x10((0, 1, 0, 0, 1), c.lin(1)), 0, None)
     assert rc == 2  # radix 0
+    rc = c._split(fake, fake, fake, 10, 10, 64, 100, 64, c._i64x10(c.lin(10), c.lin(1)), 0, None)
+    assert rc == 2  # piece runs past the row pitch
 
 
 def test_three_digit_map_helpers():

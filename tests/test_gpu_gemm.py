@@ -73,3 +73,74 @@ def test_every_pipeline_shape(C, cfg, kind):
         assert _rel(got, A @ B.t()) < TOL[kind]
     finally:
         autotune.set_config(*old)
+
+
+@pytest.mark.parametrize("kind", ["bf16x3", "tf32x3"])
+@pytest.mark.parametrize("transposed", [False, True])
+def test_persistent_tiles_and_epilogue_orientation(C, kind, transposed):
+    """More output tiles than two rounds of CTAs (both TMEM accumulators reused
+    several times); beta != 0; output written row-contiguous (lanes along
+    columns) or column-contiguous (lanes along rows)."""
+    M, N, K = 2000, 5000, 128
+    g = torch.Generator(device="cuda").manual_seed(5)
+    A = torch.randn(M, K, dtype=torch.float64, device="cuda", generator=g)
+    B = torch.randn(N, K, dtype=torch.float64, device="cuda", generator=g)
+    k = C.KIND[kind]
+    a = C.Split(M, K, k).fill(A, C.lin(K), C.lin(1))
+    b = C.Split(N, K, k).fill(B, C.lin(K), C.lin(1))
+    C0 = torch.randn(M * N, dtype=torch.float64, device="cuda", generator=g)
+    out = C0.clone()
+    fr, fc = (C.lin(1), C.lin(M)) if transposed else (C.lin(N), C.lin(1))
+    st = C.gemm_(a, b, out, fr, fc, 0.5, -1.0)
+    torch.cuda.synchronize()
+    assert int(st.item()) == 0
+    ref = 0.5 * (A @ B.t())
+    got = (out.view(N, M).t() if transposed else out.view(M, N)) + (C0.view(N, M).t() if transposed else C0.view(M, N))
+    assert _rel(got, ref) < TOL[kind]
+
+
+@pytest.mark.parametrize("kind", ["bf16x3", "tf32x3"])
+def test_concatenated_pieces_and_leading_columns(C, kind):
+    """[A1 | A2] [B1 | B2]^T = A1 B1^T + A2 B2^T over a K-concatenated split, and a
+    GEMM over the leading piece only (ldb > Kp) with an A that covers just that piece."""
+    M, N, K1, K2 = 300, 700, 90, 50
+    g = torch.Generator(device="cuda").manual_seed(6)
+    A1 = torch.randn(M, K1, dtype=torch.float64, device="cuda", generator=g)
+    A2t = torch.randn(K2, M, dtype=torch.float64, device="cuda", generator=g)  # stored k-major
+    B1 = torch.randn(N, K1, dtype=torch.float64, device="cuda", generator=g)
+    B2 = torch.randn(N, K2, dtype=torch.float64, device="cuda", generator=g)
+    k = C.KIND[kind]
+    a = C.Split(M, kind=k, pieces=[K1, K2])
+    a.fill_piece(0, A1, C.lin(K1), C.lin(1)).fill_piece(1, A2t, C.lin(1), C.lin(M))
+    b = C.Split(N, kind=k, pieces=[K1, K2])
+    b.fill_piece(0, B1, C.lin(K1), C.lin(1)).fill_piece(1, B2, C.lin(K2), C.lin(1))
+    out = torch.zeros(M, N, dtype=torch.float64, device="cuda")
+    st = C.gemm_(a, b, out, C.lin(N), C.lin(1), 1.0, 0.0)
+    ref = A1 @ B1.t() + A2t.t() @ B2.t()
+    a1 = C.Split(M, K1, k).fill(A1, C.lin(K1), C.lin(1))
+    out1 = torch.zeros(M, N, dtype=torch.float64, device="cuda")
+    st1 = C.gemm_(a1, b, out1, C.lin(N), C.lin(1), 1.0, 0.0, Kp=a1.Kp)
+    torch.cuda.synchronize()
+    assert int(st.item()) == 0 and int(st1.item()) == 0
+    assert _rel(out, ref) < TOL[kind]
+    assert _rel(out1, A1 @ B1.t()) < TOL[kind]
+
+
+@pytest.mark.parametrize("kind", ["bf16x3", "tf32x3"])
+def test_split_middle_digit_rows(C, kind):
+    """Rows (p, x, y) whose contiguous source index is the middle digit x (the
+    split's third read orientation) give the same GEMM as a plain transpose."""
+    P, X, Yd, K = 6, 40, 7, 33
+    g = torch.Generator(device="cuda").manual_seed(7)
+    src = torch.randn(P, K, Yd, X, dtype=torch.float64, device="cuda", generator=g)  # [p][k][y][x]
+    Bm = torch.randn(50, K, dtype=torch.float64, device="cuda", generator=g)
+    k = C.KIND[kind]
+    # row m = (p, x, y): p stride K*Yd*X, x stride 1, y stride X; k stride Yd*X
+    a = C.Split(P * X * Yd, K, k).fill(src, C.three(X, Yd, K * Yd * X, 1, X), C.lin(Yd * X))
+    b = C.Split(50, K, k).fill(Bm, C.lin(K), C.lin(1))
+    out = torch.zeros(P * X * Yd, 50, dtype=torch.float64, device="cuda")
+    st = C.gemm_(a, b, out, C.lin(50), C.lin(1), 1.0, 0.0)
+    torch.cuda.synchronize()
+    assert int(st.item()) == 0
+    Am = src.permute(0, 3, 2, 1).reshape(P * X * Yd, K)
+    assert _rel(out, Am @ Bm.t()) < TOL[kind]

@@ -312,3 +312,18 @@ def test_q_division_and_factor(C, oracle):
     want2 = oracle.t4_multiply_factor(want.copy(), factor, blk, blk, blk, blk, nocc)
     cq.t4_multiply_factor_(d, dev(factor), blk, blk, blk, blk, nocc)
     assert np.array_equal(host(d), want2)
+
+
+@pytest.mark.parametrize("nocc,nvir", [(1, 3), (3, 5), (4, 9), (3, 17)])
+def test_unpack_all(C, oracle, nocc, nvir):
+    from dcc import t3_residual
+    rng = np.random.default_rng(13)
+    n3 = nocc * (nocc + 1) * (nocc + 2) // 6
+    t3 = rng.standard_normal((n3,) + (nvir,) * 3)
+    loc = np.arange(n3, dtype=np.int64)
+    U = torch.full((nocc ** 3,) + (nvir,) * 3, 7.0, dtype=torch.float64, device="cuda")
+    t3_residual.unpack_all_(dev(t3), U, nocc, nvir)
+    got = host(U)
+    for q, (i, j, k) in enumerate(itertools.product(range(nocc), repeat=3)):
+        want, rc = oracle.take_t3(t3, loc, i, j, k, nocc, nvir)
+        assert rc == 0 and np.array_equal(got[q], want)

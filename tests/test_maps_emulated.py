@@ -28,48 +28,63 @@ NO, NV = 3, 4
 e = np.einsum
 
 
-def test_oo_maps():
+def split_pieces(srcs, M, pieces, Kp):
+    """Emulated K-concatenated Split: piece i = (offset, K_i, width) filled from srcs[i] = (src, fm, fk)."""
+    A = np.zeros((M, Kp))
+    for (off, k, _), (src, fm, fk) in zip(pieces, srcs):
+        A[:, off:off + k] = split(src, M, k, fm, fk)
+    return A
+
+
+def test_s_plan_maps():
+    """The GEMMs of t3_residual.s_plan build S = X + T1 + T2 + T5/2 in S's layout."""
+    import torch
+    from dcc import t3_residual as tr
     no, nv = NO, NV
     rng = np.random.default_rng(1)
+    Wvvvo, t2 = rng.standard_normal((nv, nv, nv, no)), rng.standard_normal((no, no, nv, nv))
     Wov, Wvo = rng.standard_normal((no, nv, no, nv)), rng.standard_normal((no, nv, nv, no))
     U = rng.standard_normal((no, no, no, nv, nv, nv))
-    G2 = (-0.5 * (Wov + Wvo.transpose(0, 1, 3, 2))).transpose(2, 1, 0, 3).copy()
-    ref = (-e('lbid,jkldca->ijkabc', Wov, U) + e('iald,jkldcb->ijkabc', G2, U) + e('iald,jklbdc->ijkabc', G2, U)
-           - e('lcid,jklbda->ijkabc', Wov, U) + e('ladi,jklbcd->ijkabc', Wvo, U))
-    n3v = nv ** 3
-    Z = np.zeros(no ** 3 * n3v)
-    zr = lambda xs: c.two(nv, no * no * n3v, xs)  # noqa: E731
-    zc = lambda ys, zs: c.three(nv, nv, n3v, ys, zs)  # noqa: E731
-    ur = lambda ys, zs: c.three(nv, nv, no * n3v, ys, zs)  # noqa: E731
-    wov = (c.two(nv, nv, no * nv), c.two(nv, nv * no * nv, 1))
-    g2 = (c.lin(no * nv), c.lin(1))
-    wvo = (c.two(nv, 1, nv * no), c.two(nv, nv * nv * no, no))
-    K, M, N = no * nv, no * nv, no * no * nv * nv
-    B0 = split(U, N, K, ur(nv, 1), c.two(nv, n3v, nv * nv))
-    gemm(split(Wov, M, K, *wov), B0, Z, zr(nv), zc(1, nv * nv), -1.0, 0.0)
-    gemm(split(G2, M, K, *g2), B0, Z, zr(nv * nv), zc(1, nv), 1.0, 1.0)
-    B1 = split(U, N, K, ur(nv * nv, 1), c.two(nv, n3v, nv))
-    gemm(split(G2, M, K, *g2), B1, Z, zr(nv * nv), zc(nv, 1), 1.0, 1.0)
-    gemm(split(Wov, M, K, *wov), B1, Z, zr(1), zc(nv, nv * nv), -1.0, 1.0)
-    B2 = split(U, N, K, ur(nv * nv, nv), c.two(nv, n3v, 1))
-    gemm(split(Wvo, M, K, *wvo), B2, Z, zr(nv * nv), zc(nv, 1), 1.0, 1.0)
-    np.testing.assert_allclose(Z.reshape(ref.shape), ref, rtol=0, atol=1e-12)
+    G2 = -0.5 * (Wov + Wvo.transpose(0, 1, 3, 2))  # [l,a,i,d]
+    ref = (e('abdj,ikdc->ijkabc', Wvvvo, t2) - e('lbid,jkldca->ijkabc', Wov, U) + e('laid,jkldcb->ijkabc', G2, U)
+           + 0.5 * e('ladi,jklbcd->ijkabc', Wvo, U))
+    src = {"W_vvvo": Wvvvo, "t2": t2, "W_ovov": Wov, "Wvo_half": 0.5 * Wvo, "U": U,
+           "G2": G2.transpose(2, 1, 0, 3).copy()}
+    plan = tr.s_plan(no, nv)
+    S = np.full(ref.size, np.nan)
+    K = no * nv
+    shapes = {"x": (no * nv * nv, no * no * nv, [nv]), "oo": (no * nv, no * no * nv * nv, [K, K])}
+    ops = {}
+    for key, (M, N, pieces) in shapes.items():
+        sp = c.Split(M, kind=0, device="cpu", pieces=pieces)
+        ent = plan[key]
+        A = split_pieces([(src[n], fm, fk) for n, fm, fk in ent["a"]], M, sp.pieces, sp.Kp)
+        B = split_pieces([(src[n], fm, fk) for n, fm, fk in ent["b"]], N, sp.pieces, sp.Kp)
+        ops[key] = (A, B)
+        if key == "x":
+            S[:] = 0.0  # beta = 0 of the first GEMM overwrites S
+        gemm(A, B, S, *ent["out"], ent["alpha"], ent["beta"])
+    t1 = plan["t1"]
+    sp = c.Split(no * nv, K, 0, device="cpu")
+    A = split_pieces([(src[n], fm, fk) for n, fm, fk in t1["a"]], no * nv, sp.pieces, sp.Kp)
+    B = ops["oo"][1][:, :sp.Kp]  # leading columns of the T2/T5 U operand
+    gemm(A, B, S, *t1["out"], t1["alpha"], t1["beta"])
+    del torch
+    np.testing.assert_allclose(S.reshape(ref.shape), ref, rtol=0, atol=1e-12)
 
 
-def test_xy_maps():
+def test_y_strides():
+    """Y[(i,j,a),(k,b,c)] read through T3Residual.y_strides is Y[ijk][abc]."""
     no, nv = NO, NV
     rng = np.random.default_rng(2)
-    Wvvvo, Wvooo = rng.standard_normal((nv, nv, nv, no)), rng.standard_normal((nv, no, no, no))
-    t2 = rng.standard_normal((no, no, nv, nv))
-    N = no * no * nv
-    X = np.zeros(no * nv * nv * N)
-    gemm(split(Wvvvo, no * nv * nv, nv, c.two(nv * nv, 1, nv * no), c.lin(no)),
-         split(t2, no * no * nv, nv, c.two(nv, nv * nv, 1), c.lin(nv)), X, c.lin(N), c.lin(1), 1.0, 0.0)
-    gemm(split(Wvooo, no * no * nv, no, c.three(no, nv, no, 1, no ** 3), c.lin(no * no)),
-         split(t2, no * nv * nv, no, c.lin(1), c.lin(no * nv * nv)), X,
-         c.three(no, nv, no * nv, nv * nv * N, nv * N), c.three(nv, nv, nv, N, 1), -1.0, 1.0)
-    ref = e('abdj,ikdc->jabikc', Wvvvo, t2) - e('alij,lkbc->jabikc', Wvooo, t2)
-    np.testing.assert_allclose(X.reshape(ref.shape), ref, rtol=0, atol=1e-12)
+    Wvooo, t2 = rng.standard_normal((nv, no, no, no)), rng.standard_normal((no, no, nv, nv))
+    Y = (Wvooo.transpose(2, 3, 0, 1).reshape(no * no * nv, no) @ t2.transpose(1, 2, 3, 0).reshape(no * nv * nv, no).T)
+    Ny = no * nv * nv
+    st = (no * nv * Ny, nv * Ny, nv * nv, Ny, nv, 1)
+    ref = e('alij,lkbc->ijkabc', Wvooo, t2)
+    idx = np.indices(ref.shape).reshape(6, -1)
+    got = Y.ravel()[sum(idx[m] * st[m] for m in range(6))]
+    np.testing.assert_allclose(got, ref.ravel(), rtol=0, atol=1e-13)
 
 
 def test_wvvvv_maps():
