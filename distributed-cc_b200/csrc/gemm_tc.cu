@@ -24,13 +24,16 @@
 #include <stdint.h>
 #include <string.h>
 
+#include "async_util.cuh"
 #include "dcc_common.cuh"
 
 namespace dcc {
 
 constexpr int GM = 128;       // tile rows (UMMA M)
 constexpr int GN = 256;       // tile cols (UMMA N)
-constexpr int G_THREADS = 192;
+// CTA = warp 0 (TMA producer) + warp 1 (MMA issuer) + EPI epilogue warps
+template <int EPI>
+constexpr int gemm_threads() { return 64 + 32 * EPI; }
 
 // Tunable pipeline shape: bytes of K per operand row and k-block (128, 64 or
 // 32 -> 128/64/32-byte swizzle), ring depth, and the number of M-tiles per
@@ -39,7 +42,6 @@ struct GemmConfig {
     int kb_bytes, stages, group_m;
 };
 static GemmConfig g_cfg = {64, 4, 16};
-constexpr uint64_t WAIT_NS = 2000000000ull;  // 2 s bound on any single wait
 
 // off(m) = (m / (R1*R2)) * S0 + ((m / R2) % R1) * S1 + (m % R2) * S2
 struct Map3 {
@@ -54,68 +56,12 @@ struct GemmEpi {
     Map3 row, col;
 };
 
-// ----------------------------------------------------------------- PTX helpers
-
-__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
-
-__device__ __forceinline__ uint64_t globaltimer() {
-    uint64_t t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    return t;
-}
-
-__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count));
-}
-
-__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
-}
-
-__device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
-    uint32_t ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(ok)
-        : "r"(bar), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-
-// Bounded wait: false (and *status set) when the phase did not complete in time.
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, int *status) {
-    if (mbar_try(bar, parity)) return true;
-    uint64_t t0 = globaltimer();
-    for (uint32_t it = 1;; it++) {
-        if (mbar_try(bar, parity)) return true;
-        if ((it & 255) == 0) {
-            if (*(volatile int *)status != 0) return false;  // another role already gave up
-            if (globaltimer() - t0 > WAIT_NS) {
-                atomicExch(status, DCC_ERR_TIMEOUT);
-                return false;
-            }
-        }
-    }
-}
-
-// Bounded wait that reports nothing (used while draining after an abort).
-__device__ __forceinline__ void mbar_wait_quiet(uint32_t bar, uint32_t parity) {
-    uint64_t t0 = globaltimer();
-    while (!mbar_try(bar, parity))
-        if (globaltimer() - t0 > WAIT_NS) return;
-}
-
-__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap *map, uint32_t bar, int c0, int c1) {
-    asm volatile(
-        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];"
-        ::"r"(dst), "l"(map), "r"(bar), "r"(c0), "r"(c1)
-        : "memory");
-}
-
-__device__ __forceinline__ void tma_prefetch_desc(const CUtensorMap *map) {
-    asm volatile("prefetch.tensormap [%0];" ::"l"(map) : "memory");
+// map3 for m < 2^31 and R1*R2 < 2^31 (checked on the host): 32-bit divisions.
+__device__ __forceinline__ int64_t map3_32(const Map3 &f, uint32_t m) {
+    const uint32_t r2 = (uint32_t)f.R2, r12 = (uint32_t)(f.R1 * f.R2);
+    const uint32_t d0 = m / r12, mr = m - d0 * r12;
+    const uint32_t d1 = mr / r2, d2 = mr - d1 * r2;
+    return (int64_t)d0 * f.S0 + (int64_t)d1 * f.S1 + (int64_t)d2 * f.S2;
 }
 
 // K-major, swizzled operand tile with rows of KB bytes (KB = 128/64/32 ->
@@ -181,9 +127,8 @@ struct GemmSmem {
     uint32_t tmem_base;
 };
 
-constexpr int EPI_WARPS = 4;
-// per epilogue warp: a 32x33 float transpose buffer and 32 row (or column) offsets
-constexpr uint32_t EPI_WARP_BYTES = 32 * 33 * 4 + 32 * 8;
+// per epilogue warp: a 32x33 float transpose buffer, 32 row and 32 column offsets
+constexpr uint32_t EPI_WARP_BYTES = 32 * 33 * 4 + 64 * 8;
 
 __device__ __forceinline__ void tile_coords(int t, int num_m, int num_n, int group_m, int &tm, int &tn) {
     const int per_group = group_m * num_n;
@@ -198,8 +143,8 @@ __device__ __forceinline__ void tile_coords(int t, int num_m, int num_n, int gro
 // MMAs of tile t+1 run while the epilogue warps drain tile t.
 // KIND 0: bf16 pieces; KIND 1: tf32 pieces.  KB: bytes of K per row and
 // k-block; ST: ring depth.
-template <int KIND, int KB, int ST>
-__global__ void __launch_bounds__(G_THREADS, 1)
+template <int KIND, int KB, int ST, int EPI>
+__global__ void __launch_bounds__(gemm_threads<EPI>(), 1)
     k_gemm_split3(const __grid_constant__ CUtensorMap tmAh, const __grid_constant__ CUtensorMap tmAl,
                   const __grid_constant__ CUtensorMap tmBh, const __grid_constant__ CUtensorMap tmBl, int M, int N,
                   int nkb, double *C, GemmEpi epi, double alpha, double beta, int *status, int group_m,
@@ -210,7 +155,7 @@ __global__ void __launch_bounds__(G_THREADS, 1)
     constexpr uint32_t A_BYTES = GM * KB, B_BYTES = GN * KB;
     constexpr uint32_t STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;
     uint8_t *epi_base = base + ST * STAGE_BYTES;
-    GemmSmem<ST> *cs = (GemmSmem<ST> *)(epi_base + EPI_WARPS * EPI_WARP_BYTES);
+    GemmSmem<ST> *cs = (GemmSmem<ST> *)(epi_base + EPI * EPI_WARP_BYTES);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int num_m = (M + GM - 1) / GM, num_n = (N + GN - 1) / GN, ntiles = num_m * num_n;
@@ -222,7 +167,7 @@ __global__ void __launch_bounds__(G_THREADS, 1)
         }
         for (int b = 0; b < 2; b++) {
             mbar_init(smem_u32(&cs->acc_full[b]), 1);
-            mbar_init(smem_u32(&cs->acc_empty[b]), EPI_WARPS);
+            mbar_init(smem_u32(&cs->acc_empty[b]), EPI);
         }
         mbar_init(smem_u32(&cs->drain), 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -317,6 +262,9 @@ __global__ void __launch_bounds__(G_THREADS, 1)
     } else if (warp >= 2) {
         // ---------------- epilogue: TMEM -> FP64 C
         const int q = warp & 3;  // TMEM lane quarter of this warp
+        // EPI / 4 warps share a lane quarter, each draining GN * 4 / EPI columns
+        constexpr int CW = GN * 4 / EPI;
+        const int cbeg = ((warp - 2) / 4) * CW, cend = cbeg + CW;
         float *stg = reinterpret_cast<float *>(epi_base + (warp - 2) * EPI_WARP_BYTES);
         int64_t *offs = reinterpret_cast<int64_t *>(epi_base + (warp - 2) * EPI_WARP_BYTES + 32 * 33 * 4);
         int it = 0;
@@ -330,12 +278,13 @@ __global__ void __launch_bounds__(G_THREADS, 1)
             tile_coords(t, num_m, num_n, group_m, tm, tn);
             const int m0 = tm * GM + q * 32, n0 = tn * GN;  // first row of this warp, first column of the tile
             const int m = m0 + lane;
-            const int64_t roff = map3(epi.row, (int64_t)m);
-            if (epi_cols) offs[lane] = roff;
-            for (int c = 0; c < GN; c += 32) {
+            const int64_t roff = map3_32(epi.row, (uint32_t)(m < M ? m : 0));
+            const int nrow = (M - m0) < 32 ? (M - m0) : 32;
+            offs[lane] = roff;  // cols mode: row offsets of the warp's 32 rows
+            for (int c = cbeg; c < cend; c += 32) {
                 float v[32];
                 tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * GN + c), v);
-                if (c == GN - 32) {
+                if (c == cend - 32) {
                     // the accumulator is in registers: hand it back to the MMA warp
                     tc_fence_before();
                     __syncwarp();
@@ -345,44 +294,52 @@ __global__ void __launch_bounds__(G_THREADS, 1)
                 }
                 const int col = n0 + c + lane;
                 const bool cval = col < N;
-                const int64_t coff = map3(epi.col, (int64_t)(cval ? col : 0));
+                const int64_t coff = map3_32(epi.col, (uint32_t)(cval ? col : 0));
                 if (epi_cols) {
                     // lanes walk the 32 columns of one row at a time (columns contiguous in C)
 #pragma unroll
                     for (int j = 0; j < 32; j++) stg[lane * 33 + j] = v[j];
                     __syncwarp();
-                    const int nrow = (M - m0) < 32 ? (M - m0) : 32;
+                    double *cp = C + coff;
+                    const bool full_chunk = __all_sync(0xffffffffu, cval) && nrow == 32;
                     if (beta == 0.0) {
+                        if (full_chunk) {
 #pragma unroll 8
-                        for (int r = 0; r < 32; r++)
-                            if (cval && r < nrow) C[offs[r] + coff] = alpha * (double)stg[r * 33 + lane];
-                    } else {
+                            for (int r = 0; r < 32; r++) cp[offs[r]] = alpha * (double)stg[r * 33 + lane];
+                        } else {
+                            for (int r = 0; r < nrow; r++)
+                                if (cval) cp[offs[r]] = alpha * (double)stg[r * 33 + lane];
+                        }
+                    } else if (full_chunk) {
                         double old[32];
 #pragma unroll
-                        for (int r = 0; r < 32; r++)
-                            old[r] = (cval && r < nrow) ? __ldcg(C + offs[r] + coff) : 0.0;
+                        for (int r = 0; r < 32; r++) old[r] = __ldcg(cp + offs[r]);
 #pragma unroll
-                        for (int r = 0; r < 32; r++)
-                            if (cval && r < nrow) C[offs[r] + coff] = fma(beta, old[r], alpha * (double)stg[r * 33 + lane]);
+                        for (int r = 0; r < 32; r++) cp[offs[r]] = fma(beta, old[r], alpha * (double)stg[r * 33 + lane]);
+                    } else {
+                        for (int r = 0; r < nrow; r++)
+                            if (cval) cp[offs[r]] = fma(beta, __ldcg(cp + offs[r]), alpha * (double)stg[r * 33 + lane]);
                     }
                     __syncwarp();
                 } else {
                     // lanes are rows (rows contiguous in C): each thread writes its row's 32 columns
-                    offs[lane] = coff;
+                    int64_t *coffs = offs + 32;
+                    coffs[lane] = coff;
                     __syncwarp();
                     const int nvalid = (N - n0 - c) < 32 ? (N - n0 - c) : 32;
                     if (m < M) {
+                        double *rp = C + roff;
                         if (beta == 0.0) {
 #pragma unroll
                             for (int j = 0; j < 32; j++)
-                                if (j < nvalid) C[roff + offs[j]] = alpha * (double)v[j];
+                                if (j < nvalid) rp[coffs[j]] = alpha * (double)v[j];
                         } else {
                             double old[32];
 #pragma unroll
-                            for (int j = 0; j < 32; j++) old[j] = (j < nvalid) ? __ldcg(C + roff + offs[j]) : 0.0;
+                            for (int j = 0; j < 32; j++) old[j] = (j < nvalid) ? __ldcg(rp + coffs[j]) : 0.0;
 #pragma unroll
                             for (int j = 0; j < 32; j++)
-                                if (j < nvalid) C[roff + offs[j]] = fma(beta, old[j], alpha * (double)v[j]);
+                                if (j < nvalid) rp[coffs[j]] = fma(beta, old[j], alpha * (double)v[j]);
                         }
                     }
                     __syncwarp();
@@ -522,22 +479,6 @@ static bool map3_ok(const int64_t *f) { return f[0] >= 1 && f[1] >= 1 && f[0] * 
 
 // ----------------------------------------------------------------- host side
 
-typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
-                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
-                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
-
-static EncodeTiledFn encode_fn() {
-    static EncodeTiledFn fn = nullptr;
-    if (!fn) {
-        void *p = nullptr;
-        cudaDriverEntryPointQueryResult q;
-        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
-            q == cudaDriverEntryPointSuccess)
-            fn = (EncodeTiledFn)p;
-    }
-    return fn;
-}
-
 // 2-D K-major piece [rows][Kp] with a (k-block x box_rows) box and the
 // swizzle that matches kb_bytes.
 static int make_map(CUtensorMap *map, const void *ptr, int kind, int64_t rows, int64_t Kp, int64_t ld,
@@ -564,27 +505,27 @@ static int make_map(CUtensorMap *map, const void *ptr, int kind, int64_t rows, i
     return DCC_OK;
 }
 
-template <int ST>
+template <int ST, int EPI>
 static size_t gemm_smem_bytes(int kb_bytes) {
-    return 1024 + ST * (size_t)(2 * GM * kb_bytes + 2 * GN * kb_bytes) + EPI_WARPS * EPI_WARP_BYTES +
+    return 1024 + ST * (size_t)(2 * GM * kb_bytes + 2 * GN * kb_bytes) + EPI * EPI_WARP_BYTES +
            sizeof(GemmSmem<ST>);
 }
 
-template <int KIND, int KB, int ST>
+template <int KIND, int KB, int ST, int EPI>
 static int gemm_launch(const CUtensorMap &a, const CUtensorMap &b, const CUtensorMap &c, const CUtensorMap &d, int M,
                        int N, int nkb, double *C, const GemmEpi &epi, double alpha, double beta, int *status,
                        int group_m, cudaStream_t st) {
     // write along columns when the column map's fastest digit is contiguous,
     // along rows when only the row map's is
     const int epi_cols = (epi.col.S2 == 1 || epi.row.S2 != 1) ? 1 : 0;
-    size_t smem = gemm_smem_bytes<ST>(KB);
+    size_t smem = gemm_smem_bytes<ST, EPI>(KB);
     const int64_t tiles = (int64_t)ceil_div(N, GN) * (int64_t)ceil_div(M, GM);
     DCC_REQUIRE(tiles < (1ll << 31), DCC_ERR_SHAPE, "too many output tiles");
     int dev = 0, nsm = 148;
     if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     const unsigned grid = (unsigned)(tiles < nsm ? tiles : nsm);  // persistent: one CTA per SM
-    cudaFuncSetAttribute(k_gemm_split3<KIND, KB, ST>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k_gemm_split3<KIND, KB, ST><<<grid, G_THREADS, smem, st>>>(a, b, c, d, M, N, nkb, C, epi, alpha, beta, status,
+    cudaFuncSetAttribute(k_gemm_split3<KIND, KB, ST, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_gemm_split3<KIND, KB, ST, EPI><<<grid, gemm_threads<EPI>(), smem, st>>>(a, b, c, d, M, N, nkb, C, epi, alpha, beta, status,
                                                                 group_m, epi_cols);
     return launch_status("gemm_split3");
 }
@@ -653,19 +594,27 @@ extern "C" int dcc_gemm_split3_ld(const void *A_hi, const void *A_lo, int64_t ld
     const GemmConfig cfg = g_cfg;
     DCC_REQUIRE(Kp % (cfg.kb_bytes / (kind == 0 ? 2 : 4)) == 0, DCC_ERR_SHAPE,
                 "Kp (%lld) must be a multiple of the k-block", (long long)Kp);
+    // Short contractions are bound by the FP64 epilogue: eight epilogue warps
+    // (two per TMEM lane quarter) double its memory parallelism; the ring then
+    // is three 64-byte stages to make room for their staging buffers.
+    const int esz = kind == 0 ? 2 : 4;
+    const bool wide_epi = Kp <= 4096;
+    const int kb = wide_epi ? 64 : cfg.kb_bytes;
     CUtensorMap mAh, mAl, mBh, mBl;
     int rc;
-    if ((rc = make_map(&mAh, A_hi, kind, M, Kp, lda, GM, cfg.kb_bytes)) ||
-        (rc = make_map(&mAl, A_lo, kind, M, Kp, lda, GM, cfg.kb_bytes)) ||
-        (rc = make_map(&mBh, B_hi, kind, N, Kp, ldb, GN, cfg.kb_bytes)) ||
-        (rc = make_map(&mBl, B_lo, kind, N, Kp, ldb, GN, cfg.kb_bytes)))
+    if ((rc = make_map(&mAh, A_hi, kind, M, Kp, lda, GM, kb)) || (rc = make_map(&mAl, A_lo, kind, M, Kp, lda, GM, kb)) ||
+        (rc = make_map(&mBh, B_hi, kind, N, Kp, ldb, GN, kb)) || (rc = make_map(&mBl, B_lo, kind, N, Kp, ldb, GN, kb)))
         return rc;
     cudaStream_t st = as_stream(stream);
-    const int nkb = (int)(Kp / (cfg.kb_bytes / (kind == 0 ? 2 : 4)));
+    const int nkb = (int)(Kp / (kb / esz));
     const int iM = (int)M, iN = (int)N, gm = cfg.group_m;
+    if (wide_epi) {
+        if (kind == 0) return gemm_launch<0, 64, 3, 8>(mAh, mAl, mBh, mBl, iM, iN, nkb, C, epi, alpha, beta, status, gm, st);
+        return gemm_launch<1, 64, 3, 8>(mAh, mAl, mBh, mBl, iM, iN, nkb, C, epi, alpha, beta, status, gm, st);
+    }
 #define DCC_GEMM_CASE(K_, KB_, ST_)                                                                           \
     if (kind == K_ && cfg.kb_bytes == KB_ && cfg.stages == ST_)                                              \
-        return gemm_launch<K_, KB_, ST_>(mAh, mAl, mBh, mBl, iM, iN, nkb, C, epi, alpha, beta, status, gm, st);
+        return gemm_launch<K_, KB_, ST_, 4>(mAh, mAl, mBh, mBl, iM, iN, nkb, C, epi, alpha, beta, status, gm, st);
     DCC_GEMM_CASE(0, 128, 2)
     DCC_GEMM_CASE(0, 64, 4)
     DCC_GEMM_CASE(0, 64, 3)

@@ -12,6 +12,7 @@
 #include <stdarg.h>
 #include <string.h>
 
+#include "async_util.cuh"
 #include "dcc_common.cuh"
 
 namespace dcc {
@@ -1156,6 +1157,325 @@ extern "C" int dcc_t3_s3_gather(double *r3, const int32_t *ijk, int64_t nblocks,
     int masks[2] = {63, 63};
     if (u1) DCC_REQUIRE(strides1, DCC_ERR_NULL, "strides1 is NULL");
     return dcc_t3_perm_gather(r3, ijk, nblocks, nvir, beta, u1 ? 2 : 1, bases, scales, st, masks, stream);
+}
+
+// ---------------------------------------------------------------- permutation gather, TMA pipeline
+
+namespace dcc {
+
+constexpr int TG_WARPS = 8;                   // compute warps
+constexpr int TG_THREADS = 32 * (TG_WARPS + 1);  // + one producer warp
+constexpr uint32_t TG_TILE_BYTES = TE3 * 8;   // one dense 8x8x8 FP64 tile
+constexpr int TG_SMEM_BUDGET = 200 * 1024;
+
+struct TmaMaps {
+    CUtensorMap m[PG_MAX_SRC + 1];  // sources, then r3
+};
+
+struct TmaGatherArgs {
+    int nslot;  // (source, permutation) pairs
+    double slot_scale[PG_MAX_SLOTS];
+    int slot_perm[PG_MAX_SLOTS];
+    // per load (slots, then the r3 tile): map, output-tile axis feeding c / b / a,
+    // block-coordinate coefficients of (o_x, o_y, o_z) for the two block dims,
+    // and the logical coordinate (c, b, a, block 0, block 1) of each TMA dim
+    int map[PG_MAX_SLOTS + 1];
+    int tax[PG_MAX_SLOTS + 1][3];
+    int cb0[PG_MAX_SLOTS + 1][3], cb1[PG_MAX_SLOTS + 1][3];
+    int sel[PG_MAX_SLOTS + 1][5];
+};
+
+__device__ __forceinline__ int pick5(int k, int v0, int v1, int v2, int v3, int v4) {
+    return k == 0 ? v0 : (k == 1 ? v1 : (k == 2 ? v2 : (k == 3 ? v3 : v4)));
+}
+
+// Element of the 8^3 tile owned by thread t (0..255), half h.  A linear map
+// over GF(2) of the thread bits chosen so that, for every simultaneous
+// permutation p, the 32 lanes of a warp reading position p(u) of a dense
+// [a][b][c] tile touch each 8-byte bank pair exactly twice (the minimum for
+// 256 bytes), i.e. all six permuted read patterns are conflict-free.
+__device__ __forceinline__ void tg_element(int t, int h, int u[3]) {
+    const int l = t & 31, w = t >> 5;
+    const int l0 = l & 1, l1 = (l >> 1) & 1, l2 = (l >> 2) & 1, l3 = (l >> 3) & 1, l4 = (l >> 4) & 1;
+    u[0] = l & 7;
+    u[1] = l3 | (l4 << 1) | ((l1 ^ l2 ^ (w & 1)) << 2);
+    u[2] = (l1 ^ l3 ^ ((w >> 1) & 1)) | ((l2 ^ l4 ^ ((w >> 2) & 1)) << 1) | ((l0 ^ l1 ^ h) << 2);
+}
+
+__device__ __forceinline__ void named_sync_compute() { asm volatile("bar.sync 1, %0;" ::"n"(32 * TG_WARPS) : "memory"); }
+
+// Persistent gather: work item w = (block q, output tile T).  Warp 8 issues
+// one TMA box load per (source, permutation) slot (plus the r3 tile when
+// beta != 0) into a ring of stages; warps 0..7 sum the slots from shared
+// memory, write the output tile densely and one thread stores it with TMA
+// (out-of-range elements of edge tiles are clipped by the copy engine).
+// Every mbarrier wait is bounded; after a timeout the CTA finishes its
+// iterations without waiting or storing so the named barriers stay matched.
+__global__ void __launch_bounds__(TG_THREADS, 1)
+    k_perm_gather_tma(const __grid_constant__ TmaMaps maps, const int32_t *ijk, int64_t nwork, int ntile, double beta,
+                      TmaGatherArgs g, int stages, int *status) {
+    extern __shared__ __align__(1024) uint8_t tg_smem[];
+    uint8_t *base = (uint8_t *)(((uintptr_t)tg_smem + 1023) & ~(uintptr_t)1023);
+    const int nload = g.nslot + (beta != 0.0 ? 1 : 0);
+    const uint32_t stage_bytes = (uint32_t)nload * TG_TILE_BYTES;
+    double *outb = (double *)(base + (size_t)stages * stage_bytes);  // 2 output tiles
+    uint64_t *full = (uint64_t *)(base + (size_t)stages * stage_bytes + 2 * TG_TILE_BYTES);
+    uint64_t *empty = full + stages;
+    const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+    const int nt3 = ntile * ntile * ntile;
+    if (t == 0) {
+        for (int s = 0; s < stages; s++) {
+            mbar_init(smem_u32(&full[s]), 1);
+            mbar_init(smem_u32(&empty[s]), TG_WARPS);
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+
+    if (warp == TG_WARPS) {
+        // ---------------- producer warp: lane l issues load l of each work item
+        if (lane <= PG_MAX_SRC) tma_prefetch_desc(&maps.m[lane]);
+        int64_t it = 0;
+        for (int64_t w = blockIdx.x; w < nwork; w += gridDim.x, it++) {
+            const int s = (int)(it % stages);
+            const uint32_t ph = (uint32_t)(it / stages) & 1u;
+            bool ok = lane == 0 ? mbar_wait(smem_u32(&empty[s]), ph ^ 1u, status) : true;
+            ok = __shfl_sync(0xffffffffu, ok, 0);
+            if (!ok) break;
+            const uint32_t fb = smem_u32(&full[s]);
+            if (lane == 0) mbar_expect_tx(fb, (uint32_t)nload * TG_TILE_BYTES);
+            __syncwarp();
+            if (lane < nload) {
+                const int64_t q = w / nt3;
+                const int T = (int)(w % nt3);
+                const int TT[3] = {T / (ntile * ntile), (T / ntile) % ntile, T % ntile};
+                const int o0 = ijk[3 * q], o1 = ijk[3 * q + 1], o2 = ijk[3 * q + 2];
+                const int l = lane;
+                const int vc = TT[g.tax[l][0]] * TE, vb = TT[g.tax[l][1]] * TE, va = TT[g.tax[l][2]] * TE;
+                int v3 = o0 * g.cb0[l][0] + o1 * g.cb0[l][1] + o2 * g.cb0[l][2];
+                const int v4 = o0 * g.cb1[l][0] + o1 * g.cb1[l][1] + o2 * g.cb1[l][2];
+                if (l == g.nslot) v3 = (int)q;  // the r3 tile
+                tma_load_5d(smem_u32(base + (size_t)s * stage_bytes + (size_t)l * TG_TILE_BYTES), &maps.m[g.map[l]], fb,
+                            pick5(g.sel[l][0], vc, vb, va, v3, v4), pick5(g.sel[l][1], vc, vb, va, v3, v4),
+                            pick5(g.sel[l][2], vc, vb, va, v3, v4), pick5(g.sel[l][3], vc, vb, va, v3, v4),
+                            pick5(g.sel[l][4], vc, vb, va, v3, v4));
+            }
+        }
+        // no copy may still be landing in this CTA's shared memory when it exits (the compute
+        // warps stop waiting for them after a timeout): wait, bounded, for the last ones issued
+        if (lane == 0) {
+            const int64_t first = it > stages ? it - stages : 0;
+            for (int64_t k = first; k < it; k++)
+                mbar_wait_quiet(smem_u32(&full[k % stages]), (uint32_t)(k / stages) & 1u);
+        }
+        return;
+    }
+
+    // ---------------- compute warps
+    int rd[PG_MAX_SLOTS][2];
+    int oidx[2];
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+        int u[3];
+        tg_element(t, h, u);
+        oidx[h] = u[0] * 64 + u[1] * 8 + u[2];
+#pragma unroll
+        for (int sl = 0; sl < PG_MAX_SLOTS; sl++) {
+            const int p = sl < g.nslot ? g.slot_perm[sl] : 0;
+            rd[sl][h] = sl * TE3 + u[perm3(p, 0)] * 64 + u[perm3(p, 1)] * 8 + u[perm3(p, 2)];
+        }
+    }
+    bool dry = false;
+    int64_t it = 0;
+    for (int64_t w = blockIdx.x; w < nwork; w += gridDim.x, it++) {
+        const int s = (int)(it % stages);
+        const uint32_t ph = (uint32_t)(it / stages) & 1u;
+        if (!dry && !mbar_wait(smem_u32(&full[s]), ph, status)) dry = true;
+        const double *st = (const double *)(base + (size_t)s * stage_bytes);
+        double acc[2];
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            double a = 0.0;
+#pragma unroll
+            for (int sl = 0; sl < PG_MAX_SLOTS; sl++)
+                if (sl < g.nslot) a = fma(g.slot_scale[sl], st[rd[sl][h]], a);
+            acc[h] = beta != 0.0 ? fma(beta, st[g.nslot * TE3 + oidx[h]], a) : a;
+        }
+        __syncwarp();
+        if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&empty[s])) : "memory");
+        double *ob = outb + (it & 1) * TE3;
+        if (t == 0) bulk_wait_read<1>();  // the store of two items ago has read this buffer
+        named_sync_compute();
+        ob[oidx[0]] = acc[0];
+        ob[oidx[1]] = acc[1];
+        fence_proxy_async_smem();
+        named_sync_compute();
+        if (t == 0 && !dry) {
+            const int64_t q = w / nt3;
+            const int T = (int)(w % nt3);
+            const int vc = (T % ntile) * TE, vb = ((T / ntile) % ntile) * TE, va = (T / (ntile * ntile)) * TE;
+            const int v3 = (int)q;
+            const int *sl = g.sel[PG_MAX_SLOTS];
+            tma_store_5d(&maps.m[PG_MAX_SRC], smem_u32(ob), pick5(sl[0], vc, vb, va, v3, 0),
+                         pick5(sl[1], vc, vb, va, v3, 0), pick5(sl[2], vc, vb, va, v3, 0),
+                         pick5(sl[3], vc, vb, va, v3, 0), pick5(sl[4], vc, vb, va, v3, 0));
+            bulk_commit();
+        }
+    }
+    if (t == 0) bulk_wait<0>();
+}
+
+// Tensor map over a strided FP64 array given as (extent, stride in elements)
+// pairs with the unit-stride dimension first; the other dimensions are
+// ordered by stride, and pos[k] records where input dimension k went.
+static int encode_strided(CUtensorMap *map, const double *base, const int64_t ext[5], const int64_t str[5],
+                          const uint32_t box[5], int pos[5]) {
+    EncodeTiledFn fn = encode_fn();
+    if (!fn) {
+        set_error("cuTensorMapEncodeTiled is unavailable");
+        return DCC_ERR_CUDA;
+    }
+    int order[5] = {0, 1, 2, 3, 4};
+    for (int i = 1; i < 5; i++)  // insertion sort of dims 1..4 by stride
+        for (int j = i; j > 1 && str[order[j]] < str[order[j - 1]]; j--) {
+            int tmp = order[j];
+            order[j] = order[j - 1];
+            order[j - 1] = tmp;
+        }
+    cuuint64_t dims[5], strides[4];
+    cuuint32_t bx[5], es[5] = {1, 1, 1, 1, 1};
+    for (int i = 0; i < 5; i++) {
+        dims[i] = (cuuint64_t)ext[order[i]];
+        bx[i] = box[order[i]];
+        pos[order[i]] = i;
+        if (i > 0) strides[i - 1] = (cuuint64_t)(str[order[i]] * 8);
+    }
+    CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 5, const_cast<double *>(base), dims, strides, bx, es,
+                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) {
+        set_error("cuTensorMapEncodeTiled failed (%d)", (int)r);
+        return DCC_ERR_CUDA;
+    }
+    return DCC_OK;
+}
+
+// Block dimensions of a source as one or two TMA dims: the three block strides
+// (x, y, z) collapse when one is nocc times another.  Returns false when they
+// do not.
+static bool block_dims(const int64_t st[3], int64_t no, int64_t ext[2], int64_t str[2], int c1[3], int c2[3]) {
+    for (int i = 0; i < 3; i++) c1[i] = c2[i] = 0;
+    // all three merge: st[p] = no^2 st[r], st[q] = no st[r]
+    for (int p = 0; p < 3; p++)
+        for (int q = 0; q < 3; q++) {
+            const int r = 3 - p - q;
+            if (p == q || r < 0 || r > 2 || r == p || r == q) continue;
+            if (st[p] == no * st[q] && st[q] == no * st[r]) {
+                ext[0] = no * no * no, str[0] = st[r], ext[1] = 1, str[1] = st[p] * no;
+                c1[p] = (int)(no * no), c1[q] = (int)no, c1[r] = 1;
+                return true;
+            }
+        }
+    for (int p = 0; p < 3; p++)
+        for (int q = 0; q < 3; q++) {
+            if (p == q) continue;
+            const int r = 3 - p - q;
+            if (st[p] == no * st[q]) {
+                ext[0] = no * no, str[0] = st[q], ext[1] = no, str[1] = st[r];
+                c1[p] = (int)no, c1[q] = 1, c2[r] = 1;
+                return true;
+            }
+        }
+    return false;
+}
+
+}  // namespace dcc
+
+extern "C" int dcc_t3_perm_gather_tma(double *r3, const int32_t *ijk, int64_t nblocks, int64_t nocc, int64_t nvir,
+                                      double beta, int nsrc, const double *const *bases, const double *scales,
+                                      const int64_t *strides, const int *masks, int *status, void *stream) {
+    clear_error();
+    DCC_REQUIRE(nblocks >= 0 && nvir >= 0 && nocc >= 0, DCC_ERR_SHAPE, "negative size");
+    DCC_REQUIRE(nsrc >= 1 && nsrc <= PG_MAX_SRC, DCC_ERR_SHAPE, "1..%d sources", PG_MAX_SRC);
+    if (nblocks == 0 || nvir == 0) return DCC_OK;
+    DCC_REQUIRE(r3 && ijk && bases && scales && strides && masks && status, DCC_ERR_NULL, "NULL argument");
+    // the copy engine needs 16-byte strides, a unit-stride c and b faster than a; otherwise the
+    // cp.async kernel serves the call
+    bool tma = nvir % 2 == 0 && nocc >= 1 && nocc <= 1290 && nvir <= 65536;
+    TmaGatherArgs g{};
+    TmaMaps maps;
+    memset(&maps, 0, sizeof(maps));
+    int nslot = 0;
+    for (int s = 0; s < nsrc && tma; s++) {
+        const int64_t *st = strides + 6 * s;
+        DCC_REQUIRE(bases[s], DCC_ERR_NULL, "source %d is NULL", s);
+        DCC_REQUIRE(masks[s] > 0 && masks[s] < 64, DCC_ERR_SHAPE, "source %d: permutation mask must be in 1..63", s);
+        bool even = true;
+        for (int m = 0; m < 5; m++) even = even && st[m] > 0 && st[m] % 2 == 0;
+        if (!even || st[5] != 1 || st[4] >= st[3] || ((uintptr_t)bases[s] & 15)) {
+            tma = false;
+            break;
+        }
+        int64_t bext[2], bstr[2];
+        int c1[3], c2[3];
+        if (!block_dims(st, nocc, bext, bstr, c1, c2)) {
+            tma = false;
+            break;
+        }
+        const int64_t ext[5] = {nvir, nvir, nvir, bext[0], bext[1]};
+        const int64_t str[5] = {1, st[4], st[3], bstr[0], bstr[1]};
+        const uint32_t box[5] = {TE, TE, TE, 1, 1};
+        int pos[5];
+        int rc = encode_strided(&maps.m[s], bases[s], ext, str, box, pos);
+        if (rc) return rc;
+        for (int p = 0; p < 6; p++)
+            if (masks[s] & (1 << p)) {
+                DCC_REQUIRE(nslot < PG_MAX_SLOTS, DCC_ERR_UNSUPPORTED, "more than %d source tiles", PG_MAX_SLOTS);
+                const int P[3] = {perm3(p, 0), perm3(p, 1), perm3(p, 2)};
+                g.slot_perm[nslot] = p;
+                g.slot_scale[nslot] = scales[s];
+                g.map[nslot] = s;
+                // slot tile = p(T): its c / b / a tiles are T[P2] / T[P1] / T[P0]; its block is
+                // (o[P0], o[P1], o[P2]) as the source's (x, y, z)
+                g.tax[nslot][0] = P[2], g.tax[nslot][1] = P[1], g.tax[nslot][2] = P[0];
+                for (int m = 0; m < 3; m++) {
+                    g.cb0[nslot][P[m]] = c1[m];
+                    g.cb1[nslot][P[m]] = c2[m];
+                }
+                for (int k = 0; k < 5; k++) g.sel[nslot][pos[k]] = k;
+                nslot++;
+            }
+    }
+    if (!tma || ((uintptr_t)r3 & 15))
+        return dcc_t3_perm_gather(r3, ijk, nblocks, nvir, beta, nsrc, bases, scales, strides, masks, stream);
+    g.nslot = nslot;
+    {
+        const int64_t ext[5] = {nvir, nvir, nvir, nblocks, 1};
+        const int64_t str[5] = {1, nvir, nvir * nvir, nvir * nvir * nvir, nvir * nvir * nvir * nblocks};
+        const uint32_t box[5] = {TE, TE, TE, 1, 1};
+        int pos[5];
+        int rc = encode_strided(&maps.m[PG_MAX_SRC], r3, ext, str, box, pos);
+        if (rc) return rc;
+        // the r3 tile (load slot nslot when beta != 0, and the store): tile (a, b, c) = T, block q
+        for (int k = 0; k < 5; k++) g.sel[PG_MAX_SLOTS][pos[k]] = k;
+        g.map[nslot] = PG_MAX_SRC;
+        g.tax[nslot][0] = 2, g.tax[nslot][1] = 1, g.tax[nslot][2] = 0;
+        for (int k = 0; k < 5; k++) g.sel[nslot][k] = g.sel[PG_MAX_SLOTS][k];
+    }
+    const int ntile = (int)ceil_div(nvir, TE);
+    const int64_t nwork = nblocks * ntile * ntile * ntile;
+    const int nload = nslot + (beta != 0.0 ? 1 : 0);
+    int stages = (int)((TG_SMEM_BUDGET - 2 * TG_TILE_BYTES) / (nload * TG_TILE_BYTES));
+    stages = stages > 8 ? 8 : stages;
+    DCC_REQUIRE(stages >= 2, DCC_ERR_UNSUPPORTED, "too many source tiles for the pipeline");
+    const size_t smem = 1024 + (size_t)stages * nload * TG_TILE_BYTES + 2 * TG_TILE_BYTES + 2 * stages * 8;
+    int dev = 0, nsm = 148;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    const int64_t grid = nwork < nsm ? nwork : nsm;
+    cudaFuncSetAttribute(k_perm_gather_tma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_perm_gather_tma<<<(unsigned)grid, TG_THREADS, smem, as_stream(stream)>>>(maps, ijk, nwork, ntile, beta, g, stages,
+                                                                               status);
+    return launch_status("t3_perm_gather_tma");
 }
 
 // ---------------------------------------------------------------- no-allocation update

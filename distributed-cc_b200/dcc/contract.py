@@ -152,7 +152,13 @@ def wvvvv_maps(nv):
 
 
 class WvvvvT3:
-    """Split-precision W_vvvv . t3 for a fixed (nblocks, nvir); buffers are reused across calls."""
+    """Split-precision W_vvvv . t3 for a fixed (nblocks, nvir); buffers are reused across calls.
+
+    With F given, the three F_vv . t3 strings (distr_cc/rccsdt.py:400-402) ride
+    along in the same GEMMs: over the contraction pair (d,e),
+      'ad,dbc' + 'bd,adc' = (F[a,d] delta(b,e) + delta(a,d) F[b,e]) t3[q,d,e,c]   (first GEMM)
+      'cd,abd'            = delta(b,d) F[c,e] t3[q,a,d,e]                          (third GEMM)
+    so the first and third GEMMs take W plus those rank-deficient terms."""
 
     def __init__(self, nblocks, nvir, kind="bf16x3", device="cuda"):
         self.n, self.nv, self.kind = int(nblocks), int(nvir), KIND[kind]
@@ -161,15 +167,29 @@ class WvvvvT3:
         self.A = Split(self.n * nvir, K, self.kind, device)
         self.status = torch.zeros(1, dtype=torch.int32, device=device)
         self.maps = wvvvv_maps(nvir)
+        self.WF = None
 
-    def __call__(self, r3, W, t3, alpha=1.0):
+    def __call__(self, r3, W, t3, alpha=1.0, F=None):
         nv = self.nv
         L.as_tensor(r3, f64, "r3")
         L.as_tensor(t3, f64, "t3")
-        self.W.fill(W.reshape(nv * nv, nv * nv), lin(nv * nv), lin(1))
-        for am, ak, er, ec in self.maps:
+        if F is None:
+            ws = [self.W.fill(W.reshape(nv * nv, nv * nv), lin(nv * nv), lin(1))] * 3
+        else:
+            if self.WF is None:
+                self.WF = [Split(nv * nv, nv * nv, self.kind, r3.device) for _ in range(2)]
+            W1 = W.clone()
+            W1.diagonal(0, 1, 3).add_(F.unsqueeze(2))  # F[a,d] delta(b,e)
+            W1.diagonal(0, 0, 2).add_(F.unsqueeze(2))  # delta(a,d) F[b,e]
+            self.WF[0].fill(W1.reshape(nv * nv, nv * nv), lin(nv * nv), lin(1))
+            W1.copy_(W)
+            W1.diagonal(0, 0, 2).add_(F.unsqueeze(2))  # delta(b,d) F[c,e]
+            self.WF[1].fill(W1.reshape(nv * nv, nv * nv), lin(nv * nv), lin(1))
+            del W1
+            ws = [self.WF[0], self.W.fill(W.reshape(nv * nv, nv * nv), lin(nv * nv), lin(1)), self.WF[1]]
+        for (am, ak, er, ec), w in zip(self.maps, ws):
             self.A.fill(t3, am, ak)
-            gemm_(self.A, self.W, r3, er, ec, alpha, 1.0, self.status)
+            gemm_(self.A, w, r3, er, ec, alpha, 1.0, self.status)
         return r3
 
 

@@ -83,7 +83,7 @@ def case_gather(reps, nocc=10):
     src = [(S, 1.0, t3_residual.full_strides(nocc, 90), t3_residual.ALL_S3),
            (Y, -1.0, tr.y_strides, t3_residual.ALL_S3)]
     for _ in range(reps):
-        t3_residual.perm_gather_(r3, d.ijk, 90, 0.0, src)
+        t3_residual.perm_gather_(r3, d.ijk, 90, 0.0, src, nocc=nocc)
     torch.cuda.synchronize()
 
 

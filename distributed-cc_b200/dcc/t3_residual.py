@@ -30,9 +30,10 @@ In mixed precision S is built by three split-precision tcgen05 GEMMs written
 straight into S's [i][j][k][a][b][c] layout (X; T2 and T5/2 as one GEMM over
 the concatenated contraction index; T1 reusing T2's U operand) plus an FP64
 GEMM for the K = nocc^2 W_oooo / F_oo part, and one gather kernel applies the
-symmetrization to S and Y.  F_vv.t3 (three strings) are FP64 batched GEMMs;
-W_vvvv.t3 (three strings, the dominant cost) are three split-precision GEMMs
-that accumulate straight into r3.
+symmetrization to S and Y.  W_vvvv.t3 (three strings, the dominant cost) are
+three split-precision GEMMs that accumulate straight into r3; the three
+F_vv.t3 strings ride in them as extra terms of the W operand
+(contract.WvvvvT3).  The FP64 path runs F_vv.t3 as batched DGEMMs.
 
 precision = "fp64" runs every contraction in FP64 (cuBLAS DGEMM through
 torch): the plain FP64 GPU path.  "bf16x3" / "tf32x3" run the large
@@ -76,15 +77,36 @@ OO_SET = (1 << 0) | (1 << 2) | (1 << 4)  # identity, (j,i,k;b,a,c), (k,i,j;c,a,b
 OOOO_SET = (1 << 0) | (1 << 1) | (1 << 3)  # identity, (i,k,j;a,c,b), (j,k,i;b,c,a)
 
 
-def perm_gather_(r3, ijk, nvir, beta, sources):
-    """r3 = beta*r3 + sum over sources (tensor, scale, strides6, mask) of the masked permutation sums."""
+_pgather_tma = L.bind("dcc_t3_perm_gather_tma", [L.c_vp, L.c_vp, L.c_i64, L.c_i64, L.c_i64, L.c_dbl, L.c_int, L.c_vp,
+                                                 L.c_vp, L.c_vp, L.c_vp, L.c_vp, L.c_vp])
+_status_cache = {}
+
+
+def _default_status(device):
+    key = str(device)
+    if key not in _status_cache:
+        _status_cache[key] = torch.zeros(1, dtype=torch.int32, device=device)
+    return _status_cache[key]
+
+
+def perm_gather_(r3, ijk, nvir, beta, sources, nocc=None, status=None):
+    """r3 = beta*r3 + sum over sources (tensor, scale, strides6, mask) of the masked permutation sums.
+
+    With nocc given the TMA-pipelined kernel runs (it reports bounded-wait
+    timeouts in `status`, a device int32); without, the cp.async kernel."""
     n = len(sources)
     bases = (ctypes.c_void_p * n)(*[t.data_ptr() for t, _, _, _ in sources])
     scales = (ctypes.c_double * n)(*[float(sc) for _, sc, _, _ in sources])
     strides = (ctypes.c_int64 * (6 * n))(*[int(x) for _, _, st, _ in sources for x in st])
     masks = (ctypes.c_int * n)(*[int(m) for _, _, _, m in sources])
-    L.check(_pgather(L.ptr(r3), L.ptr(ijk), r3.shape[0], nvir, float(beta), n, bases, scales, strides, masks,
-                     L.stream_ptr()))
+    if nocc is None:
+        L.check(_pgather(L.ptr(r3), L.ptr(ijk), r3.shape[0], nvir, float(beta), n, bases, scales, strides, masks,
+                         L.stream_ptr()))
+    else:
+        if status is None:
+            status = _default_status(r3.device)
+        L.check(_pgather_tma(L.ptr(r3), L.ptr(ijk), r3.shape[0], int(nocc), nvir, float(beta), n, bases, scales,
+                             strides, masks, L.ptr(status), L.stream_ptr()))
     return r3
 
 
@@ -163,6 +185,7 @@ class T3Residual:
         Ny = no * nv * nv
         self.y_strides = (no * nv * Ny, nv * Ny, nv * nv, Ny, nv, 1)
         self.Ganti = None
+        self.gstatus = torch.zeros(1, dtype=torch.int32, device=device)  # gather pipeline timeouts
         if precision != "fp64":
             k = contract.KIND[precision]
             self.kind = k
@@ -258,9 +281,10 @@ class T3Residual:
         return r3
 
     def wvvvv_(self, r3, d, t3):
+        """W_vvvv.t3 (distr_cc/rccsdt.py:421-427); in split precision F_vv.t3 rides in the same GEMMs."""
         if self.precision == "fp64":
             return contract.wvvvv_t3_fp64_(r3, d.W_vvvv, t3)
-        return self.wvvvv(r3, d.W_vvvv, t3)
+        return self.wvvvv(r3, d.W_vvvv, t3, F=d.F_vv)
 
     def compute(self, d, t3, r3=None):
         """r3 = compute_r3_tri for canonical t3 (the OO batch terms included when with_oo)."""
@@ -269,14 +293,19 @@ class T3Residual:
         no, nv = self.no, self.nv
         S = self.s_(d, t3)
         Y = self.y_(d)
-        perm_gather_(r3, d.ijk, nv, 0.0, [(S, 1.0, full_strides(no, nv), ALL_S3), (Y, -1.0, self.y_strides, ALL_S3)])
+        perm_gather_(r3, d.ijk, nv, 0.0, [(S, 1.0, full_strides(no, nv), ALL_S3), (Y, -1.0, self.y_strides, ALL_S3)],
+                     nocc=no, status=self.gstatus)
         if self.Ganti is not None:
-            perm_gather_(r3, d.ijk, nv, 1.0, [(self.Ganti, 1.0, full_strides(no, nv), OOOO_SET)])
-        self.fvv_(r3, d, t3)
+            perm_gather_(r3, d.ijk, nv, 1.0, [(self.Ganti, 1.0, full_strides(no, nv), OOOO_SET)], nocc=no,
+                         status=self.gstatus)
+        if self.precision == "fp64":
+            self.fvv_(r3, d, t3)
         self.wvvvv_(r3, d, t3)
         return r3
 
     def status_ok(self):
+        if int(self.gstatus.item()) != 0:
+            return False
         if self.precision == "fp64":
             return True
         return int(self.status.item()) == 0 and int(self.wvvvv.status.item()) == 0

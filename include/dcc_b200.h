@@ -170,6 +170,18 @@ DCC_API int dcc_t3_perm_gather(double *r3, const int32_t *ijk, int64_t nblocks, 
                                const double *const *bases, const double *scales, const int64_t *strides,
                                const int *masks, void *stream);
 
+/* dcc_t3_perm_gather for sources laid out as blocks of nocc-digit (x, y, z)
+ * (nocc is needed for the block coordinates): one persistent kernel in which
+ * a producer warp moves each (source, permutation) tile with a TMA box load
+ * and the summed tile leaves through a TMA store.  Falls back to the
+ * cp.async kernel when a source does not fit the copy engine (odd nvir, a
+ * non-unit c stride, b slower than a, or block strides that do not collapse
+ * into two dimensions).  *status (DEVICE int, zero before the call) becomes
+ * DCC_ERR_TIMEOUT if a bounded wait gave up. */
+DCC_API int dcc_t3_perm_gather_tma(double *r3, const int32_t *ijk, int64_t nblocks, int64_t nocc, int64_t nvir,
+                                   double beta, int nsrc, const double *const *bases, const double *scales,
+                                   const int64_t *strides, const int *masks, int *status, void *stream);
+
 /* ----------------------------------------------------------------------
  * T4 helpers (replace src/rccsdtq.c and PySCF libccsdt.t4_add_)
  * ---------------------------------------------------------------------- */

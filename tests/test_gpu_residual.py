@@ -25,7 +25,7 @@ def _ref_r3(er, dn, with_oo=True):
     return er.compute_r3_tri_ref(imds, dn.t2, dn.t3, dn.nocc, with_oo=with_oo)
 
 
-@pytest.mark.parametrize("nocc,nvir", [(2, 5), (3, 7), (4, 10)])
+@pytest.mark.parametrize("nocc,nvir", [(2, 5), (3, 7), (4, 10), (3, 18)])
 @pytest.mark.parametrize("precision", ["fp64", "bf16x3", "tf32x3"])
 @pytest.mark.parametrize("with_oo", [False, True])
 def test_residual(mods, nocc, nvir, precision, with_oo):
@@ -54,3 +54,51 @@ def test_update(mods, nocc, nvir, nact):
     assert np.array_equal(r3.cpu().numpy(), want_r3)
     assert np.array_equal(t3.cpu().numpy(), want_t3)
     np.testing.assert_allclose(norms.cpu().numpy(), want_n, rtol=1e-12)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "bf16x3"])
+def test_residual_without_woooo_pair_symmetry(mods, precision):
+    """A W_oooo without W[l,m,i,j] = W[m,l,j,i] keeps its antisymmetric part on the
+    reference's own permutation set (a second gather pass)."""
+    syn, tr, er = mods
+    nocc, nvir = 3, 10
+    d = syn.make_inputs(nocc, nvir, seed=4)
+    g = torch.Generator(device="cuda").manual_seed(9)
+    d.W_oooo = d.W_oooo + 0.05 * torch.randn(d.W_oooo.shape, dtype=torch.float64, device="cuda", generator=g)
+    dn = syn.to_numpy(d)
+    want = _ref_r3(er, dn, True)
+    res = tr.T3Residual(nocc, nvir, precision, with_oo=True)
+    got = res.compute(d, d.t3).cpu().numpy()
+    assert res.status_ok() and res.Ganti is not None
+    if precision == "fp64":
+        np.testing.assert_allclose(got, want, rtol=1e-11, atol=1e-11 * np.abs(want).max())
+    else:
+        assert np.abs(got - want).max() / np.abs(want).max() < TOL[precision]
+
+
+@pytest.mark.parametrize("nvir", [10, 18, 9])
+@pytest.mark.parametrize("beta", [0.0, 0.75])
+def test_tma_gather_matches_cp_async_gather(mods, nvir, beta):
+    """The TMA-pipelined permutation gather equals the cp.async kernel bit for bit
+    (same summation order) for the full-layout and the Y-layout sources, every
+    mask used by the residual, edge tiles (nvir = 10, 18) and the fallback (nvir = 9)."""
+    syn, tr, er = mods
+    no = 4
+    d = syn.make_inputs(no, nvir, seed=1, with_t3=False)
+    n3 = d.ijk.shape[0]
+    g = torch.Generator(device="cuda").manual_seed(nvir)
+    full = torch.randn((no ** 3, nvir, nvir, nvir), dtype=torch.float64, device="cuda", generator=g)
+    Y = torch.randn((no * no * nvir, no * nvir * nvir), dtype=torch.float64, device="cuda", generator=g)
+    Ny = no * nvir * nvir
+    ys = (no * nvir * Ny, nvir * Ny, nvir * nvir, Ny, nvir, 1)
+    r0 = torch.randn((n3, nvir, nvir, nvir), dtype=torch.float64, device="cuda", generator=g)
+    for src in ([(full, 1.0, tr.full_strides(no, nvir), tr.ALL_S3), (Y, -1.0, ys, tr.ALL_S3)],
+                [(full, 0.5, tr.full_strides(no, nvir), tr.OOOO_SET)],
+                [(full, 1.0, tr.full_strides(no, nvir), tr.OO_SET), (Y, 2.0, ys, tr.OOOO_SET)]):
+        a, b = r0.clone(), r0.clone()
+        st = torch.zeros(1, dtype=torch.int32, device="cuda")
+        tr.perm_gather_(a, d.ijk, nvir, beta, src)
+        tr.perm_gather_(b, d.ijk, nvir, beta, src, nocc=no, status=st)
+        torch.cuda.synchronize()
+        assert int(st.item()) == 0
+        assert torch.equal(a, b)
