@@ -286,8 +286,11 @@ class T3Residual:
             return contract.wvvvv_t3_fp64_(r3, d.W_vvvv, t3)
         return self.wvvvv(r3, d.W_vvvv, t3, F=d.F_vv)
 
-    def compute(self, d, t3, r3=None):
-        """r3 = compute_r3_tri for canonical t3 (the OO batch terms included when with_oo)."""
+    def compute(self, d, t3, r3=None, wvvvv_ready=None):
+        """r3 = compute_r3_tri for canonical t3 (the OO batch terms included when with_oo).
+
+        wvvvv_ready: optional CUDA event the W_vvvv.t3 part waits for, so a caller can
+        stream W_vvvv to the device while the other terms run."""
         if r3 is None:
             r3 = torch.empty_like(t3)
         no, nv = self.no, self.nv
@@ -298,6 +301,8 @@ class T3Residual:
         if self.Ganti is not None:
             perm_gather_(r3, d.ijk, nv, 1.0, [(self.Ganti, 1.0, full_strides(no, nv), OOOO_SET)], nocc=no,
                          status=self.gstatus)
+        if wvvvv_ready is not None:
+            torch.cuda.current_stream().wait_event(wvvvv_ready)
         if self.precision == "fp64":
             self.fvv_(r3, d, t3)
         self.wvvvv_(r3, d, t3)
