@@ -121,9 +121,13 @@ struct P3Coef {
     double p0, p1, p2, p3, p4, alpha, beta, p012, ap34;
 };
 
-// kComp[X][s]: the axis map equal to "s, then X" (X(s(u)) = kComp[X][s](u)).
-__constant__ int kComp[6][6] = {{0, 1, 2, 3, 4, 5}, {1, 0, 3, 2, 5, 4}, {2, 4, 0, 5, 1, 3},
-                                {3, 5, 1, 4, 0, 2}, {4, 2, 5, 0, 3, 1}, {5, 3, 4, 1, 2, 0}};
+// comp6(X, s): the axis map equal to "s, then X" (X(s(u)) = comp6(X, s)(u)),
+// i.e. the table {0,1,2,3,4,5}, {1,0,3,2,5,4}, {2,4,0,5,1,3}, {3,5,1,4,0,2},
+// {4,2,5,0,3,1}, {5,3,4,1,2,0}.  constexpr, so that with unrolled s the
+// register-array indices it yields are compile-time constants.
+__host__ __device__ constexpr int comp6(int X, int s) {
+    return X == 0 ? (s == 0 ? 0 : (s == 1 ? 1 : (s == 2 ? 2 : (s == 3 ? 3 : (s == 4 ? 4 : (5)))))) : (X == 1 ? (s == 0 ? 1 : (s == 1 ? 0 : (s == 2 ? 3 : (s == 3 ? 2 : (s == 4 ? 5 : (4)))))) : (X == 2 ? (s == 0 ? 2 : (s == 1 ? 4 : (s == 2 ? 0 : (s == 3 ? 5 : (s == 4 ? 1 : (3)))))) : (X == 3 ? (s == 0 ? 3 : (s == 1 ? 5 : (s == 2 ? 1 : (s == 3 ? 4 : (s == 4 ? 0 : (2)))))) : (X == 4 ? (s == 0 ? 4 : (s == 1 ? 2 : (s == 2 ? 5 : (s == 3 ? 0 : (s == 4 ? 3 : (1)))))) : (s == 0 ? 5 : (s == 1 ? 3 : (s == 2 ? 4 : (s == 3 ? 1 : (s == 4 ? 2 : (0))))))))));
+}
 
 // P3 spin summation of a whole orbit set in shared memory, in place.  Each
 // thread takes canonical positions u (global u0 <= u1 <= u2, all inside slot
@@ -157,8 +161,8 @@ __device__ __forceinline__ void p3_orbits_inplace(double *buf, const OrbitSet &o
         double r[6];
 #pragma unroll
         for (int q = 0; q < 6; q++) {
-            double tu = dadd(dadd(dmul(k.p0, v[q]), dmul(k.p1, v[kComp[5][q]])), dmul(k.p2, v[kComp[2][q]]));
-            double tw = dadd(dadd(dmul(k.p0, v[kComp[1][q]]), dmul(k.p1, v[kComp[3][q]])), dmul(k.p2, v[kComp[4][q]]));
+            double tu = dadd(dadd(dmul(k.p0, v[q]), dmul(k.p1, v[comp6(5, q)])), dmul(k.p2, v[comp6(2, q)]));
+            double tw = dadd(dadd(dmul(k.p0, v[comp6(1, q)]), dmul(k.p1, v[comp6(3, q)])), dmul(k.p2, v[comp6(4, q)]));
             r[q] = dadd(dmul(k.beta, v[q]), dmul(k.alpha, dadd(dmul(k.p3, tu), dmul(k.p4, tw))));
         }
 #pragma unroll
@@ -349,9 +353,9 @@ __global__ void __launch_bounds__(OT_THREADS, 3) k_p3_inplace(double *A, int64_t
             double r[6];
 #pragma unroll
             for (int q = 0; q < 6; q++) {
-                double tu = dadd(dadd(dmul(k.p0, v[q]), dmul(k.p1, v[kComp[5][q]])), dmul(k.p2, v[kComp[2][q]]));
+                double tu = dadd(dadd(dmul(k.p0, v[q]), dmul(k.p1, v[comp6(5, q)])), dmul(k.p2, v[comp6(2, q)]));
                 double tw =
-                    dadd(dadd(dmul(k.p0, v[kComp[1][q]]), dmul(k.p1, v[kComp[3][q]])), dmul(k.p2, v[kComp[4][q]]));
+                    dadd(dadd(dmul(k.p0, v[comp6(1, q)]), dmul(k.p1, v[comp6(3, q)])), dmul(k.p2, v[comp6(4, q)]));
                 r[q] = dadd(dmul(k.beta, v[q]), dmul(k.alpha, dadd(dmul(k.p3, tu), dmul(k.p4, tw))));
             }
 #pragma unroll
@@ -363,6 +367,133 @@ __global__ void __launch_bounds__(OT_THREADS, 3) k_p3_inplace(double *A, int64_t
         for (int j = 0; j < 12; j++)
             if (nload & (1u << j)) blk[goff[j]] = buf[soff[j]];
         __syncthreads();  // buf is refilled two iterations later
+    }
+}
+
+// Element of an 8^3 tile for lane l (0..31) and step j (0..15): a linear
+// map over GF(2) of the lane and step bits, chosen so that for every
+// simultaneous permutation p the 16 lanes of each half-warp reading position
+// p(u) of a dense [a][b][c] tile hit 16 different 8-byte bank pairs (a 64-bit
+// shared access is served per half-warp), i.e. all six permuted read patterns
+// are conflict-free; over (l, j) it is a bijection onto the 512 positions.
+__device__ __forceinline__ void tile_element(int l, int j, int u[3]) {
+    const int l0 = l & 1, l1 = (l >> 1) & 1, l2 = (l >> 2) & 1, l3 = (l >> 3) & 1, l4 = (l >> 4) & 1;
+    const int j0 = j & 1, j1 = (j >> 1) & 1, j2 = (j >> 2) & 1, j3 = (j >> 3) & 1;
+    u[0] = l0 | (l1 << 1) | (l2 << 2);
+    u[1] = l3 | ((l1 ^ l4) << 1) | ((l2 ^ j0) << 2);
+    u[2] = (l0 ^ l3 ^ j3) | ((l1 ^ j1) << 1) | ((l2 ^ j2) << 2);
+}
+
+// Element owned by thread t (0..255) of a CTA, half h: the step is (warp, h).
+__device__ __forceinline__ void tg_element(int t, int h, int u[3]) { tile_element(t & 31, (t >> 5) | (h << 3), u); }
+
+// In-place P3 spin summation, one warp per orbit set.  Each warp owns a
+// dense 6 x 8^3 buffer: it copies the distinct permuted tiles of its canonical
+// tile triple for one block (16-byte cp.async), evaluates every canonical
+// position of the set (lanes/steps follow tile_element, so the six permuted
+// reads and writes are conflict-free) and stores the tiles back with 16-byte
+// stores, then moves to its next block.  No CTA-wide barrier: the warps of an
+// SM (three CTAs of three warps) overlap each other's copies, sums and stores.
+// Same arithmetic as k_p3_inplace; FULL (P3_full) drops the unit
+// coefficients (x * 1.0 == x exactly).
+constexpr int PW_WARPS = 3;
+
+template <bool FULL>
+__global__ void __launch_bounds__(32 * PW_WARPS, 3) k_p3_warp(double *A, int64_t nblocks, int nv, int ntile, P3Coef k) {
+    extern __shared__ __align__(16) double sm[];  // PW_WARPS x 6 x TE3 doubles
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    double *buf = sm + w * 6 * TE3;
+    int t0, t1, t2;
+    decode_tri3(blockIdx.x, ntile, t0, t1, t2);
+    auto tsel = [&](int m) { return m == 0 ? t0 : (m == 1 ? t1 : t2); };
+    // slot s holds tile perm_s(T); slot_of(s) = first slot with the same tile (3 bits per slot)
+    unsigned slot_of = 0;
+#pragma unroll
+    for (int sl = 0; sl < 6; sl++) {
+        int first = sl;
+#pragma unroll
+        for (int q = sl - 1; q >= 0; q--)
+            if (tsel(perm3(q, 0)) == tsel(perm3(sl, 0)) && tsel(perm3(q, 1)) == tsel(perm3(sl, 1)) &&
+                tsel(perm3(q, 2)) == tsel(perm3(sl, 2)))
+                first = q;
+        slot_of |= (unsigned)first << (3 * sl);
+    }
+    auto sof = [&](int sl) { return (int)((slot_of >> (3 * sl)) & 7u); };
+    const int64_t n3 = (int64_t)nv * nv * nv;
+    const int cy = lane >> 2, cz = 2 * (lane & 3);  // this lane's 16-byte chunk of every tile row pair
+    const unsigned sbase = (unsigned)__cvta_generic_to_shared(buf);
+    const int64_t stride = (int64_t)gridDim.y * PW_WARPS;
+    for (int64_t b = (int64_t)blockIdx.y * PW_WARPS + w; b < nblocks; b += stride) {
+        double *blk = A + b * n3;
+#pragma unroll 1
+        for (int sl = 0; sl < 6; sl++) {
+            if (sof(sl) != sl) continue;
+            const int gx0 = tsel(perm3(sl, 0)) * TE, gy = tsel(perm3(sl, 1)) * TE + cy, gz = tsel(perm3(sl, 2)) * TE + cz;
+            if (gy >= nv || gz >= nv) continue;
+            const double *src = blk + ((int64_t)gx0 * nv + gy) * nv + gz;
+            const unsigned dst = sbase + 8u * (unsigned)(sl * TE3 + cy * 8 + cz);
+#pragma unroll
+            for (int x = 0; x < TE; x++)
+                if (gx0 + x < nv)
+                    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst + 8u * 64u * x),
+                                 "l"(src + (int64_t)x * nv * nv));
+        }
+        cp_async_commit();
+        cp_async_wait<0>();
+        __syncwarp();
+#pragma unroll 2
+        for (int j = 0; j < 16; j++) {
+            int u[3];
+            tile_element(lane, j, u);
+            const int x = u[0], y = u[1], z = u[2];
+            if (t0 * TE + x >= nv || t1 * TE + y >= nv || t2 * TE + z >= nv || (t0 == t1 && x > y) ||
+                (t1 == t2 && y > z))
+                continue;
+            int a[6];
+            a[0] = sof(0) * TE3 + x * 64 + y * 8 + z;
+            a[1] = sof(1) * TE3 + x * 64 + z * 8 + y;
+            a[2] = sof(2) * TE3 + y * 64 + x * 8 + z;
+            a[3] = sof(3) * TE3 + y * 64 + z * 8 + x;
+            a[4] = sof(4) * TE3 + z * 64 + x * 8 + y;
+            a[5] = sof(5) * TE3 + z * 64 + y * 8 + x;
+            double v[6];
+#pragma unroll
+            for (int q = 0; q < 6; q++) v[q] = buf[a[q]];
+            if (t0 == t1 && t1 == t2 && x == y && y == z) {
+                buf[a[0]] = dadd(dmul(k.beta, v[0]), dmul(k.ap34, dmul(k.p012, v[0])));
+                continue;
+            }
+            double r[6];
+#pragma unroll
+            for (int q = 0; q < 6; q++) {
+                if (FULL) {
+                    const double tu = dadd(dadd(v[q], v[comp6(5, q)]), v[comp6(2, q)]);
+                    const double tw = dadd(dadd(v[comp6(1, q)], v[comp6(3, q)]), v[comp6(4, q)]);
+                    r[q] = dadd(dmul(k.beta, v[q]), dmul(k.alpha, dadd(tu, tw)));
+                } else {
+                    const double tu =
+                        dadd(dadd(dmul(k.p0, v[q]), dmul(k.p1, v[comp6(5, q)])), dmul(k.p2, v[comp6(2, q)]));
+                    const double tw = dadd(dadd(dmul(k.p0, v[comp6(1, q)]), dmul(k.p1, v[comp6(3, q)])),
+                                           dmul(k.p2, v[comp6(4, q)]));
+                    r[q] = dadd(dmul(k.beta, v[q]), dmul(k.alpha, dadd(dmul(k.p3, tu), dmul(k.p4, tw))));
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < 6; q++) buf[a[q]] = r[q];
+        }
+        __syncwarp();
+#pragma unroll 1
+        for (int sl = 0; sl < 6; sl++) {
+            if (sof(sl) != sl) continue;
+            const int gx0 = tsel(perm3(sl, 0)) * TE, gy = tsel(perm3(sl, 1)) * TE + cy, gz = tsel(perm3(sl, 2)) * TE + cz;
+            if (gy >= nv || gz >= nv) continue;
+            double *dst = blk + ((int64_t)gx0 * nv + gy) * nv + gz;
+            const double *src = buf + sl * TE3 + cy * 8 + cz;
+#pragma unroll
+            for (int x = 0; x < TE; x++)
+                if (gx0 + x < nv) *(double2 *)(dst + (int64_t)x * nv * nv) = *(const double2 *)(src + x * 64);
+        }
+        __syncwarp();
     }
 }
 
@@ -394,6 +525,24 @@ static int orbit3_launch(int mode, const double *in, double *o0, double *o1, dou
     dim3 grid((unsigned)ntri, (unsigned)gy);
     size_t smem = 2 * 6 * SLOT * sizeof(double);
     cudaStream_t st = as_stream(stream);
+    if (mode == 0 && nvir % 2 == 0 && ((uintptr_t)o0 & 15) == 0) {  // 16-byte rows
+        const size_t wsm = (size_t)PW_WARPS * 6 * TE3 * sizeof(double);
+        // about 4 waves of 148 SMs x 3 CTAs, each warp walking several blocks
+        int64_t wy = (148 * 3 * 4 + ntri - 1) / ntri;
+        const int64_t maxy = (nblocks + PW_WARPS - 1) / PW_WARPS;
+        wy = wy < 1 ? 1 : (wy > maxy ? maxy : wy);
+        wy = wy > 65535 ? 65535 : wy;
+        dim3 wgrid((unsigned)ntri, (unsigned)wy);
+        const bool full = k.p0 == 1.0 && k.p1 == 1.0 && k.p2 == 1.0 && k.p3 == 1.0 && k.p4 == 1.0;
+        if (full) {
+            cudaFuncSetAttribute(k_p3_warp<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wsm);
+            k_p3_warp<true><<<wgrid, 32 * PW_WARPS, wsm, st>>>(o0, nblocks, (int)nvir, ntile, k);
+        } else {
+            cudaFuncSetAttribute(k_p3_warp<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wsm);
+            k_p3_warp<false><<<wgrid, 32 * PW_WARPS, wsm, st>>>(o0, nblocks, (int)nvir, ntile, k);
+        }
+        return launch_status("P3 spin summation");
+    }
     if (mode == 0 && nvir <= 1290) {  // 32-bit element offsets inside a block
         cudaFuncSetAttribute(k_p3_inplace, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         k_p3_inplace<<<grid, OT_THREADS, smem, st>>>(o0, nblocks, (int)nvir, ntile, k);
@@ -1187,19 +1336,6 @@ struct TmaGatherArgs {
 
 __device__ __forceinline__ int pick5(int k, int v0, int v1, int v2, int v3, int v4) {
     return k == 0 ? v0 : (k == 1 ? v1 : (k == 2 ? v2 : (k == 3 ? v3 : v4)));
-}
-
-// Element of the 8^3 tile owned by thread t (0..255), half h.  A linear map
-// over GF(2) of the thread bits chosen so that, for every simultaneous
-// permutation p, the 32 lanes of a warp reading position p(u) of a dense
-// [a][b][c] tile touch each 8-byte bank pair exactly twice (the minimum for
-// 256 bytes), i.e. all six permuted read patterns are conflict-free.
-__device__ __forceinline__ void tg_element(int t, int h, int u[3]) {
-    const int l = t & 31, w = t >> 5;
-    const int l0 = l & 1, l1 = (l >> 1) & 1, l2 = (l >> 2) & 1, l3 = (l >> 3) & 1, l4 = (l >> 4) & 1;
-    u[0] = l & 7;
-    u[1] = l3 | (l4 << 1) | ((l1 ^ l2 ^ (w & 1)) << 2);
-    u[2] = (l1 ^ l3 ^ ((w >> 1) & 1)) | ((l2 ^ l4 ^ ((w >> 2) & 1)) << 1) | ((l0 ^ l1 ^ h) << 2);
 }
 
 __device__ __forceinline__ void named_sync_compute() { asm volatile("bar.sync 1, %0;" ::"n"(32 * TG_WARPS) : "memory"); }

@@ -33,7 +33,7 @@ def C():
     return _c_rccsdt, _c_rccsdt_q, _c_rccsdtq
 
 
-@pytest.mark.parametrize("nvir", [1, 2, 5, 8, 13, 17, 90])
+@pytest.mark.parametrize("nvir", [1, 2, 5, 8, 10, 13, 17, 18, 90])
 @pytest.mark.parametrize("pattern", P3)
 def test_t3_spin_sum(C, oracle, nvir, pattern):
     c3 = C[0]
