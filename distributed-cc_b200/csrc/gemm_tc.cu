@@ -43,25 +43,39 @@ struct GemmConfig {
 };
 static GemmConfig g_cfg = {64, 4, 16};
 
-// off(m) = (m / (R1*R2)) * S0 + ((m / R2) % R1) * S1 + (m % R2) * S2
-struct Map3 {
-    int64_t R1, R2, S0, S1, S2;
+// Four-digit mixed-radix address map:
+//   off(m) = (m / (R1 R2 R3)) S0 + ((m / (R2 R3)) % R1) S1 + ((m / R3) % R2) S2 + (m % R3) S3.
+// A three-digit map {R1, R2, S0, S1, S2} is {R1, R2, 1, S0, S1, S2, 0}.
+struct Map4 {
+    int64_t R1, R2, R3, S0, S1, S2, S3;
 };
 
-__host__ __device__ __forceinline__ int64_t map3(const Map3 &f, int64_t m) {
-    return (m / (f.R1 * f.R2)) * f.S0 + ((m / f.R2) % f.R1) * f.S1 + (m % f.R2) * f.S2;
+__host__ __device__ __forceinline__ int64_t map4(const Map4 &f, int64_t m) {
+    const int64_t r23 = f.R2 * f.R3;
+    return (m / (f.R1 * r23)) * f.S0 + ((m / r23) % f.R1) * f.S1 + ((m / f.R3) % f.R2) * f.S2 + (m % f.R3) * f.S3;
 }
 
 struct GemmEpi {
-    Map3 row, col;
+    Map4 row, col;
 };
 
-// map3 for m < 2^31 and R1*R2 < 2^31 (checked on the host): 32-bit divisions.
-__device__ __forceinline__ int64_t map3_32(const Map3 &f, uint32_t m) {
-    const uint32_t r2 = (uint32_t)f.R2, r12 = (uint32_t)(f.R1 * f.R2);
-    const uint32_t d0 = m / r12, mr = m - d0 * r12;
-    const uint32_t d1 = mr / r2, d2 = mr - d1 * r2;
-    return (int64_t)d0 * f.S0 + (int64_t)d1 * f.S1 + (int64_t)d2 * f.S2;
+// map4 for m < 2^31 and R1 R2 R3 < 2^31 (checked on the host): 32-bit divisions.
+__device__ __forceinline__ int64_t map4_32(const Map4 &f, uint32_t m) {
+    const uint32_t r3 = (uint32_t)f.R3, r23 = (uint32_t)(f.R2 * f.R3), r123 = (uint32_t)(f.R1 * f.R2 * f.R3);
+    const uint32_t d0 = m / r123, m1 = m - d0 * r123;
+    const uint32_t d1 = m1 / r23, m2 = m1 - d1 * r23;
+    const uint32_t d2 = m2 / r3, d3 = m2 - d2 * r3;
+    return (int64_t)d0 * f.S0 + (int64_t)d1 * f.S1 + (int64_t)d2 * f.S2 + (int64_t)d3 * f.S3;
+}
+
+// Stride and radix of the fastest digit that varies (R3 == 1: the map has three digits).
+__host__ __forceinline__ void fast_digit(const Map4 &f, int64_t &stride, int64_t &radix) {
+    stride = f.R3 > 1 ? f.S3 : f.S2;
+    radix = f.R3 > 1 ? f.R3 : f.R2;
+}
+
+__host__ __forceinline__ Map4 map_from(const int64_t *v, bool four) {
+    return four ? Map4{v[0], v[1], v[2], v[3], v[4], v[5], v[6]} : Map4{v[0], v[1], 1, v[2], v[3], v[4], 0};
 }
 
 // K-major, swizzled operand tile with rows of KB bytes (KB = 128/64/32 ->
@@ -278,7 +292,7 @@ __global__ void __launch_bounds__(gemm_threads<EPI>(), 1)
             tile_coords(t, num_m, num_n, group_m, tm, tn);
             const int m0 = tm * GM + q * 32, n0 = tn * GN;  // first row of this warp, first column of the tile
             const int m = m0 + lane;
-            const int64_t roff = map3_32(epi.row, (uint32_t)(m < M ? m : 0));
+            const int64_t roff = map4_32(epi.row, (uint32_t)(m < M ? m : 0));
             const int nrow = (M - m0) < 32 ? (M - m0) : 32;
             offs[lane] = roff;  // cols mode: row offsets of the warp's 32 rows
             for (int c = cbeg; c < cend; c += 32) {
@@ -294,7 +308,7 @@ __global__ void __launch_bounds__(gemm_threads<EPI>(), 1)
                 }
                 const int col = n0 + c + lane;
                 const bool cval = col < N;
-                const int64_t coff = map3_32(epi.col, (uint32_t)(cval ? col : 0));
+                const int64_t coff = map4_32(epi.col, (uint32_t)(cval ? col : 0));
                 if (epi_cols) {
                     // lanes walk the 32 columns of one row at a time (columns contiguous in C)
 #pragma unroll
@@ -385,21 +399,22 @@ __device__ __forceinline__ void split_tf32(double x, float &hi, float &lo) {
 // contiguous in the source (mode 0: k; mode 1: m; mode 2: the middle digit of
 // m, the tile's rows then step that digit), writes are 16-byte packs along k.
 struct SplitMap {
-    Map3 m, k;
+    Map4 m, k;
 };
 
 constexpr int SP_TM = 32, SP_TK = 64;
 
 template <int KIND>
 __global__ void __launch_bounds__(256) k_split(const double *src, void *hi, void *lo, int64_t M, int64_t K, int64_t kw,
-                                               int64_t ld, int64_t k0, SplitMap mp, int mode, int64_t nty) {
+                                               int64_t ld, int64_t k0, SplitMap mp, int mode, int64_t nty,
+                                               int64_t rmid, int64_t rfast) {
     __shared__ double tile[SP_TM][SP_TK + 1];
     __shared__ int64_t smo[SP_TM], srow[SP_TM], sko[SP_TK];
     const int t = threadIdx.x;
     const int64_t kt = (int64_t)blockIdx.x * SP_TK;
     if (t < SP_TK) {
         const int64_t k = kt + t;
-        sko[t] = k < K ? map3(mp.k, k) : -1;  // -1: zero column (padding) or outside the piece
+        sko[t] = k < K ? map4(mp.k, k) : -1;  // -1: zero column (padding) or outside the piece
     }
     for (int64_t ty = blockIdx.y; ty < nty; ty += gridDim.y) {
         __syncthreads();  // previous tile fully consumed
@@ -407,7 +422,8 @@ __global__ void __launch_bounds__(256) k_split(const double *src, void *hi, void
             int64_t m;
             bool valid;
             if (mode == 2) {
-                const int64_t R1 = mp.m.R1, R2 = mp.m.R2, nb1 = (R1 + SP_TM - 1) / SP_TM;
+                // rows step the second-fastest digit (radix rmid) of m; the fastest has radix rfast
+                const int64_t R1 = rmid, R2 = rfast, nb1 = (R1 + SP_TM - 1) / SP_TM;
                 const int64_t a2 = ty % R2, a1 = ((ty / R2) % nb1) * SP_TM + t, a0 = ty / (R2 * nb1);
                 valid = a1 < R1;
                 m = (a0 * R1 + a1) * R2 + a2;
@@ -416,7 +432,7 @@ __global__ void __launch_bounds__(256) k_split(const double *src, void *hi, void
                 valid = m < M;
             }
             srow[t] = valid ? m : -1;
-            smo[t] = valid ? map3(mp.m, m) : 0;
+            smo[t] = valid ? map4(mp.m, m) : 0;
         }
         __syncthreads();
         if (mode == 0) {
@@ -475,7 +491,9 @@ __global__ void __launch_bounds__(256) k_split(const double *src, void *hi, void
     }
 }
 
-static bool map3_ok(const int64_t *f) { return f[0] >= 1 && f[1] >= 1 && f[0] * f[1] < (1ll << 31); }
+static bool map_ok(const Map4 &f) {
+    return f.R1 >= 1 && f.R2 >= 1 && f.R3 >= 1 && f.R1 * f.R2 < (1ll << 31) && f.R1 * f.R2 * f.R3 < (1ll << 31);
+}
 
 // ----------------------------------------------------------------- host side
 
@@ -517,7 +535,10 @@ static int gemm_launch(const CUtensorMap &a, const CUtensorMap &b, const CUtenso
                        int group_m, cudaStream_t st) {
     // write along columns when the column map's fastest digit is contiguous,
     // along rows when only the row map's is
-    const int epi_cols = (epi.col.S2 == 1 || epi.row.S2 != 1) ? 1 : 0;
+    int64_t cs, cr, rs, rr;
+    fast_digit(epi.col, cs, cr);
+    fast_digit(epi.row, rs, rr);
+    const int epi_cols = (cs == 1 || rs != 1) ? 1 : 0;
     size_t smem = gemm_smem_bytes<ST, EPI>(KB);
     const int64_t tiles = (int64_t)ceil_div(N, GN) * (int64_t)ceil_div(M, GM);
     DCC_REQUIRE(tiles < (1ll << 31), DCC_ERR_SHAPE, "too many output tiles");
@@ -534,38 +555,50 @@ static int gemm_launch(const CUtensorMap &a, const CUtensorMap &b, const CUtenso
 
 using namespace dcc;
 
-extern "C" int dcc_split_operand_at(const double *src, void *hi, void *lo, int64_t M, int64_t K, int64_t kw,
-                                    int64_t ld, int64_t k0, const int64_t *map10, int kind, void *stream) {
+static int split_operand(const double *src, void *hi, void *lo, int64_t M, int64_t K, int64_t kw, int64_t ld,
+                         int64_t k0, const int64_t *maps, bool four, int kind, void *stream) {
     clear_error();
     DCC_REQUIRE(M >= 0 && K >= 0 && kw >= K && k0 >= 0 && k0 + kw <= ld, DCC_ERR_SHAPE,
                 "bad split sizes (M=%lld K=%lld kw=%lld k0=%lld ld=%lld)", (long long)M, (long long)K, (long long)kw,
                 (long long)k0, (long long)ld);
     DCC_REQUIRE(kind == 0 || kind == 1, DCC_ERR_UNSUPPORTED, "split kind must be 0 (bf16) or 1 (tf32)");
     if (M == 0 || kw == 0) return DCC_OK;
-    DCC_REQUIRE(src && hi && lo && map10, DCC_ERR_NULL, "NULL buffer");
-    DCC_REQUIRE(map3_ok(map10) && map3_ok(map10 + 5), DCC_ERR_SHAPE, "map radices must be >= 1 with R1*R2 < 2^31");
+    DCC_REQUIRE(src && hi && lo && maps, DCC_ERR_NULL, "NULL buffer");
+    SplitMap mp{map_from(maps, four), map_from(maps + (four ? 7 : 5), four)};
+    DCC_REQUIRE(map_ok(mp.m) && map_ok(mp.k), DCC_ERR_SHAPE, "map radices must be >= 1 with products < 2^31");
     DCC_REQUIRE(M < (1ll << 31) && ld < (1ll << 31), DCC_ERR_SHAPE, "split sizes must fit in 31 bits");
-    SplitMap mp{{map10[0], map10[1], map10[2], map10[3], map10[4]}, {map10[5], map10[6], map10[7], map10[8], map10[9]}};
-    // read along the contiguous source index: k, else m, else m's middle digit
+    // read along the contiguous source index: k, else m, else m's second-fastest digit
+    int64_t ks, kr, ms, mr;
+    fast_digit(mp.k, ks, kr);
+    fast_digit(mp.m, ms, mr);
+    const int64_t mid_s = mp.m.R3 > 1 ? mp.m.S2 : mp.m.S1, mid_r = mp.m.R3 > 1 ? mp.m.R2 : mp.m.R1;
     int mode;
-    if (mp.k.S2 == 1 && mp.k.R2 >= 16)
+    if (ks == 1 && kr >= 16)
         mode = 0;
-    else if (mp.m.S2 == 1 || mp.m.R2 == 1)
+    else if (ms == 1 || mr == 1)
         mode = 1;
-    else if (mp.m.S1 == 1 && mp.m.R1 > 1)
+    else if (mid_s == 1 && mid_r > 1)
         mode = 2;
     else
-        mode = mp.k.S2 == 1 ? 0 : 1;
-    if (mode == 2) DCC_REQUIRE(mp.m.R1 * mp.m.R2 * ((M + mp.m.R1 * mp.m.R2 - 1) / (mp.m.R1 * mp.m.R2)) == M,
-                               DCC_ERR_SHAPE, "row map does not tile M");
-    const int64_t nty = mode == 2 ? (M / (mp.m.R1 * mp.m.R2)) * ((mp.m.R1 + SP_TM - 1) / SP_TM) * mp.m.R2
-                                  : (M + SP_TM - 1) / SP_TM;
+        mode = ks == 1 ? 0 : 1;
+    if (mode == 2) DCC_REQUIRE(M % (mid_r * mr) == 0, DCC_ERR_SHAPE, "row map does not tile M");
+    const int64_t nty = mode == 2 ? (M / (mid_r * mr)) * ((mid_r + SP_TM - 1) / SP_TM) * mr : (M + SP_TM - 1) / SP_TM;
     dim3 grid(ceil_div(kw, SP_TK), (unsigned)(nty < 65535 ? nty : 65535));
     if (kind == 0)
-        k_split<0><<<grid, 256, 0, as_stream(stream)>>>(src, hi, lo, M, K, kw, ld, k0, mp, mode, nty);
+        k_split<0><<<grid, 256, 0, as_stream(stream)>>>(src, hi, lo, M, K, kw, ld, k0, mp, mode, nty, mid_r, mr);
     else
-        k_split<1><<<grid, 256, 0, as_stream(stream)>>>(src, hi, lo, M, K, kw, ld, k0, mp, mode, nty);
+        k_split<1><<<grid, 256, 0, as_stream(stream)>>>(src, hi, lo, M, K, kw, ld, k0, mp, mode, nty, mid_r, mr);
     return launch_status("split_operand");
+}
+
+extern "C" int dcc_split_operand_at(const double *src, void *hi, void *lo, int64_t M, int64_t K, int64_t kw,
+                                    int64_t ld, int64_t k0, const int64_t *map10, int kind, void *stream) {
+    return split_operand(src, hi, lo, M, K, kw, ld, k0, map10, false, kind, stream);
+}
+
+extern "C" int dcc_split_operand_at4(const double *src, void *hi, void *lo, int64_t M, int64_t K, int64_t kw,
+                                     int64_t ld, int64_t k0, const int64_t *map14, int kind, void *stream) {
+    return split_operand(src, hi, lo, M, K, kw, ld, k0, map14, true, kind, stream);
 }
 
 extern "C" int dcc_split_operand(const double *src, void *hi, void *lo, int64_t M, int64_t K, int64_t Kp,
@@ -573,10 +606,9 @@ extern "C" int dcc_split_operand(const double *src, void *hi, void *lo, int64_t 
     return dcc_split_operand_at(src, hi, lo, M, K, Kp, Kp, 0, map10, kind, stream);
 }
 
-extern "C" int dcc_gemm_split3_ld(const void *A_hi, const void *A_lo, int64_t lda, const void *B_hi,
-                                  const void *B_lo, int64_t ldb, int64_t M, int64_t N, int64_t Kp, double *C,
-                                  const int64_t *epi10, double alpha, double beta, int kind, int *status,
-                                  void *stream) {
+static int gemm_split3(const void *A_hi, const void *A_lo, int64_t lda, const void *B_hi, const void *B_lo,
+                       int64_t ldb, int64_t M, int64_t N, int64_t Kp, double *C, const int64_t *epi, bool four,
+                       double alpha, double beta, int kind, int *status, void *stream) {
     clear_error();
     DCC_REQUIRE(kind == 0 || kind == 1, DCC_ERR_UNSUPPORTED, "kind must be 0 (bf16x3) or 1 (tf32x3)");
     const int kblk = kind == 0 ? 64 : 32;
@@ -587,10 +619,10 @@ extern "C" int dcc_gemm_split3_ld(const void *A_hi, const void *A_lo, int64_t ld
                 DCC_ERR_SHAPE, "row pitches (lda=%lld ldb=%lld) must be >= Kp and multiples of 8", (long long)lda,
                 (long long)ldb);
     if (M == 0 || N == 0) return DCC_OK;
-    DCC_REQUIRE(A_hi && A_lo && B_hi && B_lo && C && epi10 && status, DCC_ERR_NULL, "NULL buffer");
+    DCC_REQUIRE(A_hi && A_lo && B_hi && B_lo && C && epi && status, DCC_ERR_NULL, "NULL buffer");
     DCC_REQUIRE(Kp > 0, DCC_ERR_SHAPE, "empty contraction");
-    DCC_REQUIRE(map3_ok(epi10) && map3_ok(epi10 + 5), DCC_ERR_SHAPE, "map radices must be >= 1 with R1*R2 < 2^31");
-    GemmEpi epi{{epi10[0], epi10[1], epi10[2], epi10[3], epi10[4]}, {epi10[5], epi10[6], epi10[7], epi10[8], epi10[9]}};
+    GemmEpi ep{map_from(epi, four), map_from(epi + (four ? 7 : 5), four)};
+    DCC_REQUIRE(map_ok(ep.row) && map_ok(ep.col), DCC_ERR_SHAPE, "map radices must be >= 1 with products < 2^31");
     const GemmConfig cfg = g_cfg;
     DCC_REQUIRE(Kp % (cfg.kb_bytes / (kind == 0 ? 2 : 4)) == 0, DCC_ERR_SHAPE,
                 "Kp (%lld) must be a multiple of the k-block", (long long)Kp);
@@ -609,12 +641,12 @@ extern "C" int dcc_gemm_split3_ld(const void *A_hi, const void *A_lo, int64_t ld
     const int nkb = (int)(Kp / (kb / esz));
     const int iM = (int)M, iN = (int)N, gm = cfg.group_m;
     if (wide_epi) {
-        if (kind == 0) return gemm_launch<0, 64, 3, 8>(mAh, mAl, mBh, mBl, iM, iN, nkb, C, epi, alpha, beta, status, gm, st);
-        return gemm_launch<1, 64, 3, 8>(mAh, mAl, mBh, mBl, iM, iN, nkb, C, epi, alpha, beta, status, gm, st);
+        if (kind == 0) return gemm_launch<0, 64, 3, 8>(mAh, mAl, mBh, mBl, iM, iN, nkb, C, ep, alpha, beta, status, gm, st);
+        return gemm_launch<1, 64, 3, 8>(mAh, mAl, mBh, mBl, iM, iN, nkb, C, ep, alpha, beta, status, gm, st);
     }
 #define DCC_GEMM_CASE(K_, KB_, ST_)                                                                           \
     if (kind == K_ && cfg.kb_bytes == KB_ && cfg.stages == ST_)                                              \
-        return gemm_launch<K_, KB_, ST_, 4>(mAh, mAl, mBh, mBl, iM, iN, nkb, C, epi, alpha, beta, status, gm, st);
+        return gemm_launch<K_, KB_, ST_, 4>(mAh, mAl, mBh, mBl, iM, iN, nkb, C, ep, alpha, beta, status, gm, st);
     DCC_GEMM_CASE(0, 128, 2)
     DCC_GEMM_CASE(0, 64, 4)
     DCC_GEMM_CASE(0, 64, 3)
@@ -626,6 +658,20 @@ extern "C" int dcc_gemm_split3_ld(const void *A_hi, const void *A_lo, int64_t ld
 #undef DCC_GEMM_CASE
     set_error("no kernel for k-block %d bytes x %d stages", cfg.kb_bytes, cfg.stages);
     return DCC_ERR_UNSUPPORTED;
+}
+
+extern "C" int dcc_gemm_split3_ld(const void *A_hi, const void *A_lo, int64_t lda, const void *B_hi,
+                                  const void *B_lo, int64_t ldb, int64_t M, int64_t N, int64_t Kp, double *C,
+                                  const int64_t *epi10, double alpha, double beta, int kind, int *status,
+                                  void *stream) {
+    return gemm_split3(A_hi, A_lo, lda, B_hi, B_lo, ldb, M, N, Kp, C, epi10, false, alpha, beta, kind, status, stream);
+}
+
+extern "C" int dcc_gemm_split3_ld4(const void *A_hi, const void *A_lo, int64_t lda, const void *B_hi,
+                                   const void *B_lo, int64_t ldb, int64_t M, int64_t N, int64_t Kp, double *C,
+                                   const int64_t *epi14, double alpha, double beta, int kind, int *status,
+                                   void *stream) {
+    return gemm_split3(A_hi, A_lo, lda, B_hi, B_lo, ldb, M, N, Kp, C, epi14, true, alpha, beta, kind, status, stream);
 }
 
 extern "C" int dcc_gemm_split3(const void *A_hi, const void *A_lo, const void *B_hi, const void *B_lo, int64_t M,

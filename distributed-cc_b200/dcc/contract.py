@@ -22,8 +22,8 @@ f64 = torch.float64
 KIND = {"bf16x3": 0, "tf32x3": 1}
 _KBLK = {0: 64, 1: 32}
 
-_split = L.bind("dcc_split_operand_at", [L.c_vp, L.c_vp, L.c_vp] + [L.c_i64] * 5 + [L.c_vp, L.c_int, L.c_vp])
-_gemm = L.bind("dcc_gemm_split3_ld", [L.c_vp, L.c_vp, L.c_i64, L.c_vp, L.c_vp] + [L.c_i64] * 4 +
+_split = L.bind("dcc_split_operand_at4", [L.c_vp, L.c_vp, L.c_vp] + [L.c_i64] * 5 + [L.c_vp, L.c_int, L.c_vp])
+_gemm = L.bind("dcc_gemm_split3_ld4", [L.c_vp, L.c_vp, L.c_i64, L.c_vp, L.c_vp] + [L.c_i64] * 4 +
                [L.c_vp, L.c_vp, L.c_dbl, L.c_dbl, L.c_int, L.c_vp, L.c_vp])
 
 BIG = 1 << 30  # radix that makes a digit of a map a plain stride (< 2^31)
@@ -44,12 +44,47 @@ def three(R1, R2, S0, S1, S2):
     return (R1, R2, S0, S1, S2)
 
 
-def _i64x10(f, g):
-    """Two three-digit maps as the HOST int64[10] the C ABI takes."""
-    v = tuple(f) + tuple(g)
-    if len(v) != 10:
-        raise ValueError("a map pair needs 2 x 5 values")
-    return (ctypes.c_int64 * 10)(*[int(x) for x in v])
+def four(R1, R2, R3, S0, S1, S2, S3):
+    """m -> (m / (R1 R2 R3)) S0 + ((m / (R2 R3)) % R1) S1 + ((m / R3) % R2) S2 + (m % R3) S3."""
+    return (R1, R2, R3, S0, S1, S2, S3)
+
+
+def as4(f):
+    """A three-digit map (5 values) as the equivalent four-digit map (7 values)."""
+    if len(f) == 7:
+        return tuple(f)
+    if len(f) != 5:
+        raise ValueError("a map has 5 (three-digit) or 7 (four-digit) values")
+    R1, R2, S0, S1, S2 = f
+    return (R1, R2, 1, S0, S1, S2, 0)
+
+
+def _i64x14(f, g):
+    """Two address maps as the HOST int64[14] (two four-digit maps) the C ABI takes."""
+    return (ctypes.c_int64 * 14)(*[int(x) for x in as4(f) + as4(g)])
+
+
+def _max_offset(f, n):
+    """Upper bound of f(m) over m < n for a map with non-negative strides."""
+    R1, R2, R3, S0, S1, S2, S3 = as4(f)
+    if n <= 0:
+        return 0
+    top = (n - 1) // (R1 * R2 * R3)
+    return (top * S0 + min(R1 - 1, (n - 1) // (R2 * R3)) * S1 + min(R2 - 1, (n - 1) // R3) * S2
+            + min(R3 - 1, n - 1) * S3)
+
+
+def _check_span(t, fm, M, fk, K, name):
+    """The maps stay inside t's storage (from t's first element); t is FP64 on a CUDA device."""
+    if not isinstance(t, torch.Tensor) or t.dtype != f64:
+        raise TypeError("%s must be a float64 torch.Tensor" % name)
+    if not t.is_cuda:
+        raise ValueError("%s must be on a CUDA device" % name)
+    if any(x < 0 for x in as4(fm)[3:] + as4(fk)[3:]):
+        raise ValueError("%s: negative map strides" % name)
+    span = t.untyped_storage().nbytes() // 8 - t.storage_offset()
+    if M > 0 and K > 0 and _max_offset(fm, M) + _max_offset(fk, K) >= span:
+        raise ValueError("%s: the address maps reach past the tensor's storage" % name)
 
 
 def padded_k(K, kind):
@@ -84,10 +119,12 @@ class Split:
             self.hi, self.lo = buffers
 
     def fill_piece(self, i, src, fm, fk):
-        """Columns of piece i: dst[m][off + k] = src[fm(m) + fk(k)] (zero past the piece's K)."""
-        L.as_tensor(src, f64, "src")
+        """Columns of piece i: dst[m][off + k] = src[fm(m) + fk(k)] (zero past the piece's K).
+
+        src may be any strided view: the maps address its storage from src's first element."""
+        _check_span(src, fm, self.M, fk, self.pieces[i][1], "src")
         off, k, w = self.pieces[i]
-        L.check(_split(L.ptr(src), L.ptr(self.hi), L.ptr(self.lo), self.M, k, w, self.Kp, off, _i64x10(fm, fk),
+        L.check(_split(L.ptr(src), L.ptr(self.hi), L.ptr(self.lo), self.M, k, w, self.Kp, off, _i64x14(fm, fk),
                        self.kind, L.stream_ptr()))
         return self
 
@@ -110,11 +147,11 @@ def gemm_(A, B, C, frow, fcol, alpha=1.0, beta=1.0, status=None, Kp=None):
         Kp = A.Kp
     if Kp > A.Kp or Kp > B.Kp:
         raise ValueError("Kp exceeds an operand's columns")
-    L.as_tensor(C, f64, "C")
+    _check_span(C, frow, A.M, fcol, B.M, "C")
     if status is None:
         status = torch.zeros(1, dtype=torch.int32, device=C.device)
     L.check(_gemm(L.ptr(A.hi), L.ptr(A.lo), A.Kp, L.ptr(B.hi), L.ptr(B.lo), B.Kp, A.M, B.M, int(Kp), L.ptr(C),
-                  _i64x10(frow, fcol), float(alpha), float(beta), A.kind, L.ptr(status), L.stream_ptr()))
+                  _i64x14(frow, fcol), float(alpha), float(beta), A.kind, L.ptr(status), L.stream_ptr()))
     return status
 
 
@@ -128,6 +165,121 @@ def matmul_split3(A, B, kind="bf16x3"):
     C = torch.zeros((M, N), dtype=f64, device=A.device)
     st = gemm_(a, b, C, lin(N), lin(1), 1.0, 0.0)
     return C, st
+
+
+_status_cache = {}
+
+
+def gemm_status(device):
+    """Device status word shared by the einsum_gemm calls on `device` (zero = no timeout)."""
+    key = str(device)
+    if key not in _status_cache:
+        _status_cache[key] = torch.zeros(1, dtype=torch.int32, device=device)
+    return _status_cache[key]
+
+
+def _group_digits(order, size, strides):
+    """Merge consecutive indices of `order` into digits whose linear index is a
+    single stride in every stride table (dict index -> stride) of `strides`.
+    Returns [(indices, extent, {table: stride})] from slowest to fastest."""
+    groups = []
+    for c in order:
+        if groups:
+            g, ext, st = groups[-1]
+            if all(st[t] == size[c] * tab[c] for t, tab in enumerate(strides)):
+                groups[-1] = (g + [c], ext * size[c], [tab[c] for tab in strides])
+                continue
+        groups.append(([c], size[c], [tab[c] for tab in strides]))
+    return groups
+
+
+def _digit_orders(idx, size, strides, max_digits=4):
+    """An order of idx whose digit grouping has at most max_digits digits (None if none)."""
+    import itertools
+    cand = [list(idx)] + [list(p) for p in itertools.permutations(idx)] if len(idx) <= 6 else [list(idx)]
+    best = None
+    for order in cand:
+        g = _group_digits(order, size, strides)
+        if len(g) <= max_digits:
+            return g
+        if best is None or len(g) < len(best):
+            best = g
+    return None
+
+
+def _map_of(groups, t):
+    """Address map of a digit grouping for stride table t."""
+    if not groups:
+        return lin(0)
+    if len(groups) == 1:
+        return lin(groups[0][2][t])
+    if len(groups) == 2:
+        return two(groups[1][1], groups[0][2][t], groups[1][2][t])
+    if len(groups) == 3:
+        return three(groups[1][1], groups[2][1], groups[0][2][t], groups[1][2][t], groups[2][2][t])
+    return four(groups[1][1], groups[2][1], groups[3][1], groups[0][2][t], groups[1][2][t], groups[2][2][t],
+                groups[3][2][t])
+
+
+def einsum_into(subs, X, Y, out, alpha=1.0, beta=1.0, kind=0, status=None):
+    """out = alpha * einsum(subs, X, Y) + beta * out as ONE split-precision GEMM
+    that reads X and Y in place (no transposed copies) and accumulates straight
+    into `out` (any strides) through the epilogue maps.  Every index must be
+    kept by exactly one operand or contracted (no batch indices), and each of
+    the row, column and contraction index sets must fold into at most four
+    strided digits consistently for the tensors that carry it; otherwise the
+    FP64 torch path is used.  Returns out."""
+    ins, o = subs.split("->")
+    xs, ys = ins.split(",")
+    K = [c for c in xs if c in ys]
+    Mi = [c for c in xs if c not in ys]
+    Ni = [c for c in ys if c not in xs]
+    ok = (sorted(Mi + Ni) == sorted(o) and not any(c in o for c in K) and len(set(xs)) == len(xs)
+          and len(set(ys)) == len(ys) and kind is not None and Mi and Ni and K)
+    gM = gN = gK = None
+    X0, Y0 = X, Y
+    if ok:
+        size = {c: X.shape[xs.index(c)] for c in xs}
+        size.update({c: Y.shape[ys.index(c)] for c in ys})
+        sO = {c: out.stride(o.index(c)) for c in o}
+
+        def strides(T, ts):
+            return {c: T.stride(ts.index(c)) for c in ts}
+
+        gM = _digit_orders(Mi, size, [strides(X, xs), sO])
+        if gM is None:
+            # copy X as [free indices in output order][contracted indices in Y's order]
+            order = sorted(Mi, key=o.index) + K
+            X, xs = X.permute([xs.index(c) for c in order]).contiguous(), "".join(order)
+            gM = _digit_orders(Mi, size, [strides(X, xs), sO])
+        gN = _digit_orders(Ni, size, [strides(Y, ys), sO])
+        if gN is None:
+            order = sorted(Ni, key=o.index) + [c for c in xs if c in K]
+            Y, ys = Y.permute([ys.index(c) for c in order]).contiguous(), "".join(order)
+            gN = _digit_orders(Ni, size, [strides(Y, ys), sO])
+        gK = _digit_orders(K, size, [strides(X, xs), strides(Y, ys)])
+        if gK is None:
+            order = [c for c in ys if c not in K] + [c for c in xs if c in K]
+            Y, ys = Y.permute([ys.index(c) for c in order]).contiguous(), "".join(order)
+            gN = _digit_orders(Ni, size, [strides(Y, ys), sO])
+            gK = _digit_orders(K, size, [strides(X, xs), strides(Y, ys)])
+    if gM is None or gN is None or gK is None:
+        res = torch.einsum(subs, X0, Y0)
+        if beta == 0.0:
+            out.copy_(res).mul_(alpha) if alpha != 1.0 else out.copy_(res)
+        else:
+            if beta != 1.0:
+                out.mul_(beta)
+            out.add_(res, alpha=alpha)
+        return out
+    m = int(np.prod([size[c] for c in Mi]))
+    n = int(np.prod([size[c] for c in Ni]))
+    k = int(np.prod([size[c] for c in K]))
+    a = Split(m, k, kind, X.device).fill(X, _map_of(gM, 0), _map_of(gK, 0))
+    b = Split(n, k, kind, X.device).fill(Y, _map_of(gN, 0), _map_of(gK, 1))
+    st = status if status is not None else gemm_status(X.device)
+    gemm_(a, b, out, _map_of(gM, 1), _map_of(gN, 1), alpha, beta, st)
+    return out
 
 
 # ----------------------------------------------------------------------------

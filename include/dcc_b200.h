@@ -293,6 +293,18 @@ DCC_API int dcc_gemm_split3(const void *A_hi, const void *A_lo, const void *B_hi
                             int64_t N, int64_t Kp, double *C, const int64_t *epi10, double alpha, double beta,
                             int kind, int *status, void *stream);
 
+/* Four-digit address maps, f = {R1, R2, R3, S0, S1, S2, S3}:
+ *   f(m) = (m / (R1 R2 R3)) S0 + ((m / (R2 R3)) % R1) S1 + ((m / R3) % R2) S2 + (m % R3) S3,
+ * for operands and outputs whose row or column index set folds into four
+ * strided digits (the 8-index T4/(Q) blocks of distr_cc/rccsdt_q.py:1014-1129).
+ * Same semantics as dcc_split_operand_at / dcc_gemm_split3_ld otherwise;
+ * map14 / epi14 hold two such maps (HOST). */
+DCC_API int dcc_split_operand_at4(const double *src, void *hi, void *lo, int64_t M, int64_t K, int64_t kw,
+                                  int64_t ld, int64_t k0, const int64_t *map14, int kind, void *stream);
+DCC_API int dcc_gemm_split3_ld4(const void *A_hi, const void *A_lo, int64_t lda, const void *B_hi, const void *B_lo,
+                                int64_t ldb, int64_t M, int64_t N, int64_t Kp, double *C, const int64_t *epi14,
+                                double alpha, double beta, int kind, int *status, void *stream);
+
 /* dcc_gemm_split3 over the first Kp columns of pieces whose rows are lda / ldb
  * elements apart (multiples of 8, >= Kp): one operand of a K-concatenated
  * pair serves a GEMM that needs only its leading piece. */

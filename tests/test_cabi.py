@@ -109,7 +109,7 @@ def test_split_gemm_host_validation_accepts_our_maps(L):
         sp = c.Split(rows, kind=0, device="cpu", pieces=[K, K])
         splits += [(rows, k, w, sp.Kp, off, fm, fk) for (off, k, w), (_, fm, fk) in zip(sp.pieces, ent)]
     for M, Kk, kw, ld, k0, fm, fk in splits:
-        rc = c._split(fake, fake, fake, M, Kk, kw, ld, k0, c._i64x10(fm, fk), 0, None)
+        rc = c._split(fake, fake, fake, M, Kk, kw, ld, k0, c._i64x14(fm, fk), 0, None)
         assert rc == 4, L.last_error()
     # (M, N, Kp, lda, ldb, out maps) of every GEMM
     epis = [(n * nv, nv * nv, 8128, 8128, 8128, er, ec) for _, _, er, ec in c.wvvvv_maps(nv)]
@@ -117,17 +117,17 @@ def test_split_gemm_host_validation_accepts_our_maps(L):
              (no * nv, no * no * nv * nv, 1856, 1856, 1856) + plan["oo"]["out"],
              (no * nv, no * no * nv * nv, 960, 960, 1856) + plan["t1"]["out"]]
     for M, Nn, Kp, lda, ldb, fr, fc in epis:
-        rc = c._gemm(fake, fake, lda, fake, fake, ldb, M, Nn, Kp, fake, c._i64x10(fr, fc), 1.0, 1.0, 0, fake, None)
+        rc = c._gemm(fake, fake, lda, fake, fake, ldb, M, Nn, Kp, fake, c._i64x14(fr, fc), 1.0, 1.0, 0, fake, None)
         assert rc == 4, L.last_error()
-    rc = c._gemm(fake, fake, 100, fake, fake, 100, 10, 10, 100, fake, c._i64x10(c.lin(10), c.lin(1)), 1.0, 0.0, 0,
+    rc = c._gemm(fake, fake, 100, fake, fake, 100, 10, 10, 100, fake, c._i64x14(c.lin(10), c.lin(1)), 1.0, 0.0, 0,
                  fake, None)
     assert rc == 2  # Kp not a multiple of 64
-    rc = c._gemm(fake, fake, 64, fake, fake, 60, 10, 10, 64, fake, c._i64x10(c.lin(10), c.lin(1)), 1.0, 0.0, 0,
+    rc = c._gemm(fake, fake, 64, fake, fake, 60, 10, 10, 64, fake, c._i64x14(c.lin(10), c.lin(1)), 1.0, 0.0, 0,
                  fake, None)
     assert rc == 2  # ldb < Kp
-    rc = c._split(fake, fake, fake, 10, 10, 64, 64, 0, c._i64x10((0, 1, 0, 0, 1), c.lin(1)), 0, None)
+    rc = c._split(fake, fake, fake, 10, 10, 64, 64, 0, c._i64x14((0, 1, 0, 0, 1), c.lin(1)), 0, None)
     assert rc == 2  # radix 0
-    rc = c._split(fake, fake, fake, 10, 10, 64, 100, 64, c._i64x10(c.lin(10), c.lin(1)), 0, None)
+    rc = c._split(fake, fake, fake, 10, 10, 64, 100, 64, c._i64x14(c.lin(10), c.lin(1)), 0, None)
     assert rc == 2  # piece runs past the row pitch
 
 

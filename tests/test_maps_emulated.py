@@ -8,9 +8,9 @@ from dcc import contract as c
 
 
 def fmap(f, m):
-    R1, R2, S0, S1, S2 = f
+    R1, R2, R3, S0, S1, S2, S3 = c.as4(f)
     m = np.asarray(m, dtype=np.int64)
-    return (m // (R1 * R2)) * S0 + ((m // R2) % R1) * S1 + (m % R2) * S2
+    return (m // (R1 * R2 * R3)) * S0 + ((m // (R2 * R3)) % R1) * S1 + ((m // R3) % R2) * S2 + (m % R3) * S3
 
 
 def split(src, M, K, fm, fk):
@@ -97,3 +97,49 @@ def test_wvvvv_maps():
         gemm(split(t3, nb * nv, nv * nv, am, ak), Ws, r, er, ec, 1.0, 1.0)
     ref = e('abde,qdec->qabc', W, t3) + e('acde,qdbe->qabc', W, t3) + e('bcde,qade->qabc', W, t3)
     np.testing.assert_allclose(r.reshape(ref.shape), ref, rtol=0, atol=1e-12)
+
+
+def test_einsum_into_maps():
+    """contract.einsum_into's digit grouping: the split and epilogue maps it builds,
+    emulated in numpy, reproduce torch.einsum for (Q)-style strings, including
+    sliced (non-contiguous) operands and a strided output."""
+    import torch
+    rng = np.random.default_rng(4)
+    no, nv = 2, 5
+    T = torch.from_numpy(rng.standard_normal((3, 4, nv, no, no, no)))
+    W = torch.from_numpy(rng.standard_normal((nv, nv, nv, no)))
+    V = torch.from_numpy(rng.standard_normal((nv, no, no, no)))
+    t2 = torch.from_numpy(rng.standard_normal((nv, nv, no, no)))
+    cases = [('cdel,abeijk->abcdijkl', W[1:3, 2:5], T), ('dmli,abcmjk->abcdijkl', V[2:5], T[:, :, 1:3]),
+             ('cmki,abdmjl->abcdijkl', V[1:3], T[:, :, 2:5]), ('abef,fcjk->abcejk', W[..., 0].reshape(nv, nv, nv, 1)
+                                                                  .expand(nv, nv, nv, nv)[0:2, 1:4].contiguous(), t2[:, 1:3]),
+             ('mnki,abnj->abmijk', torch.from_numpy(rng.standard_normal((no,) * 4)), t2[1:4, 0:2]),
+             ('acdekl,ebij->abcdijkl', torch.from_numpy(rng.standard_normal((2, 3, 2, nv, no, no))), t2[:, 1:3])]
+    checked = 0
+    for subs, X, Y in cases:
+        ref = torch.einsum(subs, X, Y)
+        base = torch.zeros(ref.numel() * 2, dtype=torch.float64)
+        out = base[::2].view(ref.shape)  # every other element: a strided output
+        ins, o = subs.split('->')
+        xs, ys = ins.split(',')
+        K = [ch for ch in xs if ch in ys]
+        Mi = [ch for ch in xs if ch not in ys]
+        Ni = [ch for ch in ys if ch not in xs]
+        size = {ch: X.shape[xs.index(ch)] for ch in xs}
+        size.update({ch: Y.shape[ys.index(ch)] for ch in ys})
+        sX = {ch: X.stride(xs.index(ch)) for ch in xs}
+        sY = {ch: Y.stride(ys.index(ch)) for ch in ys}
+        sO = {ch: out.stride(o.index(ch)) for ch in o}
+        gM, gN, gK = (c._digit_orders(Mi, size, [sX, sO]), c._digit_orders(Ni, size, [sY, sO]),
+                      c._digit_orders(K, size, [sX, sY]))
+        if gM is None or gN is None or gK is None:
+            continue  # more than four digits: einsum_into takes the FP64 path
+        checked += 1
+        m, n, k = (int(np.prod([size[ch] for ch in g])) for g in (Mi, Ni, K))
+        xf = X.as_strided((X.storage().size() - X.storage_offset(),), (1,)).numpy()
+        yf = Y.as_strided((Y.storage().size() - Y.storage_offset(),), (1,)).numpy()
+        A = xf[fmap(c._map_of(gM, 0), np.arange(m))[:, None] + fmap(c._map_of(gK, 0), np.arange(k))[None, :]]
+        B = yf[fmap(c._map_of(gN, 0), np.arange(n))[:, None] + fmap(c._map_of(gK, 1), np.arange(k))[None, :]]
+        gemm(A, B, base.numpy(), c._map_of(gM, 1), c._map_of(gN, 1), 1.0, 0.0)
+        np.testing.assert_allclose(out.numpy(), ref.numpy(), rtol=0, atol=1e-12)
+    assert checked >= 4
