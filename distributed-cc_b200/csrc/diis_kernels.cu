@@ -1,0 +1,197 @@
+// Device DIIS for the unified T1/T2/T3 vector (distr_cc/diis.py:105-177,
+// distr_cc/rccsdt.py:1026-1067): the two vector-length passes of one update.
+//
+//   push:    v = concat(scale_s * seg_s);  e = v - xprev;  x_slot = v;  e_slot = e;
+//            dots[s] = <e, e_other[s]> (s < nother), dots[nother] = <e, e>
+//   combine: xnew = sum_s c_s x_s (in slot order, products rounded before each
+//            addition as numpy's `xnew += xi * ci`);  delta = |xnew - xprev|^2;
+//            xprev = xnew;  seg_s = xnew / scale_s (the unpack of the caller's amplitudes)
+//
+// Both are HBM-bound single passes; the small B-matrix solve stays on the host
+// (numpy eigh / solve, as the reference).  Sums are per-CTA partials reduced in
+// CTA order by a second kernel, so results do not depend on scheduling.
+#include <stdint.h>
+
+#include "dcc_common.cuh"
+
+namespace dcc {
+
+constexpr int DI_THREADS = 256;
+constexpr int DI_MAXS = 16;    // DIIS slots
+constexpr int DI_MAXSEG = 4;   // amplitude segments in the vector
+constexpr int DI_GRID = 148 * 4;
+
+struct DiisSegs {
+    double *p[DI_MAXSEG];
+    double scale[DI_MAXSEG];
+    int64_t start[DI_MAXSEG + 1];  // segment s covers [start[s], start[s+1])
+    int nseg;
+};
+
+struct DiisPtrs {
+    const double *p[DI_MAXS];
+    double c[DI_MAXS];
+    int n;
+};
+
+// Segment holding element i: its base pointer (already offset so that base[i]
+// is the element), and its scale.  Unrolled selects keep everything in registers.
+__device__ __forceinline__ void seg_of(const DiisSegs &g, int64_t i, double *&base, double &scale) {
+    base = g.p[0] - g.start[0];
+    scale = g.scale[0];
+#pragma unroll
+    for (int q = 1; q < DI_MAXSEG; q++)
+        if (q < g.nseg && i >= g.start[q]) {
+            base = g.p[q] - g.start[q];
+            scale = g.scale[q];
+        }
+}
+
+// Block-wide sums of v[0..N) into partial[blockIdx.x * stride + s] for s < n,
+// and of `last` into partial[blockIdx.x * stride + n] (thread 0 writes).
+template <int N>
+__device__ __forceinline__ void block_sums(const double (&v)[N], double last, int n, double *partial, int stride) {
+    __shared__ double red[DI_THREADS / 32][N + 1];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+    for (int s = 0; s <= N; s++) {
+        double x = s < N ? v[s] : last;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+        if (lane == 0) red[w][s] = x;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int s = 0; s <= n; s++) {
+            double x = 0.0;
+            for (int q = 0; q < DI_THREADS / 32; q++) x += red[q][s < n ? s : N];
+            partial[(int64_t)blockIdx.x * stride + s] = x;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(DI_THREADS) k_diis_push(DiisSegs x, int64_t n, double *xprev, double *xslot,
+                                                          double *eslot, DiisPtrs eo, double *partial) {
+    double acc[DI_MAXS];
+    double ee = 0.0;
+#pragma unroll
+    for (int s = 0; s < DI_MAXS; s++) acc[s] = 0.0;
+    for (int64_t i = (int64_t)blockIdx.x * DI_THREADS + threadIdx.x; i < n; i += (int64_t)gridDim.x * DI_THREADS) {
+        double *base;
+        double sc;
+        seg_of(x, i, base, sc);
+        const double v = dmul(sc, base[i]);
+        const double e = dsub(v, xprev[i]);
+        xslot[i] = v;
+        eslot[i] = e;
+#pragma unroll
+        for (int s = 0; s < DI_MAXS; s++)
+            if (s < eo.n) acc[s] = fma(e, eo.p[s][i], acc[s]);
+        ee = fma(e, e, ee);
+    }
+    block_sums(acc, ee, eo.n, partial, DI_MAXS + 1);  // <e, e_s> then <e, e>
+}
+
+__global__ void __launch_bounds__(DI_THREADS) k_diis_combine(DiisPtrs xs, int64_t n, double *xprev, DiisSegs out,
+                                                             double *partial) {
+    double dd = 0.0;
+    for (int64_t i = (int64_t)blockIdx.x * DI_THREADS + threadIdx.x; i < n; i += (int64_t)gridDim.x * DI_THREADS) {
+        double v = 0.0;
+#pragma unroll
+        for (int s = 0; s < DI_MAXS; s++)
+            if (s < xs.n) v = dadd(v, dmul(xs.p[s][i], xs.c[s]));
+        const double d = dsub(v, xprev[i]);
+        dd = fma(d, d, dd);
+        xprev[i] = v;
+        double *base;
+        double sc;
+        seg_of(out, i, base, sc);
+        base[i] = sc == 1.0 ? v : __ddiv_rn(v, sc);
+    }
+    const double none[1] = {0.0};
+    block_sums(none, dd, 0, partial, DI_MAXS + 1);
+}
+
+// out[s] = sum over CTAs of partial[cta][s], CTAs in order.
+__global__ void k_diis_finish(const double *partial, int nblk, int nsum, double *out) {
+    const int s = threadIdx.x;
+    if (s >= nsum) return;
+    double x = 0.0;
+    for (int b = 0; b < nblk; b++) x += partial[(int64_t)b * (DI_MAXS + 1) + s];
+    out[s] = x;
+}
+
+static int make_segs(DiisSegs &g, double *const *seg, const int64_t *seg_n, const double *scale, int nseg,
+                     int64_t &n) {
+    DCC_REQUIRE(nseg >= 1 && nseg <= DI_MAXSEG, DCC_ERR_SHAPE, "1..%d segments", DI_MAXSEG);
+    DCC_REQUIRE(seg && seg_n && scale, DCC_ERR_NULL, "NULL segment table");
+    g = DiisSegs{};
+    g.nseg = nseg;
+    n = 0;
+    for (int s = 0; s < nseg; s++) {
+        DCC_REQUIRE(seg_n[s] >= 0 && (seg[s] || seg_n[s] == 0), DCC_ERR_NULL, "segment %d is NULL", s);
+        DCC_REQUIRE(scale[s] != 0.0, DCC_ERR_SHAPE, "segment %d has scale 0", s);
+        g.p[s] = seg[s];
+        g.scale[s] = scale[s];
+        g.start[s] = n;
+        n += seg_n[s];
+    }
+    for (int s = nseg; s <= DI_MAXSEG; s++) g.start[s] = n;
+    return DCC_OK;
+}
+
+}  // namespace dcc
+
+using namespace dcc;
+
+extern "C" size_t dcc_diis_workspace_bytes(void) { return (size_t)DI_GRID * (DI_MAXS + 1) * sizeof(double); }
+
+extern "C" int dcc_diis_push(double *const *seg, const int64_t *seg_n, const double *seg_scale, int nseg,
+                             double *xprev, double *x_slot, double *e_slot, const double *const *e_other, int nother,
+                             double *dots, void *workspace, size_t workspace_bytes, void *stream) {
+    clear_error();
+    DiisSegs g;
+    int64_t n = 0;
+    int rc = make_segs(g, seg, seg_n, seg_scale, nseg, n);
+    if (rc) return rc;
+    DCC_REQUIRE(nother >= 0 && nother < DI_MAXS, DCC_ERR_SHAPE, "0..%d other slots", DI_MAXS - 1);
+    DCC_REQUIRE(xprev && x_slot && e_slot && dots && workspace && (nother == 0 || e_other), DCC_ERR_NULL,
+                "NULL buffer");
+    DCC_REQUIRE(workspace_bytes >= dcc_diis_workspace_bytes(), DCC_ERR_SHAPE, "workspace too small");
+    DiisPtrs eo{};
+    eo.n = nother;
+    for (int s = 0; s < nother; s++) {
+        DCC_REQUIRE(e_other[s], DCC_ERR_NULL, "other slot %d is NULL", s);
+        eo.p[s] = e_other[s];
+    }
+    cudaStream_t st = as_stream(stream);
+    double *partial = (double *)workspace;
+    k_diis_push<<<DI_GRID, DI_THREADS, 0, st>>>(g, n, xprev, x_slot, e_slot, eo, partial);
+    k_diis_finish<<<1, 32, 0, st>>>(partial, DI_GRID, nother + 1, dots);
+    return launch_status("diis_push");
+}
+
+extern "C" int dcc_diis_combine(const double *const *xs, const double *coef, int nd, double *xprev,
+                                double *const *out_seg, const int64_t *seg_n, const double *seg_scale, int nseg,
+                                double *delta, void *workspace, size_t workspace_bytes, void *stream) {
+    clear_error();
+    DiisSegs g;
+    int64_t n = 0;
+    int rc = make_segs(g, out_seg, seg_n, seg_scale, nseg, n);
+    if (rc) return rc;
+    DCC_REQUIRE(nd >= 1 && nd <= DI_MAXS, DCC_ERR_SHAPE, "1..%d slots", DI_MAXS);
+    DCC_REQUIRE(xs && coef && xprev && delta && workspace, DCC_ERR_NULL, "NULL buffer");
+    DCC_REQUIRE(workspace_bytes >= dcc_diis_workspace_bytes(), DCC_ERR_SHAPE, "workspace too small");
+    DiisPtrs p{};
+    p.n = nd;
+    for (int s = 0; s < nd; s++) {
+        DCC_REQUIRE(xs[s], DCC_ERR_NULL, "slot %d is NULL", s);
+        p.p[s] = xs[s];
+        p.c[s] = coef[s];
+    }
+    cudaStream_t st = as_stream(stream);
+    double *partial = (double *)workspace;
+    k_diis_combine<<<DI_GRID, DI_THREADS, 0, st>>>(p, n, xprev, g, partial);
+    k_diis_finish<<<1, 32, 0, st>>>(partial, DI_GRID, 1, delta);
+    return launch_status("diis_combine");
+}

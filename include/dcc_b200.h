@@ -183,6 +183,31 @@ DCC_API int dcc_t3_perm_gather_tma(double *r3, const int32_t *ijk, int64_t nbloc
                                    const int64_t *strides, const int *masks, int *status, void *stream);
 
 /* ----------------------------------------------------------------------
+ * Device DIIS (replaces the vector passes of distr_cc/diis.py:105-177 as
+ * driven by run_diis_t3, distr_cc/rccsdt.py:1026-1067)
+ * ---------------------------------------------------------------------- */
+
+/* Bytes of the workspace both DIIS passes take (per-CTA partial sums). */
+DCC_API size_t dcc_diis_workspace_bytes(void);
+
+/* v = concat(seg_scale[s] * seg[s]) (nseg <= 4 DEVICE segments of seg_n[s]
+ * doubles, HOST tables); e = v - xprev; x_slot = v; e_slot = e;
+ * dots[s] = <e, e_other[s]> for s < nother (<= 15), dots[nother] = <e, e>
+ * (DEVICE).  The B-matrix row of DIIS.update (distr_cc/diis.py:121-133). */
+DCC_API int dcc_diis_push(double *const *seg, const int64_t *seg_n, const double *seg_scale, int nseg, double *xprev,
+                          double *x_slot, double *e_slot, const double *const *e_other, int nother, double *dots,
+                          void *workspace, size_t workspace_bytes, void *stream);
+
+/* xnew = sum_s coef[s] xs[s] (HOST coefficients, nd <= 16 DEVICE slots, each
+ * product rounded before its addition as distr_cc/diis.py:172-176);
+ * delta[0] = |xnew - xprev|^2 (distr_cc/_runtime.py:90); xprev = xnew;
+ * out_seg[s] = xnew / seg_scale[s] over the segments (the unpack of
+ * distr_cc/_runtime.py:168-187). */
+DCC_API int dcc_diis_combine(const double *const *xs, const double *coef, int nd, double *xprev,
+                             double *const *out_seg, const int64_t *seg_n, const double *seg_scale, int nseg,
+                             double *delta, void *workspace, size_t workspace_bytes, void *stream);
+
+/* ----------------------------------------------------------------------
  * T4 helpers (replace src/rccsdtq.c and PySCF libccsdt.t4_add_)
  * ---------------------------------------------------------------------- */
 
