@@ -1,0 +1,209 @@
+"""The "cuda" einsum backend: the drop-in that routes the reference driver's
+triples hot path onto this library (distr_cc/rccsdt.py, distr_cc/rccsdt_q.py).
+
+`install(rccsdt_module, rccsdt_q_module)` wraps the reference's hot functions
+
+    r1r2_add_t3_tri_(mycc, imds, r1, r2, t3)          distr_cc/rccsdt.py:253
+    intermediates_t3_add_t3_tri(mycc, imds, t3)        distr_cc/rccsdt.py:323
+    compute_r3_tri(mycc, imds, t2, t3)                 distr_cc/rccsdt.py:368
+    rccsdt_q.kernel(mycc, eris, tamps, blksize, comm)  distr_cc/rccsdt_q.py:227
+
+so that, when `mycc.einsum_backend == "cuda"` (set through the reference's
+own RCCSDT.set_einsum_backend, distr_cc/rccsdt.py:1255), they run on the GPU
+with the reference's argument meaning and return values; any other backend
+string calls the original.  The GPU path is one rank only: a communicator of
+size > 1 raises.  When mpi4py is absent, `SingleRankComm` stands in for
+MPI.COMM_WORLD.  Host numpy arrays cross to the device on entry and back on
+exit; the per-shape GPU objects (buffers, splits) are cached on `mycc`.
+"""
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+f64 = torch.float64
+BACKEND = "cuda"
+
+
+class SingleRankComm:
+    """The part of an MPI communicator the reference's one-rank path uses."""
+
+    rank, size = 0, 1
+
+    def Get_rank(self):
+        return 0
+
+    def Get_size(self):
+        return 1
+
+    def bcast(self, obj, root=0):
+        return obj
+
+    def Barrier(self):
+        return None
+
+    def Allreduce(self, sendbuf, recvbuf=None, op=None):
+        # MPI.IN_PLACE or (send, recv) at one rank: recv = send
+        if recvbuf is not None and not isinstance(sendbuf, (str, type(None))) and sendbuf is not recvbuf:
+            try:
+                np.copyto(recvbuf, sendbuf)
+            except TypeError:
+                pass
+        return None
+
+    def allreduce(self, obj, op=None):
+        return obj
+
+
+def comm_size(mycc):
+    comm = getattr(mycc, "comm", None)
+    return 1 if comm is None else int(comm.Get_size())
+
+
+def require_single_rank(mycc):
+    if comm_size(mycc) != 1:
+        raise RuntimeError('einsum backend "cuda" runs on one rank; got a communicator of size %d' % comm_size(mycc))
+
+
+def uses_cuda(mycc):
+    return getattr(mycc, "einsum_backend", None) == BACKEND
+
+
+def _dev(a, device):
+    return torch.as_tensor(np.ascontiguousarray(a), dtype=f64, device=device)
+
+
+class _Inputs:
+    pass
+
+
+def _ijk(nocc, device):
+    from .synthetic import canonical_ijk
+    return torch.tensor(canonical_ijk(nocc), dtype=torch.int32, device=device)
+
+
+def _state(mycc):
+    st = getattr(mycc, "_dcc_state", None)
+    if st is None:
+        st = {}
+        mycc._dcc_state = st
+    return st
+
+
+def precision_of(mycc):
+    return getattr(mycc, "dcc_precision", "bf16x3")
+
+
+def compute_r3_tri(mycc, imds, t2, t3):
+    """r3 for the canonical blocks (distr_cc/rccsdt.py:368-433, OO terms :435-732) on the GPU."""
+    from . import t3_residual
+    require_single_rank(mycc)
+    dev = getattr(mycc, "dcc_device", "cuda")
+    nocc, nvir = mycc.nocc, mycc.nmo - mycc.nocc
+    _, t3_local = t3
+    st = _state(mycc)
+    key = ("r3", nocc, nvir, precision_of(mycc))
+    if key not in st:
+        st[key] = t3_residual.T3Residual(nocc, nvir, precision_of(mycc), dev, with_oo=True)
+    res = st[key]
+    d = _Inputs()
+    for name in ("F_vv", "F_oo", "W_vvvo", "W_vooo", "W_vvvv", "W_ovov", "W_ovvo", "W_oooo"):
+        setattr(d, name, _dev(getattr(imds, name), dev))
+    d.t2 = _dev(t2, dev)
+    d.ijk = _ijk(nocc, dev)
+    r3 = res.compute(d, _dev(t3_local, dev))
+    if not res.status_ok():
+        raise RuntimeError("a bounded wait in a GPU kernel gave up (timeout)")
+    return r3.cpu().numpy()
+
+
+def r1r2_add_t3_tri_(mycc, imds, r1, r2, t3):
+    """distr_cc/rccsdt.py:253-321 on the GPU; r1, r2 updated in place and returned."""
+    from . import t3_feedback
+    require_single_rank(mycc)
+    dev = getattr(mycc, "dcc_device", "cuda")
+    nocc = mycc.nocc
+    _, t3_local = t3
+    dt3 = _dev(t3_local, dev)
+    eris = _dev(imds.t1_eris, dev)
+    d1, d2 = _dev(r1, dev), _dev(r2, dev)
+    t3_feedback.r1_add_t3_(d1, eris, dt3, _ijk(nocc, dev), nocc)
+    X = t3_feedback.p3_201_all(dt3, nocc)
+    t3_feedback.r2_add_t3_(d2, _dev(imds.t1_fock, dev), eris, X, nocc)
+    r1[...] = d1.cpu().numpy()
+    r2[...] = d2.cpu().numpy()
+    return r1, r2
+
+
+def intermediates_t3_add_t3_tri(mycc, imds, t3):
+    """distr_cc/rccsdt.py:323-366 on the GPU; imds.W_vooo, imds.W_vvvo updated in place."""
+    from . import t3_feedback
+    require_single_rank(mycc)
+    dev = getattr(mycc, "dcc_device", "cuda")
+    nocc = mycc.nocc
+    _, t3_local = t3
+    X = t3_feedback.p3_201_all(_dev(t3_local, dev), nocc)
+    Wo, Wv = _dev(imds.W_vooo, dev), _dev(imds.W_vvvo, dev)
+    t3_feedback.intermediates_t3_add_(Wo, Wv, _dev(imds.t1_eris, dev), X, nocc)
+    imds.W_vooo[...] = Wo.cpu().numpy()
+    imds.W_vvvo[...] = Wv.cpu().numpy()
+    return imds
+
+
+def q_kernel(mycc, eris=None, tamps=None, blksize=4, comm=None, job_idx=0, n_jobs=1, log_redistribution=False):
+    """(e_q_bracket, e_q_paren) of distr_cc/rccsdt_q.py:227 on the GPU, one rank, all tasks."""
+    from . import rccsdt_q
+    if comm is not None and int(comm.Get_size()) != 1:
+        raise RuntimeError('einsum backend "cuda" runs on one rank')
+    if n_jobs != 1 or job_idx != 0:
+        raise NotImplementedError("job splitting is a multi-process feature of the reference")
+    dev = getattr(mycc, "dcc_device", "cuda")
+    nocc, nmo = mycc.nocc, mycc.nmo
+    if eris is None:
+        eris = mycc.ao2mo(mycc.mo_coeff)
+    tamps = tamps if tamps is not None else mycc.tamps
+    _, t2, t3 = tamps
+    _, t3_local = t3
+    p = eris.pppp
+    o, v = slice(0, nocc), slice(nocc, nmo)
+    er = {"vvvo": p[v, v, v, o], "vooo": p[v, o, o, o], "vvoo": p[v, v, o, o], "ovvo": p[o, v, v, o],
+          "ovov": p[o, v, o, v], "vvvv": p[v, v, v, v], "oooo": p[o, o, o, o]}
+    er = {k: _dev(a, dev) for k, a in er.items()}
+    nvir = nmo - nocc
+    t2q = t2 if t2.shape == (nvir, nvir, nocc, nocc) else np.ascontiguousarray(np.transpose(t2, (2, 3, 0, 1)))
+    e = np.asarray(eris.mo_energy)
+    return rccsdt_q.q_energy(er, _dev(t2q, dev), _dev(t3_local, dev), _dev(e[:nocc], dev), _dev(e[nocc:], dev),
+                             nocc, nvir, blksize, precision_of(mycc))
+
+
+_ROUTES = {"r1r2_add_t3_tri_": r1r2_add_t3_tri_, "intermediates_t3_add_t3_tri": intermediates_t3_add_t3_tri,
+           "compute_r3_tri": compute_r3_tri}
+
+
+def install(rccsdt_module, rccsdt_q_module=None):
+    """Route the reference's hot functions to the GPU when mycc.einsum_backend == "cuda".
+    Idempotent; returns the names it wrapped."""
+    wrapped = []
+    for name, fn in _ROUTES.items():
+        orig = getattr(rccsdt_module, name, None)
+        if orig is None or getattr(orig, "_dcc_wrapped", False):
+            continue
+
+        def wrapper(mycc, *args, _orig=orig, _fn=fn, **kw):
+            return _fn(mycc, *args, **kw) if uses_cuda(mycc) else _orig(mycc, *args, **kw)
+
+        wrapper._dcc_wrapped = True
+        wrapper.__name__ = name
+        wrapper.__doc__ = orig.__doc__
+        setattr(rccsdt_module, name, wrapper)
+        wrapped.append(name)
+    if rccsdt_q_module is not None:
+        orig = getattr(rccsdt_q_module, "kernel", None)
+        if orig is not None and not getattr(orig, "_dcc_wrapped", False):
+            def qwrap(mycc, *args, _orig=orig, **kw):
+                return q_kernel(mycc, *args, **kw) if uses_cuda(mycc) else _orig(mycc, *args, **kw)
+            qwrap._dcc_wrapped = True
+            qwrap.__name__ = "kernel"
+            rccsdt_q_module.kernel = qwrap
+            wrapped.append("rccsdt_q.kernel")
+    return wrapped

@@ -1,0 +1,60 @@
+"""The "cuda" einsum-backend router on the CPU: wrapped reference functions
+call the GPU implementations only when mycc.einsum_backend == "cuda", call
+the originals otherwise, refuse communicators of more than one rank, and
+install is idempotent; the one-rank communicator shim behaves as MPI at one
+rank."""
+import types
+
+import numpy as np
+import pytest
+
+from dcc import backend
+
+
+def _fake_module():
+    calls = []
+    mod = types.SimpleNamespace()
+    for name in ("r1r2_add_t3_tri_", "intermediates_t3_add_t3_tri", "compute_r3_tri"):
+        def f(mycc, *a, _n=name, **k):
+            calls.append(("orig", _n))
+            return "orig:" + _n
+        setattr(mod, name, f)
+    qmod = types.SimpleNamespace(kernel=lambda mycc, *a, **k: calls.append(("orig", "q")) or "orig:q")
+    return mod, qmod, calls
+
+
+def test_routing_and_idempotence(monkeypatch):
+    mod, qmod, calls = _fake_module()
+    routed = []
+    monkeypatch.setitem(backend._ROUTES, "compute_r3_tri", lambda mycc, *a, **k: routed.append("r3") or "gpu:r3")
+    names = backend.install(mod, qmod)
+    assert set(names) == {"r1r2_add_t3_tri_", "intermediates_t3_add_t3_tri", "compute_r3_tri", "rccsdt_q.kernel"}
+    assert backend.install(mod, qmod) == []  # already wrapped
+    mycc = types.SimpleNamespace(einsum_backend="numpy", comm=backend.SingleRankComm())
+    assert mod.compute_r3_tri(mycc, None, None, None) == "orig:compute_r3_tri"
+    assert qmod.kernel(mycc) == "orig:q"
+    mycc.einsum_backend = "cuda"
+    assert mod.compute_r3_tri(mycc, None, None, None) == "gpu:r3"
+    assert routed == ["r3"]
+
+
+def test_multi_rank_refused():
+    class TwoRanks(backend.SingleRankComm):
+        def Get_size(self):
+            return 2
+    mycc = types.SimpleNamespace(einsum_backend="cuda", comm=TwoRanks(), nocc=2, nmo=5)
+    with pytest.raises(RuntimeError, match="one rank"):
+        backend.compute_r3_tri(mycc, None, None, (None, None))
+    with pytest.raises(RuntimeError, match="one rank"):
+        backend.q_kernel(mycc, comm=TwoRanks())
+
+
+def test_single_rank_comm():
+    c = backend.SingleRankComm()
+    assert c.Get_rank() == 0 and c.Get_size() == 1 and c.bcast(5) == 5 and c.allreduce(3.0) == 3.0
+    send, recv = np.arange(4.0), np.zeros(4)
+    c.Allreduce(send, recv)
+    np.testing.assert_array_equal(recv, send)
+    buf = np.ones(3)
+    c.Allreduce(buf)  # in place
+    np.testing.assert_array_equal(buf, np.ones(3))
