@@ -30,6 +30,7 @@ sys.path.insert(0, ROOT)
 sys.path.insert(0, os.path.join(ROOT, "distributed-cc_b200"))
 
 NOCC, NVIR = 10, 90
+Q_BLK, Q_GROUPS = 4, 24  # (Q) task block and the number of sampled task groups
 METRIC = "RCCSDT T3 iteration time (mixed split-BF16x3 batched path), nocc=10 nvir=90 synthetic"
 UNIT = "s/iter"
 
@@ -229,6 +230,7 @@ def main():
     ap.add_argument("--precision", default="bf16x3", choices=["bf16x3", "tf32x3"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64-path comparison (profiling runs)")
+    ap.add_argument("--no-q", action="store_true", help="skip the (Q) energy sample")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -383,6 +385,38 @@ def main():
     barrier()
     e2e_ms = e0.elapsed_time(e1) / e2e_steps
 
+    # (Q): [Q]/(Q) energies on a sample of task groups (every group = the tasks sharing
+    # (a, b, c) blocks), split path and FP64 path, scaled to all tasks by task count
+    q_line = None
+    if not args.no_q:
+        from dcc import rccsdt_q, _c_rccsdt
+        er = {"vvvo": d.W_vvvo, "vooo": d.W_vooo, "vvoo": d.eris_vvoo, "ovvo": d.W_ovvo, "ovov": d.W_ovov,
+              "vvvv": d.W_vvvv, "oooo": d.W_oooo}
+        t2q = d.t2.permute(2, 3, 0, 1).contiguous()
+        t3_abc = _c_rccsdt.redistribute_ijk_to_abc(d.t3, NOCC, NVIR)
+        G = rccsdt_q.groups(NVIR, Q_BLK)
+        sample = G[::max(1, len(G) // Q_GROUPS)][:Q_GROUPS]
+        ntask = len(rccsdt_q.task_list(NVIR, Q_BLK))
+        nsample = sum(len(rccsdt_q.prange(g[4], NVIR, Q_BLK)) for g in sample)
+        q_line = {"blksize": Q_BLK, "tasks": ntask, "sample_groups": len(sample), "sample_tasks": nsample}
+        for prec in (args.precision, "fp64"):
+            q = rccsdt_q.QEnergy(NOCC, NVIR, Q_BLK, prec)
+            q.run(er, t2q, t3_abc, d.e_occ, d.e_vir, sample[:1])  # warm-up
+            q.out.zero_()
+            barrier()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            q.run(er, t2q, t3_abc, d.e_occ, d.e_vir, sample)
+            e1.record()
+            barrier()
+            ms = e0.elapsed_time(e1)
+            q_line[prec] = {"s_sample": ms / 1e3, "s_all_tasks_est": ms / 1e3 * ntask / nsample,
+                            "e_bracket_sample": float(q.out[0]), "e_paren_sample": float(q.out[1]),
+                            "status_ok": q.status_ok()}
+        q_line["speedup_vs_fp64"] = q_line["fp64"]["s_sample"] / q_line[args.precision]["s_sample"]
+        q_line["abs_dE_paren_sample"] = abs(q_line["fp64"]["e_paren_sample"] - q_line[args.precision]["e_paren_sample"])
+        del t3_abc
+
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
         dt, scale, kind, n = cpu_sample(2)
@@ -413,6 +447,7 @@ def main():
         "cpu_baseline": cpu,
         "e2e": {"value": e2e_ms / 1e3, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "gpu_launches": launches_per_step * args.steps,
+        "q_energy": q_line,
         "clocks": clk.summary(),
     }
     if rank == 0:

@@ -221,6 +221,18 @@ def _map_of(groups, t):
                 groups[3][2][t])
 
 
+_plan_cache = {}
+_split_pool = {}
+
+
+def _pooled_split(m, k, kind, device):
+    """Split buffers reused across einsum_into calls of the same shape (one per role)."""
+    key = (m, k, kind, str(device))
+    if key not in _split_pool:
+        _split_pool[key] = [Split(m, k, kind, device), Split(m, k, kind, device)]
+    return _split_pool[key]
+
+
 def einsum_into(subs, X, Y, out, alpha=1.0, beta=1.0, kind=0, status=None):
     """out = alpha * einsum(subs, X, Y) + beta * out as ONE split-precision GEMM
     that reads X and Y in place (no transposed copies) and accumulates straight
@@ -238,6 +250,16 @@ def einsum_into(subs, X, Y, out, alpha=1.0, beta=1.0, kind=0, status=None):
           and len(set(ys)) == len(ys) and kind is not None and Mi and Ni and K)
     gM = gN = gK = None
     X0, Y0 = X, Y
+    key = (subs, kind, tuple(X.shape), X.stride(), tuple(Y.shape), Y.stride(), out.stride()) if ok else None
+    plan = _plan_cache.get(key)
+    if plan is not None:
+        gM, gN, gK, cx, cy = plan
+        if cx is not None:
+            X, xs = X.permute([xs.index(c) for c in cx]).contiguous(), cx
+        if cy is not None:
+            Y, ys = Y.permute([ys.index(c) for c in cy]).contiguous(), cy
+        ok = False  # planned
+    cx = cy = None
     if ok:
         size = {c: X.shape[xs.index(c)] for c in xs}
         size.update({c: Y.shape[ys.index(c)] for c in ys})
@@ -249,20 +271,22 @@ def einsum_into(subs, X, Y, out, alpha=1.0, beta=1.0, kind=0, status=None):
         gM = _digit_orders(Mi, size, [strides(X, xs), sO])
         if gM is None:
             # copy X as [free indices in output order][contracted indices in Y's order]
-            order = sorted(Mi, key=o.index) + K
-            X, xs = X.permute([xs.index(c) for c in order]).contiguous(), "".join(order)
+            cx = "".join(sorted(Mi, key=o.index) + K)
+            X, xs = X.permute([xs.index(c) for c in cx]).contiguous(), cx
             gM = _digit_orders(Mi, size, [strides(X, xs), sO])
         gN = _digit_orders(Ni, size, [strides(Y, ys), sO])
         if gN is None:
-            order = sorted(Ni, key=o.index) + [c for c in xs if c in K]
-            Y, ys = Y.permute([ys.index(c) for c in order]).contiguous(), "".join(order)
+            cy = "".join(sorted(Ni, key=o.index) + [c for c in xs if c in K])
+            Y, ys = Y.permute([ys.index(c) for c in cy]).contiguous(), cy
             gN = _digit_orders(Ni, size, [strides(Y, ys), sO])
         gK = _digit_orders(K, size, [strides(X, xs), strides(Y, ys)])
         if gK is None:
-            order = [c for c in ys if c not in K] + [c for c in xs if c in K]
-            Y, ys = Y.permute([ys.index(c) for c in order]).contiguous(), "".join(order)
+            cy = "".join([c for c in ys if c not in K] + [c for c in xs if c in K])
+            Y, ys = Y.permute([ys.index(c) for c in cy]).contiguous(), cy
             gN = _digit_orders(Ni, size, [strides(Y, ys), sO])
             gK = _digit_orders(K, size, [strides(X, xs), strides(Y, ys)])
+        if gM is not None and gN is not None and gK is not None:
+            _plan_cache[key] = (gM, gN, gK, cx, cy)
     if gM is None or gN is None or gK is None:
         res = torch.einsum(subs, X0, Y0)
         if beta == 0.0:
@@ -272,11 +296,11 @@ def einsum_into(subs, X, Y, out, alpha=1.0, beta=1.0, kind=0, status=None):
                 out.mul_(beta)
             out.add_(res, alpha=alpha)
         return out
-    m = int(np.prod([size[c] for c in Mi]))
-    n = int(np.prod([size[c] for c in Ni]))
-    k = int(np.prod([size[c] for c in K]))
-    a = Split(m, k, kind, X.device).fill(X, _map_of(gM, 0), _map_of(gK, 0))
-    b = Split(n, k, kind, X.device).fill(Y, _map_of(gN, 0), _map_of(gK, 1))
+    m = int(np.prod([g[1] for g in gM]))
+    n = int(np.prod([g[1] for g in gN]))
+    k = int(np.prod([g[1] for g in gK]))
+    a = _pooled_split(m, k, kind, X.device)[0].fill(X, _map_of(gM, 0), _map_of(gK, 0))
+    b = _pooled_split(n, k, kind, X.device)[1].fill(Y, _map_of(gN, 0), _map_of(gK, 1))
     st = status if status is not None else gemm_status(X.device)
     gemm_(a, b, out, _map_of(gM, 1), _map_of(gN, 1), alpha, beta, st)
     return out
