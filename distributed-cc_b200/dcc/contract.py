@@ -233,14 +233,16 @@ def _pooled_split(m, k, kind, device):
     return _split_pool[key]
 
 
-def einsum_into(subs, X, Y, out, alpha=1.0, beta=1.0, kind=0, status=None):
+def einsum_into(subs, X, Y, out, alpha=1.0, beta=1.0, kind=0, status=None, max_k=None):
     """out = alpha * einsum(subs, X, Y) + beta * out as ONE split-precision GEMM
     that reads X and Y in place (no transposed copies) and accumulates straight
     into `out` (any strides) through the epilogue maps.  Every index must be
     kept by exactly one operand or contracted (no batch indices), and each of
     the row, column and contraction index sets must fold into at most four
     strided digits consistently for the tensors that carry it; otherwise the
-    FP64 torch path is used.  Returns out."""
+    FP64 torch path is used.  max_k: contractions longer than this also take
+    the FP64 path (FP32 accumulation over very long sums, e.g. the reductions
+    of an adjoint, loses digits).  Returns out."""
     ins, o = subs.split("->")
     xs, ys = ins.split(",")
     K = [c for c in xs if c in ys]
@@ -248,6 +250,8 @@ def einsum_into(subs, X, Y, out, alpha=1.0, beta=1.0, kind=0, status=None):
     Ni = [c for c in ys if c not in xs]
     ok = (sorted(Mi + Ni) == sorted(o) and not any(c in o for c in K) and len(set(xs)) == len(xs)
           and len(set(ys)) == len(ys) and kind is not None and Mi and Ni and K)
+    if ok and max_k is not None and int(np.prod([X.shape[xs.index(c)] for c in K])) > max_k:
+        ok = False
     gM = gN = gK = None
     X0, Y0 = X, Y
     key = (subs, kind, tuple(X.shape), X.stride(), tuple(Y.shape), Y.stride(), out.stride()) if ok else None
