@@ -154,15 +154,19 @@ def s_plan(no, nv):
     }
 
 
-def woooo_foo_matrix(W_oooo, F_oo, sym_tol=1e-14):
+def woooo_foo_matrix(W_oooo, F_oo, sym_tol=1e-14, assume_symmetric=False):
     """(A, W_anti): A[(i,j)][(l,m)] = (Ws[l,m,i,j] - F_oo[l,i] delta_mj) / 2 with Ws the
     pair-symmetric part of W_oooo; W_anti = the antisymmetric part, or None when it is
-    below sym_tol relative to max|W_oooo| (one device-to-host read of two scalars)."""
+    below sym_tol relative to max|W_oooo| (one device-to-host read of two scalars) or
+    when assume_symmetric (no host read: usable inside CUDA-graph capture)."""
     no = W_oooo.shape[0]
     Wt = W_oooo.permute(1, 0, 3, 2)
     Wa = 0.5 * (W_oooo - Wt)
-    big = torch.stack([Wa.abs().max(), W_oooo.abs().max()]).cpu()
-    anti = float(big[0]) > sym_tol * max(float(big[1]), 1e-300)
+    if assume_symmetric:
+        anti = False
+    else:
+        big = torch.stack([Wa.abs().max(), W_oooo.abs().max()]).cpu()
+        anti = float(big[0]) > sym_tol * max(float(big[1]), 1e-300)
     Ws = W_oooo - Wa if anti else W_oooo
     eye = torch.eye(no, dtype=W_oooo.dtype, device=W_oooo.device)
     A = 0.5 * Ws.permute(2, 3, 0, 1) - 0.5 * torch.einsum("li,mj->ijlm", F_oo, eye)
@@ -172,8 +176,11 @@ def woooo_foo_matrix(W_oooo, F_oo, sym_tol=1e-14):
 class T3Residual:
     """compute_r3_tri for all canonical blocks of one rank."""
 
-    def __init__(self, nocc, nvir, precision="fp64", device="cuda", with_oo=True):
+    def __init__(self, nocc, nvir, precision="fp64", device="cuda", with_oo=True, woooo_pair_symmetric=False):
         self.no, self.nv, self.precision = int(nocc), int(nvir), precision
+        # True: W_oooo has the pair symmetry of RHF (its antisymmetric part is not checked
+        # for, so compute() reads nothing back to the host and can be captured in a graph)
+        self.woooo_pair_symmetric = woooo_pair_symmetric
         no, nv = self.no, self.nv
         self.n3 = no * (no + 1) * (no + 2) // 6
         self.dev = device
@@ -222,7 +229,7 @@ class T3Residual:
         else:
             self._s_split(d)
         if self.with_oo:
-            A, Wa = woooo_foo_matrix(d.W_oooo, d.F_oo)
+            A, Wa = woooo_foo_matrix(d.W_oooo, d.F_oo, assume_symmetric=self.woooo_pair_symmetric)
             S.view(no * no, -1).addmm_(A, self.U.view(no * no, -1))
             if Wa is not None:
                 if self.Ganti is None:
