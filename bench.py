@@ -329,6 +329,25 @@ def main():
     fp64_steps = max(2, args.steps // 3)
     ms_fp64 = timed_run(fp64, fp64_steps, 3) if fp64 is not None else None
 
+    # the same step captured as one CUDA graph (the synthetic W_oooo has the RHF pair symmetry)
+    from dcc import graph as dgraph
+    mixed.woooo_pair_symmetric = True
+    t3g = d.t3.clone()
+    gstep = dgraph.T3IterationGraph(mixed, d, t3g, r3=r3, norms=norms, workspace=ws)
+    for _ in range(2):
+        gstep.replay()
+    barrier()
+    g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    g0.record()
+    for _ in range(args.steps):
+        gstep.replay()
+    g1.record()
+    barrier()
+    graph_ms = g0.elapsed_time(g1) / args.steps
+    graph_ok = gstep.status_ok()
+    del gstep, t3g
+    mixed.woooo_pair_symmetric = False
+
     gemm_ms = [a.elapsed_time(b) for a, b in gemm_ev]
     gemm_avg = statistics.mean(gemm_ms) if gemm_ms else None
     flops_launch = 2.0 * n3 * NVIR ** 5  # one of the three W_vvvv.t3 strings
@@ -438,6 +457,7 @@ def main():
         "fp64_path_s_per_iter": ms_fp64 / fp64_steps / 1e3 if ms_fp64 else None,
         "speedup_vs_fp64": (ms_fp64 / fp64_steps) / (ms_mixed / args.steps) if ms_fp64 else None,
         "r3_max_rel_err_vs_fp64": rel_err, "device_status_ok": ok,
+        "cuda_graph_ms_per_step": graph_ms, "cuda_graph_status_ok": graph_ok,
         "roofline": {"kernel": "dcc::k_gemm_split3<0> (W_vvvv.t3 string)", "bound": "tensor",
                      "achieved": achieved, "peak": peak_useful, "unit": "TFLOP/s",
                      "frac": (achieved / peak_useful) if achieved else None,
