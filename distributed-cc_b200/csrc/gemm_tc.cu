@@ -414,7 +414,7 @@ __global__ void __launch_bounds__(256) k_split(const double *src, void *hi, void
     const int64_t kt = (int64_t)blockIdx.x * SP_TK;
     if (t < SP_TK) {
         const int64_t k = kt + t;
-        sko[t] = k < K ? map4(mp.k, k) : -1;  // -1: zero column (padding) or outside the piece
+        sko[t] = k < K ? map4_32(mp.k, (uint32_t)k) : -1;  // -1: zero column (padding) or outside the piece
     }
     for (int64_t ty = blockIdx.y; ty < nty; ty += gridDim.y) {
         __syncthreads();  // previous tile fully consumed
@@ -432,7 +432,7 @@ __global__ void __launch_bounds__(256) k_split(const double *src, void *hi, void
                 valid = m < M;
             }
             srow[t] = valid ? m : -1;
-            smo[t] = valid ? map4(mp.m, m) : 0;
+            smo[t] = valid ? map4_32(mp.m, (uint32_t)m) : 0;
         }
         __syncthreads();
         if (mode == 0) {

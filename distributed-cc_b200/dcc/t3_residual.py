@@ -230,6 +230,8 @@ class T3Residual:
             self._s_split(d)
         if self.with_oo:
             A, Wa = woooo_foo_matrix(d.W_oooo, d.F_oo, assume_symmetric=self.woooo_pair_symmetric)
+            # K = nocc^2 against 5.8 GB of U: bandwidth-bound, FP64 (cuBLAS) in both precisions (a split
+            # GEMM would first write a 3.7 GB transposed split of U)
             S.view(no * no, -1).addmm_(A, self.U.view(no * no, -1))
             if Wa is not None:
                 if self.Ganti is None:

@@ -314,7 +314,7 @@ def test_q_division_and_factor(C, oracle):
     assert np.array_equal(host(d), want2)
 
 
-@pytest.mark.parametrize("nocc,nvir", [(1, 3), (3, 5), (4, 9), (3, 17)])
+@pytest.mark.parametrize("nocc,nvir", [(1, 3), (3, 5), (4, 9), (3, 17), (2, 4), (3, 10), (4, 18)])
 def test_unpack_all(C, oracle, nocc, nvir):
     from dcc import t3_residual
     rng = np.random.default_rng(13)
