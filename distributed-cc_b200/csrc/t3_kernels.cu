@@ -1124,110 +1124,6 @@ __global__ void __launch_bounds__(OT_THREADS) k_unpack_all(const double *t3, dou
     }
 }
 
-// Warp-per-orbit-set unpack for even nvir: a warp copies the orbit set of its
-// canonical tile triple for block q (16-byte cp.async into a dense buffer),
-// then for every distinct ordering of q's triple and every tile of the set
-// permutes the source tile into a staging tile (lanes/steps follow
-// tile_element: the permuted reads and the identity writes are conflict-free)
-// and stores it with 16-byte stores.  No CTA-wide barrier.
-constexpr int UW_WARPS = 2;
-// The warp-per-orbit unpack measured slower than k_unpack_all on B200 (5.9 vs 5.4 ms for
-// nocc=10/nvir=90: two warps per CTA leave the SM issue-bound); kept, not dispatched.
-constexpr bool use_warp_unpack = false;
-
-__global__ void __launch_bounds__(32 * UW_WARPS) k_unpack_warp(const double *t3, double *U, int64_t nblocks, int nocc,
-                                                               int nv, int ntile) {
-    extern __shared__ __align__(16) double sm[];  // UW_WARPS x (6 x TE3 + TE3) doubles
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    double *buf = sm + w * 7 * TE3;
-    double *stg = buf + 6 * TE3;
-    int t0, t1, t2;
-    decode_tri3(blockIdx.x, ntile, t0, t1, t2);
-    auto tsel = [&](int m) { return m == 0 ? t0 : (m == 1 ? t1 : t2); };
-    unsigned slot_of = 0;  // slot s holds tile perm_s(T); first slot with the same tile, 3 bits each
-#pragma unroll
-    for (int sl = 0; sl < 6; sl++) {
-        int first = sl;
-#pragma unroll
-        for (int q = sl - 1; q >= 0; q--)
-            if (tsel(perm3(q, 0)) == tsel(perm3(sl, 0)) && tsel(perm3(q, 1)) == tsel(perm3(sl, 1)) &&
-                tsel(perm3(q, 2)) == tsel(perm3(sl, 2)))
-                first = q;
-        slot_of |= (unsigned)first << (3 * sl);
-    }
-    auto sof = [&](int sl) { return (int)((slot_of >> (3 * sl)) & 7u); };
-    const int64_t n3 = (int64_t)nv * nv * nv;
-    const int cy = lane >> 2, cz = 2 * (lane & 3);
-    const unsigned sbase = (unsigned)__cvta_generic_to_shared(buf);
-    for (int64_t q = (int64_t)blockIdx.y * UW_WARPS + w; q < nblocks; q += (int64_t)gridDim.y * UW_WARPS) {
-        const double *blk = t3 + q * n3;
-#pragma unroll 1
-        for (int sl = 0; sl < 6; sl++) {
-            if (sof(sl) != sl) continue;
-            const int gx0 = tsel(perm3(sl, 0)) * TE, gy = tsel(perm3(sl, 1)) * TE + cy, gz = tsel(perm3(sl, 2)) * TE + cz;
-            if (gy >= nv || gz >= nv) continue;
-            const double *src = blk + ((int64_t)gx0 * nv + gy) * nv + gz;
-            const unsigned dst = sbase + 8u * (unsigned)(sl * TE3 + cy * 8 + cz);
-#pragma unroll
-            for (int x = 0; x < TE; x++)
-                if (gx0 + x < nv)
-                    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst + 8u * 64u * x),
-                                 "l"(src + (int64_t)x * nv * nv));
-        }
-        cp_async_commit();
-        int o[3];
-        decode_tri3(q, nocc, o[0], o[1], o[2]);
-        cp_async_wait<0>();
-        __syncwarp();
-#pragma unroll 1
-        for (int sg = 0; sg < 6; sg++) {
-            const int xyz[3] = {o[perm3(sg, 0)], o[perm3(sg, 1)], o[perm3(sg, 2)]};
-            bool dup = false;  // the same ordered triple from an earlier map (repeated indices)
-            for (int sp = 0; sp < sg; sp++)
-                if (o[perm3(sp, 0)] == xyz[0] && o[perm3(sp, 1)] == xyz[1] && o[perm3(sp, 2)] == xyz[2]) dup = true;
-            if (dup) continue;
-            int64_t srt[3];
-            const int cs = order_case3(xyz[0], xyz[1], xyz[2], srt);
-            const int pi = cs == 3 ? 4 : (cs == 4 ? 3 : cs);  // inverse of each axis map
-            const int p0 = perm3(pi, 0), p1 = perm3(pi, 1), p2 = perm3(pi, 2);
-            double *dblk = U + (((int64_t)xyz[0] * nocc + xyz[1]) * nocc + xyz[2]) * n3;
-#pragma unroll 1
-            for (int s = 0; s < 6; s++) {
-                if (sof(s) != s) continue;
-                // output tile = tile s's position; its values come from the slot holding perm_pi(tile s)
-                const int a = tsel(perm3(s, 0)), b = tsel(perm3(s, 1)), c = tsel(perm3(s, 2));
-                auto pick = [&](int m, int v0, int v1, int v2) { return m == 0 ? v0 : (m == 1 ? v1 : v2); };
-                const int want0 = pick(p0, a, b, c), want1 = pick(p1, a, b, c), want2 = pick(p2, a, b, c);
-                int src_slot = 0;
-#pragma unroll
-                for (int r = 5; r >= 0; r--)
-                    if (tsel(perm3(r, 0)) == want0 && tsel(perm3(r, 1)) == want1 && tsel(perm3(r, 2)) == want2)
-                        src_slot = r;
-                src_slot = sof(src_slot);
-                const double *sb = buf + src_slot * TE3;
-#pragma unroll 4
-                for (int j = 0; j < 16; j++) {
-                    int u[3];
-                    tile_element(lane, j, u);
-                    stg[u[0] * 64 + u[1] * 8 + u[2]] =
-                        sb[pick(p0, u[0], u[1], u[2]) * 64 + pick(p1, u[0], u[1], u[2]) * 8 + pick(p2, u[0], u[1], u[2])];
-                }
-                __syncwarp();
-                const int gx0 = a * TE, gy = b * TE + cy, gz = c * TE + cz;
-                if (gy < nv && gz < nv) {
-                    double *dst = dblk + ((int64_t)gx0 * nv + gy) * nv + gz;
-#pragma unroll
-                    for (int x = 0; x < TE; x++)
-                        if (gx0 + x < nv)
-                            *(double2 *)(dst + (int64_t)x * nv * nv) = *(const double2 *)(stg + x * 64 + cy * 8 + cz);
-                }
-                __syncwarp();
-            }
-        }
-        __syncwarp();  // every lane is done with buf before the next block's copies land
-    }
-}
-
 }  // namespace dcc
 
 extern "C" int dcc_t3_unpack_all(const double *t3, double *U, int64_t nocc, int64_t nvir, void *stream) {
@@ -1240,17 +1136,6 @@ extern "C" int dcc_t3_unpack_all(const double *t3, double *U, int64_t nocc, int6
     int64_t ntri = (int64_t)ntile * (ntile + 1) * (ntile + 2) / 6;
     int64_t gy = (148 * 4 * 8 + ntri - 1) / ntri;
     gy = gy < 1 ? 1 : (gy > nblocks ? nblocks : gy);
-    if (use_warp_unpack && nvir % 2 == 0 && ((uintptr_t)t3 & 15) == 0 && ((uintptr_t)U & 15) == 0) {
-        const size_t wsm = (size_t)UW_WARPS * 7 * TE3 * sizeof(double);
-        int64_t wy = (148 * 4 * 4 + ntri - 1) / ntri;
-        const int64_t maxy = (nblocks + UW_WARPS - 1) / UW_WARPS;
-        wy = wy < 1 ? 1 : (wy > maxy ? maxy : wy);
-        wy = wy > 65535 ? 65535 : wy;
-        cudaFuncSetAttribute(k_unpack_warp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wsm);
-        k_unpack_warp<<<dim3((unsigned)ntri, (unsigned)wy), 32 * UW_WARPS, wsm, as_stream(stream)>>>(
-            t3, U, nblocks, (int)nocc, (int)nvir, ntile);
-        return launch_status("t3_unpack_all");
-    }
     size_t smem = 2 * 6 * SLOT * sizeof(double);
     cudaFuncSetAttribute(k_unpack_all, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     k_unpack_all<<<dim3((unsigned)ntri, (unsigned)gy), OT_THREADS, smem, as_stream(stream)>>>(t3, U, nblocks, (int)nocc,
