@@ -393,102 +393,157 @@ __device__ __forceinline__ void split_tf32(double x, float &hi, float &lo) {
 
 // Generic split of a strided FP64 operand into K-major pieces:
 //   dst[m][k0 + k] for m < M, k < kw (k >= K zero-filled) from src[mmap(m) + kmap(k)]
-// with three-digit mixed-radix maps; dst rows are ld elements apart, so a
-// K-concatenated operand is filled piece by piece.  A CTA moves a 32-row x
-// 64-k tile through shared memory: reads run along whichever index is
-// contiguous in the source (mode 0: k; mode 1: m; mode 2: the middle digit of
-// m, the tile's rows then step that digit), writes are 16-byte packs along k.
+// with four-digit mixed-radix maps; dst rows are ld elements apart, so a
+// K-concatenated operand is filled piece by piece.  Reads run along whichever
+// index is contiguous in the source (mode 0: k; mode 1: m; mode 2: the middle
+// digit of m, the tile's rows then step that digit), writes are 16-byte packs
+// along k.
 struct SplitMap {
     Map4 m, k;
 };
 
 constexpr int SP_TM = 32, SP_TK = 64;
+constexpr int SP_WARPS = 4;          // warps per CTA, each with its own tile
+constexpr int SP_PITCH = SP_TK + 1;  // staged elements per row (odd: conflict-free column stores)
 
+// One staged element: the two pieces of one FP64 value.  bf16: hi in the low
+// half-word, lo in the high one; tf32: the two floats.
 template <int KIND>
-__global__ void __launch_bounds__(256) k_split(const double *src, void *hi, void *lo, int64_t M, int64_t K, int64_t kw,
-                                               int64_t ld, int64_t k0, SplitMap mp, int mode, int64_t nty,
-                                               int64_t rmid, int64_t rfast) {
-    __shared__ double tile[SP_TM][SP_TK + 1];
-    __shared__ int64_t smo[SP_TM], srow[SP_TM], sko[SP_TK];
-    const int t = threadIdx.x;
-    const int64_t kt = (int64_t)blockIdx.x * SP_TK;
-    if (t < SP_TK) {
-        const int64_t k = kt + t;
-        sko[t] = k < K ? map4_32(mp.k, (uint32_t)k) : -1;  // -1: zero column (padding) or outside the piece
+struct SplitWord;
+template <>
+struct SplitWord<0> {
+    using T = uint32_t;
+    static __device__ __forceinline__ T make(double x) {
+        __nv_bfloat16 h, l;
+        split_bf16(x, h, l);
+        return (uint32_t)__bfloat16_as_ushort(h) | ((uint32_t)__bfloat16_as_ushort(l) << 16);
     }
-    for (int64_t ty = blockIdx.y; ty < nty; ty += gridDim.y) {
-        __syncthreads();  // previous tile fully consumed
-        if (t < SP_TM) {
-            int64_t m;
-            bool valid;
-            if (mode == 2) {
-                // rows step the second-fastest digit (radix rmid) of m; the fastest has radix rfast
-                const int64_t R1 = rmid, R2 = rfast, nb1 = (R1 + SP_TM - 1) / SP_TM;
-                const int64_t a2 = ty % R2, a1 = ((ty / R2) % nb1) * SP_TM + t, a0 = ty / (R2 * nb1);
-                valid = a1 < R1;
-                m = (a0 * R1 + a1) * R2 + a2;
-            } else {
-                m = ty * SP_TM + t;
-                valid = m < M;
-            }
-            srow[t] = valid ? m : -1;
-            smo[t] = valid ? map4_32(mp.m, (uint32_t)m) : 0;
+};
+template <>
+struct SplitWord<1> {
+    using T = uint2;
+    static __device__ __forceinline__ T make(double x) {
+        float h, l;
+        split_tf32(x, h, l);
+        return make_uint2(__float_as_uint(h), __float_as_uint(l));
+    }
+};
+
+// One warp moves one 32-row x 64-k tile at a time, with no CTA-wide barrier.
+// Each lane holds its tile row's source address (64-bit) and two contraction
+// offsets (32-bit), broadcast by shuffles; loads are issued 16 deep, split at
+// once and staged as pieces (4 bytes per element for bf16, so 24 warps fit on
+// an SM), then 8 lanes per row gather 8 staged elements each and write one
+// 16-byte pack per piece (two for tf32).
+template <int KIND>
+__global__ void __launch_bounds__(32 * SP_WARPS, KIND == 0 ? 6 : 3)
+    k_split(const double *__restrict__ src, void *hi, void *lo, int64_t M, int64_t K, int64_t kw, int64_t ld,
+            int64_t k0, SplitMap mp, int mode, int64_t nty, int64_t rmid, int64_t rfast) {
+    using W = typename SplitWord<KIND>::T;
+    extern __shared__ __align__(16) unsigned char sp_raw[];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    W *tile = reinterpret_cast<W *>(sp_raw) + w * SP_TM * SP_PITCH;
+    const int64_t ntk = (kw + SP_TK - 1) / SP_TK;
+    const int64_t ntiles = nty * ntk;
+    for (int64_t t = (int64_t)blockIdx.x * SP_WARPS + w; t < ntiles; t += (int64_t)gridDim.x * SP_WARPS) {
+        const int64_t ty = t / ntk, kt = (t % ntk) * SP_TK;
+        int64_t row;
+        bool rvalid;
+        if (mode == 2) {
+            const int64_t R1 = rmid, R2 = rfast, nb1 = (R1 + SP_TM - 1) / SP_TM;
+            const int64_t a2 = ty % R2, a1 = ((ty / R2) % nb1) * SP_TM + lane, a0 = ty / (R2 * nb1);
+            rvalid = a1 < R1;
+            row = (a0 * R1 + a1) * R2 + a2;
+        } else {
+            row = ty * SP_TM + lane;
+            rvalid = row < M;
         }
-        __syncthreads();
+        // invalid rows read nothing: their base stays at src and every k offset is masked
+        const double *base = src + (rvalid ? map4_32(mp.m, (uint32_t)row) : 0);
+        const int64_t ka = kt + lane, kb = ka + 32;
+        const int koa = ka < K ? (int)map4_32(mp.k, (uint32_t)ka) : -1;
+        const int kob = kb < K ? (int)map4_32(mp.k, (uint32_t)kb) : -1;
         if (mode == 0) {
-            const int kk = t & (SP_TK - 1);
-            const int64_t ko = sko[kk];
-#pragma unroll
-            for (int r = t >> 6; r < SP_TM; r += 4)
-                tile[r][kk] = (srow[r] >= 0 && ko >= 0) ? __ldg(src + smo[r] + ko) : 0.0;
+#pragma unroll 8
+            for (int r = 0; r < SP_TM; r++) {
+                const double *b = (const double *)__shfl_sync(0xffffffffu, (unsigned long long)base, r);
+                const bool rv = __shfl_sync(0xffffffffu, rvalid, r);
+                const double va = (rv && koa >= 0) ? __ldg(b + koa) : 0.0;
+                const double vb = (rv && kob >= 0) ? __ldg(b + kob) : 0.0;
+                tile[r * SP_PITCH + lane] = SplitWord<KIND>::make(va);
+                tile[r * SP_PITCH + lane + 32] = SplitWord<KIND>::make(vb);
+            }
         } else {
-            const int r = t & 31;
-            const bool rv = srow[r] >= 0;
-            const int64_t mo = smo[r];
-#pragma unroll
-            for (int kk = t >> 5; kk < SP_TK; kk += 8) {
-                const int64_t ko = sko[kk];
-                tile[r][kk] = (rv && ko >= 0) ? __ldg(src + mo + ko) : 0.0;
+#pragma unroll 16
+            for (int kk = 0; kk < SP_TK; kk++) {
+                const int ko = __shfl_sync(0xffffffffu, kk < 32 ? koa : kob, kk & 31);
+                const double v = (rvalid && ko >= 0) ? __ldg(base + ko) : 0.0;
+                tile[lane * SP_PITCH + kk] = SplitWord<KIND>::make(v);
             }
         }
-        __syncthreads();
-        const int r = t >> 3, kc = (t & 7) * 8;
-        const int64_t row = srow[r];
+        __syncwarp();
+        const int kc = (lane & 7) * 8;
         const int64_t kbeg = kt + kc;
-        if (row < 0 || kbeg >= kw) continue;
-        const int64_t dst = row * ld + k0 + kbeg;
-        if (KIND == 0) {
-            __nv_bfloat16 h[8], l[8];
+#pragma unroll 2
+        for (int rr = 0; rr < SP_TM; rr += 4) {
+            const int r = rr + (lane >> 3);
+            const int64_t rrow = __shfl_sync(0xffffffffu, row, r);
+            const bool rv = __shfl_sync(0xffffffffu, rvalid, r);
+            if (!rv || kbeg >= kw) continue;
+            const int64_t dst = rrow * ld + k0 + kbeg;
+            const W *tv = tile + r * SP_PITCH + kc;
+            if constexpr (KIND == 0) {
+                uint32_t e[8];
 #pragma unroll
-            for (int j = 0; j < 8; j++) split_bf16(tile[r][kc + j], h[j], l[j]);
-            __nv_bfloat16 *H = (__nv_bfloat16 *)hi + dst, *Lo = (__nv_bfloat16 *)lo + dst;
-            if (kbeg + 8 <= kw && (dst & 7) == 0) {
-                *(uint4 *)H = *(uint4 *)h;
-                *(uint4 *)Lo = *(uint4 *)l;
-            } else {
-                for (int j = 0; j < 8 && kbeg + j < kw; j++) {
-                    H[j] = h[j];
-                    Lo[j] = l[j];
+                for (int j = 0; j < 8; j++) e[j] = tv[j];
+                __nv_bfloat16 *H = (__nv_bfloat16 *)hi + dst, *Lo = (__nv_bfloat16 *)lo + dst;
+                if (kbeg + 8 <= kw && (dst & 7) == 0) {
+                    uint4 ph, pl;
+                    ph.x = __byte_perm(e[0], e[1], 0x5410);
+                    ph.y = __byte_perm(e[2], e[3], 0x5410);
+                    ph.z = __byte_perm(e[4], e[5], 0x5410);
+                    ph.w = __byte_perm(e[6], e[7], 0x5410);
+                    pl.x = __byte_perm(e[0], e[1], 0x7632);
+                    pl.y = __byte_perm(e[2], e[3], 0x7632);
+                    pl.z = __byte_perm(e[4], e[5], 0x7632);
+                    pl.w = __byte_perm(e[6], e[7], 0x7632);
+                    *(uint4 *)H = ph;
+                    *(uint4 *)Lo = pl;
+                } else {
+                    for (int j = 0; j < 8 && kbeg + j < kw; j++) {
+                        H[j] = __ushort_as_bfloat16((unsigned short)(e[j] & 0xffffu));
+                        Lo[j] = __ushort_as_bfloat16((unsigned short)(e[j] >> 16));
+                    }
                 }
-            }
-        } else {
-            float h[8], l[8];
-#pragma unroll
-            for (int j = 0; j < 8; j++) split_tf32(tile[r][kc + j], h[j], l[j]);
-            float *H = (float *)hi + dst, *Lo = (float *)lo + dst;
-            if (kbeg + 8 <= kw && (dst & 3) == 0) {
-                ((float4 *)H)[0] = *(float4 *)h;
-                ((float4 *)H)[1] = *(float4 *)(h + 4);
-                ((float4 *)Lo)[0] = *(float4 *)l;
-                ((float4 *)Lo)[1] = *(float4 *)(l + 4);
             } else {
-                for (int j = 0; j < 8 && kbeg + j < kw; j++) {
-                    H[j] = h[j];
-                    Lo[j] = l[j];
+                uint2 e[8];
+#pragma unroll
+                for (int j = 0; j < 8; j++) e[j] = tv[j];
+                float *H = (float *)hi + dst, *Lo = (float *)lo + dst;
+                if (kbeg + 8 <= kw && (dst & 3) == 0) {
+                    ((uint4 *)H)[0] = make_uint4(e[0].x, e[1].x, e[2].x, e[3].x);
+                    ((uint4 *)H)[1] = make_uint4(e[4].x, e[5].x, e[6].x, e[7].x);
+                    ((uint4 *)Lo)[0] = make_uint4(e[0].y, e[1].y, e[2].y, e[3].y);
+                    ((uint4 *)Lo)[1] = make_uint4(e[4].y, e[5].y, e[6].y, e[7].y);
+                } else {
+                    for (int j = 0; j < 8 && kbeg + j < kw; j++) {
+                        H[j] = __uint_as_float(e[j].x);
+                        Lo[j] = __uint_as_float(e[j].y);
+                    }
                 }
             }
         }
+        __syncwarp();  // the tile is rewritten by the warp's next item
     }
+}
+
+// Bound on |offset| over the first n indices of a map (a digit never exceeds
+// its radix - 1, nor (n - 1) / the product of the radices inside it).
+static int64_t map_span(const Map4 &f, int64_t n) {
+    const int64_t m = n - 1, r3 = f.R3, r23 = f.R2 * r3, r123 = f.R1 * r23;
+    const int64_t d0 = m / r123, d1 = std::min(f.R1 - 1, m / r23), d2 = std::min(f.R2 - 1, m / r3),
+                  d3 = std::min(f.R3 - 1, m);
+    return d0 * llabs(f.S0) + d1 * llabs(f.S1) + d2 * llabs(f.S2) + d3 * llabs(f.S3);
 }
 
 static bool map_ok(const Map4 &f) {
@@ -567,6 +622,7 @@ static int split_operand(const double *src, void *hi, void *lo, int64_t M, int64
     SplitMap mp{map_from(maps, four), map_from(maps + (four ? 7 : 5), four)};
     DCC_REQUIRE(map_ok(mp.m) && map_ok(mp.k), DCC_ERR_SHAPE, "map radices must be >= 1 with products < 2^31");
     DCC_REQUIRE(M < (1ll << 31) && ld < (1ll << 31), DCC_ERR_SHAPE, "split sizes must fit in 31 bits");
+    DCC_REQUIRE(K == 0 || map_span(mp.k, K) < (1ll << 31), DCC_ERR_SHAPE, "contraction offsets must fit in 31 bits");
     // read along the contiguous source index: k, else m, else m's second-fastest digit
     int64_t ks, kr, ms, mr;
     fast_digit(mp.k, ks, kr);
@@ -583,11 +639,20 @@ static int split_operand(const double *src, void *hi, void *lo, int64_t M, int64
         mode = ks == 1 ? 0 : 1;
     if (mode == 2) DCC_REQUIRE(M % (mid_r * mr) == 0, DCC_ERR_SHAPE, "row map does not tile M");
     const int64_t nty = mode == 2 ? (M / (mid_r * mr)) * ((mid_r + SP_TM - 1) / SP_TM) * mr : (M + SP_TM - 1) / SP_TM;
-    dim3 grid(ceil_div(kw, SP_TK), (unsigned)(nty < 65535 ? nty : 65535));
-    if (kind == 0)
-        k_split<0><<<grid, 256, 0, as_stream(stream)>>>(src, hi, lo, M, K, kw, ld, k0, mp, mode, nty, mid_r, mr);
-    else
-        k_split<1><<<grid, 256, 0, as_stream(stream)>>>(src, hi, lo, M, K, kw, ld, k0, mp, mode, nty, mid_r, mr);
+    const int64_t ntiles = nty * ((kw + SP_TK - 1) / SP_TK);
+    const int64_t nwarp_blocks = (ntiles + SP_WARPS - 1) / SP_WARPS;
+    const int per_sm = kind == 0 ? 6 : 3;  // resident CTAs per SM (shared memory bound)
+    const unsigned grid = (unsigned)(nwarp_blocks < 148 * per_sm ? nwarp_blocks : 148 * per_sm);  // persistent
+    const size_t smem = (size_t)SP_WARPS * SP_TM * SP_PITCH * (kind == 0 ? 4 : 8);
+    if (kind == 0) {
+        cudaFuncSetAttribute(k_split<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        k_split<0><<<grid, 32 * SP_WARPS, smem, as_stream(stream)>>>(src, hi, lo, M, K, kw, ld, k0, mp, mode, nty,
+                                                                      mid_r, mr);
+    } else {
+        cudaFuncSetAttribute(k_split<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        k_split<1><<<grid, 32 * SP_WARPS, smem, as_stream(stream)>>>(src, hi, lo, M, K, kw, ld, k0, mp, mode, nty,
+                                                                      mid_r, mr);
+    }
     return launch_status("split_operand");
 }
 
