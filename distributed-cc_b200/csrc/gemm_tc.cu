@@ -429,111 +429,160 @@ struct SplitWord<1> {
     }
 };
 
-// One warp moves one 32-row x 64-k tile at a time, with no CTA-wide barrier.
-// Each lane holds its tile row's source address (64-bit) and two contraction
-// offsets (32-bit), broadcast by shuffles; loads are issued 16 deep, split at
-// once and staged as pieces (4 bytes per element for bf16, so 24 warps fit on
-// an SM), then 8 lanes per row gather 8 staged elements each and write one
-// 16-byte pack per piece (two for tf32).
+// Split parameters of one operand (a row of the grouped split's table).
+struct SplitArgs {
+    void *hi, *lo;
+    int64_t M, K, kw, ld, k0;
+    SplitMap mp;
+    int64_t nty, rmid, rfast;
+    int32_t mode, src_f32;
+};
+
+__device__ __forceinline__ double split_src(const double *p, int o) { return __ldg(p + o); }
+__device__ __forceinline__ double split_src(const float *p, int o) { return (double)__ldg(p + o); }
+
+// One warp moves one 32-row x 64-k tile (tile row ty, first column kt) with no
+// CTA-wide barrier.  Each lane holds its tile row's source address (64-bit)
+// and two contraction offsets (32-bit), broadcast by shuffles; loads are
+// issued 16 deep, split at once and staged as pieces (4 bytes per element for
+// bf16, so 24 warps fit on an SM), then 8 lanes per row gather 8 staged
+// elements each and write one 16-byte pack per piece (two for tf32).
+template <int KIND, typename S>
+__device__ __forceinline__ void split_tile(const S *__restrict__ src, const SplitArgs &a, int64_t ty, int64_t kt,
+                                           typename SplitWord<KIND>::T *tile, int lane) {
+    using W = typename SplitWord<KIND>::T;
+    int64_t row;
+    bool rvalid;
+    if (a.mode == 2) {
+        const int64_t R1 = a.rmid, R2 = a.rfast, nb1 = (R1 + SP_TM - 1) / SP_TM;
+        const int64_t a2 = ty % R2, a1 = ((ty / R2) % nb1) * SP_TM + lane, a0 = ty / (R2 * nb1);
+        rvalid = a1 < R1;
+        row = (a0 * R1 + a1) * R2 + a2;
+    } else {
+        row = ty * SP_TM + lane;
+        rvalid = row < a.M;
+    }
+    // invalid rows read nothing: their base stays at src and every k offset is masked
+    const S *base = src + (rvalid ? map4_32(a.mp.m, (uint32_t)row) : 0);
+    const int64_t ka = kt + lane, kb = ka + 32;
+    const int koa = ka < a.K ? (int)map4_32(a.mp.k, (uint32_t)ka) : -1;
+    const int kob = kb < a.K ? (int)map4_32(a.mp.k, (uint32_t)kb) : -1;
+    if (a.mode == 0) {
+#pragma unroll 8
+        for (int r = 0; r < SP_TM; r++) {
+            const S *b = (const S *)__shfl_sync(0xffffffffu, (unsigned long long)base, r);
+            const bool rv = __shfl_sync(0xffffffffu, rvalid, r);
+            const double va = (rv && koa >= 0) ? split_src(b, koa) : 0.0;
+            const double vb = (rv && kob >= 0) ? split_src(b, kob) : 0.0;
+            tile[r * SP_PITCH + lane] = SplitWord<KIND>::make(va);
+            tile[r * SP_PITCH + lane + 32] = SplitWord<KIND>::make(vb);
+        }
+    } else {
+#pragma unroll 16
+        for (int kk = 0; kk < SP_TK; kk++) {
+            const int ko = __shfl_sync(0xffffffffu, kk < 32 ? koa : kob, kk & 31);
+            const double v = (rvalid && ko >= 0) ? split_src(base, ko) : 0.0;
+            tile[lane * SP_PITCH + kk] = SplitWord<KIND>::make(v);
+        }
+    }
+    __syncwarp();
+    const int kc = (lane & 7) * 8;
+    const int64_t kbeg = kt + kc;
+#pragma unroll 2
+    for (int rr = 0; rr < SP_TM; rr += 4) {
+        const int r = rr + (lane >> 3);
+        const int64_t rrow = __shfl_sync(0xffffffffu, row, r);
+        const bool rv = __shfl_sync(0xffffffffu, rvalid, r);
+        if (!rv || kbeg >= a.kw) continue;
+        const int64_t dst = rrow * a.ld + a.k0 + kbeg;
+        const W *tv = tile + r * SP_PITCH + kc;
+        if constexpr (KIND == 0) {
+            uint32_t e[8];
+#pragma unroll
+            for (int j = 0; j < 8; j++) e[j] = tv[j];
+            __nv_bfloat16 *H = (__nv_bfloat16 *)a.hi + dst, *Lo = (__nv_bfloat16 *)a.lo + dst;
+            if (kbeg + 8 <= a.kw && (dst & 7) == 0) {
+                uint4 ph, pl;
+                ph.x = __byte_perm(e[0], e[1], 0x5410);
+                ph.y = __byte_perm(e[2], e[3], 0x5410);
+                ph.z = __byte_perm(e[4], e[5], 0x5410);
+                ph.w = __byte_perm(e[6], e[7], 0x5410);
+                pl.x = __byte_perm(e[0], e[1], 0x7632);
+                pl.y = __byte_perm(e[2], e[3], 0x7632);
+                pl.z = __byte_perm(e[4], e[5], 0x7632);
+                pl.w = __byte_perm(e[6], e[7], 0x7632);
+                *(uint4 *)H = ph;
+                *(uint4 *)Lo = pl;
+            } else {
+                for (int j = 0; j < 8 && kbeg + j < a.kw; j++) {
+                    H[j] = __ushort_as_bfloat16((unsigned short)(e[j] & 0xffffu));
+                    Lo[j] = __ushort_as_bfloat16((unsigned short)(e[j] >> 16));
+                }
+            }
+        } else {
+            uint2 e[8];
+#pragma unroll
+            for (int j = 0; j < 8; j++) e[j] = tv[j];
+            float *H = (float *)a.hi + dst, *Lo = (float *)a.lo + dst;
+            if (kbeg + 8 <= a.kw && (dst & 3) == 0) {
+                ((uint4 *)H)[0] = make_uint4(e[0].x, e[1].x, e[2].x, e[3].x);
+                ((uint4 *)H)[1] = make_uint4(e[4].x, e[5].x, e[6].x, e[7].x);
+                ((uint4 *)Lo)[0] = make_uint4(e[0].y, e[1].y, e[2].y, e[3].y);
+                ((uint4 *)Lo)[1] = make_uint4(e[4].y, e[5].y, e[6].y, e[7].y);
+            } else {
+                for (int j = 0; j < 8 && kbeg + j < a.kw; j++) {
+                    H[j] = __uint_as_float(e[j].x);
+                    Lo[j] = __uint_as_float(e[j].y);
+                }
+            }
+        }
+    }
+    __syncwarp();  // the tile is rewritten by the warp's next item
+}
+
+// Persistent: warp w of CTA c takes tiles c * SP_WARPS + w, + gridDim.x * SP_WARPS, ...
 template <int KIND>
 __global__ void __launch_bounds__(32 * SP_WARPS, KIND == 0 ? 6 : 3)
-    k_split(const double *__restrict__ src, void *hi, void *lo, int64_t M, int64_t K, int64_t kw, int64_t ld,
-            int64_t k0, SplitMap mp, int mode, int64_t nty, int64_t rmid, int64_t rfast) {
-    using W = typename SplitWord<KIND>::T;
+    k_split(const double *__restrict__ src, SplitArgs a) {
     extern __shared__ __align__(16) unsigned char sp_raw[];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    W *tile = reinterpret_cast<W *>(sp_raw) + w * SP_TM * SP_PITCH;
-    const int64_t ntk = (kw + SP_TK - 1) / SP_TK;
-    const int64_t ntiles = nty * ntk;
-    for (int64_t t = (int64_t)blockIdx.x * SP_WARPS + w; t < ntiles; t += (int64_t)gridDim.x * SP_WARPS) {
-        const int64_t ty = t / ntk, kt = (t % ntk) * SP_TK;
-        int64_t row;
-        bool rvalid;
-        if (mode == 2) {
-            const int64_t R1 = rmid, R2 = rfast, nb1 = (R1 + SP_TM - 1) / SP_TM;
-            const int64_t a2 = ty % R2, a1 = ((ty / R2) % nb1) * SP_TM + lane, a0 = ty / (R2 * nb1);
-            rvalid = a1 < R1;
-            row = (a0 * R1 + a1) * R2 + a2;
-        } else {
-            row = ty * SP_TM + lane;
-            rvalid = row < M;
-        }
-        // invalid rows read nothing: their base stays at src and every k offset is masked
-        const double *base = src + (rvalid ? map4_32(mp.m, (uint32_t)row) : 0);
-        const int64_t ka = kt + lane, kb = ka + 32;
-        const int koa = ka < K ? (int)map4_32(mp.k, (uint32_t)ka) : -1;
-        const int kob = kb < K ? (int)map4_32(mp.k, (uint32_t)kb) : -1;
-        if (mode == 0) {
-#pragma unroll 8
-            for (int r = 0; r < SP_TM; r++) {
-                const double *b = (const double *)__shfl_sync(0xffffffffu, (unsigned long long)base, r);
-                const bool rv = __shfl_sync(0xffffffffu, rvalid, r);
-                const double va = (rv && koa >= 0) ? __ldg(b + koa) : 0.0;
-                const double vb = (rv && kob >= 0) ? __ldg(b + kob) : 0.0;
-                tile[r * SP_PITCH + lane] = SplitWord<KIND>::make(va);
-                tile[r * SP_PITCH + lane + 32] = SplitWord<KIND>::make(vb);
-            }
-        } else {
-#pragma unroll 16
-            for (int kk = 0; kk < SP_TK; kk++) {
-                const int ko = __shfl_sync(0xffffffffu, kk < 32 ? koa : kob, kk & 31);
-                const double v = (rvalid && ko >= 0) ? __ldg(base + ko) : 0.0;
-                tile[lane * SP_PITCH + kk] = SplitWord<KIND>::make(v);
-            }
-        }
-        __syncwarp();
-        const int kc = (lane & 7) * 8;
-        const int64_t kbeg = kt + kc;
-#pragma unroll 2
-        for (int rr = 0; rr < SP_TM; rr += 4) {
-            const int r = rr + (lane >> 3);
-            const int64_t rrow = __shfl_sync(0xffffffffu, row, r);
-            const bool rv = __shfl_sync(0xffffffffu, rvalid, r);
-            if (!rv || kbeg >= kw) continue;
-            const int64_t dst = rrow * ld + k0 + kbeg;
-            const W *tv = tile + r * SP_PITCH + kc;
-            if constexpr (KIND == 0) {
-                uint32_t e[8];
-#pragma unroll
-                for (int j = 0; j < 8; j++) e[j] = tv[j];
-                __nv_bfloat16 *H = (__nv_bfloat16 *)hi + dst, *Lo = (__nv_bfloat16 *)lo + dst;
-                if (kbeg + 8 <= kw && (dst & 7) == 0) {
-                    uint4 ph, pl;
-                    ph.x = __byte_perm(e[0], e[1], 0x5410);
-                    ph.y = __byte_perm(e[2], e[3], 0x5410);
-                    ph.z = __byte_perm(e[4], e[5], 0x5410);
-                    ph.w = __byte_perm(e[6], e[7], 0x5410);
-                    pl.x = __byte_perm(e[0], e[1], 0x7632);
-                    pl.y = __byte_perm(e[2], e[3], 0x7632);
-                    pl.z = __byte_perm(e[4], e[5], 0x7632);
-                    pl.w = __byte_perm(e[6], e[7], 0x7632);
-                    *(uint4 *)H = ph;
-                    *(uint4 *)Lo = pl;
-                } else {
-                    for (int j = 0; j < 8 && kbeg + j < kw; j++) {
-                        H[j] = __ushort_as_bfloat16((unsigned short)(e[j] & 0xffffu));
-                        Lo[j] = __ushort_as_bfloat16((unsigned short)(e[j] >> 16));
-                    }
-                }
-            } else {
-                uint2 e[8];
-#pragma unroll
-                for (int j = 0; j < 8; j++) e[j] = tv[j];
-                float *H = (float *)hi + dst, *Lo = (float *)lo + dst;
-                if (kbeg + 8 <= kw && (dst & 3) == 0) {
-                    ((uint4 *)H)[0] = make_uint4(e[0].x, e[1].x, e[2].x, e[3].x);
-                    ((uint4 *)H)[1] = make_uint4(e[4].x, e[5].x, e[6].x, e[7].x);
-                    ((uint4 *)Lo)[0] = make_uint4(e[0].y, e[1].y, e[2].y, e[3].y);
-                    ((uint4 *)Lo)[1] = make_uint4(e[4].y, e[5].y, e[6].y, e[7].y);
-                } else {
-                    for (int j = 0; j < 8 && kbeg + j < kw; j++) {
-                        H[j] = __uint_as_float(e[j].x);
-                        Lo[j] = __uint_as_float(e[j].y);
-                    }
-                }
-            }
-        }
-        __syncwarp();  // the tile is rewritten by the warp's next item
+    auto *tile = reinterpret_cast<typename SplitWord<KIND>::T *>(sp_raw) + w * SP_TM * SP_PITCH;
+    const int64_t ntk = (a.kw + SP_TK - 1) / SP_TK;
+    const int64_t ntiles = a.nty * ntk;
+    for (int64_t t = (int64_t)blockIdx.x * SP_WARPS + w; t < ntiles; t += (int64_t)gridDim.x * SP_WARPS)
+        split_tile<KIND>(src, a, t / ntk, (t % ntk) * SP_TK, tile, lane);
+}
+
+// Grouped split: one launch for many operands.  probs[p] holds operand p's
+// parameters and first global tile (tile_begin[p], ascending, with
+// tile_begin[nprob] = total); its source address comes from srcs.p[p], so a
+// table built once is reused with new sources.
+constexpr int SPLIT_GROUP_MAX = DCC_GROUP_MAX;
+struct SplitSrcs {
+    const void *p[SPLIT_GROUP_MAX];
+};
+struct SplitProblem {
+    SplitArgs a;
+    int64_t tile_begin, ntk;
+};
+
+template <int KIND>
+__global__ void __launch_bounds__(32 * SP_WARPS, KIND == 0 ? 6 : 3)
+    k_split_grouped(const SplitProblem *__restrict__ probs, int nprob, int64_t total,
+                    const __grid_constant__ SplitSrcs srcs) {
+    extern __shared__ __align__(16) unsigned char sp_raw[];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    auto *tile = reinterpret_cast<typename SplitWord<KIND>::T *>(sp_raw) + w * SP_TM * SP_PITCH;
+    int p = 0;
+    for (int64_t t = (int64_t)blockIdx.x * SP_WARPS + w; t < total; t += (int64_t)gridDim.x * SP_WARPS) {
+        while (p + 1 < nprob && probs[p + 1].tile_begin <= t) p++;  // t only grows
+        const SplitProblem &pr = probs[p];
+        const int64_t lt = t - pr.tile_begin;
+        const int64_t ty = lt / pr.ntk, kt = (lt % pr.ntk) * SP_TK;
+        if (pr.a.src_f32)
+            split_tile<KIND>((const float *)srcs.p[p], pr.a, ty, kt, tile, lane);
+        else
+            split_tile<KIND>((const double *)srcs.p[p], pr.a, ty, kt, tile, lane);
     }
 }
 
@@ -548,6 +597,246 @@ static int64_t map_span(const Map4 &f, int64_t n) {
 
 static bool map_ok(const Map4 &f) {
     return f.R1 >= 1 && f.R2 >= 1 && f.R3 >= 1 && f.R1 * f.R2 < (1ll << 31) && f.R1 * f.R2 * f.R3 < (1ll << 31);
+}
+
+// ----------------------------------------------------------------- grouped GEMM
+
+// One problem of a grouped GEMM: C[row(m) + col(n)] += alpha * (A B^T)[m][n]
+// through reductions in L2 (red.global.add), so problems that write the same
+// C run concurrently in one launch.  C is float (out_f32) or double.
+struct alignas(64) GemmProblem {
+    CUtensorMap tm[4];  // A hi, A lo, B hi, B lo
+    GemmEpi epi;
+    void *C;
+    double alpha;
+    int M, N, nkb, epi_cols;
+    int num_m, num_n, out_f32, tile_begin;
+};
+
+__device__ __forceinline__ void red_add(float *p, float v) { atomicAdd(p, v); }
+__device__ __forceinline__ void red_add(double *p, double v) { atomicAdd(p, v); }
+
+// Tile t's problem: the last p with tile_begin <= t (tile_begin ascending).
+__device__ __forceinline__ int grouped_find(const int *tb, int nprob, int t) {
+    int lo = 0, hi = nprob - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (tb[mid] <= t)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    return lo;
+}
+
+// One 32-column chunk of a warp's 32 rows: C[row(m) + col(n)] += alpha * v.
+// Offsets are 32-bit (checked on the host); reductions go along whichever of
+// rows or columns is contiguous in C (epi_cols: lanes walk the columns of one
+// row at a time through the warp's transpose buffer).
+template <typename T>
+__device__ __forceinline__ void grouped_store(T *C, T alpha, int epi_cols, const float (&v)[32], float *stg,
+                                              int *offs, int lane, bool rvalid, int nrow, int coff, bool cval,
+                                              int nvalid, int roff) {
+    if (epi_cols) {
+#pragma unroll
+        for (int j = 0; j < 32; j++) stg[lane * 33 + j] = v[j];
+        __syncwarp();
+        if (cval) {
+            T *cp = C + coff;
+            if (nrow == 32) {
+#pragma unroll 8
+                for (int r = 0; r < 32; r++) red_add(cp + offs[r], alpha * (T)stg[r * 33 + lane]);
+            } else {
+                for (int r = 0; r < nrow; r++) red_add(cp + offs[r], alpha * (T)stg[r * 33 + lane]);
+            }
+        }
+        __syncwarp();
+    } else {
+        int *coffs = offs + 32;
+        coffs[lane] = coff;
+        __syncwarp();
+        if (rvalid) {
+            T *rp = C + roff;
+            if (nvalid == 32) {
+#pragma unroll
+                for (int j = 0; j < 32; j++) red_add(rp + coffs[j], alpha * (T)v[j]);
+            } else {
+#pragma unroll
+                for (int j = 0; j < 32; j++)
+                    if (j < nvalid) red_add(rp + coffs[j], alpha * (T)v[j]);
+            }
+        }
+        __syncwarp();
+    }
+}
+
+// Persistent over the tiles of all problems (problem p owns global tiles
+// [tile_begin[p], tile_begin[p+1])); the pipeline is k_gemm_split3's.
+template <int KIND, int KB, int ST, int EPI, typename OutT>
+__global__ void __launch_bounds__(gemm_threads<EPI>(), 1)
+    k_gemm_grouped(const GemmProblem *__restrict__ probs, int nprob, int ntiles, int *status, int group_m) {
+    extern __shared__ __align__(1024) uint8_t g_smem[];
+    uint8_t *base = (uint8_t *)(((uintptr_t)g_smem + 1023) & ~(uintptr_t)1023);
+    constexpr uint32_t A_BYTES = GM * KB, B_BYTES = GN * KB;
+    constexpr uint32_t STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;
+    uint8_t *epi_base = base + ST * STAGE_BYTES;
+    GemmSmem<ST> *cs = (GemmSmem<ST> *)(epi_base + EPI * EPI_WARP_BYTES);
+    int *tb = (int *)(cs + 1);  // tile_begin of every problem
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    // the table's output type must be the one this instance writes
+    if (probs[0].out_f32 != (sizeof(OutT) == 4 ? 1 : 0)) {
+        if (threadIdx.x == 0) atomicExch(status, DCC_ERR_SHAPE);
+        return;
+    }
+    for (int p = threadIdx.x; p < nprob; p += blockDim.x) tb[p] = probs[p].tile_begin;
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < ST; s++) {
+            mbar_init(smem_u32(&cs->full[s]), 1);
+            mbar_init(smem_u32(&cs->empty[s]), 1);
+        }
+        for (int b = 0; b < 2; b++) {
+            mbar_init(smem_u32(&cs->acc_full[b]), 1);
+            mbar_init(smem_u32(&cs->acc_empty[b]), EPI);
+        }
+        mbar_init(smem_u32(&cs->drain), 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         smem_u32(&cs->tmem_base)),
+                     "r"(2 * GN)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = cs->tmem_base;
+
+    if (warp == 0 && lane == 0) {
+        // ---------------- TMA producer
+        uint32_t g = 0;
+        bool ok = true;
+        for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
+            const int p = grouped_find(tb, nprob, t);
+            const GemmProblem &pr = probs[p];
+            int tm, tn;
+            tile_coords(t - tb[p], pr.num_m, pr.num_n, group_m, tm, tn);
+            const int nkb = pr.nkb;
+            for (int kb = 0; kb < nkb; kb++) {
+                const uint32_t s = g % ST, ph = (g / ST) & 1u;
+                if (!mbar_wait(smem_u32(&cs->empty[s]), ph ^ 1u, status)) {
+                    ok = false;
+                    break;
+                }
+                uint8_t *st = base + s * STAGE_BYTES;
+                const uint32_t fb = smem_u32(&cs->full[s]);
+                mbar_expect_tx(fb, STAGE_BYTES);
+                const int kc = kb * (KB / (KIND == 0 ? 2 : 4));
+                tma_load_2d(smem_u32(st), &pr.tm[0], fb, kc, tm * GM);
+                tma_load_2d(smem_u32(st + A_BYTES), &pr.tm[1], fb, kc, tm * GM);
+                tma_load_2d(smem_u32(st + 2 * A_BYTES), &pr.tm[2], fb, kc, tn * GN);
+                tma_load_2d(smem_u32(st + 2 * A_BYTES + B_BYTES), &pr.tm[3], fb, kc, tn * GN);
+                g++;
+            }
+        }
+        if (!ok) {
+            const uint32_t first = g > (uint32_t)ST ? g - ST : 0u;
+            for (uint32_t k = first; k < g; k++) mbar_wait_quiet(smem_u32(&cs->full[k % ST]), (k / ST) & 1u);
+        }
+    } else if (warp == 1 && lane == 0) {
+        // ---------------- MMA issuer
+        constexpr uint32_t idesc = (1u << 4) | ((KIND == 0 ? 1u : 2u) << 7) | ((KIND == 0 ? 1u : 2u) << 10) |
+                                   ((uint32_t)(GN >> 3) << 17) | ((uint32_t)(GM >> 4) << 24);
+        constexpr int KSTEPS = KB / 32;
+        uint32_t g = 0;
+        bool ok = true;
+        int it = 0;
+        for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x, it++) {
+            const int nkb = probs[grouped_find(tb, nprob, t)].nkb;
+            const int b = it & 1;
+            if (!mbar_wait(smem_u32(&cs->acc_empty[b]), (((uint32_t)it >> 1) & 1u) ^ 1u, status)) break;
+            tc_fence_after();
+            const uint32_t d = tmem + (uint32_t)(b * GN);
+            for (int kb = 0; kb < nkb; kb++) {
+                const uint32_t s = g % ST, ph = (g / ST) & 1u;
+                if (!mbar_wait(smem_u32(&cs->full[s]), ph, status)) {
+                    ok = false;
+                    break;
+                }
+                tc_fence_after();
+                const uint32_t st = smem_u32(base + s * STAGE_BYTES);
+                const uint64_t ah = swz_desc<KB>(st), al = swz_desc<KB>(st + A_BYTES),
+                               bh = swz_desc<KB>(st + 2 * A_BYTES), bl = swz_desc<KB>(st + 2 * A_BYTES + B_BYTES);
+#pragma unroll
+                for (int k = 0; k < KSTEPS; k++) {
+                    const uint64_t dk = (uint64_t)(k * 32) >> 4;
+                    const uint32_t first = (kb | k) != 0;
+                    umma<KIND>(d, ah + dk, bh + dk, idesc, first);
+                    umma<KIND>(d, ah + dk, bl + dk, idesc, 1u);
+                    umma<KIND>(d, al + dk, bh + dk, idesc, 1u);
+                }
+                umma_commit(smem_u32(&cs->empty[s]));
+                g++;
+            }
+            if (ok) umma_commit(smem_u32(&cs->acc_full[b]));
+        }
+        umma_commit(smem_u32(&cs->drain));
+        mbar_wait_quiet(smem_u32(&cs->drain), 0u);
+    } else if (warp >= 2) {
+        // ---------------- epilogue: TMEM -> reductions into C
+        const int q = warp & 3;
+        constexpr int CW = GN * 4 / EPI;
+        const int cbeg = ((warp - 2) / 4) * CW, cend = cbeg + CW;
+        float *stg = reinterpret_cast<float *>(epi_base + (warp - 2) * EPI_WARP_BYTES);
+        int *offs = reinterpret_cast<int *>(epi_base + (warp - 2) * EPI_WARP_BYTES + 32 * 33 * 4);
+        int it = 0;
+        for (int t = blockIdx.x; t < ntiles; t += gridDim.x, it++) {
+            const int b = it & 1;
+            bool ok = mbar_wait(smem_u32(&cs->acc_full[b]), ((uint32_t)it >> 1) & 1u, status);
+            ok = __all_sync(0xffffffffu, ok && *(volatile int *)status == 0);
+            if (!ok) break;
+            tc_fence_after();
+            const int p = grouped_find(tb, nprob, t);
+            const GemmProblem &pr = probs[p];
+            const int M = pr.M, N = pr.N, epi_cols = pr.epi_cols;
+            const Map4 rmap = pr.epi.row, cmap = pr.epi.col;
+            OutT *C = (OutT *)pr.C;
+            const OutT alpha = (OutT)pr.alpha;
+            int tm, tn;
+            tile_coords(t - tb[p], pr.num_m, pr.num_n, group_m, tm, tn);
+            const int m0 = tm * GM + q * 32, n0 = tn * GN;
+            const int m = m0 + lane;
+            const int roff = (int)map4_32(rmap, (uint32_t)(m < M ? m : 0));
+            const int nrow = (M - m0) < 32 ? ((M - m0) > 0 ? (M - m0) : 0) : 32;
+            offs[lane] = roff;
+            for (int c = cbeg; c < cend; c += 32) {
+                float v[32];
+                tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * GN + c), v);
+                if (c == cend - 32) {
+                    tc_fence_before();
+                    __syncwarp();
+                    if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(
+                                                    smem_u32(&cs->acc_empty[b]))
+                                                : "memory");
+                }
+                const int col = n0 + c + lane;
+                if (n0 + c >= N) continue;  // warp-uniform: the chunk is past the last column
+                const bool cval = col < N;
+                const int coff = (int)map4_32(cmap, (uint32_t)(cval ? col : 0));
+                const int nvalid = (N - n0 - c) < 32 ? (N - n0 - c) : 32;
+                grouped_store<OutT>(C, alpha, epi_cols, v, stg, offs, lane, m < M, nrow, coff, cval, nvalid, roff);
+            }
+            __syncwarp();
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 1) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * GN) : "memory");
+    }
 }
 
 // ----------------------------------------------------------------- host side
@@ -610,50 +899,143 @@ static int gemm_launch(const CUtensorMap &a, const CUtensorMap &b, const CUtenso
 
 using namespace dcc;
 
-static int split_operand(const double *src, void *hi, void *lo, int64_t M, int64_t K, int64_t kw, int64_t ld,
-                         int64_t k0, const int64_t *maps, bool four, int kind, void *stream) {
-    clear_error();
+// Validated split parameters (mode and tile rows chosen for the maps).
+static int split_args(void *hi, void *lo, int64_t M, int64_t K, int64_t kw, int64_t ld, int64_t k0,
+                      const int64_t *maps, bool four, int src_f32, SplitArgs &a) {
     DCC_REQUIRE(M >= 0 && K >= 0 && kw >= K && k0 >= 0 && k0 + kw <= ld, DCC_ERR_SHAPE,
                 "bad split sizes (M=%lld K=%lld kw=%lld k0=%lld ld=%lld)", (long long)M, (long long)K, (long long)kw,
                 (long long)k0, (long long)ld);
-    DCC_REQUIRE(kind == 0 || kind == 1, DCC_ERR_UNSUPPORTED, "split kind must be 0 (bf16) or 1 (tf32)");
-    if (M == 0 || kw == 0) return DCC_OK;
-    DCC_REQUIRE(src && hi && lo && maps, DCC_ERR_NULL, "NULL buffer");
+    DCC_REQUIRE(hi && lo && maps, DCC_ERR_NULL, "NULL buffer");
     SplitMap mp{map_from(maps, four), map_from(maps + (four ? 7 : 5), four)};
     DCC_REQUIRE(map_ok(mp.m) && map_ok(mp.k), DCC_ERR_SHAPE, "map radices must be >= 1 with products < 2^31");
     DCC_REQUIRE(M < (1ll << 31) && ld < (1ll << 31), DCC_ERR_SHAPE, "split sizes must fit in 31 bits");
     DCC_REQUIRE(K == 0 || map_span(mp.k, K) < (1ll << 31), DCC_ERR_SHAPE, "contraction offsets must fit in 31 bits");
-    // read along the contiguous source index: k, else m, else m's second-fastest digit
+    // read along the contiguous source index: k (mode 0), else m's fastest digit
+    // (mode 1), else another digit of m (mode 2: a tile's 32 rows step that digit)
     int64_t ks, kr, ms, mr;
     fast_digit(mp.k, ks, kr);
     fast_digit(mp.m, ms, mr);
-    const int64_t mid_s = mp.m.R3 > 1 ? mp.m.S2 : mp.m.S1, mid_r = mp.m.R3 > 1 ? mp.m.R2 : mp.m.R1;
-    int mode;
-    if (ks == 1 && kr >= 16)
+    int mode = -1;
+    int64_t rrad = 1, rstep = 1;
+    if (ks == 1 && kr >= 16) {
         mode = 0;
-    else if (ms == 1 || mr == 1)
+    } else if (ms == 1 || mr == 1) {
         mode = 1;
-    else if (mid_s == 1 && mid_r > 1)
-        mode = 2;
-    else
-        mode = ks == 1 ? 0 : 1;
-    if (mode == 2) DCC_REQUIRE(M % (mid_r * mr) == 0, DCC_ERR_SHAPE, "row map does not tile M");
-    const int64_t nty = mode == 2 ? (M / (mid_r * mr)) * ((mid_r + SP_TM - 1) / SP_TM) * mr : (M + SP_TM - 1) / SP_TM;
-    const int64_t ntiles = nty * ((kw + SP_TK - 1) / SP_TK);
+    } else {
+        // digits of m from the fastest: (radix, stride, product of the radices below it)
+        const Map4 &f = mp.m;
+        const int64_t inner = f.R1 * f.R2 * f.R3;
+        const int64_t rad[4] = {f.R3, f.R2, f.R1, M % inner == 0 ? M / inner : 0};
+        const int64_t str[4] = {f.S3, f.S2, f.S1, f.S0};
+        int64_t step = 1;
+        for (int q = 0; q < 4; q++) {
+            if (rad[q] >= 2 && llabs(str[q]) == 1 && q > 0 && M % (rad[q] * step) == 0) {
+                mode = 2;
+                rrad = rad[q];
+                rstep = step;
+                break;
+            }
+            step *= rad[q] > 0 ? rad[q] : 1;
+        }
+        if (mode < 0) mode = ks == 1 ? 0 : 1;
+    }
+    const int64_t nty = mode == 2 ? (M / (rrad * rstep)) * ((rrad + SP_TM - 1) / SP_TM) * rstep : (M + SP_TM - 1) / SP_TM;
+    a = SplitArgs{hi, lo, M, K, kw, ld, k0, mp, nty, rrad, rstep, mode, src_f32};
+    return DCC_OK;
+}
+
+static size_t split_smem(int kind) { return (size_t)SP_WARPS * SP_TM * SP_PITCH * (kind == 0 ? 4 : 8); }
+
+static unsigned split_grid(int64_t ntiles, int kind) {
     const int64_t nwarp_blocks = (ntiles + SP_WARPS - 1) / SP_WARPS;
     const int per_sm = kind == 0 ? 6 : 3;  // resident CTAs per SM (shared memory bound)
-    const unsigned grid = (unsigned)(nwarp_blocks < 148 * per_sm ? nwarp_blocks : 148 * per_sm);  // persistent
-    const size_t smem = (size_t)SP_WARPS * SP_TM * SP_PITCH * (kind == 0 ? 4 : 8);
+    return (unsigned)(nwarp_blocks < 148 * per_sm ? nwarp_blocks : 148 * per_sm);  // persistent
+}
+
+static int split_operand(const double *src, void *hi, void *lo, int64_t M, int64_t K, int64_t kw, int64_t ld,
+                         int64_t k0, const int64_t *maps, bool four, int kind, void *stream) {
+    clear_error();
+    DCC_REQUIRE(kind == 0 || kind == 1, DCC_ERR_UNSUPPORTED, "split kind must be 0 (bf16) or 1 (tf32)");
+    if (M == 0 || kw == 0) return DCC_OK;
+    DCC_REQUIRE(src, DCC_ERR_NULL, "NULL buffer");
+    SplitArgs a;
+    int rc = split_args(hi, lo, M, K, kw, ld, k0, maps, four, 0, a);
+    if (rc) return rc;
+    const int64_t ntiles = a.nty * ((kw + SP_TK - 1) / SP_TK);
+    const unsigned grid = split_grid(ntiles, kind);
+    const size_t smem = split_smem(kind);
     if (kind == 0) {
         cudaFuncSetAttribute(k_split<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        k_split<0><<<grid, 32 * SP_WARPS, smem, as_stream(stream)>>>(src, hi, lo, M, K, kw, ld, k0, mp, mode, nty,
-                                                                      mid_r, mr);
+        k_split<0><<<grid, 32 * SP_WARPS, smem, as_stream(stream)>>>(src, a);
     } else {
         cudaFuncSetAttribute(k_split<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        k_split<1><<<grid, 32 * SP_WARPS, smem, as_stream(stream)>>>(src, hi, lo, M, K, kw, ld, k0, mp, mode, nty,
-                                                                      mid_r, mr);
+        k_split<1><<<grid, 32 * SP_WARPS, smem, as_stream(stream)>>>(src, a);
     }
     return launch_status("split_operand");
+}
+
+extern "C" size_t dcc_split_grouped_table_bytes(int nprob) {
+    return nprob > 0 ? (size_t)nprob * sizeof(SplitProblem) : 0;
+}
+
+extern "C" int dcc_split_grouped_table(const int64_t *spec, int nprob, void *table, size_t table_bytes,
+                                       int64_t *total_tiles) {
+    clear_error();
+    DCC_REQUIRE(nprob >= 1 && nprob <= SPLIT_GROUP_MAX, DCC_ERR_SHAPE, "nprob must be in [1, %d]",
+                SPLIT_GROUP_MAX);
+    DCC_REQUIRE(spec && table && total_tiles, DCC_ERR_NULL, "NULL argument");
+    DCC_REQUIRE(table_bytes >= dcc_split_grouped_table_bytes(nprob), DCC_ERR_WORKSPACE, "table needs %zu bytes",
+                dcc_split_grouped_table_bytes(nprob));
+    SplitProblem *h = (SplitProblem *)malloc(sizeof(SplitProblem) * nprob);
+    DCC_REQUIRE(h, DCC_ERR_CUDA, "host allocation failed");
+    int64_t total = 0;
+    for (int p = 0; p < nprob; p++) {
+        const int64_t *v = spec + (int64_t)p * DCC_SPLIT_SPEC;
+        int rc = split_args((void *)v[0], (void *)v[1], v[2], v[3], v[4], v[5], v[6], v + 7, true, (int)v[21], h[p].a);
+        if (rc == DCC_OK && !(v[21] == 0 || v[21] == 1)) {
+            set_error("source type flag must be 0 (float64) or 1 (float32)");
+            rc = DCC_ERR_SHAPE;
+        }
+        if (rc) {
+            free(h);
+            return rc;
+        }
+        h[p].ntk = (h[p].a.kw + SP_TK - 1) / SP_TK;
+        h[p].tile_begin = total;
+        total += h[p].a.M > 0 ? h[p].a.nty * h[p].ntk : 0;
+    }
+    cudaError_t e = cudaMemcpy(table, h, sizeof(SplitProblem) * nprob, cudaMemcpyHostToDevice);
+    free(h);
+    DCC_REQUIRE(e == cudaSuccess, DCC_ERR_CUDA, "table upload failed: %s", cudaGetErrorString(e));
+    *total_tiles = total;
+    return DCC_OK;
+}
+
+extern "C" int dcc_split_grouped(const void *table, int nprob, int64_t total_tiles, const void *const *srcs, int kind,
+                                 void *stream) {
+    clear_error();
+    DCC_REQUIRE(kind == 0 || kind == 1, DCC_ERR_UNSUPPORTED, "split kind must be 0 (bf16) or 1 (tf32)");
+    DCC_REQUIRE(nprob >= 1 && nprob <= SPLIT_GROUP_MAX, DCC_ERR_SHAPE, "nprob must be in [1, %d]",
+                SPLIT_GROUP_MAX);
+    DCC_REQUIRE(table && srcs, DCC_ERR_NULL, "NULL argument");
+    DCC_REQUIRE(total_tiles >= 0, DCC_ERR_SHAPE, "negative tile count");
+    if (total_tiles == 0) return DCC_OK;
+    SplitSrcs s{};
+    for (int p = 0; p < nprob; p++) {
+        DCC_REQUIRE(srcs[p], DCC_ERR_NULL, "NULL source of operand %d", p);
+        s.p[p] = srcs[p];
+    }
+    const unsigned grid = split_grid(total_tiles, kind);
+    const size_t smem = split_smem(kind);
+    const SplitProblem *pr = (const SplitProblem *)table;
+    if (kind == 0) {
+        cudaFuncSetAttribute(k_split_grouped<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        k_split_grouped<0><<<grid, 32 * SP_WARPS, smem, as_stream(stream)>>>(pr, nprob, total_tiles, s);
+    } else {
+        cudaFuncSetAttribute(k_split_grouped<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        k_split_grouped<1><<<grid, 32 * SP_WARPS, smem, as_stream(stream)>>>(pr, nprob, total_tiles, s);
+    }
+    return launch_status("split_grouped");
 }
 
 extern "C" int dcc_split_operand_at(const double *src, void *hi, void *lo, int64_t M, int64_t K, int64_t kw,
@@ -743,6 +1125,129 @@ extern "C" int dcc_gemm_split3(const void *A_hi, const void *A_lo, const void *B
                                int64_t N, int64_t Kp, double *C, const int64_t *epi10, double alpha, double beta,
                                int kind, int *status, void *stream) {
     return dcc_gemm_split3_ld(A_hi, A_lo, Kp, B_hi, B_lo, Kp, M, N, Kp, C, epi10, alpha, beta, kind, status, stream);
+}
+
+extern "C" size_t dcc_gemm_grouped_table_bytes(int nprob) {
+    return nprob > 0 ? (size_t)nprob * sizeof(GemmProblem) : 0;
+}
+
+extern "C" int dcc_gemm_grouped_table(const int64_t *spec, const double *alpha, int nprob, int kind, void *table,
+                                      size_t table_bytes, int64_t *total_tiles) {
+    clear_error();
+    DCC_REQUIRE(kind == 0 || kind == 1, DCC_ERR_UNSUPPORTED, "kind must be 0 (bf16x3) or 1 (tf32x3)");
+    DCC_REQUIRE(nprob >= 1 && nprob <= DCC_GROUP_MAX, DCC_ERR_SHAPE, "nprob must be in [1, %d]", DCC_GROUP_MAX);
+    DCC_REQUIRE(spec && alpha && table && total_tiles, DCC_ERR_NULL, "NULL argument");
+    DCC_REQUIRE(table_bytes >= dcc_gemm_grouped_table_bytes(nprob), DCC_ERR_WORKSPACE, "table needs %zu bytes",
+                dcc_gemm_grouped_table_bytes(nprob));
+    DCC_REQUIRE(((uintptr_t)table & 63) == 0, DCC_ERR_SHAPE, "table must be 64-byte aligned");
+    const int kb = 64, esz = kind == 0 ? 2 : 4, kblk = kb / esz;
+    GemmProblem *h = (GemmProblem *)aligned_alloc(64, sizeof(GemmProblem) * nprob);
+    DCC_REQUIRE(h, DCC_ERR_CUDA, "host allocation failed");
+    memset((void *)h, 0, sizeof(GemmProblem) * nprob);
+    int64_t total = 0;
+    int rc = DCC_OK;
+    for (int p = 0; p < nprob && rc == DCC_OK; p++) {
+        const int64_t *v = spec + (int64_t)p * DCC_GEMM_SPEC;
+        const int64_t lda = v[2], ldb = v[5], M = v[6], N = v[7], Kp = v[8];
+        if (!(M >= 1 && N >= 1 && M < (1ll << 31) && N < (1ll << 31) && Kp >= kblk && Kp % kblk == 0 && lda >= Kp &&
+              ldb >= Kp && lda % 8 == 0 && ldb % 8 == 0 && lda < (1ll << 31) && ldb < (1ll << 31))) {
+            set_error("problem %d: bad sizes (M=%lld N=%lld Kp=%lld lda=%lld ldb=%lld)", p, (long long)M,
+                      (long long)N, (long long)Kp, (long long)lda, (long long)ldb);
+            rc = DCC_ERR_SHAPE;
+            break;
+        }
+        if (!(v[0] && v[1] && v[3] && v[4] && v[9]) || !(v[10] == 0 || v[10] == 1)) {
+            set_error("problem %d: NULL operand or bad output type", p);
+            rc = DCC_ERR_NULL;
+            break;
+        }
+        GemmProblem &g = h[p];
+        g.epi = GemmEpi{map_from(v + 11, true), map_from(v + 18, true)};
+        if (!map_ok(g.epi.row) || !map_ok(g.epi.col)) {
+            set_error("problem %d: map radices must be >= 1 with products < 2^31", p);
+            rc = DCC_ERR_SHAPE;
+            break;
+        }
+        if ((rc = make_map(&g.tm[0], (void *)v[0], kind, M, Kp, lda, GM, kb)) ||
+            (rc = make_map(&g.tm[1], (void *)v[1], kind, M, Kp, lda, GM, kb)) ||
+            (rc = make_map(&g.tm[2], (void *)v[3], kind, N, Kp, ldb, GN, kb)) ||
+            (rc = make_map(&g.tm[3], (void *)v[4], kind, N, Kp, ldb, GN, kb)))
+            break;
+        if (map_span(g.epi.row, M) + map_span(g.epi.col, N) >= (1ll << 31)) {
+            set_error("problem %d: output offsets must fit in 31 bits", p);
+            rc = DCC_ERR_SHAPE;
+            break;
+        }
+        if (v[10] != spec[10]) {
+            set_error("problem %d: every problem of a table has the same output type", p);
+            rc = DCC_ERR_SHAPE;
+            break;
+        }
+        int64_t cs, cr, rs, rr;
+        fast_digit(g.epi.col, cs, cr);
+        fast_digit(g.epi.row, rs, rr);
+        g.epi_cols = (cs == 1 || rs != 1) ? 1 : 0;
+        g.C = (void *)v[9];
+        g.out_f32 = (int)v[10];
+        g.alpha = alpha[p];
+        g.M = (int)M;
+        g.N = (int)N;
+        g.nkb = (int)(Kp / kblk);
+        g.num_m = (int)ceil_div(M, GM);
+        g.num_n = (int)ceil_div(N, GN);
+        g.tile_begin = (int)total;
+        total += (int64_t)g.num_m * g.num_n;
+        if (total >= (1ll << 31)) {
+            set_error("too many output tiles");
+            rc = DCC_ERR_SHAPE;
+        }
+    }
+    if (rc == DCC_OK) {
+        cudaError_t e = cudaMemcpy(table, h, sizeof(GemmProblem) * nprob, cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) {
+            set_error("table upload failed: %s", cudaGetErrorString(e));
+            rc = DCC_ERR_CUDA;
+        }
+    }
+    free(h);
+    if (rc == DCC_OK) *total_tiles = total;
+    return rc;
+}
+
+extern "C" int dcc_gemm_grouped(const void *table, int nprob, int64_t total_tiles, int kind, int out_f32,
+                                int *status, void *stream) {
+    clear_error();
+    DCC_REQUIRE(kind == 0 || kind == 1, DCC_ERR_UNSUPPORTED, "kind must be 0 (bf16x3) or 1 (tf32x3)");
+    DCC_REQUIRE(nprob >= 1 && nprob <= DCC_GROUP_MAX, DCC_ERR_SHAPE, "nprob must be in [1, %d]", DCC_GROUP_MAX);
+    DCC_REQUIRE(table && status, DCC_ERR_NULL, "NULL argument");
+    DCC_REQUIRE(out_f32 == 0 || out_f32 == 1, DCC_ERR_SHAPE, "out_f32 must be 0 or 1");
+    DCC_REQUIRE(total_tiles >= 0 && total_tiles < (1ll << 31), DCC_ERR_SHAPE, "bad tile count");
+    if (total_tiles == 0) return DCC_OK;
+    int dev = 0, nsm = 148;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    const unsigned grid = (unsigned)(total_tiles < nsm ? total_tiles : nsm);
+    constexpr int GE = 16;  // epilogue warps: the reductions, not the MMAs, bound these short-K problems
+    const size_t smem = gemm_smem_bytes<3, GE>(64) + (size_t)nprob * sizeof(int);
+    const GemmProblem *pr = (const GemmProblem *)table;
+    cudaStream_t st = as_stream(stream);
+    const int gm = g_cfg.group_m;
+#define DCC_GROUPED(K_, T_)                                                                                       \
+    do {                                                                                                          \
+        cudaFuncSetAttribute(k_gemm_grouped<K_, 64, 3, GE, T_>, cudaFuncAttributeMaxDynamicSharedMemorySize,     \
+                             (int)smem);                                                                          \
+        k_gemm_grouped<K_, 64, 3, GE, T_><<<grid, gemm_threads<GE>(), smem, st>>>(pr, nprob, (int)total_tiles,   \
+                                                                                  status, gm);                   \
+    } while (0)
+    if (kind == 0 && out_f32)
+        DCC_GROUPED(0, float);
+    else if (kind == 0)
+        DCC_GROUPED(0, double);
+    else if (out_f32)
+        DCC_GROUPED(1, float);
+    else
+        DCC_GROUPED(1, double);
+#undef DCC_GROUPED
+    return launch_status("gemm_grouped");
 }
 
 extern "C" int dcc_gemm_set_config(int kb_bytes, int stages, int group_m) {

@@ -2,6 +2,8 @@
 // factor kernels, and one fused per-task epilogue that evaluates
 //   t~4 = factor(abcd) * P4_444_ijkl((t4 + z4) / D)
 // and both energy dot products without writing any block back.
+#include <utility>
+
 #include "s4_orbit.cuh"
 
 namespace dcc {
@@ -149,6 +151,184 @@ __global__ void k_q_finish(const double *ws, int64_t n, double *out) {
     }
 }
 
+// ----------------------------------------------------------------- group epilogue
+//
+// A task group's blocks z4 (T3-connected) and t4 (T2-connected), stored
+// [i][j][k][l][ia][ib][ic][id] with the virtual quadruple fastest: one warp
+// takes one ijkl orbit and 32 consecutive quadruples (lanes), so every load
+// of a position is one coalesced row, and each lane holds its quadruple's 24
+// orbit values in registers.  The P4 stages then read partners at compile-time
+// register indices; per position the arithmetic is the task epilogue's
+// expression, term for term.
+
+// p[m] of the lexicographic permutation l of {0,1,2,3}
+__host__ __device__ constexpr int perm4_at(int l, int m) {
+    int avail[4] = {0, 1, 2, 3}, p[4] = {0, 0, 0, 0}, f[3] = {6, 2, 1}, n = 4;
+    for (int s = 0; s < 3; s++) {
+        const int q = l / f[s];
+        l %= f[s];
+        p[s] = avail[q];
+        for (int t = q; t < n - 1; t++) avail[t] = avail[t + 1];
+        n--;
+    }
+    p[3] = avail[0];
+    return p[m];
+}
+
+// lane of the permutation l with slots of transposition s (ab, ac, ad, bc, bd, cd) swapped
+__host__ __device__ constexpr int partner4(int l, int s) {
+    int q[4] = {perm4_at(l, 0), perm4_at(l, 1), perm4_at(l, 2), perm4_at(l, 3)};
+    const int i = (s < 3) ? 0 : (s < 5 ? 1 : 2), j = (s < 3) ? s + 1 : (s < 5 ? s - 1 : 3);
+    const int t = q[i];
+    q[i] = q[j];
+    q[j] = t;
+    int r = 0, f[3] = {6, 2, 1};
+    for (int m = 0; m < 3; m++) {
+        int smaller = 0;
+        for (int u = m + 1; u < 4; u++) smaller += q[u] < q[m];
+        r += smaller * f[m];
+    }
+    return r;
+}
+
+template <int S>
+__device__ __forceinline__ double p4_t1_at(const double (&x)[24], const P4Coef &k) {
+    constexpr int ab = partner4(S, 0), ac = partner4(S, 1), ad = partner4(S, 2);
+    return dadd(dadd(dadd(dmul(k.p[0], x[S]), dmul(k.p[1], x[ab])), dmul(k.p[2], x[ac])), dmul(k.p[3], x[ad]));
+}
+template <int S>
+__device__ __forceinline__ double p4_t2_at(const double (&t1)[24], const P4Coef &k) {
+    constexpr int bc = partner4(S, 3), bd = partner4(S, 4);
+    return dadd(dadd(dmul(k.p[4], t1[S]), dmul(k.p[5], t1[bc])), dmul(k.p[6], t1[bd]));
+}
+// R without its beta term (beta = 0 for P4_444: beta * x adds a signed zero only)
+template <int S>
+__device__ __forceinline__ double p4_r0_at(const double (&t2)[24], const P4Coef &k) {
+    constexpr int cd = partner4(S, 5);
+    return dmul(k.alpha, dadd(dmul(k.p[7], t2[S]), dmul(k.p[8], t2[cd])));
+}
+template <int... S>
+__device__ __forceinline__ void p4_t1_all(const double (&x)[24], double (&t1)[24], const P4Coef &k,
+                                          std::integer_sequence<int, S...>) {
+    ((t1[S] = p4_t1_at<S>(x, k)), ...);
+}
+template <int... S>
+__device__ __forceinline__ void p4_t2_all(const double (&t1)[24], double (&t2)[24], const P4Coef &k,
+                                          std::integer_sequence<int, S...>) {
+    ((t2[S] = p4_t2_at<S>(t1, k)), ...);
+}
+template <int... S>
+__device__ __forceinline__ void p4_r0_all(const double (&t2)[24], double (&r)[24], const P4Coef &k,
+                                          std::integer_sequence<int, S...>) {
+    ((r[S] = p4_r0_at<S>(t2, k)), ...);
+}
+
+struct QGroup {
+    int a0, b0, c0, d0, ba, bb, bc, dn;
+};
+
+constexpr int QG_THREADS = 128;
+constexpr int QG_WARPS = QG_THREADS / 32;
+
+__device__ __forceinline__ double q_load(const double *p) { return __ldcs(p); }
+__device__ __forceinline__ double q_load(const float *p) { return (double)__ldcs(p); }
+
+// vvooT / t2T: [x][p][q][y] = vvoo / t2 [x][y][p][q] (second virtual fastest).
+template <typename T>
+__global__ void __launch_bounds__(QG_THREADS) k_q_group_epilogue(const T *t4, const T *z4, const double *vvooT,
+                                                                 const double *t2T, const double *eo, const double *ev,
+                                                                 QGroup g, int no, int nv, int64_t norb, P4Coef k,
+                                                                 double *ws) {
+    const int lane = threadIdx.x & 31;
+    const int64_t V = (int64_t)g.ba * g.bb * g.bc * g.dn;
+    const int64_t nchunk = (V + 31) / 32, total = norb * nchunk;
+    double s_br = 0.0, s_pa = 0.0;
+    for (int64_t w = (int64_t)blockIdx.x * QG_WARPS + (threadIdx.x >> 5); w < total;
+         w += (int64_t)gridDim.x * QG_WARPS) {
+        const int64_t r = w / nchunk, v = (w % nchunk) * 32 + lane;
+        // orbit positions: lane s < 24 computes position s, then all lanes take them by shuffle
+        int asc[4], base[4], pos[4];
+        decode_tri4(r, no, asc);
+        base[0] = asc[3];
+        base[1] = asc[2];
+        base[2] = asc[1];
+        base[3] = asc[0];
+        const int64_t my_off = s4_lane_offset(lane, base, no, pos);
+        const unsigned first = __ballot_sync(0xffffffffu, s4_first_holder(lane, my_off));
+        const int my_pos = pos[0] | (pos[1] << 8) | (pos[2] << 16) | (pos[3] << 24);
+        double my_eo = dadd(dadd(eo[pos[0]], eo[pos[1]]), dadd(eo[pos[2]], eo[pos[3]]));
+        const bool valid = v < V;
+        const int64_t vv = valid ? v : 0;
+        const int id = (int)(vv % g.dn), ic = (int)((vv / g.dn) % g.bc), ib = (int)((vv / ((int64_t)g.dn * g.bc)) % g.bb),
+                  ia = (int)(vv / ((int64_t)g.dn * g.bc * g.bb));
+        const int a = g.a0 + ia, b = g.b0 + ib, c = g.c0 + ic, d = g.d0 + id;
+        const double f = valid ? q_factor(a, b, c, d) : 0.0;
+        const double neg = -dadd(dadd(dadd(ev[a], ev[b]), ev[c]), ev[d]);
+        double x[24], t1[24];
+        int pss[24];
+#pragma unroll
+        for (int s = 0; s < 24; s++) {
+            const int ps = __shfl_sync(0xffffffffu, my_pos, s);
+            pss[s] = ps;
+            const double eos = __shfl_sync(0xffffffffu, my_eo, s);
+            const int64_t off = (((int64_t)(ps & 255) * no + ((ps >> 8) & 255)) * no + ((ps >> 16) & 255)) * no +
+                                (ps >> 24);
+            double xv = 0.0;
+            if (f != 0.0) {
+                xv = dadd(q_load(t4 + off * V + vv), q_load(z4 + off * V + vv));
+                const double den = dadd(eos, neg);
+                xv = (fabs(den) > 1e-15) ? __ddiv_rn(xv, den) : 0.0;
+            }
+            x[s] = xv;
+        }
+        // x -> T1 (t1) -> T2 (into x) -> R (into t1): two arrays of 24 live at a time
+        p4_t1_all(x, t1, k, std::make_integer_sequence<int, 24>{});
+        p4_t2_all(t1, x, k, std::make_integer_sequence<int, 24>{});
+        p4_r0_all(x, t1, k, std::make_integer_sequence<int, 24>{});
+        if (f != 0.0) {
+#pragma unroll
+            for (int s = 0; s < 24; s++) {
+                if (!((first >> s) & 1u)) continue;  // a repeated position counts once
+                const int ps = pss[s];
+                const int i = ps & 255, j = (ps >> 8) & 255, kk = (ps >> 16) & 255, l = ps >> 24;
+                const int64_t off = (((int64_t)i * no + j) * no + kk) * no + l;
+                const double y = dmul(t1[s], f);
+#define VT(p, m, n, q_) ((((int64_t)(p) * no + (m)) * no + (n)) * nv + (q_))
+                const double zsq = vvooT[VT(a, i, j, b)] * t2T[VT(c, kk, l, d)] + vvooT[VT(a, i, kk, c)] * t2T[VT(b, j, l, d)] +
+                                   vvooT[VT(a, i, l, d)] * t2T[VT(b, j, kk, c)] + vvooT[VT(b, j, kk, c)] * t2T[VT(a, i, l, d)] +
+                                   vvooT[VT(b, j, l, d)] * t2T[VT(a, i, kk, c)] + vvooT[VT(c, kk, l, d)] * t2T[VT(a, i, j, b)];
+#undef VT
+                s_br += y * zsq;
+                s_pa += y * q_load(z4 + off * V + vv);
+            }
+        }
+    }
+    __shared__ double red[2][QG_WARPS];
+    for (int o = 16; o > 0; o >>= 1) {
+        s_br += __shfl_down_sync(0xffffffffu, s_br, o);
+        s_pa += __shfl_down_sync(0xffffffffu, s_pa, o);
+    }
+    if (lane == 0) {
+        red[0][threadIdx.x >> 5] = s_br;
+        red[1][threadIdx.x >> 5] = s_pa;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double x = 0.0, y = 0.0;
+        for (int t = 0; t < QG_WARPS; t++) {
+            x += red[0][t];
+            y += red[1][t];
+        }
+        ws[2 * blockIdx.x] = x;
+        ws[2 * blockIdx.x + 1] = y;
+    }
+}
+
+static unsigned q_group_grid(int64_t items) {
+    int64_t g = (items + QG_WARPS - 1) / QG_WARPS;
+    return (unsigned)(g < 148 * 8 ? (g ? g : 1) : 148 * 8);
+}
+
 static unsigned q_epilogue_grid(int64_t nwarps) {
     int64_t g = (nwarps + QE_WARPS - 1) / QE_WARPS;
     return (unsigned)(g < 148 * 16 ? (g ? g : 1) : 148 * 16);
@@ -228,4 +408,44 @@ extern "C" int dcc_q_task_epilogue(const double *t4, const double *z4, const dou
     if (rc) return rc;
     k_q_finish<<<1, 256, 0, st>>>((const double *)workspace, grid, out);
     return launch_status("q_task_epilogue finish");
+}
+
+extern "C" size_t dcc_q_group_epilogue_workspace_bytes(void) { return (size_t)148 * 8 * 2 * sizeof(double); }
+
+extern "C" int dcc_q_group_epilogue(const void *t4, const void *z4, int f32, const double *vvooT,
+                                    const double *t2T, const double *e_occ, const double *e_vir, int64_t a0,
+                                    int64_t a1, int64_t b0, int64_t b1, int64_t c0, int64_t c1, int64_t d0,
+                                    int64_t d1, int64_t nocc, int64_t nvir, double *out, void *workspace,
+                                    size_t workspace_bytes, void *stream) {
+    clear_error();
+    DCC_REQUIRE(0 <= a0 && a0 <= a1 && a1 <= nvir && 0 <= b0 && b0 <= b1 && b1 <= nvir && 0 <= c0 && c0 <= c1 &&
+                    c1 <= nvir && 0 <= d0 && d0 <= d1 && d1 <= nvir,
+                DCC_ERR_SHAPE, "virtual range out of bounds");
+    DCC_REQUIRE(nocc >= 1 && nocc <= 255, DCC_ERR_SHAPE, "nocc must be in [1, 255]");
+    DCC_REQUIRE(f32 == 0 || f32 == 1, DCC_ERR_SHAPE, "f32 must be 0 or 1");
+    DCC_REQUIRE(t4 && z4 && vvooT && t2T && e_occ && e_vir && out && workspace, DCC_ERR_NULL, "NULL buffer");
+    DCC_REQUIRE(workspace_bytes >= dcc_q_group_epilogue_workspace_bytes(), DCC_ERR_WORKSPACE,
+                "workspace needs %zu bytes, got %zu", dcc_q_group_epilogue_workspace_bytes(), workspace_bytes);
+    const int64_t V = (a1 - a0) * (b1 - b0) * (c1 - c0) * (d1 - d0);
+    if (V == 0) return DCC_OK;
+    DCC_REQUIRE(V * nocc * nocc * nocc * nocc < (1ll << 40), DCC_ERR_SHAPE, "group block too large");
+    P4Coef k;
+    int rc = p4_coef("P4_444", 1.0, 0.0, k);  // beta = 0: the kernel drops the beta term
+    if (rc) return rc;
+    const int64_t norb = binom(nocc + 3, 4);
+    const unsigned grid = q_group_grid(norb * ((V + 31) / 32));
+    QGroup g{(int)a0, (int)b0, (int)c0, (int)d0, (int)(a1 - a0), (int)(b1 - b0), (int)(c1 - c0), (int)(d1 - d0)};
+    cudaStream_t st = as_stream(stream);
+    if (f32)
+        k_q_group_epilogue<float><<<grid, QG_THREADS, 0, st>>>((const float *)t4, (const float *)z4, vvooT, t2T, e_occ,
+                                                               e_vir, g, (int)nocc, (int)nvir, norb, k,
+                                                               (double *)workspace);
+    else
+        k_q_group_epilogue<double><<<grid, QG_THREADS, 0, st>>>((const double *)t4, (const double *)z4, vvooT, t2T,
+                                                                e_occ, e_vir, g, (int)nocc, (int)nvir, norb, k,
+                                                                (double *)workspace);
+    rc = launch_status("q_group_epilogue");
+    if (rc) return rc;
+    k_q_finish<<<1, 256, 0, st>>>((const double *)workspace, grid, out);
+    return launch_status("q_group_epilogue finish");
 }

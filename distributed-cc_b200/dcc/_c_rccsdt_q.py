@@ -71,3 +71,34 @@ def q_task_epilogue(t4, z4, eris_vvoo, t2_vvoo, e_occ, e_vir, task, blksize, noc
 
 def q_epilogue_workspace_bytes(blksize, nocc):
     return int(L.lib().dcc_q_epilogue_workspace_bytes(blksize, nocc))
+
+
+def q_group_epilogue(t4, z4, vvooT, t2T, e_occ, e_vir, ranges, nocc, nvir, out, workspace=None):
+    """Accumulate a task group's [Q] and (Q) contributions into out = [bracket, paren]
+    (device float64[2]).  t4 / z4: the group's T2- and T3-connected blocks stored
+    [i][j][k][l][a][b][c][d] (float64 or float32, same dtype) for the virtual ranges
+    (a0, a1, b0, b1, c0, c1, d0, d1); vvooT / t2T: eris_vvoo / t2 as [x][p][q][y]
+    (= [x][y][p][q] with the second virtual fastest)."""
+    if t4.dtype != z4.dtype or t4.dtype not in (torch.float32, f64):
+        raise TypeError("t4 and z4 must both be float64 or both float32")
+    for t, n in ((t4, "t4"), (z4, "z4")):
+        L.as_tensor(t, t4.dtype, n)
+    for t, n in ((vvooT, "vvooT"), (t2T, "t2T"), (e_occ, "e_occ"), (e_vir, "e_vir"), (out, "out")):
+        L.as_tensor(t, f64, n)
+    a0, a1, b0, b1, c0, c1, d0, d1 = ranges
+    V = (a1 - a0) * (b1 - b0) * (c1 - c0) * (d1 - d0)
+    if t4.numel() < V * nocc ** 4 or z4.numel() < V * nocc ** 4:
+        raise ValueError("t4 / z4 hold fewer than the group's elements")
+    if vvooT.numel() != nvir * nvir * nocc * nocc or t2T.numel() != vvooT.numel():
+        raise ValueError("vvooT / t2T must be nvir^2 nocc^2")
+    need = int(L.lib().dcc_q_group_epilogue_workspace_bytes())
+    if workspace is None:
+        workspace = torch.empty((need + 7) // 8, dtype=f64, device=t4.device)
+    L.call("dcc_q_group_epilogue", L.ptr(t4), L.ptr(z4), int(t4.dtype == torch.float32), L.ptr(vvooT), L.ptr(t2T),
+           L.ptr(e_occ), L.ptr(e_vir), a0, a1, b0, b1, c0, c1, d0, d1, nocc, nvir, L.ptr(out), L.ptr(workspace),
+           workspace.numel() * 8, L.stream_ptr())
+    return out
+
+
+def q_group_epilogue_workspace_bytes():
+    return int(L.lib().dcc_q_group_epilogue_workspace_bytes())

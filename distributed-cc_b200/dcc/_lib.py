@@ -72,10 +72,13 @@ _SIGS = {
     "dcc_e_abcdijkl_division": [c_vp, c_vp, c_vp] + [c_i64] * 13 + [c_vp],
     "dcc_t4_multiply_factor": [c_vp, c_vp] + [c_i64] * 5 + [c_vp],
     "dcc_q_task_epilogue": [c_vp] * 6 + [c_i64] * 11 + [c_vp, c_vp, c_size, c_vp],
+    "dcc_q_group_epilogue": [c_vp, c_vp, c_int] + [c_vp] * 4 + [c_i64] * 10 + [c_vp, c_vp, c_size, c_vp],
+    "dcc_q_group_epilogue_workspace_bytes": [],
     "dcc_t3_update_workspace_bytes": [c_i64, c_i64],
     "dcc_q_epilogue_workspace_bytes": [c_i64, c_i64],
 }
-_SIZE_FUNCS = {"dcc_t3_update_workspace_bytes", "dcc_q_epilogue_workspace_bytes"}
+_SIZE_FUNCS = {"dcc_t3_update_workspace_bytes", "dcc_q_epilogue_workspace_bytes",
+               "dcc_q_group_epilogue_workspace_bytes"}
 
 
 def _bind(name, args):

@@ -207,6 +207,24 @@ def _digit_orders(idx, size, strides, max_digits=4):
     return None
 
 
+def _digit_orders_each(idx, size, strides, max_digits=4, prefer=None):
+    """An order of idx in which every stride table, grouped on its own, has at most
+    max_digits digits: one grouping per table (each addresses the same enumeration of
+    idx).  prefer: a stride table whose descending order is tried first (so that
+    consecutive indices are as close as possible in that tensor).  None if no order
+    does."""
+    import itertools
+    first = sorted(idx, key=lambda c: -prefer[c]) if prefer is not None else list(idx)
+    cand = [first] + [list(p) for p in itertools.permutations(idx)] if len(idx) <= 6 else [first]
+    if prefer is not None:  # then orders whose fastest index is the closest one in `prefer`
+        cand = [first] + sorted(cand[1:], key=lambda o: prefer[o[-1]])
+    for order in cand:
+        gs = [_group_digits(order, size, [tab]) for tab in strides]
+        if all(len(g) <= max_digits for g in gs):
+            return gs
+    return None
+
+
 def _map_of(groups, t):
     """Address map of a digit grouping for stride table t."""
     if not groups:
@@ -308,6 +326,75 @@ def einsum_into(subs, X, Y, out, alpha=1.0, beta=1.0, kind=0, status=None, max_k
     st = status if status is not None else gemm_status(X.device)
     gemm_(a, b, out, _map_of(gM, 1), _map_of(gN, 1), alpha, beta, st)
     return out
+
+
+# ----------------------------------------------------------------------------
+# Grouped splits and GEMMs: many einsums in one launch each
+# ----------------------------------------------------------------------------
+
+_split_grouped_table = L.bind("dcc_split_grouped_table", [L.c_vp, L.c_int, L.c_vp, L.c_size, L.c_vp])
+_split_grouped = L.bind("dcc_split_grouped", [L.c_vp, L.c_int, L.c_i64, L.c_vp, L.c_int, L.c_vp])
+_gemm_grouped_table = L.bind("dcc_gemm_grouped_table", [L.c_vp, L.c_vp, L.c_int, L.c_int, L.c_vp, L.c_size,
+                                                         L.c_vp])
+_gemm_grouped = L.bind("dcc_gemm_grouped", [L.c_vp, L.c_int, L.c_i64, L.c_int, L.c_int, L.c_vp, L.c_vp])
+L.bind("dcc_split_grouped_table_bytes", [L.c_int], L.c_size)
+L.bind("dcc_gemm_grouped_table_bytes", [L.c_int], L.c_size)
+SPLIT_SPEC, GEMM_SPEC = 22, 25
+
+
+class GroupedSplit:
+    """Operand splits of many einsums in one launch (dcc_split_grouped).
+
+    spec: int64 [n, 22] rows (hi, lo, M, K, kw, ld, k0, row map(7), k map(7),
+    source is float32); run(srcs) fills every operand from its source address."""
+
+    def __init__(self, spec, kind, device):
+        spec = np.ascontiguousarray(spec, dtype=np.int64)
+        if spec.ndim != 2 or spec.shape[1] != SPLIT_SPEC:
+            raise ValueError("spec must be int64 [n, %d]" % SPLIT_SPEC)
+        self.n, self.kind = spec.shape[0], int(kind)
+        nbytes = int(L.lib().dcc_split_grouped_table_bytes(self.n))
+        self.table = torch.empty(nbytes, dtype=torch.uint8, device=device)
+        total = ctypes.c_int64(0)
+        L.check(_split_grouped_table(spec.ctypes.data_as(L.c_vp), self.n, L.ptr(self.table), nbytes,
+                                     ctypes.byref(total)))
+        self.total = total.value
+        self._srcs = (L.c_vp * self.n)()
+
+    def run(self, srcs):
+        """srcs: n device addresses (ints), operand p read from srcs[p]."""
+        if len(srcs) != self.n:
+            raise ValueError("need %d sources" % self.n)
+        for i, p in enumerate(srcs):
+            self._srcs[i] = int(p)
+        L.check(_split_grouped(L.ptr(self.table), self.n, self.total, self._srcs, self.kind, L.stream_ptr()))
+
+
+class GroupedGemm:
+    """Split-precision GEMMs of many einsums in one persistent launch
+    (dcc_gemm_grouped): C_p[row(m) + col(n)] += alpha_p (A_p B_p^T)[m][n], added by
+    reductions in L2 so several problems may share an output.
+
+    spec: int64 [n, 25] rows (A_hi, A_lo, lda, B_hi, B_lo, ldb, M, N, Kp, C,
+    C is float32, row map(7), col map(7)); alpha: float64 [n]."""
+
+    def __init__(self, spec, alpha, kind, device):
+        spec = np.ascontiguousarray(spec, dtype=np.int64)
+        alpha = np.ascontiguousarray(alpha, dtype=np.float64)
+        if spec.ndim != 2 or spec.shape[1] != GEMM_SPEC or alpha.shape != (spec.shape[0],):
+            raise ValueError("spec must be int64 [n, %d] with n alphas" % GEMM_SPEC)
+        self.n, self.kind = spec.shape[0], int(kind)
+        self.out_f32 = int(spec[0, 10])
+        nbytes = int(L.lib().dcc_gemm_grouped_table_bytes(self.n))
+        self.table = torch.empty(nbytes, dtype=torch.uint8, device=device)
+        total = ctypes.c_int64(0)
+        L.check(_gemm_grouped_table(spec.ctypes.data_as(L.c_vp), alpha.ctypes.data_as(L.c_vp), self.n, self.kind,
+                                    L.ptr(self.table), nbytes, ctypes.byref(total)))
+        self.total = total.value
+
+    def run(self, status):
+        L.check(_gemm_grouped(L.ptr(self.table), self.n, self.total, self.kind, self.out_f32, L.ptr(status),
+                              L.stream_ptr()))
 
 
 # ----------------------------------------------------------------------------

@@ -8,6 +8,7 @@
     python -m dcc.profile_cases xgemm  [--reps 3]
     python -m dcc.profile_cases oogemm [--reps 3]
     python -m dcc.profile_cases unpack [--reps 3]
+    python -m dcc.profile_cases qgroup [--reps 3]
 
 Each case builds its inputs once and launches the kernel `reps` times, so a
 profiler can skip the warm-up launches and capture the last one.  Sizes are
@@ -118,9 +119,29 @@ def case_unpack(reps, nocc=10):
     torch.cuda.synchronize()
 
 
+def case_qgroup(reps, nocc=10):
+    """One (Q) task group (a, b, c blocks 0..3, d over all 90 virtuals) on the split path:
+    two grouped splits, two grouped GEMMs and the group epilogue per repetition."""
+    from dcc import synthetic, rccsdt_q, _c_rccsdt
+    nv = 90
+    d = synthetic.make_inputs(nocc, nv, seed=0)
+    er = {"vvvo": d.W_vvvo, "vooo": d.W_vooo, "vvoo": d.eris_vvoo, "ovvo": d.W_ovvo, "ovov": d.W_ovov,
+          "vvvv": d.W_vvvv, "oooo": d.W_oooo}
+    t2 = d.t2.permute(2, 3, 0, 1).contiguous()
+    t3_abc = _c_rccsdt.redistribute_ijk_to_abc(d.t3, nocc, nv)
+    del d.t3
+    q = rccsdt_q.QEnergy(nocc, nv, 4, "bf16x3")
+    g = rccsdt_q.groups(nv, 4)[:1]
+    q.prepare(g)
+    for _ in range(reps):
+        q.run(er, t2, t3_abc, d.e_occ, d.e_vir, g)
+    torch.cuda.synchronize()
+    assert q.status_ok()
+
+
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("case", choices=["gemm", "p3", "update", "q", "gather", "xgemm", "oogemm", "unpack"])
+    ap.add_argument("case", choices=["gemm", "p3", "update", "q", "gather", "xgemm", "oogemm", "unpack", "qgroup"])
     ap.add_argument("--kind", default="bf16x3")
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--nocc", type=int, default=None, help="occupied orbitals (xgemm, oogemm, gather, unpack)")
@@ -131,8 +152,9 @@ def main():
         case_p3(a.reps)
     elif a.case == "update":
         case_update(a.reps)
-    elif a.case in ("gather", "xgemm", "oogemm", "unpack"):
-        fn = {"gather": case_gather, "xgemm": case_xgemm, "oogemm": case_oogemm, "unpack": case_unpack}[a.case]
+    elif a.case in ("gather", "xgemm", "oogemm", "unpack", "qgroup"):
+        fn = {"gather": case_gather, "xgemm": case_xgemm, "oogemm": case_oogemm, "unpack": case_unpack,
+              "qgroup": case_qgroup}[a.case]
         fn(a.reps, **({} if a.nocc is None else {"nocc": a.nocc}))
     else:
         case_q(a.reps)

@@ -9,25 +9,37 @@ disconnected z4_sq, :1131-1154).
 
 Here the tasks that share (a-block, b-block, c-block) are one group: every
 contraction runs once for the whole d range [c0, nvir) of the group, so each
-einsum is a GEMM over all of the group's d-blocks instead of one per task,
-and the T3 slabs are unpacked on the device from the ABC-ordered T3
-(dcc_fill_t3_from_abc).  Each task's epilogue is the fused
-dcc_q_task_epilogue kernel.  The energies are the sums over the same task
-set as the reference; only the summation order of the contractions differs.
+einsum covers all of the group's d-blocks, and the T3 slabs are unpacked on
+the device from the ABC-ordered T3 (dcc_fill_t3_from_abc).  The group's z4 and
+t4 are stored [i][j][k][l][a][b][c][d] (virtual quadruple fastest), which is
+what the group epilogue (dcc_q_group_epilogue) reads with coalesced rows.  The
+energies are the sums over the same task set as the reference; only the
+summation order differs.
 
-precision = "fp64": every contraction in FP64 (cuBLAS through torch).
-"bf16x3" / "tf32x3": every contraction is one split-precision tcgen05 GEMM
-that reads its operands in place and accumulates into the group tensor
-through its epilogue maps (contract.einsum_into); denominators,
+The 132 einsums of a group are data (`group_terms`): (subscripts, operand,
+operand, output, alpha) with each operand a named tensor cut by range starts.
+
+precision = "fp64": every einsum in FP64 through torch (cuBLAS), accumulated
+into FP64 group blocks.
+"bf16x3" / "tf32x3": the einsums of a group run as two grouped split-precision
+tcgen05 GEMMs (builds of the W intermediates and z4 first, then t4), each
+preceded by one grouped split of its operands; results are added into FP32
+group blocks by reductions in L2.  Splits and GEMM tables are planned once
+per group shape; a group only supplies new operand addresses.  Denominators,
 symmetrization, factors and energies stay FP64.
 """
 from __future__ import annotations
 
+import ctypes
+
+import numpy as np
 import torch
 
 from . import _c_rccsdt, _c_rccsdt_q, contract
+from . import _lib as L
 
 f64 = torch.float64
+f32 = torch.float32
 
 
 def prange(start, stop, step):
@@ -56,6 +68,235 @@ def groups(nvir, blksize):
     return out
 
 
+# ----------------------------------------------------------------------------
+# The einsums of one group as data.  Range letters: A = [a0, a0+ba),
+# B = [b0, b0+bb), C = [c0, c0+bc), D = [d0, d0+dn) (d0 = c0, dn = nvir - c0);
+# "F" is the full range of the dimension.  Operands are named tensors:
+#   integrals vvvo [nv,nv,nv,no], vooo [nv,no,no,no], vvvv [nv]^4,
+#   ovvo [no,nv,nv,no], ovov [no,nv,no,nv], oooo [no]^4, t2 [nv,nv,no,no];
+#   slabs S<xy> = T[X, Y, :, :, :, :] of the ABC-ordered T3 (x, y in a, b, c, d);
+#   intermediates W<xyw> = W_vvvvoo[X, Y, W] (distr_cc/rccsdt_q.py:390-399) and
+#   V<xy> = W_vvoooo[X, Y] (:401-408); outputs z (T3-connected), x (T2-connected).
+# ----------------------------------------------------------------------------
+
+_Z_TERMS = [
+    # (subscripts, (tensor, ranges), (tensor, ranges), alpha)        distr_cc/rccsdt_q.py:1014-1071
+    ('cdel,abeijk->abcdijkl', ("vvvo", "CDFF"), ("Sab", "FFFFFF"), 1.0),
+    ('dcek,abeijl->abcdijkl', ("vvvo", "DCFF"), ("Sab", "FFFFFF"), 1.0),
+    ('dmli,abcmjk->abcdijkl', ("vooo", "DFFF"), ("Sab", "FFCFFF"), -1.0),
+    ('dmlj,abcimk->abcdijkl', ("vooo", "DFFF"), ("Sab", "FFCFFF"), -1.0),
+    ('cmki,abdmjl->abcdijkl', ("vooo", "CFFF"), ("Sab", "FFDFFF"), -1.0),
+    ('cmkj,abdiml->abcdijkl', ("vooo", "CFFF"), ("Sab", "FFDFFF"), -1.0),
+    ('bdel,aceikj->abcdijkl', ("vvvo", "BDFF"), ("Sac", "FFFFFF"), 1.0),
+    ('dbej,aceikl->abcdijkl', ("vvvo", "DBFF"), ("Sac", "FFFFFF"), 1.0),
+    ('bmji,acdmkl->abcdijkl', ("vooo", "BFFF"), ("Sac", "FFDFFF"), -1.0),
+    ('bmjk,acdiml->abcdijkl', ("vooo", "BFFF"), ("Sac", "FFDFFF"), -1.0),
+    ('dmlk,acbimj->abcdijkl', ("vooo", "DFFF"), ("Sac", "FFBFFF"), -1.0),
+    ('bcek,adeilj->abcdijkl', ("vvvo", "BCFF"), ("Sad", "FFFFFF"), 1.0),
+    ('cbej,adeilk->abcdijkl', ("vvvo", "CBFF"), ("Sad", "FFFFFF"), 1.0),
+    ('bmjl,adcimk->abcdijkl', ("vooo", "BFFF"), ("Sad", "FFCFFF"), -1.0),
+    ('cmkl,adbimj->abcdijkl', ("vooo", "CFFF"), ("Sad", "FFBFFF"), -1.0),
+    ('adel,bcejki->abcdijkl', ("vvvo", "ADFF"), ("Sbc", "FFFFFF"), 1.0),
+    ('daei,bcejkl->abcdijkl', ("vvvo", "DAFF"), ("Sbc", "FFFFFF"), 1.0),
+    ('amij,bcdmkl->abcdijkl', ("vooo", "AFFF"), ("Sbc", "FFDFFF"), -1.0),
+    ('amik,bcdjml->abcdijkl', ("vooo", "AFFF"), ("Sbc", "FFDFFF"), -1.0),
+    ('acek,bdejli->abcdijkl', ("vvvo", "ACFF"), ("Sbd", "FFFFFF"), 1.0),
+    ('caei,bdejlk->abcdijkl', ("vvvo", "CAFF"), ("Sbd", "FFFFFF"), 1.0),
+    ('amil,bdcjmk->abcdijkl', ("vooo", "AFFF"), ("Sbd", "FFCFFF"), -1.0),
+    ('abej,cdekli->abcdijkl', ("vvvo", "ABFF"), ("Scd", "FFFFFF"), 1.0),
+    ('baei,cdeklj->abcdijkl', ("vvvo", "BAFF"), ("Scd", "FFFFFF"), 1.0),
+]
+
+# W_vvvvoo[X, Y, W] = the six strings of distr_cc/rccsdt_q.py:390-399
+_W_BUILD = [
+    ('abef,fcjk->abcejk', ("vvvv", "XYFF"), ("t2", "FWFF"), 0.5),
+    ('acef,fbkj->abcejk', ("vvvv", "XWFF"), ("t2", "FYFF"), 0.5),
+    ('mbej,acmk->abcejk', ("ovvo", "FYFF"), ("t2", "XWFF"), -1.0),
+    ('mcek,abmj->abcejk', ("ovvo", "FWFF"), ("t2", "XYFF"), -1.0),
+    ('maje,bcmk->abcejk', ("ovov", "FXFF"), ("t2", "YWFF"), -1.0),
+    ('make,cbmj->abcejk', ("ovov", "FXFF"), ("t2", "WYFF"), -1.0),
+]
+# W_vvoooo[X, Y] (distr_cc/rccsdt_q.py:401-408)
+_V_BUILD = [
+    ('mnki,abnj->abmijk', ("oooo", "FFFF"), ("t2", "XYFF"), -0.5),
+    ('mnkj,bani->abmijk', ("oooo", "FFFF"), ("t2", "YXFF"), -0.5),
+]
+_W_NAMES = ["abc", "abd", "acd", "bac", "bad", "bcd", "cab", "cad", "cbd", "dab", "dac", "dbc"]
+_V_NAMES = ["ab", "ac", "ad", "bc", "bd", "cd"]
+_X_TERMS = [
+    # distr_cc/rccsdt_q.py:1073-1129
+    ('abcejk,edil->abcdijkl', "Wabc", ("t2", "FDFF"), 1.0),
+    ('abdejl,ecik->abcdijkl', "Wabd", ("t2", "FCFF"), 1.0),
+    ('acdekl,ebij->abcdijkl', "Wacd", ("t2", "FBFF"), 1.0),
+    ('baceik,edjl->abcdijkl', "Wbac", ("t2", "FDFF"), 1.0),
+    ('badeil,ecjk->abcdijkl', "Wbad", ("t2", "FCFF"), 1.0),
+    ('bcdekl,eaji->abcdijkl', "Wbcd", ("t2", "FAFF"), 1.0),
+    ('cabeij,edkl->abcdijkl', "Wcab", ("t2", "FDFF"), 1.0),
+    ('cadeil,ebkj->abcdijkl', "Wcad", ("t2", "FBFF"), 1.0),
+    ('cbdejl,eaki->abcdijkl', "Wcbd", ("t2", "FAFF"), 1.0),
+    ('dabeij,eclk->abcdijkl', "Wdab", ("t2", "FCFF"), 1.0),
+    ('daceik,eblj->abcdijkl', "Wdac", ("t2", "FBFF"), 1.0),
+    ('dbcejk,eali->abcdijkl', "Wdbc", ("t2", "FAFF"), 1.0),
+    ('abmijk,cdml->abcdijkl', "Vab", ("t2", "CDFF"), -1.0),
+    ('abmijl,dcmk->abcdijkl', "Vab", ("t2", "DCFF"), -1.0),
+    ('acmikj,bdml->abcdijkl', "Vac", ("t2", "BDFF"), -1.0),
+    ('acmikl,dbmj->abcdijkl', "Vac", ("t2", "DBFF"), -1.0),
+    ('admilj,bcmk->abcdijkl', "Vad", ("t2", "BCFF"), -1.0),
+    ('admilk,cbmj->abcdijkl', "Vad", ("t2", "CBFF"), -1.0),
+    ('bcmjki,adml->abcdijkl', "Vbc", ("t2", "ADFF"), -1.0),
+    ('bcmjkl,dami->abcdijkl', "Vbc", ("t2", "DAFF"), -1.0),
+    ('bdmjli,acmk->abcdijkl', "Vbd", ("t2", "ACFF"), -1.0),
+    ('bdmjlk,cami->abcdijkl', "Vbd", ("t2", "CAFF"), -1.0),
+    ('cdmkli,abmj->abcdijkl', "Vcd", ("t2", "ABFF"), -1.0),
+    ('cdmklj,bami->abcdijkl', "Vcd", ("t2", "BAFF"), -1.0),
+]
+_SLABS = ["Sab", "Sac", "Sad", "Sbc", "Sbd", "Scd"]
+
+
+def group_terms():
+    """(phase, subscripts, X, Y, output, alpha) of every einsum of a group; X, Y =
+    (tensor name, ranges) with one range letter per dimension (F: full; a tensor
+    that is an intermediate or output carries its own ranges).  Phase 0: the
+    intermediates and z4; phase 1: t4 (reads the intermediates)."""
+    out = []
+    for w in _W_NAMES:
+        sub = dict(X=w[0].upper(), Y=w[1].upper(), W=w[2].upper())
+        for s, (xn, xr), (yn, yr), al in _W_BUILD:
+            out.append((0, s, (xn, "".join(sub.get(c, c) for c in xr)), (yn, "".join(sub.get(c, c) for c in yr)),
+                        "W" + w, al))
+    for v in _V_NAMES:
+        sub = dict(X=v[0].upper(), Y=v[1].upper())
+        for s, (xn, xr), (yn, yr), al in _V_BUILD:
+            out.append((0, s, (xn, xr), (yn, "".join(sub.get(c, c) for c in yr)), "V" + v, al))
+    for s, X, Y, al in _Z_TERMS:
+        out.append((0, s, X, Y, "z", al))
+    for s, wn, Y, al in _X_TERMS:
+        out.append((1, s, (wn, None), Y, "x", al))
+    return out
+
+
+class _Shapes:
+    """Lengths, strides and range starts of every named tensor of a group shape."""
+
+    def __init__(self, no, nv, ba, bb, bc, dn):
+        self.no, self.nv = no, nv
+        self.len = {"A": ba, "B": bb, "C": bc, "D": dn}
+        L_ = self.len
+        self.shape = {"vvvo": (nv, nv, nv, no), "vooo": (nv, no, no, no), "vvvv": (nv,) * 4,
+                      "ovvo": (no, nv, nv, no), "ovov": (no, nv, no, nv), "oooo": (no,) * 4, "t2": (nv, nv, no, no)}
+        for s in _SLABS:
+            self.shape[s] = (L_[s[1].upper()], L_[s[2].upper()], nv, no, no, no)
+        for w in _W_NAMES:
+            self.shape["W" + w] = (L_[w[0].upper()], L_[w[1].upper()], L_[w[2].upper()], nv, no, no)
+        for v in _V_NAMES:
+            self.shape["V" + v] = (L_[v[0].upper()], L_[v[1].upper()], no, no, no, no)
+
+    def strides(self, name):
+        if name in ("z", "x"):
+            L_, no = self.len, self.no
+            Vv = L_["A"] * L_["B"] * L_["C"] * L_["D"]
+            # [i][j][k][l][a][b][c][d]; logical order a b c d i j k l
+            return (L_["B"] * L_["C"] * L_["D"], L_["C"] * L_["D"], L_["D"], 1, no ** 3 * Vv, no * no * Vv, no * Vv, Vv)
+        sh = self.shape[name]
+        st, acc = [], 1
+        for n in reversed(sh):
+            st.append(acc)
+            acc *= n
+        return tuple(reversed(st))
+
+    def lengths(self, name, ranges):
+        if name in ("z", "x"):
+            L_ = self.len
+            return (L_["A"], L_["B"], L_["C"], L_["D"]) + (self.no,) * 4
+        sh = self.shape[name]
+        if ranges is None:
+            return sh
+        return tuple(sh[i] if r == "F" else self.len[r] for i, r in enumerate(ranges))
+
+
+def _starts(ranges, origin):
+    """Start index per dimension: origin[letter] for a range letter, 0 for F."""
+    if ranges is None:
+        return None
+    return tuple(0 if r == "F" else origin[r] for r in ranges)
+
+
+_ORIGIN_KEYS = ("A", "B", "C", "D")
+
+
+def plan_problems(no, nv, sig, terms=None):
+    """The einsums of a group shape sig = (ba, bb, bc, dn) as GEMM problems on split
+    operands.  Each problem: phase, out (z, x or an intermediate), alpha, m, n, k,
+    A / B = {src: tensor name, fm: row map, fk: contraction map, coef: element
+    offset of the operand's first element per unit of (a0, b0, c0, d0), off: a
+    constant element offset}, the output maps orow / ocol (four-digit maps,
+    contract.four order) and the output's constant offset ooff.  Rows come from
+    whichever operand wastes less of the 128 x 256 output tiles.  An einsum whose
+    free indices do not fold into four digits for both its operand and the output
+    runs as one problem per value of one of them (the shortest).
+    Also returns [(output name, elements)] of the FP32 outputs."""
+    sh = _Shapes(no, nv, *sig)
+    probs = []
+
+    def add(phase, subs, xn, xr, yn, yr, on, al, size, sx, sy, so, xoff, yoff, ooff):
+        ins, o = subs.split("->")
+        xs, ys = ins.split(",")
+        K = [c for c in xs if c in ys]
+        Mi = [c for c in xs if c not in ys and c in size]
+        Ni = [c for c in ys if c not in xs and c in size]
+        # enumerate rows and columns in the output's stride order: consecutive rows (or
+        # columns) of a tile are then neighbours in the output, so its reductions coalesce
+        gM = contract._digit_orders_each(Mi, size, [sx, so], prefer=so)
+        gN = contract._digit_orders_each(Ni, size, [sy, so], prefer=so)
+        gK = contract._digit_orders_each(K, size, [sx, sy])
+        if gK is None:
+            raise RuntimeError("einsum %s: contraction does not fold into four-digit maps" % subs)
+        if gM is None or gN is None:
+            free = Mi if gM is None else Ni
+            # the shortest index, but not the one contiguous in the output (kept for coalescing)
+            keep_fast = min(free, key=lambda q: so[q])
+            c = min([q for q in free if q != keep_fast] or free, key=lambda q: size[q])
+            sub = {q: v for q, v in size.items() if q != c}
+            for v in range(size[c]):
+                add(phase, subs, xn, xr, yn, yr, on, al, sub, sx, sy, so, xoff + v * sx.get(c, 0),
+                    yoff + v * sy.get(c, 0), ooff + v * so[c])
+            return
+        mx, ny = int(np.prod([size[q] for q in Mi])), int(np.prod([size[q] for q in Ni]))
+        waste_xy = -(-mx // 128) * 128 * (-(-ny // 256) * 256)
+        waste_yx = -(-ny // 128) * 128 * (-(-mx // 256) * 256)
+
+        def operand(name, rng, gR, gk, off):
+            coef = np.zeros(4, dtype=np.int64)
+            if rng is not None:
+                for r_, d_ in zip(rng, sh.strides(name)):
+                    if r_ != "F":
+                        coef[_ORIGIN_KEYS.index(r_)] += d_
+            return {"src": name, "fm": contract._map_of(gR, 0), "fk": contract._map_of(gk, 0), "coef": coef,
+                    "off": int(off)}
+
+        opX, opY = operand(xn, xr, gM[0], gK[0], xoff), operand(yn, yr, gN[0], gK[1], yoff)
+        pr = {"phase": phase, "subs": subs, "out": on, "alpha": al, "m": mx, "n": ny,
+              "k": int(np.prod([size[q] for q in K])), "A": opX, "B": opY,
+              "orow": contract._map_of(gM[1], 0), "ocol": contract._map_of(gN[1], 0), "ooff": int(ooff)}
+        if waste_yx < waste_xy:  # the other operand takes the rows
+            pr.update(m=ny, n=mx, A=opY, B=opX, orow=pr["ocol"], ocol=pr["orow"])
+        probs.append(pr)
+
+    for phase, subs, (xn, xr), (yn, yr), on, al in (terms if terms is not None else group_terms()):
+        ins, o = subs.split("->")
+        xs, ys = ins.split(",")
+        lx, ly = sh.lengths(xn, xr), sh.lengths(yn, yr)
+        size = {c: n for c, n in zip(xs, lx)}
+        size.update({c: n for c, n in zip(ys, ly)})
+        sx, sy = dict(zip(xs, sh.strides(xn))), dict(zip(ys, sh.strides(yn)))
+        so = dict(zip(o, sh.strides(on)))
+        add(phase, subs, xn, xr, yn, yr, on, al, size, sx, sy, so, 0, 0, 0)
+    nzx = int(np.prod(sh.lengths("z", None)))
+    outs = [("z", nzx), ("x", nzx)] + [(nm, int(np.prod(sh.shape[nm])))
+                                         for nm in ["W" + w for w in _W_NAMES] + ["V" + v for v in _V_NAMES]]
+    return probs, outs
+
+
 class QEnergy:
     """[Q] and (Q) energies for fixed (nocc, nvir, blksize) on one GPU.
 
@@ -66,139 +307,193 @@ class QEnergy:
     def __init__(self, nocc, nvir, blksize=4, precision="fp64", device="cuda"):
         self.no, self.nv, self.blk, self.precision = int(nocc), int(nvir), int(blksize), precision
         self.kind = None if precision == "fp64" else contract.KIND[precision]
-        self.dev = device
-        blk, no = self.blk, self.no
-        self.t4_task = torch.zeros((blk,) * 4 + (no,) * 4, dtype=f64, device=device)
-        self.z4_task = torch.zeros_like(self.t4_task)
-        self.ws = torch.empty((_c_rccsdt_q.q_epilogue_workspace_bytes(blk, no) + 7) // 8, dtype=f64, device=device)
-        self.out = torch.zeros(2, dtype=f64, device=device)
-        self.status = torch.zeros(1, dtype=torch.int32, device=device)
-
-    def E(self, subs, X, Y, out, alpha=1.0, beta=1.0):
-        """out = alpha * einsum(subs, X, Y) + beta * out: one split GEMM accumulating in place
-        (contract.einsum_into), or FP64 torch for precision="fp64"."""
-        return contract.einsum_into(subs, X, Y, out, alpha, beta, self.kind, self.status)
+        self.dev = torch.device(device)
+        self.ws = torch.empty((_c_rccsdt_q.q_group_epilogue_workspace_bytes() + 7) // 8, dtype=f64,
+                              device=self.dev)
+        self.out = torch.zeros(2, dtype=f64, device=self.dev)
+        self.status = torch.zeros(1, dtype=torch.int32, device=self.dev)
+        self.terms = group_terms()
+        self._plans = {}
+        self._arena = self._pool = None
+        self._vvooT = self._t2T = None
 
     def status_ok(self):
         return self.kind is None or int(self.status.item()) == 0
 
-    def slab(self, t3_abc, a0, a1, b0, b1):
-        """T[a0:a1, b0:b1, :, :, :, :] from the ABC-ordered T3."""
+    # ------------------------------------------------------------------ group data
+    def _slabs(self, t3_abc, r):
+        """The group's six T3 slabs (FP64, filled on the device)."""
         nv, no = self.nv, self.no
-        out = torch.empty((a1 - a0, b1 - b0, nv, no, no, no), dtype=f64, device=self.dev)
-        _c_rccsdt_q.fill_t3_from_abc(out, a0, a1, b0, b1, nv, no, t3_abc, b1 - b0)
+        rng = {"a": (r[0], r[1]), "b": (r[2], r[3]), "c": (r[4], r[5]), "d": (r[6], r[7])}
+        out = {}
+        for s in _SLABS:
+            (x0, x1), (y0, y1) = rng[s[1]], rng[s[2]]
+            t = torch.empty((x1 - x0, y1 - y0, nv, no, no, no), dtype=f64, device=self.dev)
+            _c_rccsdt_q.fill_t3_from_abc(t, x0, x1, y0, y1, nv, no, t3_abc, y1 - y0)
+            out[s] = t
         return out
 
-    def W_vvvvoo(self, er, t2, a0, a1, b0, b1, c0, c1):
-        """distr_cc/rccsdt_q.py:390-399 for the index ranges given."""
-        E, no, nv = self.E, self.no, self.nv
-        W = torch.empty((a1 - a0, b1 - b0, c1 - c0, nv, no, no), dtype=f64, device=self.dev)
-        E('abef,fcjk->abcejk', er["vvvv"][a0:a1, b0:b1], t2[:, c0:c1], W, 0.5, 0.0)
-        E('acef,fbkj->abcejk', er["vvvv"][a0:a1, c0:c1], t2[:, b0:b1], W, 0.5)
-        E('mbej,acmk->abcejk', er["ovvo"][:, b0:b1], t2[a0:a1, c0:c1], W, -1.0)
-        E('mcek,abmj->abcejk', er["ovvo"][:, c0:c1], t2[a0:a1, b0:b1], W, -1.0)
-        E('maje,bcmk->abcejk', er["ovov"][:, a0:a1], t2[b0:b1, c0:c1], W, -1.0)
-        E('make,cbmj->abcejk', er["ovov"][:, a0:a1], t2[c0:c1, b0:b1], W, -1.0)
-        return W
+    def _transposed(self, er, t2):
+        if self._vvooT is None:
+            self._vvooT = er["vvoo"].permute(0, 2, 3, 1).contiguous()
+            self._t2T = t2.permute(0, 2, 3, 1).contiguous()
+        return self._vvooT, self._t2T
 
-    def W_vvoooo(self, er, t2, a0, a1, b0, b1):
-        """distr_cc/rccsdt_q.py:401-408."""
-        no = self.no
-        W = torch.empty((a1 - a0, b1 - b0) + (no,) * 4, dtype=f64, device=self.dev)
-        self.E('mnki,abnj->abmijk', er["oooo"], t2[a0:a1, b0:b1], W, -0.5, 0.0)
-        self.E('mnkj,bani->abmijk', er["oooo"], t2[b0:b1, a0:a1], W, -0.5)
-        return W
+    # ------------------------------------------------------------------ FP64 path
+    def _run_fp64(self, er, t2, slabs, r):
+        no, nv = self.no, self.nv
+        a0, a1, b0, b1, c0, c1, d0, d1 = r
+        sh = _Shapes(no, nv, a1 - a0, b1 - b0, c1 - c0, d1 - d0)
+        origin = {"A": a0, "B": b0, "C": c0, "D": d0}
+        bufs = dict(er)
+        bufs["t2"] = t2
+        bufs.update(slabs)
+        V = sh.len["A"] * sh.len["B"] * sh.len["C"] * sh.len["D"]
+        z = torch.zeros((no,) * 4 + (sh.len["A"], sh.len["B"], sh.len["C"], sh.len["D"]), dtype=f64, device=self.dev)
+        x = torch.zeros_like(z)
+        outs = {"z": z, "x": x}
 
-    def group(self, er, t2, t3_abc, a0, a1, b0, b1, c0, c1):
-        """z4 and t4 [a, b, c, d, i, j, k, l] of a group, d over [c0, nvir)."""
-        E, nv, no = self.E, self.nv, self.no
-        A, B, C, D = slice(a0, a1), slice(b0, b1), slice(c0, c1), slice(c0, nv)
-        vvvo, vooo = er["vvvo"], er["vooo"]
-        shape = (a1 - a0, b1 - b0, c1 - c0, nv - c0) + (no,) * 4
-        z = torch.empty(shape, dtype=f64, device=self.dev)
-        x = torch.empty(shape, dtype=f64, device=self.dev)
-        # T3-connected (distr_cc/rccsdt_q.py:1014-1071)
-        t = self.slab(t3_abc, a0, a1, b0, b1)
-        E('cdel,abeijk->abcdijkl', vvvo[C, D], t, z, 1.0, 0.0)
-        E('dcek,abeijl->abcdijkl', vvvo[D, C], t, z)
-        E('dmli,abcmjk->abcdijkl', vooo[D], t[:, :, C], z, -1.0)
-        E('dmlj,abcimk->abcdijkl', vooo[D], t[:, :, C], z, -1.0)
-        E('cmki,abdmjl->abcdijkl', vooo[C], t[:, :, D], z, -1.0)
-        E('cmkj,abdiml->abcdijkl', vooo[C], t[:, :, D], z, -1.0)
-        t = self.slab(t3_abc, a0, a1, c0, c1)
-        E('bdel,aceikj->abcdijkl', vvvo[B, D], t, z)
-        E('dbej,aceikl->abcdijkl', vvvo[D, B], t, z)
-        E('bmji,acdmkl->abcdijkl', vooo[B], t[:, :, D], z, -1.0)
-        E('bmjk,acdiml->abcdijkl', vooo[B], t[:, :, D], z, -1.0)
-        E('dmlk,acbimj->abcdijkl', vooo[D], t[:, :, B], z, -1.0)
-        t = self.slab(t3_abc, a0, a1, c0, nv)
-        E('bcek,adeilj->abcdijkl', vvvo[B, C], t, z)
-        E('cbej,adeilk->abcdijkl', vvvo[C, B], t, z)
-        E('bmjl,adcimk->abcdijkl', vooo[B], t[:, :, C], z, -1.0)
-        E('cmkl,adbimj->abcdijkl', vooo[C], t[:, :, B], z, -1.0)
-        t = self.slab(t3_abc, b0, b1, c0, c1)
-        E('adel,bcejki->abcdijkl', vvvo[A, D], t, z)
-        E('daei,bcejkl->abcdijkl', vvvo[D, A], t, z)
-        E('amij,bcdmkl->abcdijkl', vooo[A], t[:, :, D], z, -1.0)
-        E('amik,bcdjml->abcdijkl', vooo[A], t[:, :, D], z, -1.0)
-        t = self.slab(t3_abc, b0, b1, c0, nv)
-        E('acek,bdejli->abcdijkl', vvvo[A, C], t, z)
-        E('caei,bdejlk->abcdijkl', vvvo[C, A], t, z)
-        E('amil,bdcjmk->abcdijkl', vooo[A], t[:, :, C], z, -1.0)
-        t = self.slab(t3_abc, c0, c1, c0, nv)
-        E('abej,cdekli->abcdijkl', vvvo[A, B], t, z)
-        E('baei,cdeklj->abcdijkl', vvvo[B, A], t, z)
-        del t
-        # T2-connected (distr_cc/rccsdt_q.py:1073-1129)
-        W = self.W_vvvvoo
-        d0, d1 = c0, nv
-        E('abcejk,edil->abcdijkl', W(er, t2, a0, a1, b0, b1, c0, c1), t2[:, D], x, 1.0, 0.0)
-        E('abdejl,ecik->abcdijkl', W(er, t2, a0, a1, b0, b1, d0, d1), t2[:, C], x)
-        E('acdekl,ebij->abcdijkl', W(er, t2, a0, a1, c0, c1, d0, d1), t2[:, B], x)
-        E('baceik,edjl->abcdijkl', W(er, t2, b0, b1, a0, a1, c0, c1), t2[:, D], x)
-        E('badeil,ecjk->abcdijkl', W(er, t2, b0, b1, a0, a1, d0, d1), t2[:, C], x)
-        E('bcdekl,eaji->abcdijkl', W(er, t2, b0, b1, c0, c1, d0, d1), t2[:, A], x)
-        E('cabeij,edkl->abcdijkl', W(er, t2, c0, c1, a0, a1, b0, b1), t2[:, D], x)
-        E('cadeil,ebkj->abcdijkl', W(er, t2, c0, c1, a0, a1, d0, d1), t2[:, B], x)
-        E('cbdejl,eaki->abcdijkl', W(er, t2, c0, c1, b0, b1, d0, d1), t2[:, A], x)
-        E('dabeij,eclk->abcdijkl', W(er, t2, d0, d1, a0, a1, b0, b1), t2[:, C], x)
-        E('daceik,eblj->abcdijkl', W(er, t2, d0, d1, a0, a1, c0, c1), t2[:, B], x)
-        E('dbcejk,eali->abcdijkl', W(er, t2, d0, d1, b0, b1, c0, c1), t2[:, A], x)
-        V = self.W_vvoooo
-        Wv = V(er, t2, a0, a1, b0, b1)
-        E('abmijk,cdml->abcdijkl', Wv, t2[C, D], x, -1.0)
-        E('abmijl,dcmk->abcdijkl', Wv, t2[D, C], x, -1.0)
-        Wv = V(er, t2, a0, a1, c0, c1)
-        E('acmikj,bdml->abcdijkl', Wv, t2[B, D], x, -1.0)
-        E('acmikl,dbmj->abcdijkl', Wv, t2[D, B], x, -1.0)
-        Wv = V(er, t2, a0, a1, d0, d1)
-        E('admilj,bcmk->abcdijkl', Wv, t2[B, C], x, -1.0)
-        E('admilk,cbmj->abcdijkl', Wv, t2[C, B], x, -1.0)
-        Wv = V(er, t2, b0, b1, c0, c1)
-        E('bcmjki,adml->abcdijkl', Wv, t2[A, D], x, -1.0)
-        E('bcmjkl,dami->abcdijkl', Wv, t2[D, A], x, -1.0)
-        Wv = V(er, t2, b0, b1, d0, d1)
-        E('bdmjli,acmk->abcdijkl', Wv, t2[A, C], x, -1.0)
-        E('bdmjlk,cami->abcdijkl', Wv, t2[C, A], x, -1.0)
-        Wv = V(er, t2, c0, c1, d0, d1)
-        E('cdmkli,abmj->abcdijkl', Wv, t2[A, B], x, -1.0)
-        E('cdmklj,bami->abcdijkl', Wv, t2[B, A], x, -1.0)
+        def view(name, ranges):
+            t = bufs[name]
+            if ranges is None:
+                return t
+            st = _starts(ranges, origin)
+            ln = sh.lengths(name, ranges)
+            for dim, (s0, n) in enumerate(zip(st, ln)):
+                if s0 != 0 or n != t.shape[dim]:
+                    t = t.narrow(dim, s0, n)
+            return t
+
+        for phase, subs, (xn, xr), (yn, yr), on, al in self.terms:
+            X, Y = view(xn, xr), view(yn, yr)
+            ins, o = subs.split("->")
+            if on in ("z", "x"):
+                res = torch.einsum(ins + "->" + o[4:] + o[:4], X, Y)  # storage order ijkl abcd
+                outs[on].add_(res, alpha=al)
+            else:
+                if on not in bufs:
+                    bufs[on] = torch.zeros(sh.shape[on], dtype=f64, device=self.dev)
+                bufs[on].add_(torch.einsum(subs, X, Y), alpha=al)
         return z, x
+
+    # ------------------------------------------------------------------ split path
+    @staticmethod
+    def _need(probs, outs, kind):
+        """(split-buffer bytes, FP32 output elements) of a plan, 256-byte aligned pieces."""
+        esz = 2 if kind == 0 else 4
+        nb = 0
+        for pr in probs:
+            kp = contract.padded_k(pr["k"], kind)
+            nb += 2 * ((pr["m"] * kp * esz + 255) // 256 * 256) + 2 * ((pr["n"] * kp * esz + 255) // 256 * 256)
+        ne = sum((n + 63) // 64 * 64 for _, n in outs)
+        return nb, ne
+
+    def _reserve(self, nb, ne):
+        """Shared split arena and FP32 output pool of at least nb bytes / ne elements.  All
+        group shapes reuse them (groups run in stream order); growing them drops the
+        tables that point into the old ones."""
+        if self._arena is None or self._arena.numel() < nb or self._pool.numel() < ne:
+            self._plans.clear()
+            self._arena = self._pool = None
+            self._arena = torch.empty(max(nb, 256), dtype=torch.uint8, device=self.dev)
+            self._pool = torch.empty(max(ne, 64), dtype=f32, device=self.dev)
+
+    def _plan(self, sig):
+        """Device tables of plan_problems(...) for one group shape (ba, bb, bc, dn)."""
+        no, nv, kind, dev = self.no, self.nv, self.kind, self.dev
+        probs, outs = plan_problems(no, nv, sig)
+        nb, ne = self._need(probs, outs, kind)
+        if self._arena is None:
+            # size the shared buffers for the largest group shape once
+            big = plan_problems(no, nv, (min(self.blk, nv),) * 3 + (nv,))
+            nb0, ne0 = self._need(*big, kind)
+            self._reserve(max(nb, nb0), max(ne, ne0))
+        self._reserve(nb, ne)
+        dt = torch.bfloat16 if kind == 0 else torch.float32
+        cursor = [0]
+
+        def carve(rows, kp):
+            n = rows * kp * (2 if kind == 0 else 4)
+            v = self._arena.narrow(0, cursor[0], n).view(dt).view(rows, kp)
+            cursor[0] += (n + 255) // 256 * 256
+            return v
+
+        off, out_t = 0, {}
+        for name, n in outs:
+            out_t[name] = self._pool.narrow(0, off, n)
+            off += (n + 63) // 64 * 64
+        phases = [dict(split=[], src=[], gemm=[], alpha=[]) for _ in range(2)]
+        for pr in probs:
+            kp = contract.padded_k(pr["k"], kind)
+            A = contract.Split(pr["m"], pr["k"], kind, dev, buffers=(carve(pr["m"], kp), carve(pr["m"], kp)))
+            B = contract.Split(pr["n"], pr["k"], kind, dev, buffers=(carve(pr["n"], kp), carve(pr["n"], kp)))
+            P = phases[pr["phase"]]
+            for S, op in ((A, pr["A"]), (B, pr["B"])):
+                P["split"].append([S.hi.data_ptr(), S.lo.data_ptr(), S.M, pr["k"], S.pieces[0][2], S.Kp, 0] +
+                                  list(contract.as4(op["fm"])) + list(contract.as4(op["fk"])) +
+                                  [1 if op["src"] in out_t else 0])
+                P["src"].append((op["src"], op["coef"], op["off"]))
+            P["gemm"].append([A.hi.data_ptr(), A.lo.data_ptr(), A.Kp, B.hi.data_ptr(), B.lo.data_ptr(), B.Kp,
+                              pr["m"], pr["n"], A.Kp, out_t[pr["out"]].data_ptr() + 4 * pr["ooff"], 1] +
+                             list(contract.as4(pr["orow"])) + list(contract.as4(pr["ocol"])))
+            P["alpha"].append(pr["alpha"])
+        plan = {"zero": self._pool.narrow(0, 0, off), "out": out_t, "phases": []}
+        for P in phases:
+            plan["phases"].append({
+                "split": contract.GroupedSplit(np.asarray(P["split"], dtype=np.int64), kind, dev),
+                "gemm": contract.GroupedGemm(np.asarray(P["gemm"], dtype=np.int64),
+                                             np.asarray(P["alpha"], dtype=np.float64), kind, dev),
+                "src_names": [x[0] for x in P["src"]],
+                "src_coef": np.stack([x[1] for x in P["src"]]),
+                "src_off": np.array([x[2] for x in P["src"]], dtype=np.int64),
+            })
+        return plan
+
+    def prepare(self, group_list=None):
+        """Build the grouped tables of every group shape in group_list (default: all
+        groups) ahead of run(), so no planning happens inside a timed region."""
+        if self.kind is None:
+            return
+        for (a0, a1, b0, b1, c0, c1) in (group_list if group_list is not None else groups(self.nv, self.blk)):
+            sig = (a1 - a0, b1 - b0, c1 - c0, self.nv - c0)
+            if sig not in self._plans:
+                self._plans[sig] = self._plan(sig)
+
+    def _run_split(self, er, t2, slabs, r):
+        no, nv = self.no, self.nv
+        a0, a1, b0, b1, c0, c1, d0, d1 = r
+        sig = (a1 - a0, b1 - b0, c1 - c0, d1 - d0)
+        plan = self._plans.get(sig)
+        if plan is None:
+            plan = self._plans[sig] = self._plan(sig)
+        plan["zero"].zero_()
+        base = dict(er)
+        base["t2"] = t2
+        base.update(slabs)
+        base.update(plan["out"])
+        org = np.array([a0, b0, c0, d0], dtype=np.int64)
+        for ph in plan["phases"]:
+            offs = ph["src_coef"] @ org + ph["src_off"]
+            ptrs = [base[nm].data_ptr() + int(o) * base[nm].element_size() for nm, o in zip(ph["src_names"], offs)]
+            ph["split"].run(ptrs)
+            ph["gemm"].run(self.status)
+        return plan["out"]["z"], plan["out"]["x"]
 
     def run(self, er, t2, t3_abc, e_occ, e_vir, group_list=None):
         """Accumulate [Q] and (Q) over the tasks of `group_list` (default: all groups).
         Returns the device tensor [e_bracket, e_paren]."""
-        blk, nv = self.blk, self.nv
-        for (a0, a1, b0, b1, c0, c1) in (group_list if group_list is not None else groups(nv, blk)):
-            z, x = self.group(er, t2, t3_abc, a0, a1, b0, b1, c0, c1)
-            ba, bb, bc = a1 - a0, b1 - b0, c1 - c0
-            for d0, d1 in prange(c0, nv, blk):
-                bd = d1 - d0
-                self.z4_task[:ba, :bb, :bc, :bd].copy_(z[:, :, :, d0 - c0:d1 - c0])
-                self.t4_task[:ba, :bb, :bc, :bd].copy_(x[:, :, :, d0 - c0:d1 - c0])
-                _c_rccsdt_q.q_task_epilogue(self.t4_task, self.z4_task, er["vvoo"], t2, e_occ, e_vir,
-                                            (a0, a1, b0, b1, c0, c1, d0, d1), blk, self.no, nv, self.out,
-                                            workspace=self.ws)
+        nv, no = self.nv, self.no
+        er = {k: v.contiguous() for k, v in er.items()}
+        t2 = t2.contiguous()
+        vvooT, t2T = self._transposed(er, t2)
+        for (a0, a1, b0, b1, c0, c1) in (group_list if group_list is not None else groups(nv, self.blk)):
+            r = (a0, a1, b0, b1, c0, c1, c0, nv)
+            slabs = self._slabs(t3_abc, r)
+            if self.kind is None:
+                z, x = self._run_fp64(er, t2, slabs, r)
+            else:
+                z, x = self._run_split(er, t2, slabs, r)
+            _c_rccsdt_q.q_group_epilogue(x, z, vvooT, t2T, e_occ, e_vir, r, no, nv, self.out, workspace=self.ws)
         return self.out
 
 

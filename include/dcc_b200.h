@@ -283,6 +283,20 @@ DCC_API int dcc_q_task_epilogue(const double *t4, const double *z4, const double
                         int64_t c0, int64_t c1, int64_t d0, int64_t d1, int64_t blksize, int64_t nocc,
                         int64_t nvir, double *out, void *workspace, size_t workspace_bytes, void *stream);
 
+/* The same epilogue over a whole task group (the tasks sharing a-, b- and
+ * c-blocks, d over [d0, d1)): t4 and z4 (DEVICE, float64, or float32 when
+ * f32 = 1) are stored [i][j][k][l][a][b][c][d] over the ranges [a0, a1) x
+ * [b0, b1) x [c0, c1) x [d0, d1); vvooT and t2T are eris_vvoo and t2_vvoo
+ * with the second virtual index fastest, [nvir][nocc][nocc][nvir] (DEVICE).
+ * Each (a, b, c, d) of the group enters with its factor (distr_cc/rccsdt_q.py:
+ * 410-428), so the sums equal those of the group's tasks.  workspace >=
+ * dcc_q_group_epilogue_workspace_bytes(). */
+DCC_API size_t dcc_q_group_epilogue_workspace_bytes(void);
+DCC_API int dcc_q_group_epilogue(const void *t4, const void *z4, int f32, const double *vvooT, const double *t2T,
+                                 const double *e_occ, const double *e_vir, int64_t a0, int64_t a1, int64_t b0,
+                                 int64_t b1, int64_t c0, int64_t c1, int64_t d0, int64_t d1, int64_t nocc,
+                                 int64_t nvir, double *out, void *workspace, size_t workspace_bytes, void *stream);
+
 /* ----------------------------------------------------------------------
  * Split-precision tensor-core contractions (the dense T3/T4 residual terms)
  * ---------------------------------------------------------------------- */
@@ -329,6 +343,46 @@ DCC_API int dcc_split_operand_at4(const double *src, void *hi, void *lo, int64_t
 DCC_API int dcc_gemm_split3_ld4(const void *A_hi, const void *A_lo, int64_t lda, const void *B_hi, const void *B_lo,
                                 int64_t ldb, int64_t M, int64_t N, int64_t Kp, double *C, const int64_t *epi14,
                                 double alpha, double beta, int kind, int *status, void *stream);
+
+/* Grouped split and grouped GEMM: every einsum of one (Q) task group
+ * (distr_cc/rccsdt_q.py:390-408, :1014-1129; 132 `_einsum` calls per group,
+ * each binding distr_cc/rccsdt_q.py:259) in a handful of launches instead of
+ * one split pair and one GEMM per call.
+ *
+ * dcc_split_grouped_table uploads the parameters of nprob (<= DCC_GROUP_MAX)
+ * operand splits to the DEVICE buffer `table` (dcc_split_grouped_table_bytes)
+ * and returns their total tile count; spec holds DCC_SPLIT_SPEC int64 values
+ * per operand (HOST): hi, lo (device pointers), M, K, kw, ld, k0, map14 (row
+ * map then contraction map, four digits each), source type (0 float64,
+ * 1 float32).  dcc_split_grouped then fills every operand from its source
+ * srcs[p] (HOST array of DEVICE pointers), so one table serves every group
+ * of the same shape.
+ *
+ * dcc_gemm_grouped_table encodes nprob problems C[row(m) + col(n)] +=
+ * alpha[p] * (A B^T)[m][n] into the DEVICE buffer `table` (64-byte aligned,
+ * dcc_gemm_grouped_table_bytes); spec holds DCC_GEMM_SPEC int64 values per
+ * problem (HOST): A_hi, A_lo, lda, B_hi, B_lo, ldb, M, N, Kp, C, output type
+ * (0 float64, 1 float32, the same for every problem), epi14, with output
+ * offsets below 2^31.  Kp is a multiple of 32 (bf16x3) or 16 (tf32x3).
+ * dcc_gemm_grouped runs them all in one persistent launch (out_f32: the
+ * table's output type; a mismatch stops the kernel with DCC_ERR_SHAPE in
+ * *status); the
+ * results are added with reductions in L2, so problems may share C (the
+ * summation order between problems is not fixed).  status as for
+ * dcc_gemm_split3. */
+#define DCC_GROUP_MAX 256
+#define DCC_SPLIT_SPEC 22
+#define DCC_GEMM_SPEC 25
+DCC_API size_t dcc_split_grouped_table_bytes(int nprob);
+DCC_API int dcc_split_grouped_table(const int64_t *spec, int nprob, void *table, size_t table_bytes,
+                                    int64_t *total_tiles);
+DCC_API int dcc_split_grouped(const void *table, int nprob, int64_t total_tiles, const void *const *srcs, int kind,
+                              void *stream);
+DCC_API size_t dcc_gemm_grouped_table_bytes(int nprob);
+DCC_API int dcc_gemm_grouped_table(const int64_t *spec, const double *alpha, int nprob, int kind, void *table,
+                                   size_t table_bytes, int64_t *total_tiles);
+DCC_API int dcc_gemm_grouped(const void *table, int nprob, int64_t total_tiles, int kind, int out_f32, int *status,
+                             void *stream);
 
 /* dcc_gemm_split3 over the first Kp columns of pieces whose rows are lda / ldb
  * elements apart (multiples of 8, >= Kp): one operand of a K-concatenated
