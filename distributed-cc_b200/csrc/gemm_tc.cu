@@ -478,19 +478,25 @@ __device__ __forceinline__ void split_tile(const S *__restrict__ src, const Spli
             tile[r * SP_PITCH + lane + 32] = SplitWord<KIND>::make(vb);
         }
     } else {
+        // only the tile's columns below kw are written: stop there (kw - kt is a multiple of 8)
+        const int kn = (int)((a.kw - kt) < SP_TK ? (a.kw - kt) : SP_TK);
 #pragma unroll 16
-        for (int kk = 0; kk < SP_TK; kk++) {
+        for (int kk = 0; kk < kn; kk++) {
             const int ko = __shfl_sync(0xffffffffu, kk < 32 ? koa : kob, kk & 31);
             const double v = (rvalid && ko >= 0) ? split_src(base, ko) : 0.0;
             tile[lane * SP_PITCH + kk] = SplitWord<KIND>::make(v);
         }
     }
     __syncwarp();
-    const int kc = (lane & 7) * 8;
+    // lpr lanes per row write 8 columns each: 8 lanes for a full 64-column tile, fewer
+    // (and more rows at a time) for a narrow one
+    const int64_t kleft = a.kw - kt;
+    const int lsh = kleft > 32 ? 3 : (kleft > 16 ? 2 : (kleft > 8 ? 1 : 0));  // log2(lanes per row)
+    const int kc = (lane & ((1 << lsh) - 1)) * 8;
     const int64_t kbeg = kt + kc;
-#pragma unroll 2
-    for (int rr = 0; rr < SP_TM; rr += 4) {
-        const int r = rr + (lane >> 3);
+    const int rpi = 32 >> lsh;  // rows per iteration
+    for (int rr = 0; rr < SP_TM; rr += rpi) {
+        const int r = rr + (lane >> lsh);
         const int64_t rrow = __shfl_sync(0xffffffffu, row, r);
         const bool rv = __shfl_sync(0xffffffffu, rvalid, r);
         if (!rv || kbeg >= a.kw) continue;
@@ -613,8 +619,17 @@ struct alignas(64) GemmProblem {
     int num_m, num_n, out_f32, tile_begin;
 };
 
-__device__ __forceinline__ void red_add(float *p, float v) { atomicAdd(p, v); }
-__device__ __forceinline__ void red_add(double *p, double v) { atomicAdd(p, v); }
+// Fire-and-forget reduction into global memory (red, no value returned).  The
+// pointers come from the problem table as generic addresses, for which the
+// compiler would emit a returning generic atomic; name the global space here.
+__device__ __forceinline__ void red_add(float *p, float v) {
+    asm volatile("{\n\t.reg .u64 g;\n\tcvta.to.global.u64 g, %0;\n\tred.global.add.f32 [g], %1;\n\t}" ::"l"(p), "f"(v)
+                 : "memory");
+}
+__device__ __forceinline__ void red_add(double *p, double v) {
+    asm volatile("{\n\t.reg .u64 g;\n\tcvta.to.global.u64 g, %0;\n\tred.global.add.f64 [g], %1;\n\t}" ::"l"(p), "d"(v)
+                 : "memory");
+}
 
 // Tile t's problem: the last p with tile_begin <= t (tile_begin ascending).
 __device__ __forceinline__ int grouped_find(const int *tb, int nprob, int t) {
@@ -1149,8 +1164,10 @@ extern "C" int dcc_gemm_grouped_table(const int64_t *spec, const double *alpha, 
     for (int p = 0; p < nprob && rc == DCC_OK; p++) {
         const int64_t *v = spec + (int64_t)p * DCC_GEMM_SPEC;
         const int64_t lda = v[2], ldb = v[5], M = v[6], N = v[7], Kp = v[8];
-        if (!(M >= 1 && N >= 1 && M < (1ll << 31) && N < (1ll << 31) && Kp >= kblk && Kp % kblk == 0 && lda >= Kp &&
-              ldb >= Kp && lda % 8 == 0 && ldb % 8 == 0 && lda < (1ll << 31) && ldb < (1ll << 31))) {
+        // a pitch below Kp stores only the leading lda columns: the tensor map then
+        // ends there and the TMA fills the rest of each k-block with zeros
+        if (!(M >= 1 && N >= 1 && M < (1ll << 31) && N < (1ll << 31) && Kp >= kblk && Kp % kblk == 0 && lda >= 8 &&
+              ldb >= 8 && lda % 8 == 0 && ldb % 8 == 0 && lda < (1ll << 31) && ldb < (1ll << 31))) {
             set_error("problem %d: bad sizes (M=%lld N=%lld Kp=%lld lda=%lld ldb=%lld)", p, (long long)M,
                       (long long)N, (long long)Kp, (long long)lda, (long long)ldb);
             rc = DCC_ERR_SHAPE;
@@ -1168,10 +1185,11 @@ extern "C" int dcc_gemm_grouped_table(const int64_t *spec, const double *alpha, 
             rc = DCC_ERR_SHAPE;
             break;
         }
-        if ((rc = make_map(&g.tm[0], (void *)v[0], kind, M, Kp, lda, GM, kb)) ||
-            (rc = make_map(&g.tm[1], (void *)v[1], kind, M, Kp, lda, GM, kb)) ||
-            (rc = make_map(&g.tm[2], (void *)v[3], kind, N, Kp, ldb, GN, kb)) ||
-            (rc = make_map(&g.tm[3], (void *)v[4], kind, N, Kp, ldb, GN, kb)))
+        const int64_t ka = lda < Kp ? lda : Kp, kb_ = ldb < Kp ? ldb : Kp;
+        if ((rc = make_map(&g.tm[0], (void *)v[0], kind, M, ka, lda, GM, kb)) ||
+            (rc = make_map(&g.tm[1], (void *)v[1], kind, M, ka, lda, GM, kb)) ||
+            (rc = make_map(&g.tm[2], (void *)v[3], kind, N, kb_, ldb, GN, kb)) ||
+            (rc = make_map(&g.tm[3], (void *)v[4], kind, N, kb_, ldb, GN, kb)))
             break;
         if (map_span(g.epi.row, M) + map_span(g.epi.col, N) >= (1ll << 31)) {
             set_error("problem %d: output offsets must fit in 31 bits", p);

@@ -304,8 +304,12 @@ class QEnergy:
     (physicist slices, the reference's eris.pppp cuts); t2 [a,b,i,j] (vvoo order);
     e_occ, e_vir; t3_abc: T3[a<=b<=c][i][j][k] (dcc.rccsdt.redistribute_ijk_to_abc)."""
 
-    def __init__(self, nocc, nvir, blksize=4, precision="fp64", device="cuda"):
+    def __init__(self, nocc, nvir, blksize=4, precision="fp64", device="cuda", dchunk=None):
         self.no, self.nv, self.blk, self.precision = int(nocc), int(nvir), int(blksize), precision
+        # dchunk: the split path may run a group's d range in chunks of this many virtuals
+        # (default: the whole range in one pass, which measured fastest: the reductions go
+        # through L2 whether or not the group blocks fit in it)
+        self.dchunk = int(dchunk) if dchunk else self.nv
         self.kind = None if precision == "fp64" else contract.KIND[precision]
         self.dev = torch.device(device)
         self.ws = torch.empty((_c_rccsdt_q.q_group_epilogue_workspace_bytes() + 7) // 8, dtype=f64,
@@ -321,17 +325,20 @@ class QEnergy:
         return self.kind is None or int(self.status.item()) == 0
 
     # ------------------------------------------------------------------ group data
-    def _slabs(self, t3_abc, r):
-        """The group's six T3 slabs (FP64, filled on the device)."""
+    def _slabs(self, t3_abc, r, which=_SLABS, out=None):
+        """T3 slabs of the group / d-chunk r (FP64, filled on the device)."""
         nv, no = self.nv, self.no
         rng = {"a": (r[0], r[1]), "b": (r[2], r[3]), "c": (r[4], r[5]), "d": (r[6], r[7])}
-        out = {}
-        for s in _SLABS:
+        out = {} if out is None else out
+        for s in which:
             (x0, x1), (y0, y1) = rng[s[1]], rng[s[2]]
             t = torch.empty((x1 - x0, y1 - y0, nv, no, no, no), dtype=f64, device=self.dev)
             _c_rccsdt_q.fill_t3_from_abc(t, x0, x1, y0, y1, nv, no, t3_abc, y1 - y0)
             out[s] = t
         return out
+
+    def _chunks(self, c0):
+        return [(c0, self.nv)] if self.kind is None else prange(c0, self.nv, self.dchunk)
 
     def _transposed(self, er, t2):
         if self._vvooT is None:
@@ -383,8 +390,8 @@ class QEnergy:
         esz = 2 if kind == 0 else 4
         nb = 0
         for pr in probs:
-            kp = contract.padded_k(pr["k"], kind)
-            nb += 2 * ((pr["m"] * kp * esz + 255) // 256 * 256) + 2 * ((pr["n"] * kp * esz + 255) // 256 * 256)
+            k8 = (pr["k"] + 7) // 8 * 8
+            nb += 2 * ((pr["m"] * k8 * esz + 255) // 256 * 256) + 2 * ((pr["n"] * k8 * esz + 255) // 256 * 256)
         ne = sum((n + 63) // 64 * 64 for _, n in outs)
         return nb, ne
 
@@ -405,7 +412,7 @@ class QEnergy:
         nb, ne = self._need(probs, outs, kind)
         if self._arena is None:
             # size the shared buffers for the largest group shape once
-            big = plan_problems(no, nv, (min(self.blk, nv),) * 3 + (nv,))
+            big = plan_problems(no, nv, (min(self.blk, nv),) * 3 + (min(self.dchunk, nv),))
             nb0, ne0 = self._need(*big, kind)
             self._reserve(max(nb, nb0), max(ne, ne0))
         self._reserve(nb, ne)
@@ -424,17 +431,22 @@ class QEnergy:
             off += (n + 63) // 64 * 64
         phases = [dict(split=[], src=[], gemm=[], alpha=[]) for _ in range(2)]
         for pr in probs:
-            kp = contract.padded_k(pr["k"], kind)
-            A = contract.Split(pr["m"], pr["k"], kind, dev, buffers=(carve(pr["m"], kp), carve(pr["m"], kp)))
-            B = contract.Split(pr["n"], pr["k"], kind, dev, buffers=(carve(pr["n"], kp), carve(pr["n"], kp)))
+            # operands keep only their K columns (rounded up to 8): the GEMM's tensor maps
+            # end there and read the padding up to the k-block as zeros
+            k, kp, k8 = pr["k"], contract.padded_k(pr["k"], kind), (pr["k"] + 7) // 8 * 8
+            bufs = {}
             P = phases[pr["phase"]]
-            for S, op in ((A, pr["A"]), (B, pr["B"])):
-                P["split"].append([S.hi.data_ptr(), S.lo.data_ptr(), S.M, pr["k"], S.pieces[0][2], S.Kp, 0] +
+            for side, rows in (("A", pr["m"]), ("B", pr["n"])):
+                op = pr[side]
+                hi, lo = carve(rows, k8), carve(rows, k8)
+                bufs[side] = (hi, lo)
+                P["split"].append([hi.data_ptr(), lo.data_ptr(), rows, k, k8, k8, 0] +
                                   list(contract.as4(op["fm"])) + list(contract.as4(op["fk"])) +
                                   [1 if op["src"] in out_t else 0])
                 P["src"].append((op["src"], op["coef"], op["off"]))
-            P["gemm"].append([A.hi.data_ptr(), A.lo.data_ptr(), A.Kp, B.hi.data_ptr(), B.lo.data_ptr(), B.Kp,
-                              pr["m"], pr["n"], A.Kp, out_t[pr["out"]].data_ptr() + 4 * pr["ooff"], 1] +
+            (ah, al), (bh, bl) = bufs["A"], bufs["B"]
+            P["gemm"].append([ah.data_ptr(), al.data_ptr(), k8, bh.data_ptr(), bl.data_ptr(), k8,
+                              pr["m"], pr["n"], kp, out_t[pr["out"]].data_ptr() + 4 * pr["ooff"], 1] +
                              list(contract.as4(pr["orow"])) + list(contract.as4(pr["ocol"])))
             P["alpha"].append(pr["alpha"])
         plan = {"zero": self._pool.narrow(0, 0, off), "out": out_t, "phases": []}
@@ -455,9 +467,10 @@ class QEnergy:
         if self.kind is None:
             return
         for (a0, a1, b0, b1, c0, c1) in (group_list if group_list is not None else groups(self.nv, self.blk)):
-            sig = (a1 - a0, b1 - b0, c1 - c0, self.nv - c0)
-            if sig not in self._plans:
-                self._plans[sig] = self._plan(sig)
+            for d0, d1 in self._chunks(c0):
+                sig = (a1 - a0, b1 - b0, c1 - c0, d1 - d0)
+                if sig not in self._plans:
+                    self._plans[sig] = self._plan(sig)
 
     def _run_split(self, er, t2, slabs, r):
         no, nv = self.no, self.nv
@@ -487,13 +500,15 @@ class QEnergy:
         t2 = t2.contiguous()
         vvooT, t2T = self._transposed(er, t2)
         for (a0, a1, b0, b1, c0, c1) in (group_list if group_list is not None else groups(nv, self.blk)):
-            r = (a0, a1, b0, b1, c0, c1, c0, nv)
-            slabs = self._slabs(t3_abc, r)
-            if self.kind is None:
-                z, x = self._run_fp64(er, t2, slabs, r)
-            else:
-                z, x = self._run_split(er, t2, slabs, r)
-            _c_rccsdt_q.q_group_epilogue(x, z, vvooT, t2T, e_occ, e_vir, r, no, nv, self.out, workspace=self.ws)
+            slabs = self._slabs(t3_abc, (a0, a1, b0, b1, c0, c1, c0, nv), which=("Sab", "Sac", "Sbc"))
+            for d0, d1 in self._chunks(c0):
+                r = (a0, a1, b0, b1, c0, c1, d0, d1)
+                self._slabs(t3_abc, r, which=("Sad", "Sbd", "Scd"), out=slabs)
+                if self.kind is None:
+                    z, x = self._run_fp64(er, t2, slabs, r)
+                else:
+                    z, x = self._run_split(er, t2, slabs, r)
+                _c_rccsdt_q.q_group_epilogue(x, z, vvooT, t2T, e_occ, e_vir, r, no, nv, self.out, workspace=self.ws)
         return self.out
 
 

@@ -363,7 +363,9 @@ DCC_API int dcc_gemm_split3_ld4(const void *A_hi, const void *A_lo, int64_t lda,
  * dcc_gemm_grouped_table_bytes); spec holds DCC_GEMM_SPEC int64 values per
  * problem (HOST): A_hi, A_lo, lda, B_hi, B_lo, ldb, M, N, Kp, C, output type
  * (0 float64, 1 float32, the same for every problem), epi14, with output
- * offsets below 2^31.  Kp is a multiple of 32 (bf16x3) or 16 (tf32x3).
+ * offsets below 2^31.  Kp is a multiple of 32 (bf16x3) or 16 (tf32x3);
+ * lda / ldb are multiples of 8 and may be below Kp, in which case a row holds
+ * only its first lda (ldb) columns and the rest reads as zero.
  * dcc_gemm_grouped runs them all in one persistent launch (out_f32: the
  * table's output type; a mismatch stops the kernel with DCC_ERR_SHAPE in
  * *status); the

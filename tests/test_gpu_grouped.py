@@ -133,3 +133,35 @@ def test_q_group_epilogue(mods, oracle, f32, nocc, nvir, blk, gi):
     cq.q_group_epilogue(dev(t4g, tt), dev(z4g, tt), dev(vvoo.transpose(0, 2, 3, 1)), dev(t2.transpose(0, 2, 3, 1)),
                         dev(eo), dev(ev), (a0, a1, b0, b1, c0, c1, c0, nvir), nocc, nvir, out)
     np.testing.assert_allclose(out.cpu().numpy(), tot, rtol=1e-11, atol=1e-300)
+
+
+@pytest.mark.parametrize("kind", ["bf16x3", "tf32x3"])
+@pytest.mark.parametrize("K", [6, 10, 90])
+def test_grouped_compact_k(mods, kind, K):
+    """Operands stored with only their K columns (pitch K rounded up to 8, below the
+    padded Kp): the grouped split writes them and the GEMM reads zeros past the pitch."""
+    c, _ = mods
+    k = c.KIND[kind]
+    g = torch.Generator(device="cuda").manual_seed(K)
+    M, N = 200, 300
+    k8, kp = (K + 7) // 8 * 8, c.padded_k(K, k)
+    dt = torch.bfloat16 if k == 0 else torch.float32
+    A = torch.randn(M, K, dtype=torch.float64, device="cuda", generator=g)
+    B = torch.randn(K, N, dtype=torch.float64, device="cuda", generator=g)  # K-major source for B: strided rows
+    bufs = [torch.full((r, k8), float("nan"), dtype=dt, device="cuda") for r in (M, M, N, N)]
+    spec = [[bufs[0].data_ptr(), bufs[1].data_ptr(), M, K, k8, k8, 0] + list(c.as4(c.lin(K))) + list(c.as4(c.lin(1))) + [0],
+            [bufs[2].data_ptr(), bufs[3].data_ptr(), N, K, k8, k8, 0] + list(c.as4(c.lin(1))) + list(c.as4(c.lin(N))) + [0]]
+    gs = c.GroupedSplit(np.array(spec, dtype=np.int64), k, "cuda")
+    gs.run([A.data_ptr(), B.data_ptr()])
+    out = torch.zeros(M, N, dtype=torch.float32, device="cuda")
+    row = [bufs[0].data_ptr(), bufs[1].data_ptr(), k8, bufs[2].data_ptr(), bufs[3].data_ptr(), k8, M, N, kp,
+           out.data_ptr(), 1] + list(c.as4(c.lin(N))) + list(c.as4(c.lin(1)))
+    gg = c.GroupedGemm(np.array([row], dtype=np.int64), np.array([1.0]), k, "cuda")
+    status = torch.zeros(1, dtype=torch.int32, device="cuda")
+    gg.run(status)
+    torch.cuda.synchronize()
+    assert int(status.item()) == 0
+    assert not torch.isnan(bufs[0]).any() and not torch.isnan(bufs[2]).any()
+    ref = A @ B
+    rel = float((out.double() - ref).abs().max() / ref.abs().max())
+    assert rel < TOL[kind] + 1e-6

@@ -48,3 +48,22 @@ def test_q_energy_split(mods, oracle, precision):
     got = gq.q_energy(d[0], d[1], d[2], d[3], d[4], no, nv, blk, precision)
     assert abs(got[0] - want[0]) <= 1e-4 * abs(want[0])
     assert abs(got[1] - want[1]) <= 1e-4 * abs(want[1])
+
+
+@pytest.mark.parametrize("dchunk", [1, 2, 5])
+def test_q_energy_split_d_chunks(mods, oracle, dchunk):
+    """The split path in d-chunks of a group (including chunks that cut task blocks):
+    the same energies as the oracle's task loop."""
+    gq, q_ref = mods
+    from dcc import _c_rccsdt
+    no, nv, blk = 3, 9, 3
+    er, t2, T, eo, ev = _inputs(no, nv, 19)
+    want = q_ref.q_energy_ref(er, t2, T, eo, ev, blk, oracle)
+    d = _device(er, t2, T, eo, ev, no)
+    q = gq.QEnergy(no, nv, blk, "bf16x3", dchunk=dchunk)
+    out = q.run(d[0], d[1], _c_rccsdt.redistribute_ijk_to_abc(d[2], no, nv), d[3], d[4])
+    torch.cuda.synchronize()
+    assert q.status_ok()
+    got = out.cpu().numpy()
+    assert abs(got[0] - want[0]) <= 1e-4 * abs(want[0])
+    assert abs(got[1] - want[1]) <= 1e-4 * abs(want[1])
