@@ -435,6 +435,10 @@ struct SplitArgs {
     int64_t M, K, kw, ld, k0;
     SplitMap mp;
     int64_t nty, rmid, rfast;
+    // mode 3: a tile's rows take rA values of digit A (contiguous in the source) times
+    // 32 / rA values of digit B; the other digits of m come from the tile index
+    // (low part below the lower of the two, mid part between them, the rest above)
+    int64_t rA, sA, rB, sB, low, mid, loSpan, hiSpan;
     int32_t mode, src_f32;
 };
 
@@ -458,6 +462,12 @@ __device__ __forceinline__ void split_tile(const S *__restrict__ src, const Spli
         const int64_t a2 = ty % R2, a1 = ((ty / R2) % nb1) * SP_TM + lane, a0 = ty / (R2 * nb1);
         rvalid = a1 < R1;
         row = (a0 * R1 + a1) * R2 + a2;
+    } else if (a.mode == 3) {
+        const int64_t n2 = SP_TM / a.rA, nb2 = (a.rB + n2 - 1) / n2;
+        const int64_t o = ty / nb2, u1 = lane % a.rA, u2 = (ty % nb2) * n2 + lane / a.rA;
+        rvalid = lane < a.rA * n2 && u2 < a.rB;
+        const int64_t lo = o % a.low, md = (o / a.low) % a.mid, hi = o / (a.low * a.mid);
+        row = hi * a.hiSpan + md * a.loSpan + lo + u1 * a.sA + (rvalid ? u2 : 0) * a.sB;
     } else {
         row = ty * SP_TM + lane;
         rvalid = row < a.M;
@@ -932,30 +942,62 @@ static int split_args(void *hi, void *lo, int64_t M, int64_t K, int64_t kw, int6
     fast_digit(mp.m, ms, mr);
     int mode = -1;
     int64_t rrad = 1, rstep = 1;
+    int64_t m3[8] = {1, 0, 1, 0, 1, 1, 1, 1};  // rA, sA, rB, sB, low, mid, loSpan, hiSpan
     if (ks == 1 && kr >= 16) {
         mode = 0;
     } else if (ms == 1 || mr == 1) {
         mode = 1;
     } else {
-        // digits of m from the fastest: (radix, stride, product of the radices below it)
+        // digits of m from the fastest: radix, stride, and step (product of the radices below)
         const Map4 &f = mp.m;
         const int64_t inner = f.R1 * f.R2 * f.R3;
         const int64_t rad[4] = {f.R3, f.R2, f.R1, M % inner == 0 ? M / inner : 0};
         const int64_t str[4] = {f.S3, f.S2, f.S1, f.S0};
-        int64_t step = 1;
-        for (int q = 0; q < 4; q++) {
-            if (rad[q] >= 2 && llabs(str[q]) == 1 && q > 0 && M % (rad[q] * step) == 0) {
-                mode = 2;
-                rrad = rad[q];
-                rstep = step;
+        const int64_t stp[4] = {1, f.R3, f.R2 * f.R3, inner};
+        int q1 = -1;
+        for (int q = 1; q < 4; q++)
+            if (rad[q] >= 2 && llabs(str[q]) == 1) {
+                q1 = q;
                 break;
             }
-            step *= rad[q] > 0 ? rad[q] : 1;
+        if (q1 >= 0 && rad[q1] >= SP_TM && M % (rad[q1] * stp[q1]) == 0) {
+            mode = 2;  // 32 rows along the contiguous digit
+            rrad = rad[q1];
+            rstep = stp[q1];
+        } else if (q1 >= 0 && rad[3] > 0) {
+            // a short contiguous digit: pair it with the digit that continues it in the
+            // source (stride = its radix), else with the longest other digit
+            int q2 = -1;
+            for (int q = 0; q < 4; q++)
+                if (q != q1 && rad[q] >= 2 && llabs(str[q]) == rad[q1]) q2 = q;
+            if (q2 < 0)
+                for (int q = 0; q < 4; q++)
+                    if (q != q1 && rad[q] >= 2 && (q2 < 0 || rad[q] > rad[q2])) q2 = q;
+            if (q2 >= 0) {
+                mode = 3;
+                const int ql = q1 < q2 ? q1 : q2, qh = q1 < q2 ? q2 : q1;
+                m3[0] = rad[q1];
+                m3[1] = stp[q1];
+                m3[2] = rad[q2];
+                m3[3] = stp[q2];
+                m3[4] = stp[ql];
+                m3[5] = stp[qh] / (stp[ql] * rad[ql]);
+                m3[6] = stp[ql] * rad[ql];
+                m3[7] = stp[qh] * rad[qh];
+            }
         }
         if (mode < 0) mode = ks == 1 ? 0 : 1;
     }
-    const int64_t nty = mode == 2 ? (M / (rrad * rstep)) * ((rrad + SP_TM - 1) / SP_TM) * rstep : (M + SP_TM - 1) / SP_TM;
-    a = SplitArgs{hi, lo, M, K, kw, ld, k0, mp, nty, rrad, rstep, mode, src_f32};
+    int64_t nty;
+    if (mode == 2)
+        nty = (M / (rrad * rstep)) * ((rrad + SP_TM - 1) / SP_TM) * rstep;
+    else if (mode == 3) {
+        const int64_t n2 = SP_TM / m3[0];
+        nty = (M / (m3[0] * m3[2])) * ((m3[2] + n2 - 1) / n2);
+    } else
+        nty = (M + SP_TM - 1) / SP_TM;
+    a = SplitArgs{hi, lo, M, K, kw, ld, k0, mp, nty, rrad, rstep,
+                  m3[0], m3[1], m3[2], m3[3], m3[4], m3[5], m3[6], m3[7], mode, src_f32};
     return DCC_OK;
 }
 

@@ -38,11 +38,12 @@ def test_grouped_split_bit_exact(mods, kind):
     k = c.KIND[kind]
     g = torch.Generator(device="cuda").manual_seed(5)
     X = torch.randn(6, 7, 9, 11, dtype=torch.float64, device="cuda", generator=g)
-    # (rows, K, row map, k map) cases covering the three read modes
+    # (rows, K, row map, k map) cases covering the four read modes
     cases = [(6 * 7, 9 * 11, c.two(7, 7 * 99, 99), c.lin(1)),          # k contiguous
              (9 * 11, 6 * 7, c.lin(1), c.two(7, 7 * 99, 99)),          # rows contiguous
              (6 * 9 * 11, 7, c.three(9, 11, 7 * 99, 11, 1), c.lin(99)),  # rows contiguous, k strided
-             (7 * 11, 6 * 9, c.two(11, 99, 1), c.two(9, 7 * 99, 11))]
+             (7 * 11, 6 * 9, c.two(11, 99, 1), c.two(9, 7 * 99, 11)),
+             (6 * 11 * 7, 9, c.three(11, 7, 7 * 99, 1, 99), c.lin(11))]  # short contiguous middle digit
     rows, refs, srcs = [], [], []
     for M, K, fm, fk in cases:
         S = c.Split(M, K, k, "cuda")
