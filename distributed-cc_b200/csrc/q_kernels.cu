@@ -321,6 +321,95 @@ __global__ void __launch_bounds__(QG_THREADS, 4) k_q_group_epilogue(const T *t4,
     }
 }
 
+// Adjoint of the group epilogue for the cotangents (gb, gp) of ([Q], (Q)).  With
+// X = (t4 + z4) / D, Y = f P(X) and  gb [Q] + gp (Q) = sum Y (gp z4 + (gb + gp) z4sq) / 12
+// over the distinct positions:
+//   dX = P^T(H),  H = f (gp z4 + (gb + gp) z4sq) / 12
+//   gt4 = dX / D,  gz4 = dX / D + gp f P(X) / 12,  gz4sq = (gb + gp) f P(X) / 12
+// P^T applies the same three stages in reverse order (each transposition is its
+// own transpose); on an orbit with repeated positions the slot values stay equal
+// per position, so the value at a position's first slot is the adjoint there.
+// Every position of the group is written exactly once (zero where f = 0).
+__global__ void __launch_bounds__(QG_THREADS) k_q_group_epilogue_adj(const double *t4, const double *z4,
+                                                                     const double *vvooT, const double *t2T,
+                                                                     const double *eo, const double *ev, QGroup g,
+                                                                     int no, int nv, int64_t norb, P4Coef k,
+                                                                     double gb, double gp, double *gt4, double *gz4,
+                                                                     double *gzsq) {
+    const int lane = threadIdx.x & 31;
+    const int64_t V = (int64_t)g.ba * g.bb * g.bc * g.dn;
+    const int64_t nchunk = (V + 31) / 32, total = norb * nchunk;
+    for (int64_t w = (int64_t)blockIdx.x * QG_WARPS + (threadIdx.x >> 5); w < total;
+         w += (int64_t)gridDim.x * QG_WARPS) {
+        const int64_t r = w / nchunk, v = (w % nchunk) * 32 + lane;
+        int asc[4], base[4], pos[4];
+        decode_tri4(r, no, asc);
+        base[0] = asc[3];
+        base[1] = asc[2];
+        base[2] = asc[1];
+        base[3] = asc[0];
+        const int64_t my_off = s4_lane_offset(lane, base, no, pos);
+        const unsigned first = __ballot_sync(0xffffffffu, s4_first_holder(lane, my_off));
+        const int my_pos = pos[0] | (pos[1] << 8) | (pos[2] << 16) | (pos[3] << 24);
+        const double my_eo = dadd(dadd(eo[pos[0]], eo[pos[1]]), dadd(eo[pos[2]], eo[pos[3]]));
+        const bool valid = v < V;
+        const int64_t vv = valid ? v : 0;
+        const int id = (int)(vv % g.dn), ic = (int)((vv / g.dn) % g.bc), ib = (int)((vv / ((int64_t)g.dn * g.bc)) % g.bb),
+                  ia = (int)(vv / ((int64_t)g.dn * g.bc * g.bb));
+        const int a = g.a0 + ia, b = g.b0 + ib, c = g.c0 + ic, d = g.d0 + id;
+        const double f = valid ? q_factor(a, b, c, d) : 0.0;
+        const double neg = -dadd(dadd(dadd(ev[a], ev[b]), ev[c]), ev[d]);
+        double x[24], y[24], h[24];
+#pragma unroll
+        for (int s = 0; s < 24; s++) {
+            const int ps = __shfl_sync(0xffffffffu, my_pos, s);
+            const double eos = __shfl_sync(0xffffffffu, my_eo, s);
+            const int i = ps & 255, j = (ps >> 8) & 255, kk = (ps >> 16) & 255, l = ps >> 24;
+            const int64_t off = (((int64_t)i * no + j) * no + kk) * no + l;
+            double xv = 0.0, hv = 0.0;
+            if (f != 0.0) {
+                const double zt = z4[off * V + vv];
+                xv = dadd(t4[off * V + vv], zt);
+                const double den = dadd(eos, neg);
+                xv = (fabs(den) > 1e-15) ? __ddiv_rn(xv, den) : 0.0;
+#define VT(p, m, n, q_) ((((int64_t)(p) * no + (m)) * no + (n)) * nv + (q_))
+                const double zsq = vvooT[VT(a, i, j, b)] * t2T[VT(c, kk, l, d)] + vvooT[VT(a, i, kk, c)] * t2T[VT(b, j, l, d)] +
+                                   vvooT[VT(a, i, l, d)] * t2T[VT(b, j, kk, c)] + vvooT[VT(b, j, kk, c)] * t2T[VT(a, i, l, d)] +
+                                   vvooT[VT(b, j, l, d)] * t2T[VT(a, i, kk, c)] + vvooT[VT(c, kk, l, d)] * t2T[VT(a, i, j, b)];
+#undef VT
+                hv = f * (gp * zt + (gb + gp) * zsq) / 12.0;
+            }
+            x[s] = xv;
+            h[s] = hv;
+        }
+        // y = P(x) (forward stages), then x <- P^T(h): R, T2, T1 in that order
+        p4_t1_all(x, y, k, std::make_integer_sequence<int, 24>{});
+        p4_t2_all(y, x, k, std::make_integer_sequence<int, 24>{});
+        p4_r0_all(x, y, k, std::make_integer_sequence<int, 24>{});
+        p4_r0_all(h, x, k, std::make_integer_sequence<int, 24>{});
+        p4_t2_all(x, h, k, std::make_integer_sequence<int, 24>{});
+        p4_t1_all(h, x, k, std::make_integer_sequence<int, 24>{});
+#pragma unroll
+        for (int s = 0; s < 24; s++) {
+            if (!((first >> s) & 1u)) continue;  // warp-uniform
+            const int ps = __shfl_sync(0xffffffffu, my_pos, s);
+            const double eos = __shfl_sync(0xffffffffu, my_eo, s);
+            if (!valid) continue;
+            const int64_t off = (((int64_t)(ps & 255) * no + ((ps >> 8) & 255)) * no + ((ps >> 16) & 255)) * no +
+                                (ps >> 24);
+            double gx = 0.0, gy = 0.0;
+            if (f != 0.0) {
+                const double den = dadd(eos, neg);
+                gx = (fabs(den) > 1e-15) ? x[s] / den : 0.0;
+                gy = f * y[s] / 12.0;
+            }
+            gt4[off * V + vv] = gx;
+            gz4[off * V + vv] = gx + gp * gy;
+            gzsq[off * V + vv] = (gb + gp) * gy;
+        }
+    }
+}
+
 static unsigned q_group_grid(int64_t items) {
     int64_t g = (items + QG_WARPS - 1) / QG_WARPS;
     return (unsigned)(g < 148 * 8 ? (g ? g : 1) : 148 * 8);
@@ -445,4 +534,30 @@ extern "C" int dcc_q_group_epilogue(const void *t4, const void *z4, int f32, con
     if (rc) return rc;
     k_q_finish<<<1, 256, 0, st>>>((const double *)workspace, grid, out);
     return launch_status("q_group_epilogue finish");
+}
+
+extern "C" int dcc_q_group_epilogue_adjoint(const double *t4, const double *z4, const double *vvooT,
+                                            const double *t2T, const double *e_occ, const double *e_vir, int64_t a0,
+                                            int64_t a1, int64_t b0, int64_t b1, int64_t c0, int64_t c1, int64_t d0,
+                                            int64_t d1, int64_t nocc, int64_t nvir, double g_bracket, double g_paren,
+                                            double *gt4, double *gz4, double *gz4sq, void *stream) {
+    clear_error();
+    DCC_REQUIRE(0 <= a0 && a0 <= a1 && a1 <= nvir && 0 <= b0 && b0 <= b1 && b1 <= nvir && 0 <= c0 && c0 <= c1 &&
+                    c1 <= nvir && 0 <= d0 && d0 <= d1 && d1 <= nvir,
+                DCC_ERR_SHAPE, "virtual range out of bounds");
+    DCC_REQUIRE(nocc >= 1 && nocc <= 255, DCC_ERR_SHAPE, "nocc must be in [1, 255]");
+    DCC_REQUIRE(t4 && z4 && vvooT && t2T && e_occ && e_vir && gt4 && gz4 && gz4sq, DCC_ERR_NULL, "NULL buffer");
+    const int64_t V = (a1 - a0) * (b1 - b0) * (c1 - c0) * (d1 - d0);
+    if (V == 0) return DCC_OK;
+    DCC_REQUIRE(V * nocc * nocc * nocc * nocc < (1ll << 40), DCC_ERR_SHAPE, "group block too large");
+    P4Coef k;
+    int rc = p4_coef("P4_444", 1.0, 0.0, k);
+    if (rc) return rc;
+    const int64_t norb = binom(nocc + 3, 4);
+    const unsigned grid = q_group_grid(norb * ((V + 31) / 32));
+    QGroup g{(int)a0, (int)b0, (int)c0, (int)d0, (int)(a1 - a0), (int)(b1 - b0), (int)(c1 - c0), (int)(d1 - d0)};
+    k_q_group_epilogue_adj<<<grid, QG_THREADS, 0, as_stream(stream)>>>(t4, z4, vvooT, t2T, e_occ, e_vir, g, (int)nocc,
+                                                                      (int)nvir, norb, k, g_bracket, g_paren, gt4,
+                                                                      gz4, gz4sq);
+    return launch_status("q_group_epilogue_adjoint");
 }

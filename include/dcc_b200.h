@@ -291,6 +291,17 @@ DCC_API int dcc_q_task_epilogue(const double *t4, const double *z4, const double
  * Each (a, b, c, d) of the group enters with its factor (distr_cc/rccsdt_q.py:
  * 410-428), so the sums equal those of the group's tasks.  workspace >=
  * dcc_q_group_epilogue_workspace_bytes(). */
+/* Adjoint of dcc_q_group_epilogue (float64 blocks) for the cotangents g_bracket,
+ * g_paren of the two energies: writes, for every position of the group block,
+ * the gradients of g_bracket [Q] + g_paren (Q) with respect to t4, z4 and the
+ * disconnected z4sq (same [i][j][k][l][a][b][c][d] layout, DEVICE).  No
+ * counterpart in the reference, which has no (Q) gradient; it is the first
+ * step of the hand-written (Q) VJP. */
+DCC_API int dcc_q_group_epilogue_adjoint(const double *t4, const double *z4, const double *vvooT, const double *t2T,
+                                         const double *e_occ, const double *e_vir, int64_t a0, int64_t a1,
+                                         int64_t b0, int64_t b1, int64_t c0, int64_t c1, int64_t d0, int64_t d1,
+                                         int64_t nocc, int64_t nvir, double g_bracket, double g_paren, double *gt4,
+                                         double *gz4, double *gz4sq, void *stream);
 DCC_API size_t dcc_q_group_epilogue_workspace_bytes(void);
 DCC_API int dcc_q_group_epilogue(const void *t4, const void *z4, int f32, const double *vvooT, const double *t2T,
                                  const double *e_occ, const double *e_vir, int64_t a0, int64_t a1, int64_t b0,
