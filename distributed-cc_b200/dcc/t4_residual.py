@@ -38,3 +38,210 @@ def dense_vvvv_fvv_(r4, t4, W_vvvv, F_vv, precision="fp64"):
         W = Wf if n in (0, 5) else W_vvvv
         contract.einsum_into(s, W, t4, r4, 1.0, 1.0, kind)
     return r4
+
+
+# ----------------------------------------------------------------------------
+# compute_r4_tri without its OO batch (distr_cc/rccsdtq.py:700-1058).
+#
+# The reference adds, per stored block (i<=j<=k<=l), about a hundred strings
+# "W[occupied slots of (i,j,k,l)] . T[other slots]" over the block's virtual
+# indices.  Every such string is defined for any ordering of (i,j,k,l), so here
+# each one is ONE einsum over the full ordered occupied space,
+#   R[i,j,k,l,a,b,c,d] += alpha W[...] T[...],
+# whose canonical stored blocks are r4; the W builders are full-tensor einsums
+# (the T4 part of W_oooovv / W_oovvvv sums over every ordering of the stored
+# blocks, P4_201 applied, exactly the reference's loop over distinct
+# permutations).  W_oovvvv is kept for every ordered pair (x, y) with
+# W[x, y] = W_pair(min, max): the strings only read x <= y.
+# ----------------------------------------------------------------------------
+
+import itertools  # noqa: E402
+
+import numpy as np  # noqa: E402
+
+
+def stored_quadruples(nocc):
+    """Stored T4 blocks: i<=j<=k<=l in lexicographic order without three equal indices
+    (distr_cc/distribute_t4.py:68-70)."""
+    return [(i, j, k, l) for i in range(nocc) for j in range(i, nocc) for k in range(j, nocc)
+            for l in range(k, nocc) if not (i == j == k or j == k == l)]
+
+
+def unpack_all_orderings(t4, nocc):
+    """T[o] for every ordered quadruple o: the stored canonical block with its virtual
+    axes permuted (axis p of the ordering is axis rank(p) of the canonical block, stable
+    sort of the occupied values); zero where the canonical block is not stored."""
+    nv = t4.shape[1]
+    quads = stored_quadruples(nocc)
+    index = {q: n for n, q in enumerate(quads)}
+    out = torch.zeros((nocc ** 4,) + (nv,) * 4, dtype=t4.dtype, device=t4.device)
+    groups = {}
+    for o in itertools.product(range(nocc), repeat=4):
+        order = sorted(range(4), key=lambda p: (o[p], p))
+        can = tuple(o[p] for p in order)
+        if can not in index:
+            continue
+        rank = tuple(order.index(p) for p in range(4))
+        flat = ((o[0] * nocc + o[1]) * nocc + o[2]) * nocc + o[3]
+        groups.setdefault(rank, ([], []))
+        groups[rank][0].append(flat)
+        groups[rank][1].append(index[can])
+    for rank, (dst, src) in groups.items():
+        d = torch.tensor(dst, device=t4.device)
+        s = torch.tensor(src, device=t4.device)
+        out[d] = t4[s].permute(0, *(1 + r for r in rank))
+    return out.view((nocc,) * 4 + (nv,) * 4)
+
+
+def _slots(tensor, slots, sub):
+    """Subscripts of a full tensor cut as the reference cuts it per block: `sub` are the
+    block-level subscripts, `slots` the occupied letters the reference fixes."""
+    if tensor in ("W_vvvo",):
+        return sub + slots
+    if tensor == "W_vooo":
+        return sub + slots
+    if tensor in ("W_oovvvo", "W_ooooov", "W_oooovv", "W_oovvvv", "t3", "t3p", "t3s"):
+        return slots + sub
+    if tensor in ("W_ovovvo", "W_ovovvo_s"):
+        return slots[0] + sub[0] + slots[1] + sub[1:]
+    if tensor in ("t3_m", "t3p_m", "t3s_m"):  # t3[:, x, y]
+        return sub[0] + slots + sub[1:]
+    if tensor == "t3_mn":  # t3[:, :, x]
+        return sub[:2] + slots + sub[2:]
+    if tensor == "t2_m":  # t2[:, x]
+        return sub[0] + slots + sub[1:]
+    if tensor == "t2":  # t2[x, y]
+        return slots + sub
+    raise ValueError(tensor)
+
+
+# (block string, W tensor, W slots, T tensor, T slots, alpha) of distr_cc/rccsdtq.py:862-1033
+_R4_STRINGS = [
+    ("abe,ecd", "W_vvvo", "j", "t3", "ikl", 1.0), ("ace,ebd", "W_vvvo", "k", "t3", "ijl", 1.0),
+    ("ade,ebc", "W_vvvo", "l", "t3", "ijk", 1.0), ("bae,ecd", "W_vvvo", "i", "t3", "jkl", 1.0),
+    ("cae,ebd", "W_vvvo", "i", "t3", "kjl", 1.0), ("dae,ebc", "W_vvvo", "i", "t3", "ljk", 1.0),
+    ("bce,ead", "W_vvvo", "k", "t3", "jil", 1.0), ("bde,eac", "W_vvvo", "l", "t3", "jik", 1.0),
+    ("cbe,ead", "W_vvvo", "j", "t3", "kil", 1.0), ("dbe,eac", "W_vvvo", "j", "t3", "lik", 1.0),
+    ("cde,eab", "W_vvvo", "l", "t3", "kij", 1.0), ("dce,eab", "W_vvvo", "k", "t3", "lij", 1.0),
+    ("am,mbcd", "W_vooo", "ij", "t3_m", "kl", -1.0), ("am,mcbd", "W_vooo", "ik", "t3_m", "jl", -1.0),
+    ("am,mdbc", "W_vooo", "il", "t3_m", "jk", -1.0), ("bm,macd", "W_vooo", "ji", "t3_m", "kl", -1.0),
+    ("cm,mabd", "W_vooo", "ki", "t3_m", "jl", -1.0), ("dm,mabc", "W_vooo", "li", "t3_m", "jk", -1.0),
+    ("bm,mcad", "W_vooo", "jk", "t3_m", "il", -1.0), ("bm,mdac", "W_vooo", "jl", "t3_m", "ik", -1.0),
+    ("cm,mbad", "W_vooo", "kj", "t3_m", "il", -1.0), ("dm,mbac", "W_vooo", "lj", "t3_m", "ik", -1.0),
+    ("cm,mdab", "W_vooo", "kl", "t3_m", "ij", -1.0), ("dm,mcab", "W_vooo", "lk", "t3_m", "ij", -1.0),
+    ("eabm,mecd", "W_oovvvo", "ij", "t3p_m", "kl", 0.5), ("eacm,mebd", "W_oovvvo", "ik", "t3p_m", "jl", 0.5),
+    ("eadm,mebc", "W_oovvvo", "il", "t3p_m", "jk", 0.5), ("ebcm,mead", "W_oovvvo", "jk", "t3p_m", "il", 0.5),
+    ("ebdm,meac", "W_oovvvo", "jl", "t3p_m", "ik", 0.5), ("ecdm,meab", "W_oovvvo", "kl", "t3p_m", "ij", 0.5),
+    ("ecbm,maed", "W_ovovvo", "ij", "t3_m", "kl", -1.0), ("edbm,maec", "W_ovovvo", "ij", "t3_m", "lk", -1.0),
+    ("ebcm,maed", "W_ovovvo", "ik", "t3_m", "jl", -1.0), ("ebdm,maec", "W_ovovvo", "il", "t3_m", "jk", -1.0),
+    ("edcm,maeb", "W_ovovvo", "ik", "t3_m", "lj", -1.0), ("ecdm,maeb", "W_ovovvo", "il", "t3_m", "kj", -1.0),
+    ("ecam,mbed", "W_ovovvo", "ji", "t3_m", "kl", -1.0), ("edam,mbec", "W_ovovvo", "ji", "t3_m", "lk", -1.0),
+    ("ebam,mced", "W_ovovvo", "ki", "t3_m", "jl", -1.0), ("ebam,mdec", "W_ovovvo", "li", "t3_m", "jk", -1.0),
+    ("edam,mceb", "W_ovovvo", "ki", "t3_m", "lj", -1.0), ("ecam,mdeb", "W_ovovvo", "li", "t3_m", "kj", -1.0),
+    ("eacm,mbed", "W_ovovvo", "jk", "t3_m", "il", -1.0), ("eadm,mbec", "W_ovovvo", "jl", "t3_m", "ik", -1.0),
+    ("eabm,mced", "W_ovovvo", "kj", "t3_m", "il", -1.0), ("eabm,mdec", "W_ovovvo", "lj", "t3_m", "ik", -1.0),
+    ("eadm,mceb", "W_ovovvo", "kl", "t3_m", "ij", -1.0), ("eacm,mdeb", "W_ovovvo", "lk", "t3_m", "ij", -1.0),
+    ("edcm,mbea", "W_ovovvo", "jk", "t3_m", "li", -1.0), ("ecdm,mbea", "W_ovovvo", "jl", "t3_m", "ki", -1.0),
+    ("edbm,mcea", "W_ovovvo", "kj", "t3_m", "li", -1.0), ("ecbm,mdea", "W_ovovvo", "lj", "t3_m", "ki", -1.0),
+    ("ebdm,mcea", "W_ovovvo", "kl", "t3_m", "ji", -1.0), ("ebcm,mdea", "W_ovovvo", "lk", "t3_m", "ji", -1.0),
+    ("eabm,mced", "W_ovovvo_s", "ij", "t3s_m", "kl", -0.5), ("eacm,mbed", "W_ovovvo_s", "ik", "t3s_m", "jl", -0.5),
+    ("eadm,mbec", "W_ovovvo_s", "il", "t3s_m", "jk", -0.5), ("ebcm,maed", "W_ovovvo_s", "jk", "t3s_m", "il", -0.5),
+    ("ebdm,maec", "W_ovovvo_s", "jl", "t3s_m", "ik", -0.5), ("ecdm,maeb", "W_ovovvo_s", "kl", "t3s_m", "ij", -0.5),
+    ("nma,mnbcd", "W_ooooov", "kji", "t3_mn", "l", 1.0), ("nma,mnbdc", "W_ooooov", "lji", "t3_mn", "k", 1.0),
+    ("nma,mncdb", "W_ooooov", "lki", "t3_mn", "j", 1.0), ("nmb,mnacd", "W_ooooov", "kij", "t3_mn", "l", 1.0),
+    ("nmb,mnadc", "W_ooooov", "lij", "t3_mn", "k", 1.0), ("nmb,mncda", "W_ooooov", "lkj", "t3_mn", "i", 1.0),
+    ("nmc,mnabd", "W_ooooov", "jik", "t3_mn", "l", 1.0), ("nmc,mnadb", "W_ooooov", "lik", "t3_mn", "j", 1.0),
+    ("nmc,mnbda", "W_ooooov", "ljk", "t3_mn", "i", 1.0), ("nmd,mnabc", "W_ooooov", "jil", "t3_mn", "k", 1.0),
+    ("nmd,mnacb", "W_ooooov", "kil", "t3_mn", "j", 1.0), ("nmd,mnbca", "W_ooooov", "kjl", "t3_mn", "i", 1.0),
+    ("mab,mcd", "W_oooovv", "ijk", "t2_m", "l", -1.0), ("mab,mdc", "W_oooovv", "ijl", "t2_m", "k", -1.0),
+    ("mac,mbd", "W_oooovv", "ikj", "t2_m", "l", -1.0), ("mad,mbc", "W_oooovv", "ilj", "t2_m", "k", -1.0),
+    ("mac,mdb", "W_oooovv", "ikl", "t2_m", "j", -1.0), ("mad,mcb", "W_oooovv", "ilk", "t2_m", "j", -1.0),
+    ("mbc,mad", "W_oooovv", "jki", "t2_m", "l", -1.0), ("mbd,mac", "W_oooovv", "jli", "t2_m", "k", -1.0),
+    ("mcd,mab", "W_oooovv", "kli", "t2_m", "j", -1.0), ("mbc,mda", "W_oooovv", "jkl", "t2_m", "i", -1.0),
+    ("mbd,mca", "W_oooovv", "jlk", "t2_m", "i", -1.0), ("mcd,mba", "W_oooovv", "klj", "t2_m", "i", -1.0),
+    ("abce,ed", "W_oovvvv", "jk", "t2", "il", 1.0), ("abde,ec", "W_oovvvv", "jl", "t2", "ik", 1.0),
+    ("acde,eb", "W_oovvvv", "kl", "t2", "ij", 1.0), ("bace,ed", "W_oovvvv", "ik", "t2", "jl", 1.0),
+    ("bade,ec", "W_oovvvv", "il", "t2", "jk", 1.0), ("cabe,ed", "W_oovvvv", "ij", "t2", "kl", 1.0),
+    ("dabe,ec", "W_oovvvv", "ij", "t2", "lk", 1.0), ("cade,eb", "W_oovvvv", "il", "t2", "kj", 1.0),
+    ("dace,eb", "W_oovvvv", "ik", "t2", "lj", 1.0), ("bcde,ea", "W_oovvvv", "kl", "t2", "ji", 1.0),
+    ("cbde,ea", "W_oovvvv", "jl", "t2", "ki", 1.0), ("dbce,ea", "W_oovvvv", "jk", "t2", "li", 1.0),
+]
+
+
+def _einsum(kind, subs, X, Y, out, alpha):
+    if kind is None:
+        ins, o = subs.split("->")
+        out.add_(torch.einsum(subs, X, Y), alpha=alpha)
+    else:
+        contract.einsum_into(subs, X, Y, out, alpha, 1.0, kind)
+
+
+def build_intermediates(eris, W_oooo, W_ovov, W_vvvv, t2, t3, t3p, t4, nocc, spin4):
+    """The W builders of distr_cc/rccsdtq.py:700-833 as full tensors (FP64, torch)."""
+    e = torch.einsum
+    o, v = slice(0, nocc), slice(nocc, None)
+    W = {}
+    X = 2.0 * e('maef,jibf->ijeabm', eris[o, v, v, v], t2) - e('mafe,jibf->ijeabm', eris[o, v, v, v], t2)
+    X = X - 2.0 * e('mnei,njab->ijeabm', eris[o, o, v, o], t2) + e('nmei,njab->ijeabm', eris[o, o, v, o], t2)
+    X = X + 0.5 * e('nmfe,nijfab->ijeabm', eris[o, o, v, v], t3p) - 0.25 * e('mnfe,nijfab->ijeabm', eris[o, o, v, v], t3p)
+    W["W_oovvvo"] = X + X.permute(1, 0, 2, 4, 3, 5)
+    X = e('mafe,jibf->iejabm', eris[o, v, v, v], t2) - e('mnie,njab->iejabm', eris[o, o, o, v], t2)
+    W["W_ovovvo"] = X - 0.5 * e('nmef,injfab->iejabm', eris[o, o, v, v], t3)
+    W["W_ovovvo_s"] = W["W_ovovvo"] + W["W_ovovvo"].permute(2, 1, 0, 4, 3, 5)
+    X = e('mnek,ijae->kjinma', eris[o, o, v, o], t2) + 0.5 * e('mnef,ijkaef->kjinma', eris[o, o, v, v], t3)
+    W["W_ooooov"] = X + X.permute(1, 0, 2, 4, 3, 5)
+    # W_oooovv / W_oovvvv: the T4 sums over every ordering (P4_201 applied per ordering)
+    T4s = unpack_all_orderings(t4, nocc)
+    spin4(T4s)
+    Woo = 0.5 * e('mief,ijklfabe->jklmab', eris[o, o, v, v], T4s)
+    Word = -0.5 * e('jief,ijklfabc->klabce', eris[o, o, v, v], T4s)
+    del T4s
+    Woo = Woo + e('amef,ijkebf->ijkmab', eris[v, o, v, v], t3)
+    c_t2 = 2.0 * t2 - t2.permute(0, 1, 3, 2)
+    tmp = (eris[o, v, v, o] + e('nmfe,nifa->maei', eris[o, o, v, v], c_t2)
+           - 0.5 * e('mnfe,nifa->maei', eris[o, o, v, v], c_t2) - 0.5 * e('nmef,infa->maei', eris[o, o, v, v], t2))
+    Woo = Woo + e('maei,jkbe->ijkmab', tmp, t2) + e('make,jibe->ijkmab', W_ovov, t2)
+    Woo = Woo - 0.5 * e('mnki,njab->ijkmab', W_oooo, t2)
+    W["W_oooovv"] = Woo + Woo.permute(1, 0, 2, 3, 5, 4)
+    # pair (x <= y): T4 part of orderings (x, y) plus (y, x) with b, c swapped, then the replicated terms
+    Wp = Word + Word.permute(1, 0, 2, 4, 3, 5)
+    Wp = Wp + 0.5 * e('abef,xyfc->xyabce', W_vvvv, t2) + 0.5 * e('acef,yxfb->xyabce', W_vvvv, t2)
+    lo = torch.tensor([min(x, y) for x in range(nocc) for y in range(nocc)], device=t2.device)
+    hi = torch.tensor([max(x, y) for x in range(nocc) for y in range(nocc)], device=t2.device)
+    W["W_oovvvv"] = Wp[lo, hi].view(Wp.shape)
+    return W
+
+
+def compute_r4_tri_(r4, eris, F_vv, W_vvvo, W_vooo, W_vvvv, W_oooo, W_ovov, t2, t3, t4, nocc, precision="fp64",
+                    spin3=None, spin4=None):
+    """r4[stored blocks] = compute_r4_tri without its OO batch (distr_cc/rccsdtq.py:834-1058).
+
+    eris: t1-dressed ERIs [nmo]^4 (the reference's imds.t1_eris); t2 [i,j,a,b]; t3 full
+    [i,j,k,a,b,c]; t4 and r4 [nstored, nvir^4] in stored_quadruples order.  spin3 / spin4
+    apply P3_201 / P4_201 in place to [n, nvir^3] / [n, nvir^4] blocks (default: this
+    library's kernels).  precision "bf16x3"/"tf32x3" runs the full-space strings and the
+    W_vvvv.t4 strings as split GEMMs; the builders stay FP64."""
+    from . import _c_rccsdt, _c_rccsdt_q
+    kind = None if precision == "fp64" else contract.KIND[precision]
+    nv = t2.shape[2]
+    if spin3 is None:
+        spin3 = lambda A: _c_rccsdt.t3_spin_summation_inplace_(A, A.numel() // nv ** 3, nv, "P3_201", 1.0, 0.0)  # noqa: E731
+    if spin4 is None:
+        spin4 = lambda A: _c_rccsdt_q.t4_spin_summation_inplace_(A, A.numel() // nv ** 4, nv, "P4_201", 1.0, 0.0)  # noqa: E731
+    t3 = t3.contiguous()
+    t3p = t3.clone()
+    spin3(t3p)
+    W = build_intermediates(eris, W_oooo, W_ovov, W_vvvv, t2, t3, t3p, t4, nocc, spin4)
+    W["W_vvvo"], W["W_vooo"] = W_vvvo, W_vooo
+    T = {"t3": t3, "t3_m": t3, "t3_mn": t3, "t3p_m": t3p, "t3s_m": t3 + t3.permute(0, 1, 2, 4, 5, 3),
+         "t2_m": t2, "t2": t2}
+    R = torch.zeros((nocc,) * 4 + (nv,) * 4, dtype=t3.dtype, device=t3.device)
+    for sub, wn, ws, tn, ts, al in _R4_STRINGS:
+        sw, st = sub.split(",")
+        subs = _slots(wn, ws, sw) + "," + _slots(tn, ts, st) + "->ijklabcd"
+        _einsum(kind, subs, W[wn], T[tn], R, al)
+    quads = stored_quadruples(nocc)
+    idx = torch.tensor([((i * nocc + j) * nocc + k) * nocc + l for i, j, k, l in quads], device=t3.device)
+    r4.copy_(R.view(nocc ** 4, -1)[idx].view(r4.shape))
+    del R
+    return dense_vvvv_fvv_(r4, t4, W_vvvv, F_vv, precision)

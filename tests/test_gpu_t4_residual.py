@@ -1,6 +1,8 @@
-"""Dense T4-residual strings (F_vv.t4, W_vvvv.t4; distr_cc/rccsdtq.py:1039-1055)
-on the GPU against the oracle's per-block einsums.  FP64: 1e-12 relative;
-split paths: 1e-4 of the largest |r4| change."""
+"""T4 residual on the GPU against the oracle's per-block einsums: the dense
+F_vv.t4 / W_vvvv.t4 strings (distr_cc/rccsdtq.py:1039-1055) and the whole of
+compute_r4_tri without its OO batch (:700-1058, W builders included), up to
+the N2 6-31G shape (nocc=7, nvir=11, 161 stored blocks).  FP64: 1e-11
+relative; split paths: 1e-4 of the largest |r4|."""
 import numpy as np
 import pytest
 
@@ -27,3 +29,23 @@ def test_dense_t4(precision, nblk, nv):
     got = r.cpu().numpy()
     tol = 1e-12 if precision == "fp64" else 1e-4
     assert np.abs(got - want).max() <= tol * np.abs(want - r0).max()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "bf16x3"])
+@pytest.mark.parametrize("no,nv", [(4, 5), (7, 11)])
+def test_compute_r4_tri(oracle, precision, no, nv):
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from dcc import t4_residual
+    from oracle import t4_ref
+    from test_t4_residual_algebra import _inputs
+    d = _inputs(no, nv, 5 + no)
+    want = t4_ref.compute_r4_tri_ref(d["eris"], d["F_vv"], d["W_vvvo"], d["W_vooo"], d["W_vvvv"], d["W_oooo"],
+                                     d["W_ovov"], d["t2"], d["t3"], d["t4"], no, oracle)
+    t = {k: torch.from_numpy(np.ascontiguousarray(v)).cuda() for k, v in d.items()}
+    r4 = torch.zeros_like(t["t4"])
+    t4_residual.compute_r4_tri_(r4, t["eris"], t["F_vv"], t["W_vvvo"], t["W_vooo"], t["W_vvvv"], t["W_oooo"],
+                                t["W_ovov"], t["t2"], t["t3"], t["t4"], no, precision)
+    got = r4.cpu().numpy()
+    tol = 1e-11 if precision == "fp64" else 1e-4
+    assert np.abs(got - want).max() <= tol * np.abs(want).max()
