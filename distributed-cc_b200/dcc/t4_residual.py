@@ -213,8 +213,9 @@ def build_intermediates(eris, W_oooo, W_ovov, W_vvvv, t2, t3, t3p, t4, nocc, spi
 
 
 def compute_r4_tri_(r4, eris, F_vv, W_vvvo, W_vooo, W_vvvv, W_oooo, W_ovov, t2, t3, t4, nocc, precision="fp64",
-                    spin3=None, spin4=None):
-    """r4[stored blocks] = compute_r4_tri without its OO batch (distr_cc/rccsdtq.py:834-1058).
+                    spin3=None, spin4=None, F_oo=None, W_ovvo=None, forms=None):
+    """r4[stored blocks] = compute_r4_tri (distr_cc/rccsdtq.py:834-1060); with F_oo and W_ovvo
+    given it includes the OO batch (oo_batch_, :1062-1349), else it stops before it.
 
     eris: t1-dressed ERIs [nmo]^4 (the reference's imds.t1_eris); t2 [i,j,a,b]; t3 full
     [i,j,k,a,b,c]; t4 and r4 [nstored, nvir^4] in stored_quadruples order.  spin3 / spin4
@@ -244,4 +245,149 @@ def compute_r4_tri_(r4, eris, F_vv, W_vvvo, W_vooo, W_vvvv, W_oooo, W_ovov, t2, 
     idx = torch.tensor([((i * nocc + j) * nocc + k) * nocc + l for i, j, k, l in quads], device=t3.device)
     r4.copy_(R.view(nocc ** 4, -1)[idx].view(r4.shape))
     del R
-    return dense_vvvv_fvv_(r4, t4, W_vvvv, F_vv, precision)
+    dense_vvvv_fvv_(r4, t4, W_vvvv, F_vv, precision)
+    if F_oo is not None:
+        oo_batch_(r4, t4, F_oo, W_oooo, W_ovvo, W_ovov, nocc, forms)
+    return r4
+
+
+# ----------------------------------------------------------------------------
+# The OO batch (distr_cc/rccsdtq.py:1062-1349).
+#
+# F_oo and W_oooo: the reference's 24 prefactor slots sum, for each output
+# block, every ordering of the stored blocks that places m (and n) at output
+# positions; over the full ordered space these are the plain strings
+#   R[ijkl] -= F_oo[m,i] T[mjkl] + ... (4),   R[ijkl] += W_oooo[m,n,i,j] T[mnkl] + ... (6).
+# W_ovov / W_voov: for each output block, group g (the position whose index
+# enters W) and case c (where m sits in the stored source block), a fixed set
+# of strings on the source block, its transpose-add or one of its four
+# quadruple-symmetrized forms.  The (source, output, m) pairs of each (g, c)
+# are listed once per nocc and every string runs as one batched einsum over
+# its pairs, scattered into r4.
+# ----------------------------------------------------------------------------
+
+# (W tensor, string, alpha, source form) for group g (W at output position g) and case c;
+# forms: "T" the block, "T3" its transpose-add, "V0".."V3" its quadruple-symmetrized forms
+_OO_TABLE = {
+    0: [[("ovov", "be,aecd", -1.0, "T"), ("ovov", "ce,abed", -1.0, "T"), ("ovov", "de,abce", -1.0, "T"),
+         ("voov", "ae,ebcd", 0.5, "V3"), ("ovov", "ae,becd", -0.5, "T3")],
+        [("ovov", "be,eacd", -1.0, "T"), ("ovov", "ce,baed", -1.0, "T"), ("ovov", "de,bace", -1.0, "T"),
+         ("voov", "ae,becd", 0.5, "V2"), ("ovov", "ae,ebcd", -0.5, "T"), ("ovov", "ae,bced", -0.5, "T"),
+         ("ovov", "ae,bdce", -0.5, "T")],
+        [("ovov", "be,ecad", -1.0, "T"), ("ovov", "ce,bead", -1.0, "T"), ("ovov", "de,bcae", -1.0, "T"),
+         ("voov", "ae,bced", 0.5, "V1"), ("ovov", "ae,ecbd", -0.5, "T"), ("ovov", "ae,becd", -0.5, "T"),
+         ("ovov", "ae,bcde", -0.5, "T")],
+        [("ovov", "be,ecda", -1.0, "T"), ("ovov", "ce,beda", -1.0, "T"), ("ovov", "de,bcea", -1.0, "T"),
+         ("voov", "ae,bcde", 0.5, "V0"), ("ovov", "ae,ecdb", -0.5, "T"), ("ovov", "ae,bedc", -0.5, "T"),
+         ("ovov", "ae,bced", -0.5, "T")]],
+    1: [[("ovov", "ae,becd", -1.0, "T"), ("ovov", "ce,baed", -1.0, "T"), ("ovov", "de,bace", -1.0, "T"),
+         ("voov", "be,eacd", 0.5, "V3"), ("ovov", "be,aecd", -0.5, "T3")],
+        [("ovov", "ae,ebcd", -1.0, "T"), ("ovov", "ce,abed", -1.0, "T"), ("ovov", "de,abce", -1.0, "T"),
+         ("voov", "be,aecd", 0.5, "V2"), ("ovov", "be,eacd", -0.5, "T"), ("ovov", "be,aced", -0.5, "T"),
+         ("ovov", "be,adce", -0.5, "T")],
+        [("ovov", "ae,ecbd", -1.0, "T"), ("ovov", "ce,aebd", -1.0, "T"), ("ovov", "de,acbe", -1.0, "T"),
+         ("voov", "be,aced", 0.5, "V1"), ("ovov", "be,ecad", -0.5, "T"), ("ovov", "be,aecd", -0.5, "T"),
+         ("ovov", "be,acde", -0.5, "T")],
+        [("ovov", "ae,ecdb", -1.0, "T"), ("ovov", "ce,aedb", -1.0, "T"), ("ovov", "de,aceb", -1.0, "T"),
+         ("voov", "be,acde", 0.5, "V0"), ("ovov", "be,ecda", -0.5, "T"), ("ovov", "be,aedc", -0.5, "T"),
+         ("ovov", "be,aced", -0.5, "T")]],
+    2: [[("ovov", "ae,cebd", -1.0, "T"), ("ovov", "be,caed", -1.0, "T"), ("ovov", "de,cabe", -1.0, "T"),
+         ("voov", "ce,eabd", 0.5, "V3"), ("ovov", "ce,aebd", -0.5, "T3")],
+        [("ovov", "ae,ecbd", -1.0, "T"), ("ovov", "be,aced", -1.0, "T"), ("ovov", "de,acbe", -1.0, "T"),
+         ("voov", "ce,aebd", 0.5, "V2"), ("ovov", "ce,eabd", -0.5, "T"), ("ovov", "ce,abed", -0.5, "T"),
+         ("ovov", "ce,adbe", -0.5, "T")],
+        [("ovov", "ae,ebcd", -1.0, "T"), ("ovov", "be,aecd", -1.0, "T"), ("ovov", "de,abce", -1.0, "T"),
+         ("voov", "ce,abed", 0.5, "V1"), ("ovov", "ce,ebad", -0.5, "T"), ("ovov", "ce,aebd", -0.5, "T"),
+         ("ovov", "ce,abde", -0.5, "T")],
+        [("ovov", "ae,ebdc", -1.0, "T"), ("ovov", "be,aedc", -1.0, "T"), ("ovov", "de,abec", -1.0, "T"),
+         ("voov", "ce,abde", 0.5, "V0"), ("ovov", "ce,ebda", -0.5, "T"), ("ovov", "ce,aedb", -0.5, "T"),
+         ("ovov", "ce,abed", -0.5, "T")]],
+    3: [[("ovov", "ae,debc", -1.0, "T"), ("ovov", "be,daec", -1.0, "T"), ("ovov", "ce,dabe", -1.0, "T"),
+         ("voov", "de,eabc", 0.5, "V3"), ("ovov", "de,aebc", -0.5, "T3")],
+        [("ovov", "ae,edbc", -1.0, "T"), ("ovov", "be,adec", -1.0, "T"), ("ovov", "ce,adbe", -1.0, "T"),
+         ("voov", "de,aebc", 0.5, "V2"), ("ovov", "de,eabc", -0.5, "T"), ("ovov", "de,abec", -0.5, "T"),
+         ("ovov", "de,acbe", -0.5, "T")],
+        [("ovov", "ae,ebdc", -1.0, "T"), ("ovov", "be,aedc", -1.0, "T"), ("ovov", "ce,abde", -1.0, "T"),
+         ("voov", "de,abec", 0.5, "V1"), ("ovov", "de,ebac", -0.5, "T"), ("ovov", "de,aebc", -0.5, "T"),
+         ("ovov", "de,abce", -0.5, "T")],
+        [("ovov", "ae,ebcd", -1.0, "T"), ("ovov", "be,aecd", -1.0, "T"), ("ovov", "ce,abed", -1.0, "T"),
+         ("voov", "de,abce", 0.5, "V0"), ("ovov", "de,ebca", -0.5, "T"), ("ovov", "de,aecb", -0.5, "T"),
+         ("ovov", "de,abec", -0.5, "T")]],
+}
+
+_OO_PAIRS = {}
+
+
+def oo_pairs(nocc):
+    """{(g, c): (source blocks, output blocks, m, W index)} of the OO batch: output block t
+    with t[g] = x and the other three positions equal to the source block s without its
+    position c (m = s[c]; for c > 0 the source's s[c-1] != s[c])."""
+    if nocc in _OO_PAIRS:
+        return _OO_PAIRS[nocc]
+    quads = stored_quadruples(nocc)
+    index = {q: n for n, q in enumerate(quads)}
+    out = {}
+    for si, s in enumerate(quads):
+        for c in range(4):
+            if c > 0 and s[c - 1] == s[c]:
+                continue
+            rest = s[:c] + s[c + 1:]
+            for g in range(4):
+                for x in range(nocc):
+                    t = rest[:g] + (x,) + rest[g:]
+                    ti = index.get(t)
+                    if ti is None:
+                        continue
+                    lst = out.setdefault((g, c), ([], [], [], []))
+                    lst[0].append(si)
+                    lst[1].append(ti)
+                    lst[2].append(s[c])
+                    lst[3].append(x)
+    _OO_PAIRS[nocc] = out
+    return out
+
+
+def oo_batch_(r4, t4, F_oo, W_oooo, W_ovvo, W_ovov, nocc, forms=None):
+    """r4 += the OO batch of compute_r4_tri (distr_cc/rccsdtq.py:1062-1349), FP64.
+
+    forms(t4) -> (T3, [V0, V1, V2, V3]) per stored block (default: this library's
+    t4_transpose_add and quadruple-sym kernels, one block at a time)."""
+    e = torch.einsum
+    nv = t4.shape[1]
+    dev = t4.device
+    if forms is None:
+        from . import _c_rccsdtq
+
+        def forms(t):
+            T3 = torch.empty_like(t)
+            V = [torch.empty_like(t) for _ in range(4)]
+            for q in range(t.shape[0]):
+                _c_rccsdtq.t4_transpose_add_(t[q], T3[q], nv)
+                _c_rccsdtq.t4_spin_summation_quadruple_sym_(t[q], V[0][q], V[1][q], V[2][q], V[3][q], nv)
+            return T3, V
+    # F_oo and W_oooo over the full ordered space
+    T = unpack_all_orderings(t4, nocc)
+    R = torch.zeros_like(T)
+    R -= (e('mi,mjklabcd->ijklabcd', F_oo, T) + e('mj,imklabcd->ijklabcd', F_oo, T)
+          + e('mk,ijmlabcd->ijklabcd', F_oo, T) + e('ml,ijkmabcd->ijklabcd', F_oo, T))
+    R += (e('mnij,mnklabcd->ijklabcd', W_oooo, T) + e('mnik,mjnlabcd->ijklabcd', W_oooo, T)
+          + e('mnil,mjknabcd->ijklabcd', W_oooo, T) + e('mnjk,imnlabcd->ijklabcd', W_oooo, T)
+          + e('mnjl,imknabcd->ijklabcd', W_oooo, T) + e('mnkl,ijmnabcd->ijklabcd', W_oooo, T))
+    del T
+    quads = stored_quadruples(nocc)
+    idx = torch.tensor([((i * nocc + j) * nocc + k) * nocc + l for i, j, k, l in quads], device=dev)
+    r4 += R.view(nocc ** 4, -1)[idx].view(r4.shape)
+    del R
+    # W_ovov / W_voov strings, batched over the (source, output) pairs of each group and case
+    T3, V = forms(t4)
+    src = {"T": t4, "T3": T3, "V0": V[0], "V1": V[1], "V2": V[2], "V3": V[3]}
+    W_voov = W_ovvo.permute(1, 0, 3, 2).contiguous()
+    for (g, c), (si, ti, m, x) in oo_pairs(nocc).items():
+        si, ti, m, x = (torch.tensor(v, device=dev) for v in (si, ti, m, x))
+        Wo = W_ovov[m, :, x, :]   # [P, a, e] = W_ovov[m, :, x, :]
+        Wv = W_voov[:, m, x, :].permute(1, 0, 2)  # [P, a, e] = W_voov[:, m, x, :]
+        for wn, s, al, form in _OO_TABLE[g][c]:
+            ws, ts = s.split(",")
+            upd = e("p" + ws + ",p" + ts + "->pabcd", Wo if wn == "ovov" else Wv, src[form][si])
+            r4.index_add_(0, ti, upd, alpha=al)
+    return r4

@@ -128,8 +128,10 @@ def build_w_oooovv_oovvvv(eris, t2, t3, t4, quads, W_oooo, W_ovov, W_vvvv, nocc,
     return W_oooovv, W_oovvvv
 
 
-def compute_r4_tri_ref(eris, F_vv, W_vvvo, W_vooo, W_vvvv, W_oooo, W_ovov, t2, t3, t4, nocc, orc):
-    """r4 of every stored block without the OO batch (distr_cc/rccsdtq.py:834-1058).
+def compute_r4_tri_ref(eris, F_vv, W_vvvo, W_vooo, W_vvvv, W_oooo, W_ovov, t2, t3, t4, nocc, orc, F_oo=None,
+                       W_ovvo=None):
+    """r4 of every stored block (distr_cc/rccsdtq.py:834-1060), with the OO batch when F_oo and
+    W_ovvo are given (oo_batch_ref).
     eris: t1-dressed ERIs [nmo]^4 (physicist slices as the reference cuts them);
     t2 [i,j,a,b]; t3 full [i,j,k,a,b,c]; t4 [nstored, nvir^4]."""
     e = np.einsum
@@ -228,7 +230,10 @@ def compute_r4_tri_ref(eris, F_vv, W_vvvo, W_vooo, W_vvvv, W_oooo, W_ovov, t2, t
         r += e("bcde,ea->abcd", P(k, l), t2[j, i])
         r += e("cbde,ea->abcd", P(j, l), t2[k, i])
         r += e("dbce,ea->abcd", P(j, k), t2[l, i])
-    return dense_vvvv_fvv_ref(r4, t4, W_vvvv, F_vv)
+    r4 = dense_vvvv_fvv_ref(r4, t4, W_vvvv, F_vv)
+    if F_oo is not None:
+        r4 = oo_batch_ref(r4, t4, F_oo, W_oooo, W_ovvo, W_ovov, nocc, orc)
+    return r4
 
 
 # (string, W_ovovvo occupied slots, t3 occupied slots) of distr_cc/rccsdtq.py:913-938
@@ -246,3 +251,183 @@ _OVOV_T3 = [
     ("edbm,mcea->abcd", ("k", "j"), ("l", "i")), ("ecbm,mdea->abcd", ("l", "j"), ("k", "i")),
     ("ebdm,mcea->abcd", ("k", "l"), ("j", "i")), ("ebcm,mdea->abcd", ("l", "k"), ("j", "i")),
 ]
+
+
+# ----------------------------------------------------------------------------
+# The OO batch of the T4 residual (distr_cc/rccsdtq.py:1062-1349), literal:
+# the F_oo / W_oooo prefactor slots (:140-237) and, per stored source block and
+# stored output block, the W_ovov / W_voov strings of the four placements of m.
+# ----------------------------------------------------------------------------
+
+def _canon_perm(v):
+    order = sorted(range(4), key=lambda p: (v[p], p))
+    return tuple(v[p] for p in order), tuple(order.index(p) for p in range(4))
+
+
+def _foo_terms(can, target):
+    """(p, m, output axes of the canonical block) of distr_cc/rccsdtq.py:198-227."""
+    import itertools
+    out = []
+    for p in range(4):
+        comp = tuple(x for x in range(4) if x != p)
+        tail = tuple(target[x] for x in comp)
+        to_out = (p,) + comp
+        tr = tuple(to_out.index(x) for x in range(4))
+        seen = set()
+        for req in itertools.permutations(can):
+            if req in seen:
+                continue
+            seen.add(req)
+            if req[1:] != tail:
+                continue
+            c, perm = _canon_perm(req)
+            if c != can:
+                continue
+            out.append((p, req[0], ''.join("abcd"[perm[x]] for x in tr)))
+    return out
+
+
+def _woooo_terms(can, target):
+    """(p, q, m, n, output axes of the canonical block) of distr_cc/rccsdtq.py:166-196."""
+    import itertools
+    out = []
+    for p, q in ((0, 1), (0, 2), (0, 3), (1, 2), (1, 3), (2, 3)):
+        comp = tuple(x for x in range(4) if x not in (p, q))
+        head = (target[comp[0]], target[comp[1]])
+        to_out = comp + (p, q)
+        tr = tuple(to_out.index(x) for x in range(4))
+        seen = set()
+        for req in itertools.permutations(can):
+            if req in seen:
+                continue
+            seen.add(req)
+            if req[:2] != head:
+                continue
+            c, perm = _canon_perm(req)
+            if c != can:
+                continue
+            out.append((p, q, req[2], req[3], ''.join("abcd"[perm[x]] for x in tr)))
+    return out
+
+
+def oo_batch_ref(r4, t4, F_oo, W_oooo, W_ovvo, W_ovov, nocc, orc):
+    """r4 += the OO batch for every stored output block (one batch of all blocks)."""
+    import itertools
+    e = np.einsum
+    nvir = t4.shape[1]
+    quads = stored_quadruples(nocc)
+    W_voov = np.ascontiguousarray(W_ovvo.transpose(1, 0, 3, 2))
+    slots = {''.join(p): s for s, p in enumerate(itertools.permutations("abcd"))}
+    pfs = np.zeros((24, len(quads), len(quads)))
+    for s_idx, can in enumerate(quads):
+        for o_idx, tgt in enumerate(quads):
+            for p, m, ax in _foo_terms(can, tgt):
+                pfs[slots[ax], s_idx, o_idx] -= F_oo[m, tgt[p]]
+            for p, q, m, n, ax in _woooo_terms(can, tgt):
+                pfs[slots[ax], s_idx, o_idx] += W_oooo[m, n, tgt[p], tgt[q]]
+    for ax, s in slots.items():
+        r4 += e("pq,pabcd->q" + ax, pfs[s], t4)
+    W = W_ovov
+    for s_idx, (o0, o1, o2, o3) in enumerate(quads):
+        T = t4[s_idx]
+        T3 = orc.t4_transpose_add(np.ascontiguousarray(T), nvir)
+        V0, V1, V2, V3 = orc.t4_quadruple_sym(np.ascontiguousarray(T), nvir)
+        for o_idx, (i, j, k, l) in enumerate(quads):
+            r = r4[o_idx]
+            # j k l (W at i)
+            if j == o1 and k == o2 and l == o3:
+                r -= e("be,aecd->abcd", W[o0, :, i, :], T) + e("ce,abed->abcd", W[o0, :, i, :], T)
+                r -= e("de,abce->abcd", W[o0, :, i, :], T)
+                r += 0.5 * e("ae,ebcd->abcd", W_voov[:, o0, i, :], V3)
+                r -= 0.5 * e("ae,becd->abcd", W[o0, :, i, :], T3)
+            if o0 != o1 and j == o0 and k == o2 and l == o3:
+                r -= e("be,eacd->abcd", W[o1, :, i, :], T) + e("ce,baed->abcd", W[o1, :, i, :], T)
+                r -= e("de,bace->abcd", W[o1, :, i, :], T)
+                r += 0.5 * e("ae,becd->abcd", W_voov[:, o1, i, :], V2)
+                r -= 0.5 * (e("ae,ebcd->abcd", W[o1, :, i, :], T) + e("ae,bced->abcd", W[o1, :, i, :], T)
+                            + e("ae,bdce->abcd", W[o1, :, i, :], T))
+            if o1 != o2 and j == o0 and k == o1 and l == o3:
+                r -= e("be,ecad->abcd", W[o2, :, i, :], T) + e("ce,bead->abcd", W[o2, :, i, :], T)
+                r -= e("de,bcae->abcd", W[o2, :, i, :], T)
+                r += 0.5 * e("ae,bced->abcd", W_voov[:, o2, i, :], V1)
+                r -= 0.5 * (e("ae,ecbd->abcd", W[o2, :, i, :], T) + e("ae,becd->abcd", W[o2, :, i, :], T)
+                            + e("ae,bcde->abcd", W[o2, :, i, :], T))
+            if o2 != o3 and j == o0 and k == o1 and l == o2:
+                r -= e("be,ecda->abcd", W[o3, :, i, :], T) + e("ce,beda->abcd", W[o3, :, i, :], T)
+                r -= e("de,bcea->abcd", W[o3, :, i, :], T)
+                r += 0.5 * e("ae,bcde->abcd", W_voov[:, o3, i, :], V0)
+                r -= 0.5 * (e("ae,ecdb->abcd", W[o3, :, i, :], T) + e("ae,bedc->abcd", W[o3, :, i, :], T)
+                            + e("ae,bced->abcd", W[o3, :, i, :], T))
+            # i k l (W at j)
+            if i == o1 and k == o2 and l == o3:
+                r -= e("ae,becd->abcd", W[o0, :, j, :], T) + e("ce,baed->abcd", W[o0, :, j, :], T)
+                r -= e("de,bace->abcd", W[o0, :, j, :], T)
+                r += 0.5 * e("be,eacd->abcd", W_voov[:, o0, j, :], V3)
+                r -= 0.5 * e("be,aecd->abcd", W[o0, :, j, :], T3)
+            if o0 != o1 and i == o0 and k == o2 and l == o3:
+                r -= e("ae,ebcd->abcd", W[o1, :, j, :], T) + e("ce,abed->abcd", W[o1, :, j, :], T)
+                r -= e("de,abce->abcd", W[o1, :, j, :], T)
+                r += 0.5 * e("be,aecd->abcd", W_voov[:, o1, j, :], V2)
+                r -= 0.5 * (e("be,eacd->abcd", W[o1, :, j, :], T) + e("be,aced->abcd", W[o1, :, j, :], T)
+                            + e("be,adce->abcd", W[o1, :, j, :], T))
+            if o1 != o2 and i == o0 and k == o1 and l == o3:
+                r -= e("ae,ecbd->abcd", W[o2, :, j, :], T) + e("ce,aebd->abcd", W[o2, :, j, :], T)
+                r -= e("de,acbe->abcd", W[o2, :, j, :], T)
+                r += 0.5 * e("be,aced->abcd", W_voov[:, o2, j, :], V1)
+                r -= 0.5 * (e("be,ecad->abcd", W[o2, :, j, :], T) + e("be,aecd->abcd", W[o2, :, j, :], T)
+                            + e("be,acde->abcd", W[o2, :, j, :], T))
+            if o2 != o3 and i == o0 and k == o1 and l == o2:
+                r -= e("ae,ecdb->abcd", W[o3, :, j, :], T) + e("ce,aedb->abcd", W[o3, :, j, :], T)
+                r -= e("de,aceb->abcd", W[o3, :, j, :], T)
+                r += 0.5 * e("be,acde->abcd", W_voov[:, o3, j, :], V0)
+                r -= 0.5 * (e("be,ecda->abcd", W[o3, :, j, :], T) + e("be,aedc->abcd", W[o3, :, j, :], T)
+                            + e("be,aced->abcd", W[o3, :, j, :], T))
+            # i j l (W at k)
+            if i == o1 and j == o2 and l == o3:
+                r -= e("ae,cebd->abcd", W[o0, :, k, :], T) + e("be,caed->abcd", W[o0, :, k, :], T)
+                r -= e("de,cabe->abcd", W[o0, :, k, :], T)
+                r += 0.5 * e("ce,eabd->abcd", W_voov[:, o0, k, :], V3)
+                r -= 0.5 * e("ce,aebd->abcd", W[o0, :, k, :], T3)
+            if o0 != o1 and i == o0 and j == o2 and l == o3:
+                r -= e("ae,ecbd->abcd", W[o1, :, k, :], T) + e("be,aced->abcd", W[o1, :, k, :], T)
+                r -= e("de,acbe->abcd", W[o1, :, k, :], T)
+                r += 0.5 * e("ce,aebd->abcd", W_voov[:, o1, k, :], V2)
+                r -= 0.5 * (e("ce,eabd->abcd", W[o1, :, k, :], T) + e("ce,abed->abcd", W[o1, :, k, :], T)
+                            + e("ce,adbe->abcd", W[o1, :, k, :], T))
+            if o1 != o2 and i == o0 and j == o1 and l == o3:
+                r -= e("ae,ebcd->abcd", W[o2, :, k, :], T) + e("be,aecd->abcd", W[o2, :, k, :], T)
+                r -= e("de,abce->abcd", W[o2, :, k, :], T)
+                r += 0.5 * e("ce,abed->abcd", W_voov[:, o2, k, :], V1)
+                r -= 0.5 * (e("ce,ebad->abcd", W[o2, :, k, :], T) + e("ce,aebd->abcd", W[o2, :, k, :], T)
+                            + e("ce,abde->abcd", W[o2, :, k, :], T))
+            if o2 != o3 and i == o0 and j == o1 and l == o2:
+                r -= e("ae,ebdc->abcd", W[o3, :, k, :], T) + e("be,aedc->abcd", W[o3, :, k, :], T)
+                r -= e("de,abec->abcd", W[o3, :, k, :], T)
+                r += 0.5 * e("ce,abde->abcd", W_voov[:, o3, k, :], V0)
+                r -= 0.5 * (e("ce,ebda->abcd", W[o3, :, k, :], T) + e("ce,aedb->abcd", W[o3, :, k, :], T)
+                            + e("ce,abed->abcd", W[o3, :, k, :], T))
+            # i j k (W at l)
+            if i == o1 and j == o2 and k == o3:
+                r -= e("ae,debc->abcd", W[o0, :, l, :], T) + e("be,daec->abcd", W[o0, :, l, :], T)
+                r -= e("ce,dabe->abcd", W[o0, :, l, :], T)
+                r += 0.5 * e("de,eabc->abcd", W_voov[:, o0, l, :], V3)
+                r -= 0.5 * e("de,aebc->abcd", W[o0, :, l, :], T3)
+            if o0 != o1 and i == o0 and j == o2 and k == o3:
+                r -= e("ae,edbc->abcd", W[o1, :, l, :], T) + e("be,adec->abcd", W[o1, :, l, :], T)
+                r -= e("ce,adbe->abcd", W[o1, :, l, :], T)
+                r += 0.5 * e("de,aebc->abcd", W_voov[:, o1, l, :], V2)
+                r -= 0.5 * (e("de,eabc->abcd", W[o1, :, l, :], T) + e("de,abec->abcd", W[o1, :, l, :], T)
+                            + e("de,acbe->abcd", W[o1, :, l, :], T))
+            if o1 != o2 and i == o0 and j == o1 and k == o3:
+                r -= e("ae,ebdc->abcd", W[o2, :, l, :], T) + e("be,aedc->abcd", W[o2, :, l, :], T)
+                r -= e("ce,abde->abcd", W[o2, :, l, :], T)
+                r += 0.5 * e("de,abec->abcd", W_voov[:, o2, l, :], V1)
+                r -= 0.5 * (e("de,ebac->abcd", W[o2, :, l, :], T) + e("de,aebc->abcd", W[o2, :, l, :], T)
+                            + e("de,abce->abcd", W[o2, :, l, :], T))
+            if o2 != o3 and i == o0 and j == o1 and k == o2:
+                r -= e("ae,ebcd->abcd", W[o3, :, l, :], T) + e("be,aecd->abcd", W[o3, :, l, :], T)
+                r -= e("ce,abed->abcd", W[o3, :, l, :], T)
+                r += 0.5 * e("de,abce->abcd", W_voov[:, o3, l, :], V0)
+                r -= 0.5 * (e("de,ebca->abcd", W[o3, :, l, :], T) + e("de,aecb->abcd", W[o3, :, l, :], T)
+                            + e("de,abec->abcd", W[o3, :, l, :], T))
+    return r4

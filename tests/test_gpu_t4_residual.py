@@ -1,6 +1,6 @@
 """T4 residual on the GPU against the oracle's per-block einsums: the dense
 F_vv.t4 / W_vvvv.t4 strings (distr_cc/rccsdtq.py:1039-1055) and the whole of
-compute_r4_tri without its OO batch (:700-1058, W builders included), up to
+compute_r4_tri with its OO batch (:700-1349, W builders included), up to
 the N2 6-31G shape (nocc=7, nvir=11, 161 stored blocks).  FP64: 1e-11
 relative; split paths: 1e-4 of the largest |r4|."""
 import numpy as np
@@ -31,21 +31,38 @@ def test_dense_t4(precision, nblk, nv):
     assert np.abs(got - want).max() <= tol * np.abs(want - r0).max()
 
 
+_REF = {}
+
+
+def _case(oracle, no, nv):
+    """Inputs and the oracle's r4 (computed once per shape)."""
+    if (no, nv) not in _REF:
+        from oracle import t4_ref
+        from test_t4_residual_algebra import _inputs, stab_symmetric
+        d = _inputs(no, nv, 5 + no)
+        rng = np.random.default_rng(no)
+        d["t4"] = stab_symmetric(d["t4"], t4_ref.stored_quadruples(no))
+        d["F_oo"] = rng.standard_normal((no, no))
+        d["W_ovvo"] = rng.standard_normal((no, nv, nv, no)) * 0.1
+        want = t4_ref.compute_r4_tri_ref(d["eris"], d["F_vv"], d["W_vvvo"], d["W_vooo"], d["W_vvvv"], d["W_oooo"],
+                                         d["W_ovov"], d["t2"], d["t3"], d["t4"], no, oracle, d["F_oo"],
+                                         d["W_ovvo"])
+        _REF[(no, nv)] = (d, want)
+    return _REF[(no, nv)]
+
+
 @pytest.mark.parametrize("precision", ["fp64", "bf16x3"])
 @pytest.mark.parametrize("no,nv", [(4, 5), (7, 11)])
 def test_compute_r4_tri(oracle, precision, no, nv):
     if not torch.cuda.is_available():
         pytest.skip("no CUDA device")
     from dcc import t4_residual
-    from oracle import t4_ref
-    from test_t4_residual_algebra import _inputs
-    d = _inputs(no, nv, 5 + no)
-    want = t4_ref.compute_r4_tri_ref(d["eris"], d["F_vv"], d["W_vvvo"], d["W_vooo"], d["W_vvvv"], d["W_oooo"],
-                                     d["W_ovov"], d["t2"], d["t3"], d["t4"], no, oracle)
+    d, want = _case(oracle, no, nv)
     t = {k: torch.from_numpy(np.ascontiguousarray(v)).cuda() for k, v in d.items()}
     r4 = torch.zeros_like(t["t4"])
     t4_residual.compute_r4_tri_(r4, t["eris"], t["F_vv"], t["W_vvvo"], t["W_vooo"], t["W_vvvv"], t["W_oooo"],
-                                t["W_ovov"], t["t2"], t["t3"], t["t4"], no, precision)
+                                t["W_ovov"], t["t2"], t["t3"], t["t4"], no, precision, F_oo=t["F_oo"],
+                                W_ovvo=t["W_ovvo"])
     got = r4.cpu().numpy()
     tol = 1e-11 if precision == "fp64" else 1e-4
     assert np.abs(got - want).max() <= tol * np.abs(want).max()

@@ -60,3 +60,39 @@ def test_unpack_all_orderings_matches_oracle(oracle):
     for o in itertools.product(range(no), repeat=4):
         want, rc = oracle.unpack_t4(t4, f2l, *o, no, nv)
         assert np.array_equal(full[o], want), o
+
+
+def stab_symmetric(t4, quads):
+    """Each stored block averaged over the virtual-axis permutations that fix its occupied
+    tuple (i = j, k = l, ...): the symmetry every T4 block has, which the reference's
+    prefactor slots rely on when they read a block in another ordering."""
+    import itertools
+    out = np.empty_like(t4)
+    for q, quad in enumerate(quads):
+        ps = [p for p in itertools.permutations(range(4)) if tuple(quad[x] for x in p) == quad]
+        out[q] = sum(t4[q].transpose(p) for p in ps) / len(ps)
+    return out
+
+
+@pytest.mark.parametrize("no,nv", [(4, 3), (5, 3)])
+def test_oo_batch_matches_literal_blocks(oracle, no, nv):
+    rng = np.random.default_rng(no)
+    n4 = len(t4_ref.stored_quadruples(no))
+    t4 = stab_symmetric(rng.standard_normal((n4,) + (nv,) * 4) * 0.01, t4_ref.stored_quadruples(no))
+    F_oo = rng.standard_normal((no, no))
+    W_oooo = rng.standard_normal((no,) * 4) * 0.1
+    W_ovvo = rng.standard_normal((no, nv, nv, no)) * 0.1
+    W_ovov = rng.standard_normal((no, nv, no, nv)) * 0.1
+    r0 = rng.standard_normal(t4.shape) * 0.01
+    want = t4_ref.oo_batch_ref(r0.copy(), t4, F_oo, W_oooo, W_ovvo, W_ovov, no, oracle)
+
+    def forms(t):
+        a = t.numpy()
+        T3 = np.stack([oracle.t4_transpose_add(np.ascontiguousarray(b), nv) for b in a])
+        Vs = [oracle.t4_quadruple_sym(np.ascontiguousarray(b), nv) for b in a]
+        return torch.from_numpy(T3), [torch.from_numpy(np.stack([v[x] for v in Vs])) for x in range(4)]
+
+    tt = lambda a: torch.from_numpy(np.ascontiguousarray(a))  # noqa: E731
+    r4 = tt(r0.copy())
+    tr.oo_batch_(r4, tt(t4), tt(F_oo), tt(W_oooo), tt(W_ovvo), tt(W_ovov), no, forms=forms)
+    np.testing.assert_allclose(r4.numpy(), want, rtol=1e-12, atol=1e-13 * np.abs(want - r0).max())
