@@ -1,12 +1,15 @@
 """The "cuda" einsum backend: the drop-in that routes the reference driver's
-triples hot path onto this library (distr_cc/rccsdt.py, distr_cc/rccsdt_q.py).
+triples / quadruples hot path onto this library (distr_cc/rccsdt.py,
+distr_cc/rccsdt_q.py, distr_cc/rccsdtq.py).
 
-`install(rccsdt_module, rccsdt_q_module)` wraps the reference's hot functions
+`install(rccsdt_module, rccsdt_q_module, rccsdtq_module)` wraps the reference's
+hot functions
 
     r1r2_add_t3_tri_(mycc, imds, r1, r2, t3)          distr_cc/rccsdt.py:253
     intermediates_t3_add_t3_tri(mycc, imds, t3)        distr_cc/rccsdt.py:323
     compute_r3_tri(mycc, imds, t2, t3)                 distr_cc/rccsdt.py:368
     rccsdt_q.kernel(mycc, eris, tamps, blksize, comm)  distr_cc/rccsdt_q.py:227
+    compute_r4_tri(mycc, imds, t2, t3, t4)             distr_cc/rccsdtq.py:834
 
 so that, when `mycc.einsum_backend == "cuda"` (set through the reference's
 own RCCSDT.set_einsum_backend, distr_cc/rccsdt.py:1255), they run on the GPU
@@ -176,11 +179,41 @@ def q_kernel(mycc, eris=None, tamps=None, blksize=4, comm=None, job_idx=0, n_job
                              nocc, nvir, blksize, precision_of(mycc))
 
 
+# imds fields compute_r4_tri releases on return (distr_cc/rccsdtq.py:899-1349)
+_R4_RELEASED = ("W_vvvo", "W_vooo", "W_oovvvo", "W_ovovvo", "W_ooooov", "W_oooovv", "W_oovvvv", "t1_eris", "F_vv",
+                "W_vvvv", "F_oo", "W_oooo", "W_ovvo", "W_ovov")
+
+
+def compute_r4_tri(mycc, imds, t2, t3, t4):
+    """r4_local of distr_cc/rccsdtq.py:834 (with its OO batch, :1062) on the GPU, one rank:
+    t2 [i,j,a,b], t3 the full [i,j,k,a,b,c], t4 = (dt4, t4_local) with every stored block local."""
+    from . import t4_residual
+    require_single_rank(mycc)
+    dev = getattr(mycc, "dcc_device", "cuda")
+    nocc = mycc.nocc
+    dt4, t4_local = t4
+    quads = t4_residual.stored_quadruples(nocc)
+    local = [tuple(int(x) for x in q[:4]) for q in dt4.iter_local_ijkl()] if hasattr(dt4, "iter_local_ijkl") \
+        else quads
+    if local != quads or len(t4_local) != len(quads):
+        raise RuntimeError('einsum backend "cuda" needs every stored T4 block local, in stored order')
+    d = lambda a: _dev(a, dev)  # noqa: E731
+    r4 = torch.zeros((len(quads),) + tuple(t4_local.shape[1:]), dtype=f64, device=dev)
+    t4_residual.compute_r4_tri_(r4, d(imds.t1_eris), d(imds.F_vv), d(imds.W_vvvo), d(imds.W_vooo), d(imds.W_vvvv),
+                                d(imds.W_oooo), d(imds.W_ovov), d(t2), d(t3), d(t4_local), nocc,
+                                precision_of(mycc), F_oo=d(imds.F_oo), W_ovvo=d(imds.W_ovvo))
+    out = r4.cpu().numpy()
+    for name in _R4_RELEASED:
+        if hasattr(imds, name):
+            setattr(imds, name, None)
+    return out
+
+
 _ROUTES = {"r1r2_add_t3_tri_": r1r2_add_t3_tri_, "intermediates_t3_add_t3_tri": intermediates_t3_add_t3_tri,
            "compute_r3_tri": compute_r3_tri}
 
 
-def install(rccsdt_module, rccsdt_q_module=None):
+def install(rccsdt_module, rccsdt_q_module=None, rccsdtq_module=None):
     """Route the reference's hot functions to the GPU when mycc.einsum_backend == "cuda".
     Idempotent; returns the names it wrapped."""
     wrapped = []
@@ -206,4 +239,14 @@ def install(rccsdt_module, rccsdt_q_module=None):
             qwrap.__name__ = "kernel"
             rccsdt_q_module.kernel = qwrap
             wrapped.append("rccsdt_q.kernel")
+    if rccsdtq_module is not None:
+        orig = getattr(rccsdtq_module, "compute_r4_tri", None)
+        if orig is not None and not getattr(orig, "_dcc_wrapped", False):
+            def r4wrap(mycc, *args, _orig=orig, **kw):
+                return compute_r4_tri(mycc, *args, **kw) if uses_cuda(mycc) else _orig(mycc, *args, **kw)
+            r4wrap._dcc_wrapped = True
+            r4wrap.__name__ = "compute_r4_tri"
+            r4wrap.__doc__ = orig.__doc__
+            rccsdtq_module.compute_r4_tri = r4wrap
+            wrapped.append("rccsdtq.compute_r4_tri")
     return wrapped

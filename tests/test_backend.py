@@ -58,3 +58,20 @@ def test_single_rank_comm():
     buf = np.ones(3)
     c.Allreduce(buf)  # in place
     np.testing.assert_array_equal(buf, np.ones(3))
+
+
+def test_rccsdtq_route(monkeypatch):
+    """compute_r4_tri of distr_cc/rccsdtq.py is wrapped once and routed by the backend string."""
+    orig_calls = []
+    r4mod = types.SimpleNamespace(compute_r4_tri=lambda mycc, *a, **k: orig_calls.append("orig") or "orig:r4")
+    routed = []
+    monkeypatch.setattr(backend, "compute_r4_tri", lambda mycc, *a, **k: routed.append("gpu") or "gpu:r4")
+    mod, qmod, _ = _fake_module()
+    names = backend.install(mod, qmod, r4mod)
+    assert "rccsdtq.compute_r4_tri" in names
+    assert "rccsdtq.compute_r4_tri" not in backend.install(mod, qmod, r4mod)
+    mycc = types.SimpleNamespace(einsum_backend="numpy", comm=backend.SingleRankComm())
+    assert r4mod.compute_r4_tri(mycc, None, None, None, None) == "orig:r4"
+    mycc.einsum_backend = "cuda"
+    assert r4mod.compute_r4_tri(mycc, None, None, None, None) == "gpu:r4"
+    assert orig_calls == ["orig"] and routed == ["gpu"]

@@ -84,3 +84,28 @@ def test_q_kernel(mods, oracle):
     want = q_ref.q_energy_ref(er, t2.transpose(2, 3, 0, 1), T, eris.mo_energy[:no], eris.mo_energy[no:], 2, oracle)
     got = backend.q_kernel(mycc, eris=eris, tamps=[None, t2, (None, t3)], blksize=2)
     np.testing.assert_allclose(got, want, rtol=1e-10, atol=1e-14)
+
+
+def test_compute_r4_tri_route(mods, oracle):
+    """The reference's compute_r4_tri(mycc, imds, t2, t3, (dt4, t4_local)) on host numpy
+    inputs through the backend, against the oracle's literal loop (OO batch included)."""
+    backend = mods[0]
+    from oracle import t4_ref
+    from test_t4_residual_algebra import _inputs, stab_symmetric
+    no, nv = 4, 5
+    d = _inputs(no, nv, 21)
+    quads = t4_ref.stored_quadruples(no)
+    d["t4"] = stab_symmetric(d["t4"], quads)
+    rng = np.random.default_rng(4)
+    F_oo, W_ovvo = rng.standard_normal((no, no)), rng.standard_normal((no, nv, nv, no)) * 0.1
+    want = t4_ref.compute_r4_tri_ref(d["eris"], d["F_vv"], d["W_vvvo"], d["W_vooo"], d["W_vvvv"], d["W_oooo"],
+                                     d["W_ovov"], d["t2"], d["t3"], d["t4"], no, oracle, F_oo, W_ovvo)
+    imds = types.SimpleNamespace(t1_eris=d["eris"], F_vv=d["F_vv"], W_vvvo=d["W_vvvo"], W_vooo=d["W_vooo"],
+                                 W_vvvv=d["W_vvvv"], W_oooo=d["W_oooo"], W_ovov=d["W_ovov"], F_oo=F_oo,
+                                 W_ovvo=W_ovvo)
+    dt4 = types.SimpleNamespace(iter_local_ijkl=lambda: [q + (n,) for n, q in enumerate(quads)])
+    mycc = types.SimpleNamespace(einsum_backend="cuda", comm=backend.SingleRankComm(), nocc=no,
+                                 dcc_precision="fp64")
+    got = backend.compute_r4_tri(mycc, imds, d["t2"], d["t3"], (dt4, d["t4"]))
+    assert np.abs(got - want).max() <= 1e-11 * np.abs(want).max()
+    assert imds.W_vvvo is None and imds.t1_eris is None  # released as the reference does
