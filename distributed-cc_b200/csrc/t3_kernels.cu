@@ -1074,6 +1074,10 @@ __global__ void __launch_bounds__(OT_THREADS) k_unpack_all(const double *t3, dou
     build_orbit_set(os, t0, t1, t2);
     const int64_t n3 = (int64_t)nv * nv * nv;
     const int pinv[6] = {0, 1, 2, 4, 3, 5};  // inverse of each axis map
+    // even nvir: every row starts on 16 bytes (U 16-byte aligned), so threads write (z, z+1) pairs
+    const bool vec = (nv & 1) == 0 && ((uintptr_t)U & 15) == 0 && blockDim.x == TE3 / 2;
+    const int px = threadIdx.x >> 5, py = (threadIdx.x >> 2) & 7, pz = (threadIdx.x & 3) * 2;
+    const int64_t prel = ((int64_t)px * nv + py) * nv + pz;
     int64_t q = blockIdx.y;
     if (q >= nblocks) return;
     load_orbit_tiles_async(sm, os, t3 + q * n3, nv);
@@ -1108,6 +1112,21 @@ __global__ void __launch_bounds__(OT_THREADS) k_unpack_all(const double *t3, dou
             const int cs = order_case3(xyz[0], xyz[1], xyz[2], srt);
             const int pi = pinv[cs];
             double *dst = U + (((int64_t)xyz[0] * nocc + xyz[1]) * nocc + xyz[2]) * n3;
+            if (vec) {
+                // one 16-byte pair (z, z+1) per thread: its two shared-memory sources for this
+                // axis map, then one store per tile of the set
+                auto c0 = [&](int m) { return m == 0 ? px : (m == 1 ? py : pz); };
+                auto c1 = [&](int m) { return m == 0 ? px : (m == 1 ? py : pz + 1); };
+                const int off0 = sidx(c0(perm3(pi, 0)), c0(perm3(pi, 1)), c0(perm3(pi, 2)));
+                const int off1 = sidx(c1(perm3(pi, 0)), c1(perm3(pi, 1)), c1(perm3(pi, 2)));
+                for (int s = 0; s < os.nslot; s++) {
+                    const int X0 = os.tile[s][0] * TE, Y0 = os.tile[s][1] * TE, Z0 = os.tile[s][2] * TE;
+                    if (X0 + px >= nv || Y0 + py >= nv || Z0 + pz >= nv) continue;
+                    const double *b = buf + os.nbr[s][pi] * SLOT;
+                    *(double2 *)(dst + ((int64_t)X0 * nv + Y0) * nv + Z0 + prel) = make_double2(b[off0], b[off1]);
+                }
+                continue;
+            }
             for (int s = 0; s < os.nslot; s++) {
                 const int src_slot = os.nbr[s][pi];
                 const int X0 = os.tile[s][0] * TE, Y0 = os.tile[s][1] * TE, Z0 = os.tile[s][2] * TE;
