@@ -387,66 +387,116 @@ __device__ __forceinline__ void tile_element(int l, int j, int u[3]) {
 // Element owned by thread t (0..255) of a CTA, half h: the step is (warp, h).
 __device__ __forceinline__ void tg_element(int t, int h, int u[3]) { tile_element(t & 31, (t >> 5) | (h << 3), u); }
 
-// In-place P3 spin summation, one warp per orbit set.  Each warp owns a
-// dense 6 x 8^3 buffer: it copies the distinct permuted tiles of its canonical
-// tile triple for one block (16-byte cp.async), evaluates every canonical
-// position of the set (lanes/steps follow tile_element, so the six permuted
-// reads and writes are conflict-free) and stores the tiles back with 16-byte
-// stores, then moves to its next block.  No CTA-wide barrier: the warps of an
-// SM (three CTAs of three warps) overlap each other's copies, sums and stores.
-// Same arithmetic as k_p3_inplace; FULL (P3_full) drops the unit
-// coefficients (x * 1.0 == x exactly).
-constexpr int PW_WARPS = 3;
+// In-place P3 spin summation with TMA-moved orbit tiles.  A CTA of two warps
+// owns one orbit set at a time: one thread loads the distinct permuted 8^3
+// tiles of its canonical tile triple (cp.async.bulk.tensor, box 8 x 8 x 8 of
+// the [nblocks][nv][nv][nv] array; the ragged edge is zero-filled on load and
+// clipped on store) into a dense 6 x 8^3 buffer, the two warps evaluate every
+// canonical position of the set in shared memory (lanes/steps follow
+// tile_element, so the six permuted reads and writes are conflict-free), and
+// the same thread stores the tiles back with TMA.  Two buffers per CTA: the
+// tiles of the CTA's next set are in flight while the current set is summed
+// and stored; four CTAs per SM.  Same arithmetic as k_p3_inplace; FULL
+// (P3_full) drops the unit coefficients (x * 1.0 == x exactly).
+//
+// Each wait on a load is bounded: thread 0 waits (WAIT_NS of %globaltimer),
+// and on a timeout records DCC_ERR_TIMEOUT in *status, waits (bounded) for
+// its copies in flight and the CTA returns.
+constexpr int P3T_WARPS = 2;
+constexpr int P3T_CTAS_PER_SM = 4;  // 48 KB of shared memory each
+
+__device__ __forceinline__ bool p3_wait_bounded(uint32_t bar, uint32_t parity, int *status) {
+    if (mbar_try(bar, parity)) return true;
+    const uint64_t t0 = globaltimer();
+    for (;;) {
+        if (mbar_try(bar, parity)) return true;
+        if (globaltimer() - t0 > WAIT_NS) {
+            atomicExch(status, DCC_ERR_TIMEOUT);
+            return false;
+        }
+    }
+}
 
 template <bool FULL>
-__global__ void __launch_bounds__(32 * PW_WARPS, 3) k_p3_warp(double *A, int64_t nblocks, int nv, int ntile, P3Coef k) {
-    extern __shared__ __align__(16) double sm[];  // PW_WARPS x 6 x TE3 doubles
+__global__ void __launch_bounds__(32 * P3T_WARPS, P3T_CTAS_PER_SM)
+    k_p3_tma(const __grid_constant__ CUtensorMap map, int64_t nblocks, int nv, int ntile, P3Coef k, int *status) {
+    extern __shared__ __align__(128) double smbuf[];  // 2 x 6 x TE3 doubles
+    __shared__ __align__(8) uint64_t bar[2];
+    __shared__ int s_ok;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    double *buf = sm + w * 6 * TE3;
-    const int64_t n3 = (int64_t)nv * nv * nv;
-    const int cy = lane >> 2, cz = 2 * (lane & 3);  // this lane's 16-byte chunk of every tile row pair
-    const unsigned sbase = (unsigned)__cvta_generic_to_shared(buf);
-    // work item = (block, tile triple), triples fastest: the orbit sets of one block are in
-    // flight together, so both 64-byte halves of each 128-byte line are read while in L2
     const int64_t ntri = (int64_t)ntile * (ntile + 1) * (ntile + 2) / 6;
-    const int64_t nwork = nblocks * ntri, stride = (int64_t)gridDim.x * PW_WARPS;
-    for (int64_t wi = (int64_t)blockIdx.x * PW_WARPS + w; wi < nwork; wi += stride) {
-        const int64_t b = wi / ntri;
-        int t0, t1, t2;
-        decode_tri3(wi % ntri, ntile, t0, t1, t2);
-        auto tsel = [&](int m) { return m == 0 ? t0 : (m == 1 ? t1 : t2); };
-        // slot s holds tile perm_s(T); slot_of(s) = first slot with the same tile (3 bits per slot)
-        unsigned slot_of = 0;
+    const int64_t nwork = nblocks * ntri;
+    if (threadIdx.x == 0) {
+        mbar_init(smem_u32(&bar[0]), 1);
+        mbar_init(smem_u32(&bar[1]), 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    // work item = (block, tile triple), triples fastest
+    struct Item {
+        int64_t b;
+        int t[3];
+        unsigned slot_of;  // slot s holds tile perm_s(T); slot_of = first slot with the same tile (3 bits per slot)
+    };
+    auto make = [&](int64_t wi) {
+        Item it;
+        it.b = wi / ntri;
+        decode_tri3(wi % ntri, ntile, it.t[0], it.t[1], it.t[2]);
+        unsigned so = 0;
 #pragma unroll
         for (int sl = 0; sl < 6; sl++) {
             int first = sl;
 #pragma unroll
             for (int q = sl - 1; q >= 0; q--)
-                if (tsel(perm3(q, 0)) == tsel(perm3(sl, 0)) && tsel(perm3(q, 1)) == tsel(perm3(sl, 1)) &&
-                    tsel(perm3(q, 2)) == tsel(perm3(sl, 2)))
+                if (it.t[perm3(q, 0)] == it.t[perm3(sl, 0)] && it.t[perm3(q, 1)] == it.t[perm3(sl, 1)] &&
+                    it.t[perm3(q, 2)] == it.t[perm3(sl, 2)])
                     first = q;
-            slot_of |= (unsigned)first << (3 * sl);
+            so |= (unsigned)first << (3 * sl);
         }
-        auto sof = [&](int sl) { return (int)((slot_of >> (3 * sl)) & 7u); };
-        double *blk = A + b * n3;
-#pragma unroll 1
-        for (int sl = 0; sl < 6; sl++) {
-            if (sof(sl) != sl) continue;
-            const int gx0 = tsel(perm3(sl, 0)) * TE, gy = tsel(perm3(sl, 1)) * TE + cy, gz = tsel(perm3(sl, 2)) * TE + cz;
-            if (gy >= nv || gz >= nv) continue;
-            const double *src = blk + ((int64_t)gx0 * nv + gy) * nv + gz;
-            const unsigned dst = sbase + 8u * (unsigned)(sl * TE3 + cy * 8 + cz);
+        it.slot_of = so;
+        return it;
+    };
+    auto distinct = [](const Item &it, int sl) { return ((it.slot_of >> (3 * sl)) & 7u) == (unsigned)sl; };
+    auto issue = [&](const Item &it, int bi) {  // thread 0
+        int nd = 0;
+        for (int sl = 0; sl < 6; sl++) nd += distinct(it, sl);
+        const uint32_t b = smem_u32(&bar[bi]);
+        mbar_expect_tx(b, (uint32_t)nd * TE3 * 8);
+        for (int sl = 0; sl < 6; sl++)
+            if (distinct(it, sl))
+                tma_load_5d(smem_u32(smbuf + (bi * 6 + sl) * TE3), &map, b, it.t[perm3(sl, 2)] * TE,
+                            it.t[perm3(sl, 1)] * TE, it.t[perm3(sl, 0)] * TE, (int)it.b, 0);
+    };
+    int64_t wi = blockIdx.x;
+    if (wi >= nwork) return;
+    Item cur = make(wi);
+    if (threadIdx.x == 0) issue(cur, 0);
+    uint32_t phase = 0;  // bit i: parity of buffer i
+    for (int bi = 0; wi < nwork; wi += gridDim.x, bi ^= 1) {
+        const int64_t wn = wi + gridDim.x;
+        Item nxt = cur;
+        if (wn < nwork) nxt = make(wn);
+        if (threadIdx.x == 0) {
+            if (wn < nwork) {
+                bulk_wait_read<0>();  // the stores of the buffer about to be refilled have read it
+                issue(nxt, bi ^ 1);
+            }
+            s_ok = p3_wait_bounded(smem_u32(&bar[bi]), (phase >> bi) & 1u, status);
+            if (!s_ok) {  // drain this CTA's copies in flight, then leave
+                mbar_wait_quiet(smem_u32(&bar[bi ^ 1]), (phase >> (bi ^ 1)) & 1u);
+                bulk_wait<0>();
+            }
+        }
+        __syncthreads();
+        if (!s_ok) return;
+        mbar_wait_quiet(smem_u32(&bar[bi]), (phase >> bi) & 1u);  // complete already: acquires the tiles
+        phase ^= 1u << bi;
+        double *buf = smbuf + bi * 6 * TE3;
+        const int t0 = cur.t[0], t1 = cur.t[1], t2 = cur.t[2];
+        auto sof = [&](int sl) { return (int)((cur.slot_of >> (3 * sl)) & 7u); };
 #pragma unroll
-            for (int x = 0; x < TE; x++)
-                if (gx0 + x < nv)
-                    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst + 8u * 64u * x),
-                                 "l"(src + (int64_t)x * nv * nv));
-        }
-        cp_async_commit();
-        cp_async_wait<0>();
-        __syncwarp();
-#pragma unroll 2
-        for (int j = 0; j < 16; j++) {
+        for (int jj = 0; jj < 16 / P3T_WARPS; jj++) {
+            const int j = w * (16 / P3T_WARPS) + jj;
             int u[3];
             tile_element(lane, j, u);
             const int x = u[0], y = u[1], z = u[2];
@@ -485,20 +535,18 @@ __global__ void __launch_bounds__(32 * PW_WARPS, 3) k_p3_warp(double *A, int64_t
 #pragma unroll
             for (int q = 0; q < 6; q++) buf[a[q]] = r[q];
         }
-        __syncwarp();
-#pragma unroll 1
-        for (int sl = 0; sl < 6; sl++) {
-            if (sof(sl) != sl) continue;
-            const int gx0 = tsel(perm3(sl, 0)) * TE, gy = tsel(perm3(sl, 1)) * TE + cy, gz = tsel(perm3(sl, 2)) * TE + cz;
-            if (gy >= nv || gz >= nv) continue;
-            double *dst = blk + ((int64_t)gx0 * nv + gy) * nv + gz;
-            const double *src = buf + sl * TE3 + cy * 8 + cz;
-#pragma unroll
-            for (int x = 0; x < TE; x++)
-                if (gx0 + x < nv) *(double2 *)(dst + (int64_t)x * nv * nv) = *(const double2 *)(src + x * 64);
+        fence_proxy_async_smem();  // the sums become visible to the TMA stores
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            for (int sl = 0; sl < 6; sl++)
+                if (distinct(cur, sl))
+                    tma_store_5d(&map, smem_u32(buf + sl * TE3), cur.t[perm3(sl, 2)] * TE, cur.t[perm3(sl, 1)] * TE,
+                                 cur.t[perm3(sl, 0)] * TE, (int)cur.b, 0);
+            bulk_commit();
         }
-        __syncwarp();
+        cur = nxt;
     }
+    if (threadIdx.x == 0) bulk_wait<0>();
 }
 
 int p3_pattern(const char *name, double p[5]) {
@@ -517,6 +565,22 @@ int p3_pattern(const char *name, double p[5]) {
     return -1;
 }
 
+// Status word of the bounded waits in the TMA symmetrizer (0, or DCC_ERR_TIMEOUT once a
+// wait gave up); one per device, read and cleared by dcc_t3_symmetrize_status.
+static __device__ int g_sym_status;
+
+static int *sym_status_word() {
+    static int *cache[64] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
+    if (!cache[dev]) {
+        void *p = nullptr;
+        if (cudaGetSymbolAddress(&p, g_sym_status) != cudaSuccess) return nullptr;
+        cache[dev] = (int *)p;
+    }
+    return cache[dev];
+}
+
 static int orbit3_launch(int mode, const double *in, double *o0, double *o1, double *o2, int64_t nblocks,
                          int64_t nvir, const P3Coef &k, void *stream) {
     if (nblocks == 0 || nvir == 0) return DCC_OK;
@@ -529,20 +593,32 @@ static int orbit3_launch(int mode, const double *in, double *o0, double *o1, dou
     dim3 grid((unsigned)ntri, (unsigned)gy);
     size_t smem = 2 * 6 * SLOT * sizeof(double);
     cudaStream_t st = as_stream(stream);
-    if (mode == 0 && nvir % 2 == 0 && ((uintptr_t)o0 & 15) == 0) {  // 16-byte rows
-        const size_t wsm = (size_t)PW_WARPS * 6 * TE3 * sizeof(double);
-        // persistent: three CTAs per SM walk the (block, triple) items
-        const int64_t nwarps = (nblocks * ntri + PW_WARPS - 1) / PW_WARPS;
-        const unsigned wgrid = (unsigned)(nwarps < 148 * 3 ? nwarps : 148 * 3);
-        const bool full = k.p0 == 1.0 && k.p1 == 1.0 && k.p2 == 1.0 && k.p3 == 1.0 && k.p4 == 1.0;
-        if (full) {
-            cudaFuncSetAttribute(k_p3_warp<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wsm);
-            k_p3_warp<true><<<wgrid, 32 * PW_WARPS, wsm, st>>>(o0, nblocks, (int)nvir, ntile, k);
-        } else {
-            cudaFuncSetAttribute(k_p3_warp<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wsm);
-            k_p3_warp<false><<<wgrid, 32 * PW_WARPS, wsm, st>>>(o0, nblocks, (int)nvir, ntile, k);
+    if (mode == 0 && nvir % 2 == 0 && ((uintptr_t)o0 & 15) == 0 && nblocks < (1ll << 31)) {  // 16-byte rows
+        CUtensorMap map;
+        EncodeTiledFn fn = encode_fn();
+        const cuuint64_t nv = (cuuint64_t)nvir;
+        const cuuint64_t dims[5] = {nv, nv, nv, (cuuint64_t)nblocks, 1};
+        const cuuint64_t strides[4] = {nv * 8, nv * nv * 8, nv * nv * nv * 8, nv * nv * nv * 8 * (cuuint64_t)nblocks};
+        const cuuint32_t box[5] = {TE, TE, TE, 1, 1}, es[5] = {1, 1, 1, 1, 1};
+        int *status = sym_status_word();
+        if (fn && status &&
+            fn(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 5, o0, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+               CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS) {
+            const size_t tsm = (size_t)2 * 6 * TE3 * sizeof(double);
+            int dev = 0, nsm = 148;
+            if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+            const int64_t nwork = nblocks * ntri, cap = (int64_t)nsm * P3T_CTAS_PER_SM;
+            const unsigned tgrid = (unsigned)(nwork < cap ? nwork : cap);
+            const bool full = k.p0 == 1.0 && k.p1 == 1.0 && k.p2 == 1.0 && k.p3 == 1.0 && k.p4 == 1.0;
+            if (full) {
+                cudaFuncSetAttribute(k_p3_tma<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tsm);
+                k_p3_tma<true><<<tgrid, 32 * P3T_WARPS, tsm, st>>>(map, nblocks, (int)nvir, ntile, k, status);
+            } else {
+                cudaFuncSetAttribute(k_p3_tma<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tsm);
+                k_p3_tma<false><<<tgrid, 32 * P3T_WARPS, tsm, st>>>(map, nblocks, (int)nvir, ntile, k, status);
+            }
+            return launch_status("P3 spin summation");
         }
-        return launch_status("P3 spin summation");
     }
     if (mode == 0 && nvir <= 1290) {  // 32-bit element offsets inside a block
         cudaFuncSetAttribute(k_p3_inplace, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -927,6 +1003,18 @@ extern "C" int dcc_t3_transpose_add(const double *A, double *B, int64_t nblocks,
     DCC_REQUIRE(A != B, DCC_ERR_SHAPE, "transpose_add is out of place");
     P3Coef k{};
     return orbit3_launch(2, A, B, nullptr, nullptr, nblocks, nvir, k, stream);
+}
+
+extern "C" int dcc_t3_symmetrize_status(int *out, void *stream) {
+    clear_error();
+    DCC_REQUIRE(out, DCC_ERR_NULL, "out is NULL");
+    int *word = sym_status_word();
+    DCC_REQUIRE(word, DCC_ERR_CUDA, "status word unavailable");
+    cudaStream_t st = as_stream(stream);
+    if (cudaMemcpyAsync(out, word, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess || cudaMemsetAsync(word, 0, sizeof(int), st) != cudaSuccess)
+        return launch_status("symmetrize status");
+    return DCC_OK;
 }
 
 extern "C" int dcc_take_t3_batched(const double *t3_local, double *out, const int32_t *ijk,

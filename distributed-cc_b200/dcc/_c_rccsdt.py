@@ -32,6 +32,16 @@ def t3_spin_summation_inplace_(A, nblocks, nvir, pattern, alpha=1.0, beta=0.0):
     return A
 
 
+def symmetrize_status():
+    """Status word of the bounded waits in the TMA spin-summation kernel on the current
+    device (0, or DCC_ERR_TIMEOUT once a wait gave up); reading clears it and
+    synchronizes the current stream."""
+    import ctypes
+    out = ctypes.c_int(0)
+    L.call("dcc_t3_symmetrize_status", ctypes.addressof(out), L.stream_ptr())
+    return out.value
+
+
 def _nblk(A, nvir):
     if A.numel() % max(nvir ** 3, 1):
         raise ValueError("buffer is not a whole number of nvir^3 blocks")

@@ -74,6 +74,12 @@ DCC_API int dcc_t3_spin_summation_triple_sym(const double *A, double *B0, double
  * Replaces t3_transpose_add_ (src/rccsdt.c:320-375). */
 DCC_API int dcc_t3_transpose_add(const double *A, double *B, int64_t nblocks, int64_t nvir, void *stream);
 
+/* Copies into *out (host int) the status word of the bounded waits of the
+ * TMA spin-summation kernel on the current device (0, or DCC_ERR_TIMEOUT
+ * once a wait gave up) and clears it; synchronizes `stream`.  No reference
+ * counterpart: the reference symmetrizers run on the host. */
+DCC_API int dcc_t3_symmetrize_status(int *out, void *stream);
+
 /* t3_blk = T3[i,j,k] for any ordering, unpacked from canonical storage.
  * ijk_to_local_idx is a HOST array of nocc3 int64 (-1: not stored).  Returns
  * DCC_ERR_NOT_LOCAL when the block is not stored (the reference silently
