@@ -42,6 +42,15 @@ def symmetrize_status():
     return out.value
 
 
+def t3_orbit_roundtrip_(A, nblocks, nvir):
+    """Diagnostic: the spin-summation kernel's tile traffic with no arithmetic (A unchanged)."""
+    A = L.as_tensor(A, f64, "A")
+    if A.numel() != nblocks * nvir ** 3:
+        raise ValueError("A must hold nblocks nvir^3 blocks")
+    L.call("dcc_t3_orbit_roundtrip", L.ptr(A), nblocks, nvir, L.stream_ptr())
+    return A
+
+
 def _nblk(A, nvir):
     if A.numel() % max(nvir ** 3, 1):
         raise ValueError("buffer is not a whole number of nvir^3 blocks")

@@ -55,6 +55,7 @@ _SIGS = {
     "dcc_t3_spin_summation_triple_sym": [c_vp, c_vp, c_vp, c_vp, c_i64, c_i64, c_vp],
     "dcc_t3_transpose_add": [c_vp, c_vp, c_i64, c_i64, c_vp],
     "dcc_t3_symmetrize_status": [c_vp, c_vp],
+    "dcc_t3_orbit_roundtrip": [c_vp, c_i64, c_i64, c_vp],
     "dcc_take_t3_ijk_single": [c_vp, c_vp, c_vp] + [c_i64] * 5 + [c_vp],
     "dcc_take_t3_batched": [c_vp, c_vp, c_vp, c_vp, c_i64, c_i64, c_i64, c_vp],
     "dcc_fill_local_data_ijk": [c_vp, c_vp, c_vp, c_vp, c_i64, c_i64, c_vp],

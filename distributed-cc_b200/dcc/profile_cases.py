@@ -1,7 +1,7 @@
 """Small, self-contained launches of single kernels for profiler captures.
 
     python -m dcc.profile_cases gemm   [--kind bf16x3] [--reps 3]
-    python -m dcc.profile_cases p3     [--reps 3]
+    python -m dcc.profile_cases p3     [--reps 3] [--nvir 90] [--roundtrip]
     python -m dcc.profile_cases update [--reps 3]
     python -m dcc.profile_cases q      [--reps 3]
     python -m dcc.profile_cases gather [--reps 3]
@@ -42,12 +42,19 @@ def case_gemm(kind, reps):
     assert int(op.status.item()) == 0
 
 
-def case_p3(reps):
+def case_p3(reps, nvir=90, roundtrip=False):
+    """P3_full on 1.28 GB of blocks (220 blocks at nvir=90; as many nvir^3 blocks as fit in the
+    same bytes otherwise); --roundtrip moves the same tiles with no arithmetic."""
     from dcc import _c_rccsdt
-    t3 = torch.randn(220, 90, 90, 90, dtype=torch.float64, device="cuda")
+    nb = 220 * 90 ** 3 // nvir ** 3
+    t3 = torch.randn(nb, nvir, nvir, nvir, dtype=torch.float64, device="cuda")
     for _ in range(reps):
-        _c_rccsdt.t3_spin_summation_inplace_(t3, 220, 90, "P3_full", -1.0 / 6.0, 1.0)
+        if roundtrip:
+            _c_rccsdt.t3_orbit_roundtrip_(t3, nb, nvir)
+        else:
+            _c_rccsdt.t3_spin_summation_inplace_(t3, nb, nvir, "P3_full", -1.0 / 6.0, 1.0)
     torch.cuda.synchronize()
+    assert _c_rccsdt.symmetrize_status() == 0
 
 
 def case_update(reps):
@@ -145,11 +152,13 @@ def main():
     ap.add_argument("--kind", default="bf16x3")
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--nocc", type=int, default=None, help="occupied orbitals (xgemm, oogemm, gather, unpack)")
+    ap.add_argument("--nvir", type=int, default=90, help="virtual orbitals (p3)")
+    ap.add_argument("--roundtrip", action="store_true", help="p3: the tile traffic with no arithmetic")
     a = ap.parse_args()
     if a.case == "gemm":
         case_gemm(a.kind, a.reps)
     elif a.case == "p3":
-        case_p3(a.reps)
+        case_p3(a.reps, a.nvir, a.roundtrip)
     elif a.case == "update":
         case_update(a.reps)
     elif a.case in ("gather", "xgemm", "oogemm", "unpack", "qgroup"):

@@ -74,6 +74,13 @@ DCC_API int dcc_t3_spin_summation_triple_sym(const double *A, double *B0, double
  * Replaces t3_transpose_add_ (src/rccsdt.c:320-375). */
 DCC_API int dcc_t3_transpose_add(const double *A, double *B, int64_t nblocks, int64_t nvir, void *stream);
 
+/* Diagnostic: moves every orbit tile set of nblocks nvir^3 blocks through the
+ * spin-summation kernel's TMA loads and stores with no arithmetic (A is left
+ * unchanged): the traffic ceiling of that kernel on this layout.  Even nvir
+ * and a 16-byte aligned A only (else DCC_ERR_UNSUPPORTED).  No reference
+ * counterpart. */
+DCC_API int dcc_t3_orbit_roundtrip(double *A, int64_t nblocks, int64_t nvir, void *stream);
+
 /* Copies into *out (host int) the status word of the bounded waits of the
  * TMA spin-summation kernel on the current device (0, or DCC_ERR_TIMEOUT
  * once a wait gave up) and clears it; synchronizes `stream`.  No reference

@@ -57,6 +57,17 @@ def test_t3_spin_sum(C, oracle, nvir, pattern):
     assert c3.symmetrize_status() == 0
 
 
+@pytest.mark.parametrize("nvir", [2, 10, 90])
+def test_orbit_roundtrip_is_identity(C, nvir):
+    """The diagnostic tile round trip of the spin-summation kernel leaves every block unchanged."""
+    c3 = C[0]
+    A = np.random.default_rng(nvir).standard_normal((3,) + (nvir,) * 3)
+    d = dev(A)
+    c3.t3_orbit_roundtrip_(d, 3, nvir)
+    assert np.array_equal(host(d), A)
+    assert c3.symmetrize_status() == 0
+
+
 @pytest.mark.parametrize("nvir", [1, 3, 8, 11, 90])
 def test_triple_sym_transpose_add(C, oracle, nvir):
     c3 = C[0]
