@@ -421,12 +421,21 @@ __device__ __forceinline__ bool p3_wait_bounded(uint32_t bar, uint32_t parity, i
     }
 }
 
-// MODE 0: general pattern; 1: P3_full; 2: no arithmetic (the tiles go back unchanged: the
-// traffic of the kernel alone, for measuring the layout's ceiling).
+// MODE 0: P3, general pattern; 1: P3_full; 2: no arithmetic (the tiles go back unchanged:
+// the traffic of the kernel alone, for measuring the layout's ceiling); 3: triple-sym into
+// out[0..2]; 4: transpose-add into out[0].  Modes 0-2 work in place (out[0] is the input's map).
+// Modes 3 and 4 write out[0] through the input buffer (each element is read and written by
+// the one thread owning its canonical position) and mode 3 out[1], out[2] through two more
+// 6 x 8^3 buffers.
+struct OrbitMaps {
+    CUtensorMap in, out[3];
+};
+
 template <int MODE>
 __global__ void __launch_bounds__(32 * P3T_WARPS, P3T_CTAS_PER_SM)
-    k_p3_tma(const __grid_constant__ CUtensorMap map, int64_t nblocks, int nv, int ntile, P3Coef k, int *status) {
-    extern __shared__ __align__(128) double smbuf[];  // 2 x 6 x TE3 doubles
+    k_orbit_tma(const __grid_constant__ OrbitMaps maps, int64_t nblocks, int nv, int ntile, P3Coef k, int *status) {
+    extern __shared__ __align__(128) double smbuf[];  // 2 x 6 x TE3 doubles (+ 2 x 6 x TE3 for mode 3)
+    double *xbuf = smbuf + 12 * TE3;                  // mode 3: out[1], out[2]
     __shared__ __align__(8) uint64_t bar[2];
     __shared__ int s_ok;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -470,7 +479,7 @@ __global__ void __launch_bounds__(32 * P3T_WARPS, P3T_CTAS_PER_SM)
         mbar_expect_tx(b, (uint32_t)nd * TE3 * 8);
         for (int sl = 0; sl < 6; sl++)
             if (distinct(it, sl))
-                tma_load_5d(smem_u32(smbuf + (bi * 6 + sl) * TE3), &map, b, it.t[perm3(sl, 2)] * TE,
+                tma_load_5d(smem_u32(smbuf + (bi * 6 + sl) * TE3), &maps.in, b, it.t[perm3(sl, 2)] * TE,
                             it.t[perm3(sl, 1)] * TE, it.t[perm3(sl, 0)] * TE, (int)it.b, 0);
     };
     int64_t wi = blockIdx.x;
@@ -483,10 +492,9 @@ __global__ void __launch_bounds__(32 * P3T_WARPS, P3T_CTAS_PER_SM)
         Item nxt = cur;
         if (wn < nwork) nxt = make(wn);
         if (threadIdx.x == 0) {
-            if (wn < nwork) {
-                bulk_wait_read<0>();  // the stores of the buffer about to be refilled have read it
-                issue(nxt, bi ^ 1);
-            }
+            // the stores of the buffer about to be refilled (and, mode 3, of the extra buffers) have read it
+            if (wn < nwork || MODE == 3) bulk_wait_read<0>();
+            if (wn < nwork) issue(nxt, bi ^ 1);
             s_ok = p3_wait_bounded(smem_u32(&bar[bi]), (phase >> bi) & 1u, status);
             if (!s_ok) {  // drain this CTA's copies in flight, then leave
                 mbar_wait_quiet(smem_u32(&bar[bi ^ 1]), (phase >> (bi ^ 1)) & 1u);
@@ -520,6 +528,32 @@ __global__ void __launch_bounds__(32 * P3T_WARPS, P3T_CTAS_PER_SM)
             double v[6];
 #pragma unroll
             for (int q = 0; q < 6; q++) v[q] = buf[a[q]];
+            if (MODE == 3) {  // B0 = 2T - T_acb - T_cba, B1 = 2T - T_bac - T_acb, B2 = B0 + T_acb - T_bac
+                double o0[6], o1[6], o2[6];
+#pragma unroll
+                for (int q = 0; q < 6; q++) {
+                    const double acb = v[comp6(1, q)], cba = v[comp6(5, q)], bac = v[comp6(2, q)];
+                    const double two = dmul(2.0, v[q]);
+                    o0[q] = dsub(dsub(two, acb), cba);
+                    o1[q] = dsub(dsub(two, bac), acb);
+                    o2[q] = dsub(dadd(o0[q], acb), bac);
+                }
+#pragma unroll
+                for (int q = 0; q < 6; q++) {
+                    buf[a[q]] = o0[q];
+                    xbuf[a[q]] = o1[q];
+                    xbuf[6 * TE3 + a[q]] = o2[q];
+                }
+                continue;
+            }
+            if (MODE == 4) {  // B = T + T_cab
+                double o[6];
+#pragma unroll
+                for (int q = 0; q < 6; q++) o[q] = dadd(v[q], v[comp6(4, q)]);
+#pragma unroll
+                for (int q = 0; q < 6; q++) buf[a[q]] = o[q];
+                continue;
+            }
             if (t0 == t1 && t1 == t2 && x == y && y == z) {
                 buf[a[0]] = dadd(dmul(k.beta, v[0]), dmul(k.ap34, dmul(k.p012, v[0])));
                 continue;
@@ -546,9 +580,14 @@ __global__ void __launch_bounds__(32 * P3T_WARPS, P3T_CTAS_PER_SM)
         __syncthreads();
         if (threadIdx.x == 0) {
             for (int sl = 0; sl < 6; sl++)
-                if (distinct(cur, sl))
-                    tma_store_5d(&map, smem_u32(buf + sl * TE3), cur.t[perm3(sl, 2)] * TE, cur.t[perm3(sl, 1)] * TE,
-                                 cur.t[perm3(sl, 0)] * TE, (int)cur.b, 0);
+                if (distinct(cur, sl)) {
+                    const int c0 = cur.t[perm3(sl, 2)] * TE, c1 = cur.t[perm3(sl, 1)] * TE, c2 = cur.t[perm3(sl, 0)] * TE;
+                    tma_store_5d(&maps.out[0], smem_u32(buf + sl * TE3), c0, c1, c2, (int)cur.b, 0);
+                    if (MODE == 3) {
+                        tma_store_5d(&maps.out[1], smem_u32(xbuf + sl * TE3), c0, c1, c2, (int)cur.b, 0);
+                        tma_store_5d(&maps.out[2], smem_u32(xbuf + (6 + sl) * TE3), c0, c1, c2, (int)cur.b, 0);
+                    }
+                }
             bulk_commit();
         }
         cur = nxt;
@@ -588,38 +627,53 @@ static int *sym_status_word() {
     return cache[dev];
 }
 
-// The TMA orbit-tile kernel on nblocks nvir^3 blocks (even nvir, 16-byte aligned A);
+// The TMA orbit-tile kernel on nblocks nvir^3 blocks (even nvir, 16-byte aligned buffers);
 // DCC_ERR_UNSUPPORTED when the layout does not allow it (the caller then uses another kernel).
-static int p3_tma_launch(int mode, double *A, int64_t nblocks, int64_t nvir, const P3Coef &k, cudaStream_t st) {
-    if (nvir % 2 != 0 || ((uintptr_t)A & 15) != 0 || nblocks >= (1ll << 31) || nvir > 65536) return DCC_ERR_UNSUPPORTED;
+static int orbit_tma_launch(int mode, const double *in, double *const out[3], int64_t nblocks, int64_t nvir,
+                            const P3Coef &k, cudaStream_t st) {
+    const int nout = mode == 3 ? 3 : 1;
+    if (nvir % 2 != 0 || ((uintptr_t)in & 15) != 0 || nblocks >= (1ll << 31) || nvir > 65536) return DCC_ERR_UNSUPPORTED;
+    for (int o = 0; o < nout; o++)
+        if (((uintptr_t)out[o] & 15) != 0) return DCC_ERR_UNSUPPORTED;
     EncodeTiledFn fn = encode_fn();
     int *status = sym_status_word();
     if (!fn || !status) return DCC_ERR_UNSUPPORTED;
-    CUtensorMap map;
+    OrbitMaps maps;
+    memset(&maps, 0, sizeof(maps));
     const cuuint64_t nv = (cuuint64_t)nvir;
     const cuuint64_t dims[5] = {nv, nv, nv, (cuuint64_t)nblocks, 1};
     const cuuint64_t strides[4] = {nv * 8, nv * nv * 8, nv * nv * nv * 8, nv * nv * nv * 8 * (cuuint64_t)nblocks};
     const cuuint32_t box[5] = {TE, TE, TE, 1, 1}, es[5] = {1, 1, 1, 1, 1};
-    if (fn(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 5, A, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
-           CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
-        return DCC_ERR_UNSUPPORTED;
+    for (int o = -1; o < nout; o++) {
+        CUtensorMap *m = o < 0 ? &maps.in : &maps.out[o];
+        void *base = o < 0 ? const_cast<double *>(in) : out[o];
+        if (fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 5, base, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+               CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+            return DCC_ERR_UNSUPPORTED;
+    }
     const int ntile = (int)ceil_div(nvir, TE);
     const int64_t ntri = (int64_t)ntile * (ntile + 1) * (ntile + 2) / 6;
-    const size_t tsm = (size_t)2 * 6 * TE3 * sizeof(double);
+    const size_t tsm = (size_t)(mode == 3 ? 4 : 2) * 6 * TE3 * sizeof(double);
     int dev = 0, nsm = 148;
     if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    const int64_t nwork = nblocks * ntri, cap = (int64_t)nsm * P3T_CTAS_PER_SM;
+    // triple-sym writes three outputs per tile: half the sets in flight keeps its lines in L2
+    const int64_t nwork = nblocks * ntri, cap = (int64_t)nsm * (mode == 3 ? 1 : P3T_CTAS_PER_SM);
     const unsigned grid = (unsigned)(nwork < cap ? nwork : cap);
-    if (mode == 0) {
-        cudaFuncSetAttribute(k_p3_tma<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tsm);
-        k_p3_tma<0><<<grid, 32 * P3T_WARPS, tsm, st>>>(map, nblocks, (int)nvir, ntile, k, status);
-    } else if (mode == 1) {
-        cudaFuncSetAttribute(k_p3_tma<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tsm);
-        k_p3_tma<1><<<grid, 32 * P3T_WARPS, tsm, st>>>(map, nblocks, (int)nvir, ntile, k, status);
-    } else {
-        cudaFuncSetAttribute(k_p3_tma<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tsm);
-        k_p3_tma<2><<<grid, 32 * P3T_WARPS, tsm, st>>>(map, nblocks, (int)nvir, ntile, k, status);
+#define DCC_ORBIT_TMA(M)                                                                                  \
+    case M:                                                                                               \
+        cudaFuncSetAttribute(k_orbit_tma<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tsm);      \
+        k_orbit_tma<M><<<grid, 32 * P3T_WARPS, tsm, st>>>(maps, nblocks, (int)nvir, ntile, k, status);   \
+        break;
+    switch (mode) {
+        DCC_ORBIT_TMA(0)
+        DCC_ORBIT_TMA(1)
+        DCC_ORBIT_TMA(2)
+        DCC_ORBIT_TMA(3)
+        DCC_ORBIT_TMA(4)
+        default:
+            return DCC_ERR_UNSUPPORTED;
     }
+#undef DCC_ORBIT_TMA
     return DCC_OK;
 }
 
@@ -635,9 +689,12 @@ static int orbit3_launch(int mode, const double *in, double *o0, double *o1, dou
     dim3 grid((unsigned)ntri, (unsigned)gy);
     size_t smem = 2 * 6 * SLOT * sizeof(double);
     cudaStream_t st = as_stream(stream);
-    if (mode == 0) {
+    {
         const bool full = k.p0 == 1.0 && k.p1 == 1.0 && k.p2 == 1.0 && k.p3 == 1.0 && k.p4 == 1.0;
-        if (p3_tma_launch(full ? 1 : 0, o0, nblocks, nvir, k, st) == DCC_OK) return launch_status("P3 spin summation");
+        const int tm = mode == 0 ? (full ? 1 : 0) : (mode == 1 ? 3 : 4);
+        double *const outs[3] = {o0, o1, o2};
+        if (orbit_tma_launch(tm, in, outs, nblocks, nvir, k, st) == DCC_OK)
+            return launch_status(mode == 0 ? "P3 spin summation" : "orbit-tile T3 kernel");
     }
     if (mode == 0 && nvir <= 1290) {  // 32-bit element offsets inside a block
         cudaFuncSetAttribute(k_p3_inplace, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -1030,7 +1087,8 @@ extern "C" int dcc_t3_orbit_roundtrip(double *A, int64_t nblocks, int64_t nvir, 
     if (nblocks == 0 || nvir == 0) return DCC_OK;
     DCC_REQUIRE(A, DCC_ERR_NULL, "A is NULL");
     P3Coef k{};
-    DCC_REQUIRE(p3_tma_launch(2, A, nblocks, nvir, k, as_stream(stream)) == DCC_OK, DCC_ERR_UNSUPPORTED,
+    double *const outs[3] = {A, nullptr, nullptr};
+    DCC_REQUIRE(orbit_tma_launch(2, A, outs, nblocks, nvir, k, as_stream(stream)) == DCC_OK, DCC_ERR_UNSUPPORTED,
                 "needs even nvir and a 16-byte aligned buffer");
     return launch_status("orbit tile round trip");
 }

@@ -68,22 +68,33 @@ def test_orbit_roundtrip_is_identity(C, nvir):
     assert c3.symmetrize_status() == 0
 
 
-@pytest.mark.parametrize("nvir", [1, 3, 8, 11, 90])
-def test_triple_sym_transpose_add(C, oracle, nvir):
+@pytest.mark.parametrize("nvir", [1, 2, 3, 8, 10, 11, 18, 90])
+@pytest.mark.parametrize("aligned", [True, False])
+def test_triple_sym_transpose_add(C, oracle, nvir, aligned):
+    """Even nvir with 16-byte aligned buffers run the TMA orbit-tile kernel, the rest the cp.async one."""
     c3 = C[0]
     rng = np.random.default_rng(1)
     nblk = 2 if nvir == 90 else 3
     A = rng.standard_normal((nblk,) + (nvir,) * 3)
-    dA = dev(A)
-    B = [torch.empty_like(dA) for _ in range(3)]
+
+    def buf():
+        if aligned:
+            return torch.empty(A.shape, dtype=torch.float64, device="cuda")
+        return torch.empty(A.size + 1, dtype=torch.float64, device="cuda")[1:].view(A.shape)
+
+    dA = buf()
+    dA.copy_(dev(A))
+    B = [buf() for _ in range(3)]
     c3.t3_spin_summation_triple_sym_(dA, *B, nvir)
-    T = torch.empty_like(dA)
+    T = buf()
     c3.t3_transpose_add_(dA, T, nvir)
     for b in range(nblk):
         want = oracle.t3_triple_sym(np.ascontiguousarray(A[b]), nvir)
         for m in range(3):
             assert np.array_equal(host(B[m])[b], want[m])
         assert np.array_equal(host(T)[b], oracle.t3_transpose_add(np.ascontiguousarray(A[b]), nvir))
+    assert np.array_equal(host(dA), A)
+    assert c3.symmetrize_status() == 0
 
 
 @pytest.mark.parametrize("nocc,nvir", [(1, 3), (3, 5), (4, 9), (3, 17)])
