@@ -423,7 +423,8 @@ __device__ __forceinline__ bool p3_wait_bounded(uint32_t bar, uint32_t parity, i
 
 // MODE 0: P3, general pattern; 1: P3_full; 2: no arithmetic (the tiles go back unchanged:
 // the traffic of the kernel alone, for measuring the layout's ceiling); 3: triple-sym into
-// out[0..2]; 4: transpose-add into out[0].  Modes 0-2 work in place (out[0] is the input's map).
+// out[0..2]; 4: transpose-add into out[0]; 5, 6, 7: output B0, B1 or B2 of triple-sym alone
+// into out[0].  Modes 0-2 work in place (out[0] is the input's map).
 // Modes 3 and 4 write out[0] through the input buffer (each element is read and written by
 // the one thread owning its canonical position) and mode 3 out[1], out[2] through two more
 // 6 x 8^3 buffers.
@@ -544,6 +545,19 @@ __global__ void __launch_bounds__(32 * P3T_WARPS, P3T_CTAS_PER_SM)
                     xbuf[a[q]] = o1[q];
                     xbuf[6 * TE3 + a[q]] = o2[q];
                 }
+                continue;
+            }
+            if (MODE >= 5) {  // one output of triple-sym: B0 (5), B1 (6) or B2 (7), same operations
+                double o[6];
+#pragma unroll
+                for (int q = 0; q < 6; q++) {
+                    const double acb = v[comp6(1, q)], cba = v[comp6(5, q)], bac = v[comp6(2, q)];
+                    const double two = dmul(2.0, v[q]);
+                    const double b0 = dsub(dsub(two, acb), cba);
+                    o[q] = MODE == 5 ? b0 : (MODE == 6 ? dsub(dsub(two, bac), acb) : dsub(dadd(b0, acb), bac));
+                }
+#pragma unroll
+                for (int q = 0; q < 6; q++) buf[a[q]] = o[q];
                 continue;
             }
             if (MODE == 4) {  // B = T + T_cab
@@ -670,6 +684,9 @@ static int orbit_tma_launch(int mode, const double *in, double *const out[3], in
         DCC_ORBIT_TMA(2)
         DCC_ORBIT_TMA(3)
         DCC_ORBIT_TMA(4)
+        DCC_ORBIT_TMA(5)
+        DCC_ORBIT_TMA(6)
+        DCC_ORBIT_TMA(7)
         default:
             return DCC_ERR_UNSUPPORTED;
     }
@@ -693,8 +710,19 @@ static int orbit3_launch(int mode, const double *in, double *o0, double *o1, dou
         const bool full = k.p0 == 1.0 && k.p1 == 1.0 && k.p2 == 1.0 && k.p3 == 1.0 && k.p4 == 1.0;
         const int tm = mode == 0 ? (full ? 1 : 0) : (mode == 1 ? 3 : 4);
         double *const outs[3] = {o0, o1, o2};
-        if (orbit_tma_launch(tm, in, outs, nblocks, nvir, k, st) == DCC_OK)
+        if (mode == 1 && nvir % 8 != 0) {
+            // rows not 64-byte aligned: three single-output passes (each output's partial lines
+            // merge in L2 one stream at a time), measured 2x faster than one pass with three
+            // output streams at nvir = 90
+            int rc = DCC_OK;
+            for (int o = 0; o < 3 && rc == DCC_OK; o++) {
+                double *const one[3] = {outs[o], nullptr, nullptr};
+                rc = orbit_tma_launch(5 + o, in, one, nblocks, nvir, k, st);
+            }
+            if (rc == DCC_OK) return launch_status("orbit-tile T3 kernel");
+        } else if (orbit_tma_launch(tm, in, outs, nblocks, nvir, k, st) == DCC_OK) {
             return launch_status(mode == 0 ? "P3 spin summation" : "orbit-tile T3 kernel");
+        }
     }
     if (mode == 0 && nvir <= 1290) {  // 32-bit element offsets inside a block
         cudaFuncSetAttribute(k_p3_inplace, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
