@@ -1,7 +1,7 @@
 """Small, self-contained launches of single kernels for profiler captures.
 
     python -m dcc.profile_cases gemm   [--kind bf16x3] [--reps 3]
-    python -m dcc.profile_cases p3     [--reps 3] [--nvir 90] [--roundtrip]
+    python -m dcc.profile_cases p3     [--reps 3] [--nvir 90] [--op p3|p3_422|roundtrip|triple|transpose] [--time]
     python -m dcc.profile_cases update [--reps 3]
     python -m dcc.profile_cases q      [--reps 3]
     python -m dcc.profile_cases gather [--reps 3]
@@ -42,19 +42,41 @@ def case_gemm(kind, reps):
     assert int(op.status.item()) == 0
 
 
-def case_p3(reps, nvir=90, roundtrip=False):
-    """P3_full on 1.28 GB of blocks (220 blocks at nvir=90; as many nvir^3 blocks as fit in the
-    same bytes otherwise); --roundtrip moves the same tiles with no arithmetic."""
+def case_p3(reps, nvir=90, op="p3", time=False):
+    """A T3 symmetrizer on 1.28 GB of blocks (220 blocks at nvir=90; as many nvir^3 blocks as fit in
+    the same bytes otherwise).  op: p3 (P3_full, in place), p3_422, roundtrip (the P3 kernel's tile
+    traffic with no arithmetic), triple (triple-sym, three outputs), transpose (transpose-add).
+    With time=True every launch is timed with CUDA events after a 256 MB L2 flush and the mean
+    of all but the first two is printed with the algorithmic bandwidth."""
     from dcc import _c_rccsdt
     nb = 220 * 90 ** 3 // nvir ** 3
     t3 = torch.randn(nb, nvir, nvir, nvir, dtype=torch.float64, device="cuda")
-    for _ in range(reps):
-        if roundtrip:
-            _c_rccsdt.t3_orbit_roundtrip_(t3, nb, nvir)
-        else:
-            _c_rccsdt.t3_spin_summation_inplace_(t3, nb, nvir, "P3_full", -1.0 / 6.0, 1.0)
+    outs = [torch.zeros_like(t3) for _ in range(3 if op == "triple" else 1 if op == "transpose" else 0)]
+    run, nbytes = {
+        "p3": (lambda: _c_rccsdt.t3_spin_summation_inplace_(t3, nb, nvir, "P3_full", -1.0 / 6.0, 1.0), 16),
+        "p3_422": (lambda: _c_rccsdt.t3_spin_summation_inplace_(t3, nb, nvir, "P3_422", 1.0, 0.0), 16),
+        "roundtrip": (lambda: _c_rccsdt.t3_orbit_roundtrip_(t3, nb, nvir), 16),
+        "triple": (lambda: _c_rccsdt.t3_spin_summation_triple_sym_(t3, *outs, nvir), 32),
+        "transpose": (lambda: _c_rccsdt.t3_transpose_add_(t3, outs[0] if outs else None, nvir), 16),
+    }[op]
+    flush = torch.empty(256 << 20, dtype=torch.int8, device="cuda") if time else None
+    times = []
+    for r in range(reps):
+        if time:
+            flush.fill_(r & 127)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+        run()
+        if time:
+            e1.record()
+            e1.synchronize()
+            times.append(e0.elapsed_time(e1))
     torch.cuda.synchronize()
     assert _c_rccsdt.symmetrize_status() == 0
+    if time and len(times) > 2:
+        ms = sum(times[2:]) / len(times[2:])
+        print(f"{op} nvir={nvir} blocks={nb}: {ms:.4f} ms, {nbytes * nb * nvir ** 3 / ms * 1e-6:.0f} GB/s "
+              f"({nbytes} B per element)")
 
 
 def case_update(reps):
@@ -153,12 +175,14 @@ def main():
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--nocc", type=int, default=None, help="occupied orbitals (xgemm, oogemm, gather, unpack)")
     ap.add_argument("--nvir", type=int, default=90, help="virtual orbitals (p3)")
-    ap.add_argument("--roundtrip", action="store_true", help="p3: the tile traffic with no arithmetic")
+    ap.add_argument("--op", default="p3", choices=["p3", "p3_422", "roundtrip", "triple", "transpose"],
+                    help="p3 case: which symmetrizer")
+    ap.add_argument("--time", action="store_true", help="p3 case: print CUDA-event timings")
     a = ap.parse_args()
     if a.case == "gemm":
         case_gemm(a.kind, a.reps)
     elif a.case == "p3":
-        case_p3(a.reps, a.nvir, a.roundtrip)
+        case_p3(a.reps, a.nvir, a.op, a.time)
     elif a.case == "update":
         case_update(a.reps)
     elif a.case in ("gather", "xgemm", "oogemm", "unpack", "qgroup"):
