@@ -435,6 +435,19 @@ def main():
                             "status_ok": q.status_ok()}
         q_line["speedup_vs_fp64"] = q_line["fp64"]["s_sample"] / q_line[args.precision]["s_sample"]
         q_line["abs_dE_paren_sample"] = abs(q_line["fp64"]["e_paren_sample"] - q_line[args.precision]["e_paren_sample"])
+        # the synthetic amplitudes give energies of O(10) Eh: the same sample with t2 and t3 scaled by
+        # one factor s so that the FP64 (Q) energy is -1e-3 Eh (a molecular (Q) correction), untimed
+        s = (1e-3 / max(abs(q_line["fp64"]["e_paren_sample"]), 1e-300)) ** 0.5
+        ms_line = {"amplitude_scale": s}
+        for prec in (args.precision, "fp64"):
+            q = rccsdt_q.QEnergy(NOCC, NVIR, Q_BLK, prec)
+            q.prepare(sample)
+            q.run(er, t2q * s, t3_abc * s, d.e_occ, d.e_vir, sample)
+            ms_line[prec] = {"e_bracket_sample": float(q.out[0]), "e_paren_sample": float(q.out[1]),
+                             "status_ok": q.status_ok()}
+        ms_line["abs_dE_bracket"] = abs(ms_line["fp64"]["e_bracket_sample"] - ms_line[args.precision]["e_bracket_sample"])
+        ms_line["abs_dE_paren"] = abs(ms_line["fp64"]["e_paren_sample"] - ms_line[args.precision]["e_paren_sample"])
+        q_line["molecule_scale"] = ms_line
         del t3_abc
 
     cpu = None

@@ -67,3 +67,33 @@ def test_q_energy_split_d_chunks(mods, oracle, dchunk):
     got = out.cpu().numpy()
     assert abs(got[0] - want[0]) <= 1e-4 * abs(want[0])
     assert abs(got[1] - want[1]) <= 1e-4 * abs(want[1])
+
+
+@pytest.mark.parametrize("precision", ["bf16x3", "tf32x3"])
+def test_q_energy_split_microhartree(mods, precision):
+    """The 1 uEh bar against the plain FP64 GPU path, at nocc=6 / nvir=40 on every task.  The
+    seeded synthetic amplitudes give an (Q) energy of O(1) Eh, far above a molecule's; t2 and t3
+    are scaled by one factor s so that the FP64 (Q) energy is -1e-3 Eh (the size of a molecular
+    (Q) correction), and both energies of the split path must then lie within 1e-6 Eh of FP64."""
+    gq, _ = mods
+    from dcc import _c_rccsdt, synthetic
+    no, nv, blk = 6, 40, 4
+    d = synthetic.make_inputs(no, nv, seed=41)
+    er = {"vvvo": d.W_vvvo, "vooo": d.W_vooo, "vvoo": d.eris_vvoo, "ovvo": d.W_ovvo, "ovov": d.W_ovov,
+          "vvvv": d.W_vvvv, "oooo": d.W_oooo}
+    t2 = d.t2.permute(2, 3, 0, 1).contiguous()
+    t3 = _c_rccsdt.redistribute_ijk_to_abc(d.t3, no, nv)
+
+    def energies(prec, s):
+        q = gq.QEnergy(no, nv, blk, prec)
+        out = q.run(er, t2 * s, t3 * s, d.e_occ, d.e_vir).cpu().numpy()
+        assert q.status_ok()
+        return out
+
+    e1 = energies("fp64", 1.0)
+    s = (1e-3 / abs(e1[1])) ** 0.5
+    want = energies("fp64", s)
+    got = energies(precision, s)
+    assert 1e-4 < abs(want[1]) < 1e-2
+    assert abs(got[0] - want[0]) < 1e-6, (got, want)
+    assert abs(got[1] - want[1]) < 1e-6, (got, want)
