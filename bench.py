@@ -196,6 +196,41 @@ def cpu_sample(nblk_sample=2, seed=0):
     return dt, len(trip) / len(sample), kind, len(sample)
 
 
+def iteration_energy_proxy(d, r_ref, r_mix):
+    """How the split path's error in one T3 iteration reaches the correlation energy.
+
+    Both residuals go through the same update (P3_full, divide, t3 += r3); the difference of the
+    two new T3 is fed to the T2 residual by the T3 -> r2 strings (distr_cc/rccsdt.py:300-316, FP64)
+    and, divided by the T2 denominators, to E = sum (2<ij|ab> - <ij|ba>) t2.  The same chain on the
+    FP64 T3 itself gives the triples' share of E.  r3 is linear in (t2, t3), so the ratio of the
+    two is independent of the amplitudes' scale: abs_dE_at_10mEh is the error of a molecule whose
+    triples contribute 10 mEh (the synthetic amplitudes are far larger than a molecule's)."""
+    import torch
+    from dcc import t3_feedback, t3_residual
+    no, nv = d.nocc, d.nvir
+    ws = torch.empty(1 << 16, dtype=torch.float64, device="cuda")
+    t3f, t3m = d.t3.clone(), d.t3.clone()
+    t3_residual.update_t3_(t3f, r_ref.clone(), d, workspace=ws)
+    t3_residual.update_t3_(t3m, r_mix.clone(), d, workspace=ws)
+    E_vovv = d.W_vvvo.permute(2, 3, 0, 1)  # <cx|ad> = <ad|cx>
+    E_ooov = d.W_vooo.permute(3, 2, 1, 0)  # <zx|la> = <al|xz>
+    D2 = (d.e_occ[:, None, None, None] + d.e_occ[None, :, None, None]
+          - d.e_vir[None, None, :, None] - d.e_vir[None, None, None, :])
+    L = 2.0 * d.eris_vvoo.permute(2, 3, 0, 1) - d.eris_vvoo.permute(2, 3, 1, 0)  # [i,j,a,b]
+
+    def energy(t3):
+        X = t3_feedback.p3_201_all(t3, no)
+        r2 = torch.einsum('cxad,xyzdba->yzbc', E_vovv, X) - torch.einsum('zxla,xyzabc->ylbc', E_ooov, X)
+        del X
+        return float((L * (r2 + r2.permute(1, 0, 3, 2)) / 2 / D2).sum())
+
+    e_t3 = energy(t3f)
+    de = energy(t3m - t3f)
+    del t3f, t3m
+    return {"e_t3_share_fp64": e_t3, "abs_dE": abs(de), "relative": abs(de / e_t3),
+            "abs_dE_at_10mEh": abs(de / e_t3) * 1e-2}
+
+
 def reference_arm(args, rank, world):
     """`--impl reference`: the reference's CPU path on this host's cores."""
     if rank != 0:
@@ -265,11 +300,13 @@ def main():
 
     # accuracy of the split path against the FP64 path on identical inputs
     rel_err = None
+    energy_proxy = None
     if fp64 is not None:
         r_ref = fp64.compute(d, d.t3)
         r_mix = mixed.compute(d, d.t3)
         torch.cuda.synchronize()
         rel_err = float((r_mix - r_ref).abs().max() / r_ref.abs().max())
+        energy_proxy = iteration_energy_proxy(d, r_ref, r_mix)
         del r_ref, r_mix
 
     def barrier():
@@ -470,7 +507,7 @@ def main():
                    "parallelism": "replicas" if world > 1 else "single"},
         "fp64_path_s_per_iter": ms_fp64 / fp64_steps / 1e3 if ms_fp64 else None,
         "speedup_vs_fp64": (ms_fp64 / fp64_steps) / (ms_mixed / args.steps) if ms_fp64 else None,
-        "r3_max_rel_err_vs_fp64": rel_err, "device_status_ok": ok,
+        "r3_max_rel_err_vs_fp64": rel_err, "iteration_energy_error": energy_proxy, "device_status_ok": ok,
         "cuda_graph_ms_per_step": graph_ms, "cuda_graph_status_ok": graph_ok,
         "roofline": {"kernel": "dcc::k_gemm_split3<0> (W_vvvv.t3 string)", "bound": "tensor",
                      "achieved": achieved, "peak": peak_useful, "unit": "TFLOP/s",
