@@ -273,18 +273,17 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
 
+    if args.impl == "reference":
+        # the reference's CPU path needs no GPU and no process group: rank 0 alone runs it
+        return reference_arm(args, rank, world)
     import torch
+    from dcc import ranks
     dist = None
     if world > 1:
         import datetime
         import torch.distributed as dist
         torch.cuda.set_device(local)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
-    if args.impl == "reference":
-        rc = reference_arm(args, rank, world)
-        if dist is not None:
-            dist.destroy_process_group()
-        return rc
 
     torch.cuda.set_device(local)
     from dcc import synthetic, t3_residual, contract
@@ -310,9 +309,7 @@ def main():
         del r_ref, r_mix
 
     def barrier():
-        if dist is not None:
-            dist.barrier()
-        torch.cuda.synchronize()
+        ranks.barrier("cuda")
 
     def step(res):
         res.compute(d, t3w, r3)
@@ -344,12 +341,7 @@ def main():
         e1.record()
         barrier()
         contract.gemm_ = orig_gemm
-        ms = e0.elapsed_time(e1)
-        if dist is not None:
-            t = torch.tensor([ms], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
-        return ms
+        return ranks.max_over_ranks(e0.elapsed_time(e1), "cuda")
 
     # this library's kernels per mixed step, counted on one untimed step
     from torch.profiler import profile, ProfilerActivity
@@ -380,7 +372,7 @@ def main():
         gstep.replay()
     g1.record()
     barrier()
-    graph_ms = g0.elapsed_time(g1) / args.steps
+    graph_ms = ranks.max_over_ranks(g0.elapsed_time(g1), "cuda") / args.steps
     graph_ok = gstep.status_ok()
     del gstep, t3g
     mixed.woooo_pair_symmetric = False
@@ -439,7 +431,8 @@ def main():
         e2e_step()
     e1.record()
     barrier()
-    e2e_ms = e0.elapsed_time(e1) / e2e_steps
+    e2e_ms_max = ranks.max_over_ranks(e0.elapsed_time(e1), "cuda")
+    e2e_ms = e2e_ms_max / e2e_steps
 
     # (Q): [Q]/(Q) energies on a sample of task groups (every group = the tasks sharing
     # (a, b, c) blocks), split path and FP64 path, scaled to all tasks by task count
@@ -494,7 +487,7 @@ def main():
                "sample": "%d of 220 blocks of one step, scaled by 220/%d; reference C helpers (OpenMP) for "
                          "P3/divide/transpose-add/triple-sym + numpy/BLAS einsums" % (n, n)}
 
-    value = ms_mixed / args.steps / 1e3 / world  # whole-job s per iteration (replicas)
+    value = ranks.job_seconds_per_iteration(ms_mixed, args.steps, world)  # whole job, replicas
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms_mixed / args.steps, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
@@ -516,7 +509,8 @@ def main():
                      "flops_per_launch": flops_launch, "launch_ms": gemm_avg,
                      "traffic": profile_traffic("gemm_split3_wvvvv_nocc10_nvir90")},
         "cpu_baseline": cpu,
-        "e2e": {"value": e2e_ms / 1e3, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "e2e": {"value": ranks.job_seconds_per_iteration(e2e_ms_max, e2e_steps, world), "unit": UNIT,
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "gpu_launches": launches_per_step * args.steps,
         "q_energy": q_line,
         "clocks": clk.summary(),
