@@ -26,11 +26,11 @@ permutation, hence the halves.  A W_oooo without the pair symmetry keeps its
 antisymmetric part on the reference's own permutation set
 {identity, (i,k,j; a,c,b), (j,k,i; b,c,a)}.
 
-In mixed precision S is built by three split-precision tcgen05 GEMMs written
+In mixed precision S is built by four split-precision tcgen05 GEMMs written
 straight into S's [i][j][k][a][b][c] layout (X; T2 and T5/2 as one GEMM over
-the concatenated contraction index; T1 reusing T2's U operand) plus an FP64
-GEMM for the K = nocc^2 W_oooo / F_oo part, and one gather kernel applies the
-symmetrization to S and Y.  W_vvvv.t3 (three strings, the dominant cost) are
+the concatenated contraction index; T1 reusing T2's U operand; the K = nocc^2
+W_oooo / F_oo part over a K-major split of U), and one gather kernel applies
+the symmetrization to S and Y.  W_vvvv.t3 (three strings, the dominant cost) are
 three split-precision GEMMs that accumulate straight into r3; the three
 F_vv.t3 strings ride in them as extra terms of the W operand
 (contract.WvvvvT3).  The FP64 path runs F_vv.t3 as batched DGEMMs.
@@ -206,6 +206,9 @@ class T3Residual:
                 self.ooa = contract.Split(no * nv, kind=k, device=device, pieces=[K, K])
                 self.oob = contract.Split(no * no * nv * nv, kind=k, device=device, pieces=[K, K])
                 self.t1a = contract.Split(no * nv, K, k, device)
+                # W_oooo / F_oo . U: rows (i,j), columns (k,a,b,c), K = (l,m)
+                self.wooa = contract.Split(no * no, no * no, k, device)
+                self.woob = contract.Split(no * nv ** 3, no * no, k, device)
         else:
             self.X = torch.empty((no * nv * nv, no * no * nv), dtype=f64, device=device)  # [(j,a,b),(i,k,c)]
 
@@ -230,9 +233,15 @@ class T3Residual:
             self._s_split(d)
         if self.with_oo:
             A, Wa = woooo_foo_matrix(d.W_oooo, d.F_oo, assume_symmetric=self.woooo_pair_symmetric)
-            # K = nocc^2 against 5.8 GB of U: bandwidth-bound, FP64 (cuBLAS) in both precisions (a split
-            # GEMM would first write a 3.7 GB transposed split of U)
-            S.view(no * no, -1).addmm_(A, self.U.view(no * no, -1))
+            if self.precision == "fp64":
+                S.view(no * no, -1).addmm_(A, self.U.view(no * no, -1))
+            else:
+                # S[(i,j)][(k,abc)] += A[(i,j)][(l,m)] U[(l,m)][(k,abc)] as a split GEMM: the K-major split
+                # of U (no nv^3 rows of no^2) costs one pass over U, the FP64 DGEMM took twice as long
+                n = no * nv ** 3
+                self.wooa.fill(A.contiguous(), contract.lin(no * no), contract.lin(1))
+                self.woob.fill(self.U, contract.lin(1), contract.lin(n))
+                contract.gemm_(self.wooa, self.woob, S, contract.lin(n), contract.lin(1), 1.0, 1.0, self.status)
             if Wa is not None:
                 if self.Ganti is None:
                     self.Ganti = torch.empty_like(self.S)
