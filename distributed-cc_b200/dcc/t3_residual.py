@@ -200,6 +200,8 @@ class T3Residual:
             self.xa = contract.Split(no * nv * nv, nv, k, device)
             self.xb = contract.Split(no * no * nv, nv, k, device)
             self.wvvvv = contract.WvvvvT3(self.n3, nv, precision, device)
+            self.ya = contract.Split(no * no * nv, no, k, device)
+            self.yb = contract.Split(no * nv * nv, no, k, device)
             self.status = torch.zeros(1, dtype=torch.int32, device=device)
             if with_oo:
                 K = no * nv
@@ -214,11 +216,19 @@ class T3Residual:
 
     # ------------------------------------------------------------ pieces
     def y_(self, d):
-        """Y[(i,j,a),(k,b,c)] = sum_l W_vooo[a,l,i,j] t2[l,k,b,c] (FP64: K = nocc is bandwidth-bound)."""
+        """Y[(i,j,a),(k,b,c)] = sum_l W_vooo[a,l,i,j] t2[l,k,b,c] (K = nocc: bound by writing Y; a
+        split GEMM in mixed precision, which writes Y at a higher rate than the FP64 DGEMM)."""
         no, nv = self.no, self.nv
-        A = d.W_vooo.permute(2, 3, 0, 1).reshape(no * no * nv, no)
-        Bm = d.t2.permute(1, 2, 3, 0).reshape(no * nv * nv, no)
-        torch.matmul(A, Bm.t(), out=self.Y)
+        if self.precision == "fp64":
+            A = d.W_vooo.permute(2, 3, 0, 1).reshape(no * no * nv, no)
+            Bm = d.t2.permute(1, 2, 3, 0).reshape(no * nv * nv, no)
+            torch.matmul(A, Bm.t(), out=self.Y)
+            return self.Y
+        c = contract
+        # A rows (i,j,a) of W_vooo[a,l,i,j], K = l; B rows (k,b,c) of t2[l,k,b,c], K = l
+        self.ya.fill(d.W_vooo, c.three(no, nv, no, 1, no ** 3), c.lin(no * no))
+        self.yb.fill(d.t2, c.lin(1), c.lin(no * nv * nv))
+        c.gemm_(self.ya, self.yb, self.Y, c.lin(no * nv * nv), c.lin(1), 1.0, 0.0, self.status)
         return self.Y
 
     def s_(self, d, t3):
