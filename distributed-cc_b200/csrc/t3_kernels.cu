@@ -1347,6 +1347,129 @@ __global__ void __launch_bounds__(OT_THREADS) k_unpack_all(const double *t3, dou
     }
 }
 
+// Unpack of every ordering by output row bands (even nvir, 16-byte aligned buffers).  A work
+// item is one ordered output block U[x,y,z] and one band of 8 x 8 of its rows (all of c): one
+// thread loads the band's source tiles (one 8^3 TMA box per output tile, from the canonical
+// block with its axes permuted), the CTA transposes them into a dense [8][8][nvir] band in
+// shared memory (lanes/steps follow tile_element, so the permuted tile reads are free of bank
+// conflicts), and the band goes out as one TMA store of whole rows.  Whole rows reach DRAM as
+// whole lines, where the orbit-tile kernel's 64-byte row pieces did not.  Items run
+// block-major, so the orderings of one canonical block read it from L2.
+// NB source buffers and NB band buffers per CTA of NT threads (with NB = 2 the tiles of the
+// next item load while the current band is transposed).  The launcher runs NB = 1 with two
+// CTAs per SM: one CTA of 16 warps with NB = 2 measured 1.9x slower.
+template <int NB, int NT>
+__global__ void __launch_bounds__(NT, NB == 2 ? 1 : 2)
+    k_unpack_band(const __grid_constant__ CUtensorMap src, const __grid_constant__ CUtensorMap dst, int64_t nblocks,
+                  int nocc, int nv, int ntile, int *status) {
+    extern __shared__ __align__(128) double sm[];  // NB x ntile x TE3 source tiles, then NB x 8 x 8 x nv bands
+    const size_t tile_dbl = (size_t)ntile * TE3, band_dbl = (size_t)TE * TE * nv;
+    __shared__ __align__(8) uint64_t bar[NB];
+    __shared__ int s_ok;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    constexpr int STEPS = 16 / (NT / 32);  // tile_element steps per warp and tile
+    const int pinv[6] = {0, 1, 2, 4, 3, 5};  // inverse of each axis map
+    const int64_t per_q = 6 * (int64_t)ntile * ntile, nwork = nblocks * per_q;
+    struct Item {
+        int64_t w;
+        int64_t out;  // output block (x * nocc + y) * nocc + z
+        int q, pi, X, Y;
+    };
+    // the first item at or after wi (stepping by the grid) whose ordering is new for its block
+    auto next_item = [&](int64_t wi) {
+        Item it{};
+        for (; wi < nwork; wi += gridDim.x) {
+            const int64_t q = wi / per_q;
+            const int g = (int)((wi / ((int64_t)ntile * ntile)) % 6);
+            int o[3];
+            decode_tri3(q, nocc, o[0], o[1], o[2]);
+            const int xyz[3] = {o[perm3(g, 0)], o[perm3(g, 1)], o[perm3(g, 2)]};
+            bool dup = false;
+            for (int sp = 0; sp < g; sp++)
+                if (o[perm3(sp, 0)] == xyz[0] && o[perm3(sp, 1)] == xyz[1] && o[perm3(sp, 2)] == xyz[2]) dup = true;
+            if (dup) continue;
+            int64_t srt[3];
+            it.pi = pinv[order_case3(xyz[0], xyz[1], xyz[2], srt)];
+            it.out = ((int64_t)xyz[0] * nocc + xyz[1]) * nocc + xyz[2];
+            it.q = (int)q;
+            const int xy = (int)(wi % ((int64_t)ntile * ntile));
+            it.X = xy / ntile;
+            it.Y = xy % ntile;
+            break;
+        }
+        it.w = wi;
+        return it;
+    };
+    auto issue = [&](const Item &it, int bi) {  // thread 0: the band's source tiles into buffer bi
+        const uint32_t b = smem_u32(&bar[bi]);
+        mbar_expect_tx(b, (uint32_t)ntile * TE3 * 8);
+        for (int zt = 0; zt < ntile; zt++) {
+            const int T[3] = {it.X, it.Y, zt};
+            tma_load_5d(smem_u32(sm + bi * tile_dbl + zt * TE3), &src, b, T[perm3(it.pi, 2)] * TE,
+                        T[perm3(it.pi, 1)] * TE, T[perm3(it.pi, 0)] * TE, it.q, 0);
+        }
+    };
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < NB; i++) mbar_init(smem_u32(&bar[i]), 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    Item cur = next_item(blockIdx.x);
+    if (cur.w >= nwork) return;
+    Item ahead = cur;  // the last item whose loads were issued
+    if (threadIdx.x == 0) issue(cur, 0);
+    for (int i = 1; i < NB; i++) {
+        ahead = next_item(ahead.w + gridDim.x);
+        if (threadIdx.x == 0 && ahead.w < nwork) issue(ahead, i);
+    }
+    for (int n = 0; cur.w < nwork; n++) {
+        const int bi = n % NB;
+        const uint32_t par = (uint32_t)(n / NB) & 1u;
+        if (threadIdx.x == 0) {
+            bulk_wait_read<NB - 1>();  // the store that last used band buffer bi has read it
+            s_ok = p3_wait_bounded(smem_u32(&bar[bi]), par, status);
+            if (!s_ok) {  // drain this CTA's copies in flight, then leave
+                for (int i = 0; i < NB; i++) mbar_wait_quiet(smem_u32(&bar[(n + i) % NB]), (uint32_t)((n + i) / NB) & 1u);
+                bulk_wait<0>();
+            }
+        }
+        __syncthreads();
+        if (!s_ok) return;
+        mbar_wait_quiet(smem_u32(&bar[bi]), par);  // complete already: acquires the tiles
+        const double *tiles = sm + bi * tile_dbl;
+        double *band = sm + NB * tile_dbl + bi * band_dbl;
+        const int p0 = perm3(cur.pi, 0), p1 = perm3(cur.pi, 1), p2 = perm3(cur.pi, 2);
+        // this thread's elements of every output tile: source offset in the tile, band offset, z
+        int soff[STEPS], boff[STEPS], zl[STEPS];
+#pragma unroll
+        for (int jj = 0; jj < STEPS; jj++) {
+            int u[3];
+            tile_element(lane, w * STEPS + jj, u);
+            auto sel = [&](int m) { return m == 0 ? u[0] : (m == 1 ? u[1] : u[2]); };
+            soff[jj] = (sel(p0) * TE + sel(p1)) * TE + sel(p2);
+            boff[jj] = (u[0] * TE + u[1]) * nv + u[2];
+            zl[jj] = u[2];
+        }
+        for (int zt = 0; zt < ntile; zt++) {
+            const double *tl = tiles + zt * TE3;
+            const int zrem = nv - zt * TE;  // elements of this tile inside the row
+#pragma unroll
+            for (int jj = 0; jj < STEPS; jj++)
+                if (zl[jj] < zrem) band[boff[jj] + zt * TE] = tl[soff[jj]];
+        }
+        fence_proxy_async_smem();  // the band becomes visible to the TMA store
+        __syncthreads();           // every thread is done with the source tiles
+        ahead = next_item(ahead.w + gridDim.x);
+        if (threadIdx.x == 0) {
+            if (ahead.w < nwork) issue(ahead, bi);  // buffer bi is free again
+            tma_store_5d(&dst, smem_u32(band), 0, cur.Y * TE, cur.X * TE, (int)cur.out, 0);
+            bulk_commit();
+        }
+        cur = next_item(cur.w + gridDim.x);
+    }
+    if (threadIdx.x == 0) bulk_wait<0>();
+}
+
 }  // namespace dcc
 
 extern "C" int dcc_t3_unpack_all(const double *t3, double *U, int64_t nocc, int64_t nvir, void *stream) {
@@ -1356,6 +1479,41 @@ extern "C" int dcc_t3_unpack_all(const double *t3, double *U, int64_t nocc, int6
     DCC_REQUIRE(t3 && U && t3 != U, DCC_ERR_NULL, "NULL or aliased buffer");
     const int64_t nblocks = nocc * (nocc + 1) * (nocc + 2) / 6;
     int ntile = (int)ceil_div(nvir, TE);
+    {
+        // band kernel: even nvir (16-byte rows), aligned buffers, box sides <= 256, shared memory
+        const size_t bsm = ((size_t)ntile * TE3 + (size_t)TE * TE * nvir) * sizeof(double);
+        EncodeTiledFn fn = encode_fn();
+        int *status = sym_status_word();
+        if (nvir % 2 == 0 && nvir <= 256 && bsm <= 200 * 1024 && ((uintptr_t)t3 & 15) == 0 &&
+            ((uintptr_t)U & 15) == 0 && nocc * nocc * nocc < (1ll << 31) && fn && status) {
+            const cuuint64_t nv = (cuuint64_t)nvir, n3 = nv * nv * nv;
+            const cuuint64_t sdims[5] = {nv, nv, nv, (cuuint64_t)nblocks, 1};
+            const cuuint64_t ddims[5] = {nv, nv, nv, (cuuint64_t)(nocc * nocc * nocc), 1};
+            const cuuint64_t sstr[4] = {nv * 8, nv * nv * 8, n3 * 8, n3 * 8 * (cuuint64_t)nblocks};
+            const cuuint64_t dstr[4] = {nv * 8, nv * nv * 8, n3 * 8, n3 * 8 * (cuuint64_t)(nocc * nocc * nocc)};
+            const cuuint32_t sbox[5] = {TE, TE, TE, 1, 1}, dbox[5] = {(cuuint32_t)nvir, TE, TE, 1, 1};
+            const cuuint32_t es[5] = {1, 1, 1, 1, 1};
+            CUtensorMap ms, md;
+            if (fn(&ms, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 5, const_cast<double *>(t3), sdims, sstr, sbox, es,
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS &&
+                fn(&md, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 5, U, ddims, dstr, dbox, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                   CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS) {
+                int dev = 0, nsm = 148;
+                if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+                const int64_t nwork = nblocks * 6 * (int64_t)ntile * ntile;
+                // one buffer and two CTAs of 8 warps per SM (two buffers in one CTA of 16 warps measured
+                // 1.9x slower at nocc = 10, nvir = 90)
+                const int64_t cap = (int64_t)nsm * (bsm <= 100 * 1024 ? 2 : 1);
+                const unsigned grid = (unsigned)(nwork < cap ? nwork : cap);
+                cudaFuncSetAttribute(k_unpack_band<1, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bsm);
+                k_unpack_band<1, 256><<<grid, 256, bsm, as_stream(stream)>>>(ms, md, nblocks, (int)nocc, (int)nvir, ntile,
+                                                                             status);
+                return launch_status("t3_unpack_all");
+            }
+        }
+    }
     int64_t ntri = (int64_t)ntile * (ntile + 1) * (ntile + 2) / 6;
     int64_t gy = (148 * 4 * 8 + ntri - 1) / ntri;
     gy = gy < 1 ? 1 : (gy > nblocks ? nblocks : gy);

@@ -343,16 +343,24 @@ def test_q_division_and_factor(C, oracle):
     assert np.array_equal(host(d), want2)
 
 
-@pytest.mark.parametrize("nocc,nvir", [(1, 3), (3, 5), (4, 9), (3, 17), (2, 4), (3, 10), (4, 18)])
-def test_unpack_all(C, oracle, nocc, nvir):
+@pytest.mark.parametrize("nocc,nvir,aligned", [(1, 3, True), (3, 5, True), (4, 9, True), (3, 17, True), (2, 4, True),
+                                               (3, 10, True), (4, 18, True), (1, 2, True), (5, 8, True), (2, 90, True),
+                                               (3, 10, False)])
+def test_unpack_all(C, oracle, nocc, nvir, aligned):
+    """Even nvir with 16-byte aligned buffers run the row-band TMA kernel, the rest the orbit-tile one."""
     from dcc import t3_residual
     rng = np.random.default_rng(13)
     n3 = nocc * (nocc + 1) * (nocc + 2) // 6
     t3 = rng.standard_normal((n3,) + (nvir,) * 3)
     loc = np.arange(n3, dtype=np.int64)
-    U = torch.full((nocc ** 3,) + (nvir,) * 3, 7.0, dtype=torch.float64, device="cuda")
+    shape = (nocc ** 3,) + (nvir,) * 3
+    if aligned:
+        U = torch.full(shape, 7.0, dtype=torch.float64, device="cuda")
+    else:
+        U = torch.full((int(np.prod(shape)) + 1,), 7.0, dtype=torch.float64, device="cuda")[1:].view(shape)
     t3_residual.unpack_all_(dev(t3), U, nocc, nvir)
     got = host(U)
     for q, (i, j, k) in enumerate(itertools.product(range(nocc), repeat=3)):
         want, rc = oracle.take_t3(t3, loc, i, j, k, nocc, nvir)
         assert rc == 0 and np.array_equal(got[q], want)
+    assert C[0].symmetrize_status() == 0
