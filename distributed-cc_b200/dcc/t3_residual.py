@@ -26,11 +26,12 @@ permutation, hence the halves.  A W_oooo without the pair symmetry keeps its
 antisymmetric part on the reference's own permutation set
 {identity, (i,k,j; a,c,b), (j,k,i; b,c,a)}.
 
-In mixed precision S is built by four split-precision tcgen05 GEMMs written
-straight into S's [i][j][k][a][b][c] layout (X; T2 and T5/2 as one GEMM over
-the concatenated contraction index; T1 reusing T2's U operand; the K = nocc^2
-W_oooo / F_oo part over a K-major split of U), and one gather kernel applies
-the symmetrization to S and Y.  W_vvvv.t3 (three strings, the dominant cost) are
+In mixed precision S is built by five split-precision tcgen05 GEMMs written
+straight into S's [i][j][k][a][b][c] layout (-Y first, which initializes S; X;
+T2 and T5/2 as one GEMM over the concatenated contraction index; T1 reusing
+T2's U operand; the K = nocc^2 W_oooo / F_oo part over a K-major split of U),
+and one gather kernel applies the symmetrization to S (the FP64 path keeps Y
+apart and gathers S and Y).  W_vvvv.t3 (three strings, the dominant cost) are
 three split-precision GEMMs that accumulate straight into r3; the three
 F_vv.t3 strings ride in them as extra terms of the W operand
 (contract.WvvvvT3).  The FP64 path runs F_vv.t3 as batched DGEMMs.
@@ -188,7 +189,7 @@ class T3Residual:
         full = (no ** 3, nv, nv, nv)
         self.S = torch.empty(full, dtype=f64, device=device)  # [i][j][k][a][b][c]
         self.U = torch.empty(full, dtype=f64, device=device) if with_oo else None
-        self.Y = torch.empty((no * no * nv, no * nv * nv), dtype=f64, device=device)  # [(i,j,a),(k,b,c)]
+        self.Y = None  # [(i,j,a),(k,b,c)], allocated by y_ (the FP64 path; the split path adds -Y into S)
         Ny = no * nv * nv
         self.y_strides = (no * nv * Ny, nv * Ny, nv * nv, Ny, nv, 1)
         self.Ganti = None
@@ -219,6 +220,8 @@ class T3Residual:
         """Y[(i,j,a),(k,b,c)] = sum_l W_vooo[a,l,i,j] t2[l,k,b,c] (K = nocc: bound by writing Y; a
         split GEMM in mixed precision, which writes Y at a higher rate than the FP64 DGEMM)."""
         no, nv = self.no, self.nv
+        if self.Y is None:
+            self.Y = torch.empty((no * no * nv, no * nv * nv), dtype=f64, device=self.dev)
         if self.precision == "fp64":
             A = d.W_vooo.permute(2, 3, 0, 1).reshape(no * no * nv, no)
             Bm = d.t2.permute(1, 2, 3, 0).reshape(no * nv * nv, no)
@@ -230,6 +233,16 @@ class T3Residual:
         self.yb.fill(d.t2, c.lin(1), c.lin(no * nv * nv))
         c.gemm_(self.ya, self.yb, self.Y, c.lin(no * nv * nv), c.lin(1), 1.0, 0.0, self.status)
         return self.Y
+
+    def _y_into_s(self, d):
+        """S = -Y in S's [i][j][k][a][b][c] layout (split path): rows (i,j,a), columns (k,b,c).  Y
+        then rides in S's permutation sum, and the gather reads one source instead of two."""
+        no, nv = self.no, self.nv
+        c = contract
+        self.ya.fill(d.W_vooo, c.three(no, nv, no, 1, no ** 3), c.lin(no * no))
+        self.yb.fill(d.t2, c.lin(1), c.lin(no * nv * nv))
+        c.gemm_(self.ya, self.yb, self.S, c.three(no, nv, no * no * nv ** 3, no * nv ** 3, nv * nv),
+                c.two(nv * nv, nv ** 3, 1), -1.0, 0.0, self.status)
 
     def s_(self, d, t3):
         """S (see the module docstring); U = unpacked t3 when the OO terms are on."""
@@ -266,9 +279,10 @@ class T3Residual:
         no, nv = self.no, self.nv
         S = self.S
         x = pl["x"]
+        self._y_into_s(d)  # writes S first
         self.xa.fill(d.W_vvvo, *x["a"][0][1:])
         self.xb.fill(d.t2, *x["b"][0][1:])
-        c.gemm_(self.xa, self.xb, S, *x["out"], x["alpha"], x["beta"], st)
+        c.gemm_(self.xa, self.xb, S, *x["out"], x["alpha"], 1.0, st)
         if not self.with_oo:
             return
         src = {"G2": (-0.5 * (d.W_ovov + d.W_ovvo.permute(0, 1, 3, 2))).permute(2, 1, 0, 3).contiguous(),
@@ -323,9 +337,12 @@ class T3Residual:
             r3 = torch.empty_like(t3)
         no, nv = self.no, self.nv
         S = self.s_(d, t3)
-        Y = self.y_(d)
-        perm_gather_(r3, d.ijk, nv, 0.0, [(S, 1.0, full_strides(no, nv), ALL_S3), (Y, -1.0, self.y_strides, ALL_S3)],
-                     nocc=no, status=self.gstatus)
+        if self.precision == "fp64":
+            Y = self.y_(d)
+            sources = [(S, 1.0, full_strides(no, nv), ALL_S3), (Y, -1.0, self.y_strides, ALL_S3)]
+        else:
+            sources = [(S, 1.0, full_strides(no, nv), ALL_S3)]  # S holds -Y already
+        perm_gather_(r3, d.ijk, nv, 0.0, sources, nocc=no, status=self.gstatus)
         if self.Ganti is not None:
             perm_gather_(r3, d.ijk, nv, 1.0, [(self.Ganti, 1.0, full_strides(no, nv), OOOO_SET)], nocc=no,
                          status=self.gstatus)
