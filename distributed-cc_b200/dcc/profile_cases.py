@@ -109,9 +109,8 @@ def case_gather(reps, nocc=10):
     d = synthetic.make_inputs(nocc, 90, seed=0)
     tr = t3_residual.T3Residual(nocc, 90, "bf16x3", with_oo=False)
     r3 = torch.empty_like(d.t3)
-    S, Y = tr.s_(d, d.t3), tr.y_(d)
-    src = [(S, 1.0, t3_residual.full_strides(nocc, 90), t3_residual.ALL_S3),
-           (Y, -1.0, tr.y_strides, t3_residual.ALL_S3)]
+    S = tr.s_(d, d.t3)  # the split path's S holds -W_vooo.t2 as well: one source
+    src = [(S, 1.0, t3_residual.full_strides(nocc, 90), t3_residual.ALL_S3)]
     for _ in range(reps):
         t3_residual.perm_gather_(r3, d.ijk, 90, 0.0, src, nocc=nocc)
     torch.cuda.synchronize()
