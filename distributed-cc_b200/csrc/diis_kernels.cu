@@ -8,7 +8,9 @@
 //            xprev = xnew;  seg_s = xnew / scale_s (the unpack of the caller's amplitudes)
 //
 // Both are HBM-bound single passes; the small B-matrix solve stays on the host
-// (numpy eigh / solve, as the reference).  Sums are per-CTA partials reduced in
+// (numpy eigh / solve, as the reference).  A slot may also live in pinned host memory
+// (the out-of-core slots of distr_cc/diis.py:25-103 kept in host RAM instead of files):
+// the kernels then read and write it over the host link through its unified address.  Sums are per-CTA partials reduced in
 // CTA order by a second kernel, so results do not depend on scheduling.
 #include <stdint.h>
 
@@ -146,6 +148,23 @@ using namespace dcc;
 
 extern "C" size_t dcc_diis_workspace_bytes(void) { return (size_t)DI_GRID * (DI_MAXS + 1) * sizeof(double); }
 
+// A slot pointer the kernels can dereference: device, managed or pinned (page-locked) host
+// memory.  Pageable host memory is refused before any launch.
+static int check_slot(const void *p, const char *what, int s) {
+    cudaPointerAttributes a;
+    cudaError_t e = cudaPointerGetAttributes(&a, p);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        set_error("%s %d: cudaPointerGetAttributes: %s", what, s, cudaGetErrorString(e));
+        return DCC_ERR_CUDA;
+    }
+    DCC_REQUIRE(a.type != cudaMemoryTypeUnregistered, DCC_ERR_UNSUPPORTED,
+                "%s %d is pageable host memory; slots must be device or pinned host memory", what, s);
+    DCC_REQUIRE(a.type != cudaMemoryTypeHost || a.devicePointer == p, DCC_ERR_UNSUPPORTED,
+                "%s %d: pinned host memory whose device address differs from its host address", what, s);
+    return DCC_OK;
+}
+
 extern "C" int dcc_diis_push(double *const *seg, const int64_t *seg_n, const double *seg_scale, int nseg,
                              double *xprev, double *x_slot, double *e_slot, const double *const *e_other, int nother,
                              double *dots, void *workspace, size_t workspace_bytes, void *stream) {
@@ -162,8 +181,10 @@ extern "C" int dcc_diis_push(double *const *seg, const int64_t *seg_n, const dou
     eo.n = nother;
     for (int s = 0; s < nother; s++) {
         DCC_REQUIRE(e_other[s], DCC_ERR_NULL, "other slot %d is NULL", s);
+        if ((rc = check_slot(e_other[s], "other error slot", s))) return rc;
         eo.p[s] = e_other[s];
     }
+    if ((rc = check_slot(x_slot, "x slot", 0)) || (rc = check_slot(e_slot, "error slot", 0))) return rc;
     cudaStream_t st = as_stream(stream);
     double *partial = (double *)workspace;
     k_diis_push<<<DI_GRID, DI_THREADS, 0, st>>>(g, n, xprev, x_slot, e_slot, eo, partial);
@@ -186,6 +207,7 @@ extern "C" int dcc_diis_combine(const double *const *xs, const double *coef, int
     p.n = nd;
     for (int s = 0; s < nd; s++) {
         DCC_REQUIRE(xs[s], DCC_ERR_NULL, "slot %d is NULL", s);
+        if ((rc = check_slot(xs[s], "x slot", s))) return rc;
         p.p[s] = xs[s];
         p.c[s] = coef[s];
     }

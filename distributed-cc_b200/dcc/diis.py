@@ -8,8 +8,14 @@ device memory; one update is two single passes over the vector
 (dcc_diis_push: error vector, slot copies and the new B-matrix row;
 dcc_diis_combine: extrapolation, update norm, and the unpack back into the
 segments, divided by their scales) plus the (space+1)^2 host solve the
-reference does with numpy.  Out-of-core scratch slots are not provided: at
-180 GB of HBM the slots of a 1.3 GB T3 vector fit on the device."""
+reference does with numpy.
+
+Out-of-core slots.  The reference can keep the slots from index scratch_start on in .npy
+files and read them back each update (distr_cc/diis.py:25-103).  Here those slots live in
+pinned host memory instead, and the two passes read and write them in place through their
+unified addresses, over the host link: HBM then holds only scratch_start (x, e) slot pairs.
+At 180 GB of HBM the slots of a 1.3 GB T3 vector fit on the device, so the default keeps
+every slot there."""
 from __future__ import annotations
 
 import ctypes
@@ -30,12 +36,20 @@ _combine = L.bind("dcc_diis_combine", [L.c_vp, L.c_vp, L.c_int, L.c_vp, L.c_vp, 
 class DIIS:
     """update(segments, scales) extrapolates in place; the first call only records x_prev."""
 
-    def __init__(self, space=6, device="cuda"):
+    def __init__(self, space=6, device="cuda", scratch_start=None):
         self.space = int(space)
         if self.space <= 0 or self.space > 16:
             raise ValueError("DIIS space must be in 1..16")
         self.dev = device
+        # Slots with index >= scratch_start in pinned host memory (clamped to 0..space as
+        # distr_cc/diis.py:44 does); None keeps every slot in HBM.
+        self.scratch_start = self.space if scratch_start is None else max(0, min(int(scratch_start), self.space))
         self.reset()
+
+    def _slot(self, idx, n):
+        if idx >= self.scratch_start:
+            return torch.empty(n, dtype=f64, pin_memory=True)
+        return torch.empty(n, dtype=f64, device=self.dev)
 
     def reset(self):
         self.xs, self.es = [None] * self.space, [None] * self.space
@@ -70,8 +84,8 @@ class DIIS:
             raise ValueError("DIIS vector length changed")
         h = self._head
         if self.xs[h] is None:
-            self.xs[h] = torch.empty(n, dtype=f64, device=self.dev)
-            self.es[h] = torch.empty(n, dtype=f64, device=self.dev)
+            self.xs[h] = self._slot(h, n)
+            self.es[h] = self._slot(h, n)
         others = [i for i in range(self.space) if self._filled[i] and i != h]
         optr = (ctypes.c_void_p * max(1, len(others)))(*[self.es[i].data_ptr() for i in others])
         L.check(_push(ptr, num, sc, len(segments), L.ptr(self._xprev), L.ptr(self.xs[h]), L.ptr(self.es[h]), optr,
