@@ -266,6 +266,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64-path comparison (profiling runs)")
     ap.add_argument("--no-q", action="store_true", help="skip the (Q) energy sample")
+    ap.add_argument("--no-t4", action="store_true", help="skip the T4 update at the N2 6-31G shape")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -480,6 +481,43 @@ def main():
         q_line["molecule_scale"] = ms_line
         del t3_abc
 
+    # One T4 update (compute_r4_tri with its OO batch, projector, divide, norms, t4 += r4) at the
+    # N2 6-31G shape (nocc=7, nvir=11, 161 stored blocks): eager and replayed as one CUDA graph.
+    t4_line = None
+    if not args.no_t4:
+        from dcc import graph as dgraph, synthetic as dsyn
+        t4_line = {"nocc": 7, "nvir": 11, "stored_blocks": 161}
+
+        def t4_ms(fn, n=5):
+            for _ in range(3):
+                fn()
+            barrier()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            for _ in range(n):
+                fn()
+            b.record()
+            barrier()
+            return ranks.max_over_ranks(a.elapsed_time(b), "cuda") / n
+
+        for prec in (args.precision, "fp64"):
+            it = dgraph.T4Iteration(dsyn.make_t4_inputs(7, 11, seed=3), prec)
+            t4_line[prec] = {"eager_ms": t4_ms(it.step)}
+            del it
+            gt4 = dgraph.T4IterationGraph(dgraph.T4Iteration(dsyn.make_t4_inputs(7, 11, seed=3), prec))
+            t4_line[prec]["graph_ms"] = t4_ms(gt4.replay)
+            del gt4
+        d4 = dsyn.make_t4_inputs(7, 11, seed=3)
+        r4s = {}
+        from dcc import t4_residual as dt4
+        for prec in (args.precision, "fp64"):
+            r4s[prec] = torch.zeros_like(d4.t4)
+            dt4.compute_r4_tri_(r4s[prec], d4.eris, d4.F_vv, d4.W_vvvo, d4.W_vooo, d4.W_vvvv, d4.W_oooo,
+                                d4.W_ovov, d4.t2, d4.t3, d4.t4, 7, prec, F_oo=d4.F_oo, W_ovvo=d4.W_ovvo)
+        t4_line["r4_max_rel_err_vs_fp64"] = float((r4s[args.precision] - r4s["fp64"]).abs().max()
+                                                  / r4s["fp64"].abs().max())
+        del d4, r4s
+
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
         dt, scale, kind, n = cpu_sample(2)
@@ -513,6 +551,7 @@ def main():
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "gpu_launches": launches_per_step * args.steps,
         "q_energy": q_line,
+        "t4_iteration": t4_line,
         "clocks": clk.summary(),
     }
     if rank == 0:

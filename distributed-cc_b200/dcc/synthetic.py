@@ -100,3 +100,38 @@ def to_numpy(d):
     for k, v in vars(d).items():
         setattr(out, k, v.detach().cpu().numpy() if isinstance(v, torch.Tensor) else v)
     return out
+
+
+def make_t4_inputs(nocc, nvir, seed=0, device="cuda"):
+    """Inputs of one T4 update (compute_r4_tri and the steps after it) with the
+    distributions above: the full ERI tensor <pq|rs> as the t1-dressed `eris`, the
+    physicist slices as the W intermediates, a full T3 [nocc^3, nvir^3] and the stored
+    T4 blocks [n4, nvir^4] (i<=j<=k<=l without the zero-rule blocks), both invariant
+    under simultaneous permutations of occupied and virtual indices (t3 N(0, 1e-3),
+    t4 N(0, 1e-4) before symmetrisation); `ijkl` lists the stored quadruples (int32)."""
+    from .t4_residual import stored_quadruples
+    d = make_inputs(nocc, nvir, seed=seed, device=device, with_t3=False)
+    gen = torch.Generator(device=device)
+    gen.manual_seed(seed + 1)
+    no, nv = nocc, nvir
+    nmo = no + nv
+    eri = _sym8(torch.randn(nmo, nmo, nmo, nmo, dtype=f64, device=device, generator=gen) * 0.1)
+    d.eris = eri.permute(0, 2, 1, 3).contiguous()
+    del eri
+    full = torch.randn((no,) * 3 + (nv,) * 3, dtype=f64, device=device, generator=gen) * 1e-3
+    t3 = torch.zeros_like(full)
+    for p in itertools.permutations(range(3)):
+        t3 += full.permute(p + tuple(3 + x for x in p))
+    d.t3 = (t3 / 6.0).contiguous()
+    del full, t3
+    full = torch.randn((no,) * 4 + (nv,) * 4, dtype=f64, device=device, generator=gen) * 1e-4
+    t4 = torch.zeros_like(full)
+    for p in itertools.permutations(range(4)):
+        t4 += full.permute(p + tuple(4 + x for x in p))
+    del full
+    quads = stored_quadruples(no)
+    rows = torch.tensor([((i * no + j) * no + k) * no + l for i, j, k, l in quads], device=device)
+    d.t4 = (t4.view(no ** 4, -1)[rows] / 24.0).view((len(quads),) + (nv,) * 4).contiguous()
+    del t4
+    d.ijkl = torch.tensor(quads, dtype=torch.int32, device=device)
+    return d

@@ -67,28 +67,52 @@ def stored_quadruples(nocc):
             for l in range(k, nocc) if not (i == j == k or j == k == l)]
 
 
+_DEV_CACHE = {}
+
+
+def _cached(key, device, build):
+    """Index tensors built once per (key, device) and kept on the device, so that a step
+    makes no host-to-device copy (a requirement of CUDA-graph capture)."""
+    k = key + (str(torch.device(device)),)
+    if k not in _DEV_CACHE:
+        _DEV_CACHE[k] = build()
+    return _DEV_CACHE[k]
+
+
+def _unpack_groups(nocc, device):
+    """[(axis ranks, ordered-tuple rows, stored-block rows)] grouped by the virtual-axis
+    permutation that takes the stored block to the ordering."""
+    def build():
+        index = {q: n for n, q in enumerate(stored_quadruples(nocc))}
+        groups = {}
+        for o in itertools.product(range(nocc), repeat=4):
+            order = sorted(range(4), key=lambda p: (o[p], p))
+            can = tuple(o[p] for p in order)
+            if can not in index:
+                continue
+            rank = tuple(order.index(p) for p in range(4))
+            flat = ((o[0] * nocc + o[1]) * nocc + o[2]) * nocc + o[3]
+            groups.setdefault(rank, ([], []))
+            groups[rank][0].append(flat)
+            groups[rank][1].append(index[can])
+        return [(rank, torch.tensor(d, device=device), torch.tensor(s, device=device))
+                for rank, (d, s) in groups.items()]
+    return _cached(("unpack", nocc), device, build)
+
+
+def _stored_rows(nocc, device):
+    """Row of each stored block in the [nocc^4] ordered space."""
+    return _cached(("stored", nocc), device, lambda: torch.tensor(
+        [((i * nocc + j) * nocc + k) * nocc + l for i, j, k, l in stored_quadruples(nocc)], device=device))
+
+
 def unpack_all_orderings(t4, nocc):
     """T[o] for every ordered quadruple o: the stored canonical block with its virtual
     axes permuted (axis p of the ordering is axis rank(p) of the canonical block, stable
     sort of the occupied values); zero where the canonical block is not stored."""
     nv = t4.shape[1]
-    quads = stored_quadruples(nocc)
-    index = {q: n for n, q in enumerate(quads)}
     out = torch.zeros((nocc ** 4,) + (nv,) * 4, dtype=t4.dtype, device=t4.device)
-    groups = {}
-    for o in itertools.product(range(nocc), repeat=4):
-        order = sorted(range(4), key=lambda p: (o[p], p))
-        can = tuple(o[p] for p in order)
-        if can not in index:
-            continue
-        rank = tuple(order.index(p) for p in range(4))
-        flat = ((o[0] * nocc + o[1]) * nocc + o[2]) * nocc + o[3]
-        groups.setdefault(rank, ([], []))
-        groups[rank][0].append(flat)
-        groups[rank][1].append(index[can])
-    for rank, (dst, src) in groups.items():
-        d = torch.tensor(dst, device=t4.device)
-        s = torch.tensor(src, device=t4.device)
+    for rank, d, s in _unpack_groups(nocc, t4.device):
         out[d] = t4[s].permute(0, *(1 + r for r in rank))
     return out.view((nocc,) * 4 + (nv,) * 4)
 
@@ -206,8 +230,9 @@ def build_intermediates(eris, W_oooo, W_ovov, W_vvvv, t2, t3, t3p, t4, nocc, spi
     # pair (x <= y): T4 part of orderings (x, y) plus (y, x) with b, c swapped, then the replicated terms
     Wp = Word + Word.permute(1, 0, 2, 4, 3, 5)
     Wp = Wp + 0.5 * e('abef,xyfc->xyabce', W_vvvv, t2) + 0.5 * e('acef,yxfb->xyabce', W_vvvv, t2)
-    lo = torch.tensor([min(x, y) for x in range(nocc) for y in range(nocc)], device=t2.device)
-    hi = torch.tensor([max(x, y) for x in range(nocc) for y in range(nocc)], device=t2.device)
+    lo, hi = _cached(("pair", nocc), t2.device, lambda: (
+        torch.tensor([min(x, y) for x in range(nocc) for y in range(nocc)], device=t2.device),
+        torch.tensor([max(x, y) for x in range(nocc) for y in range(nocc)], device=t2.device)))
     W["W_oovvvv"] = Wp[lo, hi].view(Wp.shape)
     return W
 
@@ -241,9 +266,7 @@ def compute_r4_tri_(r4, eris, F_vv, W_vvvo, W_vooo, W_vvvv, W_oooo, W_ovov, t2, 
         sw, st = sub.split(",")
         subs = _slots(wn, ws, sw) + "," + _slots(tn, ts, st) + "->ijklabcd"
         _einsum(kind, subs, W[wn], T[tn], R, al)
-    quads = stored_quadruples(nocc)
-    idx = torch.tensor([((i * nocc + j) * nocc + k) * nocc + l for i, j, k, l in quads], device=t3.device)
-    r4.copy_(R.view(nocc ** 4, -1)[idx].view(r4.shape))
+    r4.copy_(R.view(nocc ** 4, -1)[_stored_rows(nocc, t3.device)].view(r4.shape))
     del R
     dense_vvvv_fvv_(r4, t4, W_vvvv, F_vv, precision)
     if F_oo is not None:
@@ -374,16 +397,15 @@ def oo_batch_(r4, t4, F_oo, W_oooo, W_ovvo, W_ovov, nocc, forms=None):
           + e('mnil,mjknabcd->ijklabcd', W_oooo, T) + e('mnjk,imnlabcd->ijklabcd', W_oooo, T)
           + e('mnjl,imknabcd->ijklabcd', W_oooo, T) + e('mnkl,ijmnabcd->ijklabcd', W_oooo, T))
     del T
-    quads = stored_quadruples(nocc)
-    idx = torch.tensor([((i * nocc + j) * nocc + k) * nocc + l for i, j, k, l in quads], device=dev)
-    r4 += R.view(nocc ** 4, -1)[idx].view(r4.shape)
+    r4 += R.view(nocc ** 4, -1)[_stored_rows(nocc, dev)].view(r4.shape)
     del R
     # W_ovov / W_voov strings, batched over the (source, output) pairs of each group and case
     T3, V = forms(t4)
     src = {"T": t4, "T3": T3, "V0": V[0], "V1": V[1], "V2": V[2], "V3": V[3]}
     W_voov = W_ovvo.permute(1, 0, 3, 2).contiguous()
-    for (g, c), (si, ti, m, x) in oo_pairs(nocc).items():
-        si, ti, m, x = (torch.tensor(v, device=dev) for v in (si, ti, m, x))
+    pairs = _cached(("oo_pairs", nocc), dev, lambda: [
+        (gc, tuple(torch.tensor(v, device=dev) for v in lists)) for gc, lists in oo_pairs(nocc).items()])
+    for (g, c), (si, ti, m, x) in pairs:
         Wo = W_ovov[m, :, x, :]   # [P, a, e] = W_ovov[m, :, x, :]
         Wv = W_voov[:, m, x, :].permute(1, 0, 2)  # [P, a, e] = W_voov[:, m, x, :]
         for wn, s, al, form in _OO_TABLE[g][c]:
