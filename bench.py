@@ -344,6 +344,10 @@ def main():
         contract.gemm_ = orig_gemm
         return ranks.max_over_ranks(e0.elapsed_time(e1), "cuda")
 
+    # pipeline shape of the W_vvvv.t3 GEMMs chosen by the autotuner (untimed, like planning)
+    from dcc import autotune
+    tuned = mixed.tune(d, t3w)
+
     # this library's kernels per mixed step, counted on one untimed step
     from torch.profiler import profile, ProfilerActivity
     with profile(activities=[ProfilerActivity.CUDA]) as prof:
@@ -540,6 +544,10 @@ def main():
         "speedup_vs_fp64": (ms_fp64 / fp64_steps) / (ms_mixed / args.steps) if ms_fp64 else None,
         "r3_max_rel_err_vs_fp64": rel_err, "iteration_energy_error": energy_proxy, "device_status_ok": ok,
         "cuda_graph_ms_per_step": graph_ms, "cuda_graph_status_ok": graph_ok,
+        "wvvvv_gemm_pipeline": None if tuned is None else {
+            "kb_bytes": tuned[0], "stages": tuned[1], "group_m": tuned[2], "chosen_by": "dcc.autotune",
+            "candidates_ms": {"%d/%d/%d" % c: round(ms, 4) for c, ms in
+                              (autotune.timings(mixed.wvvvv.key()) or {}).items()}},
         "roofline": {"kernel": "dcc::k_gemm_split3<0> (W_vvvv.t3 string)", "bound": "tensor",
                      "achieved": achieved, "peak": peak_useful, "unit": "TFLOP/s",
                      "frac": (achieved / peak_useful) if achieved else None,

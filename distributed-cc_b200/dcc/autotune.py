@@ -20,6 +20,7 @@ _get = L.bind("dcc_gemm_get_config", [L.c_vp, L.c_vp, L.c_vp])
 PIPELINES = [(128, 2), (64, 4), (64, 3), (32, 8)]
 GROUPS = [8, 16, 32]
 _cache = {}
+_times = {}
 
 
 def set_config(kb_bytes, stages, group_m):
@@ -36,27 +37,40 @@ def candidates():
     return [(kb, st, g) for kb, st in PIPELINES for g in GROUPS]
 
 
-def tune(key, run, reps=2, cands=None):
-    """Time run() under each candidate configuration; keep and return the fastest."""
+def tune(key, run, reps=2, cands=None, rounds=3):
+    """Time run() under each candidate configuration; keep and return the fastest.
+
+    Every candidate runs once untimed, then `rounds` rounds time each candidate over `reps`
+    runs, the order reversed every other round, and a candidate's time is its best round.
+    Under the power cap the SM clock drifts during tuning; interleaving the candidates
+    spreads that drift over all of them instead of favouring the first ones timed."""
     if key in _cache:
         set_config(*_cache[key])
         return _cache[key]
-    best, best_ms = None, float("inf")
-    for cfg in (cands or candidates()):
+    cands = list(cands or candidates())
+    for cfg in cands:
         set_config(*cfg)
         run()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
-        for _ in range(reps):
-            run()
-        e1.record()
-        torch.cuda.synchronize()
-        ms = e0.elapsed_time(e1) / reps
-        if ms < best_ms:
-            best, best_ms = cfg, ms
-    _cache[key] = best
+    best_ms = {cfg: float("inf") for cfg in cands}
+    for r in range(rounds):
+        for cfg in (cands if r % 2 == 0 else cands[::-1]):
+            set_config(*cfg)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for _ in range(reps):
+                run()
+            e1.record()
+            torch.cuda.synchronize()
+            best_ms[cfg] = min(best_ms[cfg], e0.elapsed_time(e1) / reps)
+    best = min(cands, key=lambda c: best_ms[c])
+    _cache[key], _times[key] = best, best_ms
     set_config(*best)
     return best
+
+
+def timings(key):
+    """{candidate: best ms per run()} measured when `key` was tuned (None if it was not)."""
+    return _times.get(key)
 
 
 def use(key):

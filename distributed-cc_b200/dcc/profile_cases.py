@@ -167,9 +167,20 @@ def case_qgroup(reps, nocc=10):
     assert q.status_ok()
 
 
+def case_t4(reps, kind="bf16x3"):
+    """T4 updates at the N2 6-31G shape (nocc=7, nvir=11, 161 stored blocks): compute_r4_tri
+    with its OO batch, projector, divide, norms, t4 += r4 (dcc.graph.T4Iteration), eager."""
+    from dcc import graph, synthetic
+    it = graph.T4Iteration(synthetic.make_t4_inputs(7, 11, seed=3), kind)
+    for _ in range(reps):
+        it.step()
+    torch.cuda.synchronize()
+
+
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("case", choices=["gemm", "p3", "update", "q", "gather", "xgemm", "oogemm", "unpack", "qgroup"])
+    ap.add_argument("case", choices=["gemm", "p3", "update", "q", "gather", "xgemm", "oogemm", "unpack", "qgroup",
+                                         "t4"])
     ap.add_argument("--kind", default="bf16x3")
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--nocc", type=int, default=None, help="occupied orbitals (xgemm, oogemm, gather, unpack)")
@@ -184,6 +195,8 @@ def main():
         case_p3(a.reps, a.nvir, a.op, a.time)
     elif a.case == "update":
         case_update(a.reps)
+    elif a.case == "t4":
+        case_t4(a.reps, a.kind)
     elif a.case in ("gather", "xgemm", "oogemm", "unpack", "qgroup"):
         fn = {"gather": case_gather, "xgemm": case_xgemm, "oogemm": case_oogemm, "unpack": case_unpack,
               "qgroup": case_qgroup}[a.case]

@@ -328,6 +328,13 @@ class T3Residual:
             return contract.wvvvv_t3_fp64_(r3, d.W_vvvv, t3)
         return self.wvvvv(r3, d.W_vvvv, t3, F=d.F_vv)
 
+    def tune(self, d, t3):
+        """Autotune the pipeline shape of the W_vvvv.t3 GEMMs (the split precisions; the
+        FP64 path has nothing to tune).  Returns the chosen (k-block bytes, stages, group)."""
+        if self.precision == "fp64":
+            return None
+        return self.wvvvv.tune(torch.empty_like(t3), d.W_vvvv, t3, F=d.F_vv)
+
     def compute(self, d, t3, r3=None, wvvvv_ready=None):
         """r3 = compute_r3_tri for canonical t3 (the OO batch terms included when with_oo).
 

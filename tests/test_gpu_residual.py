@@ -102,3 +102,27 @@ def test_tma_gather_matches_cp_async_gather(mods, nvir, beta):
         torch.cuda.synchronize()
         assert int(st.item()) == 0
         assert torch.equal(a, b)
+
+
+@pytest.mark.parametrize("precision", ["bf16x3", "tf32x3"])
+def test_autotuned_wvvvv_gemms(mods, precision):
+    """T3Residual.tune times every pipeline candidate of the W_vvvv.t3 GEMMs (K = nvir^2 >
+    4096 takes the configurable pipeline) and keeps the fastest; the tuned residual still
+    matches the FP64 path within the split tolerance, and t3 is not modified by tuning."""
+    syn, tr, _ = mods
+    from dcc import autotune
+    old = autotune.get_config()
+    try:
+        d = syn.make_inputs(2, 72, seed=7)
+        t3_0 = d.t3.clone()
+        res = tr.T3Residual(2, 72, precision, with_oo=True)
+        cfg = res.tune(d, d.t3)
+        assert cfg in autotune.candidates() and autotune.get_config() == cfg
+        assert torch.equal(d.t3, t3_0)
+        autotune.set_config(*old)  # the residual re-applies its tuned shape itself
+        got = res.compute(d, d.t3)
+        assert autotune.get_config() == cfg and res.status_ok()
+        want = tr.T3Residual(2, 72, "fp64", with_oo=True).compute(d, d.t3)
+        assert float((got - want).abs().max() / want.abs().max()) < TOL[precision]
+    finally:
+        autotune.set_config(*old)
