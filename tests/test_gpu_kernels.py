@@ -33,7 +33,7 @@ def C():
     return _c_rccsdt, _c_rccsdt_q, _c_rccsdtq
 
 
-@pytest.mark.parametrize("nvir", [1, 2, 5, 8, 10, 13, 17, 18, 90])
+@pytest.mark.parametrize("nvir", [1, 2, 5, 8, 10, 13, 17, 18, 30, 50, 90])
 @pytest.mark.parametrize("pattern", P3)
 def test_t3_spin_sum(C, oracle, nvir, pattern):
     c3 = C[0]
@@ -57,7 +57,7 @@ def test_t3_spin_sum(C, oracle, nvir, pattern):
     assert c3.symmetrize_status() == 0
 
 
-@pytest.mark.parametrize("nvir", [2, 10, 90])
+@pytest.mark.parametrize("nvir", [2, 10, 30, 90])
 def test_orbit_roundtrip_is_identity(C, nvir):
     """The diagnostic tile round trip of the spin-summation kernel leaves every block unchanged."""
     c3 = C[0]
@@ -68,7 +68,7 @@ def test_orbit_roundtrip_is_identity(C, nvir):
     assert c3.symmetrize_status() == 0
 
 
-@pytest.mark.parametrize("nvir", [1, 2, 3, 8, 10, 11, 18, 90])
+@pytest.mark.parametrize("nvir", [1, 2, 3, 8, 10, 11, 18, 30, 50, 90])
 @pytest.mark.parametrize("aligned", [True, False])
 def test_triple_sym_transpose_add(C, oracle, nvir, aligned):
     """Even nvir with 16-byte aligned buffers run the TMA orbit-tile kernel, the rest the cp.async one."""
