@@ -244,12 +244,16 @@ class T3Residual:
         c.gemm_(self.ya, self.yb, self.S, c.three(no, nv, no * no * nv ** 3, no * nv ** 3, nv * nv),
                 c.two(nv * nv, nv ** 3, 1), -1.0, 0.0, self.status)
 
-    def s_(self, d, t3):
-        """S (see the module docstring); U = unpacked t3 when the OO terms are on."""
+    def s_(self, d, t3, inputs_ready=None):
+        """S (see the module docstring); U = unpacked t3 when the OO terms are on.  The unpack
+        reads only t3, so it runs before the wait on `inputs_ready` (an optional CUDA event that
+        marks the arrival of d's tensors)."""
         no, nv = self.no, self.nv
         S = self.S
         if self.with_oo:
             unpack_all_(t3, self.U, no, nv)
+        if inputs_ready is not None:
+            torch.cuda.current_stream().wait_event(inputs_ready)
         if self.precision == "fp64":
             self._s_fp64(d)
         else:
@@ -335,15 +339,17 @@ class T3Residual:
             return None
         return self.wvvvv.tune(torch.empty_like(t3), d.W_vvvv, t3, F=d.F_vv)
 
-    def compute(self, d, t3, r3=None, wvvvv_ready=None):
+    def compute(self, d, t3, r3=None, wvvvv_ready=None, inputs_ready=None):
         """r3 = compute_r3_tri for canonical t3 (the OO batch terms included when with_oo).
 
         wvvvv_ready: optional CUDA event the W_vvvv.t3 part waits for, so a caller can
-        stream W_vvvv to the device while the other terms run."""
+        stream W_vvvv to the device while the other terms run.  inputs_ready: optional CUDA
+        event for d's other tensors, waited for after the unpack of t3 (which needs none of
+        them), so their upload overlaps it."""
         if r3 is None:
             r3 = torch.empty_like(t3)
         no, nv = self.no, self.nv
-        S = self.s_(d, t3)
+        S = self.s_(d, t3, inputs_ready)
         if self.precision == "fp64":
             Y = self.y_(d)
             sources = [(S, 1.0, full_strides(no, nv), ALL_S3), (Y, -1.0, self.y_strides, ALL_S3)]

@@ -126,3 +126,33 @@ def test_autotuned_wvvvv_gemms(mods, precision):
         assert float((got - want).abs().max() / want.abs().max()) < TOL[precision]
     finally:
         autotune.set_config(*old)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "bf16x3"])
+def test_inputs_uploaded_during_the_unpack(mods, precision):
+    """compute(..., inputs_ready=event): the intermediates arrive on a copy stream from pinned
+    host memory while the unpack of t3 runs; the residual equals the one with resident inputs
+    bit for bit (same kernels in the same order)."""
+    syn, tr, _ = mods
+    d = syn.make_inputs(4, 10, seed=21)
+    res = tr.T3Residual(4, 10, precision, with_oo=True)
+    want = res.compute(d, d.t3).clone()
+    names = ("t2", "W_vvvo", "W_vooo", "W_vvvv", "W_ovov", "W_ovvo", "W_oooo", "F_vv", "F_oo")
+    host = {k: getattr(d, k).cpu().pin_memory() for k in names}
+
+    class Dev:
+        pass
+
+    dd = Dev()
+    dd.ijk = d.ijk
+    for k, v in host.items():
+        setattr(dd, k, torch.full(v.shape, float("nan"), dtype=v.dtype, device="cuda"))
+    torch.cuda.synchronize()
+    side, ready = torch.cuda.Stream(), torch.cuda.Event()
+    with torch.cuda.stream(side):
+        for k, v in host.items():
+            getattr(dd, k).copy_(v, non_blocking=True)
+        ready.record(side)
+    got = res.compute(dd, d.t3, inputs_ready=ready)
+    torch.cuda.synchronize()
+    assert torch.equal(got, want) and res.status_ok()
