@@ -35,3 +35,27 @@ def test_device_checkpoint_round_trip(kind, nocc, nvir, distribution, nranks, tm
     _, z = load(str(tmp_path / "d_"), device="cuda", out=out)
     assert z is out and torch.equal(out, x)
     os.remove(tmp_path / "ref.npy")
+
+
+def test_restart_from_checkpoint_continues_the_iteration(tmp_path):
+    """The device counterpart of the reference's restart test (tests/test_rccsdt.py,
+    _test_restart): two T3 iterations in a row equal one iteration, a checkpoint written and
+    read back (here as a 3-rank round_robin checkpoint), and the second iteration."""
+    from dcc import synthetic, t3_residual
+    nocc, nvir = 4, 12
+    d = synthetic.make_inputs(nocc, nvir, seed=5)
+    res = t3_residual.T3Residual(nocc, nvir, "fp64", with_oo=True)
+    t3a = d.t3.clone()
+    for _ in range(2):
+        r3 = res.compute(d, t3a)
+        t3_residual.update_t3_(t3a, r3, d)
+    t3b = d.t3.clone()
+    r3 = res.compute(d, t3b)
+    t3_residual.update_t3_(t3b, r3, d)
+    C.save_t3(t3b, str(tmp_path / "run_"), nocc, nvir, distribution="round_robin", nranks=3)
+    del t3b
+    _, t3c = C.load_t3(str(tmp_path / "run_"), device="cuda")
+    r3 = res.compute(d, t3c)
+    t3_residual.update_t3_(t3c, r3, d)
+    torch.cuda.synchronize()
+    assert torch.equal(t3c, t3a)
