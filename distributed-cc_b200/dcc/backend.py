@@ -154,12 +154,12 @@ def intermediates_t3_add_t3_tri(mycc, imds, t3):
 
 
 def q_kernel(mycc, eris=None, tamps=None, blksize=4, comm=None, job_idx=0, n_jobs=1, log_redistribution=False):
-    """(e_q_bracket, e_q_paren) of distr_cc/rccsdt_q.py:227 on the GPU, one rank, all tasks."""
+    """(e_q_bracket, e_q_paren) of distr_cc/rccsdt_q.py:227 on the GPU, one rank: every task,
+    or with n_jobs > 1 the tasks of job `job_idx` (the reference's contiguous slice of its task
+    order, distr_cc/rccsdt_q.py:359-366), whose energies add up over the jobs."""
     from . import rccsdt_q
     if comm is not None and int(comm.Get_size()) != 1:
         raise RuntimeError('einsum backend "cuda" runs on one rank')
-    if n_jobs != 1 or job_idx != 0:
-        raise NotImplementedError("job splitting is a multi-process feature of the reference")
     dev = getattr(mycc, "dcc_device", "cuda")
     nocc, nmo = mycc.nocc, mycc.nmo
     if eris is None:
@@ -176,7 +176,7 @@ def q_kernel(mycc, eris=None, tamps=None, blksize=4, comm=None, job_idx=0, n_job
     t2q = t2 if t2.shape == (nvir, nvir, nocc, nocc) else np.ascontiguousarray(np.transpose(t2, (2, 3, 0, 1)))
     e = np.asarray(eris.mo_energy)
     return rccsdt_q.q_energy(er, _dev(t2q, dev), _dev(t3_local, dev), _dev(e[:nocc], dev), _dev(e[nocc:], dev),
-                             nocc, nvir, blksize, precision_of(mycc))
+                             nocc, nvir, blksize, precision_of(mycc), job_idx=job_idx, n_jobs=n_jobs)
 
 
 # imds fields compute_r4_tri releases on return (distr_cc/rccsdtq.py:899-1349)

@@ -68,6 +68,28 @@ def groups(nvir, blksize):
     return out
 
 
+def job_d_ranges(nvir, blksize, job_idx=0, n_jobs=1):
+    """{(a0, a1, b0, b1, c0, c1): (d0, d1)}: the tasks of job `job_idx` of `n_jobs` as group d
+    ranges.  A job takes the contiguous slice [j*ceil(T/n), min((j+1)*ceil(T/n), T)) of the
+    canonical task order (distr_cc/rccsdt_q.py:359-366); that order runs d-blocks outermost, so
+    within one (a, b, c) group a job's d-blocks are consecutive."""
+    if n_jobs < 1 or not 0 <= job_idx < n_jobs:
+        raise ValueError("job_idx must be in [0, n_jobs)")
+    tasks = task_list(nvir, blksize)
+    per = (len(tasks) + n_jobs - 1) // n_jobs
+    start, end = job_idx * per, min(job_idx * per + per, len(tasks))
+    out, nblk = {}, {}
+    for t in tasks[start:end]:
+        key = (t[0], t[1], t[3], t[4], t[6], t[7])
+        d0, d1 = out.get(key, (t[9], t[10]))
+        out[key] = (min(d0, t[9]), max(d1, t[10]))
+        nblk[key] = nblk.get(key, 0) + 1
+    for key, (d0, d1) in out.items():
+        if len(prange(d0, d1, blksize)) != nblk[key]:
+            raise AssertionError("d-blocks of group %s are not consecutive in job %d" % (key, job_idx))
+    return out
+
+
 # ----------------------------------------------------------------------------
 # The einsums of one group as data.  Range letters: A = [a0, a0+ba),
 # B = [b0, b0+bb), C = [c0, c0+bc), D = [d0, d0+dn) (d0 = c0, dn = nvir - c0);
@@ -337,8 +359,17 @@ class QEnergy:
             out[s] = t
         return out
 
-    def _chunks(self, c0):
-        return [(c0, self.nv)] if self.kind is None else prange(c0, self.nv, self.dchunk)
+    def _chunks(self, d0, d1=None):
+        d1 = self.nv if d1 is None else d1
+        return [(d0, d1)] if self.kind is None else prange(d0, d1, self.dchunk)
+
+    def _work(self, group_list, d_ranges):
+        """(group, d0, d1) to run: every group's tasks (d from the c-block on), or those of
+        d_ranges (job_d_ranges) when given."""
+        gl = group_list if group_list is not None else groups(self.nv, self.blk)
+        if d_ranges is None:
+            return [(g, g[4], self.nv) for g in gl]
+        return [(g,) + tuple(d_ranges[g]) for g in gl if g in d_ranges]
 
     def _transposed(self, er, t2):
         if self._vvooT is None:
@@ -461,13 +492,14 @@ class QEnergy:
             })
         return plan
 
-    def prepare(self, group_list=None):
+    def prepare(self, group_list=None, d_ranges=None):
         """Build the grouped tables of every group shape in group_list (default: all
-        groups) ahead of run(), so no planning happens inside a timed region."""
+        groups; d_ranges as in run) ahead of run(), so no planning happens inside a timed
+        region."""
         if self.kind is None:
             return
-        for (a0, a1, b0, b1, c0, c1) in (group_list if group_list is not None else groups(self.nv, self.blk)):
-            for d0, d1 in self._chunks(c0):
+        for (a0, a1, b0, b1, c0, c1), dlo, dhi in self._work(group_list, d_ranges):
+            for d0, d1 in self._chunks(dlo, dhi):
                 sig = (a1 - a0, b1 - b0, c1 - c0, d1 - d0)
                 if sig not in self._plans:
                     self._plans[sig] = self._plan(sig)
@@ -492,16 +524,17 @@ class QEnergy:
             ph["gemm"].run(self.status)
         return plan["out"]["z"], plan["out"]["x"]
 
-    def run(self, er, t2, t3_abc, e_occ, e_vir, group_list=None):
-        """Accumulate [Q] and (Q) over the tasks of `group_list` (default: all groups).
-        Returns the device tensor [e_bracket, e_paren]."""
+    def run(self, er, t2, t3_abc, e_occ, e_vir, group_list=None, d_ranges=None):
+        """Accumulate [Q] and (Q) over the tasks of `group_list` (default: all groups), or,
+        with d_ranges ({group: (d0, d1)}, job_d_ranges), over the listed groups' d ranges
+        only.  Returns the device tensor [e_bracket, e_paren]."""
         nv, no = self.nv, self.no
         er = {k: v.contiguous() for k, v in er.items()}
         t2 = t2.contiguous()
         vvooT, t2T = self._transposed(er, t2)
-        for (a0, a1, b0, b1, c0, c1) in (group_list if group_list is not None else groups(nv, self.blk)):
+        for (a0, a1, b0, b1, c0, c1), dlo, dhi in self._work(group_list, d_ranges):
             slabs = self._slabs(t3_abc, (a0, a1, b0, b1, c0, c1, c0, nv), which=("Sab", "Sac", "Sbc"))
-            for d0, d1 in self._chunks(c0):
+            for d0, d1 in self._chunks(dlo, dhi):
                 r = (a0, a1, b0, b1, c0, c1, d0, d1)
                 self._slabs(t3_abc, r, which=("Sad", "Sbd", "Scd"), out=slabs)
                 if self.kind is None:
@@ -512,11 +545,14 @@ class QEnergy:
         return self.out
 
 
-def q_energy(er, t2, t3_ijk, e_occ, e_vir, nocc, nvir, blksize=4, precision="fp64", group_list=None):
-    """(e_bracket, e_paren) from canonical IJK-ordered T3 on the device."""
+def q_energy(er, t2, t3_ijk, e_occ, e_vir, nocc, nvir, blksize=4, precision="fp64", group_list=None, job_idx=0,
+             n_jobs=1):
+    """(e_bracket, e_paren) from canonical IJK-ordered T3 on the device; with n_jobs > 1, the
+    share of job `job_idx` (the energies of all jobs add up to the full ones)."""
     t3_abc = _c_rccsdt.redistribute_ijk_to_abc(t3_ijk, nocc, nvir)
     q = QEnergy(nocc, nvir, blksize, precision, device=t3_ijk.device)
-    out = q.run(er, t2, t3_abc, e_occ, e_vir, group_list)
+    d_ranges = None if n_jobs == 1 else job_d_ranges(nvir, blksize, job_idx, n_jobs)
+    out = q.run(er, t2, t3_abc, e_occ, e_vir, group_list, d_ranges)
     eb, ep = float(out[0]), float(out[1])
     if not q.status_ok():
         raise RuntimeError("split GEMM reported a timeout")

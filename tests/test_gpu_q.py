@@ -97,3 +97,20 @@ def test_q_energy_split_microhartree(mods, precision):
     assert 1e-4 < abs(want[1]) < 1e-2
     assert abs(got[0] - want[0]) < 1e-6, (got, want)
     assert abs(got[1] - want[1]) < 1e-6, (got, want)
+
+
+@pytest.mark.parametrize("precision,n_jobs", [("fp64", 3), ("fp64", 7), ("bf16x3", 4)])
+def test_q_energy_split_jobs(mods, oracle, precision, n_jobs):
+    """Job splitting as the reference's test_split_jobs (tests/test_rccsdt_q.py): the energies
+    of jobs 0..n_jobs-1 add up to the oracle's full energies (FP64 1e-10; split 1e-4)."""
+    gq, q_ref = mods
+    no, nv, blk = 3, 9, 2
+    er, t2, T, eo, ev = _inputs(no, nv, 23)
+    want = q_ref.q_energy_ref(er, t2, T, eo, ev, blk, oracle)
+    d = _device(er, t2, T, eo, ev, no)
+    got = np.zeros(2)
+    for j in range(n_jobs):
+        got += gq.q_energy(d[0], d[1], d[2], d[3], d[4], no, nv, blk, precision, job_idx=j, n_jobs=n_jobs)
+    tol = 1e-10 if precision == "fp64" else 1e-4
+    assert abs(got[0] - want[0]) <= tol * abs(want[0])
+    assert abs(got[1] - want[1]) <= tol * abs(want[1])

@@ -97,3 +97,25 @@ def test_plan_fits_the_grouped_launch():
         assert cnt[0] * 2 <= 256 and cnt[1] * 2 <= 256
         for p in probs:
             assert p["m"] < 2 ** 31 and p["n"] < 2 ** 31
+
+
+@pytest.mark.parametrize("nvir,blk,n_jobs", [(9, 2, 3), (11, 4, 5), (90, 4, 7), (13, 3, 13), (7, 6, 9)])
+def test_job_d_ranges_cover_each_task_once(nvir, blk, n_jobs):
+    """job_d_ranges over all jobs hands every task of the reference's order to exactly one
+    job, as the contiguous slices of distr_cc/rccsdt_q.py:359-366 do."""
+    from dcc import rccsdt_q
+    tasks = rccsdt_q.task_list(nvir, blk)
+    per = (len(tasks) + n_jobs - 1) // n_jobs
+    seen = []
+    for j in range(n_jobs):
+        want = {(t[0], t[1], t[3], t[4], t[6], t[7], t[9]) for t in tasks[j * per:(j + 1) * per]}
+        got = set()
+        for (a0, a1, b0, b1, c0, c1), (d0, d1) in rccsdt_q.job_d_ranges(nvir, blk, j, n_jobs).items():
+            assert c0 <= d0 < d1 <= nvir
+            for dd0, _ in rccsdt_q.prange(d0, d1, blk):
+                got.add((a0, a1, b0, b1, c0, c1, dd0))
+        assert got == want
+        seen += sorted(got)
+    assert len(seen) == len(set(seen)) == len(tasks)
+    with pytest.raises(ValueError):
+        rccsdt_q.job_d_ranges(nvir, blk, n_jobs, n_jobs)
