@@ -166,7 +166,9 @@ def q_kernel(mycc, eris=None, tamps=None, blksize=4, comm=None, job_idx=0, n_job
         eris = mycc.ao2mo(mycc.mo_coeff)
     tamps = tamps if tamps is not None else mycc.tamps
     _, t2, t3 = tamps
-    _, t3_local = t3
+    dt3, t3_local = t3
+    # T3 already in the ABC layout (prepare_tamps_for_q, distr_cc/rccsdt_q.py:58-66)
+    is_abc = dt3 is not None and hasattr(dt3, "abc_to_global_idx")
     p = eris.pppp
     o, v = slice(0, nocc), slice(nocc, nmo)
     er = {"vvvo": p[v, v, v, o], "vooo": p[v, o, o, o], "vvoo": p[v, v, o, o], "ovvo": p[o, v, v, o],
@@ -175,8 +177,10 @@ def q_kernel(mycc, eris=None, tamps=None, blksize=4, comm=None, job_idx=0, n_job
     nvir = nmo - nocc
     t2q = t2 if t2.shape == (nvir, nvir, nocc, nocc) else np.ascontiguousarray(np.transpose(t2, (2, 3, 0, 1)))
     e = np.asarray(eris.mo_energy)
-    return rccsdt_q.q_energy(er, _dev(t2q, dev), _dev(t3_local, dev), _dev(e[:nocc], dev), _dev(e[nocc:], dev),
-                             nocc, nvir, blksize, precision_of(mycc), job_idx=job_idx, n_jobs=n_jobs)
+    t3d = _dev(t3_local, dev)
+    return rccsdt_q.q_energy(er, _dev(t2q, dev), None if is_abc else t3d, _dev(e[:nocc], dev), _dev(e[nocc:], dev),
+                             nocc, nvir, blksize, precision_of(mycc), job_idx=job_idx, n_jobs=n_jobs,
+                             t3_abc=t3d if is_abc else None)
 
 
 # imds fields compute_r4_tri releases on return (distr_cc/rccsdtq.py:899-1349)

@@ -546,11 +546,16 @@ class QEnergy:
 
 
 def q_energy(er, t2, t3_ijk, e_occ, e_vir, nocc, nvir, blksize=4, precision="fp64", group_list=None, job_idx=0,
-             n_jobs=1):
-    """(e_bracket, e_paren) from canonical IJK-ordered T3 on the device; with n_jobs > 1, the
-    share of job `job_idx` (the energies of all jobs add up to the full ones)."""
-    t3_abc = _c_rccsdt.redistribute_ijk_to_abc(t3_ijk, nocc, nvir)
-    q = QEnergy(nocc, nvir, blksize, precision, device=t3_ijk.device)
+             n_jobs=1, t3_abc=None):
+    """(e_bracket, e_paren) from canonical IJK-ordered T3 on the device (or from T3 already in
+    the ABC layout, `t3_abc` [a<=b<=c][i][j][k], as prepare_tamps_for_q leaves it on one rank,
+    distr_cc/rccsdt_q.py:82-96; t3_ijk is then unused); with n_jobs > 1, the share of job
+    `job_idx` (the energies of all jobs add up to the full ones)."""
+    if t3_abc is None:
+        t3_abc = _c_rccsdt.redistribute_ijk_to_abc(t3_ijk, nocc, nvir)
+    elif tuple(t3_abc.shape) != (nvir * (nvir + 1) * (nvir + 2) // 6, nocc, nocc, nocc):
+        raise ValueError("t3_abc must have shape (nvir(nvir+1)(nvir+2)/6, nocc, nocc, nocc)")
+    q = QEnergy(nocc, nvir, blksize, precision, device=t3_abc.device)
     d_ranges = None if n_jobs == 1 else job_d_ranges(nvir, blksize, job_idx, n_jobs)
     out = q.run(er, t2, t3_abc, e_occ, e_vir, group_list, d_ranges)
     eb, ep = float(out[0]), float(out[1])

@@ -109,3 +109,23 @@ def test_compute_r4_tri_route(mods, oracle):
     got = backend.compute_r4_tri(mycc, imds, d["t2"], d["t3"], (dt4, d["t4"]))
     assert np.abs(got - want).max() <= 1e-11 * np.abs(want).max()
     assert imds.W_vvvo is None and imds.t1_eris is None  # released as the reference does
+
+
+def test_q_kernel_abc_input_and_jobs(mods, oracle):
+    """rccsdt_q.kernel with T3 already in the ABC layout (what the reference's
+    prepare_tamps_for_q hands over, tests/test_rccsdt_q.py test_t3ijk_abc_transformation) and
+    with job splitting (test_split_jobs): both give the energies of the plain call."""
+    backend = mods[0]
+    from dcc import _c_rccsdt
+    mycc, imds, t2, t3, U, eris = _problem(2, 6, 3)
+    full = np.array(backend.q_kernel(mycc, eris=eris, tamps=[None, t2, (None, t3)], blksize=2))
+    t3_abc = _c_rccsdt.redistribute_ijk_to_abc(torch.from_numpy(np.ascontiguousarray(t3)).cuda(), 2, 6).cpu().numpy()
+
+    class ABC:
+        abc_to_global_idx = {}
+
+    got = backend.q_kernel(mycc, eris=eris, tamps=[None, t2, (ABC(), t3_abc)], blksize=2)
+    np.testing.assert_allclose(got, full, rtol=1e-12, atol=1e-15)
+    jobs = sum(np.array(backend.q_kernel(mycc, eris=eris, tamps=[None, t2, (None, t3)], blksize=2, job_idx=j,
+                                         n_jobs=3)) for j in range(3))
+    np.testing.assert_allclose(jobs, full, rtol=1e-10, atol=1e-15)
