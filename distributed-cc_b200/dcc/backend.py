@@ -217,10 +217,33 @@ _ROUTES = {"r1r2_add_t3_tri_": r1r2_add_t3_tri_, "intermediates_t3_add_t3_tri": 
            "compute_r3_tri": compute_r3_tri}
 
 
-def install(rccsdt_module, rccsdt_q_module=None, rccsdtq_module=None):
+HOST_EINSUM = "numpy"
+
+
+def _host_einsum(orig):
+    """The module's _einsum(backend, subscripts, *operands, out=, alpha=, beta=) with the
+    backend string "cuda" read as HOST_EINSUM: the reference code this library does not route
+    (the lower-order equations, the T4 -> r2 / r3 feedback) keeps running on the host."""
+    def einsum(backend, *args, **kw):
+        return orig(HOST_EINSUM if backend == BACKEND else backend, *args, **kw)
+    einsum._dcc_wrapped = True
+    einsum.__name__ = getattr(orig, "__name__", "_einsum")
+    einsum.__doc__ = orig.__doc__
+    return einsum
+
+
+def install(rccsdt_module, rccsdt_q_module=None, rccsdtq_module=None, host_einsum_modules=()):
     """Route the reference's hot functions to the GPU when mycc.einsum_backend == "cuda".
-    Idempotent; returns the names it wrapped."""
+    Every given module's `_einsum` (the reference modules bind PySCF's at import,
+    distr_cc/rccsdt.py:27; pass pyscf.cc.rccsdt in host_einsum_modules for PySCF's own
+    lower-order code) reads "cuda" as the host backend.  Idempotent; returns the names it
+    wrapped."""
     wrapped = []
+    for mod in (rccsdt_module, rccsdt_q_module, rccsdtq_module) + tuple(host_einsum_modules):
+        orig = getattr(mod, "_einsum", None) if mod is not None else None
+        if orig is not None and not getattr(orig, "_dcc_wrapped", False):
+            mod._einsum = _host_einsum(orig)
+            wrapped.append("%s._einsum" % getattr(mod, "__name__", "module"))
     for name, fn in _ROUTES.items():
         orig = getattr(rccsdt_module, name, None)
         if orig is None or getattr(orig, "_dcc_wrapped", False):

@@ -75,3 +75,32 @@ def test_rccsdtq_route(monkeypatch):
     mycc.einsum_backend = "cuda"
     assert r4mod.compute_r4_tri(mycc, None, None, None, None) == "gpu:r4"
     assert orig_calls == ["orig"] and routed == ["gpu"]
+
+
+def test_host_einsum_reads_cuda_as_numpy():
+    """Reference code left on the host calls `_einsum(mycc.einsum_backend, ...)`; after install
+    the backend string "cuda" reaches the original as "numpy", other strings unchanged."""
+    seen = []
+
+    def _einsum(backend, subs, *ops, out=None, alpha=1.0, beta=0.0):
+        if backend not in ("numpy", "pytblis"):
+            raise ValueError("unknown einsum backend %r" % backend)
+        seen.append(backend)
+        res = alpha * np.einsum(subs, *ops)
+        if out is None:
+            return res
+        out *= beta
+        out += res
+        return out
+
+    mod = types.SimpleNamespace(_einsum=_einsum, __name__="fake_rccsdt")
+    pyscf_mod = types.SimpleNamespace(_einsum=_einsum, __name__="fake_pyscf")
+    names = backend.install(mod, host_einsum_modules=(pyscf_mod,))
+    assert "fake_rccsdt._einsum" in names and "fake_pyscf._einsum" in names
+    assert "fake_rccsdt._einsum" not in backend.install(mod)  # idempotent
+    a, b = np.arange(6.0).reshape(2, 3), np.arange(12.0).reshape(3, 4)
+    out = np.ones((2, 4))
+    mod._einsum("cuda", "ij,jk->ik", a, b, out=out, alpha=2.0, beta=1.0)
+    np.testing.assert_allclose(out, 1.0 + 2.0 * a @ b)
+    np.testing.assert_allclose(pyscf_mod._einsum("pytblis", "ij,jk->ik", a, b), a @ b)
+    assert seen == ["numpy", "pytblis"]
