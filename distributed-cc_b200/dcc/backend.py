@@ -10,6 +10,8 @@ hot functions
     compute_r3_tri(mycc, imds, t2, t3)                 distr_cc/rccsdt.py:368
     rccsdt_q.kernel(mycc, eris, tamps, blksize, comm)  distr_cc/rccsdt_q.py:227
     compute_r4_tri(mycc, imds, t2, t3, t4)             distr_cc/rccsdtq.py:834
+    r2_add_t4_tri_(mycc, imds, r2, t4)                 distr_cc/rccsdtq.py:471
+    r3_add_t4_tri_(mycc, imds, r3, t4)                 distr_cc/rccsdtq.py:577
 
 so that, when `mycc.einsum_backend == "cuda"` (set through the reference's
 own RCCSDT.set_einsum_backend, distr_cc/rccsdt.py:1255), they run on the GPU
@@ -195,12 +197,8 @@ def compute_r4_tri(mycc, imds, t2, t3, t4):
     require_single_rank(mycc)
     dev = getattr(mycc, "dcc_device", "cuda")
     nocc = mycc.nocc
-    dt4, t4_local = t4
+    t4_local = _t4_local(mycc, t4)
     quads = t4_residual.stored_quadruples(nocc)
-    local = [tuple(int(x) for x in q[:4]) for q in dt4.iter_local_ijkl()] if hasattr(dt4, "iter_local_ijkl") \
-        else quads
-    if local != quads or len(t4_local) != len(quads):
-        raise RuntimeError('einsum backend "cuda" needs every stored T4 block local, in stored order')
     d = lambda a: _dev(a, dev)  # noqa: E731
     r4 = torch.zeros((len(quads),) + tuple(t4_local.shape[1:]), dtype=f64, device=dev)
     t4_residual.compute_r4_tri_(r4, d(imds.t1_eris), d(imds.F_vv), d(imds.W_vvvo), d(imds.W_vooo), d(imds.W_vvvv),
@@ -213,8 +211,45 @@ def compute_r4_tri(mycc, imds, t2, t3, t4):
     return out
 
 
+def _t4_local(mycc, t4):
+    from . import t4_residual
+    dt4, t4_local = t4
+    quads = t4_residual.stored_quadruples(mycc.nocc)
+    local = [tuple(int(x) for x in q[:4]) for q in dt4.iter_local_ijkl()] if hasattr(dt4, "iter_local_ijkl") \
+        else quads
+    if local != quads or len(t4_local) != len(quads):
+        raise RuntimeError('einsum backend "cuda" needs every stored T4 block local, in stored order')
+    return t4_local
+
+
+def r2_add_t4_tri_(mycc, imds, r2, t4):
+    """distr_cc/rccsdtq.py:471-575 on the GPU, one rank: r2 += the T4 part, in place."""
+    from . import t4_residual
+    require_single_rank(mycc)
+    dev = getattr(mycc, "dcc_device", "cuda")
+    t4_local = _t4_local(mycc, t4)
+    r = _dev(r2, dev)
+    t4_residual.r2_add_t4_(r, _dev(t4_local, dev), _dev(imds.t1_eris, dev), mycc.nocc, precision_of(mycc))
+    r2[...] = r.cpu().numpy()
+    return r2
+
+
+def r3_add_t4_tri_(mycc, imds, r3, t4):
+    """distr_cc/rccsdtq.py:577-683 on the GPU, one rank: r3 (full) += the T4 part, in place."""
+    from . import t4_residual
+    require_single_rank(mycc)
+    dev = getattr(mycc, "dcc_device", "cuda")
+    t4_local = _t4_local(mycc, t4)
+    r = _dev(r3, dev)
+    t4_residual.r3_add_t4_(r, _dev(t4_local, dev), _dev(imds.t1_fock, dev), _dev(imds.t1_eris, dev), mycc.nocc,
+                           precision_of(mycc))
+    r3[...] = r.cpu().numpy()
+    return r3
+
+
 _ROUTES = {"r1r2_add_t3_tri_": r1r2_add_t3_tri_, "intermediates_t3_add_t3_tri": intermediates_t3_add_t3_tri,
            "compute_r3_tri": compute_r3_tri}
+_R4_ROUTES = {"compute_r4_tri": None, "r2_add_t4_tri_": r2_add_t4_tri_, "r3_add_t4_tri_": r3_add_t4_tri_}
 
 
 HOST_EINSUM = "numpy"
@@ -267,13 +302,17 @@ def install(rccsdt_module, rccsdt_q_module=None, rccsdtq_module=None, host_einsu
             rccsdt_q_module.kernel = qwrap
             wrapped.append("rccsdt_q.kernel")
     if rccsdtq_module is not None:
-        orig = getattr(rccsdtq_module, "compute_r4_tri", None)
-        if orig is not None and not getattr(orig, "_dcc_wrapped", False):
-            def r4wrap(mycc, *args, _orig=orig, **kw):
-                return compute_r4_tri(mycc, *args, **kw) if uses_cuda(mycc) else _orig(mycc, *args, **kw)
+        for name, fn in _R4_ROUTES.items():
+            fn = compute_r4_tri if fn is None else fn
+            orig = getattr(rccsdtq_module, name, None)
+            if orig is None or getattr(orig, "_dcc_wrapped", False):
+                continue
+
+            def r4wrap(mycc, *args, _orig=orig, _fn=fn, **kw):
+                return _fn(mycc, *args, **kw) if uses_cuda(mycc) else _orig(mycc, *args, **kw)
             r4wrap._dcc_wrapped = True
-            r4wrap.__name__ = "compute_r4_tri"
+            r4wrap.__name__ = name
             r4wrap.__doc__ = orig.__doc__
-            rccsdtq_module.compute_r4_tri = r4wrap
-            wrapped.append("rccsdtq.compute_r4_tri")
+            setattr(rccsdtq_module, name, r4wrap)
+            wrapped.append("rccsdtq." + name)
     return wrapped

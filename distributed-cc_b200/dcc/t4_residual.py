@@ -413,3 +413,76 @@ def oo_batch_(r4, t4, F_oo, W_oooo, W_ovvo, W_ovov, nocc, forms=None):
             upd = e("p" + ws + ",p" + ts + "->pabcd", Wo if wn == "ovov" else Wv, src[form][si])
             r4.index_add_(0, ti, upd, alpha=al)
     return r4
+
+
+# ----------------------------------------------------------------------------
+# T4 -> r2 and T4 -> r3 feedback (r2_add_t4_tri_, distr_cc/rccsdtq.py:471-575;
+# r3_add_t4_tri_, :577-683) over the full ordered occupied space.
+#
+# The reference walks the stored blocks and, per block, the distinct ways to pull
+# a pair (r2) or one index (r3, T1-Fock part) out of its occupied multiset, with
+# weights 1/2 (1/4) where pulled or remaining indices coincide.  Over every ordered
+# tuple of T4s = P4(T[ordering]) this is one string each:
+#   r2[z,w] += W2[x,y] W2[z,w] sum_{x,y,e,f} eris[x,y,e,f] T4s_442[x,y,z,w][e,f,a,b]
+#   r3[x,y,z] += W3[x,y,z] sum_{m,e} fock[m,e] T4s_201[m,x,y,z][e,a,b,c]
+# with W2 = 1 (x < y), 1/2 (x = y), 0 (x > y) and W3 = 1 (x < y < z), 1/2 (sorted, two
+# equal), 0 otherwise; the T1-ERI part of r3 (:649-667) already runs over every
+# distinct ordering and becomes two plain strings.
+# ----------------------------------------------------------------------------
+
+def _w2(nocc, device):
+    return _cached(("w2", nocc), device, lambda: torch.tensor(
+        [[1.0 if x < y else (0.5 if x == y else 0.0) for y in range(nocc)] for x in range(nocc)],
+        dtype=torch.float64, device=device))
+
+
+def _w3(nocc, device):
+    def w(x, y, z):
+        if not x <= y <= z or x == z:
+            return 0.0
+        return 1.0 if x < y < z else 0.5
+    return _cached(("w3", nocc), device, lambda: torch.tensor(
+        [[[w(x, y, z) for z in range(nocc)] for y in range(nocc)] for x in range(nocc)],
+        dtype=torch.float64, device=device))
+
+
+def _spin4_default(nv):
+    from . import _c_rccsdt_q
+    return lambda A, pattern: _c_rccsdt_q.t4_spin_summation_inplace_(A, A.numel() // nv ** 4, nv, pattern, 1.0, 0.0)
+
+
+def r2_add_t4_(r2, t4, eris, nocc, precision="fp64", spin4=None):
+    """r2 += the T4 part of r2_add_t4_tri_ (distr_cc/rccsdtq.py:471-575).  r2 [i,j,a,b];
+    t4 the stored blocks [n4, nv^4]; eris the t1-dressed ERIs [nmo]^4.  spin4(A, pattern)
+    applies a P4 pattern in place to [n, nv^4] blocks (default: this library's kernel)."""
+    kind = None if precision == "fp64" else contract.KIND[precision]
+    nv = t4.shape[1]
+    spin4 = _spin4_default(nv) if spin4 is None else spin4
+    T = unpack_all_orderings(t4, nocc).contiguous()
+    spin4(T.view(-1, nv, nv, nv, nv), "P4_442")
+    w2 = _w2(nocc, t4.device)
+    o, v = slice(0, nocc), slice(nocc, None)
+    Ew = (eris[o, o, v, v] * w2[:, :, None, None]).contiguous()
+    R = torch.zeros((nocc, nocc, nv, nv), dtype=t4.dtype, device=t4.device)
+    _einsum(kind, "xyef,xyzwefab->zwab", Ew, T, R, 1.0)
+    r2 += R * w2[:, :, None, None]
+    return r2
+
+
+def r3_add_t4_(r3, t4, fock, eris, nocc, precision="fp64", spin4=None):
+    """r3 += the T4 part of r3_add_t4_tri_ (distr_cc/rccsdtq.py:577-683).  r3 the full
+    [i,j,k,a,b,c]; fock the t1-dressed Fock matrix [nmo, nmo]; other arguments as
+    r2_add_t4_."""
+    kind = None if precision == "fp64" else contract.KIND[precision]
+    nv = t4.shape[1]
+    spin4 = _spin4_default(nv) if spin4 is None else spin4
+    T = unpack_all_orderings(t4, nocc).contiguous()
+    spin4(T.view(-1, nv, nv, nv, nv), "P4_201")
+    o, v = slice(0, nocc), slice(nocc, None)
+    R = torch.zeros((nocc,) * 3 + (nv,) * 3, dtype=t4.dtype, device=t4.device)
+    _einsum(kind, "me,mxyzeabc->xyzabc", fock[o, v].contiguous(), T, R, 1.0)
+    R *= _w3(nocc, t4.device)[:, :, :, None, None, None]
+    _einsum(kind, "amef,mxyzfebc->xyzabc", eris[v, o, v, v].contiguous(), T, R, 0.5)
+    _einsum(kind, "myen,mxyzeabc->xnzabc", eris[o, o, v, o].contiguous(), T, R, -0.5)
+    r3 += R
+    return r3

@@ -431,3 +431,97 @@ def oo_batch_ref(r4, t4, F_oo, W_oooo, W_ovvo, W_ovov, nocc, orc):
                 r -= 0.5 * (e("de,ebca->abcd", W[o3, :, l, :], T) + e("de,aecb->abcd", W[o3, :, l, :], T)
                             + e("de,abec->abcd", W[o3, :, l, :], T))
     return r4
+
+
+# ----------------------------------------------------------------------------
+# T4 -> r2 and T4 -> r3 feedback of RCCSDTQ, literal per stored block:
+# r2_add_t4_tri_ (distr_cc/rccsdtq.py:471-575) and r3_add_t4_tri_ (:577-683).
+# ----------------------------------------------------------------------------
+
+# (unpacked ordering as positions of (i, j, k, l), alpha) per case of r2_add_t4_tri_
+# (:489-556); the term is r2[o[2], o[3]] += alpha eris[o[0], o[1], e, f] P4_442(T[o])[e,f,a,b]
+_R2_CASES = {
+    "ijkl": [((0, 1, 2, 3), 1.0), ((0, 2, 1, 3), 1.0), ((0, 3, 1, 2), 1.0), ((1, 2, 0, 3), 1.0),
+             ((1, 3, 0, 2), 1.0), ((2, 3, 0, 1), 1.0)],
+    "iikl": [((0, 1, 2, 3), 0.5), ((0, 2, 1, 3), 1.0), ((0, 3, 1, 2), 1.0), ((2, 3, 0, 1), 0.5)],
+    "ijjl": [((0, 1, 2, 3), 1.0), ((0, 3, 1, 2), 0.5), ((1, 2, 0, 3), 0.5), ((1, 3, 0, 2), 1.0)],
+    "ijkk": [((0, 1, 2, 3), 0.5), ((0, 2, 1, 3), 1.0), ((1, 2, 0, 3), 1.0), ((2, 3, 0, 1), 0.5)],
+    "iikk": [((0, 1, 2, 3), 0.25), ((0, 2, 1, 3), 1.0), ((2, 3, 0, 1), 0.25)],
+}
+# the same for the T1-Fock part of r3_add_t4_tri_ (:598-647): r3[o[1], o[2], o[3]] +=
+# alpha fock[o[0], e] P4_201(T[o])[e,a,b,c]
+_R3_CASES = {
+    "ijkl": [((0, 1, 2, 3), 1.0), ((1, 0, 2, 3), 1.0), ((2, 0, 1, 3), 1.0), ((3, 0, 1, 2), 1.0)],
+    "iikl": [((0, 1, 2, 3), 1.0), ((2, 0, 1, 3), 0.5), ((3, 0, 1, 2), 0.5)],
+    "ijjl": [((0, 1, 2, 3), 0.5), ((1, 0, 2, 3), 1.0), ((3, 0, 1, 2), 0.5)],
+    "ijkk": [((0, 1, 2, 3), 0.5), ((1, 0, 2, 3), 0.5), ((2, 0, 1, 3), 1.0)],
+    "iikk": [((0, 1, 2, 3), 0.5), ((2, 0, 1, 3), 0.5)],
+}
+
+
+def _case(q):
+    i, j, k, l = q
+    if i < j < k < l:
+        return "ijkl"
+    if i == j < k < l:
+        return "iikl"
+    if i < j == k < l:
+        return "ijjl"
+    if i < j < k == l:
+        return "ijkk"
+    if i == j < k == l:
+        return "iikk"
+    return None
+
+
+def _unpacked(t4, f2l, o, nocc, nvir, orc, pattern):
+    t, _ = orc.unpack_t4(np.ascontiguousarray(t4), f2l, o[0], o[1], o[2], o[3], nocc, nvir)
+    return orc.t4_spin_sum(t, 1, nvir, pattern, 1.0, 0.0)
+
+
+def _f2l(quads, nocc, orc):
+    nfull = nocc * (nocc + 1) * (nocc + 2) * (nocc + 3) // 24
+    f2l = np.full(nfull, -1, dtype=np.int64)
+    for n, qd in enumerate(quads):
+        f2l[orc.ijkl_to_linear(*qd, nocc)] = n
+    return f2l
+
+
+def r2_add_t4_tri_ref(r2, t4, t1_eris, nocc, orc):
+    """r2 + the T4 contributions of r2_add_t4_tri_ (t4 the stored blocks, t1_eris [nmo]^4)."""
+    e = np.einsum
+    nvir = t4.shape[1]
+    v = slice(nocc, None)
+    quads = stored_quadruples(nocc)
+    f2l = _f2l(quads, nocc, orc)
+    r2_loc = np.zeros_like(r2)
+    for q in quads:
+        for pos, alpha in _R2_CASES[_case(q)]:
+            o = tuple(q[p] for p in pos)
+            t = _unpacked(t4, f2l, o, nocc, nvir, orc, "P4_442")
+            r2_loc[o[2], o[3]] += alpha * e('ef,efab->ab', t1_eris[o[0], o[1], v, v], t)
+    return r2 + r2_loc
+
+
+def r3_add_t4_tri_ref(r3, t4, t1_fock, t1_eris, nocc, orc):
+    """r3 (full [no]^3 [nv]^3) + the T4 contributions of r3_add_t4_tri_."""
+    import itertools
+    e = np.einsum
+    nvir = t4.shape[1]
+    o_, v = slice(0, nocc), slice(nocc, None)
+    quads = stored_quadruples(nocc)
+    f2l = _f2l(quads, nocc, orc)
+    r3_loc = np.zeros_like(r3)
+    for q in quads:
+        for pos, alpha in _R3_CASES[_case(q)]:
+            o = tuple(q[p] for p in pos)
+            t = _unpacked(t4, f2l, o, nocc, nvir, orc, "P4_201")
+            r3_loc[o[1], o[2], o[3]] += alpha * e('e,eabc->abc', t1_fock[o[0], v], t)
+    for q in quads:
+        if max(q.count(x) for x in q) >= 3:
+            continue
+        for (pi, pj, pk, pl) in dict.fromkeys(itertools.permutations(q)):
+            t = _unpacked(t4, f2l, (pi, pj, pk, pl), nocc, nvir, orc, "P4_201")
+            r3_loc[pj, pk, pl] += 0.5 * e('aef,febc->abc', t1_eris[v, pi, v, v], t)
+            r3_loc[pj, :, pl] += -0.5 * e('en,eabc->nabc', t1_eris[pi, pk, v, o_], t)
+    return r3 + r3_loc

@@ -77,6 +77,20 @@ def test_rccsdtq_route(monkeypatch):
     assert orig_calls == ["orig"] and routed == ["gpu"]
 
 
+def test_t4_feedback_routes(monkeypatch):
+    """r2_add_t4_tri_ / r3_add_t4_tri_ of distr_cc/rccsdtq.py are routed by the backend string."""
+    r4mod = types.SimpleNamespace(r2_add_t4_tri_=lambda mycc, *a: "orig:r2", r3_add_t4_tri_=lambda mycc, *a: "orig:r3")
+    monkeypatch.setitem(backend._R4_ROUTES, "r2_add_t4_tri_", lambda mycc, *a: "gpu:r2")
+    monkeypatch.setitem(backend._R4_ROUTES, "r3_add_t4_tri_", lambda mycc, *a: "gpu:r3")
+    mod, qmod, _ = _fake_module()
+    names = backend.install(mod, qmod, r4mod)
+    assert {"rccsdtq.r2_add_t4_tri_", "rccsdtq.r3_add_t4_tri_"} <= set(names)
+    mycc = types.SimpleNamespace(einsum_backend="numpy", comm=backend.SingleRankComm())
+    assert (r4mod.r2_add_t4_tri_(mycc, 0, 0, 0), r4mod.r3_add_t4_tri_(mycc, 0, 0, 0)) == ("orig:r2", "orig:r3")
+    mycc.einsum_backend = "cuda"
+    assert (r4mod.r2_add_t4_tri_(mycc, 0, 0, 0), r4mod.r3_add_t4_tri_(mycc, 0, 0, 0)) == ("gpu:r2", "gpu:r3")
+
+
 def test_host_einsum_reads_cuda_as_numpy():
     """Reference code left on the host calls `_einsum(mycc.einsum_backend, ...)`; after install
     the backend string "cuda" reaches the original as "numpy", other strings unchanged."""

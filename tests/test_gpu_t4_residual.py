@@ -66,3 +66,29 @@ def test_compute_r4_tri(oracle, precision, no, nv):
     got = r4.cpu().numpy()
     tol = 1e-11 if precision == "fp64" else 1e-4
     assert np.abs(got - want).max() <= tol * np.abs(want).max()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "bf16x3"])
+@pytest.mark.parametrize("no,nv", [(4, 5), (7, 11)])
+def test_t4_feedback(oracle, precision, no, nv):
+    """r2_add_t4_tri_ / r3_add_t4_tri_ (distr_cc/rccsdtq.py:471-683) on the GPU (P4_442 /
+    P4_201 kernels, full-space strings) against the oracle's literal per-block loops."""
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from dcc import t4_residual
+    from oracle import t4_ref
+    rng = np.random.default_rng(7 * no + nv)
+    nmo = no + nv
+    t4 = rng.standard_normal((len(t4_ref.stored_quadruples(no)),) + (nv,) * 4) * 0.01
+    eris = rng.standard_normal((nmo,) * 4) * 0.1
+    fock = rng.standard_normal((nmo, nmo)) * 0.1
+    r2 = rng.standard_normal((no, no, nv, nv)) * 1e-3
+    r3 = rng.standard_normal((no,) * 3 + (nv,) * 3) * 1e-3
+    want2 = t4_ref.r2_add_t4_tri_ref(r2, t4, eris, no, oracle)
+    want3 = t4_ref.r3_add_t4_tri_ref(r3, t4, fock, eris, no, oracle)
+    dev = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()  # noqa: E731
+    got2 = t4_residual.r2_add_t4_(dev(r2), dev(t4), dev(eris), no, precision).cpu().numpy()
+    got3 = t4_residual.r3_add_t4_(dev(r3), dev(t4), dev(fock), dev(eris), no, precision).cpu().numpy()
+    tol = 1e-11 if precision == "fp64" else 1e-4
+    assert np.abs(got2 - want2).max() <= tol * np.abs(want2 - r2).max()
+    assert np.abs(got3 - want3).max() <= tol * np.abs(want3 - r3).max()
