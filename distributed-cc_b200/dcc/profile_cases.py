@@ -167,6 +167,36 @@ def case_qgroup(reps, nocc=10):
     assert q.status_ok()
 
 
+def case_t3iter(reps, nocc, nvir, kind="bf16x3"):
+    """T3 iterations (compute_r3_tri with the OO terms, P3_full, divide, update, norms) at a
+    given shape, timed with CUDA events after two warm-up iterations; the split precisions
+    autotune their W_vvvv GEMMs first.  Prints ms per iteration."""
+    from dcc import synthetic, t3_residual
+    d = synthetic.make_inputs(nocc, nvir, seed=0)
+    res = t3_residual.T3Residual(nocc, nvir, kind, with_oo=True)
+    r3 = torch.empty_like(d.t3)
+    norms = torch.empty(2, dtype=torch.float64, device="cuda")
+    if kind != "fp64":
+        res.tune(d, d.t3)
+
+    def step():
+        res.compute(d, d.t3, r3)
+        t3_residual.update_t3_(d.t3, r3, d, norms=norms, write_r3=False)
+
+    for _ in range(2):
+        step()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        step()
+    e1.record()
+    torch.cuda.synchronize()
+    assert res.status_ok()
+    print(f"t3iter {kind} nocc={nocc} nvir={nvir} blocks={d.t3.shape[0]}: {e0.elapsed_time(e1) / reps:.2f} ms "
+          f"per iteration, peak memory {torch.cuda.max_memory_allocated() / 2**30:.1f} GiB")
+
+
 def case_t4(reps, kind="bf16x3"):
     """T4 updates at the N2 6-31G shape (nocc=7, nvir=11, 161 stored blocks): compute_r4_tri
     with its OO batch, projector, divide, norms, t4 += r4 (dcc.graph.T4Iteration), eager."""
@@ -180,7 +210,7 @@ def case_t4(reps, kind="bf16x3"):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("case", choices=["gemm", "p3", "update", "q", "gather", "xgemm", "oogemm", "unpack", "qgroup",
-                                         "t4"])
+                                         "t4", "t3iter"])
     ap.add_argument("--kind", default="bf16x3")
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--nocc", type=int, default=None, help="occupied orbitals (xgemm, oogemm, gather, unpack)")
@@ -197,6 +227,8 @@ def main():
         case_update(a.reps)
     elif a.case == "t4":
         case_t4(a.reps, a.kind)
+    elif a.case == "t3iter":
+        case_t3iter(a.reps, a.nocc or 10, a.nvir, a.kind)
     elif a.case in ("gather", "xgemm", "oogemm", "unpack", "qgroup"):
         fn = {"gather": case_gather, "xgemm": case_xgemm, "oogemm": case_oogemm, "unpack": case_unpack,
               "qgroup": case_qgroup}[a.case]

@@ -155,6 +155,19 @@ def s_plan(no, nv):
     }
 
 
+def woooo_k_pieces(no, nv, limit=(1 << 31) - 1):
+    """Contraction pieces of the K-major split of U for the W_oooo / F_oo GEMM: K = nocc^2
+    cut so that a piece's offsets (k * nocc nvir^3) stay below `limit`, every piece but the
+    last a multiple of 8 columns."""
+    stride, K = no * nv ** 3, no * no
+    if (K - 1) * stride < limit:
+        return [K]
+    step = (limit // stride) // 8 * 8
+    if step < 8:
+        raise ValueError("nocc * nvir^3 = %d is too large for 31-bit split offsets" % stride)
+    return [min(step, K - k0) for k0 in range(0, K, step)]
+
+
 def woooo_foo_matrix(W_oooo, F_oo, sym_tol=1e-14, assume_symmetric=False):
     """(A, W_anti): A[(i,j)][(l,m)] = (Ws[l,m,i,j] - F_oo[l,i] delta_mj) / 2 with Ws the
     pair-symmetric part of W_oooo; W_anti = the antisymmetric part, or None when it is
@@ -177,7 +190,8 @@ def woooo_foo_matrix(W_oooo, F_oo, sym_tol=1e-14, assume_symmetric=False):
 class T3Residual:
     """compute_r3_tri for all canonical blocks of one rank."""
 
-    def __init__(self, nocc, nvir, precision="fp64", device="cuda", with_oo=True, woooo_pair_symmetric=False):
+    def __init__(self, nocc, nvir, precision="fp64", device="cuda", with_oo=True, woooo_pair_symmetric=False,
+                 woooo_piece_limit=(1 << 31) - 1):
         self.no, self.nv, self.precision = int(nocc), int(nvir), precision
         # True: W_oooo has the pair symmetry of RHF (its antisymmetric part is not checked
         # for, so compute() reads nothing back to the host and can be captured in a graph)
@@ -209,9 +223,17 @@ class T3Residual:
                 self.ooa = contract.Split(no * nv, kind=k, device=device, pieces=[K, K])
                 self.oob = contract.Split(no * no * nv * nv, kind=k, device=device, pieces=[K, K])
                 self.t1a = contract.Split(no * nv, K, k, device)
-                # W_oooo / F_oo . U: rows (i,j), columns (k,a,b,c), K = (l,m)
-                self.wooa = contract.Split(no * no, no * no, k, device)
-                self.woob = contract.Split(no * nv ** 3, no * no, k, device)
+                # W_oooo / F_oo . U: rows (i,j), columns (k,a,b,c), K = (l,m).  The split kernel
+                # addresses a piece's contraction with 31-bit offsets and U's (l,m) stride is
+                # nocc nvir^3, so K is cut into pieces of whole multiples of 8 below 2^31 / stride
+                # (one piece up to about nocc=12 / nvir=90; two at nocc=15 / nvir=93)
+                self.woo_pieces = woooo_k_pieces(no, nv, woooo_piece_limit)
+                if len(self.woo_pieces) == 1:
+                    self.wooa = contract.Split(no * no, no * no, k, device)
+                    self.woob = contract.Split(no * nv ** 3, no * no, k, device)
+                else:
+                    self.wooa = contract.Split(no * no, kind=k, device=device, pieces=self.woo_pieces)
+                    self.woob = contract.Split(no * nv ** 3, kind=k, device=device, pieces=self.woo_pieces)
         else:
             self.X = torch.empty((no * nv * nv, no * no * nv), dtype=f64, device=device)  # [(j,a,b),(i,k,c)]
 
@@ -266,8 +288,17 @@ class T3Residual:
                 # S[(i,j)][(k,abc)] += A[(i,j)][(l,m)] U[(l,m)][(k,abc)] as a split GEMM: the K-major split
                 # of U (no nv^3 rows of no^2) costs one pass over U, the FP64 DGEMM took twice as long
                 n = no * nv ** 3
-                self.wooa.fill(A.contiguous(), contract.lin(no * no), contract.lin(1))
-                self.woob.fill(self.U, contract.lin(1), contract.lin(n))
+                A = A.contiguous()
+                if len(self.woo_pieces) == 1:
+                    self.wooa.fill(A, contract.lin(no * no), contract.lin(1))
+                    self.woob.fill(self.U, contract.lin(1), contract.lin(n))
+                else:
+                    k0 = 0
+                    Uf = self.U.view(no * no, n)
+                    for i, kk in enumerate(self.woo_pieces):
+                        self.wooa.fill_piece(i, A[:, k0:k0 + kk], contract.lin(no * no), contract.lin(1))
+                        self.woob.fill_piece(i, Uf[k0:k0 + kk], contract.lin(1), contract.lin(n))
+                        k0 += kk
                 contract.gemm_(self.wooa, self.woob, S, contract.lin(n), contract.lin(1), 1.0, 1.0, self.status)
             if Wa is not None:
                 if self.Ganti is None:

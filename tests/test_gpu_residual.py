@@ -156,3 +156,21 @@ def test_inputs_uploaded_during_the_unpack(mods, precision):
     got = res.compute(dd, d.t3, inputs_ready=ready)
     torch.cuda.synchronize()
     assert torch.equal(got, want) and res.status_ok()
+
+
+@pytest.mark.parametrize("precision", ["bf16x3", "tf32x3"])
+def test_woooo_split_in_k_pieces(mods, precision):
+    """The W_oooo / F_oo GEMM with its K-major U operand cut into K pieces (what nocc=15 /
+    nvir=93 needs to keep the split's offsets within 31 bits), forced here at a small shape:
+    same residual as one piece, within the split tolerance of the FP64 path."""
+    syn, tr, _ = mods
+    d = syn.make_inputs(5, 6, seed=31)
+    one = tr.T3Residual(5, 6, precision, with_oo=True)
+    cut = tr.T3Residual(5, 6, precision, with_oo=True, woooo_piece_limit=8 * 5 * 6 ** 3 + 1)
+    assert one.woo_pieces == [25] and cut.woo_pieces == [8, 8, 8, 1]
+    want = tr.T3Residual(5, 6, "fp64", with_oo=True).compute(d, d.t3)
+    a, b = one.compute(d, d.t3), cut.compute(d, d.t3)
+    assert one.status_ok() and cut.status_ok()
+    scale = want.abs().max()
+    assert float((b - want).abs().max() / scale) < TOL[precision]
+    assert float((b - a).abs().max() / scale) < 1e-6
