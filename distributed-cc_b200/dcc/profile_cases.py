@@ -197,6 +197,36 @@ def case_t3iter(reps, nocc, nvir, kind="bf16x3"):
           f"per iteration, peak memory {torch.cuda.max_memory_allocated() / 2**30:.1f} GiB")
 
 
+def case_qsample(nocc, nvir, kind="bf16x3", ngroups=12, blksize=4):
+    """[Q] / (Q) on `ngroups` task groups spread over all groups (as the bench samples them),
+    split path and FP64 path on the same inputs: ms and energies of each, printed."""
+    from dcc import synthetic, rccsdt_q, _c_rccsdt
+    d = synthetic.make_inputs(nocc, nvir, seed=0)
+    er = {"vvvo": d.W_vvvo, "vooo": d.W_vooo, "vvoo": d.eris_vvoo, "ovvo": d.W_ovvo, "ovov": d.W_ovov,
+          "vvvv": d.W_vvvv, "oooo": d.W_oooo}
+    t2 = d.t2.permute(2, 3, 0, 1).contiguous()
+    t3_abc = _c_rccsdt.redistribute_ijk_to_abc(d.t3, nocc, nvir)
+    del d.t3
+    G = rccsdt_q.groups(nvir, blksize)
+    sample = G[::max(1, len(G) // ngroups)][:ngroups]
+    for prec in (kind, "fp64"):
+        q = rccsdt_q.QEnergy(nocc, nvir, blksize, prec)
+        q.prepare(sample)
+        q.run(er, t2, t3_abc, d.e_occ, d.e_vir, sample[:1])
+        q.out.zero_()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        q.run(er, t2, t3_abc, d.e_occ, d.e_vir, sample)
+        e1.record()
+        torch.cuda.synchronize()
+        assert q.status_ok()
+        print(f"qsample {prec} nocc={nocc} nvir={nvir} groups={len(sample)}: {e0.elapsed_time(e1):.2f} ms, "
+              f"E[Q]={float(q.out[0]):.10e} E(Q)={float(q.out[1]):.10e}, "
+              f"peak memory {torch.cuda.max_memory_allocated() / 2**30:.1f} GiB")
+        del q
+
+
 def case_t4(reps, kind="bf16x3"):
     """T4 updates at the N2 6-31G shape (nocc=7, nvir=11, 161 stored blocks): compute_r4_tri
     with its OO batch, projector, divide, norms, t4 += r4 (dcc.graph.T4Iteration), eager."""
@@ -210,7 +240,7 @@ def case_t4(reps, kind="bf16x3"):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("case", choices=["gemm", "p3", "update", "q", "gather", "xgemm", "oogemm", "unpack", "qgroup",
-                                         "t4", "t3iter"])
+                                         "t4", "t3iter", "qsample"])
     ap.add_argument("--kind", default="bf16x3")
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--nocc", type=int, default=None, help="occupied orbitals (xgemm, oogemm, gather, unpack)")
@@ -229,6 +259,8 @@ def main():
         case_t4(a.reps, a.kind)
     elif a.case == "t3iter":
         case_t3iter(a.reps, a.nocc or 10, a.nvir, a.kind)
+    elif a.case == "qsample":
+        case_qsample(a.nocc or 10, a.nvir, a.kind)
     elif a.case in ("gather", "xgemm", "oogemm", "unpack", "qgroup"):
         fn = {"gather": case_gather, "xgemm": case_xgemm, "oogemm": case_oogemm, "unpack": case_unpack,
               "qgroup": case_qgroup}[a.case]
