@@ -258,7 +258,7 @@ HOST_EINSUM = "numpy"
 def _host_einsum(orig):
     """The module's _einsum(backend, subscripts, *operands, out=, alpha=, beta=) with the
     backend string "cuda" read as HOST_EINSUM: the reference code this library does not route
-    (the lower-order equations, the T4 -> r2 / r3 feedback) keeps running on the host."""
+    (the lower-order equations and the other intermediates) keeps running on the host."""
     def einsum(backend, *args, **kw):
         return orig(HOST_EINSUM if backend == BACKEND else backend, *args, **kw)
     einsum._dcc_wrapped = True
