@@ -197,7 +197,7 @@ def case_t3iter(reps, nocc, nvir, kind="bf16x3"):
           f"per iteration, peak memory {torch.cuda.max_memory_allocated() / 2**30:.1f} GiB")
 
 
-def case_qsample(nocc, nvir, kind="bf16x3", ngroups=12, blksize=4):
+def case_qsample(nocc, nvir, kind="bf16x3", ngroups=12, blksize=4, dchunk=None):
     """[Q] / (Q) on `ngroups` task groups spread over all groups (as the bench samples them),
     split path and FP64 path on the same inputs: ms and energies of each, printed."""
     from dcc import synthetic, rccsdt_q, _c_rccsdt
@@ -210,7 +210,7 @@ def case_qsample(nocc, nvir, kind="bf16x3", ngroups=12, blksize=4):
     G = rccsdt_q.groups(nvir, blksize)
     sample = G[::max(1, len(G) // ngroups)][:ngroups]
     for prec in (kind, "fp64"):
-        q = rccsdt_q.QEnergy(nocc, nvir, blksize, prec)
+        q = rccsdt_q.QEnergy(nocc, nvir, blksize, prec, dchunk=dchunk)
         q.prepare(sample)
         q.run(er, t2, t3_abc, d.e_occ, d.e_vir, sample[:1])
         q.out.zero_()
@@ -221,7 +221,8 @@ def case_qsample(nocc, nvir, kind="bf16x3", ngroups=12, blksize=4):
         e1.record()
         torch.cuda.synchronize()
         assert q.status_ok()
-        print(f"qsample {prec} nocc={nocc} nvir={nvir} groups={len(sample)}: {e0.elapsed_time(e1):.2f} ms, "
+        print(f"qsample {prec} nocc={nocc} nvir={nvir} groups={len(sample)} dchunk={dchunk}: "
+              f"{e0.elapsed_time(e1):.2f} ms, "
               f"E[Q]={float(q.out[0]):.10e} E(Q)={float(q.out[1]):.10e}, "
               f"peak memory {torch.cuda.max_memory_allocated() / 2**30:.1f} GiB")
         del q
@@ -248,6 +249,7 @@ def main():
     ap.add_argument("--op", default="p3", choices=["p3", "p3_422", "roundtrip", "triple", "transpose"],
                     help="p3 case: which symmetrizer")
     ap.add_argument("--time", action="store_true", help="p3 case: print CUDA-event timings")
+    ap.add_argument("--dchunk", type=int, default=None, help="qsample case: d-chunk of the split path")
     a = ap.parse_args()
     if a.case == "gemm":
         case_gemm(a.kind, a.reps)
@@ -260,7 +262,7 @@ def main():
     elif a.case == "t3iter":
         case_t3iter(a.reps, a.nocc or 10, a.nvir, a.kind)
     elif a.case == "qsample":
-        case_qsample(a.nocc or 10, a.nvir, a.kind)
+        case_qsample(a.nocc or 10, a.nvir, a.kind, dchunk=a.dchunk)
     elif a.case in ("gather", "xgemm", "oogemm", "unpack", "qgroup"):
         fn = {"gather": case_gather, "xgemm": case_xgemm, "oogemm": case_oogemm, "unpack": case_unpack,
               "qgroup": case_qgroup}[a.case]
