@@ -68,6 +68,14 @@ def groups(nvir, blksize):
     return out
 
 
+def default_dchunk(nocc, nvir, blksize, limit=1 << 30):
+    """Virtuals per d-chunk of the split path: the largest multiple of blksize whose two FP32
+    group blocks (blksize^3 x chunk x nocc^4 each) fit in `limit` bytes, at least blksize and at
+    most nvir (one pass over the whole d range)."""
+    per_d = 2 * 4 * blksize ** 3 * nocc ** 4
+    return min(nvir, max(blksize, limit // per_d // blksize * blksize))
+
+
 def job_d_ranges(nvir, blksize, job_idx=0, n_jobs=1):
     """{(a0, a1, b0, b1, c0, c1): (d0, d1)}: the tasks of job `job_idx` of `n_jobs` as group d
     ranges.  A job takes the contiguous slice [j*ceil(T/n), min((j+1)*ceil(T/n), T)) of the
@@ -333,11 +341,7 @@ class QEnergy:
         # 1 GB, which is the whole range up to nocc ~ 12 at nvir ~ 90 (one pass measured fastest
         # at nocc=10: the reductions go through L2 whether or not the blocks fit in it); at
         # nocc=15 / nvir=93 chunks of 24 and 48 measured 7 % and 3 % faster than one pass.
-        if dchunk:
-            self.dchunk = int(dchunk)
-        else:
-            per_d = 2 * 4 * self.blk ** 3 * self.no ** 4
-            self.dchunk = min(self.nv, max(self.blk, (1 << 30) // per_d // self.blk * self.blk))
+        self.dchunk = int(dchunk) if dchunk else default_dchunk(self.no, self.nv, self.blk)
         self.kind = None if precision == "fp64" else contract.KIND[precision]
         self.dev = torch.device(device)
         self.ws = torch.empty((_c_rccsdt_q.q_group_epilogue_workspace_bytes() + 7) // 8, dtype=f64,

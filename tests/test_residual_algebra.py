@@ -63,3 +63,17 @@ def test_s3_form_matches_oracle(oracle, pair_symmetric):
     r3 += e('ad,qdbc->qabc', Fvv, t3) + e('bd,qadc->qabc', Fvv, t3) + e('cd,qabd->qabc', Fvv, t3)
     r3 += e('abde,qdec->qabc', Wvvvv, t3) + e('acde,qdbe->qabc', Wvvvv, t3) + e('bcde,qade->qabc', Wvvvv, t3)
     np.testing.assert_allclose(r3, ref, rtol=0, atol=1e-10 * np.abs(ref).max())
+
+
+def test_woooo_k_pieces():
+    """K pieces of the K-major U split: one piece while (K - 1) * stride fits in 31 bits, else
+    pieces of whole multiples of 8 (the last one the rest) whose offsets all fit."""
+    from dcc.t3_residual import woooo_k_pieces
+    assert woooo_k_pieces(10, 90) == [100]
+    p = woooo_k_pieces(15, 93)
+    stride = 15 * 93 ** 3
+    assert p == [176, 49] and sum(p) == 225 and all(k % 8 == 0 for k in p[:-1])
+    assert all((k - 1) * stride < (1 << 31) - 1 for k in p)
+    assert woooo_k_pieces(5, 6, limit=8 * 5 * 6 ** 3 + 1) == [8, 8, 8, 1]
+    with pytest.raises(ValueError):
+        woooo_k_pieces(4, 10, limit=100)
