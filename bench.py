@@ -244,7 +244,7 @@ def reference_arm(args, rank, world):
     v = statistics.mean(times)
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": v * 1e3, "higher_is_better": False, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded numpy, BASELINE config 2 distributions)",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded numpy; e_occ U[-1.5,-0.3], e_vir U[0.1,3.0], t2 N(0,1e-2), ERIs N(0,0.1) 8-fold symmetric)",
             "config": {"workload": "rccsdt_t3_iteration", "nocc": NOCC, "nvir": NVIR, "n_blocks": 220},
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": os.cpu_count(), "kind": kind,
                              "sample": "%d of 220 blocks per step, scaled by 220/%d; reference C helpers (OpenMP) for "
@@ -537,7 +537,7 @@ def main():
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms_mixed / args.steps, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64 storage; " + args.precision + " products, f32 accumulate",
-        "data": "synthetic (seeded torch generator; BASELINE config 2 distributions)",
+        "data": "synthetic (seeded torch generator; e_occ U[-1.5,-0.3], e_vir U[0.1,3.0], t2 N(0,1e-2), ERIs N(0,0.1) 8-fold symmetric)",
         "config": {"workload": "rccsdt_t3_iteration", "nocc": NOCC, "nvir": NVIR, "n_blocks": n3,
                    "terms": "compute_r3_tri (W_vvvo.t2, W_vooo.t2, F_vv.t3, OO W_ovov/W_ovvo/F_oo/W_oooo.t3, "
                             "W_vvvv.t3), P3_full, divide, update, norms",

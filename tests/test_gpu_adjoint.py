@@ -5,7 +5,7 @@
   * central finite differences (h = 1e-5) of <lam, r3> along 64 random
     directions in all inputs at once equal <grad, direction>;
   * the split-precision backward agrees with FP64 to the split accuracy.
-nocc=6, nvir=40 (BASELINE adjoint configuration) and a small case."""
+nocc=6, nvir=40 (the adjoint-check size, seeded synthetic inputs) and a small case."""
 import itertools
 
 import numpy as np

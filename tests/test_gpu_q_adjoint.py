@@ -6,7 +6,7 @@
     blocks), relative 1e-10 of the largest entry, at nocc=3 / nvir=7;
   * central finite differences (h = 1e-5) of g_b [Q] + g_p (Q) along 64 random
     directions in all inputs at once equal <grad, direction> to 1e-6 relative,
-    at nocc=6 / nvir=40 (the BASELINE adjoint configuration)."""
+    at nocc=6 / nvir=40 (the adjoint-check size, seeded synthetic inputs)."""
 import numpy as np
 import pytest
 
