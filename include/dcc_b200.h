@@ -40,7 +40,7 @@ enum {
     DCC_ERR_NULL = 3,        /* required pointer is NULL */
     DCC_ERR_CUDA = 4,        /* CUDA runtime / launch failure */
     DCC_ERR_TIMEOUT = 5,     /* a bounded device-side wait gave up */
-    DCC_ERR_UNSUPPORTED = 6, /* valid request this build does not implement */
+    DCC_ERR_UNSUPPORTED = 6, /* valid request the library does not implement */
     DCC_ERR_NOT_LOCAL = 7,   /* requested block is not stored (reference: silent no-op) */
     DCC_ERR_WORKSPACE = 8    /* workspace argument too small */
 };
