@@ -24,9 +24,14 @@ _dbl = ctypes.c_double
 _vp = ctypes.c_void_p
 
 
-def build():
-    """Compile the C restatement (and the reference library when its sources exist)."""
-    subprocess.run(["make", "-s", "-C", HERE], check=True)
+def build(reference_dir=None):
+    """Compile the C restatement, and the reference library when `reference_dir` (default:
+    the DCC_REFERENCE environment variable) names a reference checkout with its sources."""
+    reference_dir = reference_dir or os.environ.get("DCC_REFERENCE")
+    cmd = ["make", "-s", "-C", HERE]
+    if reference_dir and os.path.isdir(os.path.join(reference_dir, "src")):
+        cmd.append("REF_SRC=%s" % os.path.join(reference_dir, "src"))
+    subprocess.run(cmd, check=True)
 
 
 def _ptr(a):
