@@ -1,4 +1,5 @@
 // Error reporting and small shared tables of the dcc_b200 library.
+#include <cuda.h>
 #include <stdarg.h>
 #include <string.h>
 
@@ -24,6 +25,28 @@ int launch_status(const char *what) {
         return DCC_ERR_CUDA;
     }
     return DCC_OK;
+}
+
+unsigned long long current_context_id() {
+    typedef CUresult (*GetCurrentFn)(CUcontext *);
+    typedef CUresult (*GetIdFn)(CUcontext, unsigned long long *);
+    static GetCurrentFn get_current = [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        return (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
+                q == cudaDriverEntryPointSuccess) ? (GetCurrentFn)p : (GetCurrentFn)nullptr;
+    }();
+    static GetIdFn get_id = [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        return (cudaGetDriverEntryPoint("cuCtxGetId", &p, cudaEnableDefault, &q) == cudaSuccess &&
+                q == cudaDriverEntryPointSuccess) ? (GetIdFn)p : (GetIdFn)nullptr;
+    }();
+    CUcontext ctx = nullptr;
+    if (!get_current || get_current(&ctx) != CUDA_SUCCESS || !ctx) return 0;
+    unsigned long long id = 0;
+    if (get_id && get_id(ctx, &id) == CUDA_SUCCESS) return id + 1;
+    return (unsigned long long)(uintptr_t)ctx;
 }
 
 int p4_pattern(const char *name, double p[9]) {

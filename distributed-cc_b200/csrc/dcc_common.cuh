@@ -26,6 +26,11 @@ int p4_pattern(const char *name, double p[9]);
 // Status after a launch: DCC_ERR_CUDA with the runtime's message on failure.
 int launch_status(const char *what);
 
+// A process-unique id of the calling thread's current CUDA context (0 when there is none).
+// Caches of device-symbol addresses key on it, so a context created after a device reset
+// looks the addresses up again instead of using the dead context's.
+unsigned long long current_context_id();
+
 #define DCC_REQUIRE(cond, code, ...)      \
     do {                                  \
         if (!(cond)) {                    \

@@ -12,6 +12,8 @@
 #include <stdarg.h>
 #include <string.h>
 
+#include <mutex>
+
 #include "async_util.cuh"
 #include "dcc_common.cuh"
 
@@ -630,15 +632,22 @@ int p3_pattern(const char *name, double p[5]) {
 static __device__ int g_sym_status;
 
 static int *sym_status_word() {
-    static int *cache[64] = {};
+    static std::mutex mu;
+    static struct {
+        unsigned long long ctx;
+        int *addr;
+    } cache[64] = {};
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
-    if (!cache[dev]) {
+    std::lock_guard<std::mutex> lock(mu);
+    unsigned long long ctx = current_context_id();
+    if (!cache[dev].addr || !ctx || cache[dev].ctx != ctx) {
         void *p = nullptr;
         if (cudaGetSymbolAddress(&p, g_sym_status) != cudaSuccess) return nullptr;
-        cache[dev] = (int *)p;
+        cache[dev].addr = (int *)p;
+        cache[dev].ctx = current_context_id();
     }
-    return cache[dev];
+    return cache[dev].addr;
 }
 
 // The TMA orbit-tile kernel on nblocks nvir^3 blocks (even nvir, 16-byte aligned buffers);
@@ -1998,7 +2007,6 @@ extern "C" int dcc_t3_perm_gather_tma(double *r3, const int32_t *ijk, int64_t nb
 
 // ---------------------------------------------------------------- no-allocation update
 
-#include <mutex>
 
 namespace dcc {
 
@@ -2013,12 +2021,15 @@ constexpr int64_t NOALLOC_MAX_CTAS = 8192;
 // all calls on a device share it.
 static __device__ __align__(256) double g_update_scratch[2 * NOALLOC_MAX_CTAS];
 
-// Device address of g_update_scratch for the current device, looked up once per
-// device.  In host code the symbol names a host-side stand-in, so kernels must
-// be given this address instead.
+// Device address of g_update_scratch for the current device, looked up once per device
+// (again only if the device's context was replaced, e.g. after cudaDeviceReset).  In host
+// code the symbol names a host-side stand-in, so kernels must be given this address instead.
 static int update_scratch_address(double **out) {
     static std::mutex mu;
-    static double *addr[128] = {nullptr};
+    static struct {
+        unsigned long long ctx;
+        double *addr;
+    } cache[128] = {};
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) {
@@ -2030,16 +2041,18 @@ static int update_scratch_address(double **out) {
         return DCC_ERR_UNSUPPORTED;
     }
     std::lock_guard<std::mutex> lock(mu);
-    if (!addr[dev]) {
+    unsigned long long ctx = current_context_id();
+    if (!cache[dev].addr || !ctx || cache[dev].ctx != ctx) {
         void *p = nullptr;
         e = cudaGetSymbolAddress(&p, g_update_scratch);
         if (e != cudaSuccess || !p) {
             set_error("cudaGetSymbolAddress(update scratch): %s", cudaGetErrorString(e));
             return DCC_ERR_CUDA;
         }
-        addr[dev] = (double *)p;
+        cache[dev].addr = (double *)p;
+        cache[dev].ctx = current_context_id();
     }
-    *out = addr[dev];
+    *out = cache[dev].addr;
     return DCC_OK;
 }
 

@@ -490,13 +490,3 @@ def wvvvv_t3_fp64_(r3, W, t3, alpha=1.0):
 def wvvvv_flops(nblocks, nvir):
     """Algorithmic FLOPs of the three einsums (2 M N K each)."""
     return 3 * 2 * nblocks * nvir ** 5
-
-
-def einsum_reference(W, t3):
-    """numpy FP64 restatement of the three einsums (test oracle helper)."""
-    r = np.zeros_like(t3)
-    for q in range(t3.shape[0]):
-        r[q] += np.einsum("abde,dec->abc", W, t3[q])
-        r[q] += np.einsum("acde,dbe->abc", W, t3[q])
-        r[q] += np.einsum("bcde,ade->abc", W, t3[q])
-    return r

@@ -40,13 +40,14 @@ def _case_coefficients(ijk):
     return c1, c2, c3
 
 
-def r1_add_t3_(r1, t1_eris, t3, ijk, nocc):
-    """r1 += T3 part of r1 (distr_cc/rccsdt.py:262-296); t3 canonical blocks."""
+def r1_add_t3_(r1, t1_eris, t3, ijk, nocc, oovv=None, V=None):
+    """r1 += T3 part of r1 (distr_cc/rccsdt.py:262-296); t3 canonical blocks.  oovv: the
+    [o,o,v,v] slice of t1_eris when the caller passes the slice alone (t1_eris None);
+    V: a scratch buffer of t3's size."""
     nvir = t3.shape[1]
-    o, v = slice(0, nocc), slice(nocc, None)
-    V = t3.clone()
+    V = t3.clone() if V is None else V.copy_(t3)
     _c_rccsdt.t3_spin_summation_inplace_(V, V.shape[0], nvir, "P3_422", 1.0, 0.0)
-    E = t1_eris[o, o, v, v]
+    E = oovv if oovv is not None else eris_slices(t1_eris, None, nocc)["oovv"]
     il, jl, kl = ijk[:, 0].long(), ijk[:, 1].long(), ijk[:, 2].long()
     c1, c2, c3 = _case_coefficients(ijk)
     Ra = torch.einsum('qbc,qabc->qa', E[jl, kl], V) * c1[:, None]
@@ -57,31 +58,65 @@ def r1_add_t3_(r1, t1_eris, t3, ijk, nocc):
     return r1
 
 
-def p3_201_all(t3, nocc, U=None):
-    """X = P3_201 of every ordered block of the unpacked T3 [x][y][z][a][b][c]."""
+def p3_201_all(t3, nocc, U=None, out=None):
+    """X = P3_201 of every ordered block of the unpacked T3 [x][y][z][a][b][c].
+
+    U: the unpacked T3 when the caller has it already (unpacked here otherwise);
+    out: a buffer of U's size to hold X (a fresh one otherwise)."""
     nvir = t3.shape[1]
     if U is None:
         U = torch.empty((nocc ** 3, nvir, nvir, nvir), dtype=f64, device=t3.device)
         unpack_all_(t3, U, nocc, nvir)
-    X = U.clone()
+    X = U.clone() if out is None else out.view(U.shape).copy_(U)
     _c_rccsdt.t3_spin_summation_inplace_(X, X.shape[0], nvir, "P3_201", 1.0, 0.0)
     return X.view(nocc, nocc, nocc, nvir, nvir, nvir)
 
 
+def eris_slices(t1_eris, t1_fock, nocc):
+    """The pieces of the dressed Fock matrix and ERIs the feedback reads (so a caller can
+    upload these instead of the whole [nmo]^4 tensor): fock_ov [o,v], oovv, vovv, ooov."""
+    o, v = slice(0, nocc), slice(nocc, None)
+    sl = {"oovv": t1_eris[o, o, v, v], "vovv": t1_eris[v, o, v, v], "ooov": t1_eris[o, o, o, v]}
+    if t1_fock is not None:
+        sl["fock_ov"] = t1_fock[o, v]
+    return sl
+
+
+def r2_add_t3_x_(r2, fock_ov, vovv, ooov, X):
+    """r2 += T3 part of r2 (distr_cc/rccsdt.py:300-316) from X = p3_201_all(t3), one leading
+    occupied index x at a time (the temporaries stay one 1/nocc slice of X):
+        r2[y,z,b,c] += 1/2 f[x,a] X[x,y,z,a,b,c] + E[c,x,a,d] X[x,y,z,d,b,a]
+        r2[y,l,b,c] -= E[z,x,l,a] X[x,y,z,a,b,c]."""
+    no, nv = X.shape[0], X.shape[3]
+    e = torch.einsum
+    for x in range(no):
+        Xx = X[x]
+        r2.view(no * no, nv * nv).add_(
+            torch.matmul(fock_ov[x].view(1, 1, nv), Xx.reshape(no * no, nv, nv * nv)).view(no * no, nv * nv),
+            alpha=0.5)
+        r2 += e('cad,yzdba->yzbc', vovv[:, x], Xx)
+        r2 -= e('zla,yzabc->ylbc', ooov[:, x], Xx)
+    return r2
+
+
 def r2_add_t3_(r2, t1_fock, t1_eris, X, nocc):
     """r2 += T3 part of r2 (distr_cc/rccsdt.py:300-316) from X = p3_201_all(t3)."""
-    o, v = slice(0, nocc), slice(nocc, None)
+    sl = eris_slices(t1_eris, t1_fock, nocc)
+    return r2_add_t3_x_(r2, sl["fock_ov"], sl["vovv"], sl["ooov"], X)
+
+
+def intermediates_t3_add_x_(W_vooo, W_vvvo, oovv, X):
+    """W_vooo, W_vvvo += T3 parts (distr_cc/rccsdt.py:323-366) from X = p3_201_all(t3), one
+    leading occupied index x at a time:
+        W_vooo[a,m,y,z] += E[m,x,d,e] X[x,y,z,e,a,d],  W_vvvo[a,b,d,y] -= E[z,x,d,e] X[x,y,z,e,b,a]."""
+    no = X.shape[0]
     e = torch.einsum
-    r2 += 0.5 * e('xa,xyzabc->yzbc', t1_fock[o, v], X)
-    r2 += e('cxad,xyzdba->yzbc', t1_eris[v, o, v, v], X)
-    r2 -= e('zxla,xyzabc->ylbc', t1_eris[o, o, o, v], X)
-    return r2
+    for x in range(no):
+        W_vooo += e('mde,yzead->amyz', oovv[:, x], X[x])
+        W_vvvo -= e('zde,yzeba->abdy', oovv[:, x], X[x])
+    return W_vooo, W_vvvo
 
 
 def intermediates_t3_add_(W_vooo, W_vvvo, t1_eris, X, nocc):
     """W_vooo, W_vvvo += T3 parts (distr_cc/rccsdt.py:323-366) from X = p3_201_all(t3)."""
-    o, v = slice(0, nocc), slice(nocc, None)
-    E = t1_eris[o, o, v, v]
-    W_vooo += torch.einsum('mxde,xyzead->amyz', E, X)
-    W_vvvo -= torch.einsum('zxde,xyzeba->abdy', E, X)
-    return W_vooo, W_vvvo
+    return intermediates_t3_add_x_(W_vooo, W_vvvo, eris_slices(t1_eris, None, nocc)["oovv"], X)

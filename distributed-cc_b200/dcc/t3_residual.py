@@ -30,8 +30,8 @@ In mixed precision S is built by five split-precision tcgen05 GEMMs written
 straight into S's [i][j][k][a][b][c] layout (-Y first, which initializes S; X;
 T2 and T5/2 as one GEMM over the concatenated contraction index; T1 reusing
 T2's U operand; the K = nocc^2 W_oooo / F_oo part over a K-major split of U),
-and one gather kernel applies the symmetrization to S (the FP64 path keeps Y
-apart and gathers S and Y).  W_vvvv.t3 (three strings, the dominant cost) are
+and one gather kernel applies the symmetrization to S (the FP64 path builds S
+the same way from DGEMMs, one occupied slice at a time).  W_vvvv.t3 (three strings, the dominant cost) are
 three split-precision GEMMs that accumulate straight into r3; the three
 F_vv.t3 strings ride in them as extra terms of the W operand
 (contract.WvvvvT3).  The FP64 path runs F_vv.t3 as batched DGEMMs.
@@ -203,9 +203,6 @@ class T3Residual:
         full = (no ** 3, nv, nv, nv)
         self.S = torch.empty(full, dtype=f64, device=device)  # [i][j][k][a][b][c]
         self.U = torch.empty(full, dtype=f64, device=device) if with_oo else None
-        self.Y = None  # [(i,j,a),(k,b,c)], allocated by y_ (the FP64 path; the split path adds -Y into S)
-        Ny = no * nv * nv
-        self.y_strides = (no * nv * Ny, nv * Ny, nv * nv, Ny, nv, 1)
         self.Ganti = None
         self.gstatus = torch.zeros(1, dtype=torch.int32, device=device)  # gather pipeline timeouts
         if precision != "fp64":
@@ -234,28 +231,8 @@ class T3Residual:
                 else:
                     self.wooa = contract.Split(no * no, kind=k, device=device, pieces=self.woo_pieces)
                     self.woob = contract.Split(no * nv ** 3, kind=k, device=device, pieces=self.woo_pieces)
-        else:
-            self.X = torch.empty((no * nv * nv, no * no * nv), dtype=f64, device=device)  # [(j,a,b),(i,k,c)]
 
     # ------------------------------------------------------------ pieces
-    def y_(self, d):
-        """Y[(i,j,a),(k,b,c)] = sum_l W_vooo[a,l,i,j] t2[l,k,b,c] (K = nocc: bound by writing Y; a
-        split GEMM in mixed precision, which writes Y at a higher rate than the FP64 DGEMM)."""
-        no, nv = self.no, self.nv
-        if self.Y is None:
-            self.Y = torch.empty((no * no * nv, no * nv * nv), dtype=f64, device=self.dev)
-        if self.precision == "fp64":
-            A = d.W_vooo.permute(2, 3, 0, 1).reshape(no * no * nv, no)
-            Bm = d.t2.permute(1, 2, 3, 0).reshape(no * nv * nv, no)
-            torch.matmul(A, Bm.t(), out=self.Y)
-            return self.Y
-        c = contract
-        # A rows (i,j,a) of W_vooo[a,l,i,j], K = l; B rows (k,b,c) of t2[l,k,b,c], K = l
-        self.ya.fill(d.W_vooo, c.three(no, nv, no, 1, no ** 3), c.lin(no * no))
-        self.yb.fill(d.t2, c.lin(1), c.lin(no * nv * nv))
-        c.gemm_(self.ya, self.yb, self.Y, c.lin(no * nv * nv), c.lin(1), 1.0, 0.0, self.status)
-        return self.Y
-
     def _y_into_s(self, d):
         """S = -Y in S's [i][j][k][a][b][c] layout (split path): rows (i,j,a), columns (k,b,c).  Y
         then rides in S's permutation sum, and the gather reads one source instead of two."""
@@ -266,14 +243,18 @@ class T3Residual:
         c.gemm_(self.ya, self.yb, self.S, c.three(no, nv, no * no * nv ** 3, no * nv ** 3, nv * nv),
                 c.two(nv * nv, nv ** 3, 1), -1.0, 0.0, self.status)
 
-    def s_(self, d, t3, inputs_ready=None):
-        """S (see the module docstring); U = unpacked t3 when the OO terms are on.  The unpack
-        reads only t3, so it runs before the wait on `inputs_ready` (an optional CUDA event that
-        marks the arrival of d's tensors)."""
+    def unpack_(self, t3):
+        """U = t3 unpacked to every ordered (i,j,k) (the operand of the OO terms)."""
+        return unpack_all_(t3, self.U, self.no, self.nv)
+
+    def s_(self, d, t3, inputs_ready=None, unpacked=False):
+        """S (see the module docstring); U = unpacked t3 when the OO terms are on (already
+        there when `unpacked`).  The unpack reads only t3, so it runs before the wait on
+        `inputs_ready` (an optional CUDA event that marks the arrival of d's tensors)."""
         no, nv = self.no, self.nv
         S = self.S
-        if self.with_oo:
-            unpack_all_(t3, self.U, no, nv)
+        if self.with_oo and not unpacked:
+            self.unpack_(t3)
         if inputs_ready is not None:
             torch.cuda.current_stream().wait_event(inputs_ready)
         if self.precision == "fp64":
@@ -333,20 +314,32 @@ class T3Residual:
         c.gemm_(self.t1a, self.oob, S, *t1["out"], t1["alpha"], t1["beta"], st, Kp=self.t1a.Kp)
 
     def _s_fp64(self, d):
+        """S in FP64 (cuBLAS DGEMM through torch), one occupied slice at a time so the
+        temporaries stay 1/nocc of S: S = X - Y (+ the OO terms when with_oo)."""
         no, nv = self.no, self.nv
         Sv = self.S.view(no, no, no, nv, nv, nv)
-        Wt = d.W_vvvo.permute(3, 0, 1, 2).reshape(no * nv * nv, nv)
-        T2m = d.t2.permute(0, 1, 3, 2).reshape(no * no * nv, nv)
-        torch.matmul(Wt, T2m.t(), out=self.X)
-        Sv.copy_(self.X.view(no, nv, nv, no, no, nv).permute(3, 0, 4, 1, 2, 5))  # (j,a,b,i,k,c) -> (i,j,k,a,b,c)
+        # X[i,j,k,a,b,c] = sum_d W_vvvo[a,b,d,j] t2[i,k,d,c]: per j, [(a,b), d] . [d, (i,k,c)]
+        T2m = d.t2.permute(2, 0, 1, 3).reshape(nv, no * no * nv)
+        for j in range(no):
+            Xj = torch.matmul(d.W_vvvo[..., j].reshape(nv * nv, nv), T2m)
+            Sv[:, j].copy_(Xj.view(nv, nv, no, no, nv).permute(2, 3, 0, 1, 4))
+        # - Y[i,j,k,a,b,c] = - sum_l W_vooo[a,l,i,j] t2[l,k,b,c]: per i, [(j,a), l] . [l, (k,b,c)]
+        T2l = d.t2.reshape(no, no * nv * nv)
+        for i in range(no):
+            Yi = torch.matmul(d.W_vooo[:, :, i, :].permute(2, 0, 1).reshape(no * nv, no), T2l)
+            Sv[i].sub_(Yi.view(no, nv, no, nv, nv).permute(0, 2, 1, 3, 4))
         if not self.with_oo:
             return
         Uv = self.U.view(no, no, no, nv, nv, nv)
         e = torch.einsum
         G2 = -0.5 * (d.W_ovov + d.W_ovvo.permute(0, 1, 3, 2))
-        Sv.sub_(e('lbid,jkldca->ijkabc', d.W_ovov, Uv))
-        Sv.add_(e('laid,jkldcb->ijkabc', G2, Uv))
-        Sv.add_(e('ladi,jklbcd->ijkabc', 0.5 * d.W_ovvo, Uv))
+        Wh = 0.5 * d.W_ovvo
+        for j in range(no):
+            Uj = Uv[j]  # [k][l][...]
+            Sj = Sv[:, j]
+            Sj.sub_(e('lbid,kldca->ikabc', d.W_ovov, Uj))
+            Sj.add_(e('laid,kldcb->ikabc', G2, Uj))
+            Sj.add_(e('ladi,klbcd->ikabc', Wh, Uj))
 
     def fvv_(self, r3, d, t3):
         """F_vv.t3 (distr_cc/rccsdt.py:400-402), FP64 in both precisions (bandwidth-bound)."""
@@ -370,22 +363,18 @@ class T3Residual:
             return None
         return self.wvvvv.tune(torch.empty_like(t3), d.W_vvvv, t3, F=d.F_vv)
 
-    def compute(self, d, t3, r3=None, wvvvv_ready=None, inputs_ready=None):
+    def compute(self, d, t3, r3=None, wvvvv_ready=None, inputs_ready=None, unpacked=False):
         """r3 = compute_r3_tri for canonical t3 (the OO batch terms included when with_oo).
 
         wvvvv_ready: optional CUDA event the W_vvvv.t3 part waits for, so a caller can
         stream W_vvvv to the device while the other terms run.  inputs_ready: optional CUDA
         event for d's other tensors, waited for after the unpack of t3 (which needs none of
-        them), so their upload overlaps it."""
+        them), so their upload overlaps it.  unpacked: U holds t3 unpacked already (unpack_)."""
         if r3 is None:
             r3 = torch.empty_like(t3)
         no, nv = self.no, self.nv
-        S = self.s_(d, t3, inputs_ready)
-        if self.precision == "fp64":
-            Y = self.y_(d)
-            sources = [(S, 1.0, full_strides(no, nv), ALL_S3), (Y, -1.0, self.y_strides, ALL_S3)]
-        else:
-            sources = [(S, 1.0, full_strides(no, nv), ALL_S3)]  # S holds -Y already
+        S = self.s_(d, t3, inputs_ready, unpacked=unpacked)
+        sources = [(S, 1.0, full_strides(no, nv), ALL_S3)]  # S holds -Y already
         perm_gather_(r3, d.ijk, nv, 0.0, sources, nocc=no, status=self.gstatus)
         if self.Ganti is not None:
             perm_gather_(r3, d.ijk, nv, 1.0, [(self.Ganti, 1.0, full_strides(no, nv), OOOO_SET)], nocc=no,

@@ -1,14 +1,14 @@
 """Small, self-contained launches of single kernels for profiler captures.
 
-    python -m dcc.profile_cases gemm   [--kind bf16x3] [--reps 3]
-    python -m dcc.profile_cases p3     [--reps 3] [--nvir 90] [--op p3|p3_422|roundtrip|triple|transpose] [--time]
-    python -m dcc.profile_cases update [--reps 3]
-    python -m dcc.profile_cases q      [--reps 3]
-    python -m dcc.profile_cases gather [--reps 3]
-    python -m dcc.profile_cases xgemm  [--reps 3]
-    python -m dcc.profile_cases oogemm [--reps 3]
-    python -m dcc.profile_cases unpack [--reps 3]
-    python -m dcc.profile_cases qgroup [--reps 3]
+    python profile_cases.py gemm   [--kind bf16x3] [--reps 3]
+    python profile_cases.py p3     [--reps 3] [--nvir 90] [--op p3|p3_422|roundtrip|triple|transpose] [--time]
+    python profile_cases.py update [--reps 3]
+    python profile_cases.py q      [--reps 3]
+    python profile_cases.py gather [--reps 3]
+    python profile_cases.py xgemm  [--reps 3]
+    python profile_cases.py oogemm [--reps 3]
+    python profile_cases.py unpack [--reps 3]
+    python profile_cases.py qgroup [--reps 3]
 
 Each case builds its inputs once and launches the kernel `reps` times, so a
 profiler can skip the warm-up launches and capture the last one.  Sizes are
@@ -20,7 +20,7 @@ import argparse
 import os
 import sys
 
-sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, os.path.join(os.path.dirname(os.path.abspath(__file__)), "distributed-cc_b200"))
 
 import torch  # noqa: E402
 

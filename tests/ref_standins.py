@@ -395,3 +395,72 @@ def unpack_unique_replicated_tamps(mycc, vector, template_tamps, scale=1.0):
         out.append(t)
         offset += size
     return out, offset
+
+
+# ------------------------------------- the DIIS helpers of distr_cc/_runtime.py, rccsdt.py
+
+def norm_sq_from_norms(norms):
+    """distr_cc/_runtime.py:87-88."""
+    return sum(float(n) * float(n) for n in norms)
+
+
+def resolve_nvir_diis(mycc, nvir):
+    """distr_cc/_runtime.py:121-128."""
+    nd = getattr(mycc, "nvir_diis", None)
+    return nvir if nd is None else min(int(nd), nvir)
+
+
+def _safe_update_norm(norm_sq):
+    return np.sqrt(max(float(norm_sq), 0.0))
+
+
+def _max_t_diis_update_norm(mycc, res_norm, normt, adiis, nvir_diis, nvir, total_attr, active_attr):
+    """distr_cc/rccsdt.py:990-999 (with _safe_update_norm, :979-980)."""
+    delta = getattr(adiis, "last_delta_norm_sq", None)
+    if delta is None:
+        return float(normt) if res_norm is None else _safe_update_norm(norm_sq_from_norms(res_norm))
+    delta = float(delta)
+    if nvir_diis < nvir:
+        total = float(getattr(mycc, total_attr, res_norm[-1] * res_norm[-1]))
+        active = float(getattr(mycc, active_attr, total))
+        delta += max(total - active, 0.0)
+    return _safe_update_norm(delta)
+
+
+class IMDS:
+    """pyscf.cc.rccsdt._IMDS: a bag of intermediates."""
+
+
+def route_module(replay):
+    """A namespace carrying what the routed update_amps_rccsdt_tri_ / run_diis_t3 take from the
+    reference module they are installed in: the lower-order replay, _IMDS and the DIIS
+    helpers above."""
+    ns = types.SimpleNamespace(_IMDS=IMDS, resolve_nvir_diis=resolve_nvir_diis,
+                               pack_unique_replicated_tamps=pack_unique_replicated_tamps,
+                               unpack_unique_replicated_tamps=unpack_unique_replicated_tamps,
+                               _max_t_diis_update_norm=_max_t_diis_update_norm,
+                               norm_sq_from_norms=norm_sq_from_norms)
+    return replay.bind(ns)
+
+
+class CanonicalT3Dist:
+    """One rank holding every canonical block in canonical order (the reference's
+    DistributedT3IJK at one rank)."""
+
+    def __init__(self, nocc):
+        self.local_triples = [(i, j, k) for i in range(nocc) for j in range(i, nocc) for k in range(j, nocc)]
+
+    def iter_local_ijk(self):
+        for q, (i, j, k) in enumerate(self.local_triples):
+            yield i, j, k, q
+
+
+class StoredT4Dist:
+    """One rank holding the listed stored T4 blocks in that order."""
+
+    def __init__(self, ijkl):
+        self.local_quadruples = [tuple(int(x) for x in q) for q in ijkl]
+
+    def iter_local_ijkl(self):
+        for q, (i, j, k, l) in enumerate(self.local_quadruples):
+            yield i, j, k, l, q

@@ -38,6 +38,65 @@ def test_routing_and_idempotence(monkeypatch):
     assert routed == ["r3"]
 
 
+def test_update_and_diis_routes_and_class_attributes(monkeypatch):
+    """update_amps_rccsdt_tri_ / run_diis_t3 route as module functions (called with the module,
+    whose lower-order functions they use) and as the RCCSDT class attributes the reference's
+    kernel calls (distr_cc/rccsdt.py:1266, 1271)."""
+    calls = []
+
+    def upd(mycc, tamps, eris):
+        calls.append("orig_upd")
+        return "orig"
+
+    def diis(mycc, *a, **k):
+        calls.append("orig_diis")
+        return "orig"
+
+    class RCCSDT:
+        update_amps_ = upd
+        run_diis_t3 = diis
+
+    mod = types.SimpleNamespace(update_amps_rccsdt_tri_=upd, run_diis_t3=diis, RCCSDT=RCCSDT)
+    got = {}
+    monkeypatch.setitem(backend._MOD_ROUTES, "update_amps_rccsdt_tri_",
+                        lambda mycc, tamps, eris, mod=None: got.setdefault("upd_mod", mod) and "gpu")
+    monkeypatch.setitem(backend._MOD_ROUTES, "run_diis_t3",
+                        lambda mycc, *a, mod=None, **k: got.setdefault("diis_mod", mod) and "gpu")
+    names = backend.install(mod)
+    assert {"update_amps_rccsdt_tri_", "run_diis_t3", "RCCSDT.update_amps_", "RCCSDT.run_diis_t3"} <= set(names)
+    cc = RCCSDT()
+    cc.einsum_backend, cc.comm = "numpy", backend.SingleRankComm()
+    assert cc.update_amps_([], None) == "orig" and cc.run_diis_t3([], None, 0, 0.0, 0.0, None) == "orig"
+    cc.einsum_backend = "cuda"
+    assert cc.update_amps_([], None) == "gpu" and cc.run_diis_t3([], None, 0, 0.0, 0.0, None) == "gpu"
+    assert got["upd_mod"] is mod and got["diis_mod"] is mod
+    assert calls == ["orig_upd", "orig_diis"]
+    assert backend.install(mod) == []
+
+
+def test_t3_local_order_checked():
+    """A t3_local whose blocks are not in canonical order (e.g. loaded from a checkpoint of
+    another distribution) is refused instead of being read in the wrong order."""
+    from dcc.synthetic import canonical_ijk
+    nocc = 3
+    trip = canonical_ijk(nocc)
+
+    class Dist:
+        def __init__(self, order):
+            self.order = order
+
+        def iter_local_ijk(self):
+            for q, (i, j, k) in enumerate(self.order):
+                yield i, j, k, q
+    mycc = types.SimpleNamespace(nocc=nocc, nmo=nocc + 4)
+    t3 = np.zeros((len(trip), 4, 4, 4))
+    assert backend._t3_local(mycc, (Dist(trip), t3)) is t3
+    with pytest.raises(RuntimeError, match="canonical order"):
+        backend._t3_local(mycc, (Dist(trip[::-1]), t3))
+    with pytest.raises(RuntimeError, match="canonical order"):
+        backend._t3_local(mycc, (Dist(trip), t3[:-1]))
+
+
 def test_multi_rank_refused():
     class TwoRanks(backend.SingleRankComm):
         def Get_size(self):
@@ -47,6 +106,8 @@ def test_multi_rank_refused():
         backend.compute_r3_tri(mycc, None, None, (None, None))
     with pytest.raises(RuntimeError, match="one rank"):
         backend.q_kernel(mycc, comm=TwoRanks())
+    with pytest.raises(RuntimeError, match="one rank"):
+        backend.q_kernel(mycc)  # comm=None falls back to mycc.comm, as the reference does
 
 
 def test_single_rank_comm():

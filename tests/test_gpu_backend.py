@@ -50,10 +50,12 @@ def test_compute_r3_tri(mods):
     mycc, imds, t2, t3, _, _ = _problem(3, 8, 1)
     want = er.compute_r3_tri_ref(er.Imds(imds.F_vv, imds.F_oo, imds.W_vvvo, imds.W_vooo, imds.W_vvvv, imds.W_ovov,
                                          imds.W_ovvo, imds.W_oooo), t2, t3, 3, with_oo=True)
+    fields = dict(vars(imds))
     got = backend.compute_r3_tri(mycc, imds, t2, (None, t3))
     np.testing.assert_allclose(got, want, rtol=0, atol=1e-11 * np.abs(want).max())
+    assert imds.W_vvvv is None and imds.W_ovov is None  # released as the reference does
     mycc.dcc_precision = "bf16x3"
-    got = backend.compute_r3_tri(mycc, imds, t2, (None, t3))
+    got = backend.compute_r3_tri(mycc, types.SimpleNamespace(**fields), t2, (None, t3))
     assert np.abs(got - want).max() <= 1e-4 * np.abs(want).max()
 
 

@@ -20,6 +20,16 @@ def C():
     return contract
 
 
+def einsum_reference(W, t3):
+    """numpy FP64 restatement of the three W_vvvv.t3 einsums (distr_cc/rccsdt.py:421-427)."""
+    r = np.zeros_like(t3)
+    for q in range(t3.shape[0]):
+        r[q] += np.einsum("abde,dec->abc", W, t3[q])
+        r[q] += np.einsum("acde,dbe->abc", W, t3[q])
+        r[q] += np.einsum("bcde,ade->abc", W, t3[q])
+    return r
+
+
 def _rel(a, b):
     return float((a - b).abs().max() / b.abs().max())
 
@@ -44,7 +54,7 @@ def test_wvvvv_t3_matches_einsum(C, kind, nblk, nv):
     W = rng.standard_normal((nv,) * 4) * 0.1
     t3 = rng.standard_normal((nblk,) + (nv,) * 3) * 1e-3
     r0 = rng.standard_normal(t3.shape) * 1e-3
-    want = r0 + C.einsum_reference(W, t3)
+    want = r0 + einsum_reference(W, t3)
     dW, dt3 = torch.from_numpy(W).cuda(), torch.from_numpy(t3).cuda()
     r = torch.from_numpy(r0.copy()).cuda()
     op = C.WvvvvT3(nblk, nv, kind)
@@ -157,7 +167,7 @@ def test_wvvvv_with_fvv_folded(C, kind):
     F = rng.standard_normal((nv, nv))
     t3 = rng.standard_normal((nblk,) + (nv,) * 3) * 1e-3
     e = np.einsum
-    want = C.einsum_reference(W, t3) + e('ad,qdbc->qabc', F, t3) + e('bd,qadc->qabc', F, t3) + e('cd,qabd->qabc', F, t3)
+    want = einsum_reference(W, t3) + e('ad,qdbc->qabc', F, t3) + e('bd,qadc->qabc', F, t3) + e('cd,qabd->qabc', F, t3)
     r = torch.zeros(t3.shape, dtype=torch.float64, device="cuda")
     op = C.WvvvvT3(nblk, nv, kind)
     op(r, torch.from_numpy(W).cuda(), torch.from_numpy(t3).cuda(), F=torch.from_numpy(F).cuda())

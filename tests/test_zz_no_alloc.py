@@ -63,7 +63,16 @@ def test_noalloc_matches_workspace_entry_twice(lib, nocc, nvir, nact):
 
 
 def test_noalloc_rejects_sizes_beyond_its_scratch(lib):
+    """One row more than the static array covers is refused before any launch.  The buffers
+    are real and sized for the call (nvir = 2, so 2^21 + 1 blocks are 134 MB each), so even a
+    launch would stay in bounds."""
     L, noalloc = lib
-    fake = ctypes.c_void_p(256)
-    rc = noalloc(fake, fake, fake, fake, 1100, 90, 90, 1, fake, None)  # 8.91e6 rows > 8 388 608
+    nblk, nvir = (1 << 21) + 1, 2  # rows = nblk * nvir^2 = 8 388 612 > 8 388 608
+    t3 = torch.zeros((nblk, nvir, nvir, nvir), dtype=torch.float64, device="cuda")
+    r3 = torch.zeros_like(t3)
+    eia = torch.full((1, nvir), -1.0, dtype=torch.float64, device="cuda")
+    ijk = torch.zeros((nblk, 3), dtype=torch.int32, device="cuda")
+    norms = torch.zeros(2, dtype=torch.float64, device="cuda")
+    stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    rc = noalloc(L.ptr(t3), L.ptr(r3), L.ptr(eia), L.ptr(ijk), nblk, nvir, nvir, 1, L.ptr(norms), stream)
     assert rc == 2 and "no-allocation limit" in L.last_error()
