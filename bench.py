@@ -470,17 +470,39 @@ def t4_line(torch, ranks, precision):
     return out
 
 
+class TriplesEnergy:
+    """E(t3): the T3 -> r2 strings (distr_cc/rccsdt.py:300-316, FP64), r2 symmetrized and
+    divided by the T2 denominators, contracted with (2<ij|ab> - <ij|ba>) -- how T3 reaches
+    the correlation energy through t2.  Linear in t3."""
+
+    def __init__(self, torch, d):
+        self.torch, self.d = torch, d
+        self.E_vovv = d.W_vvvo.permute(2, 3, 0, 1)  # <cx|ad> = <ad|cx>
+        self.E_ooov = d.W_vooo.permute(3, 2, 1, 0)  # <zx|la> = <al|xz>
+        self.D2 = (d.e_occ[:, None, None, None] + d.e_occ[None, :, None, None]
+                   - d.e_vir[None, None, :, None] - d.e_vir[None, None, None, :])
+        self.L = 2.0 * d.eris_vvoo.permute(2, 3, 0, 1) - d.eris_vvoo.permute(2, 3, 1, 0)
+        self.fock0 = torch.zeros(d.nocc, d.nvir, dtype=torch.float64, device="cuda")
+
+    def __call__(self, t3):
+        from dcc import t3_feedback
+        torch, d = self.torch, self.d
+        X = t3_feedback.p3_201_all(t3, d.nocc)
+        r2 = torch.zeros(d.nocc, d.nocc, d.nvir, d.nvir, dtype=torch.float64, device="cuda")
+        t3_feedback.r2_add_t3_x_(r2, self.fock0, self.E_vovv, self.E_ooov, X)
+        del X
+        return float((self.L * (r2 + r2.permute(1, 0, 3, 2)) / 2 / self.D2).sum())
+
+
 def iteration_energy_error(torch, nocc, nvir, precision):
     """How the split path's error in one T3 iteration reaches the correlation energy.
 
     The FP64 and split residuals of the same inputs go through the same update (P3_full,
-    divide, t3 += r3); the difference of the two new T3 is fed to the T2 residual by the
-    T3 -> r2 strings (distr_cc/rccsdt.py:300-316, FP64) and, divided by the T2 denominators,
-    to E = sum (2<ij|ab> - <ij|ba>) t2.  The same chain on the FP64 T3 itself gives the
-    triples' share of E.  r3 is linear in (t2, t3), so the ratio is independent of the
-    amplitudes' scale: abs_dE_at_10mEh is the error of a molecule whose triples contribute
-    10 mEh (the synthetic amplitudes are far larger than a molecule's)."""
-    from dcc import synthetic, t3_feedback, t3_residual
+    divide, t3 += r3); the difference of the two new T3 goes through TriplesEnergy, and so
+    does the FP64 T3 itself (the triples' share of E).  r3 is linear in (t2, t3), so the ratio
+    is independent of the amplitudes' scale: abs_dE_at_10mEh is the error of a molecule whose
+    triples contribute 10 mEh (the synthetic amplitudes are far larger than a molecule's)."""
+    from dcc import synthetic, t3_residual
     d = synthetic.make_inputs(nocc, nvir, seed=0)
     rs = {}
     for prec in ("fp64", precision):
@@ -494,26 +516,60 @@ def iteration_energy_error(torch, nocc, nvir, precision):
     t3_residual.update_t3_(t3m, rs[precision].clone(), d, workspace=ws)
     rel_r3 = float((rs[precision] - rs["fp64"]).abs().max() / rs["fp64"].abs().max())
     del rs
-    E_vovv = d.W_vvvo.permute(2, 3, 0, 1)
-    E_ooov = d.W_vooo.permute(3, 2, 1, 0)
-    D2 = (d.e_occ[:, None, None, None] + d.e_occ[None, :, None, None]
-          - d.e_vir[None, None, :, None] - d.e_vir[None, None, None, :])
-    L = 2.0 * d.eris_vvoo.permute(2, 3, 0, 1) - d.eris_vvoo.permute(2, 3, 1, 0)
-    fock0 = torch.zeros(nocc, nvir, dtype=torch.float64, device="cuda")
-
-    def energy(t3):
-        X = t3_feedback.p3_201_all(t3, nocc)
-        r2 = torch.zeros(nocc, nocc, nvir, nvir, dtype=torch.float64, device="cuda")
-        t3_feedback.r2_add_t3_x_(r2, fock0, E_vovv, E_ooov, X)
-        del X
-        return float((L * (r2 + r2.permute(1, 0, 3, 2)) / 2 / D2).sum())
-
+    energy = TriplesEnergy(torch, d)
     e_t3 = energy(t3f)
     de = energy(t3m - t3f)
-    del t3f, t3m, d
+    del t3f, t3m, d, energy
     torch.cuda.empty_cache()
     return {"nocc": nocc, "nvir": nvir, "r3_max_rel_err_vs_fp64": rel_r3, "e_t3_share_fp64": e_t3,
             "abs_dE": abs(de), "relative": abs(de / e_t3), "abs_dE_at_10mEh": abs(de / e_t3) * 1e-2}
+
+
+def converged_energy_error(torch, nocc, nvir, precision, sigma=0.2, tol=1e-9, max_iter=80, space=8):
+    """The T3 equations alone (t2 and the intermediates fixed) iterated to convergence with
+    DIIS in FP64 and in split precision from t3 = 0: t3 += P3_full(r3)/D with r3 =
+    compute_r3_tri (the update of distr_cc/rccsdt.py:941-971), DIIS over t3 (distr_cc/diis.py).
+    The intermediates that couple t3 to itself (W_vvvv, W_ovov, W_ovvo, W_oooo) are scaled by
+    `sigma` so that this fixed-point iteration contracts for the synthetic integrals (molecular
+    ones do without help).  The converged T3 of the two precisions go through TriplesEnergy;
+    their difference, relative to the FP64 triples share, is scaled to a molecule whose
+    triples contribute 10 mEh."""
+    import math
+    from dcc import synthetic, t3_residual
+    from dcc.diis import DIIS
+    d = synthetic.make_inputs(nocc, nvir, seed=0)
+    for k in ("W_vvvv", "W_ovov", "W_ovvo", "W_oooo"):
+        setattr(d, k, getattr(d, k) * sigma)
+    energy = TriplesEnergy(torch, d)
+    out = {"nocc": nocc, "nvir": nvir, "coupling_scale": sigma, "tol": tol}
+    t3s = {}
+    for prec in ("fp64", precision):
+        res = t3_residual.T3Residual(nocc, nvir, prec, with_oo=True)
+        t3 = torch.zeros_like(d.t3)
+        r3 = torch.empty_like(t3)
+        diis = DIIS(space)
+        rel = None
+        for it in range(1, max_iter + 1):
+            res.compute(d, t3, r3)
+            n = t3_residual.update_t3_(t3, r3, d, write_r3=True)
+            diis.update([t3])
+            rel = math.sqrt(float(n[0])) / max(float(t3.norm()), 1e-300)
+            if rel < tol:
+                break
+        out[prec] = {"iterations": it, "final_rel_update": rel, "converged": rel < tol,
+                     "e_t3_share": energy(t3), "status_ok": res.status_ok()}
+        t3s[prec] = t3
+        del res, r3, diis
+        torch.cuda.empty_cache()
+    de = energy(t3s[precision] - t3s["fp64"])
+    e = out["fp64"]["e_t3_share"]
+    out["abs_dE"] = abs(de)
+    out["relative"] = abs(de / e)
+    out["abs_dE_at_10mEh"] = abs(de / e) * 1e-2
+    out["t3_max_rel_diff"] = float((t3s[precision] - t3s["fp64"]).abs().max() / t3s["fp64"].abs().max())
+    del t3s, d, energy
+    torch.cuda.empty_cache()
+    return out
 
 
 def main():
@@ -587,6 +643,8 @@ def main():
         extras["q_energy_nocc10_nvir90"] = q_line(torch, ranks, s_no, s_nv, args.precision, 24)
         extras["t4_iteration"] = t4_line(torch, ranks, args.precision)
         extras["iteration_energy_error"] = iteration_energy_error(torch, s_no, s_nv, args.precision)
+        extras["converged_energy_error"] = [converged_energy_error(torch, 6, 40, args.precision),
+                                            converged_energy_error(torch, s_no, s_nv, args.precision)]
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:

@@ -9,6 +9,7 @@
     python profile_cases.py oogemm [--reps 3]
     python profile_cases.py unpack [--reps 3]
     python profile_cases.py qgroup [--reps 3]
+    python profile_cases.py t3half [--reps 3] [--nocc 15 --nvir 93] [--kind bf16x3|fp64] [--breakdown]
 
 Each case builds its inputs once and launches the kernel `reps` times, so a
 profiler can skip the warm-up launches and capture the last one.  Sizes are
@@ -197,6 +198,47 @@ def case_t3iter(reps, nocc, nvir, kind="bf16x3"):
           f"per iteration, peak memory {torch.cuda.max_memory_allocated() / 2**30:.1f} GiB")
 
 
+def case_t3half(reps, nocc, nvir, kind="bf16x3", breakdown=False):
+    """The bench step (the T3 half-iteration: feedback, compute_r3_tri, P3_full, divide, update,
+    norms, unified DIIS; bench.Workload) at a given shape: three warm-up steps, then `reps`
+    steps timed with CUDA events.  With breakdown, one more step under torch.profiler prints
+    the device time of every kernel name (this library's and cuBLAS's / torch's)."""
+    sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+    import bench
+    from dcc.t3_iteration import T3Iteration
+    w = bench.Workload(torch, nocc, nvir)
+    it = T3Iteration(nocc, nvir, kind)
+    if kind != "fp64":
+        it.res.tune(w.dd, w.t3_0)
+    w.start(it)
+    for _ in range(3):
+        w.step(it)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        w.step(it)
+    e1.record()
+    torch.cuda.synchronize()
+    assert it.status_ok()
+    print(f"t3half {kind} nocc={nocc} nvir={nvir}: {e0.elapsed_time(e1) / max(reps, 1):.2f} ms per step, "
+          f"peak memory {torch.cuda.max_memory_allocated() / 2**30:.1f} GiB")
+    if breakdown:
+        from torch.profiler import profile, ProfilerActivity
+        with profile(activities=[ProfilerActivity.CUDA]) as prof:
+            w.step(it)
+            torch.cuda.synchronize()
+        tot = {}
+        for ev in prof.events():
+            if ev.device_type == torch.autograd.DeviceType.CUDA:
+                n, t = tot.get(ev.name, (0, 0.0))
+                tot[ev.name] = (n + 1, t + ev.device_time_total / 1e3)
+        total = sum(t for _, t in tot.values())
+        print(f"breakdown: {total:.2f} ms of kernels in one step")
+        for name, (n, t) in sorted(tot.items(), key=lambda kv: -kv[1][1])[:40]:
+            print(f"  {t:9.3f} ms {100 * t / total:5.1f} % x{n:<4d} {name[:150]}")
+
+
 def case_qsample(nocc, nvir, kind="bf16x3", ngroups=12, blksize=4, dchunk=None):
     """[Q] / (Q) on `ngroups` task groups spread over all groups (as the bench samples them),
     split path and FP64 path on the same inputs: ms and energies of each, printed."""
@@ -241,7 +283,7 @@ def case_t4(reps, kind="bf16x3"):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("case", choices=["gemm", "p3", "update", "q", "gather", "xgemm", "oogemm", "unpack", "qgroup",
-                                         "t4", "t3iter", "qsample"])
+                                         "t4", "t3iter", "qsample", "t3half"])
     ap.add_argument("--kind", default="bf16x3")
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--nocc", type=int, default=None, help="occupied orbitals (xgemm, oogemm, gather, unpack)")
@@ -250,6 +292,7 @@ def main():
                     help="p3 case: which symmetrizer")
     ap.add_argument("--time", action="store_true", help="p3 case: print CUDA-event timings")
     ap.add_argument("--dchunk", type=int, default=None, help="qsample case: d-chunk of the split path")
+    ap.add_argument("--breakdown", action="store_true", help="t3half case: per-kernel device times")
     a = ap.parse_args()
     if a.case == "gemm":
         case_gemm(a.kind, a.reps)
@@ -261,6 +304,8 @@ def main():
         case_t4(a.reps, a.kind)
     elif a.case == "t3iter":
         case_t3iter(a.reps, a.nocc or 10, a.nvir, a.kind)
+    elif a.case == "t3half":
+        case_t3half(a.reps, a.nocc or 15, a.nvir if a.nvir != 90 else 93, a.kind, a.breakdown)
     elif a.case == "qsample":
         case_qsample(a.nocc or 10, a.nvir, a.kind, dchunk=a.dchunk)
     elif a.case in ("gather", "xgemm", "oogemm", "unpack", "qgroup"):
