@@ -1,6 +1,10 @@
 // Device DIIS for the unified T1/T2/T3 vector (distr_cc/diis.py:105-177,
 // distr_cc/rccsdt.py:1026-1067): the two vector-length passes of one update.
 //
+// The vector (slots, xprev) holds the segments one after the other, each starting on a
+// multiple of 32 elements (dcc_diis_vector_length), the gaps zero, so every slot is read
+// and written in aligned 16-byte pairs whatever the segments' lengths.
+//
 //   push:    v = concat(scale_s * seg_s);  e = v - xprev;  x_slot = v;  e_slot = e;
 //            dots[s] = <e, e_other[s]> (s < nother), dots[nother] = <e, e>
 //   combine: xnew = sum_s c_s x_s (in slot order, products rounded before each
@@ -21,12 +25,17 @@ namespace dcc {
 constexpr int DI_THREADS = 256;
 constexpr int DI_MAXS = 16;    // DIIS slots
 constexpr int DI_MAXSEG = 4;   // amplitude segments in the vector
-constexpr int DI_GRID = 148 * 4;
+constexpr int DI_GRID = 148 * 8;
+constexpr int64_t DI_PAD = 32; // every segment starts on a multiple of 32 elements of the vector
 
+// The vector's segments: segment s holds n[s] elements at vector positions [off[s], off[s] + n[s]);
+// off[s + 1] - off[s] - n[s] padding elements (zero in every slot) follow it.
 struct DiisSegs {
     double *p[DI_MAXSEG];
     double scale[DI_MAXSEG];
-    int64_t start[DI_MAXSEG + 1];  // segment s covers [start[s], start[s+1])
+    int64_t n[DI_MAXSEG];
+    int64_t off[DI_MAXSEG + 1];
+    int vec[DI_MAXSEG];  // p[s] is 16-byte aligned (pair loads and stores)
     int nseg;
 };
 
@@ -36,18 +45,37 @@ struct DiisPtrs {
     int n;
 };
 
-// Segment holding element i: its base pointer (already offset so that base[i]
-// is the element), and its scale.  Unrolled selects keep everything in registers.
-__device__ __forceinline__ void seg_of(const DiisSegs &g, int64_t i, double *&base, double &scale) {
-    base = g.p[0] - g.start[0];
-    scale = g.scale[0];
+// Segment of vector position j (even): base pointer, length, scale and the local index.
+__device__ __forceinline__ int seg_at(const DiisSegs &g, int64_t j, int64_t &l) {
+    int s = 0;
 #pragma unroll
     for (int q = 1; q < DI_MAXSEG; q++)
-        if (q < g.nseg && i >= g.start[q]) {
-            base = g.p[q] - g.start[q];
-            scale = g.scale[q];
-        }
+        if (q < g.nseg && j >= g.off[q]) s = q;
+    l = j - g.off[s];
+    return s;
 }
+
+// The two segment elements at local index l, l + 1 (zero past the segment's end).
+__device__ __forceinline__ double2 seg_load(const DiisSegs &g, int s, int64_t l) {
+    const double *p = g.p[s];
+    const int64_t n = g.n[s];
+    if (g.vec[s] && l + 1 < n) return *reinterpret_cast<const double2 *>(p + l);
+    return make_double2(l < n ? p[l] : 0.0, l + 1 < n ? p[l + 1] : 0.0);
+}
+
+__device__ __forceinline__ void seg_store(const DiisSegs &g, int s, int64_t l, double2 v) {
+    double *p = g.p[s];
+    const int64_t n = g.n[s];
+    if (g.vec[s] && l + 1 < n) {
+        *reinterpret_cast<double2 *>(p + l) = v;
+        return;
+    }
+    if (l < n) p[l] = v.x;
+    if (l + 1 < n) p[l + 1] = v.y;
+}
+
+__device__ __forceinline__ double2 ld2(const double *p, int64_t j) { return *reinterpret_cast<const double2 *>(p + j); }
+__device__ __forceinline__ void st2(double *p, int64_t j, double2 v) { *reinterpret_cast<double2 *>(p + j) = v; }
 
 // Block-wide sums of v[0..N) into partial[blockIdx.x * stride + s] for s < n,
 // and of `last` into partial[blockIdx.x * stride + n] (thread 0 writes).
@@ -72,43 +100,60 @@ __device__ __forceinline__ void block_sums(const double (&v)[N], double last, in
     }
 }
 
-__global__ void __launch_bounds__(DI_THREADS) k_diis_push(DiisSegs x, int64_t n, double *xprev, double *xslot,
-                                                          double *eslot, DiisPtrs eo, double *partial) {
+// One pass over the vector in element pairs (16-byte loads and stores of every slot).
+__global__ void __launch_bounds__(DI_THREADS) k_diis_push(DiisSegs x, double *xprev, double *xslot, double *eslot,
+                                                          DiisPtrs eo, double *partial) {
     double acc[DI_MAXS];
     double ee = 0.0;
 #pragma unroll
     for (int s = 0; s < DI_MAXS; s++) acc[s] = 0.0;
-    for (int64_t i = (int64_t)blockIdx.x * DI_THREADS + threadIdx.x; i < n; i += (int64_t)gridDim.x * DI_THREADS) {
-        double *base;
-        double sc;
-        seg_of(x, i, base, sc);
-        const double v = dmul(sc, base[i]);
-        const double e = dsub(v, xprev[i]);
-        xslot[i] = v;
-        eslot[i] = e;
+    const int64_t npair = x.off[x.nseg] / 2, stride = (int64_t)gridDim.x * DI_THREADS;
+    for (int64_t q = (int64_t)blockIdx.x * DI_THREADS + threadIdx.x; q < npair; q += stride) {
+        const int64_t j = 2 * q;
+        int64_t l;
+        const int s = seg_at(x, j, l);
+        const double2 a = seg_load(x, s, l), xp = ld2(xprev, j);
+        const double sc = x.scale[s];
+        const double2 v = make_double2(dmul(sc, a.x), dmul(sc, a.y));
+        const double2 e = make_double2(dsub(v.x, xp.x), dsub(v.y, xp.y));
+        st2(xslot, j, v);
+        st2(eslot, j, e);
 #pragma unroll
-        for (int s = 0; s < DI_MAXS; s++)
-            if (s < eo.n) acc[s] = fma(e, eo.p[s][i], acc[s]);
-        ee = fma(e, e, ee);
+        for (int t = 0; t < DI_MAXS; t++)
+            if (t < eo.n) {
+                const double2 o = ld2(eo.p[t], j);
+                acc[t] = fma(e.y, o.y, fma(e.x, o.x, acc[t]));
+            }
+        ee = fma(e.y, e.y, fma(e.x, e.x, ee));
     }
     block_sums(acc, ee, eo.n, partial, DI_MAXS + 1);  // <e, e_s> then <e, e>
 }
 
-__global__ void __launch_bounds__(DI_THREADS) k_diis_combine(DiisPtrs xs, int64_t n, double *xprev, DiisSegs out,
+__global__ void __launch_bounds__(DI_THREADS) k_diis_combine(DiisPtrs xs, double *xprev, DiisSegs out,
                                                              double *partial) {
     double dd = 0.0;
-    for (int64_t i = (int64_t)blockIdx.x * DI_THREADS + threadIdx.x; i < n; i += (int64_t)gridDim.x * DI_THREADS) {
-        double v = 0.0;
+    const int64_t npair = out.off[out.nseg] / 2, stride = (int64_t)gridDim.x * DI_THREADS;
+    for (int64_t q = (int64_t)blockIdx.x * DI_THREADS + threadIdx.x; q < npair; q += stride) {
+        const int64_t j = 2 * q;
+        double2 xi[DI_MAXS];
 #pragma unroll
-        for (int s = 0; s < DI_MAXS; s++)
-            if (s < xs.n) v = dadd(v, dmul(xs.p[s][i], xs.c[s]));
-        const double d = dsub(v, xprev[i]);
-        dd = fma(d, d, dd);
-        xprev[i] = v;
-        double *base;
-        double sc;
-        seg_of(out, i, base, sc);
-        base[i] = sc == 1.0 ? v : __ddiv_rn(v, sc);
+        for (int t = 0; t < DI_MAXS; t++)
+            if (t < xs.n) xi[t] = ld2(xs.p[t], j);
+        const double2 xp = ld2(xprev, j);
+        double vx = 0.0, vy = 0.0;
+#pragma unroll
+        for (int t = 0; t < DI_MAXS; t++)
+            if (t < xs.n) {
+                vx = dadd(vx, dmul(xi[t].x, xs.c[t]));
+                vy = dadd(vy, dmul(xi[t].y, xs.c[t]));
+            }
+        const double dx = dsub(vx, xp.x), dy = dsub(vy, xp.y);
+        dd = fma(dy, dy, fma(dx, dx, dd));
+        st2(xprev, j, make_double2(vx, vy));
+        int64_t l;
+        const int s = seg_at(out, j, l);
+        const double sc = out.scale[s];
+        seg_store(out, s, l, sc == 1.0 ? make_double2(vx, vy) : make_double2(__ddiv_rn(vx, sc), __ddiv_rn(vy, sc)));
     }
     const double none[1] = {0.0};
     block_sums(none, dd, 0, partial, DI_MAXS + 1);
@@ -135,10 +180,12 @@ static int make_segs(DiisSegs &g, double *const *seg, const int64_t *seg_n, cons
         DCC_REQUIRE(scale[s] != 0.0, DCC_ERR_SHAPE, "segment %d has scale 0", s);
         g.p[s] = seg[s];
         g.scale[s] = scale[s];
-        g.start[s] = n;
-        n += seg_n[s];
+        g.n[s] = seg_n[s];
+        g.off[s] = n;
+        g.vec[s] = ((uintptr_t)seg[s] & 15) == 0;
+        n += (seg_n[s] + DI_PAD - 1) / DI_PAD * DI_PAD;
     }
-    for (int s = nseg; s <= DI_MAXSEG; s++) g.start[s] = n;
+    for (int s = nseg; s <= DI_MAXSEG; s++) g.off[s] = n;
     return DCC_OK;
 }
 
@@ -147,6 +194,26 @@ static int make_segs(DiisSegs &g, double *const *seg, const int64_t *seg_n, cons
 using namespace dcc;
 
 extern "C" size_t dcc_diis_workspace_bytes(void) { return (size_t)DI_GRID * (DI_MAXS + 1) * sizeof(double); }
+
+extern "C" int64_t dcc_diis_vector_length(const int64_t *seg_n, int nseg, int64_t *seg_off) {
+    clear_error();
+    if (!seg_n || nseg < 1 || nseg > DI_MAXSEG) {
+        set_error("1..%d segments", DI_MAXSEG);
+        return -1;
+    }
+    int64_t n = 0;
+    for (int s = 0; s < nseg; s++) {
+        if (seg_n[s] < 0) {
+            set_error("segment %d has a negative length", s);
+            return -1;
+        }
+        if (seg_off) seg_off[s] = n;
+        n += (seg_n[s] + DI_PAD - 1) / DI_PAD * DI_PAD;
+    }
+    return n;
+}
+
+static bool aligned16(const void *p) { return ((uintptr_t)p & 15) == 0; }
 
 // A slot pointer the kernels can dereference: device, managed or pinned (page-locked) host
 // memory.  Pageable host memory is refused before any launch.
@@ -185,9 +252,13 @@ extern "C" int dcc_diis_push(double *const *seg, const int64_t *seg_n, const dou
         eo.p[s] = e_other[s];
     }
     if ((rc = check_slot(x_slot, "x slot", 0)) || (rc = check_slot(e_slot, "error slot", 0))) return rc;
+    DCC_REQUIRE(aligned16(xprev) && aligned16(x_slot) && aligned16(e_slot), DCC_ERR_UNSUPPORTED,
+                "xprev and the slots must be 16-byte aligned");
+    for (int s = 0; s < nother; s++)
+        DCC_REQUIRE(aligned16(e_other[s]), DCC_ERR_UNSUPPORTED, "other slot %d is not 16-byte aligned", s);
     cudaStream_t st = as_stream(stream);
     double *partial = (double *)workspace;
-    k_diis_push<<<DI_GRID, DI_THREADS, 0, st>>>(g, n, xprev, x_slot, e_slot, eo, partial);
+    k_diis_push<<<DI_GRID, DI_THREADS, 0, st>>>(g, xprev, x_slot, e_slot, eo, partial);
     k_diis_finish<<<1, 32, 0, st>>>(partial, DI_GRID, nother + 1, dots);
     return launch_status("diis_push");
 }
@@ -208,12 +279,14 @@ extern "C" int dcc_diis_combine(const double *const *xs, const double *coef, int
     for (int s = 0; s < nd; s++) {
         DCC_REQUIRE(xs[s], DCC_ERR_NULL, "slot %d is NULL", s);
         if ((rc = check_slot(xs[s], "x slot", s))) return rc;
+        DCC_REQUIRE(aligned16(xs[s]), DCC_ERR_UNSUPPORTED, "slot %d is not 16-byte aligned", s);
         p.p[s] = xs[s];
         p.c[s] = coef[s];
     }
+    DCC_REQUIRE(aligned16(xprev), DCC_ERR_UNSUPPORTED, "xprev must be 16-byte aligned");
     cudaStream_t st = as_stream(stream);
     double *partial = (double *)workspace;
-    k_diis_combine<<<DI_GRID, DI_THREADS, 0, st>>>(p, n, xprev, g, partial);
+    k_diis_combine<<<DI_GRID, DI_THREADS, 0, st>>>(p, xprev, g, partial);
     k_diis_finish<<<1, 32, 0, st>>>(partial, DI_GRID, 1, delta);
     return launch_status("diis_combine");
 }

@@ -2,7 +2,8 @@
 (distr_cc/diis.py:25-177, driven as in run_diis_t3, distr_cc/rccsdt.py:1026-1067).
 
 The vector is the concatenation of up to four device amplitude segments,
-each multiplied by its scale (the reference scales the packed unique T1/T2
+each starting on a multiple of 32 elements (vector_layout; the gaps are zero,
+so the passes move aligned 16-byte pairs) and multiplied by its scale (the reference scales the packed unique T1/T2
 by 1/sqrt(nranks) and appends t3_local[:, :nd, :nd, :nd]).  Slots live in
 device memory; one update is two single passes over the vector
 (dcc_diis_push: error vector, slot copies and the new B-matrix row;
@@ -31,6 +32,19 @@ _push = L.bind("dcc_diis_push", [L.c_vp, L.c_vp, L.c_vp, L.c_int, L.c_vp, L.c_vp
                                  L.c_vp, ctypes.c_size_t, L.c_vp])
 _combine = L.bind("dcc_diis_combine", [L.c_vp, L.c_vp, L.c_int, L.c_vp, L.c_vp, L.c_vp, L.c_vp, L.c_int, L.c_vp,
                                        L.c_vp, ctypes.c_size_t, L.c_vp])
+_veclen = L.bind("dcc_diis_vector_length", [L.c_vp, L.c_int, L.c_vp], restype=ctypes.c_int64)
+
+
+def vector_layout(lengths):
+    """(total length, segment offsets) of the DIIS vector for segments of these lengths: each
+    segment starts on a multiple of 32 elements, the gaps are zero."""
+    n = len(lengths)
+    seg_n = (ctypes.c_int64 * n)(*[int(x) for x in lengths])
+    off = (ctypes.c_int64 * n)()
+    total = int(_veclen(seg_n, n, off))
+    if total < 0:
+        raise L.DccError(2, L.last_error())
+    return total, list(off)
 
 
 class DIIS:
@@ -75,9 +89,12 @@ class DIIS:
         return ptr, num, sc, scales, sum(t.numel() for t in segments)
 
     def update(self, segments, scales=None):
-        ptr, num, sc, scales, n = self._segs(segments, scales)
+        ptr, num, sc, scales, _ = self._segs(segments, scales)
+        n, offs = vector_layout([t.numel() for t in segments])
         if self._xprev is None:
-            self._xprev = torch.cat([t.reshape(-1) * s for t, s in zip(segments, scales)])
+            self._xprev = torch.zeros(n, dtype=f64, device=self.dev)
+            for t, s, o in zip(segments, scales, offs):
+                self._xprev[o:o + t.numel()] = t.reshape(-1) * s
             self.last_delta_norm_sq = None
             return segments
         if self._xprev.numel() != n:

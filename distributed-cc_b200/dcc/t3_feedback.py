@@ -120,3 +120,102 @@ def intermediates_t3_add_x_(W_vooo, W_vvvo, oovv, X):
 def intermediates_t3_add_(W_vooo, W_vvvo, t1_eris, X, nocc):
     """W_vooo, W_vvvo += T3 parts (distr_cc/rccsdt.py:323-366) from X = p3_201_all(t3)."""
     return intermediates_t3_add_x_(W_vooo, W_vvvo, eris_slices(t1_eris, None, nocc)["oovv"], X)
+
+
+def _x_pieces(no, inner_span, sx, limit=(1 << 31) - 1):
+    """Cut the contracted occupied index x into runs whose contraction offsets
+    ((x - x0) * sx + inner_span) stay below `limit` (the split kernel's 31-bit contraction
+    offsets): [(x0, count)]."""
+    step = max(1, min(no, (limit - inner_span) // sx + 1))
+    return [(x0, min(step, no - x0)) for x0 in range(0, no, step)]
+
+
+class SplitFeedback:
+    """The four T3 -> lower-order strings of the split-precision path as tcgen05 GEMMs on
+    split operands (r1r2_add_t3_tri_ and intermediates_t3_add_t3_tri, distr_cc/rccsdt.py:
+    300-316, 340-358), from X = p3_201_all(t3) read in place through address maps:
+
+        r2[y,z,b,c]     += sum_{x,d,a} E_vovv[c,x,a,d] X[x,y,z,d,b,a]
+        r2[y,l,b,c]     -= sum_{x,z,a} E_ooov[z,x,l,a] X[x,y,z,a,b,c]
+        W_vooo[a,m,y,z] += sum_{x,e,d} E_oovv[m,x,d,e] X[x,y,z,e,a,d]
+        W_vvvo[a,b,d,y] -= sum_{x,z,e} E_oovv[z,x,d,e] X[x,y,z,e,b,a]
+
+    The small E slice is the GEMM's row operand (at most nvir rows, permuted once so that
+    its contraction index is contiguous) and X the column operand; each contraction runs
+    over (x, two more indices) in the order that keeps X's contiguous index innermost, with
+    x cut into runs that keep the split kernel's contraction offsets in 31 bits.  One split
+    buffer of X (nocc^2 nvir x nocc nvir^2 elements, two 2-byte pieces each in bf16x3)
+    serves the four strings in turn.  The f_ov term of r2 (K = nvir) stays an FP64 product."""
+
+    def __init__(self, nocc, nvir, precision, device="cuda"):
+        from . import contract
+        self.c = contract
+        self.no, self.nv, self.kind, self.dev = nocc, nvir, contract.KIND[precision], device
+        no, nv = nocc, nvir
+        Sz = nv ** 3
+        Sy, Sx, Sp, Sq = no * Sz, no * no * Sz, nv * nv, nv
+        self.Sx = Sx
+        c = contract
+        # N, X column map, inner contraction digits of X (R1, R2, S1, S2) after x, E slice and
+        # the permutation that puts it in [row][x][k1][k2] order, output maps, alpha, output
+        self.terms = {
+            # r2 vovv: columns (y,z,b); K = (x, d, a); E_vovv[c,x,a,d] -> [c][x][d][a]
+            "vovv": dict(N=no * no * nv, fn=c.three(no, nv, Sy, Sz, Sq), kin=(nv, nv, Sp, 1), M=nv,
+                         src="vovv", perm=(0, 1, 3, 2), orow=c.lin(1),
+                         ocol=c.three(no, nv, no * nv * nv, nv * nv, nv), alpha=1.0, out="r2"),
+            # r2 ooov: columns (y,b,c); K = (x, z, a); E_ooov[z,x,l,a] -> [l][x][z][a]
+            "ooov": dict(N=no * nv * nv, fn=c.three(nv, nv, Sy, Sq, 1), kin=(no, nv, Sz, Sp), M=no,
+                         src="ooov", perm=(2, 1, 0, 3), orow=c.lin(nv * nv),
+                         ocol=c.three(nv, nv, no * nv * nv, nv, 1), alpha=-1.0, out="r2"),
+            # W_vooo: columns (y,z,a); K = (x, e, d); E_oovv[m,x,d,e] -> [m][x][e][d]
+            "wvooo": dict(N=no * no * nv, fn=c.three(no, nv, Sy, Sz, Sq), kin=(nv, nv, Sp, 1), M=no,
+                          src="oovv", perm=(0, 1, 3, 2), orow=c.lin(no * no),
+                          ocol=c.three(no, nv, no, 1, no ** 3), alpha=1.0, out="W_vooo"),
+            # W_vvvo: columns (y,b,a); K = (x, z, e); E_oovv[z,x,d,e] -> [d][x][z][e]
+            "wvvvo": dict(N=no * nv * nv, fn=c.three(nv, nv, Sy, Sq, 1), kin=(no, nv, Sz, Sp), M=nv,
+                          src="oovv", perm=(2, 1, 0, 3), orow=c.lin(no),
+                          ocol=c.three(nv, nv, 1, no * nv, no * nv * nv), alpha=-1.0, out="W_vvvo"),
+        }
+        dt = torch.bfloat16 if self.kind == 0 else torch.float32
+        self.plans = {}
+        xmax = emax = 0
+        for name, tm in self.terms.items():
+            R1, R2, S1, S2 = tm["kin"]
+            pieces = _x_pieces(no, (R1 - 1) * S1 + (R2 - 1) * S2, Sx)
+            ks = [xc * R1 * R2 for _, xc in pieces]
+            tot = sum((k + 7) // 8 * 8 for k in ks) if len(ks) > 1 else ks[0]
+            Kp = contract.padded_k(tot, self.kind)
+            self.plans[name] = (pieces, ks, Kp)
+            xmax, emax = max(xmax, tm["N"] * Kp), max(emax, tm["M"] * Kp)
+        self._xhi = torch.empty(xmax, dtype=dt, device=device)
+        self._xlo = torch.empty(xmax, dtype=dt, device=device)
+        self._ehi = torch.empty(emax, dtype=dt, device=device)
+        self._elo = torch.empty(emax, dtype=dt, device=device)
+        self.status = torch.zeros(1, dtype=torch.int32, device=device)
+
+    def _operand(self, rows, ks, Kp, hi, lo):
+        n = rows * Kp
+        buf = (hi[:n].view(rows, Kp), lo[:n].view(rows, Kp))
+        if len(ks) > 1:
+            return self.c.Split(rows, kind=self.kind, buffers=buf, pieces=ks)
+        return self.c.Split(rows, ks[0], self.kind, buffers=buf)
+
+    def run(self, X, E, outs, names=("vovv", "ooov", "wvooo", "wvvvo")):
+        """outs[...] += the strings above.  X: [no,no,no,nv,nv,nv] FP64, contiguous; E: the
+        slices {'vovv', 'ooov', 'oovv'} of eris_slices on the device; outs: {'r2', 'W_vooo',
+        'W_vvvo'} FP64 device tensors."""
+        c = self.c
+        Xf = X.reshape(-1)
+        for name in names:
+            tm = self.terms[name]
+            pieces, ks, Kp = self.plans[name]
+            R1, R2, S1, S2 = tm["kin"]
+            B = self._operand(tm["N"], ks, Kp, self._xhi, self._xlo)
+            A = self._operand(tm["M"], ks, Kp, self._ehi, self._elo)
+            Ep = E[tm["src"]].permute(*tm["perm"]).contiguous()  # [row][x][k1][k2]
+            row = self.no * R1 * R2
+            for i, (x0, xc) in enumerate(pieces):
+                B.fill_piece(i, Xf[x0 * self.Sx:], tm["fn"], c.three(R1, R2, self.Sx, S1, S2))
+                A.fill_piece(i, Ep[:, x0:], c.lin(row), c.lin(1))
+            c.gemm_(A, B, outs[tm["out"]], tm["orow"], tm["ocol"], tm["alpha"], 1.0, self.status)
+        return outs

@@ -14,7 +14,9 @@ Here every one of them is a device step over the same resident T3.  The two
 feedback passes share one X = P3_201 of every ordered block (t3 does not
 change between them, distr_cc/rccsdt.py:916-936), built in the residual's S
 buffer from the residual's unpacked U (the unpack is done once per
-iteration), so the feedback needs no memory of its own beyond a slice.
+iteration).  In the split precisions the feedback strings are tcgen05 GEMMs
+over X read in place (t3_feedback.SplitFeedback); the FP64 path runs them as
+DGEMMs one occupied slice at a time.
 The lower-order steps between the passes (PySCF's compute_r1r2,
 intermediates_t3, the r1/r2 update) stay with the caller: they are small
 and are not on this path.
@@ -43,6 +45,8 @@ class T3Iteration:
         self.r3 = torch.empty((self.n3, nvir, nvir, nvir), dtype=f64, device=device)
         self.norms = torch.zeros(2, dtype=f64, device=device)
         self._X = None
+        # the feedback strings as split GEMMs in the split precisions (FP64 einsums otherwise)
+        self.sfb = fb.SplitFeedback(nocc, nvir, precision, device) if precision != "fp64" else None
         self.diis = None
         self._diis_key = None
         self._active = None
@@ -57,15 +61,31 @@ class T3Iteration:
         fb.r1_add_t3_(dr1, None, t3, self.ijk, no, oovv=oovv, V=self.r3)
         self.res.unpack_(t3)
         self._X = fb.p3_201_all(t3, no, U=self.res.U, out=self.res.S)
-        fb.r2_add_t3_x_(dr2, fock_ov, vovv, ooov, self._X)
+        if self.sfb is None:
+            fb.r2_add_t3_x_(dr2, fock_ov, vovv, ooov, self._X)
+        else:
+            dr2.view(no * no, nv * nv).add_(self._fock_term(fock_ov), alpha=0.5)
+            self.sfb.run(self._X, {"vovv": vovv, "ooov": ooov}, {"r2": dr2}, names=("vovv", "ooov"))
         return dr1, dr2
+
+    def _fock_term(self, fock_ov):
+        """sum_{x,a} f[x,a] X[x,y,z,a,b,c] as [(y,z), (b,c)] (FP64)."""
+        no, nv = self.no, self.nv
+        out = torch.zeros((no * no, nv * nv), dtype=f64, device=self.dev)
+        for x in range(no):
+            out += torch.matmul(fock_ov[x].view(1, 1, nv), self._X[x].reshape(no * no, nv, nv * nv)).view(no * no,
+                                                                                                          nv * nv)
+        return out
 
     def feedback_w(self, W_vooo, W_vvvo, oovv):
         """W_vooo, W_vvvo += their T3 parts (distr_cc/rccsdt.py:323-366), in place, from the X of
         the preceding feedback_r1r2 (same T3)."""
         if self._X is None:
             raise RuntimeError("feedback_w needs the X of feedback_r1r2 of the same T3")
-        fb.intermediates_t3_add_x_(W_vooo, W_vvvo, oovv, self._X)
+        if self.sfb is None:
+            fb.intermediates_t3_add_x_(W_vooo, W_vvvo, oovv, self._X)
+        else:
+            self.sfb.run(self._X, {"oovv": oovv}, {"W_vooo": W_vooo, "W_vvvo": W_vvvo}, names=("wvooo", "wvvvo"))
         return W_vooo, W_vvvo
 
     # --------------------------------------------------------------- residual + update
@@ -85,7 +105,10 @@ class T3Iteration:
         return update_t3_(t3, self.r3, d, nvir_active=nvir_active, norms=self.norms)
 
     def status_ok(self):
-        return self.res.status_ok()
+        ok = self.res.status_ok()
+        if self.sfb is not None:
+            ok = ok and int(self.sfb.status.item()) == 0
+        return ok
 
     # --------------------------------------------------------------- DIIS
     def diis_update(self, lower, t3, space, key=None, nvir_diis=None):

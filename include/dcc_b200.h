@@ -203,8 +203,15 @@ DCC_API int dcc_t3_perm_gather_tma(double *r3, const int32_t *ijk, int64_t nbloc
 /* Bytes of the workspace both DIIS passes take (per-CTA partial sums). */
 DCC_API size_t dcc_diis_workspace_bytes(void);
 
+/* Length of the DIIS vector (xprev and every slot) for nseg <= 4 segments of seg_n[s]
+ * doubles: segment s occupies [seg_off[s], seg_off[s] + seg_n[s]) (seg_off, HOST, may be
+ * NULL), every segment starting on a multiple of 32 elements; the gaps are zero.  -1 on
+ * bad sizes.  The vector of DIIS.update (distr_cc/diis.py:105-177) in this layout. */
+DCC_API int64_t dcc_diis_vector_length(const int64_t *seg_n, int nseg, int64_t *seg_off);
+
 /* v = concat(seg_scale[s] * seg[s]) (nseg <= 4 DEVICE segments of seg_n[s]
- * doubles, HOST tables); e = v - xprev; x_slot = v; e_slot = e;
+ * doubles, HOST tables, laid out as dcc_diis_vector_length gives; xprev and the
+ * slots 16-byte aligned); e = v - xprev; x_slot = v; e_slot = e;
  * dots[s] = <e, e_other[s]> for s < nother (<= 15), dots[nother] = <e, e>
  * (DEVICE).  The B-matrix row of DIIS.update (distr_cc/diis.py:121-133). */
 DCC_API int dcc_diis_push(double *const *seg, const int64_t *seg_n, const double *seg_scale, int nseg, double *xprev,

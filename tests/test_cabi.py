@@ -137,3 +137,15 @@ def test_three_digit_map_helpers():
     for m in [0, 1, 7, 89, 90, 8099, 8100, 19799]:
         assert f(m, *c.lin(3)) == 3 * m
         assert f(m, *c.two(90, 1000, 7)) == (m // 90) * 1000 + (m % 90) * 7
+
+
+def test_diis_vector_layout(L):
+    """dcc_diis_vector_length: segments start on multiples of 32 elements (host-only call)."""
+    lib = L.lib()
+    lib.dcc_diis_vector_length.restype = ctypes.c_int64
+    lib.dcc_diis_vector_length.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]
+    n = (ctypes.c_int64 * 3)(5, 40, 0)
+    off = (ctypes.c_int64 * 3)()
+    assert lib.dcc_diis_vector_length(n, 3, off) == 32 + 64 + 0
+    assert list(off) == [0, 32, 96]
+    assert lib.dcc_diis_vector_length(n, 0, None) == -1
