@@ -259,14 +259,15 @@ __global__ void __launch_bounds__(OT_THREADS) k_orbit3(const double *in, double 
     }
 }
 
-// In-place P3 spin summation.  The tile geometry of a CTA is the same for
+// P3 spin summation, in place (out == A) or out of place.  The tile geometry of a CTA is the same for
 // every block, so each thread computes its shared/global offsets once: up to
 // 12 (slot, element) copies and up to 2 canonical orbits (6 shared addresses
 // each).  Per block the CTA then issues its cp.async copies, sums its orbits
 // in shared memory and stores, while the copies of the next block are in
 // flight; thread 0 also stages its share of the block after next into L2
 // (cp.async.bulk.prefetch.L2) so the 64-byte tile rows are read from L2.
-__global__ void __launch_bounds__(OT_THREADS, 3) k_p3_inplace(double *A, int64_t nblocks, int nv, int ntile, P3Coef k) {
+__global__ void __launch_bounds__(OT_THREADS, 3) k_p3_inplace(const double *A, double *out, int64_t nblocks, int nv,
+                                                              int ntile, P3Coef k) {
     extern __shared__ double sm[];  // 2 x 6 x SLOT doubles
     __shared__ OrbitSet os;
     int t0, t1, t2;
@@ -364,7 +365,7 @@ __global__ void __launch_bounds__(OT_THREADS, 3) k_p3_inplace(double *A, int64_t
             for (int q = 0; q < 6; q++) buf[oa[h][q]] = r[q];
         }
         __syncthreads();
-        double *blk = A + b * n3;
+        double *blk = out + b * n3;
 #pragma unroll
         for (int j = 0; j < 12; j++)
             if (nload & (1u << j)) blk[goff[j]] = buf[soff[j]];
@@ -735,7 +736,7 @@ static int orbit3_launch(int mode, const double *in, double *o0, double *o1, dou
     }
     if (mode == 0 && nvir <= 1290) {  // 32-bit element offsets inside a block
         cudaFuncSetAttribute(k_p3_inplace, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        k_p3_inplace<<<grid, OT_THREADS, smem, st>>>(o0, nblocks, (int)nvir, ntile, k);
+        k_p3_inplace<<<grid, OT_THREADS, smem, st>>>(in, o0, nblocks, (int)nvir, ntile, k);
         return launch_status("P3 spin summation");
     }
     if (mode == 0) cudaFuncSetAttribute(k_orbit3<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -1092,6 +1093,20 @@ extern "C" int dcc_t3_spin_summation_inplace(double *A, int64_t nblocks, int64_t
     DCC_REQUIRE(nblocks >= 0 && nvir >= 0, DCC_ERR_SHAPE, "negative size");
     DCC_REQUIRE(A || nblocks * nvir == 0, DCC_ERR_NULL, "A is NULL");
     return orbit3_launch(0, A, A, nullptr, nullptr, nblocks, nvir, k, stream);
+}
+
+extern "C" int dcc_t3_spin_summation(const double *A, double *B, int64_t nblocks, int64_t nvir, const char *pattern,
+                                     double alpha, double beta, void *stream) {
+    clear_error();
+    P3Coef k;
+    int rc = p3_coef(pattern, alpha, beta, k);
+    if (rc) return rc;
+    DCC_REQUIRE(nblocks >= 0 && nvir >= 0, DCC_ERR_SHAPE, "negative size");
+    DCC_REQUIRE((A && B) || nblocks * nvir == 0, DCC_ERR_NULL, "NULL buffer");
+    const int64_t bytes = nblocks * nvir * nvir * nvir * (int64_t)sizeof(double);
+    DCC_REQUIRE(A == B || (const char *)B + bytes <= (const char *)A || (const char *)A + bytes <= (const char *)B,
+                DCC_ERR_SHAPE, "A and B overlap");
+    return orbit3_launch(0, A, B, nullptr, nullptr, nblocks, nvir, k, stream);
 }
 
 extern "C" int dcc_t3_single_spin_summation_inplace(double *A, int64_t nvir, const char *pattern, double alpha,

@@ -32,6 +32,18 @@ def t3_spin_summation_inplace_(A, nblocks, nvir, pattern, alpha=1.0, beta=0.0):
     return A
 
 
+def t3_spin_summation(A, B, nblocks, nvir, pattern, alpha=1.0, beta=0.0):
+    """B = beta*A + alpha*P(A) block by block, out of place (PySCF's t3_spin_summation as
+    distr_cc/rccsdtq.py:853 calls it); B may be A itself."""
+    A = L.as_tensor(A, f64, "A")
+    B = L.as_tensor(B, f64, "B")
+    if A.numel() != nblocks * nvir ** 3 or B.numel() != A.numel():
+        raise ValueError("A and B must hold nblocks nvir^3 blocks")
+    L.call("dcc_t3_spin_summation", L.ptr(A), L.ptr(B), nblocks, nvir, L.pattern(pattern), float(alpha),
+           float(beta), L.stream_ptr())
+    return B
+
+
 def symmetrize_status():
     """Status word of the bounded waits in the TMA spin-summation kernel on the current
     device (0, or DCC_ERR_TIMEOUT once a wait gave up); reading clears it and

@@ -45,8 +45,8 @@ def r1_add_t3_(r1, t1_eris, t3, ijk, nocc, oovv=None, V=None):
     [o,o,v,v] slice of t1_eris when the caller passes the slice alone (t1_eris None);
     V: a scratch buffer of t3's size."""
     nvir = t3.shape[1]
-    V = t3.clone() if V is None else V.copy_(t3)
-    _c_rccsdt.t3_spin_summation_inplace_(V, V.shape[0], nvir, "P3_422", 1.0, 0.0)
+    V = torch.empty_like(t3) if V is None else V
+    _c_rccsdt.t3_spin_summation(t3, V, t3.shape[0], nvir, "P3_422", 1.0, 0.0)
     E = oovv if oovv is not None else eris_slices(t1_eris, None, nocc)["oovv"]
     il, jl, kl = ijk[:, 0].long(), ijk[:, 1].long(), ijk[:, 2].long()
     c1, c2, c3 = _case_coefficients(ijk)
@@ -67,8 +67,8 @@ def p3_201_all(t3, nocc, U=None, out=None):
     if U is None:
         U = torch.empty((nocc ** 3, nvir, nvir, nvir), dtype=f64, device=t3.device)
         unpack_all_(t3, U, nocc, nvir)
-    X = U.clone() if out is None else out.view(U.shape).copy_(U)
-    _c_rccsdt.t3_spin_summation_inplace_(X, X.shape[0], nvir, "P3_201", 1.0, 0.0)
+    X = torch.empty_like(U) if out is None else out.view(U.shape)
+    _c_rccsdt.t3_spin_summation(U, X, U.shape[0], nvir, "P3_201", 1.0, 0.0)
     return X.view(nocc, nocc, nocc, nvir, nvir, nvir)
 
 

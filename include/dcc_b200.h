@@ -65,6 +65,13 @@ DCC_API int dcc_t3_single_spin_summation_inplace(double *A, int64_t nvir, const 
 DCC_API int dcc_t3_spin_summation_inplace(double *A, int64_t nblocks, int64_t nvir, const char *pattern, double alpha,
                                   double beta, void *stream);
 
+/* B = beta*A + alpha*P(A) block by block, out of place (A and B do not overlap, or
+ * B == A for the in-place form above); same patterns and arithmetic.  The
+ * out-of-place t3_spin_summation of PySCF's rccsdt_highm as the reference calls it
+ * (distr_cc/rccsdtq.py:853, P3_201 of the full T3 with alpha 1, beta 0). */
+DCC_API int dcc_t3_spin_summation(const double *A, double *B, int64_t nblocks, int64_t nvir, const char *pattern,
+                                  double alpha, double beta, void *stream);
+
 /* B0 = 2T - T_acb - T_cba, B1 = 2T - T_bac - T_acb, B2 = B0 + T_acb - T_bac on
  * nblocks blocks.  Replaces t3_spin_summation_triple_sym_ (src/rccsdt.c:245-310). */
 DCC_API int dcc_t3_spin_summation_triple_sym(const double *A, double *B0, double *B1, double *B2, int64_t nblocks,

@@ -30,11 +30,27 @@ class Imds:
         self.W_ovov, self.W_ovvo, self.W_oooo = W_ovov, W_ovvo, W_oooo
 
 
-def vt2_ref(imds, t2, t3, nocc):
-    """W_vvvo.t2, W_vooo.t2 and F_vv.t3 per block (distr_cc/rccsdt.py:385-402)."""
+def _rows(nocc, targets):
+    """(canonical index q, output row) of the blocks to compute: every block, or `targets`."""
+    n = len(ijk_list(nocc))
+    qs = range(n) if targets is None else targets
+    return [(q, r) for r, q in enumerate(qs)]
+
+
+def _e(*args):
+    """numpy einsum contracting through BLAS (the oracle's large-shape cases need it)."""
+    return np.einsum(*args, optimize=True)
+
+
+def vt2_ref(imds, t2, t3, nocc, targets=None):
+    """W_vvvo.t2, W_vooo.t2 and F_vv.t3 per block (distr_cc/rccsdt.py:385-402); with `targets`
+    (canonical block indices) only those blocks, as rows of the result in that order."""
     W_vvvo, W_vooo, F_vv = imds.W_vvvo, imds.W_vooo, imds.F_vv
-    r3 = np.empty_like(t3)
-    for q, (i, j, k) in enumerate(ijk_list(nocc)):
+    trip = ijk_list(nocc)
+    rows = _rows(nocc, targets)
+    r3 = np.empty((len(rows),) + t3.shape[1:])
+    for q, row in rows:
+        i, j, k = trip[q]
         r = np.einsum('abd,dc->abc', W_vvvo[..., j], t2[i, k])
         r += np.einsum('acd,db->abc', W_vvvo[..., k], t2[i, j])
         r += np.einsum('bad,dc->abc', W_vvvo[..., i], t2[j, k])
@@ -50,29 +66,31 @@ def vt2_ref(imds, t2, t3, nocc):
         r += np.einsum('ad,dbc->abc', F_vv, t3[q])
         r += np.einsum('bd,adc->abc', F_vv, t3[q])
         r += np.einsum('cd,abd->abc', F_vv, t3[q])
-        r3[q] = r
+        r3[row] = r
     return r3
 
 
-def wvvvv_ref(imds, t3, r3):
-    """W_vvvv.t3 (distr_cc/rccsdt.py:421-427)."""
+def wvvvv_ref(imds, t3, r3, targets=None):
+    """W_vvvv.t3 (distr_cc/rccsdt.py:421-427); rows of r3 as in vt2_ref."""
     W = imds.W_vvvv
-    for q in range(t3.shape[0]):
-        r3[q] += np.einsum('abde,dec->abc', W, t3[q])
-        r3[q] += np.einsum('acde,dbe->abc', W, t3[q])
-        r3[q] += np.einsum('bcde,ade->abc', W, t3[q])
+    qs = range(t3.shape[0]) if targets is None else targets
+    for row, q in enumerate(qs):
+        r3[row] += _e('abde,dec->abc', W, t3[q])
+        r3[row] += _e('acde,dbe->abc', W, t3[q])
+        r3[row] += _e('bcde,ade->abc', W, t3[q])
     return r3
 
 
-def foo_woooo_ref(imds, t3, r3, nocc):
+def foo_woooo_ref(imds, t3, r3, nocc, targets=None):
     """Prefactor-matrix form of the F_oo / W_oooo terms (distr_cc/rccsdt.py:616-732),
-    one batch holding every canonical block."""
+    one batch holding every canonical block; rows of r3 as in vt2_ref."""
     F_oo, W_oooo = imds.F_oo, imds.W_oooo
     trip = ijk_list(nocc)
     n = len(trip)
-    pfs = np.zeros((6, n, n))
+    rows = _rows(nocc, targets)
+    pfs = np.zeros((6, n, len(rows)))
     for idx, (o00, o10, o20) in enumerate(trip):
-        for q, (i, j, k) in enumerate(trip):
+        for q, (i, j, k) in [(row, trip[qq]) for qq, row in rows]:
             if k == o20:
                 pfs[0, idx, q] += W_oooo[o00, o10, i, j]
             if o10 != o20 and k == o10:
@@ -127,28 +145,38 @@ def foo_woooo_ref(imds, t3, r3, nocc):
                 pfs[1, idx, q] -= F_oo[o10, k]
             if o00 != o10 and i == o10 and j == o20:
                 pfs[4, idx, q] -= F_oo[o00, k]
-    r3 += np.einsum('pq,pabc->qabc', pfs[0], t3)
-    r3 += np.einsum('pq,pacb->qabc', pfs[1], t3)
-    r3 += np.einsum('pq,pbac->qabc', pfs[2], t3)
-    r3 += np.einsum('pq,pabc->qcab', pfs[3], t3)
-    r3 += np.einsum('pq,pabc->qbca', pfs[4], t3)
-    r3 += np.einsum('pq,pabc->qcba', pfs[5], t3)
+    r3 += _e('pq,pabc->qabc', pfs[0], t3)
+    r3 += _e('pq,pacb->qabc', pfs[1], t3)
+    r3 += _e('pq,pbac->qabc', pfs[2], t3)
+    r3 += _e('pq,pabc->qcab', pfs[3], t3)
+    r3 += _e('pq,pabc->qbca', pfs[4], t3)
+    r3 += _e('pq,pabc->qcba', pfs[5], t3)
     return r3
 
 
-def oo_ovov_ref(imds, t3, r3, nocc, orc=None):
+def oo_ovov_ref(imds, t3, r3, nocc, orc=None, targets=None):
     """Masked W_ovov / W_ovvo terms (distr_cc/rccsdt.py:532-596) with the
-    transpose-add and triple-sym variants of every batch block."""
+    transpose-add and triple-sym variants of every batch block; rows of r3 as in
+    vt2_ref.  A batch block's variants are made only when some target uses them."""
     orc = orc or Oracle()
     Wov, Wvo = imds.W_ovov, imds.W_ovvo
     nvir = t3.shape[1]
     trip = ijk_list(nocc)
-    e = np.einsum
+    rows = [(row, trip[qq]) for qq, row in _rows(nocc, targets)]
+    e = _e
     for idx, (o00, o10, o20) in enumerate(trip):
+        used = [(row, (i, j, k)) for row, (i, j, k) in rows
+                if (j == o00 and k == o10) or (o10 != o20 and j == o00 and k == o20)
+                or (o00 != o10 and j == o10 and k == o20) or (i == o00 and k == o10)
+                or (o10 != o20 and i == o00 and k == o20) or (o00 != o10 and i == o10 and k == o20)
+                or (i == o00 and j == o10) or (o10 != o20 and i == o00 and j == o20)
+                or (o00 != o10 and i == o10 and j == o20)]
+        if not used:
+            continue
         T = np.ascontiguousarray(t3[idx])
         T2 = orc.t3_transpose_add(T, nvir)
         V0, V1, V2 = orc.t3_triple_sym(T, nvir)
-        for q, (i, j, k) in enumerate(trip):
+        for q, (i, j, k) in used:
             r = r3[q]
             if j == o00 and k == o10:
                 r -= e('bd,dca->abc', Wov[o20, :, i, :], T)
@@ -198,13 +226,14 @@ def oo_ovov_ref(imds, t3, r3, nocc, orc=None):
     return r3
 
 
-def compute_r3_tri_ref(imds, t2, t3, nocc, with_oo=True):
-    """The whole compute_r3_tri at one rank (distr_cc/rccsdt.py:368-433)."""
-    r3 = vt2_ref(imds, t2, t3, nocc)
+def compute_r3_tri_ref(imds, t2, t3, nocc, with_oo=True, targets=None):
+    """The whole compute_r3_tri at one rank (distr_cc/rccsdt.py:368-433); with `targets`
+    (canonical block indices) the r3 of those blocks only, in that order."""
+    r3 = vt2_ref(imds, t2, t3, nocc, targets)
     if with_oo:
-        foo_woooo_ref(imds, t3, r3, nocc)
-        oo_ovov_ref(imds, t3, r3, nocc)
-    wvvvv_ref(imds, t3, r3)
+        foo_woooo_ref(imds, t3, r3, nocc, targets)
+        oo_ovov_ref(imds, t3, r3, nocc, targets=targets)
+    wvvvv_ref(imds, t3, r3, targets)
     return r3
 
 

@@ -57,6 +57,24 @@ def test_t3_spin_sum(C, oracle, nvir, pattern):
     assert c3.symmetrize_status() == 0
 
 
+@pytest.mark.parametrize("nvir", [1, 5, 10, 13, 30, 93])
+@pytest.mark.parametrize("pattern", P3)
+def test_t3_spin_sum_out_of_place(C, oracle, nvir, pattern):
+    """B = beta*A + alpha*P(A) out of place (the TMA kernel at even nvir, the cp.async kernel at
+    odd nvir): bit-exact with the oracle, and A untouched."""
+    c3 = C[0]
+    rng = np.random.default_rng(100 + nvir)
+    nblk = 2 if nvir >= 90 else 4
+    for alpha, beta in [(1.0, 0.0), (-1.0 / 6.0, 1.0)]:
+        A = rng.standard_normal((nblk,) + (nvir,) * 3)
+        want = oracle.t3_spin_sum(A.copy(), nvir, pattern, alpha, beta)
+        d, out = dev(A), torch.full(A.shape, float("nan"), dtype=torch.float64, device="cuda")
+        c3.t3_spin_summation(d, out, nblk, nvir, pattern, alpha, beta)
+        assert np.array_equal(host(out), want)
+        assert np.array_equal(host(d), A)
+    assert c3.symmetrize_status() == 0
+
+
 @pytest.mark.parametrize("nvir", [2, 10, 30, 90])
 def test_orbit_roundtrip_is_identity(C, nvir):
     """The diagnostic tile round trip of the spin-summation kernel leaves every block unchanged."""
