@@ -228,6 +228,7 @@ def intermediates_t3_add_t3_tri(mycc, imds, t3):
     t3d = _dev(_t3_local(mycc, t3), dev)
     # X is rebuilt here: this route may be called on its own, with a T3 other than the last one
     it._X = t3_feedback.p3_201_all(t3d, nocc, out=it.res.S)
+    it._dW = None
     sl = _feedback_slices(mycc, imds, dev)
     Wo, Wv = _dev(imds.W_vooo, dev), _dev(imds.W_vvvo, dev)
     it.feedback_w(Wo, Wv, sl["oovv"])

@@ -203,19 +203,30 @@ class SplitFeedback:
     def run(self, X, E, outs, names=("vovv", "ooov", "wvooo", "wvvvo")):
         """outs[...] += the strings above.  X: [no,no,no,nv,nv,nv] FP64, contiguous; E: the
         slices {'vovv', 'ooov', 'oovv'} of eris_slices on the device; outs: {'r2', 'W_vooo',
-        'W_vvvo'} FP64 device tensors."""
+        'W_vvvo'} FP64 device tensors.  Strings that read X the same way (vovv with W_vooo,
+        ooov with W_vvvo: the same columns and contraction over X's axes) share one split
+        of X."""
         c = self.c
         Xf = X.reshape(-1)
+        done = set()
         for name in names:
+            if name in done:
+                continue
             tm = self.terms[name]
+            group = [n for n in names if n not in done and self.terms[n]["fn"] == tm["fn"]
+                     and self.terms[n]["kin"] == tm["kin"] and self.terms[n]["N"] == tm["N"]]
             pieces, ks, Kp = self.plans[name]
             R1, R2, S1, S2 = tm["kin"]
             B = self._operand(tm["N"], ks, Kp, self._xhi, self._xlo)
-            A = self._operand(tm["M"], ks, Kp, self._ehi, self._elo)
-            Ep = E[tm["src"]].permute(*tm["perm"]).contiguous()  # [row][x][k1][k2]
-            row = self.no * R1 * R2
             for i, (x0, xc) in enumerate(pieces):
                 B.fill_piece(i, Xf[x0 * self.Sx:], tm["fn"], c.three(R1, R2, self.Sx, S1, S2))
-                A.fill_piece(i, Ep[:, x0:], c.lin(row), c.lin(1))
-            c.gemm_(A, B, outs[tm["out"]], tm["orow"], tm["ocol"], tm["alpha"], 1.0, self.status)
+            for n in group:
+                tn = self.terms[n]
+                A = self._operand(tn["M"], ks, Kp, self._ehi, self._elo)
+                Ep = E[tn["src"]].permute(*tn["perm"]).contiguous()  # [row][x][k1][k2]
+                row = self.no * R1 * R2
+                for i, (x0, xc) in enumerate(pieces):
+                    A.fill_piece(i, Ep[:, x0:], c.lin(row), c.lin(1))
+                c.gemm_(A, B, outs[tn["out"]], tn["orow"], tn["ocol"], tn["alpha"], 1.0, self.status)
+                done.add(n)
         return outs

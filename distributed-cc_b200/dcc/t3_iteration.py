@@ -45,6 +45,7 @@ class T3Iteration:
         self.r3 = torch.empty((self.n3, nvir, nvir, nvir), dtype=f64, device=device)
         self.norms = torch.zeros(2, dtype=f64, device=device)
         self._X = None
+        self._dW = None
         # the feedback strings as split GEMMs in the split precisions (FP64 einsums otherwise)
         self.sfb = fb.SplitFeedback(nocc, nvir, precision, device) if precision != "fp64" else None
         self.diis = None
@@ -64,8 +65,13 @@ class T3Iteration:
         if self.sfb is None:
             fb.r2_add_t3_x_(dr2, fock_ov, vovv, ooov, self._X)
         else:
+            # all four strings here, two splits of X between them; the W parts wait in dW for
+            # feedback_w (the host builds W_vooo / W_vvvo in between)
             dr2.view(no * no, nv * nv).add_(self._fock_term(fock_ov), alpha=0.5)
-            self.sfb.run(self._X, {"vovv": vovv, "ooov": ooov}, {"r2": dr2}, names=("vovv", "ooov"))
+            self._dW = (torch.zeros((nv, no, no, no), dtype=f64, device=self.dev),
+                        torch.zeros((nv, nv, nv, no), dtype=f64, device=self.dev))
+            self.sfb.run(self._X, {"vovv": vovv, "ooov": ooov, "oovv": oovv},
+                         {"r2": dr2, "W_vooo": self._dW[0], "W_vvvo": self._dW[1]})
         return dr1, dr2
 
     def _fock_term(self, fock_ov):
@@ -84,7 +90,11 @@ class T3Iteration:
             raise RuntimeError("feedback_w needs the X of feedback_r1r2 of the same T3")
         if self.sfb is None:
             fb.intermediates_t3_add_x_(W_vooo, W_vvvo, oovv, self._X)
-        else:
+        elif self._dW is not None:
+            W_vooo += self._dW[0]
+            W_vvvo += self._dW[1]
+            self._dW = None
+        else:  # X built without feedback_r1r2 (the route of intermediates_t3_add_t3_tri alone)
             self.sfb.run(self._X, {"oovv": oovv}, {"W_vooo": W_vooo, "W_vvvo": W_vvvo}, names=("wvooo", "wvvvo"))
         return W_vooo, W_vvvo
 
