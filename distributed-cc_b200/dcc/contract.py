@@ -99,14 +99,16 @@ class Split:
     operands (each piece starts on a multiple of 8 columns; the gaps and the
     tail are zero), filled one by one with fill_piece."""
 
-    def __init__(self, M, K=None, kind=0, device="cuda", buffers=None, pieces=None):
+    def __init__(self, M, K=None, kind=0, device="cuda", buffers=None, pieces=None, align=8):
+        """align: pieces start on multiples of this many columns (8; the k-block, so that
+        each piece can also be contracted on its own with gemm_range_)."""
         self.M, self.kind = int(M), int(kind)
         if pieces is None:
             pieces = [int(K)]
         offs, o = [], 0
         for k in pieces:
             offs.append(o)
-            o += (int(k) + 7) // 8 * 8
+            o += (int(k) + align - 1) // align * align
         self.K = o if len(pieces) > 1 else int(pieces[0])
         self.Kp = padded_k(self.K, self.kind)
         ends = offs[1:] + [self.Kp]
@@ -151,6 +153,22 @@ def gemm_(A, B, C, frow, fcol, alpha=1.0, beta=1.0, status=None, Kp=None):
     if status is None:
         status = torch.zeros(1, dtype=torch.int32, device=C.device)
     L.check(_gemm(L.ptr(A.hi), L.ptr(A.lo), A.Kp, L.ptr(B.hi), L.ptr(B.lo), B.Kp, A.M, B.M, int(Kp), L.ptr(C),
+                  _i64x14(frow, fcol), float(alpha), float(beta), A.kind, L.ptr(status), L.stream_ptr()))
+    return status
+
+
+def gemm_range_(A, B, C, frow, fcol, alpha, beta, status, col0, ncol):
+    """gemm_ over the contraction columns [col0, col0 + ncol) of both operands (col0 and ncol
+    multiples of the k-block, e.g. one piece of operands made with align = the k-block)."""
+    if A.kind != B.kind or A.Kp != B.Kp:
+        raise ValueError("A and B must be split with the same kind and padded K")
+    blk = _KBLK[A.kind]
+    if col0 % blk or ncol % blk or col0 + ncol > A.Kp:
+        raise ValueError("column range must be whole k-blocks inside the operands")
+    _check_span(C, frow, A.M, fcol, B.M, "C")
+    es = A.hi.element_size()
+    vp = lambda t: ctypes.c_void_p(t.data_ptr() + col0 * es)  # noqa: E731
+    L.check(_gemm(vp(A.hi), vp(A.lo), A.Kp, vp(B.hi), vp(B.lo), B.Kp, A.M, B.M, int(ncol), L.ptr(C),
                   _i64x14(frow, fcol), float(alpha), float(beta), A.kind, L.ptr(status), L.stream_ptr()))
     return status
 

@@ -122,14 +122,6 @@ def intermediates_t3_add_(W_vooo, W_vvvo, t1_eris, X, nocc):
     return intermediates_t3_add_x_(W_vooo, W_vvvo, eris_slices(t1_eris, None, nocc)["oovv"], X)
 
 
-def _x_pieces(no, inner_span, sx, limit=(1 << 31) - 1):
-    """Cut the contracted occupied index x into runs whose contraction offsets
-    ((x - x0) * sx + inner_span) stay below `limit` (the split kernel's 31-bit contraction
-    offsets): [(x0, count)]."""
-    step = max(1, min(no, (limit - inner_span) // sx + 1))
-    return [(x0, min(step, no - x0)) for x0 in range(0, no, step)]
-
-
 class SplitFeedback:
     """The four T3 -> lower-order strings of the split-precision path as tcgen05 GEMMs on
     split operands (r1r2_add_t3_tri_ and intermediates_t3_add_t3_tri, distr_cc/rccsdt.py:
@@ -142,8 +134,11 @@ class SplitFeedback:
 
     The small E slice is the GEMM's row operand (at most nvir rows, permuted once so that
     its contraction index is contiguous) and X the column operand; each contraction runs
-    over (x, two more indices) in the order that keeps X's contiguous index innermost, with
-    x cut into runs that keep the split kernel's contraction offsets in 31 bits.  One split
+    over (x, two more indices) in the order that keeps X's contiguous index innermost.  Every
+    value of x is its own piece of the split operands (starting on a k-block) and its own
+    GEMM: the tensor cores accumulate in FP32 over the other two indices only, and the
+    epilogue sums the nocc partial results in FP64 -- one FP32 accumulation over the whole
+    contraction (nocc nvir^2 terms at nvir ~ 90) lost four digits to cancellation.  One split
     buffer of X (nocc^2 nvir x nocc nvir^2 elements, two 2-byte pieces each in bf16x3)
     serves the four strings in turn.  The f_ov term of r2 (K = nvir) stays an FP64 product."""
 
@@ -177,14 +172,15 @@ class SplitFeedback:
                           ocol=c.three(nv, nv, 1, no * nv, no * nv * nv), alpha=-1.0, out="W_vvvo"),
         }
         dt = torch.bfloat16 if self.kind == 0 else torch.float32
+        self.blk = contract._KBLK[self.kind]
         self.plans = {}
         xmax = emax = 0
         for name, tm in self.terms.items():
             R1, R2, S1, S2 = tm["kin"]
-            pieces = _x_pieces(no, (R1 - 1) * S1 + (R2 - 1) * S2, Sx)
-            ks = [xc * R1 * R2 for _, xc in pieces]
-            tot = sum((k + 7) // 8 * 8 for k in ks) if len(ks) > 1 else ks[0]
-            Kp = contract.padded_k(tot, self.kind)
+            pieces = [(x, 1) for x in range(no)]  # one piece (and one GEMM) per value of x
+            ks = [R1 * R2] * no
+            w = contract.padded_k(R1 * R2, self.kind)
+            Kp = w * no
             self.plans[name] = (pieces, ks, Kp)
             xmax, emax = max(xmax, tm["N"] * Kp), max(emax, tm["M"] * Kp)
         self._xhi = torch.empty(xmax, dtype=dt, device=device)
@@ -196,9 +192,7 @@ class SplitFeedback:
     def _operand(self, rows, ks, Kp, hi, lo):
         n = rows * Kp
         buf = (hi[:n].view(rows, Kp), lo[:n].view(rows, Kp))
-        if len(ks) > 1:
-            return self.c.Split(rows, kind=self.kind, buffers=buf, pieces=ks)
-        return self.c.Split(rows, ks[0], self.kind, buffers=buf)
+        return self.c.Split(rows, kind=self.kind, buffers=buf, pieces=ks, align=self.blk)
 
     def run(self, X, E, outs, names=("vovv", "ooov", "wvooo", "wvvvo")):
         """outs[...] += the strings above.  X: [no,no,no,nv,nv,nv] FP64, contiguous; E: the
@@ -227,6 +221,8 @@ class SplitFeedback:
                 row = self.no * R1 * R2
                 for i, (x0, xc) in enumerate(pieces):
                     A.fill_piece(i, Ep[:, x0:], c.lin(row), c.lin(1))
-                c.gemm_(A, B, outs[tn["out"]], tn["orow"], tn["ocol"], tn["alpha"], 1.0, self.status)
+                for off, _, w in A.pieces:
+                    c.gemm_range_(A, B, outs[tn["out"]], tn["orow"], tn["ocol"], tn["alpha"], 1.0, self.status,
+                                  off, w)
                 done.add(n)
         return outs

@@ -1,7 +1,7 @@
 """The split-precision T3 feedback plan (dcc.t3_feedback.SplitFeedback) on the CPU:
-every operand split (row / contraction maps, the permuted E slices, the runs of
-the contracted occupied index cut for 31-bit offsets) and every GEMM epilogue map
-emulated in numpy FP64, against the FP64 feedback strings
+every operand split (row / contraction maps, the permuted E slices, one piece per
+value of the contracted occupied index) and every per-piece GEMM with its epilogue
+map emulated in numpy FP64, against the FP64 feedback strings
 (distr_cc/rccsdt.py:300-316, 340-358).  Relative 1e-12."""
 import numpy as np
 import pytest
@@ -14,8 +14,8 @@ from test_maps_emulated import fmap
 class _EmuSplit:
     """contract.Split with the two pieces replaced by one FP64 array (same maps, same pieces)."""
 
-    def __init__(self, M, K=None, kind=0, device="cpu", buffers=None, pieces=None):
-        ref = contract.Split(M, K, kind, device="meta", pieces=pieces)
+    def __init__(self, M, K=None, kind=0, device="cpu", buffers=None, pieces=None, align=8):
+        ref = contract.Split(M, K, kind, device="meta", pieces=pieces, align=align)
         self.M, self.K, self.Kp, self.pieces, self.kind = ref.M, ref.K, ref.Kp, ref.pieces, kind
         self.a = np.zeros((self.M, self.Kp))
 
@@ -41,27 +41,31 @@ def _emu_gemm(A, B, C, frow, fcol, alpha=1.0, beta=1.0, status=None, Kp=None):
     return status
 
 
+def _emu_gemm_range(A, B, C, frow, fcol, alpha, beta, status, col0, ncol):
+    assert col0 % 64 == 0 and ncol % 64 == 0
+    idx = fmap(frow, np.arange(A.M))[:, None] + fmap(fcol, np.arange(B.M))[None, :]
+    flat = C.view(-1).numpy()
+    flat[idx] = alpha * (A.a[:, col0:col0 + ncol] @ B.a[:, col0:col0 + ncol].T) + beta * flat[idx]
+    return status
+
+
 class _EmuContract:
-    KIND, padded_k, lin, three = contract.KIND, staticmethod(contract.padded_k), staticmethod(contract.lin), \
-        staticmethod(contract.three)
+    KIND, padded_k, lin, three, _KBLK = contract.KIND, staticmethod(contract.padded_k), \
+        staticmethod(contract.lin), staticmethod(contract.three), contract._KBLK
     Split = _EmuSplit
     gemm_ = staticmethod(_emu_gemm)
+    gemm_range_ = staticmethod(_emu_gemm_range)
 
 
-@pytest.mark.parametrize("no,nv,limit", [(3, 5, None), (4, 6, 3000), (5, 4, 1500)])
-def test_split_feedback_maps(monkeypatch, no, nv, limit):
-    """limit: a smaller offset bound than 2^31, so the x runs are cut as at the large shapes."""
-    if limit is not None:
-        orig = fb._x_pieces
-        monkeypatch.setattr(fb, "_x_pieces", lambda n, span, sx: orig(n, span, sx, limit=limit))
+@pytest.mark.parametrize("no,nv", [(3, 5), (4, 6), (5, 4)])
+def test_split_feedback_maps(no, nv):
     rng = np.random.default_rng(no * nv)
     nmo = no + nv
     g = torch.from_numpy(rng.standard_normal((nmo,) * 4))
     X = torch.from_numpy(rng.standard_normal((no, no, no, nv, nv, nv)))
     sl = {k: v.contiguous() for k, v in fb.eris_slices(g, None, no).items()}
     sfb = fb.SplitFeedback(no, nv, "bf16x3", device="cpu")
-    if limit is not None:
-        assert any(len(p[0]) > 1 for p in sfb.plans.values())  # runs are cut
+    assert all(len(p[0]) == no for p in sfb.plans.values())  # one piece per x
     sfb.c = _EmuContract
     r2 = torch.zeros(no, no, nv, nv, dtype=torch.float64)
     Wo = torch.zeros(nv, no, no, no, dtype=torch.float64)
