@@ -122,11 +122,11 @@ def test_job_d_ranges_cover_each_task_once(nvir, blk, n_jobs):
 
 
 def test_default_dchunk():
-    """One pass over the d range up to nocc ~ 12 at nvir ~ 90 (the bench shape keeps it); chunks
-    of whole task blocks whose FP32 group blocks stay within the limit beyond."""
+    """Chunks of whole task blocks whose two FP32 group blocks stay within 256 MiB (one pass
+    over the d range when they fit)."""
     from dcc import rccsdt_q
-    assert rccsdt_q.default_dchunk(10, 90, 4) == 90
+    assert rccsdt_q.default_dchunk(10, 90, 4) == 52
     assert rccsdt_q.default_dchunk(6, 40, 4) == 40
     c = rccsdt_q.default_dchunk(15, 93, 4)
-    assert c == 40 and c % 4 == 0 and 2 * 4 * 64 * 15 ** 4 * c <= 1 << 30
+    assert c == 8 and c % 4 == 0 and 2 * 4 * 64 * 15 ** 4 * c <= 1 << 28
     assert rccsdt_q.default_dchunk(40, 200, 8) == 8  # never below one block
