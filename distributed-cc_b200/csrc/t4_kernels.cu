@@ -61,6 +61,8 @@ __global__ void __launch_bounds__(S4_THREADS) k_t4_spin_sum(double *A, int64_t n
 
 __global__ void k_t4_transpose_add(const double *src, double *dst, int nv) {
     const int64_t n4 = (int64_t)nv * nv * nv * nv;
+    src += blockIdx.y * n4;  // block blockIdx.y of a batch
+    dst += blockIdx.y * n4;
     for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n4; e += (int64_t)gridDim.x * blockDim.x) {
         int d = (int)(e % nv), c = (int)((e / nv) % nv), b = (int)((e / ((int64_t)nv * nv)) % nv),
             a = (int)(e / ((int64_t)nv * nv * nv));
@@ -70,6 +72,12 @@ __global__ void k_t4_transpose_add(const double *src, double *dst, int nv) {
 
 __global__ void k_t4_quadruple_sym(const double *src, double *B0, double *B1, double *B2, double *B3, int nv) {
     const int64_t n4 = (int64_t)nv * nv * nv * nv;
+    const int64_t o = blockIdx.y * n4;  // block blockIdx.y of a batch
+    src += o;
+    B0 += o;
+    B1 += o;
+    B2 += o;
+    B3 += o;
     for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n4; e += (int64_t)gridDim.x * blockDim.x) {
         int d = (int)(e % nv), c = (int)((e / nv) % nv), b = (int)((e / ((int64_t)nv * nv)) % nv),
             a = (int)(e / ((int64_t)nv * nv * nv));
@@ -215,6 +223,32 @@ extern "C" int dcc_t4_spin_summation_quadruple_sym(const double *src, double *B0
     int64_t n4 = nvir * nvir * nvir * nvir;
     k_t4_quadruple_sym<<<grid1d(n4), 256, 0, as_stream(stream)>>>(src, B0, B1, B2, B3, (int)nvir);
     return launch_status("t4_quadruple_sym");
+}
+
+extern "C" int dcc_t4_transpose_add_batched(const double *src, double *dst, int64_t nblocks, int64_t nvir,
+                                            void *stream) {
+    clear_error();
+    DCC_REQUIRE(nvir >= 0 && nblocks >= 0 && nblocks < 65536, DCC_ERR_SHAPE, "bad size");
+    if (nvir == 0 || nblocks == 0) return DCC_OK;
+    DCC_REQUIRE(src && dst && src != dst, DCC_ERR_NULL, "NULL or aliased buffer");
+    int64_t n4 = nvir * nvir * nvir * nvir;
+    unsigned gx = grid1d(n4);
+    gx = gx > 64 ? 64 : gx;
+    k_t4_transpose_add<<<dim3(gx, (unsigned)nblocks), 256, 0, as_stream(stream)>>>(src, dst, (int)nvir);
+    return launch_status("t4_transpose_add_batched");
+}
+
+extern "C" int dcc_t4_spin_summation_quadruple_sym_batched(const double *src, double *B0, double *B1, double *B2,
+                                                           double *B3, int64_t nblocks, int64_t nvir, void *stream) {
+    clear_error();
+    DCC_REQUIRE(nvir >= 0 && nblocks >= 0 && nblocks < 65536, DCC_ERR_SHAPE, "bad size");
+    if (nvir == 0 || nblocks == 0) return DCC_OK;
+    DCC_REQUIRE(src && B0 && B1 && B2 && B3, DCC_ERR_NULL, "NULL buffer");
+    int64_t n4 = nvir * nvir * nvir * nvir;
+    unsigned gx = grid1d(n4);
+    gx = gx > 64 ? 64 : gx;
+    k_t4_quadruple_sym<<<dim3(gx, (unsigned)nblocks), 256, 0, as_stream(stream)>>>(src, B0, B1, B2, B3, (int)nvir);
+    return launch_status("t4_quadruple_sym_batched");
 }
 
 extern "C" int dcc_r4_local_tri_divide_e(double *r4_local, const double *eia, const int32_t *local_ijkl,

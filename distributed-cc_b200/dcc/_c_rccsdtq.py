@@ -51,6 +51,24 @@ def t4_spin_summation_quadruple_sym_(src, B0, B1, B2, B3, nvir):
     return B0, B1, B2, B3
 
 
+def t4_forms_batched(t4, nvir, T3=None, V=None):
+    """The transpose-add and the four quadruple-symmetrized forms of every block of t4
+    [n, nvir^4] in two launches (the forms the OO batch of compute_r4_tri takes per source
+    block, distr_cc/rccsdtq.py:1168-1169).  Returns (T3, [V0, V1, V2, V3])."""
+    t4 = L.as_tensor(t4, f64, "t4")
+    n = t4.shape[0]
+    if t4.numel() != n * nvir ** 4:
+        raise ValueError("t4 must hold n nvir^4 blocks")
+    T3 = torch.empty_like(t4) if T3 is None else L.as_tensor(T3, f64, "T3")
+    V = [torch.empty_like(t4) for _ in range(4)] if V is None else [L.as_tensor(v, f64, "V") for v in V]
+    if any(x.numel() != t4.numel() for x in [T3] + V):
+        raise ValueError("T3 and V must have t4's size")
+    L.call("dcc_t4_transpose_add_batched", L.ptr(t4), L.ptr(T3), n, nvir, L.stream_ptr())
+    L.call("dcc_t4_spin_summation_quadruple_sym_batched", L.ptr(t4), *[L.ptr(v) for v in V], n, nvir,
+           L.stream_ptr())
+    return T3, V
+
+
 def r4_local_tri_divide(r4_local, eia, local_ijkl):
     """r4[q] /= eia[i,a]+eia[j,b]+eia[k,c]+eia[l,d] (src/rccsdtq.c:1055-1088)."""
     r4_local = L.as_tensor(r4_local, f64, "r4_local")

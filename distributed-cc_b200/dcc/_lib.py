@@ -68,6 +68,8 @@ _SIGS = {
     "dcc_t4_spin_summation_inplace": [c_vp, c_i64, c_i64, c_str, c_dbl, c_dbl, c_vp],
     "dcc_t4_transpose_add": [c_vp, c_vp, c_i64, c_vp],
     "dcc_t4_spin_summation_quadruple_sym": [c_vp] * 5 + [c_i64, c_vp],
+    "dcc_t4_transpose_add_batched": [c_vp, c_vp, c_i64, c_i64, c_vp],
+    "dcc_t4_spin_summation_quadruple_sym_batched": [c_vp] * 5 + [c_i64, c_i64, c_vp],
     "dcc_r4_local_tri_divide_e": [c_vp, c_vp, c_vp, c_i64, c_i64, c_vp],
     "dcc_unpack_t4_ijkl_single": [c_vp, c_vp, c_vp] + [c_i64] * 6 + [c_vp],
     "dcc_fill_local_data_ijkl": [c_vp, c_vp, c_vp, c_vp, c_i64, c_i64, c_vp],

@@ -45,14 +45,14 @@ def dense_vvvv_fvv_(r4, t4, W_vvvv, F_vv, precision="fp64"):
 #
 # The reference adds, per stored block (i<=j<=k<=l), about a hundred strings
 # "W[occupied slots of (i,j,k,l)] . T[other slots]" over the block's virtual
-# indices.  Every such string is defined for any ordering of (i,j,k,l), so here
-# each one is ONE einsum over the full ordered occupied space,
-#   R[i,j,k,l,a,b,c,d] += alpha W[...] T[...],
-# whose canonical stored blocks are r4; the W builders are full-tensor einsums
-# (the T4 part of W_oooovv / W_oovvvv sums over every ordering of the stored
-# blocks, P4_201 applied, exactly the reference's loop over distinct
-# permutations).  W_oovvvv is kept for every ordered pair (x, y) with
-# W[x, y] = W_pair(min, max): the strings only read x <= y.
+# indices.  Here each string is ONE contraction batched over the stored blocks:
+# both operands are cut at every block's occupied slots at once (a gather by
+# the blocks' index columns) and contracted over the rest with the block as the
+# batch index, straight into r4.  The W builders are full-tensor einsums (the
+# T4 part of W_oooovv / W_oovvvv sums over every ordering of the stored blocks,
+# P4_201 applied, exactly the reference's loop over distinct permutations).
+# W_oovvvv is kept for every ordered pair (x, y) with W[x, y] = W_pair(min, max):
+# the strings only read x <= y.
 # ----------------------------------------------------------------------------
 
 import itertools  # noqa: E402
@@ -237,6 +237,23 @@ def build_intermediates(eris, W_oooo, W_ovov, W_vvvv, t2, t3, t3p, t4, nocc, spi
     return W
 
 
+def _gather_slots(X, subs, nocc, cache, name):
+    """X cut at the occupied slots of every stored block: for X with einsum subscripts `subs`
+    whose letters among i, j, k, l are the block's fixed occupied indices, the batch
+    [n_stored, ...other dims] of X[those indices of block q] and the subscripts of the other
+    dims.  Cached per (tensor, slot letters) for one compute_r4_tri call."""
+    slots = [c for c in subs if c in "ijkl"]
+    rest = "".join(c for c in subs if c not in "ijkl")
+    key = (name, tuple(subs.index(c) for c in slots), tuple(slots))
+    if key not in cache:
+        dev = X.device
+        cols = _cached(("quad_cols", nocc), dev, lambda: torch.tensor(stored_quadruples(nocc), device=dev).t().contiguous())
+        order = [subs.index(c) for c in slots] + [n for n, c in enumerate(subs) if c not in "ijkl"]
+        Xp = X.permute(*order)
+        cache[key] = Xp[tuple(cols["ijkl".index(c)] for c in slots)]
+    return cache[key], rest
+
+
 def compute_r4_tri_(r4, eris, F_vv, W_vvvo, W_vooo, W_vvvv, W_oooo, W_ovov, t2, t3, t4, nocc, precision="fp64",
                     spin3=None, spin4=None, F_oo=None, W_ovvo=None, forms=None):
     """r4[stored blocks] = compute_r4_tri (distr_cc/rccsdtq.py:834-1060); with F_oo and W_ovvo
@@ -245,8 +262,15 @@ def compute_r4_tri_(r4, eris, F_vv, W_vvvo, W_vooo, W_vvvv, W_oooo, W_ovov, t2, 
     eris: t1-dressed ERIs [nmo]^4 (the reference's imds.t1_eris); t2 [i,j,a,b]; t3 full
     [i,j,k,a,b,c]; t4 and r4 [nstored, nvir^4] in stored_quadruples order.  spin3 / spin4
     apply P3_201 / P4_201 in place to [n, nvir^3] / [n, nvir^4] blocks (default: this
-    library's kernels).  precision "bf16x3"/"tf32x3" runs the full-space strings and the
-    W_vvvv.t4 strings as split GEMMs; the builders stay FP64."""
+    library's kernels).
+
+    The ~100 per-block strings of distr_cc/rccsdtq.py:862-1033 each run as ONE batched
+    contraction over the stored blocks: every operand is cut at the block's occupied slots
+    for all blocks at once (_gather_slots) and the strings contract over the remaining
+    virtual (and summed occupied) indices with the block as the batch index, straight into
+    r4 -- the work and memory of the stored blocks only.  Their contractions are short
+    (K = nvir or nocc), so they stay FP64 in every precision; precision "bf16x3"/"tf32x3"
+    runs the W_vvvv.t4 strings (K = nvir^2) as split GEMMs; the builders stay FP64."""
     from . import _c_rccsdt, _c_rccsdt_q
     kind = None if precision == "fp64" else contract.KIND[precision]
     nv = t2.shape[2]
@@ -261,13 +285,14 @@ def compute_r4_tri_(r4, eris, F_vv, W_vvvo, W_vooo, W_vvvv, W_oooo, W_ovov, t2, 
     W["W_vvvo"], W["W_vooo"] = W_vvvo, W_vooo
     T = {"t3": t3, "t3_m": t3, "t3_mn": t3, "t3p_m": t3p, "t3s_m": t3 + t3.permute(0, 1, 2, 4, 5, 3),
          "t2_m": t2, "t2": t2}
-    R = torch.zeros((nocc,) * 4 + (nv,) * 4, dtype=t3.dtype, device=t3.device)
+    r4.zero_()
+    gathered = {}
     for sub, wn, ws, tn, ts, al in _R4_STRINGS:
         sw, st = sub.split(",")
-        subs = _slots(wn, ws, sw) + "," + _slots(tn, ts, st) + "->ijklabcd"
-        _einsum(kind, subs, W[wn], T[tn], R, al)
-    r4.copy_(R.view(nocc ** 4, -1)[_stored_rows(nocc, t3.device)].view(r4.shape))
-    del R
+        gw, lw = _gather_slots(W[wn], _slots(wn, ws, sw), nocc, gathered, wn)
+        gt, lt = _gather_slots(T[tn], _slots(tn, ts, st), nocc, gathered, tn)
+        r4.view((-1,) + (nv,) * 4).add_(torch.einsum("q" + lw + ",q" + lt + "->qabcd", gw, gt), alpha=al)
+    del gathered
     dense_vvvv_fvv_(r4, t4, W_vvvv, F_vv, precision)
     if F_oo is not None:
         oo_batch_(r4, t4, F_oo, W_oooo, W_ovvo, W_ovov, nocc, forms)
@@ -373,21 +398,16 @@ def oo_pairs(nocc):
 def oo_batch_(r4, t4, F_oo, W_oooo, W_ovvo, W_ovov, nocc, forms=None):
     """r4 += the OO batch of compute_r4_tri (distr_cc/rccsdtq.py:1062-1349), FP64.
 
-    forms(t4) -> (T3, [V0, V1, V2, V3]) per stored block (default: this library's
-    t4_transpose_add and quadruple-sym kernels, one block at a time)."""
+    forms(t4) -> (T3, [V0, V1, V2, V3]) per stored block (default: this library's batched
+    t4_transpose_add and quadruple-sym kernels, all blocks in one launch each)."""
     e = torch.einsum
     nv = t4.shape[1]
     dev = t4.device
     if forms is None:
         from . import _c_rccsdtq
 
-        def forms(t):
-            T3 = torch.empty_like(t)
-            V = [torch.empty_like(t) for _ in range(4)]
-            for q in range(t.shape[0]):
-                _c_rccsdtq.t4_transpose_add_(t[q], T3[q], nv)
-                _c_rccsdtq.t4_spin_summation_quadruple_sym_(t[q], V[0][q], V[1][q], V[2][q], V[3][q], nv)
-            return T3, V
+        def forms(t):  # every stored block's transpose-add and quadruple-sym forms, two launches
+            return _c_rccsdtq.t4_forms_batched(t, nv)
     # F_oo and W_oooo over the full ordered space
     T = unpack_all_orderings(t4, nocc)
     R = torch.zeros_like(T)
@@ -408,10 +428,14 @@ def oo_batch_(r4, t4, F_oo, W_oooo, W_ovvo, W_ovov, nocc, forms=None):
     for (g, c), (si, ti, m, x) in pairs:
         Wo = W_ovov[m, :, x, :]   # [P, a, e] = W_ovov[m, :, x, :]
         Wv = W_voov[:, m, x, :].permute(1, 0, 2)  # [P, a, e] = W_voov[:, m, x, :]
+        cut, acc = {}, None  # each source form gathered once per (g, c); one scatter per (g, c)
         for wn, s, al, form in _OO_TABLE[g][c]:
             ws, ts = s.split(",")
-            upd = e("p" + ws + ",p" + ts + "->pabcd", Wo if wn == "ovov" else Wv, src[form][si])
-            r4.index_add_(0, ti, upd, alpha=al)
+            if form not in cut:
+                cut[form] = src[form][si]
+            upd = e("p" + ws + ",p" + ts + "->pabcd", Wo if wn == "ovov" else Wv, cut[form])
+            acc = upd.mul_(al) if acc is None else acc.add_(upd, alpha=al)
+        r4.view(r4.shape[0], -1).index_add_(0, ti, acc.reshape(acc.shape[0], -1))
     return r4
 
 

@@ -259,6 +259,13 @@ DCC_API int dcc_t4_transpose_add(const double *src, double *dst, int64_t nvir, v
 DCC_API int dcc_t4_spin_summation_quadruple_sym(const double *src, double *B0, double *B1, double *B2, double *B3,
                                         int64_t nvir, void *stream);
 
+/* The two above on nblocks consecutive nvir^4 blocks in one launch (nblocks < 65536): the
+ * per-source-block forms the OO batch of compute_r4_tri takes (distr_cc/rccsdtq.py:1166-1169,
+ * there one block at a time). */
+DCC_API int dcc_t4_transpose_add_batched(const double *src, double *dst, int64_t nblocks, int64_t nvir, void *stream);
+DCC_API int dcc_t4_spin_summation_quadruple_sym_batched(const double *src, double *B0, double *B1, double *B2,
+                                                        double *B3, int64_t nblocks, int64_t nvir, void *stream);
+
 /* r4[q] /= eia[i,a]+eia[j,b]+eia[k,c]+eia[l,d] for ijkl = local_ijkl[q]
  * (DEVICE int32 [nlocal][4]).  Replaces r4_local_tri_divide_e_
  * (src/rccsdtq.c:1055-1088). */

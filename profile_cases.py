@@ -224,19 +224,25 @@ def case_t3half(reps, nocc, nvir, kind="bf16x3", breakdown=False):
     print(f"t3half {kind} nocc={nocc} nvir={nvir}: {e0.elapsed_time(e1) / max(reps, 1):.2f} ms per step, "
           f"peak memory {torch.cuda.max_memory_allocated() / 2**30:.1f} GiB")
     if breakdown:
-        from torch.profiler import profile, ProfilerActivity
-        with profile(activities=[ProfilerActivity.CUDA]) as prof:
-            w.step(it)
-            torch.cuda.synchronize()
-        tot = {}
-        for ev in prof.events():
-            if ev.device_type == torch.autograd.DeviceType.CUDA:
-                n, t = tot.get(ev.name, (0, 0.0))
-                tot[ev.name] = (n + 1, t + ev.device_time_total / 1e3)
-        total = sum(t for _, t in tot.values())
-        print(f"breakdown: {total:.2f} ms of kernels in one step")
-        for name, (n, t) in sorted(tot.items(), key=lambda kv: -kv[1][1])[:40]:
-            print(f"  {t:9.3f} ms {100 * t / total:5.1f} % x{n:<4d} {name[:150]}")
+        _breakdown(lambda: w.step(it))
+
+
+def _breakdown(step, top=40):
+    """One more `step` under torch.profiler: the device time and launch count of every kernel
+    name (this library's and cuBLAS's / torch's), largest first."""
+    from torch.profiler import profile, ProfilerActivity
+    with profile(activities=[ProfilerActivity.CUDA]) as prof:
+        step()
+        torch.cuda.synchronize()
+    tot = {}
+    for ev in prof.events():
+        if ev.device_type == torch.autograd.DeviceType.CUDA:
+            n, t = tot.get(ev.name, (0, 0.0))
+            tot[ev.name] = (n + 1, t + ev.device_time_total / 1e3)
+    total = sum(t for _, t in tot.values())
+    print(f"breakdown: {total:.2f} ms of kernels in one step, {sum(n for n, _ in tot.values())} launches")
+    for name, (n, t) in sorted(tot.items(), key=lambda kv: -kv[1][1])[:top]:
+        print(f"  {t:9.3f} ms {100 * t / total:5.1f} % x{n:<4d} {name[:150]}")
 
 
 def case_qsample(nocc, nvir, kind="bf16x3", ngroups=12, blksize=4, dchunk=None):
@@ -270,14 +276,24 @@ def case_qsample(nocc, nvir, kind="bf16x3", ngroups=12, blksize=4, dchunk=None):
         del q
 
 
-def case_t4(reps, kind="bf16x3"):
+def case_t4(reps, kind="bf16x3", breakdown=False):
     """T4 updates at the N2 6-31G shape (nocc=7, nvir=11, 161 stored blocks): compute_r4_tri
-    with its OO batch, projector, divide, norms, t4 += r4 (dcc.graph.T4Iteration), eager."""
+    with its OO batch, projector, divide, norms, t4 += r4 (dcc.graph.T4Iteration), eager:
+    three warm-up steps, then `reps` steps timed with CUDA events."""
     from dcc import graph, synthetic
     it = graph.T4Iteration(synthetic.make_t4_inputs(7, 11, seed=3), kind)
-    for _ in range(reps):
+    for _ in range(3):
         it.step()
     torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        it.step()
+    e1.record()
+    torch.cuda.synchronize()
+    print(f"t4 {kind} nocc=7 nvir=11: {e0.elapsed_time(e1) / max(reps, 1):.2f} ms per step (eager)")
+    if breakdown:
+        _breakdown(it.step)
 
 
 def main():
@@ -292,7 +308,7 @@ def main():
                     help="p3 case: which symmetrizer")
     ap.add_argument("--time", action="store_true", help="p3 case: print CUDA-event timings")
     ap.add_argument("--dchunk", type=int, default=None, help="qsample case: d-chunk of the split path")
-    ap.add_argument("--breakdown", action="store_true", help="t3half case: per-kernel device times")
+    ap.add_argument("--breakdown", action="store_true", help="t3half / t4 case: per-kernel device times")
     a = ap.parse_args()
     if a.case == "gemm":
         case_gemm(a.kind, a.reps)
@@ -301,7 +317,7 @@ def main():
     elif a.case == "update":
         case_update(a.reps)
     elif a.case == "t4":
-        case_t4(a.reps, a.kind)
+        case_t4(a.reps, a.kind, a.breakdown)
     elif a.case == "t3iter":
         case_t3iter(a.reps, a.nocc or 10, a.nvir, a.kind)
     elif a.case == "t3half":

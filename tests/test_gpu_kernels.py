@@ -262,6 +262,21 @@ def test_t4_elementwise(C, oracle, nvir):
     assert np.array_equal(host(dT), A + R)
 
 
+@pytest.mark.parametrize("nblk,nvir", [(1, 3), (7, 11), (161, 11), (3, 20)])
+def test_t4_forms_batched(C, oracle, nblk, nvir):
+    """All blocks' transpose-add and quadruple-sym forms in one launch each: bit-identical
+    to the oracle applied block by block."""
+    c4 = C[2]
+    rng = np.random.default_rng(nblk + nvir)
+    A = rng.standard_normal((nblk,) + (nvir,) * 4)
+    T3, V = c4.t4_forms_batched(dev(A).view(nblk, -1), nvir)
+    T3, V = host(T3).reshape(A.shape), [host(v).reshape(A.shape) for v in V]
+    for q in range(nblk):
+        assert np.array_equal(T3[q], oracle.t4_transpose_add(A[q], nvir))
+        for m, w in enumerate(oracle.t4_quadruple_sym(A[q], nvir)):
+            assert np.array_equal(V[m][q], w)
+
+
 def test_r4_divide_unpack_gather(C, oracle):
     c4 = C[2]
     rng = np.random.default_rng(10)

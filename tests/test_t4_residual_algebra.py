@@ -1,9 +1,10 @@
-"""compute_r4_tri without its OO batch: the full-ordered-space formulation of
-dcc.t4_residual (every per-block string as one einsum over all orderings of
-(i,j,k,l), W_oovvvv kept for every ordered pair) against the oracle's literal
-per-block loop (oracle/t4_ref.py), in FP64 on the CPU, relative 1e-12.  The
-P3_201 / P4_201 spin summations are the oracle's C restatement here (the GPU
-path uses this library's kernels, checked bit for bit elsewhere)."""
+"""compute_r4_tri without its OO batch: dcc.t4_residual's formulation (every per-block
+string as one contraction batched over the stored blocks, its operands cut at each
+block's occupied slots; the W builders over every ordering of (i,j,k,l), W_oovvvv kept
+for every ordered pair) against the oracle's literal per-block loop (oracle/t4_ref.py),
+in FP64 on the CPU, relative 1e-12.  The P3_201 / P4_201 spin summations are the
+oracle's C restatement here (the GPU path uses this library's kernels, checked bit for
+bit elsewhere)."""
 import numpy as np
 import pytest
 import torch
