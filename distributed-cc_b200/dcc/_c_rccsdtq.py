@@ -2,6 +2,8 @@
 distr_cc/_rccsdtq_core.py (same names and argument meaning, torch CUDA tensors)."""
 from __future__ import annotations
 
+import ctypes
+
 import numpy as np
 import torch
 
@@ -122,3 +124,45 @@ def t4_add_(t4, r4, nocc4, nvir):
         raise ValueError("t4/r4 smaller than nocc4 * nvir^4")
     L.call("dcc_t4_add", L.ptr(t4), L.ptr(r4), n, L.stream_ptr())
     return t4
+
+
+def t4_strings(ops, desc, quads, nocc, nvir, r4, beta=0.0, status=None, pairs=None):
+    """r4 = beta r4 + every string of the descriptor table `desc` [nstr, 32] (int64, device)
+    over every stored block of `quads` [nq, 4] (int32, device), one launch (the per-block
+    strings of compute_r4_tri and its OO batch, distr_cc/rccsdtq.py:862-1349).  ops: the
+    operand tensors the descriptors index (contiguous FP64, device).  pairs: None, or
+    (pair_off [nq, ngroups+1], pair_sm [npairs, 2]) int32 device tensors for the pair-mode
+    strings.  status: int32 device word, bits set by the kernel's checks (a new zero word
+    when None).  Returns status."""
+    n = len(ops)
+    ops = [L.as_tensor(t, f64, "operand") for t in ops]
+    desc = L.as_tensor(desc, torch.int64, "desc")
+    quads = L.as_tensor(quads, torch.int32, "quads")
+    r4 = L.as_tensor(r4, f64, "r4")
+    if desc.dim() != 2 or desc.shape[1] != 32:
+        raise ValueError("desc must be [nstr, 32]")
+    nq = quads.shape[0]
+    if quads.shape != (nq, 4) or r4.numel() != nq * nvir ** 4:
+        raise ValueError("quads must be [nq, 4] and r4 [nq, nvir^4]")
+    if status is None:
+        status = torch.zeros(1, dtype=torch.int32, device=r4.device)
+    if pairs is None:
+        off = sm = None
+        ngroups = npairs = 0
+    else:
+        off = L.as_tensor(pairs[0], torch.int32, "pair_off")
+        sm = L.as_tensor(pairs[1], torch.int32, "pair_sm")
+        ngroups, npairs = off.shape[1] - 1, sm.shape[0]
+        if off.shape[0] != nq or sm.dim() != 2 or sm.shape[1] != 2:
+            raise ValueError("pair_off must be [nq, ngroups+1] and pair_sm [npairs, 2]")
+    ptrs = (ctypes.c_void_p * n)(*[t.data_ptr() for t in ops])
+    numel = (ctypes.c_int64 * n)(*[t.numel() for t in ops])
+    L.call("dcc_t4_strings", ptrs, numel, n, L.ptr(desc), desc.shape[0], L.ptr(quads), nq, L.ptr(off), L.ptr(sm),
+           ngroups, npairs, nocc, nvir, float(beta), L.ptr(r4), L.ptr(status), L.stream_ptr())
+    return status
+
+
+def t4_strings_rows_per_cta(nq, nvir):
+    """Output rows a that one CTA of t4_strings holds (-1 when nvir^3 doubles exceed its
+    shared-memory accumulator)."""
+    return int(L.lib().dcc_t4_strings_rows_per_cta(int(nq), int(nvir)))

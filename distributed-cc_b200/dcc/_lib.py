@@ -70,6 +70,9 @@ _SIGS = {
     "dcc_t4_spin_summation_quadruple_sym": [c_vp] * 5 + [c_i64, c_vp],
     "dcc_t4_transpose_add_batched": [c_vp, c_vp, c_i64, c_i64, c_vp],
     "dcc_t4_spin_summation_quadruple_sym_batched": [c_vp] * 5 + [c_i64, c_i64, c_vp],
+    "dcc_t4_strings": [c_vp, c_vp, ctypes.c_int, c_vp, ctypes.c_int, c_vp, c_i64, c_vp, c_vp, ctypes.c_int, c_i64,
+                       c_i64, c_i64, ctypes.c_double, c_vp, c_vp, c_vp],
+    "dcc_t4_strings_rows_per_cta": [c_i64, c_i64],
     "dcc_r4_local_tri_divide_e": [c_vp, c_vp, c_vp, c_i64, c_i64, c_vp],
     "dcc_unpack_t4_ijkl_single": [c_vp, c_vp, c_vp] + [c_i64] * 6 + [c_vp],
     "dcc_fill_local_data_ijkl": [c_vp, c_vp, c_vp, c_vp, c_i64, c_i64, c_vp],

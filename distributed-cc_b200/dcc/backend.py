@@ -113,6 +113,32 @@ def _dev(a, device):
     return torch.as_tensor(a, device=device)
 
 
+def _dev_async(a, device, state):
+    """A numpy array copied to the device on a side stream (counted in TRANSFER): returns the
+    device tensor and leaves in state the event that marks its arrival.  From pageable host
+    memory the call returns once the bytes are staged, while kernels already enqueued on the
+    compute stream keep running."""
+    if isinstance(a, (torch.Tensor, DeviceT3Local)):
+        t = _dev(a, device)
+        ev = torch.cuda.Event()
+        ev.record()
+        state["upload_ready"] = ev
+        return t
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    TRANSFER.h2d += a.nbytes
+    side = state.get("upload_stream")
+    if side is None:
+        side = state["upload_stream"] = torch.cuda.Stream(device=device)
+    out = torch.empty(a.shape, dtype=f64, device=device)
+    out.record_stream(side)
+    with torch.cuda.stream(side):
+        out.copy_(torch.from_numpy(a), non_blocking=True)
+        ev = torch.cuda.Event()
+        ev.record(side)
+    state["upload_ready"] = ev
+    return out
+
+
 def _host(t):
     """A device tensor read back to a numpy array (counted in TRANSFER)."""
     a = t.cpu().numpy()
@@ -311,13 +337,23 @@ def update_amps_rccsdt_tri_(mycc, tamps, eris, mod):
     mod.intermediates_t3(mycc, imds, t2)
     d = _Inputs()
     for name in _T3_IMDS:
-        setattr(d, name, _dev(getattr(imds, name), dev))
+        if name != "W_vvvv":
+            setattr(d, name, _dev(getattr(imds, name), dev))
     it.feedback_w(d.W_vooo, d.W_vvvo, sl["oovv"])
+    W_vvvv = imds.W_vvvv
     imds = None
     _state(mycc).pop("fb_slices", None)
     d.t2 = _dev(t2, dev)
     d.ijk = it.ijk
-    it.residual(d, T)
+
+    def wvvvv_ready():
+        # the largest intermediate (nvir^4) comes in while the device runs every other term
+        # of the residual; it is needed only by the W_vvvv.t3 GEMMs at the end
+        d.W_vvvv = _dev_async(W_vvvv, dev, _state(mycc))
+        return _state(mycc)["upload_ready"]
+
+    d.W_vvvv = None
+    it.residual(d, T, wvvvv_ready=wvvvv_ready)
     eia = mo_energy[:nocc, None] - mo_energy[None, nocc:] - getattr(mycc, "level_shift", 0.0)
     nd = mod.resolve_nvir_diis(mycc, nvir) if hasattr(mod, "resolve_nvir_diis") else nvir
     norms = _host(it.update(T, _dev(eia, dev), nvir_active=nd))

@@ -367,7 +367,10 @@ class T3Residual:
         """r3 = compute_r3_tri for canonical t3 (the OO batch terms included when with_oo).
 
         wvvvv_ready: optional CUDA event the W_vvvv.t3 part waits for, so a caller can
-        stream W_vvvv to the device while the other terms run.  inputs_ready: optional CUDA
+        stream W_vvvv to the device while the other terms run; or a callable, called once
+        every other term is enqueued, that brings d.W_vvvv in and returns that event (a
+        caller holding W_vvvv in pageable host memory copies it while the device works on
+        the rest).  inputs_ready: optional CUDA
         event for d's other tensors, waited for after the unpack of t3 (which needs none of
         them), so their upload overlaps it.  unpacked: U holds t3 unpacked already (unpack_)."""
         if r3 is None:
@@ -379,6 +382,8 @@ class T3Residual:
         if self.Ganti is not None:
             perm_gather_(r3, d.ijk, nv, 1.0, [(self.Ganti, 1.0, full_strides(no, nv), OOOO_SET)], nocc=no,
                          status=self.gstatus)
+        if callable(wvvvv_ready):
+            wvvvv_ready = wvvvv_ready()
         if wvvvv_ready is not None:
             torch.cuda.current_stream().wait_event(wvvvv_ready)
         if self.precision == "fp64":

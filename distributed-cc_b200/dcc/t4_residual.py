@@ -56,6 +56,7 @@ def dense_vvvv_fvv_(r4, t4, W_vvvv, F_vv, precision="fp64"):
 # ----------------------------------------------------------------------------
 
 import itertools  # noqa: E402
+import struct  # noqa: E402
 
 import numpy as np  # noqa: E402
 
@@ -200,8 +201,9 @@ def _einsum(kind, subs, X, Y, out, alpha):
         contract.einsum_into(subs, X, Y, out, alpha, 1.0, kind)
 
 
-def build_intermediates(eris, W_oooo, W_ovov, W_vvvv, t2, t3, t3p, t4, nocc, spin4):
-    """The W builders of distr_cc/rccsdtq.py:700-833 as full tensors (FP64, torch)."""
+def build_intermediates(eris, W_oooo, W_ovov, W_vvvv, t2, t3, t3p, t4, nocc, spin4, T4full=None):
+    """The W builders of distr_cc/rccsdtq.py:700-833 as full tensors (FP64, torch).  T4full:
+    unpack_all_orderings(t4) when the caller has it already."""
     e = torch.einsum
     o, v = slice(0, nocc), slice(nocc, None)
     W = {}
@@ -215,7 +217,7 @@ def build_intermediates(eris, W_oooo, W_ovov, W_vvvv, t2, t3, t3p, t4, nocc, spi
     X = e('mnek,ijae->kjinma', eris[o, o, v, o], t2) + 0.5 * e('mnef,ijkaef->kjinma', eris[o, o, v, v], t3)
     W["W_ooooov"] = X + X.permute(1, 0, 2, 4, 3, 5)
     # W_oooovv / W_oovvvv: the T4 sums over every ordering (P4_201 applied per ordering)
-    T4s = unpack_all_orderings(t4, nocc)
+    T4s = unpack_all_orderings(t4, nocc) if T4full is None else T4full.clone()
     spin4(T4s)
     Woo = 0.5 * e('mief,ijklfabe->jklmab', eris[o, o, v, v], T4s)
     Word = -0.5 * e('jief,ijklfabc->klabce', eris[o, o, v, v], T4s)
@@ -254,6 +256,159 @@ def _gather_slots(X, subs, nocc, cache, name):
     return cache[key], rest
 
 
+# The operands of the fused strings kernel (dcc_t4_strings), in its operand-table order, and
+# the tensor each T name of _R4_STRINGS reads.  The dense strings add Wf, W_vvvv and t4; the
+# OO batch adds t4, its block forms, the unpacked T4 of every ordering and its W tensors.
+_FUSED_OPS = ("W_vvvo", "W_vooo", "W_oovvvo", "W_ovovvo", "W_ovovvo_s", "W_ooooov", "W_oooovv", "W_oovvvv",
+              "t3", "t3p", "t3s", "t2")
+_DENSE_OPS = ("Wf", "W_vvvv")
+_OO_OPS = ("F_oo", "W_oooo", "T4full", "W_ovov", "W_voov", "T3", "V0", "V1", "V2", "V3")
+# the F_oo / W_oooo prefactor slots of the OO batch as strings over every ordering (subscripts, alpha)
+_OO_PLAIN = (("F_oo", "mi", "mjklabcd", -1.0), ("F_oo", "mj", "imklabcd", -1.0), ("F_oo", "mk", "ijmlabcd", -1.0),
+             ("F_oo", "ml", "ijkmabcd", -1.0), ("W_oooo", "mnij", "mnklabcd", 1.0),
+             ("W_oooo", "mnik", "mjnlabcd", 1.0), ("W_oooo", "mnil", "mjknabcd", 1.0),
+             ("W_oooo", "mnjk", "imnlabcd", 1.0), ("W_oooo", "mnjl", "imknabcd", 1.0),
+             ("W_oooo", "mnkl", "ijmnabcd", 1.0))
+_T_OPERAND = {"t3": "t3", "t3_m": "t3", "t3_mn": "t3", "t3p_m": "t3p", "t3s_m": "t3s", "t2_m": "t2", "t2": "t2"}
+
+
+def _operand_shapes(nocc, nv, nq):
+    o, v = nocc, nv
+    return {"W_vvvo": (v, v, v, o), "W_vooo": (v, o, o, o), "W_oovvvo": (o, o, v, v, v, o),
+            "W_ovovvo": (o, v, o, v, v, o), "W_ovovvo_s": (o, v, o, v, v, o), "W_ooooov": (o, o, o, o, o, v),
+            "W_oooovv": (o, o, o, o, v, v), "W_oovvvv": (o, o, v, v, v, v), "t3": (o, o, o, v, v, v),
+            "t3p": (o, o, o, v, v, v), "t3s": (o, o, o, v, v, v), "t2": (o, o, v, v), "Wf": (v, v, v, v),
+            "W_vvvv": (v, v, v, v), "t4": (nq, v, v, v, v), "F_oo": (o, o), "W_oooo": (o, o, o, o),
+            "T4full": (o, o, o, o, v, v, v, v), "W_ovov": (o, v, o, v), "W_voov": (v, o, o, v),
+            "T3": (nq, v, v, v, v), "V0": (nq, v, v, v, v), "V1": (nq, v, v, v, v), "V2": (nq, v, v, v, v),
+            "V3": (nq, v, v, v, v)}
+
+
+def string_descriptor(wsubs, wshape, wop, tsubs, tshape, top, alpha, mode=0):
+    """The 32-int64 descriptor of dcc_t4_strings for r4[q][abcd] += alpha W[wsubs] T[tsubs]:
+    i, j, k, l are the block's occupied indices, q the block index, a..d the output, every
+    other letter (at most two) is summed.  mode g+1: a pair-mode string of group g, where W's
+    letter M is the pair's occupied index and T's letter Q its source block.  Operands are
+    C-contiguous of the given shapes."""
+    def strides(shape):
+        st = [1] * len(shape)
+        for p in range(len(shape) - 2, -1, -1):
+            st[p] = st[p + 1] * shape[p + 1]
+        return st
+
+    if len(wsubs) != len(wshape) or len(tsubs) != len(tshape):
+        raise ValueError("subscripts do not match the operand ranks")
+    ws, ts = strides(wshape), strides(tshape)
+    d = [0] * 32
+    d[0], d[1] = wop, top
+    for n, c in enumerate("ijkl"):
+        d[2 + n] = ws[wsubs.index(c)] if c in wsubs else 0
+        d[6 + n] = ts[tsubs.index(c)] if c in tsubs else 0
+    d[10] = ws[wsubs.index("q")] if "q" in wsubs else 0
+    d[11] = ts[tsubs.index("q")] if "q" in tsubs else 0
+    if mode:
+        if "Q" not in tsubs or "M" not in wsubs or "q" in tsubs:
+            raise ValueError("a pair-mode string reads W at M and T at Q")
+        d[11] = ts[tsubs.index("Q")]
+        d[30] = ws[wsubs.index("M")]
+        d[31] = mode
+    mask = 0
+    for n, c in enumerate("abcd"):
+        if (c in wsubs) == (c in tsubs):
+            raise ValueError("output letter %s must be in exactly one operand" % c)
+        if c in wsubs:
+            d[12 + n] = ws[wsubs.index(c)]
+            mask |= 1 << n
+        else:
+            d[16 + n] = ts[tsubs.index(c)]
+    d[20] = mask
+    # iteration orders: W's output letters (rows) and T's (columns), slowest first, the
+    # letter with the smallest stride last; nibble p holds letter + 1 of position p
+    rows = sorted((n for n in range(4) if mask >> n & 1), key=lambda n: -d[12 + n])
+    cols = sorted((n for n in range(4) if not mask >> n & 1), key=lambda n: -d[16 + n])
+    d[28] = sum((n + 1) << (4 * p) for p, n in enumerate(rows))
+    d[29] = sum((n + 1) << (4 * p) for p, n in enumerate(cols))
+    summed = [c for c in wsubs if c not in "ijklqabcdMQ"]
+    if sorted(summed) != sorted(c for c in tsubs if c not in "ijklqabcdMQ") or len(summed) > 2:
+        raise ValueError("at most two summed letters, each in both operands")
+    ks = []
+    for c in summed:
+        if wshape[wsubs.index(c)] != tshape[tsubs.index(c)]:
+            raise ValueError("extents of %s differ" % c)
+        ks.append((wshape[wsubs.index(c)], ws[wsubs.index(c)], ts[tsubs.index(c)]))
+    ks += [(1, 0, 0)] * (2 - len(ks))
+    d[21:24], d[24:27] = ks[0], ks[1]
+    d[27] = struct.unpack("<q", struct.pack("<d", float(alpha)))[0]
+    return d
+
+
+def fused_plan(nocc, nv, dense, device, oo=False):
+    """(descriptor table [nstr, 32] int64, quads [nq, 4] int32, operand names, pair lists) of
+    the fused strings kernel: the strings of _R4_STRINGS; with `dense` the F_vv / W_vvvv
+    strings of dense_vvvv_fvv_ (W_vvvv with F_vv folded into its first and last string); with
+    `oo` the OO batch: the F_oo / W_oooo strings over the unpacked T4 of every ordering and
+    every W_ovov / W_voov string of _OO_TABLE in pair mode over oo_pairs (pair lists
+    (pair_off [nq, 17], pair_sm [npairs, 2]), None without `oo`)."""
+    def build():
+        quads = stored_quadruples(nocc)
+        nq = len(quads)
+        shp = _operand_shapes(nocc, nv, nq)
+        names = list(_FUSED_OPS) + (["t4"] if dense or oo else []) + (list(_DENSE_OPS) if dense else []) + \
+            (list(_OO_OPS) if oo else [])
+        rows = []
+        for sub, wn, ws, tn, ts, al in _R4_STRINGS:
+            sw, st = sub.split(",")
+            tname = _T_OPERAND[tn]
+            rows.append(string_descriptor(_slots(wn, ws, sw), shp[wn], names.index(wn),
+                                          _slots(tn, ts, st), shp[tname], names.index(tname), al))
+        if dense:
+            for n, s in enumerate(STRINGS):
+                wsubs, rest = s.split(",")
+                wn = "Wf" if n in (0, 5) else "W_vvvv"
+                rows.append(string_descriptor(wsubs, shp[wn], names.index(wn), rest.split("->")[0], shp["t4"],
+                                              names.index("t4"), 1.0))
+        pairs = None
+        if oo:
+            for wn, ws, ts, al in _OO_PLAIN:
+                rows.append(string_descriptor(ws, shp[wn], names.index(wn), ts, shp["T4full"],
+                                              names.index("T4full"), al))
+            groups = sorted(oo_pairs(nocc))
+            for gid, (g, c) in enumerate(groups):
+                x = "ijkl"[g]
+                for wn, sub, al, form in _OO_TABLE[g][c]:
+                    ws, ts = sub.split(",")
+                    if wn == "ovov":  # W_ovov[m, a, x, e]
+                        wsubs, wname = "M" + ws[0] + x + ws[1], "W_ovov"
+                    else:  # W_voov[a, m, x, e] = W_ovvo[m, a, e, x]
+                        wsubs, wname = ws[0] + "M" + x + ws[1], "W_voov"
+                    tname = "t4" if form == "T" else form
+                    rows.append(string_descriptor(wsubs, shp[wname], names.index(wname), "Q" + ts, shp[tname],
+                                                  names.index(tname), al, mode=gid + 1))
+            lists = oo_pairs(nocc)
+            per = [[[] for _ in groups] for _ in range(nq)]
+            for gid, gc in enumerate(groups):
+                si, ti, m, _x = lists[gc]
+                for a, b, mm in zip(si, ti, m):
+                    per[b][gid].append((a, mm))
+            off, sm = [], []
+            for q in range(nq):
+                row = [len(sm)]
+                for gid in range(len(groups)):
+                    sm.extend(per[q][gid])
+                    row.append(len(sm))
+                off.append(row)
+            pairs = (torch.tensor(off, dtype=torch.int32, device=device),
+                     torch.tensor(sm, dtype=torch.int32, device=device).view(-1, 2))
+        return (torch.tensor(rows, dtype=torch.int64, device=device),
+                torch.tensor(quads, dtype=torch.int32, device=device), names, pairs)
+    return _cached(("fused", nocc, nv, bool(dense), bool(oo)), device, build)
+
+
+def fused_status(device):
+    """The int32 status word of the fused strings kernel on `device` (0: every string ran)."""
+    return _cached(("fused_status",), device, lambda: torch.zeros(1, dtype=torch.int32, device=device))
+
+
 def compute_r4_tri_(r4, eris, F_vv, W_vvvo, W_vooo, W_vvvv, W_oooo, W_ovov, t2, t3, t4, nocc, precision="fp64",
                     spin3=None, spin4=None, F_oo=None, W_ovvo=None, forms=None):
     """r4[stored blocks] = compute_r4_tri (distr_cc/rccsdtq.py:834-1060); with F_oo and W_ovvo
@@ -264,14 +419,18 @@ def compute_r4_tri_(r4, eris, F_vv, W_vvvo, W_vooo, W_vvvv, W_oooo, W_ovov, t2, 
     apply P3_201 / P4_201 in place to [n, nvir^3] / [n, nvir^4] blocks (default: this
     library's kernels).
 
-    The ~100 per-block strings of distr_cc/rccsdtq.py:862-1033 each run as ONE batched
-    contraction over the stored blocks: every operand is cut at the block's occupied slots
-    for all blocks at once (_gather_slots) and the strings contract over the remaining
-    virtual (and summed occupied) indices with the block as the batch index, straight into
-    r4 -- the work and memory of the stored blocks only.  Their contractions are short
-    (K = nvir or nocc), so they stay FP64 in every precision; precision "bf16x3"/"tf32x3"
-    runs the W_vvvv.t4 strings (K = nvir^2) as split GEMMs; the builders stay FP64."""
-    from . import _c_rccsdt, _c_rccsdt_q
+    On a CUDA device the ~100 per-block strings of distr_cc/rccsdtq.py:862-1033 run in ONE
+    launch of the fused strings kernel (dcc_t4_strings: a CTA per stored block and row range
+    holds its r4 rows in shared memory and runs every string over them, operands read in
+    place through the descriptors of fused_plan), and with F_oo given the OO batch joins
+    the same launch (its F_oo / W_oooo slots as strings over the unpacked T4, its W_ovov /
+    W_voov strings in pair mode over the sparse (source, output) pair lists).  Their
+    contractions are short (K = nvir, nocc, nocc^2 or nocc nvir), so they are FP64 in every
+    precision; in FP64 the F_vv / W_vvvv strings join the same launch, and precision
+    "bf16x3"/"tf32x3" runs those (K = nvir^2) as split GEMMs.  The builders stay FP64.  On the CPU (the formulation
+    tests) each string is one einsum batched over the stored blocks, its operands cut at
+    every block's occupied slots (_gather_slots)."""
+    from . import _c_rccsdt, _c_rccsdt_q, _c_rccsdtq
     kind = None if precision == "fp64" else contract.KIND[precision]
     nv = t2.shape[2]
     if spin3 is None:
@@ -281,6 +440,29 @@ def compute_r4_tri_(r4, eris, F_vv, W_vvvo, W_vooo, W_vvvv, W_oooo, W_ovov, t2, 
     t3 = t3.contiguous()
     t3p = t3.clone()
     spin3(t3p)
+    nq = r4.shape[0]
+    if t3.is_cuda and _c_rccsdtq.t4_strings_rows_per_cta(nq, nv) >= 1:
+        # every string of every stored block in one launch (FP64), the OO batch included when
+        # F_oo is given; the W_vvvv strings join it in FP64 and run as split GEMMs otherwise
+        dense, oo = kind is None, F_oo is not None
+        T4full = unpack_all_orderings(t4, nocc)
+        W = build_intermediates(eris, W_oooo, W_ovov, W_vvvv, t2, t3, t3p, t4, nocc, spin4, T4full=T4full)
+        W["W_vvvo"], W["W_vooo"] = W_vvvo, W_vooo
+        desc, quads, names, pairs = fused_plan(nocc, nv, dense, t3.device, oo=oo)
+        ops = dict(W, t3=t3, t3p=t3p, t3s=t3 + t3.permute(0, 1, 2, 4, 5, 3), t2=t2, t4=t4)
+        if dense:
+            ops.update(Wf=w_with_f(W_vvvv, F_vv), W_vvvv=W_vvvv)
+        if oo:
+            if forms is None:
+                forms = lambda t: _c_rccsdtq.t4_forms_batched(t, nv)  # noqa: E731
+            T3f, V = forms(t4)
+            ops.update(F_oo=F_oo, W_oooo=W_oooo, T4full=T4full, W_ovov=W_ovov,
+                       W_voov=W_ovvo.permute(1, 0, 3, 2), T3=T3f, V0=V[0], V1=V[1], V2=V[2], V3=V[3])
+        _c_rccsdtq.t4_strings([ops[n].contiguous() for n in names], desc, quads, nocc, nv, r4.view(nq, -1),
+                              0.0, fused_status(t3.device), pairs=pairs)
+        if not dense:
+            dense_vvvv_fvv_(r4, t4, W_vvvv, F_vv, precision)
+        return r4
     W = build_intermediates(eris, W_oooo, W_ovov, W_vvvv, t2, t3, t3p, t4, nocc, spin4)
     W["W_vvvo"], W["W_vooo"] = W_vvvo, W_vooo
     T = {"t3": t3, "t3_m": t3, "t3_mn": t3, "t3p_m": t3p, "t3s_m": t3 + t3.permute(0, 1, 2, 4, 5, 3),

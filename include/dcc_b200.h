@@ -266,6 +266,42 @@ DCC_API int dcc_t4_transpose_add_batched(const double *src, double *dst, int64_t
 DCC_API int dcc_t4_spin_summation_quadruple_sym_batched(const double *src, double *B0, double *B1, double *B2,
                                                         double *B3, int64_t nblocks, int64_t nvir, void *stream);
 
+/* The per-block strings of compute_r4_tri (distr_cc/rccsdtq.py:862-1055, the reference's loop
+ * over its stored blocks) in ONE launch, FP64:
+ *   r4[q][a,b,c,d] = beta r4[q][a,b,c,d] + sum_s alpha_s sum_{k0,k1} W_s[..] T_s[..]
+ * for every stored block q (occupied indices quads[q][0..3], DEVICE int32 [nq][4]) and every
+ * string s of the DEVICE descriptor table desc[nstr][DCC_T4S_DESC_LEN] (int64):
+ *    0 W operand index   1 T operand index      (into ops / op_numel, HOST arrays of nops <= 16)
+ *    2-5  W strides of the occupied letters i, j, k, l     6-9  T strides of i, j, k, l
+ *   10 W stride of the block index q                      11 T stride of q
+ *   12-15 W strides of the output letters a, b, c, d      16-19 T strides of a, b, c, d
+ *   20 bit x set: output letter x is in W (its T stride must be 0), else in T (W stride 0)
+ *   21 K0  22 W stride  23 T stride of the first summed letter
+ *   24 K1  25 W stride  26 T stride of the second (K1 = 1 when there is none)
+ *   27 alpha as the bits of an IEEE double
+ *   28 row order: nibble p (p = 0 slowest) holds 1 + the output letter at position p of the
+ *      rows (the letters of W, each once; 0 = empty position); 29 the same for the columns
+ *      (the letters of T); the kernel iterates the last filled position fastest
+ *   30 pair mode: the W stride of the pair's occupied index m
+ *   31 mode: 0 = a string of the block itself; g + 1 = pair mode for group g < ngroups: the
+ *      string runs once for every pair (src, m) = pair_sm[p][0..1] (DEVICE int32 [npairs][2])
+ *      with p in [pair_off[q][g], pair_off[q][g+1]) (DEVICE int32 [nq][ngroups+1]); field 11
+ *      then strides the source block src instead of q, and W's base moves by m x field 30
+ *      (the OO batch's W_ovov / W_voov terms, distr_cc/rccsdtq.py:1062-1349, sparse: only the
+ *      (source, output) pairs that exist)
+ * An element of an operand is ops[n][sum of stride x index]; strides are in elements.  Every
+ * string is bounds-checked against op_numel before it runs; a failing string is skipped and
+ * sets bit 2 of *status (DEVICE int), an out-of-range occupied index bit 1, a failing pair
+ * bit 4.  ngroups = 0 allows NULL pair lists.  r4 is [nq][nvir^4]; nvir^3 doubles must fit
+ * the per-CTA accumulator (nvir <= 29); at most 32 operands, each below 2^31 elements. */
+#define DCC_T4S_DESC_LEN 32
+DCC_API int dcc_t4_strings(const double *const *ops, const int64_t *op_numel, int nops, const int64_t *desc, int nstr,
+                           const int32_t *quads, int64_t nq, const int32_t *pair_off, const int32_t *pair_sm,
+                           int ngroups, int64_t npairs, int64_t nocc, int64_t nvir, double beta, double *r4,
+                           int *status, void *stream);
+/* Output rows a per CTA that dcc_t4_strings uses for nq blocks (-1: nvir too large). */
+DCC_API int dcc_t4_strings_rows_per_cta(int64_t nq, int64_t nvir);
+
 /* r4[q] /= eia[i,a]+eia[j,b]+eia[k,c]+eia[l,d] for ijkl = local_ijkl[q]
  * (DEVICE int32 [nlocal][4]).  Replaces r4_local_tri_divide_e_
  * (src/rccsdtq.c:1055-1088). */

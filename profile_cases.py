@@ -1,6 +1,6 @@
 """Small, self-contained launches of single kernels for profiler captures.
 
-    python profile_cases.py gemm   [--kind bf16x3] [--reps 3]
+    python profile_cases.py gemm   [--kind bf16x3] [--reps 3] [--nocc 10 --nvir 90]
     python profile_cases.py p3     [--reps 3] [--nvir 90] [--op p3|p3_422|roundtrip|triple|transpose] [--time]
     python profile_cases.py update [--reps 3]
     python profile_cases.py q      [--reps 3]
@@ -10,6 +10,8 @@
     python profile_cases.py unpack [--reps 3]
     python profile_cases.py qgroup [--reps 3]
     python profile_cases.py t3half [--reps 3] [--nocc 15 --nvir 93] [--kind bf16x3|fp64] [--breakdown]
+    python profile_cases.py t4     [--reps 3] [--kind bf16x3|fp64] [--breakdown]
+    python profile_cases.py oddnv  [--reps 3] [--nocc 5 --nvir 93] [--time]
 
 Each case builds its inputs once and launches the kernel `reps` times, so a
 profiler can skip the warm-up launches and capture the last one.  Sizes are
@@ -26,9 +28,10 @@ sys.path.insert(0, os.path.join(os.path.dirname(os.path.abspath(__file__)), "dis
 import torch  # noqa: E402
 
 
-def case_gemm(kind, reps):
+def case_gemm(kind, reps, nocc=10, nvir=90):
+    """One W_vvvv.t3 string (M = n3 nvir rows, N = K = nvir^2) as a split GEMM, `reps` launches."""
     from dcc import contract
-    n3, nv = 220, 90
+    n3, nv = nocc * (nocc + 1) * (nocc + 2) // 6, nvir
     g = torch.Generator(device="cuda").manual_seed(0)
     t3 = torch.randn(n3, nv, nv, nv, dtype=torch.float64, device="cuda", generator=g) * 1e-3
     W = torch.randn(nv, nv, nv, nv, dtype=torch.float64, device="cuda", generator=g) * 0.1
@@ -146,6 +149,51 @@ def case_unpack(reps, nocc=10):
     for _ in range(reps):
         t3_residual.unpack_all_(d.t3, U, nocc, 90)
     torch.cuda.synchronize()
+
+
+def case_oddnv(reps, nocc=5, nvir=93, time=False):
+    """The memory-bound T3 passes of one half-iteration at an odd nvir (no TMA: 8-byte row
+    pitch), each on its own buffers: unpack t3 -> U (every ordering), X = P3_201(U) out of
+    place, P3_422(t3) out of place, P3_full(r3) in place, the S3 gather S -> r3.  With time=True
+    each pass is timed with CUDA events (after a 256 MB L2 flush; mean of reps) and printed with
+    its algorithmic bytes and bandwidth."""
+    from dcc import synthetic, t3_residual, _c_rccsdt
+    d = synthetic.make_inputs(nocc, nvir, seed=0)
+    n3, nu = d.t3.shape[0], nocc ** 3
+    U = torch.empty((nu, nvir, nvir, nvir), dtype=torch.float64, device="cuda")
+    X = torch.empty_like(U)
+    V = torch.empty_like(d.t3)
+    r3 = torch.randn_like(d.t3)
+    e3, eu = n3 * nvir ** 3, nu * nvir ** 3
+    passes = [
+        ("unpack t3->U", lambda: t3_residual.unpack_all_(d.t3, U, nocc, nvir), 8 * (e3 + eu)),
+        ("X=P3_201(U)", lambda: _c_rccsdt.t3_spin_summation(U, X, nu, nvir, "P3_201"), 16 * eu),
+        ("V=P3_422(t3)", lambda: _c_rccsdt.t3_spin_summation(d.t3, V, n3, nvir, "P3_422"), 16 * e3),
+        ("P3_full(r3) in place", lambda: _c_rccsdt.t3_spin_summation_inplace_(r3, n3, nvir, "P3_full", -1.0 / 6.0,
+                                                                                1.0), 16 * e3),
+        ("gather S->r3", lambda: t3_residual.perm_gather_(
+            r3, d.ijk, nvir, 0.0, [(X, 1.0, t3_residual.full_strides(nocc, nvir), t3_residual.ALL_S3)], nocc=nocc),
+         8 * (6 * e3 + e3)),
+    ]
+    flush = torch.empty(256 << 20, dtype=torch.int8, device="cuda") if time else None
+    for name, run, nbytes in passes:
+        ts = []
+        for r in range(reps):
+            if time:
+                flush.fill_(r & 127)
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record()
+            run()
+            if time:
+                e1.record()
+                e1.synchronize()
+                ts.append(e0.elapsed_time(e1))
+        torch.cuda.synchronize()
+        if time:
+            ms = sum(ts) / len(ts)
+            print(f"{name:22s} nocc={nocc} nvir={nvir}: {ms:8.3f} ms  {nbytes / 1e9:7.3f} GB  "
+                  f"{nbytes / ms * 1e-6:7.0f} GB/s")
+    assert _c_rccsdt.symmetrize_status() == 0
 
 
 def case_qgroup(reps, nocc=10):
@@ -299,7 +347,7 @@ def case_t4(reps, kind="bf16x3", breakdown=False):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("case", choices=["gemm", "p3", "update", "q", "gather", "xgemm", "oogemm", "unpack", "qgroup",
-                                         "t4", "t3iter", "qsample", "t3half"])
+                                         "t4", "t3iter", "qsample", "t3half", "oddnv"])
     ap.add_argument("--kind", default="bf16x3")
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--nocc", type=int, default=None, help="occupied orbitals (xgemm, oogemm, gather, unpack)")
@@ -311,7 +359,7 @@ def main():
     ap.add_argument("--breakdown", action="store_true", help="t3half / t4 case: per-kernel device times")
     a = ap.parse_args()
     if a.case == "gemm":
-        case_gemm(a.kind, a.reps)
+        case_gemm(a.kind, a.reps, a.nocc or 10, a.nvir)
     elif a.case == "p3":
         case_p3(a.reps, a.nvir, a.op, a.time)
     elif a.case == "update":
@@ -320,6 +368,8 @@ def main():
         case_t4(a.reps, a.kind, a.breakdown)
     elif a.case == "t3iter":
         case_t3iter(a.reps, a.nocc or 10, a.nvir, a.kind)
+    elif a.case == "oddnv":
+        case_oddnv(a.reps, a.nocc or 5, a.nvir if a.nvir != 90 else 93, a.time)
     elif a.case == "t3half":
         case_t3half(a.reps, a.nocc or 15, a.nvir if a.nvir != 90 else 93, a.kind, a.breakdown)
     elif a.case == "qsample":

@@ -66,6 +66,104 @@ def test_compute_r4_tri(oracle, precision, no, nv):
     got = r4.cpu().numpy()
     tol = 1e-11 if precision == "fp64" else 1e-4
     assert np.abs(got - want).max() <= tol * np.abs(want).max()
+    assert int(t4_residual.fused_status(r4.device).item()) == 0
+
+
+@pytest.mark.parametrize("nv", [3, 5, 11, 13])
+def test_fused_strings_split_rows(nv):
+    """The fused strings kernel at sizes where its row split (output rows a per CTA) and its
+    warp tiles are ragged: its r4 against the batched per-string einsums of the same strings
+    on the same device (rtol 1e-12)."""
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from dcc import t4_residual as tr, _c_rccsdtq
+    no = 4
+    g = torch.Generator(device="cuda").manual_seed(nv)
+    nq = len(tr.stored_quadruples(no))
+    shp = tr._operand_shapes(no, nv, nq)
+    ops = {n: torch.randn(sh, dtype=torch.float64, device="cuda", generator=g) for n, sh in shp.items()}
+    desc, quads, names, _ = tr.fused_plan(no, nv, True, "cuda")
+    status = torch.zeros(1, dtype=torch.int32, device="cuda")
+    r4 = torch.full((nq, nv ** 4), 7.0, dtype=torch.float64, device="cuda")
+    _c_rccsdtq.t4_strings([ops[n] for n in names], desc, quads, no, nv, r4, 0.0, status)
+    want = torch.zeros((nq,) + (nv,) * 4, dtype=torch.float64, device="cuda")
+    T = {"t3": ops["t3"], "t3_m": ops["t3"], "t3_mn": ops["t3"], "t3p_m": ops["t3p"], "t3s_m": ops["t3s"],
+         "t2_m": ops["t2"], "t2": ops["t2"]}
+    cache = {}
+    for sub, wn, ws, tn, ts, al in tr._R4_STRINGS:
+        sw, st = sub.split(",")
+        gw, lw = tr._gather_slots(ops[wn], tr._slots(wn, ws, sw), no, cache, wn)
+        gt, lt = tr._gather_slots(T[tn], tr._slots(tn, ts, st), no, cache, tn)
+        want.add_(torch.einsum("q" + lw + ",q" + lt + "->qabcd", gw, gt), alpha=al)
+    for n, s in enumerate(tr.STRINGS):
+        want += torch.einsum(s, ops["Wf" if n in (0, 5) else "W_vvvv"], ops["t4"])
+    torch.cuda.synchronize()
+    assert int(status.item()) == 0
+    err = (r4.view_as(want) - want).abs().max() / want.abs().max()
+    assert float(err) <= 1e-12
+    # beta = 1 adds to r4
+    r4b = r4.clone()
+    _c_rccsdtq.t4_strings([ops[n] for n in names], desc, quads, no, nv, r4b, 1.0, status)
+    assert float((r4b - 2 * r4).abs().max() / r4.abs().max()) <= 1e-15
+
+
+def test_fused_strings_checks():
+    """Descriptors, blocks and pairs the fused kernel refuses before touching memory: an
+    operand index past the table, a stride whose last element lies past its operand, an
+    occupied index out of range, a pair with m outside [0, nocc), a pair range past the list.
+    The string is skipped (status bit 2), the block left unwritten (bit 1), the pair or pair
+    range skipped (bit 4); the other strings, blocks and pairs still run."""
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from dcc import t4_residual as tr, _c_rccsdtq
+    no, nv = 4, 5
+    nq = len(tr.stored_quadruples(no))
+    shp = tr._operand_shapes(no, nv, nq)
+    g = torch.Generator(device="cuda").manual_seed(1)
+    ops = {n: torch.randn(sh, dtype=torch.float64, device="cuda", generator=g) for n, sh in shp.items()}
+    desc, quads, names, _ = tr.fused_plan(no, nv, False, "cuda")
+    args = [ops[n] for n in names]
+    good = torch.zeros(nq, nv ** 4, dtype=torch.float64, device="cuda")
+    _c_rccsdtq.t4_strings(args, desc[1:], quads, no, nv, good, 0.0)
+    for bad in ("op", "stride"):
+        d = desc.clone()
+        if bad == "op":
+            d[0, 0] = len(names)
+        else:  # W_vvvo [a, b, e, j]: stride of e grown until e's last value lies past the end
+            d[0, 22] = 1 + (ops["W_vvvo"].numel() - 1) // (d[0, 21] - 1)
+        st = torch.zeros(1, dtype=torch.int32, device="cuda")
+        r4 = torch.zeros_like(good)
+        _c_rccsdtq.t4_strings(args, d, quads, no, nv, r4, 0.0, st)
+        torch.cuda.synchronize()
+        assert int(st.item()) == 2, bad
+        assert torch.equal(r4, good), bad
+    qd = quads.clone()
+    qd[3, 2] = no
+    st = torch.zeros(1, dtype=torch.int32, device="cuda")
+    r4 = torch.full_like(good, 5.0)
+    _c_rccsdtq.t4_strings(args, desc, qd, no, nv, r4, 0.0, st)
+    torch.cuda.synchronize()
+    assert int(st.item()) == 1
+    assert bool((r4[3] == 5.0).all()) and not bool((r4[4] == 5.0).all())
+    # pair mode: a pair whose m lies outside [0, nocc), a pair range past the list
+    desc, quads, names, (off, sm) = tr.fused_plan(no, nv, False, "cuda", oo=True)
+    shp.update({n: tr._operand_shapes(no, nv, nq)[n] for n in tr._OO_OPS})
+    ops = {n: torch.randn(shp[n], dtype=torch.float64, device="cuda", generator=g) for n in names}
+    args = [ops[n] for n in names]
+    good = torch.zeros(nq, nv ** 4, dtype=torch.float64, device="cuda")
+    _c_rccsdtq.t4_strings(args, desc, quads, no, nv, good, 0.0, pairs=(off, sm))
+    for bad in ("m", "range"):
+        o2, s2 = off.clone(), sm.clone()
+        if bad == "m":
+            s2[0, 1] = no
+        else:
+            o2[2, 5] = s2.shape[0] + 1
+        st = torch.zeros(1, dtype=torch.int32, device="cuda")
+        r4 = torch.zeros_like(good)
+        _c_rccsdtq.t4_strings(args, desc, quads, no, nv, r4, 0.0, st, pairs=(o2, s2))
+        torch.cuda.synchronize()
+        assert int(st.item()) == 4, bad
+        assert torch.isfinite(r4).all(), bad
 
 
 @pytest.mark.parametrize("precision", ["fp64", "bf16x3"])
