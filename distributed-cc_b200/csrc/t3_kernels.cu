@@ -704,37 +704,17 @@ static int orbit_tma_launch(int mode, const double *in, double *const out[3], in
     return DCC_OK;
 }
 
-// CTAs of `kernel` resident on the whole device at once (SMs x active CTAs per SM).
-static int64_t resident_ctas(const void *kernel, int threads, size_t smem) {
-    int dev = 0, nsm = 148, per_sm = 1;
-    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem) != cudaSuccess || per_sm < 1)
-        per_sm = 1;
-    cudaGetLastError();  // an occupancy query that failed leaves no sticky error behind
-    return (int64_t)nsm * per_sm;
-}
-
 static int orbit3_launch(int mode, const double *in, double *o0, double *o1, double *o2, int64_t nblocks,
                          int64_t nvir, const P3Coef &k, void *stream) {
     if (nblocks == 0 || nvir == 0) return DCC_OK;
     int ntile = (int)ceil_div(nvir, TE);
     int64_t ntri = (int64_t)ntile * (ntile + 1) * (ntile + 2) / 6;
-    size_t smem = 2 * 6 * SLOT * sizeof(double);
-    // Every CTA owns one tile triple and walks the blocks b = y, y + gy, ...  All CTAs are
-    // resident at once (gy = resident CTAs / triples), so the tiles of one block are written
-    // close together in time: a tile row of an odd nvir shares its first and last 32-byte
-    // sectors with the neighbouring tiles, and a sector completed by two CTAs far apart in
-    // time leaves L2 partially written (measured 2.2x slower at 3375 blocks of 93^3 when
-    // the grid ran in waves over the blocks).
-    const void *fallback = mode == 0 && nvir <= 1290 ? (const void *)k_p3_inplace
-                           : mode == 0                ? (const void *)k_orbit3<0>
-                           : mode == 1                ? (const void *)k_orbit3<1>
-                                                      : (const void *)k_orbit3<2>;
-    cudaFuncSetAttribute(fallback, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    int64_t gy = resident_ctas(fallback, OT_THREADS, smem) / ntri;
+    // about 8 CTA waves of 148 SMs x 4 resident CTAs, each CTA walking several blocks
+    int64_t gy = (148 * 4 * 8 + ntri - 1) / ntri;
     gy = gy < 1 ? 1 : (gy > nblocks ? nblocks : gy);
     gy = gy > 65535 ? 65535 : gy;
     dim3 grid((unsigned)ntri, (unsigned)gy);
+    size_t smem = 2 * 6 * SLOT * sizeof(double);
     cudaStream_t st = as_stream(stream);
     {
         const bool full = k.p0 == 1.0 && k.p1 == 1.0 && k.p2 == 1.0 && k.p3 == 1.0 && k.p4 == 1.0;
@@ -1813,14 +1793,11 @@ extern "C" int dcc_t3_perm_gather(double *r3, const int32_t *ijk, int64_t nblock
     DCC_REQUIRE(nvir <= 1290, DCC_ERR_UNSUPPORTED, "nvir > 1290 exceeds 32-bit block offsets");
     int ntile = (int)ceil_div(nvir, TE);
     int64_t nt3 = (int64_t)ntile * ntile * ntile;
-    size_t smem = (size_t)2 * nslot * SLOT * sizeof(double);
-    cudaFuncSetAttribute(k_perm_gather, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    // every CTA owns one output tile and walks the blocks; as many block columns as keep the
-    // grid resident, so the tiles of one block are written close together in time (see
-    // orbit3_launch)
-    int64_t gy = resident_ctas((const void *)k_perm_gather, 256, smem) / nt3;
+    int64_t gy = (148 * 4 * 8 + nt3 - 1) / nt3;
     gy = gy < 1 ? 1 : (gy > nblocks ? nblocks : gy);
     gy = gy > 65535 ? 65535 : gy;
+    size_t smem = (size_t)2 * nslot * SLOT * sizeof(double);
+    cudaFuncSetAttribute(k_perm_gather, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     k_perm_gather<<<dim3((unsigned)nt3, (unsigned)gy), 256, smem, as_stream(stream)>>>(r3, ijk, nblocks, (int)nvir,
                                                                                        ntile, beta, g);
     return launch_status("t3_perm_gather");

@@ -49,3 +49,16 @@ def test_energy_independent_of_block_size(oracle):
     assert abs(e1[0]) > 0 and abs(e1[1]) > 0
     for a, b in ((e1, e2), (e1, e3)):
         np.testing.assert_allclose(a, b, rtol=1e-11, atol=1e-14)
+
+
+def test_lazy_t3_slices():
+    """tests/lazy_t3.LazyT (used at the benzene shape) gives the same slices as the full T."""
+    from lazy_t3 import LazyT
+    no, nv = 4, 7
+    _, _, T, _, _ = _inputs(no, nv, 3)
+    trip = [(i, j, k) for i in range(no) for j in range(i, no) for k in range(j, no)]
+    t3 = np.stack([T[:, :, :, i, j, k] for i, j, k in trip])
+    L = LazyT(t3, no)
+    assert L.shape == T.shape
+    for A, B in ((slice(0, 2), slice(2, 4)), (slice(4, 7), slice(0, 3)), (slice(6, 7), slice(6, 7))):
+        np.testing.assert_allclose(L[A, B], T[A, B], rtol=0, atol=1e-15)  # T is symmetric to rounding
