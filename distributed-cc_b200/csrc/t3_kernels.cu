@@ -1109,6 +1109,172 @@ extern "C" int dcc_t3_spin_summation(const double *A, double *B, int64_t nblocks
     return orbit3_launch(0, A, B, nullptr, nullptr, nblocks, nvir, k, stream);
 }
 
+namespace dcc {
+
+// Stage ordering PI's values at the orbit positions P_q(E) of a canonical element E (shared
+// addresses oa[q] in the staging buffer st and in the canonical block's orbit tiles `in`), from
+// the values v[q] = C[P_q(E)] = in[oa[q]]: U[P_q(E)] =
+// C[P_comp6(PI, q)(E)] = v[comp6(PI, q)] (xpass false), or the P3 spin summation of U there (xpass
+// true: the per-position formula of k_p3_inplace over U's values, so the result equals a P3 pass
+// over U bit for bit).  diag: all of E's indices equal (one position).
+struct OrbitAddr {
+    unsigned short a[6];
+};
+
+template <int PI>
+__device__ __forceinline__ void stage_orbit(double *st, const OrbitAddr oa, const double *in, const P3Coef &k,
+                                            bool diag, bool xpass) {
+    double v[6];
+#pragma unroll
+    for (int q = 0; q < 6; q++) v[q] = in[oa.a[q]];
+    if (diag) {
+        const double u = v[comp6(PI, 0)];
+        st[oa.a[0]] = xpass ? dadd(dmul(k.beta, u), dmul(k.ap34, dmul(k.p012, u))) : u;
+        return;
+    }
+    if (!xpass) {
+#pragma unroll
+        for (int q = 0; q < 6; q++) st[oa.a[q]] = v[comp6(PI, q)];
+        return;
+    }
+#pragma unroll
+    for (int q = 0; q < 6; q++) {
+        const double tu = dadd(dadd(dmul(k.p0, v[comp6(PI, q)]), dmul(k.p1, v[comp6(PI, comp6(5, q))])),
+                               dmul(k.p2, v[comp6(PI, comp6(2, q))]));
+        const double tw = dadd(dadd(dmul(k.p0, v[comp6(PI, comp6(1, q))]), dmul(k.p1, v[comp6(PI, comp6(3, q))])),
+                               dmul(k.p2, v[comp6(PI, comp6(4, q))]));
+        st[oa.a[q]] = dadd(dmul(k.beta, v[comp6(PI, q)]), dmul(k.alpha, dadd(dmul(k.p3, tu), dmul(k.p4, tw))));
+    }
+}
+
+// Unpack and P3 of every ordering in one pass: for every canonical block C = t3[q] and every
+// distinct ordering o of its occupied indices, U[o] = C with its virtual axes permuted (the
+// unpack of k_unpack_band / k_unpack_all) and X[o] = beta U[o] + alpha P(U[o]) (the pass
+// k_p3_inplace makes over U), both from the orbit tiles of C in shared memory.  A CTA owns one
+// tile triple (as k_p3_inplace) and walks the canonical blocks; per block it loads the (up to
+// six) orbit tiles once and writes 2 x 6 tiles per ordering through one staging buffer, so X
+// costs no read of U: at an odd nvir the two passes read U with 8-byte copies whose 64-byte tile
+// rows straddle sectors (1.9x the algorithmic DRAM reads under ncu).
+__global__ void __launch_bounds__(OT_THREADS, 2) k_unpack_p3(const double *t3, double *U, double *X, int64_t nblocks,
+                                                             int nocc, int nv, int ntile, P3Coef k) {
+    extern __shared__ double sm[];  // orbit tiles of C (6 x SLOT), staging of one output (6 x SLOT)
+    double *in = sm, *st = sm + 6 * SLOT;
+    __shared__ OrbitSet os;
+    int t0, t1, t2;
+    decode_tri3(blockIdx.x, ntile, t0, t1, t2);
+    build_orbit_set(os, t0, t1, t2);
+    const int64_t n3 = (int64_t)nv * nv * nv;
+    int goff[12];
+    unsigned short soff[12];
+    unsigned nload = 0;
+    for (int j = 0; j < 12; j++) {
+        const int sl = j >> 1, e = threadIdx.x + OT_THREADS * (j & 1);
+        goff[j] = -1;
+        soff[j] = 0;
+        if (sl >= os.nslot) continue;
+        const int x = e >> 6, y = (e >> 3) & 7, z = e & 7;
+        const int gx = os.tile[sl][0] * TE + x, gy = os.tile[sl][1] * TE + y, gz = os.tile[sl][2] * TE + z;
+        if (gx >= nv || gy >= nv || gz >= nv) continue;
+        goff[j] = (gx * nv + gy) * nv + gz;
+        soff[j] = (unsigned short)(sl * SLOT + sidx(x, y, z));
+        nload |= 1u << j;
+    }
+    OrbitAddr oa[2];
+    int ocls[2];  // 0: none, 1: generic, 2: all indices equal
+    for (int h = 0; h < 2; h++) {
+        const int e = threadIdx.x + OT_THREADS * h;
+        const int x = e >> 6, y = (e >> 3) & 7, z = e & 7;
+        const int gx = t0 * TE + x, gy = t1 * TE + y, gz = t2 * TE + z;
+        ocls[h] = 0;
+        if (gx >= nv || gy >= nv || gz >= nv || (t0 == t1 && x > y) || (t1 == t2 && y > z)) continue;
+        const int *nb = os.nbr[0];
+        oa[h].a[0] = (unsigned short)(nb[0] * SLOT + sidx(x, y, z));
+        oa[h].a[1] = (unsigned short)(nb[1] * SLOT + sidx(x, z, y));
+        oa[h].a[2] = (unsigned short)(nb[2] * SLOT + sidx(y, x, z));
+        oa[h].a[3] = (unsigned short)(nb[3] * SLOT + sidx(y, z, x));
+        oa[h].a[4] = (unsigned short)(nb[4] * SLOT + sidx(z, x, y));
+        oa[h].a[5] = (unsigned short)(nb[5] * SLOT + sidx(z, y, x));
+        ocls[h] = (gx == gy && gy == gz) ? 2 : 1;
+    }
+    for (int64_t q = blockIdx.y; q < nblocks; q += gridDim.y) {
+        const double *blk = t3 + q * n3;
+#pragma unroll
+        for (int j = 0; j < 12; j++)
+            if (nload & (1u << j)) cp_async8(in + soff[j], blk + goff[j]);
+        cp_async_commit();
+        cp_async_wait<0>();
+        __syncthreads();  // the orbit tiles of C have landed
+        int o[3];
+        decode_tri3(q, nocc, o[0], o[1], o[2]);
+        for (int g = 0; g < 6; g++) {
+            const int xyz[3] = {o[perm3(g, 0)], o[perm3(g, 1)], o[perm3(g, 2)]};
+            bool dup = false;
+            for (int sp = 0; sp < g; sp++)
+                if (o[perm3(sp, 0)] == xyz[0] && o[perm3(sp, 1)] == xyz[1] && o[perm3(sp, 2)] == xyz[2]) dup = true;
+            if (dup) continue;  // uniform over the CTA
+            int64_t srt[3];
+            const int c = order_case3(xyz[0], xyz[1], xyz[2], srt);
+            const int pi = c == 3 ? 4 : (c == 4 ? 3 : c);  // the inverse permutation of case c
+            const int64_t out = ((int64_t)xyz[0] * nocc + xyz[1]) * nocc + xyz[2];
+            for (int pass = 0; pass < 2; pass++) {
+                double *dst = pass == 0 ? U : X;
+                if (dst == nullptr) continue;
+#pragma unroll
+                for (int h = 0; h < 2; h++) {
+                    if (!ocls[h]) continue;
+                    const bool diag = ocls[h] == 2, xp = pass == 1;
+                    switch (pi) {
+                    case 0: stage_orbit<0>(st, oa[h], in, k, diag, xp); break;
+                    case 1: stage_orbit<1>(st, oa[h], in, k, diag, xp); break;
+                    case 2: stage_orbit<2>(st, oa[h], in, k, diag, xp); break;
+                    case 3: stage_orbit<3>(st, oa[h], in, k, diag, xp); break;
+                    case 4: stage_orbit<4>(st, oa[h], in, k, diag, xp); break;
+                    default: stage_orbit<5>(st, oa[h], in, k, diag, xp); break;
+                    }
+                }
+                __syncthreads();  // the staged tiles are complete
+                double *ob = dst + out * n3;
+#pragma unroll
+                for (int j = 0; j < 12; j++)
+                    if (nload & (1u << j)) ob[goff[j]] = st[soff[j]];
+                __syncthreads();  // the staging buffer is free again
+            }
+        }
+    }
+}
+
+}  // namespace dcc
+
+extern "C" int dcc_t3_unpack_p3(const double *t3, double *U, double *X, int64_t nocc, int64_t nvir,
+                                const char *pattern, double alpha, double beta, void *stream) {
+    clear_error();
+    P3Coef k;
+    int rc = p3_coef(pattern, alpha, beta, k);
+    if (rc) return rc;
+    DCC_REQUIRE(nocc >= 0 && nvir >= 0, DCC_ERR_SHAPE, "negative size");
+    if (nocc == 0 || nvir == 0) return DCC_OK;
+    DCC_REQUIRE(t3 && X, DCC_ERR_NULL, "NULL buffer");
+    DCC_REQUIRE(nvir <= 1290 && nocc < 1290, DCC_ERR_UNSUPPORTED, "nvir > 1290 exceeds 32-bit block offsets");
+    const int64_t n3 = nvir * nvir * nvir * (int64_t)sizeof(double);
+    const int64_t nblocks = nocc * (nocc + 1) * (nocc + 2) / 6, nu = nocc * nocc * nocc;
+    auto apart = [](const void *a, int64_t na, const void *b, int64_t nb) {
+        return (const char *)a + na <= (const char *)b || (const char *)b + nb <= (const char *)a;
+    };
+    DCC_REQUIRE(apart(t3, nblocks * n3, X, nu * n3) && (!U || (apart(t3, nblocks * n3, U, nu * n3) &&
+                                                            apart(U, nu * n3, X, nu * n3))),
+                DCC_ERR_SHAPE, "t3, U and X overlap");
+    const int ntile = (int)ceil_div(nvir, TE);
+    const int64_t ntri = (int64_t)ntile * (ntile + 1) * (ntile + 2) / 6;
+    int64_t gy = (148 * 4 * 8 + ntri - 1) / ntri;
+    gy = gy < 1 ? 1 : (gy > nblocks ? nblocks : gy);
+    gy = gy > 65535 ? 65535 : gy;
+    const size_t smem = 2 * 6 * SLOT * sizeof(double);
+    cudaFuncSetAttribute(k_unpack_p3, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_unpack_p3<<<dim3((unsigned)ntri, (unsigned)gy), OT_THREADS, smem, as_stream(stream)>>>(
+        t3, U, X, nblocks, (int)nocc, (int)nvir, ntile, k);
+    return launch_status("t3_unpack_p3");
+}
+
 extern "C" int dcc_t3_single_spin_summation_inplace(double *A, int64_t nvir, const char *pattern, double alpha,
                                                     double beta, void *stream) {
     return dcc_t3_spin_summation_inplace(A, 1, nvir, pattern, alpha, beta, stream);

@@ -44,6 +44,23 @@ def t3_spin_summation(A, B, nblocks, nvir, pattern, alpha=1.0, beta=0.0):
     return B
 
 
+def t3_unpack_p3(t3, U, X, nocc, nvir, pattern="P3_201", alpha=1.0, beta=0.0):
+    """U[o] = the canonical T3 unpacked to every ordered (i,j,k) o, and X[o] = beta U[o] +
+    alpha P(U[o]), in one pass over the canonical blocks (U may be None: X alone)."""
+    n3 = nocc * (nocc + 1) * (nocc + 2) // 6
+    t3 = L.as_tensor(t3, f64, "t3")
+    X = L.as_tensor(X, f64, "X")
+    if t3.numel() != n3 * nvir ** 3 or X.numel() != nocc ** 3 * nvir ** 3:
+        raise ValueError("t3 must hold the canonical blocks and X every ordered block")
+    if U is not None:
+        U = L.as_tensor(U, f64, "U")
+        if U.numel() != X.numel():
+            raise ValueError("U must hold every ordered block")
+    L.call("dcc_t3_unpack_p3", L.ptr(t3), L.ptr(U), L.ptr(X), nocc, nvir, L.pattern(pattern), float(alpha),
+           float(beta), L.stream_ptr())
+    return U, X
+
+
 def symmetrize_status():
     """Status word of the bounded waits in the TMA spin-summation kernel on the current
     device (0, or DCC_ERR_TIMEOUT once a wait gave up); reading clears it and

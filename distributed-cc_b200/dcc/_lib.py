@@ -52,6 +52,7 @@ _lib.dcc_version.argtypes = []
 _SIGS = {
     "dcc_t3_single_spin_summation_inplace": [c_vp, c_i64, c_str, c_dbl, c_dbl, c_vp],
     "dcc_t3_spin_summation_inplace": [c_vp, c_i64, c_i64, c_str, c_dbl, c_dbl, c_vp],
+    "dcc_t3_unpack_p3": [c_vp, c_vp, c_vp, c_i64, c_i64, c_str, c_dbl, c_dbl, c_vp],
     "dcc_t3_spin_summation": [c_vp, c_vp, c_i64, c_i64, c_str, c_dbl, c_dbl, c_vp],
     "dcc_t3_spin_summation_triple_sym": [c_vp, c_vp, c_vp, c_vp, c_i64, c_i64, c_vp],
     "dcc_t3_transpose_add": [c_vp, c_vp, c_i64, c_i64, c_vp],

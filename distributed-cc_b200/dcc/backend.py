@@ -103,38 +103,82 @@ class _Transfer:
 TRANSFER = _Transfer()
 
 
+class _Staging:
+    """Page-locked host buffers for the uploads of the drop-in routes.  A numpy array (any
+    positive strides, e.g. a slice of the dressed ERIs) is gathered into a pinned buffer by
+    torch's multi-threaded CPU copy and reaches the device by an asynchronous copy at the
+    link's speed; a buffer is reused once the copy that last read it has completed.  Arrays
+    above `limit` bytes (the one-time upload of T3) go through the pageable path."""
+
+    limit = 1 << 30
+
+    def __init__(self):
+        self.bufs = []  # [pinned uint8 tensor, event of its last copy or None]
+
+    def _buffer(self, nbytes):
+        for b in self.bufs:
+            if b[0].numel() >= nbytes and (b[1] is None or b[1].query()):
+                return b
+        b = [torch.empty(max(nbytes, 1 << 20), dtype=torch.uint8, pin_memory=True), None]
+        self.bufs.append(b)
+        return b
+
+    def upload(self, a, device, stream=None):
+        out = torch.empty(a.shape, dtype=f64, device=device)
+        if out.device.type != "cuda":
+            return out.copy_(torch.from_numpy(np.ascontiguousarray(a)))
+        if a.nbytes > self.limit or a.size == 0 or any(st < 0 for st in a.strides):
+            src = torch.from_numpy(np.ascontiguousarray(a))
+            if stream is None:
+                out.copy_(src)
+            else:
+                with torch.cuda.stream(stream):
+                    out.copy_(src, non_blocking=True)
+            return out
+        b = self._buffer(a.nbytes)
+        host = b[0][:a.nbytes].view(f64).view(a.shape)
+        host.copy_(torch.from_numpy(a))
+        s = stream if stream is not None else torch.cuda.current_stream(out.device)
+        with torch.cuda.stream(s):
+            out.copy_(host, non_blocking=True)
+            b[1] = torch.cuda.Event()
+            b[1].record(s)
+        return out
+
+
+_STAGING = _Staging()
+
+
 def _dev(a, device):
     if isinstance(a, DeviceT3Local):
         return a.tensor
     if isinstance(a, torch.Tensor):
         return a.to(device=device, dtype=f64)
-    a = np.ascontiguousarray(a, dtype=np.float64)
+    a = np.asarray(a, dtype=np.float64)
     TRANSFER.h2d += a.nbytes
-    return torch.as_tensor(a, device=device)
+    return _STAGING.upload(a, device)
 
 
 def _dev_async(a, device, state):
     """A numpy array copied to the device on a side stream (counted in TRANSFER): returns the
-    device tensor and leaves in state the event that marks its arrival.  From pageable host
-    memory the call returns once the bytes are staged, while kernels already enqueued on the
-    compute stream keep running."""
+    device tensor and leaves in state the event that marks its arrival.  The call returns once
+    the bytes are in page-locked memory, while kernels already enqueued on the compute stream
+    keep running."""
     if isinstance(a, (torch.Tensor, DeviceT3Local)):
         t = _dev(a, device)
         ev = torch.cuda.Event()
         ev.record()
         state["upload_ready"] = ev
         return t
-    a = np.ascontiguousarray(a, dtype=np.float64)
+    a = np.asarray(a, dtype=np.float64)
     TRANSFER.h2d += a.nbytes
     side = state.get("upload_stream")
     if side is None:
         side = state["upload_stream"] = torch.cuda.Stream(device=device)
-    out = torch.empty(a.shape, dtype=f64, device=device)
+    out = _STAGING.upload(a, device, stream=side)
     out.record_stream(side)
-    with torch.cuda.stream(side):
-        out.copy_(torch.from_numpy(a), non_blocking=True)
-        ev = torch.cuda.Event()
-        ev.record(side)
+    ev = torch.cuda.Event()
+    ev.record(side)
     state["upload_ready"] = ev
     return out
 

@@ -58,12 +58,19 @@ def r1_add_t3_(r1, t1_eris, t3, ijk, nocc, oovv=None, V=None):
     return r1
 
 
-def p3_201_all(t3, nocc, U=None, out=None):
+def p3_201_all(t3, nocc, U=None, out=None, unpack_into=None):
     """X = P3_201 of every ordered block of the unpacked T3 [x][y][z][a][b][c].
 
     U: the unpacked T3 when the caller has it already (unpacked here otherwise);
-    out: a buffer of U's size to hold X (a fresh one otherwise)."""
+    out: a buffer of U's size to hold X (a fresh one otherwise); unpack_into: a buffer that
+    receives the unpacked T3 in the same pass that writes X (one launch, dcc_t3_unpack_p3: X
+    costs no read of U; used where the rows are not 16-byte aligned and the separate passes
+    cannot use TMA)."""
     nvir = t3.shape[1]
+    if unpack_into is not None:
+        X = torch.empty_like(unpack_into) if out is None else out.view(unpack_into.shape)
+        _c_rccsdt.t3_unpack_p3(t3, unpack_into, X, nocc, nvir, "P3_201", 1.0, 0.0)
+        return X.view(nocc, nocc, nocc, nvir, nvir, nvir)
     if U is None:
         U = torch.empty((nocc ** 3, nvir, nvir, nvir), dtype=f64, device=t3.device)
         unpack_all_(t3, U, nocc, nvir)

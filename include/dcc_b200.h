@@ -65,6 +65,16 @@ DCC_API int dcc_t3_single_spin_summation_inplace(double *A, int64_t nvir, const 
 DCC_API int dcc_t3_spin_summation_inplace(double *A, int64_t nblocks, int64_t nvir, const char *pattern, double alpha,
                                   double beta, void *stream);
 
+/* U[o] = the canonical T3 (t3, [n3][nvir]^3, i<=j<=k blocks in lexicographic order) unpacked to
+ * every ordered (i,j,k) o (U: [nocc^3][nvir]^3, o = (i*nocc+j)*nocc+k, as dcc_t3_unpack_all) and
+ * X[o] = beta*U[o] + alpha*P(U[o]) (the P3 pattern of dcc_t3_spin_summation, bit-identical to it
+ * applied to U), in one pass over the canonical blocks; U may be NULL (X alone).  The
+ * take_t3_single_local + t3_single_spin_summation_inplace_(.., "P3_201") of every ordering that
+ * r1r2_add_t3_tri_ / intermediates_t3_add_t3_tri make per block (distr_cc/rccsdt.py:308-309,
+ * 351-352), for all blocks at once.  t3, U and X must not overlap. */
+DCC_API int dcc_t3_unpack_p3(const double *t3, double *U, double *X, int64_t nocc, int64_t nvir, const char *pattern,
+                             double alpha, double beta, void *stream);
+
 /* B = beta*A + alpha*P(A) block by block, out of place (A and B do not overlap, or
  * B == A for the in-place form above); same patterns and arithmetic.  The
  * out-of-place t3_spin_summation of PySCF's rccsdt_highm as the reference calls it

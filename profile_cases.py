@@ -11,7 +11,7 @@
     python profile_cases.py qgroup [--reps 3]
     python profile_cases.py t3half [--reps 3] [--nocc 15 --nvir 93] [--kind bf16x3|fp64] [--breakdown]
     python profile_cases.py t4     [--reps 3] [--kind bf16x3|fp64] [--breakdown]
-    python profile_cases.py oddnv  [--reps 3] [--nocc 5 --nvir 93] [--time]
+    python profile_cases.py oddnv  [--reps 3] [--nocc 5 --nvir 93] [--time] [--passes 0,1,...]
 
 Each case builds its inputs once and launches the kernel `reps` times, so a
 profiler can skip the warm-up launches and capture the last one.  Sizes are
@@ -151,19 +151,22 @@ def case_unpack(reps, nocc=10):
     torch.cuda.synchronize()
 
 
-def case_oddnv(reps, nocc=5, nvir=93, time=False):
+def case_oddnv(reps, nocc=5, nvir=93, time=False, only=None):
     """The memory-bound T3 passes of one half-iteration at an odd nvir (no TMA: 8-byte row
     pitch), each on its own buffers: unpack t3 -> U (every ordering), X = P3_201(U) out of
-    place, P3_422(t3) out of place, P3_full(r3) in place, the S3 gather S -> r3.  With time=True
+    place, P3_422(t3) out of place, P3_full(r3) in place, the S3 gather S -> r3, and (5) the
+    unpack and X in one pass (dcc_t3_unpack_p3).  With time=True
     each pass is timed with CUDA events (after a 256 MB L2 flush; mean of reps) and printed with
-    its algorithmic bytes and bandwidth."""
+    its algorithmic bytes and bandwidth.  only: the passes to run (indices into the list
+    above, e.g. [1] for the X pass alone; buffers of the others are not allocated)."""
     from dcc import synthetic, t3_residual, _c_rccsdt
     d = synthetic.make_inputs(nocc, nvir, seed=0)
     n3, nu = d.t3.shape[0], nocc ** 3
-    U = torch.empty((nu, nvir, nvir, nvir), dtype=torch.float64, device="cuda")
-    X = torch.empty_like(U)
-    V = torch.empty_like(d.t3)
-    r3 = torch.randn_like(d.t3)
+    only = set(range(6)) if only is None else set(only)
+    U = torch.empty((nu, nvir, nvir, nvir), dtype=torch.float64, device="cuda") if only & {0, 1, 4, 5} else None
+    X = torch.empty_like(U) if only & {1, 4, 5} else None
+    V = torch.empty_like(d.t3) if 2 in only else None
+    r3 = torch.randn_like(d.t3) if only & {3, 4} else None
     e3, eu = n3 * nvir ** 3, nu * nvir ** 3
     passes = [
         ("unpack t3->U", lambda: t3_residual.unpack_all_(d.t3, U, nocc, nvir), 8 * (e3 + eu)),
@@ -174,9 +177,12 @@ def case_oddnv(reps, nocc=5, nvir=93, time=False):
         ("gather S->r3", lambda: t3_residual.perm_gather_(
             r3, d.ijk, nvir, 0.0, [(X, 1.0, t3_residual.full_strides(nocc, nvir), t3_residual.ALL_S3)], nocc=nocc),
          8 * (6 * e3 + e3)),
+        ("unpack+X one pass", lambda: _c_rccsdt.t3_unpack_p3(d.t3, U, X, nocc, nvir, "P3_201"), 8 * (e3 + 2 * eu)),
     ]
     flush = torch.empty(256 << 20, dtype=torch.int8, device="cuda") if time else None
-    for name, run, nbytes in passes:
+    for n, (name, run, nbytes) in enumerate(passes):
+        if n not in only:
+            continue
         ts = []
         for r in range(reps):
             if time:
@@ -357,6 +363,7 @@ def main():
     ap.add_argument("--time", action="store_true", help="p3 case: print CUDA-event timings")
     ap.add_argument("--dchunk", type=int, default=None, help="qsample case: d-chunk of the split path")
     ap.add_argument("--breakdown", action="store_true", help="t3half / t4 case: per-kernel device times")
+    ap.add_argument("--passes", default=None, help="oddnv case: comma-separated pass indices (default all)")
     a = ap.parse_args()
     if a.case == "gemm":
         case_gemm(a.kind, a.reps, a.nocc or 10, a.nvir)
@@ -369,7 +376,8 @@ def main():
     elif a.case == "t3iter":
         case_t3iter(a.reps, a.nocc or 10, a.nvir, a.kind)
     elif a.case == "oddnv":
-        case_oddnv(a.reps, a.nocc or 5, a.nvir if a.nvir != 90 else 93, a.time)
+        case_oddnv(a.reps, a.nocc or 5, a.nvir if a.nvir != 90 else 93, a.time,
+                   [int(x) for x in a.passes.split(",")] if a.passes else None)
     elif a.case == "t3half":
         case_t3half(a.reps, a.nocc or 15, a.nvir if a.nvir != 90 else 93, a.kind, a.breakdown)
     elif a.case == "qsample":

@@ -75,6 +75,36 @@ def test_t3_spin_sum_out_of_place(C, oracle, nvir, pattern):
     assert c3.symmetrize_status() == 0
 
 
+@pytest.mark.parametrize("nocc,nvir", [(1, 5), (2, 1), (3, 8), (4, 13), (3, 17), (2, 93)])
+@pytest.mark.parametrize("pattern", P3)
+def test_t3_unpack_p3(C, oracle, nocc, nvir, pattern):
+    """U and X = beta U + alpha P(U) of every ordering in one pass (dcc_t3_unpack_p3): U equal to
+    the unpack of every ordering, X bit-exact with the oracle's P3 over it (the same values as a
+    P3 pass over U), with and without U, t3 untouched."""
+    from dcc import t3_residual
+    c3 = C[0]
+    rng = np.random.default_rng(7 * nocc + nvir)
+    trip = [(i, j, k) for i in range(nocc) for j in range(i, nocc) for k in range(j, nocc)]
+    full = rng.standard_normal((nocc,) * 3 + (nvir,) * 3)
+    import itertools
+    full = sum(full.transpose(p + tuple(3 + x for x in p)) for p in itertools.permutations(range(3))) / 6
+    t3 = np.stack([full[i, j, k] for i, j, k in trip])
+    d = dev(t3)
+    Uw = torch.empty((nocc ** 3,) + (nvir,) * 3, dtype=torch.float64, device="cuda")
+    t3_residual.unpack_all_(d, Uw, nocc, nvir)
+    for alpha, beta in [(1.0, 0.0), (-1.0 / 6.0, 1.0)]:
+        want = oracle.t3_spin_sum(host(Uw).copy(), nvir, pattern, alpha, beta)
+        U = torch.full_like(Uw, float("nan"))
+        X = torch.full_like(Uw, float("nan"))
+        c3.t3_unpack_p3(d, U, X, nocc, nvir, pattern, alpha, beta)
+        assert torch.equal(U, Uw)
+        assert np.array_equal(host(X), want)
+        X2 = torch.full_like(Uw, float("nan"))
+        c3.t3_unpack_p3(d, None, X2, nocc, nvir, pattern, alpha, beta)
+        assert torch.equal(X2, X)
+    assert np.array_equal(host(d), t3)
+
+
 @pytest.mark.parametrize("nvir", [2, 10, 30, 90])
 def test_orbit_roundtrip_is_identity(C, nvir):
     """The diagnostic tile round trip of the spin-summation kernel leaves every block unchanged."""
