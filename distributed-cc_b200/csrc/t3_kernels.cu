@@ -1095,6 +1095,96 @@ extern "C" int dcc_t3_spin_summation_inplace(double *A, int64_t nblocks, int64_t
     return orbit3_launch(0, A, A, nullptr, nullptr, nblocks, nvir, k, stream);
 }
 
+namespace dcc {
+
+// Out-of-place P3 for the patterns whose p4 is 0 (P3_201: B = beta A + alpha p3 (p0 A + p1 A^cba
+// + p2 A^bac)) by row pairs, for rows that are not 16-byte aligned.  Of the three terms of
+// B[a,b,:], A[a,b,:] and A[b,a,:] are whole rows (read once for the two output rows (a,b) and
+// (b,a)) and A[:,b,a] is a column; a work item is a block and a pair of 8-wide index tiles
+// (I <= J): the CTA stages the two column tiles A[c][J..][I..] and A[c][I..][J..] for every c in
+// shared memory (8-byte copies of 64-byte segments, row pitch 65 doubles so the transposed reads
+// are conflict-free), then each warp streams row pairs: coalesced loads of the two rows and
+// coalesced stores of the two output rows, whole rows of nvir elements.  Writes therefore cover
+// runs of rows instead of the 64-byte tile rows of the orbit kernel, whose partial sectors cost
+// DRAM reads at an odd nvir.  The arithmetic is the orbit kernel's with its p4 term (0 x the
+// second half) left out: equal results up to the sign of a zero.
+constexpr int PB_PITCH = 65;  // doubles per (c) row of a staged column tile: 8 x 8 + 1
+
+__global__ void __launch_bounds__(256, 2) k_p3_band3(const double *__restrict__ A, double *__restrict__ B,
+                                                     int64_t nblocks, int nv, int ntile, P3Coef k) {
+    extern __shared__ double pb_sm[];  // T1[c][r][s] = A[c][J*8+r][I*8+s], then T2 = A[c][I*8+r][J*8+s]
+    double *T1 = pb_sm, *T2 = pb_sm + (size_t)nv * PB_PITCH;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int64_t n3 = (int64_t)nv * nv * nv, nv2 = (int64_t)nv * nv;
+    const int64_t npair = (int64_t)ntile * (ntile + 1) / 2, nwork = nblocks * npair;
+    for (int64_t w = blockIdx.x; w < nwork; w += gridDim.x) {
+        const int64_t b = w / npair;
+        int r = (int)(w % npair), I = 0;
+        while (r >= ntile - I) {  // (I, J) with I <= J, J fastest
+            r -= ntile - I;
+            I++;
+        }
+        const int J = I + r;
+        const double *Ab = A + b * n3;
+        double *Bb = B + b * n3;
+        const int i0 = I * TE, j0 = J * TE;
+        // the column tiles (the second only when I != J: for I == J it equals the first)
+        for (int e = threadIdx.x; e < nv * 64; e += blockDim.x) {
+            const int c = e >> 6, rr = (e >> 3) & 7, ss = e & 7;
+            if (j0 + rr < nv && i0 + ss < nv) cp_async8(T1 + c * PB_PITCH + rr * 8 + ss, Ab + c * nv2 + (int64_t)(j0 + rr) * nv + i0 + ss);
+            if (I != J && i0 + rr < nv && j0 + ss < nv)
+                cp_async8(T2 + c * PB_PITCH + rr * 8 + ss, Ab + c * nv2 + (int64_t)(i0 + rr) * nv + j0 + ss);
+        }
+        cp_async_commit();
+        cp_async_wait<0>();
+        __syncthreads();
+        const double *T2r = I == J ? T1 : T2;
+        // row pairs (a, b) = (i0 + s, j0 + q) with the output rows B[a,b,:] and B[b,a,:];
+        // on the diagonal tile pairs with s <= q only (s == q: one row)
+        for (int pr = warp; pr < 64; pr += 8) {
+            const int s_ = pr & 7, q_ = pr >> 3;
+            if (I == J && s_ > q_) continue;
+            const int a = i0 + s_, bb = j0 + q_;
+            if (a >= nv || bb >= nv) continue;
+            const double *rab = Ab + (int64_t)a * nv2 + (int64_t)bb * nv;   // A[a,b,:]
+            const double *rba = Ab + (int64_t)bb * nv2 + (int64_t)a * nv;   // A[b,a,:]
+            double *oab = Bb + (int64_t)a * nv2 + (int64_t)bb * nv;
+            double *oba = Bb + (int64_t)bb * nv2 + (int64_t)a * nv;
+            const bool two = a != bb;
+            for (int c = lane; c < nv; c += 32) {
+                const double vab = __ldg(rab + c), vba = __ldg(rba + c);
+                // B[a,b,c]: A[c,b,a] = T1[c][q][s];  B[b,a,c]: A[c,a,b] = T2[c][s][q]
+                const double cba = T1[c * PB_PITCH + q_ * 8 + s_];
+                const double tu = dadd(dadd(dmul(k.p0, vab), dmul(k.p1, cba)), dmul(k.p2, vba));
+                oab[c] = dadd(dmul(k.beta, vab), dmul(k.alpha, dmul(k.p3, tu)));
+                if (two) {
+                    const double cab = T2r[c * PB_PITCH + s_ * 8 + q_];
+                    const double tu2 = dadd(dadd(dmul(k.p0, vba), dmul(k.p1, cab)), dmul(k.p2, vab));
+                    oba[c] = dadd(dmul(k.beta, vba), dmul(k.alpha, dmul(k.p3, tu2)));
+                }
+            }
+        }
+        __syncthreads();  // the column tiles are refilled by the next item
+    }
+}
+
+}  // namespace dcc
+
+// The row-pair kernel for out-of-place P3 with p4 == 0 at a row pitch TMA cannot describe;
+// returns DCC_ERR_UNSUPPORTED (nothing launched) where it does not apply.
+static int p3_band3_launch(const double *A, double *B, int64_t nblocks, int64_t nvir, const P3Coef &k, void *stream) {
+    if (k.p4 != 0.0 || A == B || nvir < 1 || nvir > 104 || nvir % 2 == 0) return DCC_ERR_UNSUPPORTED;
+    const int ntile = (int)ceil_div(nvir, TE);
+    const size_t smem = 2 * (size_t)nvir * PB_PITCH * sizeof(double);
+    int dev = 0, nsm = 148;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    const int64_t nwork = nblocks * (int64_t)ntile * (ntile + 1) / 2, cap = (int64_t)nsm * 2;
+    const unsigned grid = (unsigned)(nwork < cap ? nwork : cap);
+    cudaFuncSetAttribute(k_p3_band3, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_p3_band3<<<grid, 256, smem, as_stream(stream)>>>(A, B, nblocks, (int)nvir, ntile, k);
+    return DCC_OK;
+}
+
 extern "C" int dcc_t3_spin_summation(const double *A, double *B, int64_t nblocks, int64_t nvir, const char *pattern,
                                      double alpha, double beta, void *stream) {
     clear_error();
@@ -1106,6 +1196,7 @@ extern "C" int dcc_t3_spin_summation(const double *A, double *B, int64_t nblocks
     const int64_t bytes = nblocks * nvir * nvir * nvir * (int64_t)sizeof(double);
     DCC_REQUIRE(A == B || (const char *)B + bytes <= (const char *)A || (const char *)A + bytes <= (const char *)B,
                 DCC_ERR_SHAPE, "A and B overlap");
+    if (nblocks > 0 && p3_band3_launch(A, B, nblocks, nvir, k, stream) == DCC_OK) return launch_status("P3 by row pairs");
     return orbit3_launch(0, A, B, nullptr, nullptr, nblocks, nvir, k, stream);
 }
 
