@@ -48,7 +48,7 @@ __device__ __forceinline__ int t4s_ostride(int x, int nv) {  // accumulator stri
     return x == 0 ? nv * nv * nv : (x == 1 ? nv * nv : (x == 2 ? nv : 1));
 }
 
-__global__ void __launch_bounds__(T4S_THREADS, 3)
+__global__ void __launch_bounds__(T4S_THREADS, 2)
     k_t4_strings(T4StrOps ops, const int64_t *__restrict__ desc, int nstr, const int32_t *__restrict__ quads,
                  const int32_t *__restrict__ pair_off, const int32_t *__restrict__ pair_sm, int ngroups, int npairs,
                  int nocc, int nv, int na_step, int nsplit, double beta, double *__restrict__ r4, int *status) {
@@ -71,99 +71,71 @@ __global__ void __launch_bounds__(T4S_THREADS, 3)
         if (threadIdx.x == 0) atomicOr(status, 1);
         return;
     }
-    // one string's parameters, parsed and checked by thread 0 for the whole CTA
-    struct StrSm {
-        const double *W, *T;
-        int64_t wm, tq, wlim, tlim;  // pair strides; the operand sizes left above the base maxima
-        double alpha;
-        int ok, mode, K0, K1, wk0, tk0, wk1, tk1, R, C;
-        int rext[4], cext[4], rws[4], cts[4], ros[4], cos_[4];
-    };
-    __shared__ StrSm sp;
     for (int s = 0; s < nstr; ++s) {
-        __syncthreads();  // the previous string's tiles are in acc; sp is free
-        if (threadIdx.x == 0) {
-            const int64_t *d = desc + (int64_t)s * T4S_DESC;
-            const int64_t wop = d[0], top = d[1], mask = d[20], K0 = d[21], wk0 = d[22], tk0 = d[23], K1 = d[24],
-                          wk1 = d[25], tk1 = d[26], rord = d[28], cord = d[29], wm = d[30], mode = d[31];
-            bool ok = wop >= 0 && wop < ops.nops && top >= 0 && top < ops.nops && mask >= 0 && mask < 16 &&
-                      K0 >= 1 && K1 >= 1 && wk0 >= 0 && tk0 >= 0 && wk1 >= 0 && tk1 >= 0 && d[10] >= 0 &&
-                      d[11] >= 0 && rord >= 0 && rord < 65536 && cord >= 0 && cord < 65536 && wm >= 0 &&
-                      mode >= 0 && mode <= ngroups;
-            int64_t wb = 0, tb = 0, wmax = 0, tmax = 0;
-            int seen_r = 0, seen_c = 0, npos_r = 0, npos_c = 0;
-            for (int x = 0; x < 4; ++x) {
-                const int64_t ws = d[2 + x], ts = d[6 + x], wv = d[12 + x], tv = d[16 + x];
-                const bool inw = (mask >> x) & 1;
-                ok = ok && ws >= 0 && ts >= 0 && wv >= 0 && tv >= 0 && (inw ? tv == 0 : wv == 0);
-                wb += ws * occ[x];
-                tb += ts * occ[x];
-                const int ex = x == 0 ? na : nv;
-                wmax += wv * (ex - 1);
-                tmax += tv * (ex - 1);
-                const int xr = (int)((rord >> (4 * x)) & 15) - 1, xc = (int)((cord >> (4 * x)) & 15) - 1;
-                if (xr >= 0) {
-                    npos_r++;
-                    seen_r |= 1 << (xr & 7);
-                    ok = ok && xr < 4;
-                }
-                if (xc >= 0) {
-                    npos_c++;
-                    seen_c |= 1 << (xc & 7);
-                    ok = ok && xc < 4;
-                }
+        __syncthreads();  // the previous string's tiles are in acc
+        const int64_t *d = desc + (int64_t)s * T4S_DESC;
+        const int64_t wop = d[0], top = d[1], mask = d[20], K0 = d[21], wk0 = d[22], tk0 = d[23], K1 = d[24],
+                      wk1 = d[25], tk1 = d[26], rord = d[28], cord = d[29], wm = d[30], mode = d[31];
+        const double alpha = __longlong_as_double((long long)d[27]);
+        // ---- checks (uniform: every thread reads the same descriptor)
+        bool ok = wop >= 0 && wop < ops.nops && top >= 0 && top < ops.nops && mask >= 0 && mask < 16 && K0 >= 1 &&
+                  K1 >= 1 && wk0 >= 0 && tk0 >= 0 && wk1 >= 0 && tk1 >= 0 && d[10] >= 0 && d[11] >= 0 &&
+                  rord >= 0 && rord < 65536 && cord >= 0 && cord < 65536 && wm >= 0 && mode >= 0 && mode <= ngroups;
+        int64_t wb = 0, tb = 0, wmax = 0, tmax = 0;
+        int seen_r = 0, seen_c = 0, npos_r = 0, npos_c = 0;
+#pragma unroll
+        for (int x = 0; x < 4; ++x) {
+            const int64_t ws = d[2 + x], ts = d[6 + x], wv = d[12 + x], tv = d[16 + x];
+            const bool inw = (mask >> x) & 1;
+            ok = ok && ws >= 0 && ts >= 0 && wv >= 0 && tv >= 0 && (inw ? tv == 0 : wv == 0);
+            wb += ws * occ[x];
+            tb += ts * occ[x];
+            const int ex = x == 0 ? na : nv;
+            wmax += wv * (ex - 1);
+            tmax += tv * (ex - 1);
+            const int xr = (int)((rord >> (4 * x)) & 15) - 1, xc = (int)((cord >> (4 * x)) & 15) - 1;
+            if (xr >= 0) {
+                npos_r++;
+                seen_r |= 1 << (xr & 7);
+                ok = ok && xr < 4;
             }
-            // the row order lists the letters of W once each, the column order those of T
-            ok = ok && seen_r == (int)mask && seen_c == (int)(15 & ~mask) && npos_r == __popc(seen_r) &&
-                 npos_c == __popc(seen_c);
-            if (ok) {
-                wb += d[10] * q + d[12] * a0;
-                tb += (mode == 0 ? d[11] * q : 0) + d[16] * a0;  // pair mode: field 11 strides the source block
-                wmax += wb + wk0 * (K0 - 1) + wk1 * (K1 - 1);
-                tmax += tb + tk0 * (K0 - 1) + tk1 * (K1 - 1);
-                ok = wmax < ops.n[wop] && tmax < ops.n[top];
-            }
-            sp.ok = ok;
-            if (!ok) {
-                atomicOr(status, 2);
-            } else {
-                // the string as a GEMM: rows = W's output letters in the row order (the last
-                // position fastest), columns = T's in the column order
-                int R = 1, C = 1;
-                for (int p = 0; p < 4; ++p) {
-                    const int xr = (int)((rord >> (4 * p)) & 15) - 1, xc = (int)((cord >> (4 * p)) & 15) - 1;
-                    sp.rext[p] = xr < 0 ? 1 : (xr == 0 ? na : nv);
-                    sp.rws[p] = xr < 0 ? 0 : (int)d[12 + xr];
-                    sp.ros[p] = xr < 0 ? 0 : t4s_ostride(xr, nv);
-                    sp.cext[p] = xc < 0 ? 1 : (xc == 0 ? na : nv);
-                    sp.cts[p] = xc < 0 ? 0 : (int)d[16 + xc];
-                    sp.cos_[p] = xc < 0 ? 0 : t4s_ostride(xc, nv);
-                    R *= sp.rext[p];
-                    C *= sp.cext[p];
-                }
-                sp.R = R;
-                sp.C = C;
-                sp.W = ops.p[wop] + wb;
-                sp.T = ops.p[top] + tb;
-                sp.wm = wm;
-                sp.tq = d[11];
-                sp.wlim = ops.n[wop] - wmax;  // a pair may move W's base by less than this
-                sp.tlim = ops.n[top] - tmax;
-                sp.alpha = __longlong_as_double((long long)d[27]);
-                sp.mode = (int)mode;
-                sp.K0 = (int)K0;
-                sp.K1 = (int)K1;
-                sp.wk0 = (int)wk0;
-                sp.tk0 = (int)tk0;
-                sp.wk1 = (int)wk1;
-                sp.tk1 = (int)tk1;
+            if (xc >= 0) {
+                npos_c++;
+                seen_c |= 1 << (xc & 7);
+                ok = ok && xc < 4;
             }
         }
-        __syncthreads();
-        if (!sp.ok) continue;  // uniform
-        const int R = sp.R, C = sp.C, mode = sp.mode;
-        const double alpha = sp.alpha;
-        const int wk0i = sp.wk0, tk0i = sp.tk0, wk1i = sp.wk1, tk1i = sp.tk1, K0i = sp.K0, K1i = sp.K1;
+        // the row order lists the letters of W once each, the column order those of T
+        ok = ok && seen_r == (int)mask && seen_c == (int)(15 & ~mask) && npos_r == __popc(seen_r) &&
+             npos_c == __popc(seen_c);
+        if (ok) {
+            wb += d[10] * q + d[12] * a0;
+            tb += (mode == 0 ? d[11] * q : 0) + d[16] * a0;  // pair mode: field 11 strides the source block
+            wmax += wb + wk0 * (K0 - 1) + wk1 * (K1 - 1);
+            tmax += tb + tk0 * (K0 - 1) + tk1 * (K1 - 1);
+            ok = wmax < ops.n[wop] && tmax < ops.n[top];
+        }
+        if (!ok) {
+            if (threadIdx.x == 0) atomicOr(status, 2);
+            continue;
+        }
+        // ---- the string as a GEMM: rows = W's output letters in the row order (the last
+        // position fastest), columns = T's in the column order
+        int rext[4], cext[4], rws[4], cts[4], ros[4], cos_[4];
+        int R = 1, C = 1;
+#pragma unroll
+        for (int p = 0; p < 4; ++p) {
+            const int xr = (int)((rord >> (4 * p)) & 15) - 1, xc = (int)((cord >> (4 * p)) & 15) - 1;
+            rext[p] = xr < 0 ? 1 : (xr == 0 ? na : nv);
+            rws[p] = xr < 0 ? 0 : (int)d[12 + xr];
+            ros[p] = xr < 0 ? 0 : t4s_ostride(xr, nv);
+            cext[p] = xc < 0 ? 1 : (xc == 0 ? na : nv);
+            cts[p] = xc < 0 ? 0 : (int)d[16 + xc];
+            cos_[p] = xc < 0 ? 0 : t4s_ostride(xc, nv);
+            R *= rext[p];
+            C *= cext[p];
+        }
+        const int wk0i = (int)wk0, tk0i = (int)tk0, wk1i = (int)wk1, tk1i = (int)tk1, K0i = (int)K0, K1i = (int)K1;
         // a warp tile: Lr x Lc lanes, each lane 4 consecutive rows x 4 columns strided by Lc,
         // so a warp's loads of T cover Lc consecutive columns and its loads of W broadcast
         const int Lc = C > 64 ? 32 : (C > 32 ? 16 : (C > 16 ? 8 : (C > 8 ? 4 : (C > 4 ? 2 : 1))));
@@ -182,17 +154,19 @@ __global__ void __launch_bounds__(T4S_THREADS, 3)
             }
         }
         for (int pr = p0; pr < p1; ++pr) {
-        const double *W = sp.W, *T = sp.T;
+        int64_t wbp = wb, tbp = tb;
         if (mode > 0) {  // uniform: every thread reads the same pair
             const int src = pair_sm[2 * (int64_t)pr], m = pair_sm[2 * (int64_t)pr + 1];
-            const int64_t dw = sp.wm * m, dt = sp.tq * src;
-            if (src < 0 || m < 0 || m >= nocc || dw >= sp.wlim || dt >= sp.tlim) {
+            const int64_t dw = wm * m, dt = d[11] * src;
+            if (src < 0 || m < 0 || m >= nocc || wmax + dw >= ops.n[wop] || tmax + dt >= ops.n[top]) {
                 if (threadIdx.x == 0) atomicOr(status, 4);
                 continue;
             }
-            W += dw;
-            T += dt;
+            wbp += dw;
+            tbp += dt;
         }
+        const double *W = ops.p[wop] + wbp;
+        const double *T = ops.p[top] + tbp;
         for (int tile = warp; tile < nrt * nct; tile += T4S_THREADS / 32) {
             const int r0 = (tile / nct) * 4 * Lr + lr * 4, c0 = (tile % nct) * 4 * Lc + lc;
             int wo[4], to[4], oR[4], oC[4];
@@ -202,8 +176,8 @@ __global__ void __launch_bounds__(T4S_THREADS, 3)
                 int r = r0 < R ? r0 : 0;
 #pragma unroll
                 for (int p = 3; p >= 0; --p) {
-                    dg[p] = r % sp.rext[p];
-                    r /= sp.rext[p];
+                    dg[p] = r % rext[p];
+                    r /= rext[p];
                 }
             }
 #pragma unroll
@@ -212,8 +186,8 @@ __global__ void __launch_bounds__(T4S_THREADS, 3)
                 int o = 0, oa = 0;
 #pragma unroll
                 for (int p = 0; p < 4; ++p) {
-                    o += sp.rws[p] * dg[p];
-                    oa += sp.ros[p] * dg[p];
+                    o += rws[p] * dg[p];
+                    oa += ros[p] * dg[p];
                 }
                 wo[u] = rv[u] ? o : 0;
                 oR[u] = oa;
@@ -222,7 +196,7 @@ __global__ void __launch_bounds__(T4S_THREADS, 3)
                 for (int p = 3; p >= 0; --p) {
                     if (carry) {
                         dg[p] += 1;
-                        carry = dg[p] >= sp.rext[p];
+                        carry = dg[p] >= rext[p];
                         if (carry) dg[p] = 0;
                     }
                 }
@@ -233,10 +207,10 @@ __global__ void __launch_bounds__(T4S_THREADS, 3)
                 oa = 0;
 #pragma unroll
                 for (int p = 3; p >= 0; --p) {
-                    const int ix = c % sp.cext[p];
-                    c /= sp.cext[p];
-                    o += sp.cts[p] * ix;
-                    oa += sp.cos_[p] * ix;
+                    const int ix = c % cext[p];
+                    c /= cext[p];
+                    o += cts[p] * ix;
+                    oa += cos_[p] * ix;
                 }
                 to[u] = o;
                 oC[u] = oa;
