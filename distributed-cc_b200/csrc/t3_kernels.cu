@@ -2296,6 +2296,104 @@ static bool block_dims(const int64_t st[3], int64_t no, int64_t ext[2], int64_t 
 
 }  // namespace dcc
 
+namespace dcc {
+
+// The S3 gather of one full-layout source (every permutation, the residual's S) for rows that are
+// not 16-byte aligned, by rows: r3[q][a,b,c] = beta r3 + scale sum_p S[p(ijk)][p(abc)].  Of the six
+// terms of an output row (a,b,:), S[ijk][a,b,:] and S[jik][b,a,:] are whole rows; the other four
+// are columns (c in the middle or first position of the source) and come from four tiles staged
+// in shared memory for a pair of 8-wide index tiles (a in I, b in J) and a chunk of c.  Each warp
+// then streams output rows with coalesced loads and stores.  The slots are summed in the order of
+// the orbit-tile kernels (p = 0..5, one fma each), so the result is theirs bit for bit.
+constexpr int GB_PITCH = 65;
+
+__global__ void __launch_bounds__(256, 2) k_gather_band(const double *__restrict__ S, double *__restrict__ r3,
+                                                        const int32_t *__restrict__ ijk, int64_t nblocks, int nocc,
+                                                        int nv, int ntile, int cchunk, double scale, double beta) {
+    extern __shared__ double gb_sm[];  // tiles of the slots p = 1, 3, 4, 5: [cc][a_local * 8 + b_local]
+    double *T1 = gb_sm, *T3 = T1 + (size_t)cchunk * GB_PITCH, *T4 = T3 + (size_t)cchunk * GB_PITCH,
+           *T5 = T4 + (size_t)cchunk * GB_PITCH;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int64_t n3 = (int64_t)nv * nv * nv, nv2 = (int64_t)nv * nv;
+    const int nch = (nv + cchunk - 1) / cchunk;
+    const int64_t per_q = (int64_t)ntile * ntile * nch, nwork = nblocks * per_q;
+    for (int64_t w = blockIdx.x; w < nwork; w += gridDim.x) {
+        const int64_t q = w / per_q;
+        const int rem = (int)(w % per_q);
+        const int I = rem / (ntile * nch), J = (rem / nch) % ntile, ch = rem % nch;
+        const int c0 = ch * cchunk, cn = min(cchunk, nv - c0);
+        const int o[3] = {ijk[3 * q], ijk[3 * q + 1], ijk[3 * q + 2]};
+        const double *src[6];
+#pragma unroll
+        for (int p = 0; p < 6; p++)
+            src[p] = S + (((int64_t)o[perm3(p, 0)] * nocc + o[perm3(p, 1)]) * nocc + o[perm3(p, 2)]) * n3;
+        const int a0 = I * TE, b0 = J * TE;
+        for (int e = threadIdx.x; e < cn * 64; e += blockDim.x) {
+            const int cc = e >> 6, r = (e >> 3) & 7, t = e & 7, c = c0 + cc, off = cc * GB_PITCH;
+            if (a0 + r < nv && b0 + t < nv) {  // a = a0 + r, b = b0 + t: b contiguous
+                const int a = a0 + r, b = b0 + t;
+                cp_async8(T1 + off + r * 8 + t, src[1] + a * nv2 + (int64_t)c * nv + b);  // S1[a][c][b]
+                cp_async8(T4 + off + r * 8 + t, src[4] + c * nv2 + (int64_t)a * nv + b);  // S4[c][a][b]
+            }
+            if (b0 + r < nv && a0 + t < nv) {  // b = b0 + r, a = a0 + t: a contiguous
+                const int a = a0 + t, b = b0 + r;
+                cp_async8(T3 + off + t * 8 + r, src[3] + b * nv2 + (int64_t)c * nv + a);  // S3[b][c][a]
+                cp_async8(T5 + off + t * 8 + r, src[5] + c * nv2 + (int64_t)b * nv + a);  // S5[c][b][a]
+            }
+        }
+        cp_async_commit();
+        cp_async_wait<0>();
+        __syncthreads();
+        for (int rw = warp; rw < 64; rw += 8) {
+            const int al = rw >> 3, bl = rw & 7, a = a0 + al, b = b0 + bl;
+            if (a >= nv || b >= nv) continue;
+            const double *r0 = src[0] + a * nv2 + (int64_t)b * nv, *r2 = src[2] + b * nv2 + (int64_t)a * nv;
+            double *out = r3 + q * n3 + a * nv2 + (int64_t)b * nv;
+            const int ti = al * 8 + bl;
+            for (int cc = lane; cc < cn; cc += 32) {
+                const int c = c0 + cc, off = cc * GB_PITCH + ti;
+                double acc = fma(scale, __ldg(r0 + c), 0.0);
+                acc = fma(scale, T1[off], acc);
+                acc = fma(scale, __ldg(r2 + c), acc);
+                acc = fma(scale, T3[off], acc);
+                acc = fma(scale, T4[off], acc);
+                acc = fma(scale, T5[off], acc);
+                out[c] = beta == 0.0 ? acc : fma(beta, out[c], acc);
+            }
+        }
+        __syncthreads();  // the tiles are refilled by the next item
+    }
+}
+
+}  // namespace dcc
+
+// The row gather for one full-layout source with every permutation at an odd nvir; returns
+// DCC_ERR_UNSUPPORTED (nothing launched) where it does not apply.
+static int gather_band_launch(double *r3, const int32_t *ijk, int64_t nblocks, int64_t nocc, int64_t nvir, double beta,
+                              int nsrc, const double *const *bases, const double *scales, const int64_t *strides,
+                              const int *masks, void *stream) {
+    if (nsrc != 1 || masks[0] != 63 || nvir % 2 == 0 || nvir > 104 || nocc < 1 || nocc > 1290 || !bases[0])
+        return DCC_ERR_UNSUPPORTED;
+    const int64_t n3 = nvir * nvir * nvir;
+    const int64_t full[6] = {nocc * nocc * n3, nocc * n3, n3, nvir * nvir, nvir, 1};
+    for (int m = 0; m < 6; m++)
+        if (strides[m] != full[m]) return DCC_ERR_UNSUPPORTED;
+    const int64_t sbytes = nocc * nocc * nocc * n3 * (int64_t)sizeof(double), rbytes = nblocks * n3 * (int64_t)sizeof(double);
+    if (!((const char *)bases[0] + sbytes <= (const char *)r3 || (const char *)r3 + rbytes <= (const char *)bases[0]))
+        return DCC_ERR_UNSUPPORTED;
+    const int ntile = (int)ceil_div(nvir, TE);
+    const int cchunk = (int)((nvir + 1) / 2);  // two chunks of c: four tiles fit twice in an SM
+    const size_t smem = 4 * (size_t)cchunk * GB_PITCH * sizeof(double);
+    int dev = 0, nsm = 148;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    const int64_t nwork = nblocks * (int64_t)ntile * ntile * 2, cap = (int64_t)nsm * 2;
+    const unsigned grid = (unsigned)(nwork < cap ? nwork : cap);
+    cudaFuncSetAttribute(k_gather_band, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_gather_band<<<grid, 256, smem, as_stream(stream)>>>(bases[0], r3, ijk, nblocks, (int)nocc, (int)nvir, ntile,
+                                                          cchunk, scales[0], beta);
+    return DCC_OK;
+}
+
 extern "C" int dcc_t3_perm_gather_tma(double *r3, const int32_t *ijk, int64_t nblocks, int64_t nocc, int64_t nvir,
                                       double beta, int nsrc, const double *const *bases, const double *scales,
                                       const int64_t *strides, const int *masks, int *status, void *stream) {
@@ -2351,8 +2449,12 @@ extern "C" int dcc_t3_perm_gather_tma(double *r3, const int32_t *ijk, int64_t nb
                 nslot++;
             }
     }
-    if (!tma || ((uintptr_t)r3 & 15))
+    if (!tma || ((uintptr_t)r3 & 15)) {
+        if (gather_band_launch(r3, ijk, nblocks, nocc, nvir, beta, nsrc, bases, scales, strides, masks, stream) ==
+            DCC_OK)
+            return launch_status("t3_gather_band");
         return dcc_t3_perm_gather(r3, ijk, nblocks, nvir, beta, nsrc, bases, scales, strides, masks, stream);
+    }
     g.nslot = nslot;
     {
         const int64_t ext[5] = {nvir, nvir, nvir, nblocks, 1};

@@ -104,6 +104,27 @@ def test_tma_gather_matches_cp_async_gather(mods, nvir, beta):
         assert torch.equal(a, b)
 
 
+@pytest.mark.parametrize("no,nvir", [(1, 3), (2, 1), (3, 5), (4, 9), (3, 13), (2, 93)])
+@pytest.mark.parametrize("beta", [0.0, 0.75])
+def test_row_gather_matches_cp_async_gather(mods, no, nvir, beta):
+    """At an odd nvir the full-layout, every-permutation gather of the residual runs by rows (two
+    whole rows and four staged column tiles per output row): bit for bit the cp.async kernel."""
+    syn, tr, er = mods
+    d = syn.make_inputs(no, nvir, seed=2, with_t3=False)
+    n3 = d.ijk.shape[0]
+    g = torch.Generator(device="cuda").manual_seed(nvir + 7 * no)
+    full = torch.randn((no ** 3, nvir, nvir, nvir), dtype=torch.float64, device="cuda", generator=g)
+    r0 = torch.randn((n3, nvir, nvir, nvir), dtype=torch.float64, device="cuda", generator=g)
+    src = [(full, -1.25, tr.full_strides(no, nvir), tr.ALL_S3)]
+    a, b = r0.clone(), r0.clone()
+    st = torch.zeros(1, dtype=torch.int32, device="cuda")
+    tr.perm_gather_(a, d.ijk, nvir, beta, src)
+    tr.perm_gather_(b, d.ijk, nvir, beta, src, nocc=no, status=st)
+    torch.cuda.synchronize()
+    assert int(st.item()) == 0
+    assert torch.equal(a, b)
+
+
 @pytest.mark.parametrize("precision", ["bf16x3", "tf32x3"])
 def test_autotuned_wvvvv_gemms(mods, precision):
     """T3Residual.tune times every pipeline candidate of the W_vvvv.t3 GEMMs (K = nvir^2 >
