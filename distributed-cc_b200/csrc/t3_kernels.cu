@@ -1846,6 +1846,76 @@ __global__ void __launch_bounds__(NT, 2)
 
 }  // namespace dcc
 
+namespace dcc {
+
+// The unpack of every ordering for rows that are not 16-byte aligned, by rows: U[o][a,b,:] is a
+// whole row of the canonical block C when the ordering keeps c the fastest axis of C (two of the
+// six orderings), and otherwise a column of C (c as C's middle or first axis), which a work item
+// stages for a pair of 8-wide index tiles (a in I, b in J) and every c in shared memory (8-byte
+// copies of 64-byte segments) before its warps stream the 64 output rows with coalesced stores.
+// Items run canonical block by canonical block, so the orderings of a block reuse it from L2.
+constexpr int UR_PITCH = 65;
+
+__global__ void __launch_bounds__(256, 3) k_unpack_rows(const double *__restrict__ t3, double *__restrict__ U,
+                                                        int64_t nblocks, int nocc, int nv, int ntile) {
+    extern __shared__ double ur_sm[];  // [c][a_local * 8 + b_local]
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int64_t n3 = (int64_t)nv * nv * nv, nv2 = (int64_t)nv * nv;
+    const int64_t per_q = 6 * (int64_t)ntile * ntile, nwork = nblocks * per_q;
+    for (int64_t w = blockIdx.x; w < nwork; w += gridDim.x) {
+        const int64_t q = w / per_q;
+        const int rem = (int)(w % per_q), g = rem / (ntile * ntile), I = (rem / ntile) % ntile, J = rem % ntile;
+        int o[3];
+        decode_tri3(q, nocc, o[0], o[1], o[2]);
+        const int xyz[3] = {o[perm3(g, 0)], o[perm3(g, 1)], o[perm3(g, 2)]};
+        bool dup = false;
+        for (int sp = 0; sp < g; sp++)
+            if (o[perm3(sp, 0)] == xyz[0] && o[perm3(sp, 1)] == xyz[1] && o[perm3(sp, 2)] == xyz[2]) dup = true;
+        if (dup) continue;  // uniform over the CTA
+        int64_t srt[3];
+        const int cs = order_case3(xyz[0], xyz[1], xyz[2], srt);
+        const int pi = cs == 3 ? 4 : (cs == 4 ? 3 : cs);  // U[o][u] = C[u[perm3(pi, 0)], u[perm3(pi, 1)], u[perm3(pi, 2)]]
+        const double *C = t3 + q * n3;
+        double *Uo = U + (((int64_t)xyz[0] * nocc + xyz[1]) * nocc + xyz[2]) * n3;
+        const int a0 = I * TE, b0 = J * TE;
+        if (pi == 0 || pi == 2) {  // whole rows: C[a][b][:] or C[b][a][:]
+            for (int rw = warp; rw < 64; rw += 8) {
+                const int a = a0 + (rw >> 3), b = b0 + (rw & 7);
+                if (a >= nv || b >= nv) continue;
+                const double *src = C + (pi == 0 ? a * nv2 + (int64_t)b * nv : b * nv2 + (int64_t)a * nv);
+                double *dst = Uo + a * nv2 + (int64_t)b * nv;
+                for (int c = lane; c < nv; c += 32) dst[c] = __ldg(src + c);
+            }
+            continue;
+        }
+        // columns: C position (a, c, b) for pi = 1, (b, c, a) for 3, (c, a, b) for 4, (c, b, a) for 5;
+        // the copies run along C's last axis (b for 1 and 4, a for 3 and 5)
+        for (int e = threadIdx.x; e < nv * 64; e += blockDim.x) {
+            const int c = e >> 6, r = (e >> 3) & 7, t = e & 7;
+            const bool bfast = pi == 1 || pi == 4;
+            const int al = bfast ? r : t, bl = bfast ? t : r, a = a0 + al, b = b0 + bl;
+            if (a >= nv || b >= nv) continue;
+            const int64_t off = pi == 1 ? a * nv2 + (int64_t)c * nv + b
+                              : pi == 3 ? b * nv2 + (int64_t)c * nv + a
+                              : pi == 4 ? c * nv2 + (int64_t)a * nv + b
+                                        : c * nv2 + (int64_t)b * nv + a;
+            cp_async8(ur_sm + c * UR_PITCH + al * 8 + bl, C + off);
+        }
+        cp_async_commit();
+        cp_async_wait<0>();
+        __syncthreads();
+        for (int rw = warp; rw < 64; rw += 8) {
+            const int al = rw >> 3, bl = rw & 7, a = a0 + al, b = b0 + bl;
+            if (a >= nv || b >= nv) continue;
+            double *dst = Uo + a * nv2 + (int64_t)b * nv;
+            for (int c = lane; c < nv; c += 32) dst[c] = ur_sm[c * UR_PITCH + rw];
+        }
+        __syncthreads();  // the tile is refilled by the next item
+    }
+}
+
+}  // namespace dcc
+
 extern "C" int dcc_t3_unpack_all(const double *t3, double *U, int64_t nocc, int64_t nvir, void *stream) {
     clear_error();
     DCC_REQUIRE(nocc >= 0 && nvir >= 0, DCC_ERR_SHAPE, "negative size");
@@ -1889,7 +1959,18 @@ extern "C" int dcc_t3_unpack_all(const double *t3, double *U, int64_t nocc, int6
         }
     }
     {
-        // odd nvir: the same bands with cp.async loads and coalesced stores
+        // odd nvir: whole rows, columns through a staged tile (k_unpack_rows)
+        const size_t rsm = (size_t)nvir * UR_PITCH * sizeof(double);
+        if (nvir <= 104 && nocc * nocc * nocc < (1ll << 31) && nblocks < (1ll << 31) && nocc <= 1290) {
+            int dev = 0, nsm = 148;
+            if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+            const int64_t nwork = nblocks * 6 * (int64_t)ntile * ntile, cap = (int64_t)nsm * 3;
+            const unsigned grid = (unsigned)(nwork < cap ? nwork : cap);
+            cudaFuncSetAttribute(k_unpack_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rsm);
+            k_unpack_rows<<<grid, 256, rsm, as_stream(stream)>>>(t3, U, nblocks, (int)nocc, (int)nvir, ntile);
+            return launch_status("t3_unpack_all");
+        }
+        // the same bands with cp.async loads and coalesced stores
         const size_t bsm = ((size_t)ntile * TE3 + (size_t)TE * TE * nvir) * sizeof(double);
         if (nvir <= 256 && bsm <= 100 * 1024 && nocc * nocc * nocc < (1ll << 31) && nblocks < (1ll << 31)) {
             int dev = 0, nsm = 148;
