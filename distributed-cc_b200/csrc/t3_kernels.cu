@@ -1109,6 +1109,7 @@ namespace dcc {
 // DRAM reads at an odd nvir.  The arithmetic is the orbit kernel's with its p4 term (0 x the
 // second half) left out: equal results up to the sign of a zero.
 constexpr int PB_PITCH = 65;  // doubles per (c) row of a staged column tile: 8 x 8 + 1
+constexpr int GB_PITCH = PB_PITCH;
 
 __global__ void __launch_bounds__(256, 2) k_p3_band3(const double *__restrict__ A, double *__restrict__ B,
                                                      int64_t nblocks, int nv, int ntile, P3Coef k) {
@@ -2386,8 +2387,6 @@ namespace dcc {
 // in shared memory for a pair of 8-wide index tiles (a in I, b in J) and a chunk of c.  Each warp
 // then streams output rows with coalesced loads and stores.  The slots are summed in the order of
 // the orbit-tile kernels (p = 0..5, one fma each), so the result is theirs bit for bit.
-constexpr int GB_PITCH = 65;
-
 __global__ void __launch_bounds__(256, 2) k_gather_band(const double *__restrict__ S, double *__restrict__ r3,
                                                         const int32_t *__restrict__ ijk, int64_t nblocks, int nocc,
                                                         int nv, int ntile, int cchunk, double scale, double beta) {
