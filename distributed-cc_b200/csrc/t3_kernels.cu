@@ -1752,99 +1752,6 @@ __global__ void __launch_bounds__(NT, NB == 2 ? 1 : 2)
     if (threadIdx.x == 0) bulk_wait<0>();
 }
 
-// The same row-band unpack for odd nvir, whose 8-byte aligned rows TMA cannot describe:
-// cp.async copies of the band's source tiles (8 bytes each) into a dense tile buffer, the
-// conflict-free transpose into the [8][8][nvir] band as above, and the band written by the
-// whole CTA as 8 contiguous runs of up to 8 rows each (coalesced 8-byte stores).  One tile
-// buffer and one band per CTA, two CTAs per SM; the loads of the next item are issued
-// before the current band is stored.  Items run block-major, as above.
-template <int NT>
-__global__ void __launch_bounds__(NT, 2)
-    k_unpack_band_odd(const double *__restrict__ t3, double *__restrict__ U, int64_t nblocks, int nocc, int nv,
-                      int ntile) {
-    extern __shared__ __align__(128) double sm[];  // ntile x TE3 source tiles, then the 8 x 8 x nv band
-    double *tiles = sm, *band = sm + (size_t)ntile * TE3;
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    constexpr int STEPS = 16 / (NT / 32);
-    const int pinv[6] = {0, 1, 2, 4, 3, 5};
-    const int64_t per_q = 6 * (int64_t)ntile * ntile, nwork = nblocks * per_q;
-    const int64_t n3 = (int64_t)nv * nv * nv;
-    struct Item {
-        int64_t w, out;
-        int q, pi, X, Y;
-    };
-    auto next_item = [&](int64_t wi) {
-        Item it{};
-        for (; wi < nwork; wi += gridDim.x) {
-            const int64_t q = wi / per_q;
-            const int g = (int)((wi / ((int64_t)ntile * ntile)) % 6);
-            int o[3];
-            decode_tri3(q, nocc, o[0], o[1], o[2]);
-            const int xyz[3] = {o[perm3(g, 0)], o[perm3(g, 1)], o[perm3(g, 2)]};
-            bool dup = false;
-            for (int sp = 0; sp < g; sp++)
-                if (o[perm3(sp, 0)] == xyz[0] && o[perm3(sp, 1)] == xyz[1] && o[perm3(sp, 2)] == xyz[2]) dup = true;
-            if (dup) continue;
-            int64_t srt[3];
-            it.pi = pinv[order_case3(xyz[0], xyz[1], xyz[2], srt)];
-            it.out = ((int64_t)xyz[0] * nocc + xyz[1]) * nocc + xyz[2];
-            it.q = (int)q;
-            const int xy = (int)(wi % ((int64_t)ntile * ntile));
-            it.X = xy / ntile;
-            it.Y = xy % ntile;
-            break;
-        }
-        it.w = wi;
-        return it;
-    };
-    // the band's source tiles: tile zt of the band is the source tile at the permuted tile
-    // coordinates, stored dense [8][8][8] over the source's own (a, b, c)
-    auto issue = [&](const Item &it) {
-        const double *blk = t3 + (int64_t)it.q * n3;
-        for (int zt = 0; zt < ntile; zt++) {
-            const int T[3] = {it.X, it.Y, zt};
-            const int a0 = T[perm3(it.pi, 0)] * TE, b0 = T[perm3(it.pi, 1)] * TE, c0 = T[perm3(it.pi, 2)] * TE;
-            double *tl = tiles + zt * TE3;
-            for (int e = threadIdx.x; e < TE3; e += NT) {
-                const int ga = a0 + (e >> 6), gb = b0 + ((e >> 3) & 7), gc = c0 + (e & 7);
-                if (ga < nv && gb < nv && gc < nv) cp_async8(tl + e, blk + ((int64_t)ga * nv + gb) * nv + gc);
-            }
-        }
-        cp_async_commit();
-    };
-    Item cur = next_item(blockIdx.x);
-    if (cur.w >= nwork) return;
-    issue(cur);
-    while (cur.w < nwork) {
-        cp_async_wait<0>();
-        __syncthreads();  // the tiles have landed; the previous band has been stored
-        const int p0 = perm3(cur.pi, 0), p1 = perm3(cur.pi, 1), p2 = perm3(cur.pi, 2);
-#pragma unroll
-        for (int jj = 0; jj < STEPS; jj++) {
-            int u[3];
-            tile_element(lane, w * STEPS + jj, u);
-            auto sel = [&](int m) { return m == 0 ? u[0] : (m == 1 ? u[1] : u[2]); };
-            const int so = (sel(p0) * TE + sel(p1)) * TE + sel(p2);
-            const int bo = (u[0] * TE + u[1]) * nv + u[2];
-            for (int zt = 0; zt < ntile; zt++)
-                if (u[2] < nv - zt * TE) band[bo + zt * TE] = tiles[zt * TE3 + so];
-        }
-        __syncthreads();  // the band is complete; the tiles are free
-        const Item nxt = next_item(cur.w + gridDim.x);
-        if (nxt.w < nwork) issue(nxt);
-        // rows (X*8 + u0, Y*8 + u1) for u1 < 8 are contiguous in the output block: 8 runs
-        const int nrow0 = min(TE, nv - cur.X * TE), nrow1 = min(TE, nv - cur.Y * TE);
-        double *dst = U + cur.out * n3;
-        for (int u0 = 0; u0 < nrow0; u0++) {
-            double *run = dst + ((int64_t)(cur.X * TE + u0) * nv + cur.Y * TE) * nv;
-            const double *src = band + u0 * TE * nv;
-            const int len = nrow1 * nv;
-            for (int e = threadIdx.x; e < len; e += NT) run[e] = src[e];
-        }
-        cur = nxt;
-    }
-}
-
 }  // namespace dcc
 
 namespace dcc {
@@ -1925,6 +1832,20 @@ extern "C" int dcc_t3_unpack_all(const double *t3, double *U, int64_t nocc, int6
     const int64_t nblocks = nocc * (nocc + 1) * (nocc + 2) / 6;
     int ntile = (int)ceil_div(nvir, TE);
     {
+        // whole rows, columns through a staged tile (k_unpack_rows): at nocc=10 / nvir=90 3.78 ms
+        // against 5.13 ms for the TMA row bands below, and the kernel for odd nvir
+        const size_t rsm = (size_t)nvir * UR_PITCH * sizeof(double);
+        if (nvir <= 104 && nocc * nocc * nocc < (1ll << 31) && nblocks < (1ll << 31) && nocc <= 1290) {
+            int dev = 0, nsm = 148;
+            if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+            const int64_t nwork = nblocks * 6 * (int64_t)ntile * ntile, cap = (int64_t)nsm * 3;
+            const unsigned grid = (unsigned)(nwork < cap ? nwork : cap);
+            cudaFuncSetAttribute(k_unpack_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rsm);
+            k_unpack_rows<<<grid, 256, rsm, as_stream(stream)>>>(t3, U, nblocks, (int)nocc, (int)nvir, ntile);
+            return launch_status("t3_unpack_all");
+        }
+    }
+    {
         // band kernel: even nvir (16-byte rows), aligned buffers, box sides <= 256, shared memory
         const size_t bsm = ((size_t)ntile * TE3 + (size_t)TE * TE * nvir) * sizeof(double);
         EncodeTiledFn fn = encode_fn();
@@ -1957,30 +1878,6 @@ extern "C" int dcc_t3_unpack_all(const double *t3, double *U, int64_t nocc, int6
                                                                              status);
                 return launch_status("t3_unpack_all");
             }
-        }
-    }
-    {
-        // odd nvir: whole rows, columns through a staged tile (k_unpack_rows)
-        const size_t rsm = (size_t)nvir * UR_PITCH * sizeof(double);
-        if (nvir <= 104 && nocc * nocc * nocc < (1ll << 31) && nblocks < (1ll << 31) && nocc <= 1290) {
-            int dev = 0, nsm = 148;
-            if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-            const int64_t nwork = nblocks * 6 * (int64_t)ntile * ntile, cap = (int64_t)nsm * 3;
-            const unsigned grid = (unsigned)(nwork < cap ? nwork : cap);
-            cudaFuncSetAttribute(k_unpack_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rsm);
-            k_unpack_rows<<<grid, 256, rsm, as_stream(stream)>>>(t3, U, nblocks, (int)nocc, (int)nvir, ntile);
-            return launch_status("t3_unpack_all");
-        }
-        // the same bands with cp.async loads and coalesced stores
-        const size_t bsm = ((size_t)ntile * TE3 + (size_t)TE * TE * nvir) * sizeof(double);
-        if (nvir <= 256 && bsm <= 100 * 1024 && nocc * nocc * nocc < (1ll << 31) && nblocks < (1ll << 31)) {
-            int dev = 0, nsm = 148;
-            if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-            const int64_t nwork = nblocks * 6 * (int64_t)ntile * ntile, cap = (int64_t)nsm * 2;
-            const unsigned grid = (unsigned)(nwork < cap ? nwork : cap);
-            cudaFuncSetAttribute(k_unpack_band_odd<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bsm);
-            k_unpack_band_odd<256><<<grid, 256, bsm, as_stream(stream)>>>(t3, U, nblocks, (int)nocc, (int)nvir, ntile);
-            return launch_status("t3_unpack_all");
         }
     }
     int64_t ntri = (int64_t)ntile * (ntile + 1) * (ntile + 2) / 6;
@@ -2452,8 +2349,7 @@ __global__ void __launch_bounds__(256, 2) k_gather_band(const double *__restrict
 static int gather_band_launch(double *r3, const int32_t *ijk, int64_t nblocks, int64_t nocc, int64_t nvir, double beta,
                               int nsrc, const double *const *bases, const double *scales, const int64_t *strides,
                               const int *masks, void *stream) {
-    if (nsrc != 1 || masks[0] != 63 || nvir % 2 == 0 || nvir > 104 || nocc < 1 || nocc > 1290 || !bases[0])
-        return DCC_ERR_UNSUPPORTED;
+    if (nsrc != 1 || masks[0] != 63 || nvir > 104 || nocc < 1 || nocc > 1290 || !bases[0]) return DCC_ERR_UNSUPPORTED;
     const int64_t n3 = nvir * nvir * nvir;
     const int64_t full[6] = {nocc * nocc * n3, nocc * n3, n3, nvir * nvir, nvir, 1};
     for (int m = 0; m < 6; m++)
@@ -2482,6 +2378,11 @@ extern "C" int dcc_t3_perm_gather_tma(double *r3, const int32_t *ijk, int64_t nb
     DCC_REQUIRE(nsrc >= 1 && nsrc <= PG_MAX_SRC, DCC_ERR_SHAPE, "1..%d sources", PG_MAX_SRC);
     if (nblocks == 0 || nvir == 0) return DCC_OK;
     DCC_REQUIRE(r3 && ijk && bases && scales && strides && masks && status, DCC_ERR_NULL, "NULL argument");
+    // the residual's gather (one full-layout source, every permutation) runs by rows: at nocc=10 /
+    // nvir=90 2.90 ms against 3.39 ms for the TMA pipeline below, and at odd nvir, where TMA
+    // cannot describe the rows, 13.5 ms against 22.0 ms for the cp.async kernel at nocc=15
+    if (gather_band_launch(r3, ijk, nblocks, nocc, nvir, beta, nsrc, bases, scales, strides, masks, stream) == DCC_OK)
+        return launch_status("t3_gather_band");
     // the copy engine needs 16-byte strides, a unit-stride c and b faster than a; otherwise the
     // cp.async kernel serves the call
     bool tma = nvir % 2 == 0 && nocc >= 1 && nocc <= 1290 && nvir <= 65536;
@@ -2529,12 +2430,8 @@ extern "C" int dcc_t3_perm_gather_tma(double *r3, const int32_t *ijk, int64_t nb
                 nslot++;
             }
     }
-    if (!tma || ((uintptr_t)r3 & 15)) {
-        if (gather_band_launch(r3, ijk, nblocks, nocc, nvir, beta, nsrc, bases, scales, strides, masks, stream) ==
-            DCC_OK)
-            return launch_status("t3_gather_band");
+    if (!tma || ((uintptr_t)r3 & 15))
         return dcc_t3_perm_gather(r3, ijk, nblocks, nvir, beta, nsrc, bases, scales, strides, masks, stream);
-    }
     g.nslot = nslot;
     {
         const int64_t ext[5] = {nvir, nvir, nvir, nblocks, 1};

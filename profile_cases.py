@@ -357,7 +357,8 @@ def main():
     ap.add_argument("--kind", default="bf16x3")
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--nocc", type=int, default=None, help="occupied orbitals (xgemm, oogemm, gather, unpack)")
-    ap.add_argument("--nvir", type=int, default=90, help="virtual orbitals (p3)")
+    ap.add_argument("--nvir", type=int, default=None,
+                    help="virtual orbitals (default 90; 93 for oddnv and t3half)")
     ap.add_argument("--op", default="p3", choices=["p3", "p3_422", "roundtrip", "triple", "transpose"],
                     help="p3 case: which symmetrizer")
     ap.add_argument("--time", action="store_true", help="p3 case: print CUDA-event timings")
@@ -366,22 +367,22 @@ def main():
     ap.add_argument("--passes", default=None, help="oddnv case: comma-separated pass indices (default all)")
     a = ap.parse_args()
     if a.case == "gemm":
-        case_gemm(a.kind, a.reps, a.nocc or 10, a.nvir)
+        case_gemm(a.kind, a.reps, a.nocc or 10, a.nvir or 90)
     elif a.case == "p3":
-        case_p3(a.reps, a.nvir, a.op, a.time)
+        case_p3(a.reps, a.nvir or 90, a.op, a.time)
     elif a.case == "update":
         case_update(a.reps)
     elif a.case == "t4":
         case_t4(a.reps, a.kind, a.breakdown)
     elif a.case == "t3iter":
-        case_t3iter(a.reps, a.nocc or 10, a.nvir, a.kind)
+        case_t3iter(a.reps, a.nocc or 10, a.nvir or 90, a.kind)
     elif a.case == "oddnv":
-        case_oddnv(a.reps, a.nocc or 5, a.nvir if a.nvir != 90 else 93, a.time,
+        case_oddnv(a.reps, a.nocc or 5, a.nvir or 93, a.time,
                    [int(x) for x in a.passes.split(",")] if a.passes else None)
     elif a.case == "t3half":
-        case_t3half(a.reps, a.nocc or 15, a.nvir if a.nvir != 90 else 93, a.kind, a.breakdown)
+        case_t3half(a.reps, a.nocc or 15, a.nvir or 93, a.kind, a.breakdown)
     elif a.case == "qsample":
-        case_qsample(a.nocc or 10, a.nvir, a.kind, dchunk=a.dchunk)
+        case_qsample(a.nocc or 10, a.nvir or 90, a.kind, dchunk=a.dchunk)
     elif a.case in ("gather", "xgemm", "oogemm", "unpack", "qgroup"):
         fn = {"gather": case_gather, "xgemm": case_xgemm, "oogemm": case_oogemm, "unpack": case_unpack,
               "qgroup": case_qgroup}[a.case]

@@ -408,10 +408,11 @@ def test_q_division_and_factor(C, oracle):
 
 @pytest.mark.parametrize("nocc,nvir,aligned", [(1, 3, True), (3, 5, True), (4, 9, True), (3, 17, True), (2, 4, True),
                                                (3, 10, True), (4, 18, True), (1, 2, True), (5, 8, True), (2, 90, True),
-                                               (3, 10, False), (2, 93, True), (3, 25, False)])
+                                               (3, 10, False), (2, 93, True), (3, 25, False), (1, 106, True),
+                                               (2, 112, True), (1, 105, True)])
 def test_unpack_all(C, oracle, nocc, nvir, aligned):
-    """Even nvir with 16-byte aligned buffers run the row-band TMA kernel, the rest (odd nvir or
-    unaligned buffers) the row kernel with staged column tiles."""
+    """nvir <= 104 runs the row kernel with staged column tiles; above it even nvir with 16-byte
+    aligned buffers the row-band TMA kernel, the rest the orbit-tile kernel."""
     from dcc import t3_residual
     rng = np.random.default_rng(13)
     n3 = nocc * (nocc + 1) * (nocc + 2) // 6
