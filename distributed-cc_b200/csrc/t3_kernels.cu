@@ -1098,91 +1098,72 @@ extern "C" int dcc_t3_spin_summation_inplace(double *A, int64_t nblocks, int64_t
 namespace dcc {
 
 // Out-of-place P3 for the patterns whose p4 is 0 (P3_201: B = beta A + alpha p3 (p0 A + p1 A^cba
-// + p2 A^bac)) by row pairs, for rows that are not 16-byte aligned.  Of the three terms of
-// B[a,b,:], A[a,b,:] and A[b,a,:] are whole rows (read once for the two output rows (a,b) and
-// (b,a)) and A[:,b,a] is a column; a work item is a block and a pair of 8-wide index tiles
-// (I <= J): the CTA stages the two column tiles A[c][J..][I..] and A[c][I..][J..] for every c in
-// shared memory (8-byte copies of 64-byte segments, row pitch 65 doubles so the transposed reads
-// are conflict-free), then each warp streams row pairs: coalesced loads of the two rows and
-// coalesced stores of the two output rows, whole rows of nvir elements.  Writes therefore cover
-// runs of rows instead of the 64-byte tile rows of the orbit kernel, whose partial sectors cost
-// DRAM reads at an odd nvir.  The arithmetic is the orbit kernel's with its p4 term (0 x the
-// second half) left out: equal results up to the sign of a zero.
-constexpr int PB_PITCH = 65;  // doubles per (c) row of a staged column tile: 8 x 8 + 1
-constexpr int GB_PITCH = PB_PITCH;
-
-__global__ void __launch_bounds__(256, 2) k_p3_band3(const double *__restrict__ A, double *__restrict__ B,
-                                                     int64_t nblocks, int nv, int ntile, P3Coef k) {
-    extern __shared__ double pb_sm[];  // T1[c][r][s] = A[c][J*8+r][I*8+s], then T2 = A[c][I*8+r][J*8+s]
-    double *T1 = pb_sm, *T2 = pb_sm + (size_t)nv * PB_PITCH;
+// + p2 A^bac)) by strips, for nvir <= 104 at any row pitch: a work item is a block, a middle
+// index b and a tile of 32 first indices a.  The CTA stages the column strip A[:, b, a0..a0+31]
+// (every c; 256-byte segments, row pitch 33 doubles so the transposed reads are conflict-free)
+// in shared memory, then each warp writes whole output rows B[a, b, :]: it issues the loads of
+// both rows A[a,b,:] and A[b,a,:] (every c of the row at once, up to 8 in flight per lane) before
+// the arithmetic, which takes A[c,b,a] from the strip.  Every element is read three times (strip,
+// and the two rows), the repeats L2 hits: the items of one block run side by side.  The
+// arithmetic is the orbit kernel's with its p4 term (0 x the second half) left out: equal results
+// up to the sign of a zero.
+constexpr int SP3_W = 32, SP3_PITCH = 33, SP3_MAXNV = 104;
+__global__ void __launch_bounds__(256, 4) k_p3_strips(const double *__restrict__ A, double *__restrict__ B,
+                                                      int64_t nblocks, int nv, int ntile, P3Coef k) {
+    __shared__ double S[SP3_MAXNV * SP3_PITCH];  // S[c][s] = A[c][b][a0 + s]
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int64_t n3 = (int64_t)nv * nv * nv, nv2 = (int64_t)nv * nv;
-    const int64_t npair = (int64_t)ntile * (ntile + 1) / 2, nwork = nblocks * npair;
+    const int64_t per_blk = (int64_t)nv * ntile, nwork = nblocks * per_blk;
     for (int64_t w = blockIdx.x; w < nwork; w += gridDim.x) {
-        const int64_t b = w / npair;
-        int r = (int)(w % npair), I = 0;
-        while (r >= ntile - I) {  // (I, J) with I <= J, J fastest
-            r -= ntile - I;
-            I++;
-        }
-        const int J = I + r;
-        const double *Ab = A + b * n3;
-        double *Bb = B + b * n3;
-        const int i0 = I * TE, j0 = J * TE;
-        // the column tiles (the second only when I != J: for I == J it equals the first)
-        for (int e = threadIdx.x; e < nv * 64; e += blockDim.x) {
-            const int c = e >> 6, rr = (e >> 3) & 7, ss = e & 7;
-            if (j0 + rr < nv && i0 + ss < nv) cp_async8(T1 + c * PB_PITCH + rr * 8 + ss, Ab + c * nv2 + (int64_t)(j0 + rr) * nv + i0 + ss);
-            if (I != J && i0 + rr < nv && j0 + ss < nv)
-                cp_async8(T2 + c * PB_PITCH + rr * 8 + ss, Ab + c * nv2 + (int64_t)(i0 + rr) * nv + j0 + ss);
-        }
+        const int64_t blk = w / per_blk;
+        const int r = (int)(w - blk * per_blk), b = r / ntile, a0 = (r - b * ntile) * SP3_W;
+        const int h = nv - a0 < SP3_W ? nv - a0 : SP3_W;
+        const double *Ab = A + blk * n3;
+        double *Bb = B + blk * n3;
+        for (int c = warp; c < nv; c += 8)
+            if (lane < h) cp_async8(S + c * SP3_PITCH + lane, Ab + (int64_t)c * nv2 + (int64_t)b * nv + a0 + lane);
         cp_async_commit();
         cp_async_wait<0>();
         __syncthreads();
-        const double *T2r = I == J ? T1 : T2;
-        // row pairs (a, b) = (i0 + s, j0 + q) with the output rows B[a,b,:] and B[b,a,:];
-        // on the diagonal tile pairs with s <= q only (s == q: one row)
-        for (int pr = warp; pr < 64; pr += 8) {
-            const int s_ = pr & 7, q_ = pr >> 3;
-            if (I == J && s_ > q_) continue;
-            const int a = i0 + s_, bb = j0 + q_;
-            if (a >= nv || bb >= nv) continue;
-            const double *rab = Ab + (int64_t)a * nv2 + (int64_t)bb * nv;   // A[a,b,:]
-            const double *rba = Ab + (int64_t)bb * nv2 + (int64_t)a * nv;   // A[b,a,:]
-            double *oab = Bb + (int64_t)a * nv2 + (int64_t)bb * nv;
-            double *oba = Bb + (int64_t)bb * nv2 + (int64_t)a * nv;
-            const bool two = a != bb;
-            for (int c = lane; c < nv; c += 32) {
-                const double vab = __ldg(rab + c), vba = __ldg(rba + c);
-                // B[a,b,c]: A[c,b,a] = T1[c][q][s];  B[b,a,c]: A[c,a,b] = T2[c][s][q]
-                const double cba = T1[c * PB_PITCH + q_ * 8 + s_];
-                const double tu = dadd(dadd(dmul(k.p0, vab), dmul(k.p1, cba)), dmul(k.p2, vba));
-                oab[c] = dadd(dmul(k.beta, vab), dmul(k.alpha, dmul(k.p3, tu)));
-                if (two) {
-                    const double cab = T2r[c * PB_PITCH + s_ * 8 + q_];
-                    const double tu2 = dadd(dadd(dmul(k.p0, vba), dmul(k.p1, cab)), dmul(k.p2, vab));
-                    oba[c] = dadd(dmul(k.beta, vba), dmul(k.alpha, dmul(k.p3, tu2)));
+        for (int s = warp; s < h; s += 8) {
+            const int a = a0 + s;
+            const double *rab = Ab + (int64_t)a * nv2 + (int64_t)b * nv, *rba = Ab + (int64_t)b * nv2 + (int64_t)a * nv;
+            double *out = Bb + (int64_t)a * nv2 + (int64_t)b * nv;
+            double vab[4], vba[4];  // c = lane + 32 j covers nv <= 128
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                const int c = lane + 32 * j;
+                vab[j] = c < nv ? __ldg(rab + c) : 0.0;
+                vba[j] = c < nv ? __ldg(rba + c) : 0.0;
+            }
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                const int c = lane + 32 * j;
+                if (c < nv) {
+                    const double cba = S[c * SP3_PITCH + s];
+                    const double tu = dadd(dadd(dmul(k.p0, vab[j]), dmul(k.p1, cba)), dmul(k.p2, vba[j]));
+                    out[c] = dadd(dmul(k.beta, vab[j]), dmul(k.alpha, dmul(k.p3, tu)));
                 }
             }
         }
-        __syncthreads();  // the column tiles are refilled by the next item
+        __syncthreads();  // the strip is refilled by the next item
     }
 }
 
 }  // namespace dcc
 
-// The row-pair kernel for out-of-place P3 with p4 == 0 at a row pitch TMA cannot describe;
-// returns DCC_ERR_UNSUPPORTED (nothing launched) where it does not apply.
-static int p3_band3_launch(const double *A, double *B, int64_t nblocks, int64_t nvir, const P3Coef &k, void *stream) {
-    if (k.p4 != 0.0 || A == B || nvir < 1 || nvir > 104 || nvir % 2 == 0) return DCC_ERR_UNSUPPORTED;
-    const int ntile = (int)ceil_div(nvir, TE);
-    const size_t smem = 2 * (size_t)nvir * PB_PITCH * sizeof(double);
-    int dev = 0, nsm = 148;
+// The strip kernel for out-of-place P3 with p4 == 0, nvir <= 104; returns DCC_ERR_UNSUPPORTED
+// (nothing launched) where it does not apply.
+static int p3_strips_launch(const double *A, double *B, int64_t nblocks, int64_t nvir, const P3Coef &k, void *stream) {
+    if (k.p4 != 0.0 || A == B || nvir < 1 || nvir > SP3_MAXNV) return DCC_ERR_UNSUPPORTED;
+    const int ntile = (int)ceil_div(nvir, SP3_W);
+    int dev = 0, nsm = 148, per_sm = 1;
     if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    const int64_t nwork = nblocks * (int64_t)ntile * (ntile + 1) / 2, cap = (int64_t)nsm * 2;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_p3_strips, 256, 0) != cudaSuccess || per_sm < 1)
+        per_sm = 1;
+    const int64_t nwork = nblocks * nvir * ntile, cap = (int64_t)nsm * per_sm;
     const unsigned grid = (unsigned)(nwork < cap ? nwork : cap);
-    cudaFuncSetAttribute(k_p3_band3, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k_p3_band3<<<grid, 256, smem, as_stream(stream)>>>(A, B, nblocks, (int)nvir, ntile, k);
+    k_p3_strips<<<grid, 256, 0, as_stream(stream)>>>(A, B, nblocks, (int)nvir, ntile, k);
     return DCC_OK;
 }
 
@@ -1197,8 +1178,28 @@ extern "C" int dcc_t3_spin_summation(const double *A, double *B, int64_t nblocks
     const int64_t bytes = nblocks * nvir * nvir * nvir * (int64_t)sizeof(double);
     DCC_REQUIRE(A == B || (const char *)B + bytes <= (const char *)A || (const char *)A + bytes <= (const char *)B,
                 DCC_ERR_SHAPE, "A and B overlap");
-    if (nblocks > 0 && p3_band3_launch(A, B, nblocks, nvir, k, stream) == DCC_OK) return launch_status("P3 by row pairs");
+    if (nblocks > 0 && p3_strips_launch(A, B, nblocks, nvir, k, stream) == DCC_OK) return launch_status("P3 by strips");
     return orbit3_launch(0, A, B, nullptr, nullptr, nblocks, nvir, k, stream);
+}
+
+extern "C" int dcc_t3_spin_summation_kernel(const double *A, double *B, int64_t nblocks, int64_t nvir,
+                                            const char *pattern, double alpha, double beta, int kernel, void *stream) {
+    clear_error();
+    DCC_REQUIRE(kernel >= 0 && kernel <= 2, DCC_ERR_UNSUPPORTED, "kernel must be 0..2");
+    if (kernel == 0) return dcc_t3_spin_summation(A, B, nblocks, nvir, pattern, alpha, beta, stream);
+    P3Coef k;
+    int rc = p3_coef(pattern, alpha, beta, k);
+    if (rc) return rc;
+    DCC_REQUIRE(nblocks >= 0 && nvir >= 0, DCC_ERR_SHAPE, "negative size");
+    DCC_REQUIRE((A && B) || nblocks * nvir == 0, DCC_ERR_NULL, "NULL buffer");
+    const int64_t bytes = nblocks * nvir * nvir * nvir * (int64_t)sizeof(double);
+    DCC_REQUIRE(A == B || (const char *)B + bytes <= (const char *)A || (const char *)A + bytes <= (const char *)B,
+                DCC_ERR_SHAPE, "A and B overlap");
+    if (nblocks == 0) return DCC_OK;
+    if (kernel == 2) return orbit3_launch(0, A, B, nullptr, nullptr, nblocks, nvir, k, stream);
+    DCC_REQUIRE(p3_strips_launch(A, B, nblocks, nvir, k, stream) == DCC_OK, DCC_ERR_UNSUPPORTED,
+                "this kernel does not apply to the pattern or shape");
+    return launch_status("P3 by strips");
 }
 
 namespace dcc {
@@ -1756,23 +1757,26 @@ __global__ void __launch_bounds__(NT, NB == 2 ? 1 : 2)
 
 namespace dcc {
 
-// The unpack of every ordering for rows that are not 16-byte aligned, by rows: U[o][a,b,:] is a
-// whole row of the canonical block C when the ordering keeps c the fastest axis of C (two of the
-// six orderings), and otherwise a column of C (c as C's middle or first axis), which a work item
-// stages for a pair of 8-wide index tiles (a in I, b in J) and every c in shared memory (8-byte
-// copies of 64-byte segments) before its warps stream the 64 output rows with coalesced stores.
-// Items run canonical block by canonical block, so the orderings of a block reuse it from L2.
-constexpr int UR_PITCH = 65;
+// The unpack of every ordering for nvir <= 104 by strips.  A work item is a canonical block C, an
+// ordering, one fixed index x and a tile of 32 values y0.. of another; it writes the 32 output rows
+// U[o][x][y][:] (or U[o][y][x][:]).  When the ordering keeps c the fastest axis of C (two of the
+// six) those rows are whole rows of C, loaded two output rows at a time with every load issued
+// before the stores; otherwise each output row is a column of C (c as C's middle or first axis),
+// and the item stages the strip C[..c..][x][y0..y0+31] for every c in shared memory (8-byte copies
+// of 256-byte segments; row pitch 33 doubles) before its warps write the rows.  Items run
+// canonical block by canonical block, so the orderings of a block reuse it from L2.
+constexpr int US_W = 32, US_PITCH = 33, US_MAXNV = 104;
 
-__global__ void __launch_bounds__(256, 3) k_unpack_rows(const double *__restrict__ t3, double *__restrict__ U,
-                                                        int64_t nblocks, int nocc, int nv, int ntile) {
-    extern __shared__ double ur_sm[];  // [c][a_local * 8 + b_local]
+__global__ void __launch_bounds__(256, 4) k_unpack_strips(const double *__restrict__ t3, double *__restrict__ U,
+                                                          int64_t nblocks, int nocc, int nv, int ntile) {
+    __shared__ double T[US_MAXNV * US_PITCH];  // T[c][j]
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int64_t n3 = (int64_t)nv * nv * nv, nv2 = (int64_t)nv * nv;
-    const int64_t per_q = 6 * (int64_t)ntile * ntile, nwork = nblocks * per_q;
+    const int64_t per_g = (int64_t)nv * ntile, per_q = 6 * per_g, nwork = nblocks * per_q;
     for (int64_t w = blockIdx.x; w < nwork; w += gridDim.x) {
         const int64_t q = w / per_q;
-        const int rem = (int)(w % per_q), g = rem / (ntile * ntile), I = (rem / ntile) % ntile, J = rem % ntile;
+        const int rem = (int)(w - q * per_q), g = rem / (int)per_g, r2 = rem - g * (int)per_g;
+        const int x = r2 / ntile, y0 = (r2 - x * ntile) * US_W, h = nv - y0 < US_W ? nv - y0 : US_W;
         int o[3];
         decode_tri3(q, nocc, o[0], o[1], o[2]);
         const int xyz[3] = {o[perm3(g, 0)], o[perm3(g, 1)], o[perm3(g, 2)]};
@@ -1785,40 +1789,54 @@ __global__ void __launch_bounds__(256, 3) k_unpack_rows(const double *__restrict
         const int pi = cs == 3 ? 4 : (cs == 4 ? 3 : cs);  // U[o][u] = C[u[perm3(pi, 0)], u[perm3(pi, 1)], u[perm3(pi, 2)]]
         const double *C = t3 + q * n3;
         double *Uo = U + (((int64_t)xyz[0] * nocc + xyz[1]) * nocc + xyz[2]) * n3;
-        const int a0 = I * TE, b0 = J * TE;
-        if (pi == 0 || pi == 2) {  // whole rows: C[a][b][:] or C[b][a][:]
-            for (int rw = warp; rw < 64; rw += 8) {
-                const int a = a0 + (rw >> 3), b = b0 + (rw & 7);
-                if (a >= nv || b >= nv) continue;
-                const double *src = C + (pi == 0 ? a * nv2 + (int64_t)b * nv : b * nv2 + (int64_t)a * nv);
-                double *dst = Uo + a * nv2 + (int64_t)b * nv;
-                for (int c = lane; c < nv; c += 32) dst[c] = __ldg(src + c);
+        // x is a for pi = 0, 1, 4 (rows U[x][y][:]) and b for 2, 3, 5 (rows U[y][x][:])
+        const bool xa = pi == 0 || pi == 1 || pi == 4;
+        const int64_t ostep = xa ? nv : nv2;  // output row y0 + j at Uo + obase + j * ostep
+        const int64_t obase = xa ? x * nv2 + (int64_t)y0 * nv : (int64_t)y0 * nv2 + x * nv;
+        if (pi == 0 || pi == 2) {  // whole rows: C[x][y][:] (pi 0: U[x][y] = C[x][y]; pi 2: U[y][x] = C[x][y])
+            const double *src = C + x * nv2 + (int64_t)y0 * nv;
+            for (int j = warp; j < h; j += 16) {
+                double v[2][4];
+#pragma unroll
+                for (int e = 0; e < 2; e++) {
+                    const bool ok = j + 8 * e < h;
+#pragma unroll
+                    for (int m = 0; m < 4; m++) {
+                        const int c = lane + 32 * m;
+                        v[e][m] = ok && c < nv ? __ldg(src + (int64_t)(j + 8 * e) * nv + c) : 0.0;
+                    }
+                }
+#pragma unroll
+                for (int e = 0; e < 2; e++) {
+                    if (j + 8 * e >= h) continue;
+                    double *dst = Uo + obase + (int64_t)(j + 8 * e) * ostep;
+#pragma unroll
+                    for (int m = 0; m < 4; m++) {
+                        const int c = lane + 32 * m;
+                        if (c < nv) dst[c] = v[e][m];
+                    }
+                }
             }
             continue;
         }
-        // columns: C position (a, c, b) for pi = 1, (b, c, a) for 3, (c, a, b) for 4, (c, b, a) for 5;
-        // the copies run along C's last axis (b for 1 and 4, a for 3 and 5)
-        for (int e = threadIdx.x; e < nv * 64; e += blockDim.x) {
-            const int c = e >> 6, r = (e >> 3) & 7, t = e & 7;
-            const bool bfast = pi == 1 || pi == 4;
-            const int al = bfast ? r : t, bl = bfast ? t : r, a = a0 + al, b = b0 + bl;
-            if (a >= nv || b >= nv) continue;
-            const int64_t off = pi == 1 ? a * nv2 + (int64_t)c * nv + b
-                              : pi == 3 ? b * nv2 + (int64_t)c * nv + a
-                              : pi == 4 ? c * nv2 + (int64_t)a * nv + b
-                                        : c * nv2 + (int64_t)b * nv + a;
-            cp_async8(ur_sm + c * UR_PITCH + al * 8 + bl, C + off);
-        }
+        // columns: U[x][y][c] = C[x][c][y] (pi 1), C[c][x][y] (pi 4); U[y][x][c] = C[x][c][y] (pi 3),
+        // C[c][x][y] (pi 5)
+        const int64_t sc = (pi == 1 || pi == 3) ? nv : nv2, sx = (pi == 1 || pi == 3) ? nv2 : nv;
+        const double *src = C + x * sx + y0;
+        for (int c = warp; c < nv; c += 8)
+            if (lane < h) cp_async8(T + c * US_PITCH + lane, src + c * sc + lane);
         cp_async_commit();
         cp_async_wait<0>();
         __syncthreads();
-        for (int rw = warp; rw < 64; rw += 8) {
-            const int al = rw >> 3, bl = rw & 7, a = a0 + al, b = b0 + bl;
-            if (a >= nv || b >= nv) continue;
-            double *dst = Uo + a * nv2 + (int64_t)b * nv;
-            for (int c = lane; c < nv; c += 32) dst[c] = ur_sm[c * UR_PITCH + rw];
+        for (int j = warp; j < h; j += 8) {
+            double *dst = Uo + obase + (int64_t)j * ostep;
+#pragma unroll
+            for (int m = 0; m < 4; m++) {
+                const int c = lane + 32 * m;
+                if (c < nv) dst[c] = T[c * US_PITCH + j];
+            }
         }
-        __syncthreads();  // the tile is refilled by the next item
+        __syncthreads();  // the strip is refilled by the next item
     }
 }
 
@@ -1832,16 +1850,17 @@ extern "C" int dcc_t3_unpack_all(const double *t3, double *U, int64_t nocc, int6
     const int64_t nblocks = nocc * (nocc + 1) * (nocc + 2) / 6;
     int ntile = (int)ceil_div(nvir, TE);
     {
-        // whole rows, columns through a staged tile (k_unpack_rows): at nocc=10 / nvir=90 3.78 ms
-        // against 5.13 ms for the TMA row bands below, and the kernel for odd nvir
-        const size_t rsm = (size_t)nvir * UR_PITCH * sizeof(double);
-        if (nvir <= 104 && nocc * nocc * nocc < (1ll << 31) && nblocks < (1ll << 31) && nocc <= 1290) {
-            int dev = 0, nsm = 148;
+        // whole rows, columns through staged strips (k_unpack_strips); the kernel for odd nvir
+        if (nvir <= US_MAXNV && nocc * nocc * nocc < (1ll << 31) && nblocks < (1ll << 31) && nocc <= 1290) {
+            const int nst = (int)ceil_div(nvir, US_W);
+            int dev = 0, nsm = 148, per_sm = 1;
             if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-            const int64_t nwork = nblocks * 6 * (int64_t)ntile * ntile, cap = (int64_t)nsm * 3;
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_unpack_strips, 256, 0) != cudaSuccess ||
+                per_sm < 1)
+                per_sm = 1;
+            const int64_t nwork = nblocks * 6 * nvir * (int64_t)nst, cap = (int64_t)nsm * per_sm;
             const unsigned grid = (unsigned)(nwork < cap ? nwork : cap);
-            cudaFuncSetAttribute(k_unpack_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rsm);
-            k_unpack_rows<<<grid, 256, rsm, as_stream(stream)>>>(t3, U, nblocks, (int)nocc, (int)nvir, ntile);
+            k_unpack_strips<<<grid, 256, 0, as_stream(stream)>>>(t3, U, nblocks, (int)nocc, (int)nvir, nst);
             return launch_status("t3_unpack_all");
         }
     }
@@ -2284,6 +2303,7 @@ namespace dcc {
 // in shared memory for a pair of 8-wide index tiles (a in I, b in J) and a chunk of c.  Each warp
 // then streams output rows with coalesced loads and stores.  The slots are summed in the order of
 // the orbit-tile kernels (p = 0..5, one fma each), so the result is theirs bit for bit.
+constexpr int GB_PITCH = 65;  // doubles per (c) row of a staged tile: 8 x 8 + 1 (conflict-free transposed reads)
 __global__ void __launch_bounds__(256, 2) k_gather_band(const double *__restrict__ S, double *__restrict__ r3,
                                                         const int32_t *__restrict__ ijk, int64_t nblocks, int nocc,
                                                         int nv, int ntile, int cchunk, double scale, double beta) {
@@ -2321,21 +2341,45 @@ __global__ void __launch_bounds__(256, 2) k_gather_band(const double *__restrict
         cp_async_commit();
         cp_async_wait<0>();
         __syncthreads();
-        for (int rw = warp; rw < 64; rw += 8) {
-            const int al = rw >> 3, bl = rw & 7, a = a0 + al, b = b0 + bl;
-            if (a >= nv || b >= nv) continue;
-            const double *r0 = src[0] + a * nv2 + (int64_t)b * nv, *r2 = src[2] + b * nv2 + (int64_t)a * nv;
-            double *out = r3 + q * n3 + a * nv2 + (int64_t)b * nv;
-            const int ti = al * 8 + bl;
-            for (int cc = lane; cc < cn; cc += 32) {
-                const int c = c0 + cc, off = cc * GB_PITCH + ti;
-                double acc = fma(scale, __ldg(r0 + c), 0.0);
-                acc = fma(scale, T1[off], acc);
-                acc = fma(scale, __ldg(r2 + c), acc);
-                acc = fma(scale, T3[off], acc);
-                acc = fma(scale, T4[off], acc);
-                acc = fma(scale, T5[off], acc);
-                out[c] = beta == 0.0 ? acc : fma(beta, out[c], acc);
+        // two output rows per pass (al and al + 1), every global load of both (the two source
+        // rows, and the output when beta != 0; cc = lane + 32 j covers cchunk <= 64) issued
+        // before the arithmetic: up to 12 loads in flight per lane
+        for (int rw = warp; rw < 64; rw += 16) {
+            double v0[2][2], v2[2][2], vo[2][2];
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+                const int al = (rw >> 3) + h, bl = rw & 7, a = a0 + al, b = b0 + bl;
+                const bool ok = a < nv && b < nv;
+                const double *r0 = src[0] + a * nv2 + (int64_t)b * nv, *r2 = src[2] + b * nv2 + (int64_t)a * nv;
+                const double *out = r3 + q * n3 + a * nv2 + (int64_t)b * nv;
+#pragma unroll
+                for (int j = 0; j < 2; j++) {
+                    const int cc = lane + 32 * j, c = c0 + cc;
+                    const bool in = ok && cc < cn;
+                    v0[h][j] = in ? __ldg(r0 + c) : 0.0;
+                    v2[h][j] = in ? __ldg(r2 + c) : 0.0;
+                    vo[h][j] = in && beta != 0.0 ? out[c] : 0.0;
+                }
+            }
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+                const int al = (rw >> 3) + h, bl = rw & 7, a = a0 + al, b = b0 + bl;
+                if (a >= nv || b >= nv) continue;
+                double *out = r3 + q * n3 + a * nv2 + (int64_t)b * nv;
+                const int ti = al * 8 + bl;
+#pragma unroll
+                for (int j = 0; j < 2; j++) {
+                    const int cc = lane + 32 * j, c = c0 + cc;
+                    if (cc >= cn) continue;
+                    const int off = cc * GB_PITCH + ti;
+                    double acc = fma(scale, v0[h][j], 0.0);
+                    acc = fma(scale, T1[off], acc);
+                    acc = fma(scale, v2[h][j], acc);
+                    acc = fma(scale, T3[off], acc);
+                    acc = fma(scale, T4[off], acc);
+                    acc = fma(scale, T5[off], acc);
+                    out[c] = beta == 0.0 ? acc : fma(beta, vo[h][j], acc);
+                }
             }
         }
         __syncthreads();  // the tiles are refilled by the next item

@@ -32,15 +32,20 @@ def t3_spin_summation_inplace_(A, nblocks, nvir, pattern, alpha=1.0, beta=0.0):
     return A
 
 
-def t3_spin_summation(A, B, nblocks, nvir, pattern, alpha=1.0, beta=0.0):
+def t3_spin_summation(A, B, nblocks, nvir, pattern, alpha=1.0, beta=0.0, kernel=0):
     """B = beta*A + alpha*P(A) block by block, out of place (PySCF's t3_spin_summation as
-    distr_cc/rccsdtq.py:853 calls it); B may be A itself."""
+    distr_cc/rccsdtq.py:853 calls it); B may be A itself.  kernel: 0 the library's choice, or
+    1 strips (P3_201, nvir <= 104), 2 orbit tiles (an error where that kernel does not apply)."""
     A = L.as_tensor(A, f64, "A")
     B = L.as_tensor(B, f64, "B")
     if A.numel() != nblocks * nvir ** 3 or B.numel() != A.numel():
         raise ValueError("A and B must hold nblocks nvir^3 blocks")
-    L.call("dcc_t3_spin_summation", L.ptr(A), L.ptr(B), nblocks, nvir, L.pattern(pattern), float(alpha),
-           float(beta), L.stream_ptr())
+    if kernel:
+        L.call("dcc_t3_spin_summation_kernel", L.ptr(A), L.ptr(B), nblocks, nvir, L.pattern(pattern), float(alpha),
+               float(beta), int(kernel), L.stream_ptr())
+    else:
+        L.call("dcc_t3_spin_summation", L.ptr(A), L.ptr(B), nblocks, nvir, L.pattern(pattern), float(alpha),
+               float(beta), L.stream_ptr())
     return B
 
 

@@ -82,6 +82,12 @@ DCC_API int dcc_t3_unpack_p3(const double *t3, double *U, double *X, int64_t noc
 DCC_API int dcc_t3_spin_summation(const double *A, double *B, int64_t nblocks, int64_t nvir, const char *pattern,
                                   double alpha, double beta, void *stream);
 
+/* Diagnostic: dcc_t3_spin_summation through one chosen kernel: 0 the default choice, 1 strips
+ * (the patterns with p4 = 0, i.e. P3_201, at nvir <= 104), 2 orbit tiles (every pattern).
+ * DCC_ERR_UNSUPPORTED (nothing launched) where the kernel does not apply.  Same results. */
+DCC_API int dcc_t3_spin_summation_kernel(const double *A, double *B, int64_t nblocks, int64_t nvir,
+                                         const char *pattern, double alpha, double beta, int kernel, void *stream);
+
 /* B0 = 2T - T_acb - T_cba, B1 = 2T - T_bac - T_acb, B2 = B0 + T_acb - T_bac on
  * nblocks blocks.  Replaces t3_spin_summation_triple_sym_ (src/rccsdt.c:245-310). */
 DCC_API int dcc_t3_spin_summation_triple_sym(const double *A, double *B0, double *B1, double *B2, int64_t nblocks,

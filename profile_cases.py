@@ -154,17 +154,18 @@ def case_unpack(reps, nocc=10):
 def case_oddnv(reps, nocc=5, nvir=93, time=False, only=None):
     """The memory-bound T3 passes of one half-iteration at an odd nvir (no TMA: 8-byte row
     pitch), each on its own buffers: unpack t3 -> U (every ordering), X = P3_201(U) out of
-    place, P3_422(t3) out of place, P3_full(r3) in place, the S3 gather S -> r3, and (5) the
-    unpack and X in one pass (dcc_t3_unpack_p3).  With time=True
+    place, P3_422(t3) out of place, P3_full(r3) in place, the S3 gather S -> r3, (5) the
+    unpack and X in one pass (dcc_t3_unpack_p3), and the X pass through and (6) the X pass
+    through the orbit-tile kernel (the strip kernel is the default).  With time=True
     each pass is timed with CUDA events (after a 256 MB L2 flush; mean of reps) and printed with
     its algorithmic bytes and bandwidth.  only: the passes to run (indices into the list
     above, e.g. [1] for the X pass alone; buffers of the others are not allocated)."""
     from dcc import synthetic, t3_residual, _c_rccsdt
     d = synthetic.make_inputs(nocc, nvir, seed=0)
     n3, nu = d.t3.shape[0], nocc ** 3
-    only = set(range(6)) if only is None else set(only)
-    U = torch.empty((nu, nvir, nvir, nvir), dtype=torch.float64, device="cuda") if only & {0, 1, 4, 5} else None
-    X = torch.empty_like(U) if only & {1, 4, 5} else None
+    only = set(range(7)) if only is None else set(only)
+    U = torch.empty((nu, nvir, nvir, nvir), dtype=torch.float64, device="cuda") if only & {0, 1, 4, 5, 6} else None
+    X = torch.empty_like(U) if only & {1, 4, 5, 6} else None
     V = torch.empty_like(d.t3) if 2 in only else None
     r3 = torch.randn_like(d.t3) if only & {3, 4} else None
     e3, eu = n3 * nvir ** 3, nu * nvir ** 3
@@ -178,6 +179,7 @@ def case_oddnv(reps, nocc=5, nvir=93, time=False, only=None):
             r3, d.ijk, nvir, 0.0, [(X, 1.0, t3_residual.full_strides(nocc, nvir), t3_residual.ALL_S3)], nocc=nocc),
          8 * (6 * e3 + e3)),
         ("unpack+X one pass", lambda: _c_rccsdt.t3_unpack_p3(d.t3, U, X, nocc, nvir, "P3_201"), 8 * (e3 + 2 * eu)),
+        ("X by orbit tiles", lambda: _c_rccsdt.t3_spin_summation(U, X, nu, nvir, "P3_201", kernel=2), 16 * eu),
     ]
     flush = torch.empty(256 << 20, dtype=torch.int8, device="cuda") if time else None
     for n, (name, run, nbytes) in enumerate(passes):

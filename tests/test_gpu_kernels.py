@@ -57,11 +57,45 @@ def test_t3_spin_sum(C, oracle, nvir, pattern):
     assert c3.symmetrize_status() == 0
 
 
-@pytest.mark.parametrize("nvir", [1, 5, 10, 13, 30, 93])
+@pytest.mark.parametrize("nvir", [1, 2, 5, 10, 13, 30, 93, 104, 105])
+@pytest.mark.parametrize("kernel", [1, 2])
+def test_t3_spin_sum_kernels(C, oracle, nvir, kernel):
+    """Each kernel of the out-of-place P3_201 (1 strips, 2 orbit tiles) bit-exact with the oracle
+    where it applies; the strip kernel refuses larger nvir and the patterns with a p4 term and
+    launches nothing."""
+    c3 = C[0]
+    rng = np.random.default_rng(200 + nvir)
+    nblk = 2 if nvir >= 90 else 3
+    applies = kernel == 2 or nvir <= 104
+    for alpha, beta in [(1.0, 0.0), (-1.0 / 6.0, 1.0)]:
+        A = rng.standard_normal((nblk,) + (nvir,) * 3)
+        want = oracle.t3_spin_sum(A.copy(), nvir, "P3_201", alpha, beta)
+        d, out = dev(A), torch.full(A.shape, float("nan"), dtype=torch.float64, device="cuda")
+        if not applies:
+            with pytest.raises(RuntimeError, match="does not apply"):
+                c3.t3_spin_summation(d, out, nblk, nvir, "P3_201", alpha, beta, kernel=kernel)
+            assert torch.isnan(out).all()
+            continue
+        c3.t3_spin_summation(d, out, nblk, nvir, "P3_201", alpha, beta, kernel=kernel)
+        assert np.array_equal(host(out), want)
+        assert np.array_equal(host(d), A)
+    # the patterns with a p4 term run through the orbit kernel alone
+    A = rng.standard_normal((nblk,) + (nvir,) * 3)
+    d, out = dev(A), torch.empty(A.shape, dtype=torch.float64, device="cuda")
+    if kernel == 2:
+        c3.t3_spin_summation(d, out, nblk, nvir, "P3_422", 1.0, 0.0, kernel=kernel)
+        assert np.array_equal(host(out), oracle.t3_spin_sum(A.copy(), nvir, "P3_422", 1.0, 0.0))
+    else:
+        with pytest.raises(RuntimeError, match="does not apply"):
+            c3.t3_spin_summation(d, out, nblk, nvir, "P3_422", 1.0, 0.0, kernel=kernel)
+    assert c3.symmetrize_status() == 0
+
+
+@pytest.mark.parametrize("nvir", [1, 5, 10, 13, 30, 90, 93, 106])
 @pytest.mark.parametrize("pattern", P3)
 def test_t3_spin_sum_out_of_place(C, oracle, nvir, pattern):
-    """B = beta*A + alpha*P(A) out of place (the TMA kernel at even nvir, the cp.async kernel at
-    odd nvir): bit-exact with the oracle, and A untouched."""
+    """B = beta*A + alpha*P(A) out of place (the library's choice of kernel: strips for P3_201 up
+    to nvir = 104, orbit tiles otherwise): bit-exact with the oracle, and A untouched."""
     c3 = C[0]
     rng = np.random.default_rng(100 + nvir)
     nblk = 2 if nvir >= 90 else 4
