@@ -204,6 +204,64 @@ def case_oddnv(reps, nocc=5, nvir=93, time=False, only=None):
     assert _c_rccsdt.symmetrize_status() == 0
 
 
+def case_splits(reps, nocc=8, nvir=93, time=False):
+    """The operand splits of a bf16x3 half-iteration that read the full-layout T3 buffers: the
+    two U pieces of the OO GEMMs' B operand and the U operand of the W_oooo GEMM (residual),
+    and the per-x pieces of X for the feedback's two column layouts.  With time=True each is
+    timed with CUDA events (256 MB L2 flush before each; mean of reps) and printed with its
+    algorithmic bytes (8 read + 4 written per element, the pieces' padding included)."""
+    from dcc import contract, t3_feedback, t3_residual
+    R = t3_residual.T3Residual(nocc, nvir, "bf16x3", device="cuda", with_oo=True)
+    R.U.normal_()
+    c = contract
+    runs = []
+    for i, (name, fm, fk) in enumerate(R.plan["oo"]["b"]):
+        k = R.oob.pieces[i][1]
+        runs.append((f"OO B piece {i}", lambda i=i, fm=fm, fk=fk: R.oob.fill_piece(i, R.U, fm, fk),
+                     R.oob.M * (8 * k + 4 * R.oob.pieces[i][2])))
+    n = nocc * nvir ** 3
+    Uf = R.U.view(nocc * nocc, n)
+
+    def woo():
+        k0 = 0
+        for i, kk in enumerate(R.woo_pieces):
+            R.woob.fill_piece(i, Uf[k0:k0 + kk], c.lin(1), c.lin(n))
+            k0 += kk
+    runs.append(("W_oooo B", woo, n * (8 * nocc * nocc + 4 * R.woob.Kp)))
+    F = t3_feedback.SplitFeedback(nocc, nvir, "bf16x3")
+    Xf = R.U.reshape(-1)
+    for name in ("vovv", "ooov"):
+        tm = F.terms[name]
+        pieces, ks, Kp = F.plans[name]
+        R1, R2, S1, S2 = tm["kin"]
+        B = F._operand(tm["N"], ks, Kp, F._xhi, F._xlo)
+
+        def xs(B=B, tm=tm, pieces=pieces, R1=R1, R2=R2, S1=S1, S2=S2):
+            for i, (x0, xc) in enumerate(pieces):
+                B.fill_piece(i, Xf[x0 * F.Sx:], tm["fn"], c.three(R1, R2, F.Sx, S1, S2))
+        runs.append((f"feedback X ({name})", xs, tm["N"] * (8 * nocc * R1 * R2 + 4 * Kp)))
+    flush = torch.empty(256 << 20, dtype=torch.int8, device="cuda") if time else None
+    for name, run, nbytes in runs:
+        if time:
+            run()  # first launch (module load) untimed
+        ts = []
+        for r in range(reps):
+            if time:
+                flush.fill_(r & 127)
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record()
+            run()
+            if time:
+                e1.record()
+                e1.synchronize()
+                ts.append(e0.elapsed_time(e1))
+        torch.cuda.synchronize()
+        if time:
+            ms = sum(ts) / len(ts)
+            print(f"{name:22s} nocc={nocc} nvir={nvir}: {ms:8.3f} ms  {nbytes / 1e9:7.3f} GB  "
+                  f"{nbytes / ms * 1e-6:7.0f} GB/s")
+
+
 def case_qgroup(reps, nocc=10):
     """One (Q) task group (a, b, c blocks 0..3, d over all 90 virtuals) on the split path:
     two grouped splits, two grouped GEMMs and the group epilogue per repetition."""
@@ -355,12 +413,12 @@ def case_t4(reps, kind="bf16x3", breakdown=False):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("case", choices=["gemm", "p3", "update", "q", "gather", "xgemm", "oogemm", "unpack", "qgroup",
-                                         "t4", "t3iter", "qsample", "t3half", "oddnv"])
+                                         "t4", "t3iter", "qsample", "t3half", "oddnv", "splits"])
     ap.add_argument("--kind", default="bf16x3")
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--nocc", type=int, default=None, help="occupied orbitals (xgemm, oogemm, gather, unpack)")
     ap.add_argument("--nvir", type=int, default=None,
-                    help="virtual orbitals (default 90; 93 for oddnv and t3half)")
+                    help="virtual orbitals (default 90; 93 for oddnv, splits and t3half)")
     ap.add_argument("--op", default="p3", choices=["p3", "p3_422", "roundtrip", "triple", "transpose"],
                     help="p3 case: which symmetrizer")
     ap.add_argument("--time", action="store_true", help="p3 case: print CUDA-event timings")
@@ -381,6 +439,8 @@ def main():
     elif a.case == "oddnv":
         case_oddnv(a.reps, a.nocc or 5, a.nvir or 93, a.time,
                    [int(x) for x in a.passes.split(",")] if a.passes else None)
+    elif a.case == "splits":
+        case_splits(a.reps, a.nocc or 8, a.nvir or 93, a.time)
     elif a.case == "t3half":
         case_t3half(a.reps, a.nocc or 15, a.nvir or 93, a.kind, a.breakdown)
     elif a.case == "qsample":
