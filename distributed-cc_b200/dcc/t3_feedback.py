@@ -50,9 +50,14 @@ def r1_add_t3_(r1, t1_eris, t3, ijk, nocc, oovv=None, V=None):
     E = oovv if oovv is not None else eris_slices(t1_eris, None, nocc)["oovv"]
     il, jl, kl = ijk[:, 0].long(), ijk[:, 1].long(), ijk[:, 2].long()
     c1, c2, c3 = _case_coefficients(ijk)
-    Ra = torch.einsum('qbc,qabc->qa', E[jl, kl], V) * c1[:, None]
-    Rb = torch.einsum('qbc,qbac->qa', E[il, kl], V) * c2[:, None]
-    Rc = torch.einsum('qbc,qbca->qa', E[il, jl], V) * c3[:, None]
+    # three batched matrix-vector products that read V in place (no permuted copy of V):
+    # Ra[q,a] = sum_bc E[q,b,c] V[q,a,b,c]; Rb[q,a] = sum_b (V[q,b] @ E[q,b])[a];
+    # Rc[q,a] = (E[q] as a row) @ V[q] as [(b,c)][a]
+    n = V.shape[0]
+    Ra = torch.bmm(V.view(n, nvir, nvir * nvir), E[jl, kl].reshape(n, nvir * nvir, 1)).view(n, nvir)
+    Rb = torch.bmm(V.view(n * nvir, nvir, nvir), E[il, kl].reshape(n * nvir, nvir, 1)).view(n, nvir, nvir).sum(1)
+    Rc = torch.bmm(E[il, jl].reshape(n, 1, nvir * nvir), V.view(n, nvir * nvir, nvir)).view(n, nvir)
+    Ra, Rb, Rc = Ra * c1[:, None], Rb * c2[:, None], Rc * c3[:, None]
     eye = torch.eye(nocc, dtype=f64, device=t3.device)
     r1 += eye[il].t() @ Ra + eye[jl].t() @ Rb + eye[kl].t() @ Rc
     return r1
@@ -139,15 +144,21 @@ class SplitFeedback:
         W_vooo[a,m,y,z] += sum_{x,e,d} E_oovv[m,x,d,e] X[x,y,z,e,a,d]
         W_vvvo[a,b,d,y] -= sum_{x,z,e} E_oovv[z,x,d,e] X[x,y,z,e,b,a]
 
-    The small E slice is the GEMM's row operand (at most nvir rows, permuted once so that
-    its contraction index is contiguous) and X the column operand; each contraction runs
-    over (x, two more indices) in the order that keeps X's contiguous index innermost.  Every
-    value of x is its own piece of the split operands (starting on a k-block) and its own
-    GEMM: the tensor cores accumulate in FP32 over the other two indices only, and the
-    epilogue sums the nocc partial results in FP64 -- one FP32 accumulation over the whole
-    contraction (nocc nvir^2 terms at nvir ~ 90) lost four digits to cancellation.  One split
-    buffer of X (nocc^2 nvir x nocc nvir^2 elements, two 2-byte pieces each in bf16x3)
-    serves the four strings in turn.  The f_ov term of r2 (K = nvir) stays an FP64 product."""
+    The small E slices are the GEMM's row operand (permuted once so that the contraction index
+    is contiguous) and X the column operand; each contraction runs over (x, two more indices) in
+    the order that keeps X's contiguous index innermost.  The strings that read X the same way
+    (vovv with W_vooo, ooov with W_vvvo: the same columns and contraction over X's axes) are one
+    GEMM: their E slices stacked as the rows (nvir + nocc rows, one 128-row tile, so the padded
+    MMA rows and the reads of X are paid once for both).  Every value of x is its own piece of
+    the split operands (starting on a k-block) and its own GEMM: the tensor cores accumulate in
+    FP32 over the other two indices only, and the epilogue sums the nocc partial results in FP64
+    -- one FP32 accumulation over the whole contraction (nocc nvir^2 terms at nvir ~ 90) lost
+    four digits to cancellation.  The partial results accumulate in an FP64 scratch T[row][column]
+    (contiguous, so the epilogue writes whole rows; W_vvvo's own layout puts every element of an
+    epilogue row in its own sector), and each string's rows are added to its output once, with a
+    permutation.  One split buffer of X (nocc^2 nvir x nocc nvir^2 elements, two 2-byte pieces
+    each in bf16x3) serves the two GEMMs in turn.  The f_ov term of r2 (K = nvir) stays an FP64
+    product."""
 
     def __init__(self, nocc, nvir, precision, device="cuda"):
         from . import contract
@@ -159,29 +170,31 @@ class SplitFeedback:
         self.Sx = Sx
         c = contract
         # N, X column map, inner contraction digits of X (R1, R2, S1, S2) after x, E slice and
-        # the permutation that puts it in [row][x][k1][k2] order, output maps, alpha, output
+        # the permutation that puts it in [row][x][k1][k2] order, the string's block of the
+        # scratch as [row][column digits] and its permutation to the output's index order,
+        # alpha, output
         self.terms = {
-            # r2 vovv: columns (y,z,b); K = (x, d, a); E_vovv[c,x,a,d] -> [c][x][d][a]
+            # r2 vovv: rows c, columns (y,z,b); K = (x, d, a); E_vovv[c,x,a,d] -> [c][x][d][a]
             "vovv": dict(N=no * no * nv, fn=c.three(no, nv, Sy, Sz, Sq), kin=(nv, nv, Sp, 1), M=nv,
-                         src="vovv", perm=(0, 1, 3, 2), orow=c.lin(1),
-                         ocol=c.three(no, nv, no * nv * nv, nv * nv, nv), alpha=1.0, out="r2"),
-            # r2 ooov: columns (y,b,c); K = (x, z, a); E_ooov[z,x,l,a] -> [l][x][z][a]
+                         src="vovv", perm=(0, 1, 3, 2), tview=(nv, no, no, nv), tperm=(1, 2, 3, 0),
+                         alpha=1.0, out="r2"),
+            # r2 ooov: rows l, columns (y,b,c); K = (x, z, a); E_ooov[z,x,l,a] -> [l][x][z][a]
             "ooov": dict(N=no * nv * nv, fn=c.three(nv, nv, Sy, Sq, 1), kin=(no, nv, Sz, Sp), M=no,
-                         src="ooov", perm=(2, 1, 0, 3), orow=c.lin(nv * nv),
-                         ocol=c.three(nv, nv, no * nv * nv, nv, 1), alpha=-1.0, out="r2"),
-            # W_vooo: columns (y,z,a); K = (x, e, d); E_oovv[m,x,d,e] -> [m][x][e][d]
+                         src="ooov", perm=(2, 1, 0, 3), tview=(no, no, nv, nv), tperm=(1, 0, 2, 3),
+                         alpha=-1.0, out="r2"),
+            # W_vooo: rows m, columns (y,z,a); K = (x, e, d); E_oovv[m,x,d,e] -> [m][x][e][d]
             "wvooo": dict(N=no * no * nv, fn=c.three(no, nv, Sy, Sz, Sq), kin=(nv, nv, Sp, 1), M=no,
-                          src="oovv", perm=(0, 1, 3, 2), orow=c.lin(no * no),
-                          ocol=c.three(no, nv, no, 1, no ** 3), alpha=1.0, out="W_vooo"),
-            # W_vvvo: columns (y,b,a); K = (x, z, e); E_oovv[z,x,d,e] -> [d][x][z][e]
+                          src="oovv", perm=(0, 1, 3, 2), tview=(no, no, no, nv), tperm=(3, 0, 1, 2),
+                          alpha=1.0, out="W_vooo"),
+            # W_vvvo: rows d, columns (y,b,a); K = (x, z, e); E_oovv[z,x,d,e] -> [d][x][z][e]
             "wvvvo": dict(N=no * nv * nv, fn=c.three(nv, nv, Sy, Sq, 1), kin=(no, nv, Sz, Sp), M=nv,
-                          src="oovv", perm=(2, 1, 0, 3), orow=c.lin(no),
-                          ocol=c.three(nv, nv, 1, no * nv, no * nv * nv), alpha=-1.0, out="W_vvvo"),
+                          src="oovv", perm=(2, 1, 0, 3), tview=(nv, no, nv, nv), tperm=(3, 2, 0, 1),
+                          alpha=-1.0, out="W_vvvo"),
         }
         dt = torch.bfloat16 if self.kind == 0 else torch.float32
         self.blk = contract._KBLK[self.kind]
         self.plans = {}
-        xmax = emax = 0
+        xmax = 0
         for name, tm in self.terms.items():
             R1, R2, S1, S2 = tm["kin"]
             pieces = [(x, 1) for x in range(no)]  # one piece (and one GEMM) per value of x
@@ -189,11 +202,15 @@ class SplitFeedback:
             w = contract.padded_k(R1 * R2, self.kind)
             Kp = w * no
             self.plans[name] = (pieces, ks, Kp)
-            xmax, emax = max(xmax, tm["N"] * Kp), max(emax, tm["M"] * Kp)
+            xmax = max(xmax, tm["N"] * Kp)
+        # the row operand and the scratch hold both strings of a group: at most nvir + nocc rows
+        emax = (nv + no) * max(p[2] for p in self.plans.values())
+        tmax = (nv + no) * max(tm["N"] for tm in self.terms.values())
         self._xhi = torch.empty(xmax, dtype=dt, device=device)
         self._xlo = torch.empty(xmax, dtype=dt, device=device)
         self._ehi = torch.empty(emax, dtype=dt, device=device)
         self._elo = torch.empty(emax, dtype=dt, device=device)
+        self._scratch = torch.empty(tmax, dtype=f64, device=device)
         self.status = torch.zeros(1, dtype=torch.int32, device=device)
 
     def _operand(self, rows, ks, Kp, hi, lo):
@@ -204,9 +221,8 @@ class SplitFeedback:
     def run(self, X, E, outs, names=("vovv", "ooov", "wvooo", "wvvvo")):
         """outs[...] += the strings above.  X: [no,no,no,nv,nv,nv] FP64, contiguous; E: the
         slices {'vovv', 'ooov', 'oovv'} of eris_slices on the device; outs: {'r2', 'W_vooo',
-        'W_vvvo'} FP64 device tensors.  Strings that read X the same way (vovv with W_vooo,
-        ooov with W_vvvo: the same columns and contraction over X's axes) share one split
-        of X."""
+        'W_vvvo'} FP64 device tensors.  Strings that read X the same way share one split of X
+        and one GEMM per piece."""
         c = self.c
         Xf = X.reshape(-1)
         done = set()
@@ -218,18 +234,24 @@ class SplitFeedback:
                      and self.terms[n]["kin"] == tm["kin"] and self.terms[n]["N"] == tm["N"]]
             pieces, ks, Kp = self.plans[name]
             R1, R2, S1, S2 = tm["kin"]
-            B = self._operand(tm["N"], ks, Kp, self._xhi, self._xlo)
+            N = tm["N"]
+            B = self._operand(N, ks, Kp, self._xhi, self._xlo)
             for i, (x0, xc) in enumerate(pieces):
                 B.fill_piece(i, Xf[x0 * self.Sx:], tm["fn"], c.three(R1, R2, self.Sx, S1, S2))
+            # the strings' E slices stacked: [row][x][k1][k2]
+            Ep = torch.cat([E[self.terms[n]["src"]].permute(*self.terms[n]["perm"]) for n in group]).contiguous()
+            M = Ep.shape[0]
+            A = self._operand(M, ks, Kp, self._ehi, self._elo)
+            row = self.no * R1 * R2
+            for i, (x0, xc) in enumerate(pieces):
+                A.fill_piece(i, Ep[:, x0:], c.lin(row), c.lin(1))
+            T = self._scratch[:M * N].view(M, N)
+            for i, (off, _, w) in enumerate(A.pieces):
+                c.gemm_range_(A, B, T, c.lin(N), c.lin(1), 1.0, 0.0 if i == 0 else 1.0, self.status, off, w)
+            r0 = 0
             for n in group:
                 tn = self.terms[n]
-                A = self._operand(tn["M"], ks, Kp, self._ehi, self._elo)
-                Ep = E[tn["src"]].permute(*tn["perm"]).contiguous()  # [row][x][k1][k2]
-                row = self.no * R1 * R2
-                for i, (x0, xc) in enumerate(pieces):
-                    A.fill_piece(i, Ep[:, x0:], c.lin(row), c.lin(1))
-                for off, _, w in A.pieces:
-                    c.gemm_range_(A, B, outs[tn["out"]], tn["orow"], tn["ocol"], tn["alpha"], 1.0, self.status,
-                                  off, w)
+                outs[tn["out"]].add_(T[r0:r0 + tn["M"]].view(tn["tview"]).permute(*tn["tperm"]), alpha=tn["alpha"])
+                r0 += tn["M"]
                 done.add(n)
         return outs

@@ -61,7 +61,7 @@ class T3Iteration:
         dr2 = torch.zeros((no, no, nv, nv), dtype=f64, device=self.dev)
         fb.r1_add_t3_(dr1, None, t3, self.ijk, no, oovv=oovv, V=self.r3)
         # the unpack, then X = P3_201(U) (two passes: the one-pass dcc_t3_unpack_p3 measured
-        # 53.6 ms against 16.5 + 34.2 ms at nocc=15 / nvir=93)
+        # 53.6 ms against 8.0 + 8.5 ms at nocc=15 / nvir=93)
         self.res.unpack_(t3)
         self._X = fb.p3_201_all(t3, no, U=self.res.U, out=self.res.S)
         if self.sfb is None:

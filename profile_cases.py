@@ -312,7 +312,7 @@ def case_t3iter(reps, nocc, nvir, kind="bf16x3"):
           f"per iteration, peak memory {torch.cuda.max_memory_allocated() / 2**30:.1f} GiB")
 
 
-def case_t3half(reps, nocc, nvir, kind="bf16x3", breakdown=False):
+def case_t3half(reps, nocc, nvir, kind="bf16x3", breakdown=False, min_ms=1.0):
     """The bench step (the T3 half-iteration: feedback, compute_r3_tri, P3_full, divide, update,
     norms, unified DIIS; bench.Workload) at a given shape: three warm-up steps, then `reps`
     steps timed with CUDA events.  With breakdown, one more step under torch.profiler prints
@@ -338,10 +338,10 @@ def case_t3half(reps, nocc, nvir, kind="bf16x3", breakdown=False):
     print(f"t3half {kind} nocc={nocc} nvir={nvir}: {e0.elapsed_time(e1) / max(reps, 1):.2f} ms per step, "
           f"peak memory {torch.cuda.max_memory_allocated() / 2**30:.1f} GiB")
     if breakdown:
-        _breakdown(lambda: w.step(it))
+        _breakdown(lambda: w.step(it), min_ms=min_ms)
 
 
-def _breakdown(step, top=40):
+def _breakdown(step, top=40, min_ms=1.0):
     """One more `step` under torch.profiler: the device time and launch count of every kernel
     name (this library's and cuBLAS's / torch's), largest first."""
     from torch.profiler import profile, ProfilerActivity
@@ -357,6 +357,13 @@ def _breakdown(step, top=40):
     print(f"breakdown: {total:.2f} ms of kernels in one step, {sum(n for n, _ in tot.values())} launches")
     for name, (n, t) in sorted(tot.items(), key=lambda kv: -kv[1][1])[:top]:
         print(f"  {t:9.3f} ms {100 * t / total:5.1f} % x{n:<4d} {name[:150]}")
+    # the launches of min_ms or more, in launch order
+    seq = [ev for ev in prof.events() if ev.device_type == torch.autograd.DeviceType.CUDA]
+    seq.sort(key=lambda ev: ev.time_range.start)
+    print(f"launches of {min_ms} ms or more, in order:")
+    for i, ev in enumerate(seq):
+        if ev.device_time_total >= 1000 * min_ms:
+            print(f"  #{i:<4d} {ev.device_time_total / 1e3:8.3f} ms  {ev.name[:70]}")
 
 
 def case_qsample(nocc, nvir, kind="bf16x3", ngroups=12, blksize=4, dchunk=None):
@@ -424,6 +431,7 @@ def main():
     ap.add_argument("--time", action="store_true", help="p3 case: print CUDA-event timings")
     ap.add_argument("--dchunk", type=int, default=None, help="qsample case: d-chunk of the split path")
     ap.add_argument("--breakdown", action="store_true", help="t3half / t4 case: per-kernel device times")
+    ap.add_argument("--min-ms", type=float, default=1.0, help="t3half breakdown: list the launches this long or longer")
     ap.add_argument("--passes", default=None, help="oddnv case: comma-separated pass indices (default all)")
     a = ap.parse_args()
     if a.case == "gemm":
@@ -442,7 +450,7 @@ def main():
     elif a.case == "splits":
         case_splits(a.reps, a.nocc or 8, a.nvir or 93, a.time)
     elif a.case == "t3half":
-        case_t3half(a.reps, a.nocc or 15, a.nvir or 93, a.kind, a.breakdown)
+        case_t3half(a.reps, a.nocc or 15, a.nvir or 93, a.kind, a.breakdown, a.min_ms)
     elif a.case == "qsample":
         case_qsample(a.nocc or 10, a.nvir or 90, a.kind, dchunk=a.dchunk)
     elif a.case in ("gather", "xgemm", "oogemm", "unpack", "qgroup"):
