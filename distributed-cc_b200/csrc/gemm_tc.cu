@@ -575,9 +575,9 @@ __device__ __forceinline__ void split_tile_coords(const SplitArgs &a, int64_t nt
 }
 
 // Persistent: warp w of CTA c takes tiles c * SP_WARPS + w, + gridDim.x * SP_WARPS, ...
-template <int KIND>
+template <int KIND, typename S>
 __global__ void __launch_bounds__(32 * SP_WARPS, KIND == 0 ? 6 : 3)
-    k_split(const double *__restrict__ src, SplitArgs a) {
+    k_split(const S *__restrict__ src, SplitArgs a) {
     extern __shared__ __align__(16) unsigned char sp_raw[];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     auto *tile = reinterpret_cast<typename SplitWord<KIND>::T *>(sp_raw) + w * SP_TM * SP_PITCH;
@@ -1031,24 +1031,27 @@ static unsigned split_grid(int64_t ntiles, int kind) {
     return (unsigned)(nwarp_blocks < 148 * per_sm ? nwarp_blocks : 148 * per_sm);  // persistent
 }
 
-static int split_operand(const double *src, void *hi, void *lo, int64_t M, int64_t K, int64_t kw, int64_t ld,
+// S: the source type (double, or float for the FP32 copies of T3 in the split precisions; a
+// float's pieces are those of the same value as a double)
+template <typename S>
+static int split_operand(const S *src, void *hi, void *lo, int64_t M, int64_t K, int64_t kw, int64_t ld,
                          int64_t k0, const int64_t *maps, bool four, int kind, void *stream) {
     clear_error();
     DCC_REQUIRE(kind == 0 || kind == 1, DCC_ERR_UNSUPPORTED, "split kind must be 0 (bf16) or 1 (tf32)");
     if (M == 0 || kw == 0) return DCC_OK;
     DCC_REQUIRE(src, DCC_ERR_NULL, "NULL buffer");
     SplitArgs a;
-    int rc = split_args(hi, lo, M, K, kw, ld, k0, maps, four, 0, a);
+    int rc = split_args(hi, lo, M, K, kw, ld, k0, maps, four, sizeof(S) == 4 ? 1 : 0, a);
     if (rc) return rc;
     const int64_t ntiles = a.nty * ((kw + SP_TK - 1) / SP_TK);
     const unsigned grid = split_grid(ntiles, kind);
     const size_t smem = split_smem(kind);
     if (kind == 0) {
-        cudaFuncSetAttribute(k_split<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        k_split<0><<<grid, 32 * SP_WARPS, smem, as_stream(stream)>>>(src, a);
+        cudaFuncSetAttribute(k_split<0, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        k_split<0, S><<<grid, 32 * SP_WARPS, smem, as_stream(stream)>>>(src, a);
     } else {
-        cudaFuncSetAttribute(k_split<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        k_split<1><<<grid, 32 * SP_WARPS, smem, as_stream(stream)>>>(src, a);
+        cudaFuncSetAttribute(k_split<1, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        k_split<1, S><<<grid, 32 * SP_WARPS, smem, as_stream(stream)>>>(src, a);
     }
     return launch_status("split_operand");
 }
@@ -1124,6 +1127,11 @@ extern "C" int dcc_split_operand_at(const double *src, void *hi, void *lo, int64
 
 extern "C" int dcc_split_operand_at4(const double *src, void *hi, void *lo, int64_t M, int64_t K, int64_t kw,
                                      int64_t ld, int64_t k0, const int64_t *map14, int kind, void *stream) {
+    return split_operand(src, hi, lo, M, K, kw, ld, k0, map14, true, kind, stream);
+}
+
+extern "C" int dcc_split_operand_at4_f32(const float *src, void *hi, void *lo, int64_t M, int64_t K, int64_t kw,
+                                         int64_t ld, int64_t k0, const int64_t *map14, int kind, void *stream) {
     return split_operand(src, hi, lo, M, K, kw, ld, k0, map14, true, kind, stream);
 }
 

@@ -100,6 +100,13 @@ __device__ __forceinline__ void cp_async8(double *smem, const double *gmem) {
     unsigned s = (unsigned)__cvta_generic_to_shared(smem);
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem));
 }
+__device__ __forceinline__ void cp_async4(float *smem, const float *gmem) {
+    unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem));
+}
+// one element, by its size
+__device__ __forceinline__ void cp_async_el(double *smem, const double *gmem) { cp_async8(smem, gmem); }
+__device__ __forceinline__ void cp_async_el(float *smem, const float *gmem) { cp_async4(smem, gmem); }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
 template <int N>
 __device__ __forceinline__ void cp_async_wait() {
@@ -1108,9 +1115,12 @@ namespace dcc {
 // arithmetic is the orbit kernel's with its p4 term (0 x the second half) left out: equal results
 // up to the sign of a zero.
 constexpr int SP3_W = 32, SP3_PITCH = 33, SP3_MAXNV = 104;
-__global__ void __launch_bounds__(256, 4) k_p3_strips(const double *__restrict__ A, double *__restrict__ B,
+// T: the storage type of A and B (double; float for the FP32 copies of the split precisions,
+// whose values the arithmetic takes exactly as doubles, rounding the result once)
+template <typename T>
+__global__ void __launch_bounds__(256, 4) k_p3_strips(const T *__restrict__ A, T *__restrict__ B,
                                                       int64_t nblocks, int nv, int ntile, P3Coef k) {
-    __shared__ double S[SP3_MAXNV * SP3_PITCH];  // S[c][s] = A[c][b][a0 + s]
+    __shared__ T S[SP3_MAXNV * SP3_PITCH];  // S[c][s] = A[c][b][a0 + s]
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int64_t n3 = (int64_t)nv * nv * nv, nv2 = (int64_t)nv * nv;
     const int64_t per_blk = (int64_t)nv * ntile, nwork = nblocks * per_blk;
@@ -1118,31 +1128,31 @@ __global__ void __launch_bounds__(256, 4) k_p3_strips(const double *__restrict__
         const int64_t blk = w / per_blk;
         const int r = (int)(w - blk * per_blk), b = r / ntile, a0 = (r - b * ntile) * SP3_W;
         const int h = nv - a0 < SP3_W ? nv - a0 : SP3_W;
-        const double *Ab = A + blk * n3;
-        double *Bb = B + blk * n3;
+        const T *Ab = A + blk * n3;
+        T *Bb = B + blk * n3;
         for (int c = warp; c < nv; c += 8)
-            if (lane < h) cp_async8(S + c * SP3_PITCH + lane, Ab + (int64_t)c * nv2 + (int64_t)b * nv + a0 + lane);
+            if (lane < h) cp_async_el(S + c * SP3_PITCH + lane, Ab + (int64_t)c * nv2 + (int64_t)b * nv + a0 + lane);
         cp_async_commit();
         cp_async_wait<0>();
         __syncthreads();
         for (int s = warp; s < h; s += 8) {
             const int a = a0 + s;
-            const double *rab = Ab + (int64_t)a * nv2 + (int64_t)b * nv, *rba = Ab + (int64_t)b * nv2 + (int64_t)a * nv;
-            double *out = Bb + (int64_t)a * nv2 + (int64_t)b * nv;
+            const T *rab = Ab + (int64_t)a * nv2 + (int64_t)b * nv, *rba = Ab + (int64_t)b * nv2 + (int64_t)a * nv;
+            T *out = Bb + (int64_t)a * nv2 + (int64_t)b * nv;
             double vab[4], vba[4];  // c = lane + 32 j covers nv <= 128
 #pragma unroll
             for (int j = 0; j < 4; j++) {
                 const int c = lane + 32 * j;
-                vab[j] = c < nv ? __ldg(rab + c) : 0.0;
-                vba[j] = c < nv ? __ldg(rba + c) : 0.0;
+                vab[j] = c < nv ? (double)__ldg(rab + c) : 0.0;
+                vba[j] = c < nv ? (double)__ldg(rba + c) : 0.0;
             }
 #pragma unroll
             for (int j = 0; j < 4; j++) {
                 const int c = lane + 32 * j;
                 if (c < nv) {
-                    const double cba = S[c * SP3_PITCH + s];
+                    const double cba = (double)S[c * SP3_PITCH + s];
                     const double tu = dadd(dadd(dmul(k.p0, vab[j]), dmul(k.p1, cba)), dmul(k.p2, vba[j]));
-                    out[c] = dadd(dmul(k.beta, vab[j]), dmul(k.alpha, dmul(k.p3, tu)));
+                    out[c] = (T)dadd(dmul(k.beta, vab[j]), dmul(k.alpha, dmul(k.p3, tu)));
                 }
             }
         }
@@ -1154,16 +1164,17 @@ __global__ void __launch_bounds__(256, 4) k_p3_strips(const double *__restrict__
 
 // The strip kernel for out-of-place P3 with p4 == 0, nvir <= 104; returns DCC_ERR_UNSUPPORTED
 // (nothing launched) where it does not apply.
-static int p3_strips_launch(const double *A, double *B, int64_t nblocks, int64_t nvir, const P3Coef &k, void *stream) {
+template <typename T>
+static int p3_strips_launch(const T *A, T *B, int64_t nblocks, int64_t nvir, const P3Coef &k, void *stream) {
     if (k.p4 != 0.0 || A == B || nvir < 1 || nvir > SP3_MAXNV) return DCC_ERR_UNSUPPORTED;
     const int ntile = (int)ceil_div(nvir, SP3_W);
     int dev = 0, nsm = 148, per_sm = 1;
     if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_p3_strips, 256, 0) != cudaSuccess || per_sm < 1)
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_p3_strips<T>, 256, 0) != cudaSuccess || per_sm < 1)
         per_sm = 1;
     const int64_t nwork = nblocks * nvir * ntile, cap = (int64_t)nsm * per_sm;
     const unsigned grid = (unsigned)(nwork < cap ? nwork : cap);
-    k_p3_strips<<<grid, 256, 0, as_stream(stream)>>>(A, B, nblocks, (int)nvir, ntile, k);
+    k_p3_strips<T><<<grid, 256, 0, as_stream(stream)>>>(A, B, nblocks, (int)nvir, ntile, k);
     return DCC_OK;
 }
 
@@ -1200,6 +1211,23 @@ extern "C" int dcc_t3_spin_summation_kernel(const double *A, double *B, int64_t 
     DCC_REQUIRE(p3_strips_launch(A, B, nblocks, nvir, k, stream) == DCC_OK, DCC_ERR_UNSUPPORTED,
                 "this kernel does not apply to the pattern or shape");
     return launch_status("P3 by strips");
+}
+
+extern "C" int dcc_t3_spin_summation_f32(const float *A, float *B, int64_t nblocks, int64_t nvir, const char *pattern,
+                                         double alpha, double beta, void *stream) {
+    clear_error();
+    P3Coef k;
+    int rc = p3_coef(pattern, alpha, beta, k);
+    if (rc) return rc;
+    DCC_REQUIRE(nblocks >= 0 && nvir >= 0, DCC_ERR_SHAPE, "negative size");
+    DCC_REQUIRE((A && B) || nblocks * nvir == 0, DCC_ERR_NULL, "NULL buffer");
+    const int64_t bytes = nblocks * nvir * nvir * nvir * (int64_t)sizeof(float);
+    DCC_REQUIRE((const char *)B + bytes <= (const char *)A || (const char *)A + bytes <= (const char *)B,
+                DCC_ERR_SHAPE, "A and B overlap");
+    if (nblocks == 0 || nvir == 0) return DCC_OK;
+    DCC_REQUIRE(p3_strips_launch(A, B, nblocks, nvir, k, stream) == DCC_OK, DCC_ERR_UNSUPPORTED,
+                "the FP32 P3 serves the patterns without a p4 term (P3_201) at nvir <= %d", SP3_MAXNV);
+    return launch_status("P3 by strips (FP32)");
 }
 
 namespace dcc {
@@ -1767,7 +1795,10 @@ namespace dcc {
 // canonical block by canonical block, so the orderings of a block reuse it from L2.
 constexpr int US_W = 32, US_PITCH = 33, US_MAXNV = 104;
 
-__global__ void __launch_bounds__(256, 4) k_unpack_strips(const double *__restrict__ t3, double *__restrict__ U,
+// UT: the type of U (double; float for the FP32 copy of the split precisions, each value rounded
+// once)
+template <typename UT>
+__global__ void __launch_bounds__(256, 4) k_unpack_strips(const double *__restrict__ t3, UT *__restrict__ U,
                                                           int64_t nblocks, int nocc, int nv, int ntile) {
     __shared__ double T[US_MAXNV * US_PITCH];  // T[c][j]
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -1788,7 +1819,7 @@ __global__ void __launch_bounds__(256, 4) k_unpack_strips(const double *__restri
         const int cs = order_case3(xyz[0], xyz[1], xyz[2], srt);
         const int pi = cs == 3 ? 4 : (cs == 4 ? 3 : cs);  // U[o][u] = C[u[perm3(pi, 0)], u[perm3(pi, 1)], u[perm3(pi, 2)]]
         const double *C = t3 + q * n3;
-        double *Uo = U + (((int64_t)xyz[0] * nocc + xyz[1]) * nocc + xyz[2]) * n3;
+        UT *Uo = U + (((int64_t)xyz[0] * nocc + xyz[1]) * nocc + xyz[2]) * n3;
         // x is a for pi = 0, 1, 4 (rows U[x][y][:]) and b for 2, 3, 5 (rows U[y][x][:])
         const bool xa = pi == 0 || pi == 1 || pi == 4;
         const int64_t ostep = xa ? nv : nv2;  // output row y0 + j at Uo + obase + j * ostep
@@ -1809,11 +1840,11 @@ __global__ void __launch_bounds__(256, 4) k_unpack_strips(const double *__restri
 #pragma unroll
                 for (int e = 0; e < 2; e++) {
                     if (j + 8 * e >= h) continue;
-                    double *dst = Uo + obase + (int64_t)(j + 8 * e) * ostep;
+                    UT *dst = Uo + obase + (int64_t)(j + 8 * e) * ostep;
 #pragma unroll
                     for (int m = 0; m < 4; m++) {
                         const int c = lane + 32 * m;
-                        if (c < nv) dst[c] = v[e][m];
+                        if (c < nv) dst[c] = (UT)v[e][m];
                     }
                 }
             }
@@ -1829,11 +1860,11 @@ __global__ void __launch_bounds__(256, 4) k_unpack_strips(const double *__restri
         cp_async_wait<0>();
         __syncthreads();
         for (int j = warp; j < h; j += 8) {
-            double *dst = Uo + obase + (int64_t)j * ostep;
+            UT *dst = Uo + obase + (int64_t)j * ostep;
 #pragma unroll
             for (int m = 0; m < 4; m++) {
                 const int c = lane + 32 * m;
-                if (c < nv) dst[c] = T[c * US_PITCH + j];
+                if (c < nv) dst[c] = (UT)T[c * US_PITCH + j];
             }
         }
         __syncthreads();  // the strip is refilled by the next item
@@ -1841,6 +1872,33 @@ __global__ void __launch_bounds__(256, 4) k_unpack_strips(const double *__restri
 }
 
 }  // namespace dcc
+
+// The strip unpack for nvir <= 104; DCC_ERR_UNSUPPORTED (nothing launched) where it does not apply.
+template <typename UT>
+static int unpack_strips_launch(const double *t3, UT *U, int64_t nocc, int64_t nvir, void *stream) {
+    const int64_t nblocks = nocc * (nocc + 1) * (nocc + 2) / 6;
+    if (nvir > US_MAXNV || nocc * nocc * nocc >= (1ll << 31) || nblocks >= (1ll << 31) || nocc > 1290)
+        return DCC_ERR_UNSUPPORTED;
+    const int nst = (int)ceil_div(nvir, US_W);
+    int dev = 0, nsm = 148, per_sm = 1;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_unpack_strips<UT>, 256, 0) != cudaSuccess || per_sm < 1)
+        per_sm = 1;
+    const int64_t nwork = nblocks * 6 * nvir * (int64_t)nst, cap = (int64_t)nsm * per_sm;
+    const unsigned grid = (unsigned)(nwork < cap ? nwork : cap);
+    k_unpack_strips<UT><<<grid, 256, 0, as_stream(stream)>>>(t3, U, nblocks, (int)nocc, (int)nvir, nst);
+    return DCC_OK;
+}
+
+extern "C" int dcc_t3_unpack_all_f32(const double *t3, float *U, int64_t nocc, int64_t nvir, void *stream) {
+    clear_error();
+    DCC_REQUIRE(nocc >= 0 && nvir >= 0, DCC_ERR_SHAPE, "negative size");
+    if (nocc == 0 || nvir == 0) return DCC_OK;
+    DCC_REQUIRE(t3 && U && (const void *)t3 != (const void *)U, DCC_ERR_NULL, "NULL or aliased buffer");
+    DCC_REQUIRE(unpack_strips_launch(t3, U, nocc, nvir, stream) == DCC_OK, DCC_ERR_UNSUPPORTED,
+                "the FP32 unpack needs nvir <= %d", US_MAXNV);
+    return launch_status("t3_unpack_all_f32");
+}
 
 extern "C" int dcc_t3_unpack_all(const double *t3, double *U, int64_t nocc, int64_t nvir, void *stream) {
     clear_error();
@@ -1851,18 +1909,7 @@ extern "C" int dcc_t3_unpack_all(const double *t3, double *U, int64_t nocc, int6
     int ntile = (int)ceil_div(nvir, TE);
     {
         // whole rows, columns through staged strips (k_unpack_strips); the kernel for odd nvir
-        if (nvir <= US_MAXNV && nocc * nocc * nocc < (1ll << 31) && nblocks < (1ll << 31) && nocc <= 1290) {
-            const int nst = (int)ceil_div(nvir, US_W);
-            int dev = 0, nsm = 148, per_sm = 1;
-            if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_unpack_strips, 256, 0) != cudaSuccess ||
-                per_sm < 1)
-                per_sm = 1;
-            const int64_t nwork = nblocks * 6 * nvir * (int64_t)nst, cap = (int64_t)nsm * per_sm;
-            const unsigned grid = (unsigned)(nwork < cap ? nwork : cap);
-            k_unpack_strips<<<grid, 256, 0, as_stream(stream)>>>(t3, U, nblocks, (int)nocc, (int)nvir, nst);
-            return launch_status("t3_unpack_all");
-        }
+        if (unpack_strips_launch(t3, U, nocc, nvir, stream) == DCC_OK) return launch_status("t3_unpack_all");
     }
     {
         // band kernel: even nvir (16-byte rows), aligned buffers, box sides <= 256, shared memory

@@ -49,6 +49,18 @@ def t3_spin_summation(A, B, nblocks, nvir, pattern, alpha=1.0, beta=0.0, kernel=
     return B
 
 
+def t3_spin_summation_f32(A, B, nblocks, nvir, pattern="P3_201", alpha=1.0, beta=0.0):
+    """B = beta*A + alpha*P(A) out of place on FP32 blocks (FP64 arithmetic on the FP32 values,
+    the result rounded once); the patterns without a p4 term, nvir <= 104."""
+    A = L.as_tensor(A, torch.float32, "A")
+    B = L.as_tensor(B, torch.float32, "B")
+    if A.numel() != nblocks * nvir ** 3 or B.numel() != A.numel():
+        raise ValueError("A and B must hold nblocks nvir^3 blocks")
+    L.call("dcc_t3_spin_summation_f32", L.ptr(A), L.ptr(B), nblocks, nvir, L.pattern(pattern), float(alpha),
+           float(beta), L.stream_ptr())
+    return B
+
+
 def t3_unpack_p3(t3, U, X, nocc, nvir, pattern="P3_201", alpha=1.0, beta=0.0):
     """U[o] = the canonical T3 unpacked to every ordered (i,j,k) o, and X[o] = beta U[o] +
     alpha P(U[o]), in one pass over the canonical blocks (U may be None: X alone)."""

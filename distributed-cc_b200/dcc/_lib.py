@@ -54,6 +54,7 @@ _SIGS = {
     "dcc_t3_spin_summation_inplace": [c_vp, c_i64, c_i64, c_str, c_dbl, c_dbl, c_vp],
     "dcc_t3_unpack_p3": [c_vp, c_vp, c_vp, c_i64, c_i64, c_str, c_dbl, c_dbl, c_vp],
     "dcc_t3_spin_summation": [c_vp, c_vp, c_i64, c_i64, c_str, c_dbl, c_dbl, c_vp],
+    "dcc_t3_spin_summation_f32": [c_vp, c_vp, c_i64, c_i64, c_str, c_dbl, c_dbl, c_vp],
     "dcc_t3_spin_summation_kernel": [c_vp, c_vp, c_i64, c_i64, c_str, c_dbl, c_dbl, c_int, c_vp],
     "dcc_t3_spin_summation_triple_sym": [c_vp, c_vp, c_vp, c_vp, c_i64, c_i64, c_vp],
     "dcc_t3_transpose_add": [c_vp, c_vp, c_i64, c_i64, c_vp],

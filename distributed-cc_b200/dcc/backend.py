@@ -290,14 +290,19 @@ def r1r2_add_t3_tri_(mycc, imds, r1, r2, t3):
 
 def intermediates_t3_add_t3_tri(mycc, imds, t3):
     """distr_cc/rccsdt.py:323-366 on the GPU; imds.W_vooo, imds.W_vvvo updated in place."""
-    from . import t3_feedback
+    from . import t3_feedback, t3_residual
     require_single_rank(mycc)
     dev = getattr(mycc, "dcc_device", "cuda")
     nocc = mycc.nocc
     it = _iteration(mycc)
     t3d = _dev(_t3_local(mycc, t3), dev)
     # X is rebuilt here: this route may be called on its own, with a T3 other than the last one
-    it._X = t3_feedback.p3_201_all(t3d, nocc, out=it.res.S)
+    # (unpacked into a temporary of the residual's U type, so the residual's U is left alone)
+    nv = t3d.shape[1]
+    U = torch.empty((nocc ** 3, nv, nv, nv), dtype=it.res.udtype, device=t3d.device)
+    t3_residual.unpack_all_(t3d, U, nocc, nv)
+    it._X = t3_feedback.p3_201_all(t3d, nocc, U=U, out=it.res.S)
+    del U
     it._dW = None
     sl = _feedback_slices(mycc, imds, dev)
     Wo, Wv = _dev(imds.W_vooo, dev), _dev(imds.W_vvvo, dev)

@@ -23,6 +23,7 @@ KIND = {"bf16x3": 0, "tf32x3": 1}
 _KBLK = {0: 64, 1: 32}
 
 _split = L.bind("dcc_split_operand_at4", [L.c_vp, L.c_vp, L.c_vp] + [L.c_i64] * 5 + [L.c_vp, L.c_int, L.c_vp])
+_split_f32 = L.bind("dcc_split_operand_at4_f32", [L.c_vp, L.c_vp, L.c_vp] + [L.c_i64] * 5 + [L.c_vp, L.c_int, L.c_vp])
 _gemm = L.bind("dcc_gemm_split3_ld4", [L.c_vp, L.c_vp, L.c_i64, L.c_vp, L.c_vp] + [L.c_i64] * 4 +
                [L.c_vp, L.c_vp, L.c_dbl, L.c_dbl, L.c_int, L.c_vp, L.c_vp])
 
@@ -74,15 +75,16 @@ def _max_offset(f, n):
             + min(R3 - 1, n - 1) * S3)
 
 
-def _check_span(t, fm, M, fk, K, name):
-    """The maps stay inside t's storage (from t's first element); t is FP64 on a CUDA device."""
-    if not isinstance(t, torch.Tensor) or t.dtype != f64:
-        raise TypeError("%s must be a float64 torch.Tensor" % name)
+def _check_span(t, fm, M, fk, K, name, dtypes=(f64,)):
+    """The maps stay inside t's storage (from t's first element); t is on a CUDA device, of one
+    of `dtypes`."""
+    if not isinstance(t, torch.Tensor) or t.dtype not in dtypes:
+        raise TypeError("%s must be a %s torch.Tensor" % (name, " or ".join(str(d) for d in dtypes)))
     if not t.is_cuda:
         raise ValueError("%s must be on a CUDA device" % name)
     if any(x < 0 for x in as4(fm)[3:] + as4(fk)[3:]):
         raise ValueError("%s: negative map strides" % name)
-    span = t.untyped_storage().nbytes() // 8 - t.storage_offset()
+    span = t.untyped_storage().nbytes() // t.element_size() - t.storage_offset()
     if M > 0 and K > 0 and _max_offset(fm, M) + _max_offset(fk, K) >= span:
         raise ValueError("%s: the address maps reach past the tensor's storage" % name)
 
@@ -123,11 +125,13 @@ class Split:
     def fill_piece(self, i, src, fm, fk):
         """Columns of piece i: dst[m][off + k] = src[fm(m) + fk(k)] (zero past the piece's K).
 
-        src may be any strided view: the maps address its storage from src's first element."""
-        _check_span(src, fm, self.M, fk, self.pieces[i][1], "src")
+        src may be any strided view: the maps address its storage from src's first element.
+        src is FP64, or FP32 (the pieces of each value as a double)."""
+        _check_span(src, fm, self.M, fk, self.pieces[i][1], "src", (f64, torch.float32))
         off, k, w = self.pieces[i]
-        L.check(_split(L.ptr(src), L.ptr(self.hi), L.ptr(self.lo), self.M, k, w, self.Kp, off, _i64x14(fm, fk),
-                       self.kind, L.stream_ptr()))
+        fn = _split_f32 if src.dtype == torch.float32 else _split
+        L.check(fn(L.ptr(src), L.ptr(self.hi), L.ptr(self.lo), self.M, k, w, self.Kp, off, _i64x14(fm, fk),
+                   self.kind, L.stream_ptr()))
         return self
 
     def fill(self, src, fm, fk):

@@ -66,8 +66,8 @@ def r1_add_t3_(r1, t1_eris, t3, ijk, nocc, oovv=None, V=None):
 def p3_201_all(t3, nocc, U=None, out=None, unpack_into=None):
     """X = P3_201 of every ordered block of the unpacked T3 [x][y][z][a][b][c].
 
-    U: the unpacked T3 when the caller has it already (unpacked here otherwise);
-    out: a buffer of U's size to hold X (a fresh one otherwise); unpack_into: a buffer that
+    U: the unpacked T3 when the caller has it already (unpacked here otherwise), FP64 or FP32
+    (X then FP32 too); out: a buffer of at least U's bytes to hold X (a fresh one otherwise); unpack_into: a buffer that
     receives the unpacked T3 in the same pass that writes X (one launch, dcc_t3_unpack_p3: X
     costs no read of U; used where the rows are not 16-byte aligned and the separate passes
     cannot use TMA)."""
@@ -79,8 +79,14 @@ def p3_201_all(t3, nocc, U=None, out=None, unpack_into=None):
     if U is None:
         U = torch.empty((nocc ** 3, nvir, nvir, nvir), dtype=f64, device=t3.device)
         unpack_all_(t3, U, nocc, nvir)
-    X = torch.empty_like(U) if out is None else out.view(U.shape)
-    _c_rccsdt.t3_spin_summation(U, X, U.shape[0], nvir, "P3_201", 1.0, 0.0)
+    if out is None:
+        X = torch.empty_like(U)
+    else:  # X in the leading bytes of out (an FP32 X takes half of an FP64 buffer)
+        X = out.view(-1).view(torch.uint8)[:U.numel() * U.element_size()].view(U.dtype).view(U.shape)
+    if U.dtype == torch.float32:
+        _c_rccsdt.t3_spin_summation_f32(U, X, U.shape[0], nvir, "P3_201", 1.0, 0.0)
+    else:
+        _c_rccsdt.t3_spin_summation(U, X, U.shape[0], nvir, "P3_201", 1.0, 0.0)
     return X.view(nocc, nocc, nocc, nvir, nvir, nvir)
 
 

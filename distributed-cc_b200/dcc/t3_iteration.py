@@ -77,12 +77,13 @@ class T3Iteration:
         return dr1, dr2
 
     def _fock_term(self, fock_ov):
-        """sum_{x,a} f[x,a] X[x,y,z,a,b,c] as [(y,z), (b,c)] (FP64)."""
+        """sum_{x,a} f[x,a] X[x,y,z,a,b,c] as [(y,z), (b,c)], summed over x in FP64 (each x's
+        product in X's type)."""
         no, nv = self.no, self.nv
         out = torch.zeros((no * no, nv * nv), dtype=f64, device=self.dev)
+        f = fock_ov.to(self._X.dtype)
         for x in range(no):
-            out += torch.matmul(fock_ov[x].view(1, 1, nv), self._X[x].reshape(no * no, nv, nv * nv)).view(no * no,
-                                                                                                          nv * nv)
+            out += torch.matmul(f[x].view(1, 1, nv), self._X[x].reshape(no * no, nv, nv * nv)).view(no * no, nv * nv)
         return out
 
     def feedback_w(self, W_vooo, W_vvvo, oovv):

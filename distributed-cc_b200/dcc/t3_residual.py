@@ -112,12 +112,26 @@ def perm_gather_(r3, ijk, nvir, beta, sources, nocc=None, status=None):
 
 
 _unpack_all = L.bind("dcc_t3_unpack_all", [L.c_vp, L.c_vp, L.c_i64, L.c_i64, L.c_vp])
+_unpack_all_f32 = L.bind("dcc_t3_unpack_all_f32", [L.c_vp, L.c_vp, L.c_i64, L.c_i64, L.c_vp])
+
+# Largest nvir with FP32 kernels for the full-layout T3 copies (the strip kernels)
+F32_MAX_NVIR = 104
 
 
 def unpack_all_(t3, U, nocc, nvir):
-    """U[(x*nocc+y)*nocc+z] = T3[x,y,z] for every ordered triple (take_t3 of all orderings)."""
-    L.check(_unpack_all(L.ptr(t3), L.ptr(U), nocc, nvir, L.stream_ptr()))
+    """U[(x*nocc+y)*nocc+z] = T3[x,y,z] for every ordered triple (take_t3 of all orderings);
+    U FP64, or FP32 (each value rounded once; nvir <= F32_MAX_NVIR)."""
+    fn = _unpack_all_f32 if U.dtype == torch.float32 else _unpack_all
+    L.check(fn(L.ptr(t3), L.ptr(U), nocc, nvir, L.stream_ptr()))
     return U
+
+
+def full_dtype(precision, nvir):
+    """Storage type of the full-layout T3 copies U and X: FP32 for the split precisions (their
+    bf16 / tf32 pieces keep 16-22 of FP32's 24 significand bits, so the split of an FP32 copy
+    equals that of the FP64 value to within the pieces' own rounding) where the FP32 kernels
+    exist, FP64 otherwise.  Half the bytes of the unpack, the X pass and the operand splits."""
+    return torch.float32 if precision != "fp64" and nvir <= F32_MAX_NVIR else f64
 
 
 def full_strides(no, nv):
@@ -202,7 +216,8 @@ class T3Residual:
         self.with_oo = with_oo
         full = (no ** 3, nv, nv, nv)
         self.S = torch.empty(full, dtype=f64, device=device)  # [i][j][k][a][b][c]
-        self.U = torch.empty(full, dtype=f64, device=device) if with_oo else None
+        self.udtype = full_dtype(precision, nvir)
+        self.U = torch.empty(full, dtype=self.udtype, device=device) if with_oo else None
         self.Ganti = None
         self.gstatus = torch.zeros(1, dtype=torch.int32, device=device)  # gather pipeline timeouts
         if precision != "fp64":
@@ -284,8 +299,11 @@ class T3Residual:
             if Wa is not None:
                 if self.Ganti is None:
                     self.Ganti = torch.empty_like(self.S)
-                torch.matmul(Wa.reshape(no * no, no * no).t(), self.U.view(no * no, -1),
-                             out=self.Ganti.view(no * no, -1))
+                Uf = self.U.view(no * no, -1)
+                if Uf.dtype == f64:
+                    torch.matmul(Wa.reshape(no * no, no * no).t(), Uf, out=self.Ganti.view(no * no, -1))
+                else:  # an FP32 U (split precisions): the product in FP32, kept in FP64
+                    self.Ganti.view(no * no, -1).copy_(torch.matmul(Wa.reshape(no * no, no * no).t().float(), Uf))
             else:
                 self.Ganti = None
         return S

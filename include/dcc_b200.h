@@ -85,6 +85,13 @@ DCC_API int dcc_t3_spin_summation(const double *A, double *B, int64_t nblocks, i
 /* Diagnostic: dcc_t3_spin_summation through one chosen kernel: 0 the default choice, 1 strips
  * (the patterns with p4 = 0, i.e. P3_201, at nvir <= 104), 2 orbit tiles (every pattern).
  * DCC_ERR_UNSUPPORTED (nothing launched) where the kernel does not apply.  Same results. */
+/* B = beta*A + alpha*P(A) out of place on FP32 blocks (the arithmetic in FP64 on the FP32
+ * values, the result rounded once): X = P3_201 of the FP32 unpacked T3 that the split-precision
+ * feedback strings read (distr_cc/rccsdt.py:308-309, 351-352).  The patterns without a p4 term,
+ * nvir <= 104. */
+DCC_API int dcc_t3_spin_summation_f32(const float *A, float *B, int64_t nblocks, int64_t nvir, const char *pattern,
+                                      double alpha, double beta, void *stream);
+
 DCC_API int dcc_t3_spin_summation_kernel(const double *A, double *B, int64_t nblocks, int64_t nvir,
                                          const char *pattern, double alpha, double beta, int kernel, void *stream);
 
@@ -130,6 +137,10 @@ DCC_API int dcc_take_t3_batched(const double *t3_local, double *out, const int32
  * all-orderings form of take_t3_ijk_single_ (src/rccsdt.c:119-129), reading
  * every canonical block once. */
 DCC_API int dcc_t3_unpack_all(const double *t3, double *U, int64_t nocc, int64_t nvir, void *stream);
+
+/* The same into an FP32 U (each value rounded once), the copy of T3 that the split-precision
+ * contractions read (their bf16 / tf32 pieces keep fewer bits than FP32); nvir <= 104. */
+DCC_API int dcc_t3_unpack_all_f32(const double *t3, float *U, int64_t nocc, int64_t nvir, void *stream);
 
 /* send_data[r] = t3_local[ijk_to_local_idx[requests[r]]] for stored blocks
  * (DEVICE index arrays).  Replaces fill_local_data_ijk_ (src/rccsdt.c:105-117). */
@@ -437,6 +448,9 @@ DCC_API int dcc_gemm_split3(const void *A_hi, const void *A_lo, const void *B_hi
  * map14 / epi14 hold two such maps (HOST). */
 DCC_API int dcc_split_operand_at4(const double *src, void *hi, void *lo, int64_t M, int64_t K, int64_t kw,
                                   int64_t ld, int64_t k0, const int64_t *map14, int kind, void *stream);
+/* The same from an FP32 source (the pieces of each value as a double). */
+DCC_API int dcc_split_operand_at4_f32(const float *src, void *hi, void *lo, int64_t M, int64_t K, int64_t kw,
+                                      int64_t ld, int64_t k0, const int64_t *map14, int kind, void *stream);
 DCC_API int dcc_gemm_split3_ld4(const void *A_hi, const void *A_lo, int64_t lda, const void *B_hi, const void *B_lo,
                                 int64_t ldb, int64_t M, int64_t N, int64_t Kp, double *C, const int64_t *epi14,
                                 double alpha, double beta, int kind, int *status, void *stream);

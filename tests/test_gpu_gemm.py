@@ -174,3 +174,24 @@ def test_wvvvv_with_fvv_folded(C, kind):
     torch.cuda.synchronize()
     assert int(op.status.item()) == 0
     assert _rel(r, torch.from_numpy(want).cuda()) < TOL[kind]
+
+
+@pytest.mark.parametrize("kind", ["bf16x3", "tf32x3"])
+@pytest.mark.parametrize("maps", ["k_contiguous", "rows_contiguous", "middle_digit"])
+def test_split_of_fp32_source(C, kind, maps):
+    """An FP32 source splits into the pieces of the same values as FP64, bit for bit, in each
+    read mode (k contiguous, rows contiguous, rows along a middle digit)."""
+    from dcc import contract as c
+    k = c.KIND[kind]
+    rng = np.random.default_rng(5)
+    X32 = torch.from_numpy(rng.standard_normal((5, 3, 6, 40)).astype(np.float32)).cuda()  # [k][p][q][r]
+    X64 = X32.double()
+    if maps == "k_contiguous":       # rows (k,p,q), K = r
+        M, K, fm, fk = 90, 40, c.lin(40), c.lin(1)
+    elif maps == "rows_contiguous":  # rows (q,r), K = (k,p)
+        M, K, fm, fk = 240, 15, c.lin(1), c.two(3, 720, 240)
+    else:                            # rows (p,r,q): the contiguous r is the middle digit; K = k
+        M, K, fm, fk = 720, 5, c.three(40, 6, 240, 1, 40), c.lin(720)
+    s32 = c.Split(M, K, k).fill(X32, fm, fk)
+    s64 = c.Split(M, K, k).fill(X64, fm, fk)
+    assert torch.equal(s32.hi, s64.hi) and torch.equal(s32.lo, s64.lo)

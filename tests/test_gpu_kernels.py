@@ -91,6 +91,47 @@ def test_t3_spin_sum_kernels(C, oracle, nvir, kernel):
     assert c3.symmetrize_status() == 0
 
 
+@pytest.mark.parametrize("nvir", [1, 2, 5, 13, 30, 93, 104])
+def test_t3_spin_sum_f32(C, oracle, nvir):
+    """The FP32 P3_201 (X of the split precisions): FP64 arithmetic on the FP32 values, rounded
+    once, so bit-exact with the oracle on the same values cast to FP64, the result cast back;
+    A untouched; other patterns and larger nvir refused."""
+    c3 = C[0]
+    rng = np.random.default_rng(300 + nvir)
+    nblk = 2 if nvir >= 90 else 3
+    for alpha, beta in [(1.0, 0.0), (-1.0 / 6.0, 1.0)]:
+        A = rng.standard_normal((nblk,) + (nvir,) * 3).astype(np.float32)
+        want = oracle.t3_spin_sum(A.astype(np.float64), nvir, "P3_201", alpha, beta).astype(np.float32)
+        d, out = dev(A), torch.full(A.shape, float("nan"), dtype=torch.float32, device="cuda")
+        c3.t3_spin_summation_f32(d, out, nblk, nvir, "P3_201", alpha, beta)
+        assert np.array_equal(host(out), want)
+        assert np.array_equal(host(d), A)
+    with pytest.raises(RuntimeError, match="p4 term"):
+        c3.t3_spin_summation_f32(d, out, nblk, nvir, "P3_422")
+    big = torch.zeros((1,) + (105,) * 3, dtype=torch.float32, device="cuda")
+    with pytest.raises(RuntimeError, match="p4 term"):
+        c3.t3_spin_summation_f32(big, big.clone(), 1, 105, "P3_201")
+
+
+@pytest.mark.parametrize("nocc,nvir", [(1, 5), (2, 13), (3, 17), (2, 93), (2, 104)])
+def test_unpack_all_f32(C, nocc, nvir):
+    """The FP32 unpack equals the FP64 unpack rounded to FP32, element for element."""
+    from dcc import t3_residual
+    rng = np.random.default_rng(17)
+    n3 = nocc * (nocc + 1) * (nocc + 2) // 6
+    t3 = dev(rng.standard_normal((n3,) + (nvir,) * 3))
+    shape = (nocc ** 3,) + (nvir,) * 3
+    U64 = torch.empty(shape, dtype=torch.float64, device="cuda")
+    U32 = torch.full(shape, 7.0, dtype=torch.float32, device="cuda")
+    t3_residual.unpack_all_(t3, U64, nocc, nvir)
+    t3_residual.unpack_all_(t3, U32, nocc, nvir)
+    assert torch.equal(U32, U64.float())
+    with pytest.raises(RuntimeError, match="nvir <= 104"):
+        t3_residual.unpack_all_(torch.zeros((1,) + (105,) * 3, dtype=torch.float64, device="cuda"),
+                                torch.empty((1,) + (105,) * 3, dtype=torch.float32, device="cuda"), 1, 105)
+    assert C[0].symmetrize_status() == 0
+
+
 @pytest.mark.parametrize("nvir", [1, 5, 10, 13, 30, 90, 93, 106])
 @pytest.mark.parametrize("pattern", P3)
 def test_t3_spin_sum_out_of_place(C, oracle, nvir, pattern):
