@@ -9,7 +9,7 @@ minimal stand-ins for both in sys.modules (a communicator with a fixed rank and
 size, a no-op logger).  Run from the repository root, in a container that holds the
 reference sources:
 
-    python tests/golden/make_checkpoints.py [path-to-reference]
+    python tests/golden/make_checkpoints.py <path-to-reference>   (or set DCC_REFERENCE)
 
 Each case directory holds the checkpoint files and `blocks.npy`, the full
 canonical-order amplitudes the ranks' files were cut from.
@@ -100,7 +100,9 @@ def _t4_case(mod, name, nocc, nvir, size, distribution, rng):
 
 
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("DCC_REFERENCE")
+    if not ref:
+        sys.exit("usage: make_checkpoints.py <path-to-reference>  (or set DCC_REFERENCE)")
     _install_stubs()
     # The writers use no C helper; the reference refuses to import without its library
     # unless the Python fallback is allowed.

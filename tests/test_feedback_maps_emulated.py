@@ -37,7 +37,8 @@ def _emu_gemm(A, B, C, frow, fcol, alpha=1.0, beta=1.0, status=None, Kp=None):
     idx = fmap(frow, np.arange(A.M))[:, None] + fmap(fcol, np.arange(B.M))[None, :]
     assert len(np.unique(idx)) == idx.size
     flat = C.view(-1).numpy()
-    flat[idx] = alpha * (A.a @ B.a.T) + beta * flat[idx]
+    # beta = 0 overwrites without reading C (BLAS semantics, as the kernel's epilogue)
+    flat[idx] = alpha * (A.a @ B.a.T) + (beta * flat[idx] if beta != 0.0 else 0.0)
     return status
 
 
@@ -45,7 +46,8 @@ def _emu_gemm_range(A, B, C, frow, fcol, alpha, beta, status, col0, ncol):
     assert col0 % 64 == 0 and ncol % 64 == 0
     idx = fmap(frow, np.arange(A.M))[:, None] + fmap(fcol, np.arange(B.M))[None, :]
     flat = C.view(-1).numpy()
-    flat[idx] = alpha * (A.a[:, col0:col0 + ncol] @ B.a[:, col0:col0 + ncol].T) + beta * flat[idx]
+    flat[idx] = alpha * (A.a[:, col0:col0 + ncol] @ B.a[:, col0:col0 + ncol].T) + \
+        (beta * flat[idx] if beta != 0.0 else 0.0)
     return status
 
 
