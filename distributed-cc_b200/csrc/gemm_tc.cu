@@ -141,8 +141,8 @@ struct GemmSmem {
     uint32_t tmem_base;
 };
 
-// per epilogue warp: a 32x33 float transpose buffer, 32 row and 32 column offsets
-constexpr uint32_t EPI_WARP_BYTES = 32 * 33 * 4 + 64 * 8;
+// per epilogue warp: a 32x33 float transpose buffer, 32 row and 64 column offsets
+constexpr uint32_t EPI_WARP_BYTES = 32 * 33 * 4 + 96 * 8;
 
 __device__ __forceinline__ void tile_coords(int t, int num_m, int num_n, int group_m, int &tm, int &tn) {
     const int per_group = group_m * num_n;
@@ -157,11 +157,13 @@ __device__ __forceinline__ void tile_coords(int t, int num_m, int num_n, int gro
 // MMAs of tile t+1 run while the epilogue warps drain tile t.
 // KIND 0: bf16 pieces; KIND 1: tf32 pieces.  KB: bytes of K per row and
 // k-block; ST: ring depth.
-template <int KIND, int KB, int ST, int EPI>
+// CT: the storage type of C (double; float for the FP32 accumulators of the split precisions,
+// whose epilogue reads and writes half the bytes; the arithmetic stays FP64, one rounding per store).
+template <int KIND, int KB, int ST, int EPI, typename CT = double>
 __global__ void __launch_bounds__(gemm_threads<EPI>(), 1)
     k_gemm_split3(const __grid_constant__ CUtensorMap tmAh, const __grid_constant__ CUtensorMap tmAl,
                   const __grid_constant__ CUtensorMap tmBh, const __grid_constant__ CUtensorMap tmBl, int M, int N,
-                  int nkb, double *C, GemmEpi epi, double alpha, double beta, int *status, int group_m,
+                  int nkb, CT *C, GemmEpi epi, double alpha, double beta, int *status, int group_m,
                   int epi_cols) {
     extern __shared__ __align__(1024) uint8_t g_smem[];
     // operand stages first (1024-byte aligned), then the epilogue buffers and the control block
@@ -295,65 +297,104 @@ __global__ void __launch_bounds__(gemm_threads<EPI>(), 1)
             const int64_t roff = map4_32(epi.row, (uint32_t)(m < M ? m : 0));
             const int nrow = (M - m0) < 32 ? (M - m0) : 32;
             offs[lane] = roff;  // cols mode: row offsets of the warp's 32 rows
-            for (int c = cbeg; c < cend; c += 32) {
-                float v[32];
-                tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * GN + c), v);
-                if (c == cend - 32) {
-                    // the accumulator is in registers: hand it back to the MMA warp
-                    tc_fence_before();
-                    __syncwarp();
-                    if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(
-                                                    smem_u32(&cs->acc_empty[b]))
-                                                : "memory");
+            // NCH 32-column chunks per step (two chunks' loads in flight measured no faster for an FP32
+            // C: one chunk per step for either type)
+            constexpr int NCH = 1;
+            for (int c = cbeg; c < cend; c += 32 * NCH) {
+                bool cval[NCH];
+                int64_t coff[NCH];
+#pragma unroll
+                for (int h = 0; h < NCH; h++) {
+                    const int col = n0 + c + 32 * h + lane;
+                    cval[h] = col < N;
+                    coff[h] = map4_32(epi.col, (uint32_t)(cval[h] ? col : 0));
                 }
-                const int col = n0 + c + lane;
-                const bool cval = col < N;
-                const int64_t coff = map4_32(epi.col, (uint32_t)(cval ? col : 0));
+                // the chunk's accumulator columns; the warp's last load hands the accumulator back
+                auto load_acc = [&](int h, float (&v)[32]) {
+                    tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * GN + c + 32 * h), v);
+                    if (c + 32 * (h + 1) == cend) {
+                        tc_fence_before();
+                        __syncwarp();
+                        if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(
+                                                        smem_u32(&cs->acc_empty[b]))
+                                                    : "memory");
+                    }
+                };
                 if (epi_cols) {
                     // lanes walk the 32 columns of one row at a time (columns contiguous in C)
+                    bool full[NCH];
 #pragma unroll
-                    for (int j = 0; j < 32; j++) stg[lane * 33 + j] = v[j];
-                    __syncwarp();
-                    double *cp = C + coff;
-                    const bool full_chunk = __all_sync(0xffffffffu, cval) && nrow == 32;
-                    if (beta == 0.0) {
-                        if (full_chunk) {
+                    for (int h = 0; h < NCH; h++) full[h] = __all_sync(0xffffffffu, cval[h]) && nrow == 32;
+                    CT old[NCH][32];
+                    if (beta != 0.0) {
+#pragma unroll
+                        for (int h = 0; h < NCH; h++)
+                            if (full[h]) {
+#pragma unroll
+                                for (int r = 0; r < 32; r++) old[h][r] = __ldcg(C + coff[h] + offs[r]);
+                            }
+                    }
+#pragma unroll
+                    for (int h = 0; h < NCH; h++) {
+                        float v[32];
+                        load_acc(h, v);
+#pragma unroll
+                        for (int j = 0; j < 32; j++) stg[lane * 33 + j] = v[j];
+                        __syncwarp();
+                        CT *cp = C + coff[h];
+                        if (beta == 0.0) {
+                            if (full[h]) {
 #pragma unroll 8
-                            for (int r = 0; r < 32; r++) cp[offs[r]] = alpha * (double)stg[r * 33 + lane];
+                                for (int r = 0; r < 32; r++) cp[offs[r]] = (CT)(alpha * (double)stg[r * 33 + lane]);
+                            } else {
+                                for (int r = 0; r < nrow; r++)
+                                    if (cval[h]) cp[offs[r]] = (CT)(alpha * (double)stg[r * 33 + lane]);
+                            }
+                        } else if (full[h]) {
+#pragma unroll
+                            for (int r = 0; r < 32; r++)
+                                cp[offs[r]] = (CT)fma(beta, (double)old[h][r], alpha * (double)stg[r * 33 + lane]);
                         } else {
                             for (int r = 0; r < nrow; r++)
-                                if (cval) cp[offs[r]] = alpha * (double)stg[r * 33 + lane];
+                                if (cval[h])
+                                    cp[offs[r]] = (CT)fma(beta, (double)__ldcg(cp + offs[r]),
+                                                          alpha * (double)stg[r * 33 + lane]);
                         }
-                    } else if (full_chunk) {
-                        double old[32];
-#pragma unroll
-                        for (int r = 0; r < 32; r++) old[r] = __ldcg(cp + offs[r]);
-#pragma unroll
-                        for (int r = 0; r < 32; r++) cp[offs[r]] = fma(beta, old[r], alpha * (double)stg[r * 33 + lane]);
-                    } else {
-                        for (int r = 0; r < nrow; r++)
-                            if (cval) cp[offs[r]] = fma(beta, __ldcg(cp + offs[r]), alpha * (double)stg[r * 33 + lane]);
+                        __syncwarp();
                     }
-                    __syncwarp();
                 } else {
-                    // lanes are rows (rows contiguous in C): each thread writes its row's 32 columns
+                    // lanes are rows (rows contiguous in C): each thread writes its row's columns
                     int64_t *coffs = offs + 32;
-                    coffs[lane] = coff;
+#pragma unroll
+                    for (int h = 0; h < NCH; h++) coffs[32 * h + lane] = coff[h];
                     __syncwarp();
-                    const int nvalid = (N - n0 - c) < 32 ? (N - n0 - c) : 32;
-                    if (m < M) {
-                        double *rp = C + roff;
-                        if (beta == 0.0) {
+                    int nvalid[NCH];
+#pragma unroll
+                    for (int h = 0; h < NCH; h++) nvalid[h] = N - n0 - c - 32 * h;
+                    CT *rp = C + roff;
+                    CT old[NCH][32];
+                    if (beta != 0.0 && m < M) {
+#pragma unroll
+                        for (int h = 0; h < NCH; h++)
 #pragma unroll
                             for (int j = 0; j < 32; j++)
-                                if (j < nvalid) rp[coffs[j]] = alpha * (double)v[j];
-                        } else {
-                            double old[32];
+                                old[h][j] = (j < nvalid[h]) ? __ldcg(rp + coffs[32 * h + j]) : (CT)0;
+                    }
 #pragma unroll
-                            for (int j = 0; j < 32; j++) old[j] = (j < nvalid) ? __ldcg(rp + coffs[j]) : 0.0;
+                    for (int h = 0; h < NCH; h++) {
+                        float v[32];
+                        load_acc(h, v);
+                        if (m < M) {
+                            if (beta == 0.0) {
 #pragma unroll
-                            for (int j = 0; j < 32; j++)
-                                if (j < nvalid) rp[coffs[j]] = fma(beta, old[j], alpha * (double)v[j]);
+                                for (int j = 0; j < 32; j++)
+                                    if (j < nvalid[h]) rp[coffs[32 * h + j]] = (CT)(alpha * (double)v[j]);
+                            } else {
+#pragma unroll
+                                for (int j = 0; j < 32; j++)
+                                    if (j < nvalid[h])
+                                        rp[coffs[32 * h + j]] = (CT)fma(beta, (double)old[h][j], alpha * (double)v[j]);
+                            }
                         }
                     }
                     __syncwarp();
@@ -479,6 +520,7 @@ __device__ __forceinline__ void split_tile(const S *__restrict__ src, const Spli
     const int64_t ka = kt + lane, kb = ka + 32;
     const int koa = ka < a.K ? (int)map4_32(a.mp.k, (uint32_t)ka) : -1;
     const int kob = kb < a.K ? (int)map4_32(a.mp.k, (uint32_t)kb) : -1;
+    // loads in flight per lane: 16 (also for an FP32 source: 32 in flight measured 1.8x slower)
     if (a.mode == 0) {
 #pragma unroll 8
         for (int r = 0; r < SP_TM; r++) {
@@ -920,9 +962,9 @@ static size_t gemm_smem_bytes(int kb_bytes) {
            sizeof(GemmSmem<ST>);
 }
 
-template <int KIND, int KB, int ST, int EPI>
+template <int KIND, int KB, int ST, int EPI, typename CT = double>
 static int gemm_launch(const CUtensorMap &a, const CUtensorMap &b, const CUtensorMap &c, const CUtensorMap &d, int M,
-                       int N, int nkb, double *C, const GemmEpi &epi, double alpha, double beta, int *status,
+                       int N, int nkb, CT *C, const GemmEpi &epi, double alpha, double beta, int *status,
                        int group_m, cudaStream_t st) {
     // write along columns when the column map's fastest digit is contiguous,
     // along rows when only the row map's is
@@ -936,9 +978,9 @@ static int gemm_launch(const CUtensorMap &a, const CUtensorMap &b, const CUtenso
     int dev = 0, nsm = 148;
     if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     const unsigned grid = (unsigned)(tiles < nsm ? tiles : nsm);  // persistent: one CTA per SM
-    cudaFuncSetAttribute(k_gemm_split3<KIND, KB, ST, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k_gemm_split3<KIND, KB, ST, EPI><<<grid, gemm_threads<EPI>(), smem, st>>>(a, b, c, d, M, N, nkb, C, epi, alpha, beta, status,
-                                                                group_m, epi_cols);
+    cudaFuncSetAttribute(k_gemm_split3<KIND, KB, ST, EPI, CT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_gemm_split3<KIND, KB, ST, EPI, CT><<<grid, gemm_threads<EPI>(), smem, st>>>(a, b, c, d, M, N, nkb, C, epi, alpha,
+                                                                                 beta, status, group_m, epi_cols);
     return launch_status("gemm_split3");
 }
 
@@ -1141,8 +1183,8 @@ extern "C" int dcc_split_operand(const double *src, void *hi, void *lo, int64_t 
 }
 
 static int gemm_split3(const void *A_hi, const void *A_lo, int64_t lda, const void *B_hi, const void *B_lo,
-                       int64_t ldb, int64_t M, int64_t N, int64_t Kp, double *C, const int64_t *epi, bool four,
-                       double alpha, double beta, int kind, int *status, void *stream) {
+                       int64_t ldb, int64_t M, int64_t N, int64_t Kp, void *C, const int64_t *epi, bool four,
+                       double alpha, double beta, int kind, int *status, void *stream, bool c_f32 = false) {
     clear_error();
     DCC_REQUIRE(kind == 0 || kind == 1, DCC_ERR_UNSUPPORTED, "kind must be 0 (bf16x3) or 1 (tf32x3)");
     const int kblk = kind == 0 ? 64 : 32;
@@ -1164,7 +1206,8 @@ static int gemm_split3(const void *A_hi, const void *A_lo, int64_t lda, const vo
     // (two per TMEM lane quarter) double its memory parallelism; the ring then
     // is three 64-byte stages to make room for their staging buffers.
     const int esz = kind == 0 ? 2 : 4;
-    const bool wide_epi = Kp <= 4096;
+    // an FP32 C always takes the wide epilogue (its only instantiation)
+    const bool wide_epi = Kp <= 4096 || c_f32;
     const int kb = wide_epi ? 64 : cfg.kb_bytes;
     CUtensorMap mAh, mAl, mBh, mBl;
     int rc;
@@ -1174,13 +1217,19 @@ static int gemm_split3(const void *A_hi, const void *A_lo, int64_t lda, const vo
     cudaStream_t st = as_stream(stream);
     const int nkb = (int)(Kp / (kb / esz));
     const int iM = (int)M, iN = (int)N, gm = cfg.group_m;
+    if (c_f32) {
+        float *Cf = (float *)C;
+        if (kind == 0) return gemm_launch<0, 64, 3, 8>(mAh, mAl, mBh, mBl, iM, iN, nkb, Cf, ep, alpha, beta, status, gm, st);
+        return gemm_launch<1, 64, 3, 8>(mAh, mAl, mBh, mBl, iM, iN, nkb, Cf, ep, alpha, beta, status, gm, st);
+    }
+    double *Cd = (double *)C;
     if (wide_epi) {
-        if (kind == 0) return gemm_launch<0, 64, 3, 8>(mAh, mAl, mBh, mBl, iM, iN, nkb, C, ep, alpha, beta, status, gm, st);
-        return gemm_launch<1, 64, 3, 8>(mAh, mAl, mBh, mBl, iM, iN, nkb, C, ep, alpha, beta, status, gm, st);
+        if (kind == 0) return gemm_launch<0, 64, 3, 8>(mAh, mAl, mBh, mBl, iM, iN, nkb, Cd, ep, alpha, beta, status, gm, st);
+        return gemm_launch<1, 64, 3, 8>(mAh, mAl, mBh, mBl, iM, iN, nkb, Cd, ep, alpha, beta, status, gm, st);
     }
 #define DCC_GEMM_CASE(K_, KB_, ST_)                                                                           \
     if (kind == K_ && cfg.kb_bytes == KB_ && cfg.stages == ST_)                                              \
-        return gemm_launch<K_, KB_, ST_, 4>(mAh, mAl, mBh, mBl, iM, iN, nkb, C, ep, alpha, beta, status, gm, st);
+        return gemm_launch<K_, KB_, ST_, 4>(mAh, mAl, mBh, mBl, iM, iN, nkb, Cd, ep, alpha, beta, status, gm, st);
     DCC_GEMM_CASE(0, 128, 2)
     DCC_GEMM_CASE(0, 64, 4)
     DCC_GEMM_CASE(0, 64, 3)
@@ -1206,6 +1255,14 @@ extern "C" int dcc_gemm_split3_ld4(const void *A_hi, const void *A_lo, int64_t l
                                    const int64_t *epi14, double alpha, double beta, int kind, int *status,
                                    void *stream) {
     return gemm_split3(A_hi, A_lo, lda, B_hi, B_lo, ldb, M, N, Kp, C, epi14, true, alpha, beta, kind, status, stream);
+}
+
+extern "C" int dcc_gemm_split3_ld4_f32c(const void *A_hi, const void *A_lo, int64_t lda, const void *B_hi,
+                                        const void *B_lo, int64_t ldb, int64_t M, int64_t N, int64_t Kp, float *C,
+                                        const int64_t *epi14, double alpha, double beta, int kind, int *status,
+                                        void *stream) {
+    return gemm_split3(A_hi, A_lo, lda, B_hi, B_lo, ldb, M, N, Kp, C, epi14, true, alpha, beta, kind, status, stream,
+                       true);
 }
 
 extern "C" int dcc_gemm_split3(const void *A_hi, const void *A_lo, const void *B_hi, const void *B_lo, int64_t M,

@@ -2350,13 +2350,16 @@ namespace dcc {
 // in shared memory for a pair of 8-wide index tiles (a in I, b in J) and a chunk of c.  Each warp
 // then streams output rows with coalesced loads and stores.  The slots are summed in the order of
 // the orbit-tile kernels (p = 0..5, one fma each), so the result is theirs bit for bit.
-constexpr int GB_PITCH = 65;  // doubles per (c) row of a staged tile: 8 x 8 + 1 (conflict-free transposed reads)
-__global__ void __launch_bounds__(256, 2) k_gather_band(const double *__restrict__ S, double *__restrict__ r3,
+// ST: the storage type of S (double; float for the FP32 accumulator of the split precisions, whose
+// values enter the same FP64 sums exactly).
+constexpr int GB_PITCH = 65;  // elements per (c) row of a staged tile: 8 x 8 + 1 (conflict-free transposed reads)
+template <typename ST>
+__global__ void __launch_bounds__(256, 2) k_gather_band(const ST *__restrict__ S, double *__restrict__ r3,
                                                         const int32_t *__restrict__ ijk, int64_t nblocks, int nocc,
                                                         int nv, int ntile, int cchunk, double scale, double beta) {
     extern __shared__ double gb_sm[];  // tiles of the slots p = 1, 3, 4, 5: [cc][a_local * 8 + b_local]
-    double *T1 = gb_sm, *T3 = T1 + (size_t)cchunk * GB_PITCH, *T4 = T3 + (size_t)cchunk * GB_PITCH,
-           *T5 = T4 + (size_t)cchunk * GB_PITCH;
+    ST *T1 = reinterpret_cast<ST *>(gb_sm), *T3 = T1 + (size_t)cchunk * GB_PITCH, *T4 = T3 + (size_t)cchunk * GB_PITCH,
+       *T5 = T4 + (size_t)cchunk * GB_PITCH;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int64_t n3 = (int64_t)nv * nv * nv, nv2 = (int64_t)nv * nv;
     const int nch = (nv + cchunk - 1) / cchunk;
@@ -2367,7 +2370,7 @@ __global__ void __launch_bounds__(256, 2) k_gather_band(const double *__restrict
         const int I = rem / (ntile * nch), J = (rem / nch) % ntile, ch = rem % nch;
         const int c0 = ch * cchunk, cn = min(cchunk, nv - c0);
         const int o[3] = {ijk[3 * q], ijk[3 * q + 1], ijk[3 * q + 2]};
-        const double *src[6];
+        const ST *src[6];
 #pragma unroll
         for (int p = 0; p < 6; p++)
             src[p] = S + (((int64_t)o[perm3(p, 0)] * nocc + o[perm3(p, 1)]) * nocc + o[perm3(p, 2)]) * n3;
@@ -2376,13 +2379,13 @@ __global__ void __launch_bounds__(256, 2) k_gather_band(const double *__restrict
             const int cc = e >> 6, r = (e >> 3) & 7, t = e & 7, c = c0 + cc, off = cc * GB_PITCH;
             if (a0 + r < nv && b0 + t < nv) {  // a = a0 + r, b = b0 + t: b contiguous
                 const int a = a0 + r, b = b0 + t;
-                cp_async8(T1 + off + r * 8 + t, src[1] + a * nv2 + (int64_t)c * nv + b);  // S1[a][c][b]
-                cp_async8(T4 + off + r * 8 + t, src[4] + c * nv2 + (int64_t)a * nv + b);  // S4[c][a][b]
+                cp_async_el(T1 + off + r * 8 + t, src[1] + a * nv2 + (int64_t)c * nv + b);  // S1[a][c][b]
+                cp_async_el(T4 + off + r * 8 + t, src[4] + c * nv2 + (int64_t)a * nv + b);  // S4[c][a][b]
             }
             if (b0 + r < nv && a0 + t < nv) {  // b = b0 + r, a = a0 + t: a contiguous
                 const int a = a0 + t, b = b0 + r;
-                cp_async8(T3 + off + t * 8 + r, src[3] + b * nv2 + (int64_t)c * nv + a);  // S3[b][c][a]
-                cp_async8(T5 + off + t * 8 + r, src[5] + c * nv2 + (int64_t)b * nv + a);  // S5[c][b][a]
+                cp_async_el(T3 + off + t * 8 + r, src[3] + b * nv2 + (int64_t)c * nv + a);  // S3[b][c][a]
+                cp_async_el(T5 + off + t * 8 + r, src[5] + c * nv2 + (int64_t)b * nv + a);  // S5[c][b][a]
             }
         }
         cp_async_commit();
@@ -2397,14 +2400,14 @@ __global__ void __launch_bounds__(256, 2) k_gather_band(const double *__restrict
             for (int h = 0; h < 2; h++) {
                 const int al = (rw >> 3) + h, bl = rw & 7, a = a0 + al, b = b0 + bl;
                 const bool ok = a < nv && b < nv;
-                const double *r0 = src[0] + a * nv2 + (int64_t)b * nv, *r2 = src[2] + b * nv2 + (int64_t)a * nv;
+                const ST *r0 = src[0] + a * nv2 + (int64_t)b * nv, *r2 = src[2] + b * nv2 + (int64_t)a * nv;
                 const double *out = r3 + q * n3 + a * nv2 + (int64_t)b * nv;
 #pragma unroll
                 for (int j = 0; j < 2; j++) {
                     const int cc = lane + 32 * j, c = c0 + cc;
                     const bool in = ok && cc < cn;
-                    v0[h][j] = in ? __ldg(r0 + c) : 0.0;
-                    v2[h][j] = in ? __ldg(r2 + c) : 0.0;
+                    v0[h][j] = in ? (double)__ldg(r0 + c) : 0.0;
+                    v2[h][j] = in ? (double)__ldg(r2 + c) : 0.0;
                     vo[h][j] = in && beta != 0.0 ? out[c] : 0.0;
                 }
             }
@@ -2420,11 +2423,11 @@ __global__ void __launch_bounds__(256, 2) k_gather_band(const double *__restrict
                     if (cc >= cn) continue;
                     const int off = cc * GB_PITCH + ti;
                     double acc = fma(scale, v0[h][j], 0.0);
-                    acc = fma(scale, T1[off], acc);
+                    acc = fma(scale, (double)T1[off], acc);
                     acc = fma(scale, v2[h][j], acc);
-                    acc = fma(scale, T3[off], acc);
-                    acc = fma(scale, T4[off], acc);
-                    acc = fma(scale, T5[off], acc);
+                    acc = fma(scale, (double)T3[off], acc);
+                    acc = fma(scale, (double)T4[off], acc);
+                    acc = fma(scale, (double)T5[off], acc);
                     out[c] = beta == 0.0 ? acc : fma(beta, vo[h][j], acc);
                 }
             }
@@ -2437,28 +2440,48 @@ __global__ void __launch_bounds__(256, 2) k_gather_band(const double *__restrict
 
 // The row gather for one full-layout source with every permutation at an odd nvir; returns
 // DCC_ERR_UNSUPPORTED (nothing launched) where it does not apply.
+template <typename ST>
 static int gather_band_launch(double *r3, const int32_t *ijk, int64_t nblocks, int64_t nocc, int64_t nvir, double beta,
-                              int nsrc, const double *const *bases, const double *scales, const int64_t *strides,
+                              int nsrc, const ST *const *bases, const double *scales, const int64_t *strides,
                               const int *masks, void *stream) {
     if (nsrc != 1 || masks[0] != 63 || nvir > 104 || nocc < 1 || nocc > 1290 || !bases[0]) return DCC_ERR_UNSUPPORTED;
     const int64_t n3 = nvir * nvir * nvir;
     const int64_t full[6] = {nocc * nocc * n3, nocc * n3, n3, nvir * nvir, nvir, 1};
     for (int m = 0; m < 6; m++)
         if (strides[m] != full[m]) return DCC_ERR_UNSUPPORTED;
-    const int64_t sbytes = nocc * nocc * nocc * n3 * (int64_t)sizeof(double), rbytes = nblocks * n3 * (int64_t)sizeof(double);
+    const int64_t sbytes = nocc * nocc * nocc * n3 * (int64_t)sizeof(ST), rbytes = nblocks * n3 * (int64_t)sizeof(double);
     if (!((const char *)bases[0] + sbytes <= (const char *)r3 || (const char *)r3 + rbytes <= (const char *)bases[0]))
         return DCC_ERR_UNSUPPORTED;
     const int ntile = (int)ceil_div(nvir, TE);
     const int cchunk = (int)((nvir + 1) / 2);  // two chunks of c: four tiles fit twice in an SM
-    const size_t smem = 4 * (size_t)cchunk * GB_PITCH * sizeof(double);
+    const size_t smem = 4 * (size_t)cchunk * GB_PITCH * sizeof(ST);
     int dev = 0, nsm = 148;
     if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     const int64_t nwork = nblocks * (int64_t)ntile * ntile * 2, cap = (int64_t)nsm * 2;
     const unsigned grid = (unsigned)(nwork < cap ? nwork : cap);
-    cudaFuncSetAttribute(k_gather_band, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k_gather_band<<<grid, 256, smem, as_stream(stream)>>>(bases[0], r3, ijk, nblocks, (int)nocc, (int)nvir, ntile,
-                                                          cchunk, scales[0], beta);
+    cudaFuncSetAttribute(k_gather_band<ST>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_gather_band<ST><<<grid, 256, smem, as_stream(stream)>>>(bases[0], r3, ijk, nblocks, (int)nocc, (int)nvir, ntile,
+                                                              cchunk, scales[0], beta);
     return DCC_OK;
+}
+
+// r3 = beta r3 + scale sum_p S[p(ijk)][p(abc)] over every simultaneous permutation p, from a
+// full-layout FP32 S [nocc^3][nvir^3] (the split precisions' accumulator), nvir <= 104.
+extern "C" int dcc_t3_s3_gather_f32(double *r3, const int32_t *ijk, int64_t nblocks, int64_t nocc, int64_t nvir,
+                                    double beta, const float *S, double scale, void *stream) {
+    clear_error();
+    DCC_REQUIRE(nblocks >= 0 && nvir >= 0 && nocc >= 0, DCC_ERR_SHAPE, "negative size");
+    if (nblocks == 0 || nvir == 0) return DCC_OK;
+    DCC_REQUIRE(r3 && ijk && S, DCC_ERR_NULL, "NULL argument");
+    DCC_REQUIRE(nvir <= 104 && nocc >= 1 && nocc <= 1290, DCC_ERR_UNSUPPORTED,
+                "the FP32 gather serves nvir <= 104 (nvir = %lld)", (long long)nvir);
+    const int64_t n3 = nvir * nvir * nvir;
+    const int64_t full[6] = {nocc * nocc * n3, nocc * n3, n3, nvir * nvir, nvir, 1};
+    const int mask = 63;
+    const float *bases[1] = {S};
+    const int rc = gather_band_launch(r3, ijk, nblocks, nocc, nvir, beta, 1, bases, &scale, full, &mask, stream);
+    DCC_REQUIRE(rc == DCC_OK, DCC_ERR_SHAPE, "S and r3 overlap");
+    return launch_status("t3_gather_band (FP32 S)");
 }
 
 extern "C" int dcc_t3_perm_gather_tma(double *r3, const int32_t *ijk, int64_t nblocks, int64_t nocc, int64_t nvir,

@@ -26,6 +26,13 @@ _split = L.bind("dcc_split_operand_at4", [L.c_vp, L.c_vp, L.c_vp] + [L.c_i64] * 
 _split_f32 = L.bind("dcc_split_operand_at4_f32", [L.c_vp, L.c_vp, L.c_vp] + [L.c_i64] * 5 + [L.c_vp, L.c_int, L.c_vp])
 _gemm = L.bind("dcc_gemm_split3_ld4", [L.c_vp, L.c_vp, L.c_i64, L.c_vp, L.c_vp] + [L.c_i64] * 4 +
                [L.c_vp, L.c_vp, L.c_dbl, L.c_dbl, L.c_int, L.c_vp, L.c_vp])
+_gemm_f32c = L.bind("dcc_gemm_split3_ld4_f32c", [L.c_vp, L.c_vp, L.c_i64, L.c_vp, L.c_vp] + [L.c_i64] * 4 +
+                    [L.c_vp, L.c_vp, L.c_dbl, L.c_dbl, L.c_int, L.c_vp, L.c_vp])
+
+
+def _gemm_fn(C):
+    """The GEMM entry for C's storage type (FP64, or the FP32 accumulators of the split path)."""
+    return _gemm_f32c if C.dtype == torch.float32 else _gemm
 
 BIG = 1 << 30  # radix that makes a digit of a map a plain stride (< 2^31)
 
@@ -144,6 +151,7 @@ class Split:
 def gemm_(A, B, C, frow, fcol, alpha=1.0, beta=1.0, status=None, Kp=None):
     """C[frow(m) + fcol(n)] = alpha * A B^T + beta * C (A: Split [M,K], B: Split [N,K]).
 
+    C is FP64, or FP32 (the sum still taken in FP64, rounded once per store).
     Kp (default: both operands' padded K) contracts only the leading Kp columns."""
     if A.kind != B.kind:
         raise ValueError("A and B must be split with the same kind")
@@ -153,10 +161,10 @@ def gemm_(A, B, C, frow, fcol, alpha=1.0, beta=1.0, status=None, Kp=None):
         Kp = A.Kp
     if Kp > A.Kp or Kp > B.Kp:
         raise ValueError("Kp exceeds an operand's columns")
-    _check_span(C, frow, A.M, fcol, B.M, "C")
+    _check_span(C, frow, A.M, fcol, B.M, "C", (f64, torch.float32))
     if status is None:
         status = torch.zeros(1, dtype=torch.int32, device=C.device)
-    L.check(_gemm(L.ptr(A.hi), L.ptr(A.lo), A.Kp, L.ptr(B.hi), L.ptr(B.lo), B.Kp, A.M, B.M, int(Kp), L.ptr(C),
+    L.check(_gemm_fn(C)(L.ptr(A.hi), L.ptr(A.lo), A.Kp, L.ptr(B.hi), L.ptr(B.lo), B.Kp, A.M, B.M, int(Kp), L.ptr(C),
                   _i64x14(frow, fcol), float(alpha), float(beta), A.kind, L.ptr(status), L.stream_ptr()))
     return status
 
@@ -169,10 +177,10 @@ def gemm_range_(A, B, C, frow, fcol, alpha, beta, status, col0, ncol):
     blk = _KBLK[A.kind]
     if col0 % blk or ncol % blk or col0 + ncol > A.Kp:
         raise ValueError("column range must be whole k-blocks inside the operands")
-    _check_span(C, frow, A.M, fcol, B.M, "C")
+    _check_span(C, frow, A.M, fcol, B.M, "C", (f64, torch.float32))
     es = A.hi.element_size()
     vp = lambda t: ctypes.c_void_p(t.data_ptr() + col0 * es)  # noqa: E731
-    L.check(_gemm(vp(A.hi), vp(A.lo), A.Kp, vp(B.hi), vp(B.lo), B.Kp, A.M, B.M, int(ncol), L.ptr(C),
+    L.check(_gemm_fn(C)(vp(A.hi), vp(A.lo), A.Kp, vp(B.hi), vp(B.lo), B.Kp, A.M, B.M, int(ncol), L.ptr(C),
                   _i64x14(frow, fcol), float(alpha), float(beta), A.kind, L.ptr(status), L.stream_ptr()))
     return status
 

@@ -26,8 +26,9 @@ permutation, hence the halves.  A W_oooo without the pair symmetry keeps its
 antisymmetric part on the reference's own permutation set
 {identity, (i,k,j; a,c,b), (j,k,i; b,c,a)}.
 
-In mixed precision S is built by five split-precision tcgen05 GEMMs written
-straight into S's [i][j][k][a][b][c] layout (-Y first, which initializes S; X;
+In mixed precision S (FP32, the accumulation type of the split products) is
+built by five split-precision tcgen05 GEMMs written straight into S's
+[i][j][k][a][b][c] layout (-Y first, which initializes S; X;
 T2 and T5/2 as one GEMM over the concatenated contraction index; T1 reusing
 T2's U operand; the K = nocc^2 W_oooo / F_oo part over a K-major split of U),
 and one gather kernel applies the symmetrization to S (the FP64 path builds S
@@ -108,6 +109,21 @@ def perm_gather_(r3, ijk, nvir, beta, sources, nocc=None, status=None):
             status = _default_status(r3.device)
         L.check(_pgather_tma(L.ptr(r3), L.ptr(ijk), r3.shape[0], int(nocc), nvir, float(beta), n, bases, scales,
                              strides, masks, L.ptr(status), L.stream_ptr()))
+    return r3
+
+
+_gather_f32 = L.bind("dcc_t3_s3_gather_f32", [L.c_vp, L.c_vp, L.c_i64, L.c_i64, L.c_i64, L.c_dbl, L.c_vp, L.c_dbl,
+                                              L.c_vp])
+
+
+def s3_gather_f32_(r3, ijk, nvir, beta, S, scale, nocc):
+    """r3 = beta*r3 + scale * sum over the six simultaneous permutations of an FP32 full-layout S."""
+    if S.dtype != torch.float32 or r3.dtype != f64:
+        raise TypeError("S must be float32 and r3 float64")
+    if S.numel() != nocc ** 3 * nvir ** 3 or not S.is_contiguous():
+        raise ValueError("S must be a contiguous [nocc^3][nvir^3] tensor")
+    L.check(_gather_f32(L.ptr(r3), L.ptr(ijk), r3.shape[0], int(nocc), int(nvir), float(beta), L.ptr(S),
+                        float(scale), L.stream_ptr()))
     return r3
 
 
@@ -215,8 +231,11 @@ class T3Residual:
         self.dev = device
         self.with_oo = with_oo
         full = (no ** 3, nv, nv, nv)
-        self.S = torch.empty(full, dtype=f64, device=device)  # [i][j][k][a][b][c]
         self.udtype = full_dtype(precision, nvir)
+        # [i][j][k][a][b][c]; in the split precisions the accumulator of the S GEMMs is FP32 like
+        # their products' accumulation (half the bytes of the five epilogue read-modify-writes and
+        # of the gather), FP64 on the FP64 path
+        self.S = torch.empty(full, dtype=self.udtype, device=device)
         self.U = torch.empty(full, dtype=self.udtype, device=device) if with_oo else None
         self.Ganti = None
         self.gstatus = torch.zeros(1, dtype=torch.int32, device=device)  # gather pipeline timeouts
@@ -298,7 +317,7 @@ class T3Residual:
                 contract.gemm_(self.wooa, self.woob, S, contract.lin(n), contract.lin(1), 1.0, 1.0, self.status)
             if Wa is not None:
                 if self.Ganti is None:
-                    self.Ganti = torch.empty_like(self.S)
+                    self.Ganti = torch.empty(self.S.shape, dtype=f64, device=self.S.device)
                 Uf = self.U.view(no * no, -1)
                 if Uf.dtype == f64:
                     torch.matmul(Wa.reshape(no * no, no * no).t(), Uf, out=self.Ganti.view(no * no, -1))
@@ -395,8 +414,10 @@ class T3Residual:
             r3 = torch.empty_like(t3)
         no, nv = self.no, self.nv
         S = self.s_(d, t3, inputs_ready, unpacked=unpacked)
-        sources = [(S, 1.0, full_strides(no, nv), ALL_S3)]  # S holds -Y already
-        perm_gather_(r3, d.ijk, nv, 0.0, sources, nocc=no, status=self.gstatus)
+        if S.dtype == torch.float32:  # S holds -Y already
+            s3_gather_f32_(r3, d.ijk, nv, 0.0, S, 1.0, no)
+        else:
+            perm_gather_(r3, d.ijk, nv, 0.0, [(S, 1.0, full_strides(no, nv), ALL_S3)], nocc=no, status=self.gstatus)
         if self.Ganti is not None:
             perm_gather_(r3, d.ijk, nv, 1.0, [(self.Ganti, 1.0, full_strides(no, nv), OOOO_SET)], nocc=no,
                          status=self.gstatus)

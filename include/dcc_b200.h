@@ -228,6 +228,13 @@ DCC_API int dcc_t3_perm_gather(double *r3, const int32_t *ijk, int64_t nblocks, 
 DCC_API int dcc_t3_perm_gather_tma(double *r3, const int32_t *ijk, int64_t nblocks, int64_t nocc, int64_t nvir,
                                    double beta, int nsrc, const double *const *bases, const double *scales,
                                    const int64_t *strides, const int *masks, int *status, void *stream);
+/* The S3 gather of compute_r3_tri's terms (distr_cc/rccsdt.py:385-396, 435-732, as the sum over
+ * the six simultaneous permutations of one full-layout tensor) from an FP32 S [nocc^3][nvir^3]:
+ *   r3[q][a,b,c] = beta r3 + scale sum_p S[p(ijk_q)][p(abc)],
+ * summed in FP64 in the order of dcc_t3_perm_gather_tma.  S is the split precisions' FP32
+ * accumulator of the residual's GEMMs (dcc_gemm_split3_ld4_f32c); nvir <= 104. */
+DCC_API int dcc_t3_s3_gather_f32(double *r3, const int32_t *ijk, int64_t nblocks, int64_t nocc, int64_t nvir,
+                                 double beta, const float *S, double scale, void *stream);
 
 /* ----------------------------------------------------------------------
  * Device DIIS (replaces the vector passes of distr_cc/diis.py:105-177 as
@@ -454,6 +461,14 @@ DCC_API int dcc_split_operand_at4_f32(const float *src, void *hi, void *lo, int6
 DCC_API int dcc_gemm_split3_ld4(const void *A_hi, const void *A_lo, int64_t lda, const void *B_hi, const void *B_lo,
                                 int64_t ldb, int64_t M, int64_t N, int64_t Kp, double *C, const int64_t *epi14,
                                 double alpha, double beta, int kind, int *status, void *stream);
+/* The same into an FP32 C: C[...] = fp32(alpha * acc + beta * C[...]) with the sum taken in FP64
+ * (one rounding per store).  The split precisions keep the residual's intermediate S
+ * (the _einsum accumulations of compute_r3_tri, distr_cc/rccsdt.py:385-396, 435-732) in FP32,
+ * like the products' own FP32 accumulation, which halves its epilogue traffic. */
+DCC_API int dcc_gemm_split3_ld4_f32c(const void *A_hi, const void *A_lo, int64_t lda, const void *B_hi,
+                                     const void *B_lo, int64_t ldb, int64_t M, int64_t N, int64_t Kp, float *C,
+                                     const int64_t *epi14, double alpha, double beta, int kind, int *status,
+                                     void *stream);
 
 /* Grouped split and grouped GEMM: every einsum of one (Q) task group
  * (distr_cc/rccsdt_q.py:390-408, :1014-1129; 132 `_einsum` calls per group,

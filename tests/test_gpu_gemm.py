@@ -112,6 +112,39 @@ def test_persistent_tiles_and_epilogue_orientation(C, kind, transposed):
 
 
 @pytest.mark.parametrize("kind", ["bf16x3", "tf32x3"])
+@pytest.mark.parametrize("transposed", [False, True])
+@pytest.mark.parametrize("beta", [0.0, -1.0])
+def test_fp32_output(C, kind, transposed, beta):
+    """An FP32 C (the split path's S accumulator): every element is the FP64 C's result for the
+    same inputs rounded once to FP32 (the epilogue sums in FP64 either way), in both epilogue
+    orientations, with beta = 0 (C never read) and beta != 0; a ragged M and N and K > 4096
+    (an FP32 C always takes the eight-warp epilogue)."""
+    for M, N, K in ((2000, 5000, 128), (333, 517, 4200)):
+        g = torch.Generator(device="cuda").manual_seed(M + N + K)
+        A = torch.randn(M, K, dtype=torch.float64, device="cuda", generator=g)
+        B = torch.randn(N, K, dtype=torch.float64, device="cuda", generator=g)
+        k = C.KIND[kind]
+        a = C.Split(M, K, k).fill(A, C.lin(K), C.lin(1))
+        b = C.Split(N, K, k).fill(B, C.lin(K), C.lin(1))
+        C0 = torch.randn(M * N, dtype=torch.float64, device="cuda", generator=g).float()
+        if beta == 0.0:
+            C0.fill_(float("nan"))  # never read
+        out32, out64 = C0.clone(), C0.double()
+        fr, fc = (C.lin(1), C.lin(M)) if transposed else (C.lin(N), C.lin(1))
+        st = C.gemm_(a, b, out32, fr, fc, 0.5, beta)
+        C.gemm_(a, b, out64, fr, fc, 0.5, beta, st)
+        torch.cuda.synchronize()
+        assert int(st.item()) == 0
+        assert torch.equal(out32, out64.float())
+        ref = 0.5 * (A @ B.t())
+        got = out64.view(N, M).t() if transposed else out64.view(M, N)
+        if beta != 0.0:
+            got = got - beta * (C0.view(N, M).t() if transposed else C0.view(M, N)).double()
+        # the FP32 accumulation error grows with K: the bar of the short cases, times 10 at K = 4200
+        assert _rel(got, ref) < TOL[kind] * (1 if K <= 1024 else 10)
+
+
+@pytest.mark.parametrize("kind", ["bf16x3", "tf32x3"])
 def test_concatenated_pieces_and_leading_columns(C, kind):
     """[A1 | A2] [B1 | B2]^T = A1 B1^T + A2 B2^T over a K-concatenated split, and a
     GEMM over the leading piece only (ldb > Kp) with an A that covers just that piece."""

@@ -125,6 +125,27 @@ def test_row_gather_matches_cp_async_gather(mods, no, nvir, beta):
     assert torch.equal(a, b)
 
 
+@pytest.mark.parametrize("no,nvir", [(1, 3), (2, 1), (3, 5), (3, 13), (2, 93), (2, 90), (2, 104)])
+@pytest.mark.parametrize("beta", [0.0, 0.75])
+def test_fp32_gather_matches_fp64_gather(mods, no, nvir, beta):
+    """The gather from an FP32 S (the split path's accumulator) equals the FP64 row gather over
+    the same values widened to FP64, bit for bit (the same FP64 sums in the same order)."""
+    syn, tr, er = mods
+    d = syn.make_inputs(no, nvir, seed=3, with_t3=False)
+    n3 = d.ijk.shape[0]
+    g = torch.Generator(device="cuda").manual_seed(nvir + 11 * no)
+    full = torch.randn((no ** 3, nvir, nvir, nvir), dtype=torch.float64, device="cuda", generator=g).float()
+    r0 = torch.randn((n3, nvir, nvir, nvir), dtype=torch.float64, device="cuda", generator=g)
+    a, b = r0.clone(), r0.clone()
+    st = torch.zeros(1, dtype=torch.int32, device="cuda")
+    tr.s3_gather_f32_(a, d.ijk, nvir, beta, full, -1.25, no)
+    tr.perm_gather_(b, d.ijk, nvir, beta, [(full.double(), -1.25, tr.full_strides(no, nvir), tr.ALL_S3)], nocc=no,
+                    status=st)
+    torch.cuda.synchronize()
+    assert int(st.item()) == 0
+    assert torch.equal(a, b)
+
+
 @pytest.mark.parametrize("precision", ["bf16x3", "tf32x3"])
 def test_autotuned_wvvvv_gemms(mods, precision):
     """T3Residual.tune times every pipeline candidate of the W_vvvv.t3 GEMMs (K = nvir^2 >
