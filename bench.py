@@ -267,8 +267,13 @@ def t3_line(torch, ranks, contract, nocc, nvir, precision, steps, warmup, track_
         from dcc import autotune
         info["wvvvv_gemm_pipeline"] = {
             "kb_bytes": tuned[0], "stages": tuned[1], "group_m": tuned[2], "chosen_by": "dcc.autotune",
-            "candidates_ms": {"%d/%d/%d" % c: round(ms, 4) for c, ms in
-                              (autotune.timings(it.res.wvvvv.key()) or {}).items()}}
+            "tile_n": tuned[3], "candidates_ms": {"%d/%d/%d/%d" % c: round(ms, 4) for c, ms in
+                                                  (autotune.timings(it.res.wvvvv.key()) or {}).items()}}
+        # the S GEMMs' tile width (128 x 256 or 128 x 128) and raster group, each tuned alone
+        info["s_gemm_tiles"] = {
+            name: {"chosen": "%d/%d/%d/%d" % cfg,
+                   "candidates_ms": {"%d/%d/%d/%d" % c: round(ms, 4) for c, ms in times.items()}}
+            for name, (cfg, times) in it.res.s_tuning().items()}
     w.start(it)
     if count_launches:
         from torch.profiler import profile, ProfilerActivity
@@ -698,6 +703,7 @@ def main():
         "device_status_ok": mix["status_ok"] and (f64["status_ok"] if f64 else True),
         "t3_finite": mix["t3_finite"],
         "wvvvv_gemm_pipeline": mix.get("wvvvv_gemm_pipeline"),
+        "s_gemm_tiles": mix.get("s_gemm_tiles"),
         "roofline": {"kernel": "dcc::k_gemm_split3<0> (W_vvvv.t3 string)", "bound": "tensor",
                      "achieved": achieved, "peak": peak_useful, "unit": "TFLOP/s",
                      "frac": (achieved / peak_useful) if achieved else None,

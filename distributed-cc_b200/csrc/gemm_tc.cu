@@ -39,9 +39,9 @@ constexpr int gemm_threads() { return 64 + 32 * EPI; }
 // 32 -> 128/64/32-byte swizzle), ring depth, and the number of M-tiles per
 // raster group (CTAs that run together share B tiles in L2).
 struct GemmConfig {
-    int kb_bytes, stages, group_m;
+    int kb_bytes, stages, group_m, tile_n;
 };
-static GemmConfig g_cfg = {64, 4, 16};
+static GemmConfig g_cfg = {64, 4, 16, 256};
 
 // Four-digit mixed-radix address map:
 //   off(m) = (m / (R1 R2 R3)) S0 + ((m / (R2 R3)) % R1) S1 + ((m / R3) % R2) S2 + (m % R3) S3.
@@ -153,14 +153,17 @@ __device__ __forceinline__ void tile_coords(int t, int num_m, int num_n, int gro
 }
 
 // Persistent: CTA c takes tiles c, c + gridDim.x, ... (linear ids rasterized
-// in groups of group_m M-tiles).  Two TMEM accumulators of GN columns let the
+// in groups of group_m M-tiles).  Two TMEM accumulators of TN columns let the
 // MMAs of tile t+1 run while the epilogue warps drain tile t.
 // KIND 0: bf16 pieces; KIND 1: tf32 pieces.  KB: bytes of K per row and
 // k-block; ST: ring depth.
 // CT: the storage type of C (double; float for the FP32 accumulators of the split precisions,
 // whose epilogue reads and writes half the bytes; the arithmetic stays FP64, one rounding per store).
-template <int KIND, int KB, int ST, int EPI, typename CT = double>
-__global__ void __launch_bounds__(gemm_threads<EPI>(), 1)
+// TN: tile columns (UMMA N), 256 or 128.  A 128-column tile holds half the TMEM (two accumulators
+// of 128 columns) and, with two stages of 64-byte k-blocks and four epilogue warps, half the
+// shared memory, so two CTAs share an SM.
+template <int KIND, int KB, int ST, int EPI, typename CT = double, int TN = GN>
+__global__ void __launch_bounds__(gemm_threads<EPI>(), TN == GN ? 1 : 2)
     k_gemm_split3(const __grid_constant__ CUtensorMap tmAh, const __grid_constant__ CUtensorMap tmAl,
                   const __grid_constant__ CUtensorMap tmBh, const __grid_constant__ CUtensorMap tmBl, int M, int N,
                   int nkb, CT *C, GemmEpi epi, double alpha, double beta, int *status, int group_m,
@@ -168,13 +171,13 @@ __global__ void __launch_bounds__(gemm_threads<EPI>(), 1)
     extern __shared__ __align__(1024) uint8_t g_smem[];
     // operand stages first (1024-byte aligned), then the epilogue buffers and the control block
     uint8_t *base = (uint8_t *)(((uintptr_t)g_smem + 1023) & ~(uintptr_t)1023);
-    constexpr uint32_t A_BYTES = GM * KB, B_BYTES = GN * KB;
+    constexpr uint32_t A_BYTES = GM * KB, B_BYTES = TN * KB;
     constexpr uint32_t STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;
     uint8_t *epi_base = base + ST * STAGE_BYTES;
     GemmSmem<ST> *cs = (GemmSmem<ST> *)(epi_base + EPI * EPI_WARP_BYTES);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int num_m = (M + GM - 1) / GM, num_n = (N + GN - 1) / GN, ntiles = num_m * num_n;
+    const int num_m = (M + GM - 1) / GM, num_n = (N + TN - 1) / TN, ntiles = num_m * num_n;
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < ST; s++) {
@@ -195,7 +198,7 @@ __global__ void __launch_bounds__(gemm_threads<EPI>(), 1)
     if (warp == 1) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
                          smem_u32(&cs->tmem_base)),
-                     "r"(2 * GN)
+                     "r"(2 * TN)
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
@@ -223,8 +226,8 @@ __global__ void __launch_bounds__(gemm_threads<EPI>(), 1)
                 const int kc = kb * (KB / (KIND == 0 ? 2 : 4));
                 tma_load_2d(smem_u32(st), &tmAh, fb, kc, tm * GM);
                 tma_load_2d(smem_u32(st + A_BYTES), &tmAl, fb, kc, tm * GM);
-                tma_load_2d(smem_u32(st + 2 * A_BYTES), &tmBh, fb, kc, tn * GN);
-                tma_load_2d(smem_u32(st + 2 * A_BYTES + B_BYTES), &tmBl, fb, kc, tn * GN);
+                tma_load_2d(smem_u32(st + 2 * A_BYTES), &tmBh, fb, kc, tn * TN);
+                tma_load_2d(smem_u32(st + 2 * A_BYTES + B_BYTES), &tmBl, fb, kc, tn * TN);
                 g++;
             }
         }
@@ -238,7 +241,7 @@ __global__ void __launch_bounds__(gemm_threads<EPI>(), 1)
         constexpr uint32_t idesc = (1u << 4)                          // D: f32
                                    | ((KIND == 0 ? 1u : 2u) << 7)     // A: bf16 | tf32
                                    | ((KIND == 0 ? 1u : 2u) << 10)    // B: bf16 | tf32
-                                   | ((uint32_t)(GN >> 3) << 17)      // N
+                                   | ((uint32_t)(TN >> 3) << 17)      // N
                                    | ((uint32_t)(GM >> 4) << 24);     // M
         constexpr int KSTEPS = KB / 32;  // one UMMA consumes 32 bytes of K
         uint32_t g = 0;
@@ -248,7 +251,7 @@ __global__ void __launch_bounds__(gemm_threads<EPI>(), 1)
             const int b = it & 1;
             if (!mbar_wait(smem_u32(&cs->acc_empty[b]), (((uint32_t)it >> 1) & 1u) ^ 1u, status)) break;
             tc_fence_after();
-            const uint32_t d = tmem + (uint32_t)(b * GN);
+            const uint32_t d = tmem + (uint32_t)(b * TN);
             for (int kb = 0; kb < nkb; kb++) {
                 const uint32_t s = g % ST, ph = (g / ST) & 1u;
                 if (!mbar_wait(smem_u32(&cs->full[s]), ph, status)) {
@@ -278,8 +281,8 @@ __global__ void __launch_bounds__(gemm_threads<EPI>(), 1)
     } else if (warp >= 2) {
         // ---------------- epilogue: TMEM -> FP64 C
         const int q = warp & 3;  // TMEM lane quarter of this warp
-        // EPI / 4 warps share a lane quarter, each draining GN * 4 / EPI columns
-        constexpr int CW = GN * 4 / EPI;
+        // EPI / 4 warps share a lane quarter, each draining TN * 4 / EPI columns
+        constexpr int CW = TN * 4 / EPI;
         const int cbeg = ((warp - 2) / 4) * CW, cend = cbeg + CW;
         float *stg = reinterpret_cast<float *>(epi_base + (warp - 2) * EPI_WARP_BYTES);
         int64_t *offs = reinterpret_cast<int64_t *>(epi_base + (warp - 2) * EPI_WARP_BYTES + 32 * 33 * 4);
@@ -292,7 +295,7 @@ __global__ void __launch_bounds__(gemm_threads<EPI>(), 1)
             tc_fence_after();
             int tm, tn;
             tile_coords(t, num_m, num_n, group_m, tm, tn);
-            const int m0 = tm * GM + q * 32, n0 = tn * GN;  // first row of this warp, first column of the tile
+            const int m0 = tm * GM + q * 32, n0 = tn * TN;  // first row of this warp, first column of the tile
             const int m = m0 + lane;
             const int64_t roff = map4_32(epi.row, (uint32_t)(m < M ? m : 0));
             const int nrow = (M - m0) < 32 ? (M - m0) : 32;
@@ -311,7 +314,7 @@ __global__ void __launch_bounds__(gemm_threads<EPI>(), 1)
                 }
                 // the chunk's accumulator columns; the warp's last load hands the accumulator back
                 auto load_acc = [&](int h, float (&v)[32]) {
-                    tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * GN + c + 32 * h), v);
+                    tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * TN + c + 32 * h), v);
                     if (c + 32 * (h + 1) == cend) {
                         tc_fence_before();
                         __syncwarp();
@@ -407,7 +410,7 @@ __global__ void __launch_bounds__(gemm_threads<EPI>(), 1)
     __syncthreads();
     if (warp == 1) {
         tc_fence_after();
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * GN) : "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * TN) : "memory");
     }
 }
 
@@ -956,13 +959,13 @@ static int make_map(CUtensorMap *map, const void *ptr, int kind, int64_t rows, i
     return DCC_OK;
 }
 
-template <int ST, int EPI>
+template <int ST, int EPI, int TN = GN>
 static size_t gemm_smem_bytes(int kb_bytes) {
-    return 1024 + ST * (size_t)(2 * GM * kb_bytes + 2 * GN * kb_bytes) + EPI * EPI_WARP_BYTES +
+    return 1024 + ST * (size_t)(2 * GM * kb_bytes + 2 * TN * kb_bytes) + EPI * EPI_WARP_BYTES +
            sizeof(GemmSmem<ST>);
 }
 
-template <int KIND, int KB, int ST, int EPI, typename CT = double>
+template <int KIND, int KB, int ST, int EPI, typename CT = double, int TN = GN>
 static int gemm_launch(const CUtensorMap &a, const CUtensorMap &b, const CUtensorMap &c, const CUtensorMap &d, int M,
                        int N, int nkb, CT *C, const GemmEpi &epi, double alpha, double beta, int *status,
                        int group_m, cudaStream_t st) {
@@ -972,15 +975,22 @@ static int gemm_launch(const CUtensorMap &a, const CUtensorMap &b, const CUtenso
     fast_digit(epi.col, cs, cr);
     fast_digit(epi.row, rs, rr);
     const int epi_cols = (cs == 1 || rs != 1) ? 1 : 0;
-    size_t smem = gemm_smem_bytes<ST, EPI>(KB);
-    const int64_t tiles = (int64_t)ceil_div(N, GN) * (int64_t)ceil_div(M, GM);
+    size_t smem = gemm_smem_bytes<ST, EPI, TN>(KB);
+    const int64_t tiles = (int64_t)ceil_div(N, TN) * (int64_t)ceil_div(M, GM);
     DCC_REQUIRE(tiles < (1ll << 31), DCC_ERR_SHAPE, "too many output tiles");
-    int dev = 0, nsm = 148;
+    int dev = 0, nsm = 148, per_sm = 1;
     if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    const unsigned grid = (unsigned)(tiles < nsm ? tiles : nsm);  // persistent: one CTA per SM
-    cudaFuncSetAttribute(k_gemm_split3<KIND, KB, ST, EPI, CT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k_gemm_split3<KIND, KB, ST, EPI, CT><<<grid, gemm_threads<EPI>(), smem, st>>>(a, b, c, d, M, N, nkb, C, epi, alpha,
-                                                                                 beta, status, group_m, epi_cols);
+    auto kern = k_gemm_split3<KIND, KB, ST, EPI, CT, TN>;
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    // persistent: as many CTAs as fit at once (one per SM for 256-column tiles, up to two for 128)
+    constexpr int max_per_sm = TN == GN ? 1 : 2;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, gemm_threads<EPI>(), smem) != cudaSuccess ||
+        per_sm < 1)
+        per_sm = 1;
+    per_sm = per_sm > max_per_sm ? max_per_sm : per_sm;
+    const int64_t cap = (int64_t)nsm * per_sm;
+    const unsigned grid = (unsigned)(tiles < cap ? tiles : cap);
+    kern<<<grid, gemm_threads<EPI>(), smem, st>>>(a, b, c, d, M, N, nkb, C, epi, alpha, beta, status, group_m, epi_cols);
     return launch_status("gemm_split3");
 }
 
@@ -1200,7 +1210,9 @@ static int gemm_split3(const void *A_hi, const void *A_lo, int64_t lda, const vo
     GemmEpi ep{map_from(epi, four), map_from(epi + (four ? 7 : 5), four)};
     DCC_REQUIRE(map_ok(ep.row) && map_ok(ep.col), DCC_ERR_SHAPE, "map radices must be >= 1 with products < 2^31");
     const GemmConfig cfg = g_cfg;
-    DCC_REQUIRE(Kp % (cfg.kb_bytes / (kind == 0 ? 2 : 4)) == 0, DCC_ERR_SHAPE,
+    // 128-column tiles have one pipeline for every K and C type: 64-byte k-blocks, 2 stages, 4 epilogue warps
+    const bool narrow = cfg.tile_n == 128;
+    DCC_REQUIRE(Kp % ((narrow ? 64 : cfg.kb_bytes) / (kind == 0 ? 2 : 4)) == 0, DCC_ERR_SHAPE,
                 "Kp (%lld) must be a multiple of the k-block", (long long)Kp);
     // Short contractions are bound by the FP64 epilogue: eight epilogue warps
     // (two per TMEM lane quarter) double its memory parallelism; the ring then
@@ -1208,15 +1220,31 @@ static int gemm_split3(const void *A_hi, const void *A_lo, int64_t lda, const vo
     const int esz = kind == 0 ? 2 : 4;
     // an FP32 C always takes the wide epilogue (its only instantiation)
     const bool wide_epi = Kp <= 4096 || c_f32;
-    const int kb = wide_epi ? 64 : cfg.kb_bytes;
+    const int kb = (wide_epi || narrow) ? 64 : cfg.kb_bytes;
+    const int tn = narrow ? 128 : GN;
     CUtensorMap mAh, mAl, mBh, mBl;
     int rc;
     if ((rc = make_map(&mAh, A_hi, kind, M, Kp, lda, GM, kb)) || (rc = make_map(&mAl, A_lo, kind, M, Kp, lda, GM, kb)) ||
-        (rc = make_map(&mBh, B_hi, kind, N, Kp, ldb, GN, kb)) || (rc = make_map(&mBl, B_lo, kind, N, Kp, ldb, GN, kb)))
+        (rc = make_map(&mBh, B_hi, kind, N, Kp, ldb, tn, kb)) || (rc = make_map(&mBl, B_lo, kind, N, Kp, ldb, tn, kb)))
         return rc;
     cudaStream_t st = as_stream(stream);
     const int nkb = (int)(Kp / (kb / esz));
     const int iM = (int)M, iN = (int)N, gm = cfg.group_m;
+    if (narrow) {
+        if (c_f32) {
+            float *Cf = (float *)C;
+            if (kind == 0)
+                return gemm_launch<0, 64, 2, 4, float, 128>(mAh, mAl, mBh, mBl, iM, iN, nkb, Cf, ep, alpha, beta, status,
+                                                            gm, st);
+            return gemm_launch<1, 64, 2, 4, float, 128>(mAh, mAl, mBh, mBl, iM, iN, nkb, Cf, ep, alpha, beta, status, gm,
+                                                        st);
+        }
+        double *Cn = (double *)C;
+        if (kind == 0)
+            return gemm_launch<0, 64, 2, 4, double, 128>(mAh, mAl, mBh, mBl, iM, iN, nkb, Cn, ep, alpha, beta, status, gm,
+                                                         st);
+        return gemm_launch<1, 64, 2, 4, double, 128>(mAh, mAl, mBh, mBl, iM, iN, nkb, Cn, ep, alpha, beta, status, gm, st);
+    }
     if (c_f32) {
         float *Cf = (float *)C;
         if (kind == 0) return gemm_launch<0, 64, 3, 8>(mAh, mAl, mBh, mBl, iM, iN, nkb, Cf, ep, alpha, beta, status, gm, st);
@@ -1397,21 +1425,34 @@ extern "C" int dcc_gemm_grouped(const void *table, int nprob, int64_t total_tile
     return launch_status("gemm_grouped");
 }
 
-extern "C" int dcc_gemm_set_config(int kb_bytes, int stages, int group_m) {
+extern "C" int dcc_gemm_set_tile_config(int kb_bytes, int stages, int group_m, int tile_n) {
     clear_error();
-    const bool ok = (kb_bytes == 128 && stages == 2) || (kb_bytes == 64 && (stages == 3 || stages == 4)) ||
-                    (kb_bytes == 32 && stages == 8);
-    DCC_REQUIRE(ok, DCC_ERR_UNSUPPORTED, "unsupported pipeline (k-block %d bytes, %d stages)", kb_bytes, stages);
+    DCC_REQUIRE(tile_n == 256 || tile_n == 128, DCC_ERR_UNSUPPORTED, "tile_n must be 256 or 128 (%d)", tile_n);
+    const bool ok = tile_n == 128 ? (kb_bytes == 64 && stages == 2)
+                                  : ((kb_bytes == 128 && stages == 2) || (kb_bytes == 64 && (stages == 3 || stages == 4)) ||
+                                     (kb_bytes == 32 && stages == 8));
+    DCC_REQUIRE(ok, DCC_ERR_UNSUPPORTED, "unsupported pipeline (k-block %d bytes, %d stages, %d-column tiles)", kb_bytes,
+                stages, tile_n);
     DCC_REQUIRE(group_m >= 1 && group_m <= 4096, DCC_ERR_SHAPE, "group_m must be in [1, 4096]");
-    dcc::g_cfg = dcc::GemmConfig{kb_bytes, stages, group_m};
+    dcc::g_cfg = dcc::GemmConfig{kb_bytes, stages, group_m, tile_n};
+    return DCC_OK;
+}
+
+extern "C" int dcc_gemm_set_config(int kb_bytes, int stages, int group_m) {
+    return dcc_gemm_set_tile_config(kb_bytes, stages, group_m, 256);
+}
+
+extern "C" int dcc_gemm_get_tile_config(int *kb_bytes, int *stages, int *group_m, int *tile_n) {
+    clear_error();
+    DCC_REQUIRE(kb_bytes && stages && group_m && tile_n, DCC_ERR_NULL, "NULL argument");
+    *kb_bytes = dcc::g_cfg.kb_bytes;
+    *stages = dcc::g_cfg.stages;
+    *group_m = dcc::g_cfg.group_m;
+    *tile_n = dcc::g_cfg.tile_n;
     return DCC_OK;
 }
 
 extern "C" int dcc_gemm_get_config(int *kb_bytes, int *stages, int *group_m) {
-    clear_error();
-    DCC_REQUIRE(kb_bytes && stages && group_m, DCC_ERR_NULL, "NULL argument");
-    *kb_bytes = dcc::g_cfg.kb_bytes;
-    *stages = dcc::g_cfg.stages;
-    *group_m = dcc::g_cfg.group_m;
-    return DCC_OK;
+    int tn = 0;
+    return dcc_gemm_get_tile_config(kb_bytes, stages, group_m, &tn);
 }

@@ -470,19 +470,22 @@ class WvvvvT3:
         return ("wvvvv_t3", self.n, self.nv, self.kind)
 
     def tune(self, scratch, W, t3, F=None):
-        """Pick the GEMM pipeline shape (k-block width, ring depth, raster group) of these
-        launches with the autotuner (dcc.autotune: every candidate timed on this problem);
-        the candidates accumulate into `scratch` (r3-shaped, contents discarded).  Later
-        calls apply the choice."""
+        """Pick the GEMM tile and pipeline shape (tile columns, k-block width, ring depth, raster
+        group) of these launches with the autotuner (dcc.autotune: every candidate timed on this
+        problem); the candidates accumulate into `scratch` (r3-shaped, contents discarded).
+        Later calls apply the choice."""
         from . import autotune
         return autotune.tune(self.key(), lambda: self(scratch, W, t3, F=F))
 
     def __call__(self, r3, W, t3, alpha=1.0, F=None):
         from . import autotune
-        nv = self.nv
         L.as_tensor(r3, f64, "r3")
         L.as_tensor(t3, f64, "t3")
-        autotune.use(self.key())
+        with autotune.applied(self.key()):
+            return self._run(r3, W, t3, alpha, F)
+
+    def _run(self, r3, W, t3, alpha, F):
+        nv = self.nv
         if F is None:
             ws = [self.W.fill(W.reshape(nv * nv, nv * nv), lin(nv * nv), lin(1))] * 3
         else:

@@ -239,6 +239,7 @@ class T3Residual:
         self.U = torch.empty(full, dtype=self.udtype, device=device) if with_oo else None
         self.Ganti = None
         self.gstatus = torch.zeros(1, dtype=torch.int32, device=device)  # gather pipeline timeouts
+        self._sargs = {}  # the S GEMMs' last arguments, by name (tune)
         if precision != "fp64":
             k = contract.KIND[precision]
             self.kind = k
@@ -267,6 +268,17 @@ class T3Residual:
                     self.woob = contract.Split(no * nv ** 3, kind=k, device=device, pieces=self.woo_pieces)
 
     # ------------------------------------------------------------ pieces
+    def _gemm(self, name, A, B, C, frow, fcol, alpha, beta, Kp=None):
+        """One of the S GEMMs under the tile and raster configuration tuned for it (tune()); its
+        arguments are kept so that tune() can time it alone."""
+        from . import autotune
+        self._sargs[name] = (A, B, C, frow, fcol, alpha, beta, Kp)
+        with autotune.applied(self._gkey(name)):
+            contract.gemm_(A, B, C, frow, fcol, alpha, beta, self.status, Kp=Kp)
+
+    def _gkey(self, name):
+        return ("s_gemm", name, self.no, self.nv, self.kind)
+
     def _y_into_s(self, d):
         """S = -Y in S's [i][j][k][a][b][c] layout (split path): rows (i,j,a), columns (k,b,c).  Y
         then rides in S's permutation sum, and the gather reads one source instead of two."""
@@ -274,8 +286,8 @@ class T3Residual:
         c = contract
         self.ya.fill(d.W_vooo, c.three(no, nv, no, 1, no ** 3), c.lin(no * no))
         self.yb.fill(d.t2, c.lin(1), c.lin(no * nv * nv))
-        c.gemm_(self.ya, self.yb, self.S, c.three(no, nv, no * no * nv ** 3, no * nv ** 3, nv * nv),
-                c.two(nv * nv, nv ** 3, 1), -1.0, 0.0, self.status)
+        self._gemm("y", self.ya, self.yb, self.S, c.three(no, nv, no * no * nv ** 3, no * nv ** 3, nv * nv),
+                   c.two(nv * nv, nv ** 3, 1), -1.0, 0.0)
 
     def unpack_(self, t3):
         """U = t3 unpacked to every ordered (i,j,k) (the operand of the OO terms)."""
@@ -314,7 +326,7 @@ class T3Residual:
                         self.wooa.fill_piece(i, A[:, k0:k0 + kk], contract.lin(no * no), contract.lin(1))
                         self.woob.fill_piece(i, Uf[k0:k0 + kk], contract.lin(1), contract.lin(n))
                         k0 += kk
-                contract.gemm_(self.wooa, self.woob, S, contract.lin(n), contract.lin(1), 1.0, 1.0, self.status)
+                self._gemm("woooo", self.wooa, self.woob, S, contract.lin(n), contract.lin(1), 1.0, 1.0)
             if Wa is not None:
                 if self.Ganti is None:
                     self.Ganti = torch.empty(self.S.shape, dtype=f64, device=self.S.device)
@@ -335,7 +347,7 @@ class T3Residual:
         self._y_into_s(d)  # writes S first
         self.xa.fill(d.W_vvvo, *x["a"][0][1:])
         self.xb.fill(d.t2, *x["b"][0][1:])
-        c.gemm_(self.xa, self.xb, S, *x["out"], x["alpha"], 1.0, st)
+        self._gemm("x", self.xa, self.xb, S, *x["out"], x["alpha"], 1.0)
         if not self.with_oo:
             return
         src = {"G2": (-0.5 * (d.W_ovov + d.W_ovvo.permute(0, 1, 3, 2))).permute(2, 1, 0, 3).contiguous(),
@@ -347,8 +359,8 @@ class T3Residual:
             self.oob.fill_piece(i, src[name], fm, fk)
         name, fm, fk = t1["a"][0]
         self.t1a.fill(src[name], fm, fk)
-        c.gemm_(self.ooa, self.oob, S, *oo["out"], oo["alpha"], oo["beta"], st)
-        c.gemm_(self.t1a, self.oob, S, *t1["out"], t1["alpha"], t1["beta"], st, Kp=self.t1a.Kp)
+        self._gemm("oo", self.ooa, self.oob, S, *oo["out"], oo["alpha"], oo["beta"])
+        self._gemm("t1", self.t1a, self.oob, S, *t1["out"], t1["alpha"], t1["beta"], Kp=self.t1a.Kp)
 
     def _s_fp64(self, d):
         """S in FP64 (cuBLAS DGEMM through torch), one occupied slice at a time so the
@@ -394,11 +406,29 @@ class T3Residual:
         return self.wvvvv(r3, d.W_vvvv, t3, F=d.F_vv)
 
     def tune(self, d, t3):
-        """Autotune the pipeline shape of the W_vvvv.t3 GEMMs (the split precisions; the
-        FP64 path has nothing to tune).  Returns the chosen (k-block bytes, stages, group)."""
+        """Autotune the split precisions' GEMMs (the FP64 path has nothing to tune): the tile width,
+        pipeline shape and raster group of the W_vvvv.t3 GEMMs, then the tile width and raster
+        group of each S GEMM, each timed alone on this problem (their operands from one pass of
+        s_ over d and t3; S is rebuilt by the next compute).  Returns the W_vvvv choice
+        (k-block bytes, stages, group, tile columns); s_tuning() lists the others."""
         if self.precision == "fp64":
             return None
-        return self.wvvvv.tune(torch.empty_like(t3), d.W_vvvv, t3, F=d.F_vv)
+        from . import autotune
+        best = self.wvvvv.tune(torch.empty_like(t3), d.W_vvvv, t3, F=d.F_vv)
+        self.s_(d, t3)
+        for name, (A, B, C, frow, fcol, alpha, beta, Kp) in self._sargs.items():
+            old = autotune.get_config()
+            autotune.tune(self._gkey(name),
+                          lambda: contract.gemm_(A, B, C, frow, fcol, alpha, beta, self.status, Kp=Kp),
+                          cands=autotune.tile_candidates())
+            autotune.set_config(*old)
+        return best
+
+    def s_tuning(self):
+        """{S GEMM: (chosen configuration, {candidate: ms})} after tune()."""
+        from . import autotune
+        return {name: (autotune.chosen(self._gkey(name)), autotune.timings(self._gkey(name)))
+                for name in self._sargs if autotune.timings(self._gkey(name)) is not None}
 
     def compute(self, d, t3, r3=None, wvvvv_ready=None, inputs_ready=None, unpacked=False):
         """r3 = compute_r3_tri for canonical t3 (the OO batch terms included when with_oo).

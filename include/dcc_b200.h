@@ -525,6 +525,12 @@ DCC_API int dcc_gemm_split3_ld(const void *A_hi, const void *A_lo, int64_t lda, 
  * (dcc.autotune) for each problem shape; no reference counterpart. */
 DCC_API int dcc_gemm_set_config(int kb_bytes, int stages, int group_m);
 DCC_API int dcc_gemm_get_config(int *kb_bytes, int *stages, int *group_m);
+/* The same with the output tile width: tile_n = 256 (128 x 256 tiles, one persistent CTA per
+ * SM; the pipelines above) or 128 (128 x 128 tiles, up to two CTAs per SM, 64-byte k-blocks,
+ * 2 stages, four epilogue warps, for every K and C type).  dcc_gemm_set_config sets
+ * tile_n = 256.  No reference counterpart. */
+DCC_API int dcc_gemm_set_tile_config(int kb_bytes, int stages, int group_m, int tile_n);
+DCC_API int dcc_gemm_get_tile_config(int *kb_bytes, int *stages, int *group_m, int *tile_n);
 
 #ifdef __cplusplus
 }

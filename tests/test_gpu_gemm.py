@@ -34,6 +34,16 @@ def _rel(a, b):
     return float((a - b).abs().max() / b.abs().max())
 
 
+@pytest.fixture(params=[256, 128])
+def tile(request, C):
+    """Run the test under 128 x 256 tiles (default pipeline) and 128 x 128 tiles (two CTAs per SM)."""
+    from dcc import autotune
+    old = autotune.get_config()
+    autotune.set_config(*((64, 4, 16, 256) if request.param == 256 else (64, 2, 16, 128)))
+    yield request.param
+    autotune.set_config(*old)
+
+
 @pytest.mark.parametrize("kind", ["bf16x3", "tf32x3"])
 @pytest.mark.parametrize("M,N,K", [(128, 256, 64), (300, 500, 200), (1000, 257, 1000), (7, 9, 5)])
 def test_matmul(C, kind, M, N, K):
@@ -67,7 +77,8 @@ def test_wvvvv_t3_matches_einsum(C, kind, nblk, nv):
     np.testing.assert_allclose(r64.cpu().numpy(), want, rtol=1e-12, atol=1e-15)
 
 
-@pytest.mark.parametrize("cfg", [(128, 2, 16), (64, 4, 16), (64, 3, 8), (32, 8, 32), (64, 4, 1)])
+@pytest.mark.parametrize("cfg", [(128, 2, 16), (64, 4, 16), (64, 3, 8), (32, 8, 32), (64, 4, 1), (64, 2, 16, 128),
+                                 (64, 2, 1, 128)])
 @pytest.mark.parametrize("kind", ["bf16x3", "tf32x3"])
 def test_every_pipeline_shape(C, cfg, kind):
     from dcc import autotune
@@ -89,7 +100,7 @@ def test_every_pipeline_shape(C, cfg, kind):
 
 @pytest.mark.parametrize("kind", ["bf16x3", "tf32x3"])
 @pytest.mark.parametrize("transposed", [False, True])
-def test_persistent_tiles_and_epilogue_orientation(C, kind, transposed):
+def test_persistent_tiles_and_epilogue_orientation(C, kind, transposed, tile):
     """More output tiles than two rounds of CTAs (both TMEM accumulators reused
     several times); beta != 0; output written row-contiguous (lanes along
     columns) or column-contiguous (lanes along rows)."""
@@ -114,7 +125,7 @@ def test_persistent_tiles_and_epilogue_orientation(C, kind, transposed):
 @pytest.mark.parametrize("kind", ["bf16x3", "tf32x3"])
 @pytest.mark.parametrize("transposed", [False, True])
 @pytest.mark.parametrize("beta", [0.0, -1.0])
-def test_fp32_output(C, kind, transposed, beta):
+def test_fp32_output(C, kind, transposed, beta, tile):
     """An FP32 C (the split path's S accumulator): every element is the FP64 C's result for the
     same inputs rounded once to FP32 (the epilogue sums in FP64 either way), in both epilogue
     orientations, with beta = 0 (C never read) and beta != 0; a ragged M and N and K > 4096

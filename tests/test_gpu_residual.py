@@ -161,9 +161,14 @@ def test_autotuned_wvvvv_gemms(mods, precision):
         cfg = res.tune(d, d.t3)
         assert cfg in autotune.candidates() and autotune.get_config() == cfg
         assert torch.equal(d.t3, t3_0)
-        autotune.set_config(*old)  # the residual re-applies its tuned shape itself
+        # every S GEMM was tuned over the tile widths and raster groups
+        chosen = res.s_tuning()
+        assert set(chosen) == {"y", "x", "oo", "t1", "woooo"}
+        assert all(c in autotune.tile_candidates() for c, _ in chosen.values())
+        autotune.set_config(*old)
         got = res.compute(d, d.t3)
-        assert autotune.get_config() == cfg and res.status_ok()
+        # the residual applies each tuned shape around its own launches and restores the previous one
+        assert autotune.get_config() == old and autotune.chosen(res.wvvvv.key()) == cfg and res.status_ok()
         want = tr.T3Residual(2, 72, "fp64", with_oo=True).compute(d, d.t3)
         assert float((got - want).abs().max() / want.abs().max()) < TOL[precision]
     finally:
