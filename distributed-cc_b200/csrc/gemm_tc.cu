@@ -131,6 +131,19 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
 
 // ----------------------------------------------------------------- kernel
 
+// Fire-and-forget reduction into global memory (red, no value returned; the L2 adds).  The
+// pointers may be generic addresses (the grouped GEMM's problem table), for which the compiler
+// would emit a returning generic atomic; name the global space here.
+__device__ __forceinline__ void red_add(float *p, float v) {
+    asm volatile("{\n\t.reg .u64 g;\n\tcvta.to.global.u64 g, %0;\n\tred.global.add.f32 [g], %1;\n\t}" ::"l"(p), "f"(v)
+                 : "memory");
+}
+__device__ __forceinline__ void red_add(double *p, double v) {
+    asm volatile("{\n\t.reg .u64 g;\n\tcvta.to.global.u64 g, %0;\n\tred.global.add.f64 [g], %1;\n\t}" ::"l"(p), "d"(v)
+                 : "memory");
+}
+
+
 template <int ST>
 struct GemmSmem {
     uint64_t full[ST];
@@ -300,6 +313,9 @@ __global__ void __launch_bounds__(gemm_threads<EPI>(), TN == GN ? 1 : 2)
             const int64_t roff = map4_32(epi.row, (uint32_t)(m < M ? m : 0));
             const int nrow = (M - m0) < 32 ? (M - m0) : 32;
             offs[lane] = roff;  // cols mode: row offsets of the warp's 32 rows
+            // an FP32 C with beta = 1 accumulates by L2 reductions (C += fp32(alpha acc)): no load
+            // round trip per element, the limit of the short-contraction epilogues
+            const bool redc = sizeof(CT) == 4 && beta == 1.0;
             // NCH 32-column chunks per step (two chunks' loads in flight measured no faster for an FP32
             // C: one chunk per step for either type)
             constexpr int NCH = 1;
@@ -329,7 +345,7 @@ __global__ void __launch_bounds__(gemm_threads<EPI>(), TN == GN ? 1 : 2)
 #pragma unroll
                     for (int h = 0; h < NCH; h++) full[h] = __all_sync(0xffffffffu, cval[h]) && nrow == 32;
                     CT old[NCH][32];
-                    if (beta != 0.0) {
+                    if (beta != 0.0 && !redc) {
 #pragma unroll
                         for (int h = 0; h < NCH; h++)
                             if (full[h]) {
@@ -345,7 +361,11 @@ __global__ void __launch_bounds__(gemm_threads<EPI>(), TN == GN ? 1 : 2)
                         for (int j = 0; j < 32; j++) stg[lane * 33 + j] = v[j];
                         __syncwarp();
                         CT *cp = C + coff[h];
-                        if (beta == 0.0) {
+                        if (redc) {
+                            const int nr = full[h] ? 32 : (cval[h] ? nrow : 0);
+#pragma unroll 8
+                            for (int r = 0; r < nr; r++) red_add(cp + offs[r], (CT)(alpha * (double)stg[r * 33 + lane]));
+                        } else if (beta == 0.0) {
                             if (full[h]) {
 #pragma unroll 8
                                 for (int r = 0; r < 32; r++) cp[offs[r]] = (CT)(alpha * (double)stg[r * 33 + lane]);
@@ -376,7 +396,7 @@ __global__ void __launch_bounds__(gemm_threads<EPI>(), TN == GN ? 1 : 2)
                     for (int h = 0; h < NCH; h++) nvalid[h] = N - n0 - c - 32 * h;
                     CT *rp = C + roff;
                     CT old[NCH][32];
-                    if (beta != 0.0 && m < M) {
+                    if (beta != 0.0 && !redc && m < M) {
 #pragma unroll
                         for (int h = 0; h < NCH; h++)
 #pragma unroll
@@ -388,7 +408,11 @@ __global__ void __launch_bounds__(gemm_threads<EPI>(), TN == GN ? 1 : 2)
                         float v[32];
                         load_acc(h, v);
                         if (m < M) {
-                            if (beta == 0.0) {
+                            if (redc) {
+#pragma unroll
+                                for (int j = 0; j < 32; j++)
+                                    if (j < nvalid[h]) red_add(rp + coffs[32 * h + j], (CT)(alpha * (double)v[j]));
+                            } else if (beta == 0.0) {
 #pragma unroll
                                 for (int j = 0; j < 32; j++)
                                     if (j < nvalid[h]) rp[coffs[32 * h + j]] = (CT)(alpha * (double)v[j]);
@@ -695,18 +719,6 @@ struct alignas(64) GemmProblem {
     int M, N, nkb, epi_cols;
     int num_m, num_n, out_f32, tile_begin;
 };
-
-// Fire-and-forget reduction into global memory (red, no value returned).  The
-// pointers come from the problem table as generic addresses, for which the
-// compiler would emit a returning generic atomic; name the global space here.
-__device__ __forceinline__ void red_add(float *p, float v) {
-    asm volatile("{\n\t.reg .u64 g;\n\tcvta.to.global.u64 g, %0;\n\tred.global.add.f32 [g], %1;\n\t}" ::"l"(p), "f"(v)
-                 : "memory");
-}
-__device__ __forceinline__ void red_add(double *p, double v) {
-    asm volatile("{\n\t.reg .u64 g;\n\tcvta.to.global.u64 g, %0;\n\tred.global.add.f64 [g], %1;\n\t}" ::"l"(p), "d"(v)
-                 : "memory");
-}
 
 // Tile t's problem: the last p with tile_begin <= t (tile_begin ascending).
 __device__ __forceinline__ int grouped_find(const int *tb, int nprob, int t) {

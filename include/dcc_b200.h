@@ -462,7 +462,9 @@ DCC_API int dcc_gemm_split3_ld4(const void *A_hi, const void *A_lo, int64_t lda,
                                 int64_t ldb, int64_t M, int64_t N, int64_t Kp, double *C, const int64_t *epi14,
                                 double alpha, double beta, int kind, int *status, void *stream);
 /* The same into an FP32 C: C[...] = fp32(alpha * acc + beta * C[...]) with the sum taken in FP64
- * (one rounding per store).  The split precisions keep the residual's intermediate S
+ * (one rounding per store); with beta = 1, C[...] += fp32(alpha * acc) by reductions in L2
+ * (red.global.add.f32: no load round trip; each element is written by one thread, so the
+ * result is deterministic).  The split precisions keep the residual's intermediate S
  * (the _einsum accumulations of compute_r3_tri, distr_cc/rccsdt.py:385-396, 435-732) in FP32,
  * like the products' own FP32 accumulation, which halves its epilogue traffic. */
 DCC_API int dcc_gemm_split3_ld4_f32c(const void *A_hi, const void *A_lo, int64_t lda, const void *B_hi,

@@ -124,12 +124,12 @@ def test_persistent_tiles_and_epilogue_orientation(C, kind, transposed, tile):
 
 @pytest.mark.parametrize("kind", ["bf16x3", "tf32x3"])
 @pytest.mark.parametrize("transposed", [False, True])
-@pytest.mark.parametrize("beta", [0.0, -1.0])
+@pytest.mark.parametrize("beta", [0.0, -1.0, 1.0])
 def test_fp32_output(C, kind, transposed, beta, tile):
-    """An FP32 C (the split path's S accumulator): every element is the FP64 C's result for the
-    same inputs rounded once to FP32 (the epilogue sums in FP64 either way), in both epilogue
-    orientations, with beta = 0 (C never read) and beta != 0; a ragged M and N and K > 4096
-    (an FP32 C always takes the eight-warp epilogue)."""
+    """An FP32 C (the split path's S accumulator): with beta = 0 (C never read) or beta = -1 every
+    element is the FP64 C's result for the same inputs rounded once to FP32 (the epilogue sums in
+    FP64); with beta = 1 the epilogue adds fp32(alpha acc) by L2 reductions, within two FP32
+    roundings of it.  Both epilogue orientations; a ragged M and N and K > 4096."""
     for M, N, K in ((2000, 5000, 128), (333, 517, 4200)):
         g = torch.Generator(device="cuda").manual_seed(M + N + K)
         A = torch.randn(M, K, dtype=torch.float64, device="cuda", generator=g)
@@ -146,7 +146,11 @@ def test_fp32_output(C, kind, transposed, beta, tile):
         C.gemm_(a, b, out64, fr, fc, 0.5, beta, st)
         torch.cuda.synchronize()
         assert int(st.item()) == 0
-        assert torch.equal(out32, out64.float())
+        if beta == 1.0:
+            scale = float(out64.abs().max())
+            assert float((out32.double() - out64).abs().max()) <= 2.0 ** -22 * scale
+        else:
+            assert torch.equal(out32, out64.float())
         ref = 0.5 * (A @ B.t())
         got = out64.view(N, M).t() if transposed else out64.view(M, N)
         if beta != 0.0:
