@@ -4,13 +4,14 @@ The reference loops over canonical blocks and every distinct ordering of
 each, taking the block (take_t3), symmetrizing it (P3_422 / P3_201) and
 issuing small einsums into r1, r2, W_vooo and W_vvvo.  Here:
 
-* r1 (distr_cc/rccsdt.py:270-293): V = P3_422 of every canonical block
-  (one batched kernel); the paired strings of each case collapse to
+* r1 (distr_cc/rccsdt.py:270-293): with V = P3_422 of every canonical block
+  the paired strings of each case collapse to
       r1[i] += c1 <E[j,k], V[a,b,c]>,  r1[j] += c2 <E[i,k], V[b,a,c]>,
       r1[k] += c3 <E[i,j], V[b,c,a]>       (sums over b, c; E = t1_eris[o,o,v,v])
   with (c1, c2, c3) = (1, 1, 1) for i<j<k, (1, 0, 1/2) for i=j<k,
   (1/2, 1, 0) for i<j=k (the 'cb,acb' partner of a 'bc,abc' string is the same
-  sum); three batched contractions, scattered to r1 by a one-hot product
+  sum); the permutations of V move onto E, so three batched GEMMs over t3 itself
+  give all three (no V pass), scattered to r1 by a one-hot product
   (deterministic).
 * r2, W_vooo, W_vvvo (distr_cc/rccsdt.py:300-316, 340-358): the distinct
   orderings of all canonical blocks are all ordered (x,y,z) once, so with X =
@@ -42,22 +43,38 @@ def _case_coefficients(ijk):
 
 def r1_add_t3_(r1, t1_eris, t3, ijk, nocc, oovv=None, V=None):
     """r1 += T3 part of r1 (distr_cc/rccsdt.py:262-296); t3 canonical blocks.  oovv: the
-    [o,o,v,v] slice of t1_eris when the caller passes the slice alone (t1_eris None);
-    V: a scratch buffer of t3's size."""
-    nvir = t3.shape[1]
-    V = torch.empty_like(t3) if V is None else V
-    _c_rccsdt.t3_spin_summation(t3, V, t3.shape[0], nvir, "P3_422", 1.0, 0.0)
+    [o,o,v,v] slice of t1_eris when the caller passes the slice alone (t1_eris None).
+
+    The reference contracts V = P3_422(t3) of each block with E = oovv slices:
+      Ra[a] = sum_bc E[j,k][b,c] V[a,b,c], Rb[a] = sum_bc E[i,k][b,c] V[b,a,c],
+      Rc[a] = sum_bc E[i,j][b,c] V[b,c,a],
+    with V[x,y,z] = 4 t[x,y,z] - 2 (t[z,y,x] + t[y,x,z] + t[x,z,y]) + t[y,z,x] + t[z,x,y].
+    Moving the permutations onto E, each R is a sum over the free position f of t3 of
+    y_f(M)[.] = t3 contracted with a matrix M over its other two positions, where M is
+    alpha E + beta E^T:
+      Ra = y0(4E1 - 2E1^T) + y1(-2E1 + E1^T) + y2(E1 - 2E1^T)
+      Rb = y0(-2E2 + E2^T) + y1(4E2 - 2E2^T) + y2(-2E2 + E2^T)
+      Rc = y0(E3 - 2E3^T) + y1(-2E3 + E3^T) + y2(4E3 - 2E3^T)
+    (E1 = E[j,k], E2 = E[i,k], E3 = E[i,j]), so three batched GEMMs with three right-hand sides
+    read t3 once each and V is never formed.  V: unused (kept for the callers' signature)."""
+    n, nvir = t3.shape[0], t3.shape[1]
     E = oovv if oovv is not None else eris_slices(t1_eris, None, nocc)["oovv"]
     il, jl, kl = ijk[:, 0].long(), ijk[:, 1].long(), ijk[:, 2].long()
     c1, c2, c3 = _case_coefficients(ijk)
-    # three batched matrix-vector products that read V in place (no permuted copy of V):
-    # Ra[q,a] = sum_bc E[q,b,c] V[q,a,b,c]; Rb[q,a] = sum_b (V[q,b] @ E[q,b])[a];
-    # Rc[q,a] = (E[q] as a row) @ V[q] as [(b,c)][a]
-    n = V.shape[0]
-    Ra = torch.bmm(V.view(n, nvir, nvir * nvir), E[jl, kl].reshape(n, nvir * nvir, 1)).view(n, nvir)
-    Rb = torch.bmm(V.view(n * nvir, nvir, nvir), E[il, kl].reshape(n * nvir, nvir, 1)).view(n, nvir, nvir).sum(1)
-    Rc = torch.bmm(E[il, jl].reshape(n, 1, nvir * nvir), V.view(n, nvir * nvir, nvir)).view(n, nvir)
-    Ra, Rb, Rc = Ra * c1[:, None], Rb * c2[:, None], Rc * c3[:, None]
+    E1, E2, E3 = E[jl, kl], E[il, kl], E[il, jl]  # [n][nvir][nvir]
+
+    def mix(a, b, M):
+        return a * M + b * M.transpose(1, 2)
+
+    # the matrices of the three free positions, one column per output (Ra, Rb, Rc)
+    G0 = torch.stack([mix(4.0, -2.0, E1), mix(-2.0, 1.0, E2), mix(1.0, -2.0, E3)], -1)  # over (y, z)
+    G1 = torch.stack([mix(-2.0, 1.0, E1), mix(4.0, -2.0, E2), mix(-2.0, 1.0, E3)], -1)  # over (x, z)
+    G2 = torch.stack([mix(1.0, -2.0, E1), mix(-2.0, 1.0, E2), mix(4.0, -2.0, E3)], -1)  # over (x, y)
+    nv2 = nvir * nvir
+    R = torch.bmm(t3.view(n, nvir, nv2), G0.reshape(n, nv2, 3))
+    R += torch.bmm(t3.view(n * nvir, nvir, nvir), G1.reshape(n * nvir, nvir, 3)).view(n, nvir, nvir, 3).sum(1)
+    R += torch.bmm(t3.view(n, nv2, nvir).transpose(1, 2), G2.reshape(n, nv2, 3))
+    Ra, Rb, Rc = R[..., 0] * c1[:, None], R[..., 1] * c2[:, None], R[..., 2] * c3[:, None]
     eye = torch.eye(nocc, dtype=f64, device=t3.device)
     r1 += eye[il].t() @ Ra + eye[jl].t() @ Rb + eye[kl].t() @ Rc
     return r1

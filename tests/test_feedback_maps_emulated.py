@@ -81,3 +81,25 @@ def test_split_feedback_maps(no, nv):
     want_wv = -e('zxde,xyzeba->abdy', E, X)
     for got, want in ((r2, want_r2), (Wo, want_wo), (Wv, want_wv)):
         np.testing.assert_allclose(got.numpy(), want.numpy(), rtol=0, atol=1e-12 * want.abs().max().item())
+
+
+@pytest.mark.parametrize("no,nv", [(3, 5), (4, 7), (5, 4)])
+def test_r1_without_v_pass(oracle, no, nv):
+    """r1's T3 part (distr_cc/rccsdt.py:262-296) from t3 directly: the permutations of V =
+    P3_422(t3) moved onto the ERI slices, three batched GEMMs over t3 (no library call, so it
+    runs here on CPU tensors), against the oracle's literal per-block loop.  1e-12 relative."""
+    import itertools
+    from oracle import feedback_ref
+    rng = np.random.default_rng(no * 10 + nv)
+    nmo = no + nv
+    g = rng.standard_normal((nmo,) * 4) * 0.1
+    fock = rng.standard_normal((nmo, nmo)) * 0.1
+    full = rng.standard_normal((no,) * 3 + (nv,) * 3)
+    U = sum(full.transpose(p + tuple(3 + x for x in p)) for p in itertools.permutations(range(3))) / 6
+    t3 = np.stack([U[i, j, k] for i in range(no) for j in range(i, no) for k in range(j, no)])
+    ijk = np.array([(i, j, k) for i in range(no) for j in range(i, no) for k in range(j, no)], dtype=np.int32)
+    r1, r2 = rng.standard_normal((no, nv)), rng.standard_normal((no, no, nv, nv))
+    want, _ = feedback_ref.r1r2_add_t3_ref(fock, g, r1.copy(), r2.copy(), t3, no, oracle)
+    got = torch.from_numpy(r1.copy())
+    fb.r1_add_t3_(got, torch.from_numpy(g), torch.from_numpy(t3), torch.from_numpy(ijk), no)
+    np.testing.assert_allclose(got.numpy(), want, rtol=0, atol=1e-12 * np.abs(want).max())
