@@ -326,7 +326,10 @@ class T3Residual:
                         self.wooa.fill_piece(i, A[:, k0:k0 + kk], contract.lin(no * no), contract.lin(1))
                         self.woob.fill_piece(i, Uf[k0:k0 + kk], contract.lin(1), contract.lin(n))
                         k0 += kk
-                self._gemm("woooo", self.wooa, self.woob, S, contract.lin(n), contract.lin(1), 1.0, 1.0)
+                # rows (k,abc) of U's split, columns (i,j): the nocc^2 (i,j) fill one 256-column tile
+                # instead of leaving the lane quarters of a second 128-row tile idle (nocc^2 = 225 rows
+                # at nocc=15, 36 at nocc=6), and each reduction of a warp covers 32 consecutive (k,abc)
+                self._gemm("woooo", self.woob, self.wooa, S, contract.lin(1), contract.lin(n), 1.0, 1.0)
             if Wa is not None:
                 if self.Ganti is None:
                     self.Ganti = torch.empty(self.S.shape, dtype=f64, device=self.S.device)
